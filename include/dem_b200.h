@@ -1,0 +1,297 @@
+/*
+ * dem_b200.h -- C ABI of the B200-native MFiX DEM particle step.
+ *
+ * This is the drop-in boundary for the DEM hot path of MFiX
+ * (model/des).  In the reference the path is a sequence of argument-less
+ * Fortran subroutines that share the module globals of `discretelement`
+ * and are called in order by DES_TIME_STEP (model/des/des_time_march.f:293-460).
+ * Each entry point below replaces one of those calls; a Fortran driver binds
+ * them through ISO_C_BINDING (see the INTEGRATION notes) and passes its own
+ * arrays, which keep their Fortran layout:
+ *
+ *   - per-particle vectors are (MAX_PIP,3) column-major: the x, y and z
+ *     columns are three contiguous blocks of MAX_PIP doubles;
+ *   - particle, pair and facet indices are 1-based at this boundary;
+ *   - PFT_NEIGHBOR is (3,P): the three components of one pair are adjacent.
+ *
+ * Every function returns 0 on success or a DEM_ERR_* code; dem_last_error()
+ * returns the message of the last failure on a handle.  Device state is
+ * resident and authoritative between calls; the host arrays stay owned by
+ * the caller and are only read or written inside upload/download calls.
+ * Calls on one handle must come from one host thread at a time.
+ */
+#ifndef DEM_B200_H
+#define DEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DEM_ABI_VERSION 1
+
+/* Maximum number of DEM solids phases (MFiX DIM_M is 10; DEM cases use few). */
+#define DEM_MAX_PHASES 8
+
+/* DES_COLL_MODEL_ENUM (model/des/discretelement_mod.f:196-200) */
+#define DEM_COLL_LSD    0
+#define DEM_COLL_HERTZ  1
+
+/* DES_INTG_METHOD (model/des/discretelement_mod.f:205-207) */
+#define DEM_INTG_EULER  0
+#define DEM_INTG_AB2    1
+
+/* Contact-force arithmetic. FP64 reproduces CALC_FORCE_DEM in double
+ * precision with the serial reference's summation order.  SPLIT computes the
+ * relative displacement, overlap and forces in FP32 from FP64 positions,
+ * accumulates with compensated FP32 sums, and keeps FP64 integration and
+ * FP64 tangential history. */
+#define DEM_PREC_FP64   0
+#define DEM_PREC_SPLIT  1
+
+/* PARTICLE_STATE values (model/des/discretelement_mod.f:70-78) */
+#define DEM_STATE_NONEXISTENT   0
+#define DEM_STATE_NORMAL        1
+#define DEM_STATE_ENTERING      2
+#define DEM_STATE_EXITING       3
+#define DEM_STATE_RIGID         10
+#define DEM_STATE_NORMAL_GHOST  101
+
+/* Error codes */
+#define DEM_OK                   0
+#define DEM_ERR_ARG              1   /* bad argument or size */
+#define DEM_ERR_CUDA             2   /* a CUDA call failed */
+#define DEM_ERR_ZERO_DISTANCE    3   /* two particle centres coincide (calc_force_dem.f:267-271) */
+#define DEM_ERR_PAIR_OVERFLOW    4   /* pair list capacity exceeded; call again after growth */
+#define DEM_ERR_WALL_SLOTS       5   /* more than COLLISION_ARRAY_MAX wall contacts on a particle */
+#define DEM_ERR_ROGUE            6   /* NORMAL particle in a ghost cell with remove_rogue = 0 */
+#define DEM_ERR_NONFINITE        7   /* NaN/Inf found in particle state */
+#define DEM_ERR_STATE            8   /* call out of order (e.g. step before upload) */
+#define DEM_ERR_TIMEOUT          9   /* a bounded host wait expired */
+#define DEM_ERR_CAPACITY        10   /* a fixed-size buffer is too small */
+
+/*
+ * Parameters.  These mirror the DES namelist keywords and the derived
+ * tables that CHECK_SOLIDS_DEM computes (model/check_data/check_solids_dem.f:
+ * 519-782 for LSD, 798-1122 for Hertz) and the DES grid that DESGRID_INIT
+ * builds (model/des/desgrid_mod.f:506-865) for a single rank.  Phase tables
+ * are (M,L) row-major with stride DEM_MAX_PHASES, 0-based phases.
+ */
+typedef struct dem_params {
+    int32_t n_phases;            /* DES_MMAX */
+    int32_t coll_model;          /* DEM_COLL_* */
+    int32_t intg_method;         /* DEM_INTG_* */
+    int32_t neighbor_search_n;   /* NEIGHBOR_SEARCH_N */
+    int32_t force_precision;     /* DEM_PREC_* */
+    int32_t remove_rogue;        /* REMOVE_ROGUE_PARTICLES */
+    int32_t no_k;                /* 2-D case (NO_K) */
+    int32_t periodic[3];         /* DES_PERIODIC_WALLS_X/Y/Z */
+    int32_t dg_imax, dg_jmax, dg_kmax;   /* interior DES grid cells per axis */
+    int32_t collision_array_max; /* wall-history slots per particle (COLLISION_ARRAY_MAX, default 8) */
+    int32_t reserved_i[6];
+
+    double factor_rlm;           /* FACTOR_RLM (its default is the REAL(4) literal 1.2) */
+    double dtsolid;              /* DTSOLID */
+    double grav[3];              /* GRAV */
+    double kn, kt, kn_w, kt_w;   /* LSD spring constants */
+    double mew, mew_w;           /* sliding friction, particle-particle and particle-wall */
+    double mew_r, mew_rw;        /* rolling friction */
+    double max_radius;           /* MAX_RADIUS */
+    double dg_xstart, dg_ystart, dg_zstart;  /* DES grid origin (dg_xstart...) */
+    double dg_dxinv, dg_dyinv, dg_dzinv;     /* inverse DES cell widths */
+    double domain_lo[3];         /* X_MIN, Y_MIN, Z_MIN */
+    double domain_hi[3];         /* X_MAX, Y_MAX, Z_MAX */
+    double des_etan[DEM_MAX_PHASES * DEM_MAX_PHASES];  /* particle-agnostic damping */
+    double des_etat[DEM_MAX_PHASES * DEM_MAX_PHASES];
+    double hert_kn[DEM_MAX_PHASES * DEM_MAX_PHASES];   /* Hertz spring factors / sqrt(R_eff) */
+    double hert_kt[DEM_MAX_PHASES * DEM_MAX_PHASES];
+    double des_etan_wall[DEM_MAX_PHASES];
+    double des_etat_wall[DEM_MAX_PHASES];
+    double hert_kwn[DEM_MAX_PHASES];
+    double hert_kwt[DEM_MAX_PHASES];
+    double reserved_d[8];
+} dem_params;
+
+/* Statistics (model/des/des_granular_temperature.f:33-267 and the contact
+ * count of calc_force_dem.f:740-801). */
+typedef struct dem_stats {
+    int64_t n_normal;        /* NORMAL particles */
+    int64_t n_pairs;         /* half-list pairs (entries of NEIGHBORS) */
+    int64_t n_contacts;      /* pairs in contact at the last force evaluation */
+    int64_t n_wall_contacts; /* particle-facet contacts at the last force evaluation */
+    int64_t n_rogue_removed; /* particles deleted as rogue so far */
+    int64_t steps_done;      /* DES_TIME_STEP calls executed on this handle */
+    double  mean_vel[3];     /* mean particle velocity (NORMAL particles) */
+    double  gran_temp[3];    /* <(v - <v>)^2> per component */
+    double  kinetic_energy;  /* sum 0.5 m v^2 */
+    double  max_overlap_ratio; /* max overlap / R_LM over contacts */
+    double  bed_height;      /* mass-weighted mean y of NORMAL particles */
+    double  s_time;          /* accumulated solids time S_TIME */
+    double  reserved[4];
+} dem_stats;
+
+typedef struct dem_handle dem_handle;
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+/* Allocates device state for max_pip particles (MAX_PIP) on the current CUDA
+ * device.  Replaces the DES allocation in des_allocate_mod.f and the constant
+ * set-up of CHECK_SOLIDS_DEM (the derived tables are taken from *p). */
+int dem_create(const dem_params* p, int32_t max_pip, dem_handle** out);
+int dem_destroy(dem_handle* h);
+const char* dem_last_error(const dem_handle* h);
+int dem_abi_version(void);
+
+/* ---- geometry ---------------------------------------------------------- */
+
+/* Wall facets: VERTEX(3,3,F) and NORM_FACE(3,F) of cartesian_grid/stl_mod.f:21-23
+ * in Fortran layout (vertex[v + 3*c + 9*f]).  Bins them to the DES grid as
+ * BIN_FACETS_TO_DG (model/des/stl_preproc_des_mod.f:135-203, TRI_BOX_OVERLAP
+ * in stl_functions_des_mod.f:280-536) and flags edges shared by near-coplanar
+ * facets as FLAG_FACETS_WHERE_EDGE_COLLISION_IS_IGNORED (stl_preproc_des_mod.f:
+ * 361-490) does.  n_facets may be 0. */
+int dem_set_walls(dem_handle* h, const double* vertex, const double* norm_face,
+                  int32_t n_facets);
+
+/* ---- particle state ---------------------------------------------------- */
+
+/* Copies the DES arrays in: DES_POS_NEW, DES_VEL_NEW, OMEGA_NEW (max_pip,3),
+ * DES_RADIUS, PMASS, OMOI (max_pip), PARTICLE_STATE (int8) and the 1-based
+ * solids phase PIJK(:,5). (model/des/discretelement_mod.f:387-391,579-588) */
+int dem_upload_state(dem_handle* h, const double* pos, const double* vel,
+                     const double* omega, const double* radius,
+                     const double* pmass, const double* omoi,
+                     const int8_t* state, const int32_t* phase, int32_t max_pip);
+
+/* Copies DES_POS_NEW, DES_VEL_NEW, OMEGA_NEW and PARTICLE_STATE out.
+ * Any pointer may be NULL to skip that array. */
+int dem_download_state(dem_handle* h, double* pos, double* vel, double* omega,
+                       int8_t* state, int32_t max_pip);
+
+/* FC and TOW (max_pip,3) as left by the last dem_calc_force call. */
+int dem_download_forces(dem_handle* h, double* fc, double* tow, int32_t max_pip);
+
+/* The Adams-Bashforth history DES_ACC_OLD / ROT_ACC_OLD (max_pip,3) and the
+ * CFNEWVALUES first-pass flag, for restart hand-over. */
+int dem_set_ab2_history(dem_handle* h, const double* acc_old,
+                        const double* rot_acc_old, int32_t first_pass, int32_t max_pip);
+int dem_get_ab2_history(dem_handle* h, double* acc_old, double* rot_acc_old,
+                        int32_t max_pip);
+
+/* ---- pair list ----------------------------------------------------------- */
+
+/* Number of entries in NEIGHBORS after the last build. */
+int dem_pair_count(dem_handle* h, int64_t* n_pairs);
+
+/* NEIGHBOR_INDEX(max_pip) (1-based end pointers: row LL spans
+ * NEIGHBOR_INDEX(LL-1) .. NEIGHBOR_INDEX(LL)-1, row 1 starts at 1),
+ * NEIGHBORS(P) (1-based particle indices) and PFT_NEIGHBOR(3,P), in the order
+ * of the serial reference build (desgrid_mod.f:1002-1299).  Any output pointer
+ * may be NULL. capacity is the length of neighbors (pft holds 3*capacity). */
+int dem_download_pairs(dem_handle* h, int32_t* neighbor_index, int32_t* neighbors,
+                       double* pft, int64_t capacity, int32_t max_pip);
+
+/* Installs a pair list with tangential history (restart / hand-over from the
+ * CPU solver, write_res0_des.f:177-182).  The rows must be a valid half list. */
+int dem_upload_pairs(dem_handle* h, const int32_t* neighbor_index,
+                     const int32_t* neighbors, const double* pft,
+                     int64_t n_pairs, int32_t max_pip);
+
+/* Wall tangential history WALL_COLLISION_FACET_ID(cmax, max_pip) (1-based
+ * facet ids, -1 free) and WALL_COLLISION_PFT(3, cmax, max_pip)
+ * (model/des/discretelement_mod.f:637-642). */
+int dem_download_wall_history(dem_handle* h, int32_t* facet_id, double* pft,
+                              int32_t max_pip);
+
+/* ---- per-stage entry points (one per reference call site) ----------------- */
+
+/* DESGRID_PIC(.TRUE.) (desgrid_mod.f:877-995): cell of every particle and the
+ * per-cell particle lists, and for periodic axes the wrap of particles that
+ * crossed a periodic face (the self-exchange of DES_PAR_EXCHANGE). */
+int dem_desgrid_pic(dem_handle* h);
+
+/* DG_PIJK(max_pip), 1-based DES cell of each particle (0 for nonexistent). */
+int dem_download_cells(dem_handle* h, int32_t* dg_pijk, int32_t max_pip);
+
+/* NEIGHBOUR (neighbour.f:21-126): rebuild the pair list with
+ * DESGRID_NEIGH_BUILD and carry the tangential history over. */
+int dem_neighbour(dem_handle* h);
+
+/* CALC_FORCE_DEM (calc_force_dem.f:18-544) including the wall contacts
+ * CALC_DEM_FORCE_WITH_WALL_STL (calc_collision_wall_mod.f:54-794).
+ * Leaves FC and TOW on the device. */
+int dem_calc_force(dem_handle* h);
+
+/* CFUPDATEOLD + CFNEWVALUES (cfupdateold.f:15-46, cfnewvalues.f:641-864):
+ * integrates with FC/TOW and zeroes them. */
+int dem_cfnewvalues(dem_handle* h);
+
+/* MAKE_ARRAYS_DES tail (make_arrays_des.f:348-406): DESGRID_PIC + NEIGHBOUR
+ * on the uploaded positions. */
+int dem_init_neighbors(dem_handle* h);
+
+/* DES_TIME_STEP(NN) for NN = nn_first .. nn_first+nsteps-1 of a pure DEM
+ * run (des_time_march.f:293-460): force, integrate, and the rebuild when
+ * NN == 1 or mod(NN, NEIGHBOR_SEARCH_N) == 0.  Force and integration run as
+ * one fused kernel; the result is identical to dem_calc_force followed by
+ * dem_cfnewvalues. */
+int dem_step(dem_handle* h, int32_t nn_first, int32_t nsteps);
+
+/* Statistics of the current state. */
+int dem_get_stats(dem_handle* h, dem_stats* out);
+
+/* Number of kernels this handle has launched so far (for launch accounting). */
+int dem_launch_count(const dem_handle* h, int64_t* count);
+
+/* Sets the CUDA stream (cudaStream_t passed as void*) used by the handle.
+ * NULL selects the legacy default stream. */
+int dem_set_stream(dem_handle* h, void* stream);
+
+/* Per-step force error of the split-precision path: max over particles of
+ * |F_split - F_fp64| / max|F_fp64| for the current state (both computed,
+ * nothing integrated). */
+int dem_force_error(dem_handle* h, double* rel_err);
+
+/* ---- CFD-DEM coupling (model/des/drag_gs_des0.f, comp_mean_fields0.f) ---- */
+
+/* Fluid grid description for the coupled step.  Uniform Cartesian grid of
+ * imax x jmax x kmax interior cells starting at domain_lo with widths dx,dy,dz;
+ * MFiX's IJK includes one ghost layer on every side. */
+typedef struct dem_fluid_grid {
+    int32_t imax, jmax, kmax;
+    int32_t drag_model;          /* 0 = GIDASPOW (drag_gs.f:536-598) */
+    double dx, dy, dz;
+    double ro_g, mu_g;           /* gas density and viscosity (uniform) */
+    double ep_star;              /* packed-bed void fraction EP_STAR (for ep_s max) */
+    double ur_f_gs;              /* under-relaxation of F_GP (drag_gp_des.f), usually 1 */
+    double reserved[6];
+} dem_fluid_grid;
+
+/* Installs the fluid grid and the gas fields on fluid cells (including
+ * ghosts; (imax+2)*(jmax+2)*(kmax+2) values each in MFiX IJK order):
+ * EP_G, U_G, V_G, W_G (staggered face velocities), and P_FORCE (3, ncells)
+ * (may be NULL for zero). */
+int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid* g,
+                       const double* ep_g, const double* u_g, const double* v_g,
+                       const double* w_g, const double* p_force);
+
+/* Reads the mean fields of the last deposition: EP_G and ROP_S per fluid cell. */
+int dem_get_mean_fields(dem_handle* h, double* ep_g, double* rop_s);
+
+/* PARTICLES_IN_CELL + COMP_MEAN_FIELDS0 + CALC_EPG_DES. */
+int dem_comp_mean_fields(dem_handle* h);
+
+/* DRAG_GS_DES0 with GARG_2012 interpolation: adds the drag to FC.  Call after
+ * dem_calc_force and before dem_cfnewvalues. */
+int dem_drag_gs_des0(dem_handle* h);
+
+/* One coupled DES_TIME_STEP sequence: force, drag, integrate, rebuild if due,
+ * particles-in-cell and mean fields. */
+int dem_step_coupled(dem_handle* h, int32_t nn_first, int32_t nsteps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DEM_B200_H */

@@ -1,0 +1,192 @@
+"""ctypes mirror of include/dem_b200.h (structs, constants, signatures).
+
+The structures here must match the C header field for field; the tests check
+sizeof() against the library's own view through dem_abi_version and a
+round-trip of dem_params.
+"""
+import ctypes as C
+
+DEM_ABI_VERSION = 1
+DEM_MAX_PHASES = 8
+
+DEM_COLL_LSD = 0
+DEM_COLL_HERTZ = 1
+DEM_INTG_EULER = 0
+DEM_INTG_AB2 = 1
+DEM_PREC_FP64 = 0
+DEM_PREC_SPLIT = 1
+
+DEM_STATE_NONEXISTENT = 0
+DEM_STATE_NORMAL = 1
+DEM_STATE_ENTERING = 2
+DEM_STATE_EXITING = 3
+DEM_STATE_RIGID = 10
+DEM_STATE_NORMAL_GHOST = 101
+
+DEM_OK = 0
+DEM_ERR_ARG = 1
+DEM_ERR_CUDA = 2
+DEM_ERR_ZERO_DISTANCE = 3
+DEM_ERR_PAIR_OVERFLOW = 4
+DEM_ERR_WALL_SLOTS = 5
+DEM_ERR_ROGUE = 6
+DEM_ERR_NONFINITE = 7
+DEM_ERR_STATE = 8
+DEM_ERR_TIMEOUT = 9
+DEM_ERR_CAPACITY = 10
+
+ERROR_NAMES = {
+    0: "DEM_OK", 1: "DEM_ERR_ARG", 2: "DEM_ERR_CUDA", 3: "DEM_ERR_ZERO_DISTANCE",
+    4: "DEM_ERR_PAIR_OVERFLOW", 5: "DEM_ERR_WALL_SLOTS", 6: "DEM_ERR_ROGUE",
+    7: "DEM_ERR_NONFINITE", 8: "DEM_ERR_STATE", 9: "DEM_ERR_TIMEOUT",
+    10: "DEM_ERR_CAPACITY",
+}
+
+_M2 = DEM_MAX_PHASES * DEM_MAX_PHASES
+
+
+class DemParams(C.Structure):
+    _fields_ = [
+        ("n_phases", C.c_int32),
+        ("coll_model", C.c_int32),
+        ("intg_method", C.c_int32),
+        ("neighbor_search_n", C.c_int32),
+        ("force_precision", C.c_int32),
+        ("remove_rogue", C.c_int32),
+        ("no_k", C.c_int32),
+        ("periodic", C.c_int32 * 3),
+        ("dg_imax", C.c_int32),
+        ("dg_jmax", C.c_int32),
+        ("dg_kmax", C.c_int32),
+        ("collision_array_max", C.c_int32),
+        ("reserved_i", C.c_int32 * 6),
+        ("factor_rlm", C.c_double),
+        ("dtsolid", C.c_double),
+        ("grav", C.c_double * 3),
+        ("kn", C.c_double),
+        ("kt", C.c_double),
+        ("kn_w", C.c_double),
+        ("kt_w", C.c_double),
+        ("mew", C.c_double),
+        ("mew_w", C.c_double),
+        ("mew_r", C.c_double),
+        ("mew_rw", C.c_double),
+        ("max_radius", C.c_double),
+        ("dg_xstart", C.c_double),
+        ("dg_ystart", C.c_double),
+        ("dg_zstart", C.c_double),
+        ("dg_dxinv", C.c_double),
+        ("dg_dyinv", C.c_double),
+        ("dg_dzinv", C.c_double),
+        ("domain_lo", C.c_double * 3),
+        ("domain_hi", C.c_double * 3),
+        ("des_etan", C.c_double * _M2),
+        ("des_etat", C.c_double * _M2),
+        ("hert_kn", C.c_double * _M2),
+        ("hert_kt", C.c_double * _M2),
+        ("des_etan_wall", C.c_double * DEM_MAX_PHASES),
+        ("des_etat_wall", C.c_double * DEM_MAX_PHASES),
+        ("hert_kwn", C.c_double * DEM_MAX_PHASES),
+        ("hert_kwt", C.c_double * DEM_MAX_PHASES),
+        ("reserved_d", C.c_double * 8),
+    ]
+
+
+class DemStats(C.Structure):
+    _fields_ = [
+        ("n_normal", C.c_int64),
+        ("n_pairs", C.c_int64),
+        ("n_contacts", C.c_int64),
+        ("n_wall_contacts", C.c_int64),
+        ("n_rogue_removed", C.c_int64),
+        ("steps_done", C.c_int64),
+        ("mean_vel", C.c_double * 3),
+        ("gran_temp", C.c_double * 3),
+        ("kinetic_energy", C.c_double),
+        ("max_overlap_ratio", C.c_double),
+        ("bed_height", C.c_double),
+        ("s_time", C.c_double),
+        ("reserved", C.c_double * 4),
+    ]
+
+    def as_dict(self):
+        d = {}
+        for name, _ in self._fields_:
+            if name == "reserved":
+                continue
+            v = getattr(self, name)
+            d[name] = list(v) if hasattr(v, "__len__") else v
+        return d
+
+
+class DemFluidGrid(C.Structure):
+    _fields_ = [
+        ("imax", C.c_int32),
+        ("jmax", C.c_int32),
+        ("kmax", C.c_int32),
+        ("drag_model", C.c_int32),
+        ("dx", C.c_double),
+        ("dy", C.c_double),
+        ("dz", C.c_double),
+        ("ro_g", C.c_double),
+        ("mu_g", C.c_double),
+        ("ep_star", C.c_double),
+        ("ur_f_gs", C.c_double),
+        ("reserved", C.c_double * 6),
+    ]
+
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I32 = C.POINTER(C.c_int32)
+_I8 = C.POINTER(C.c_int8)
+
+# name -> (restype, argtypes); prefix is substituted ("dem_" or "orc_")
+SIGNATURES = {
+    "create": (C.c_int, [C.POINTER(DemParams), C.c_int32, C.POINTER(C.c_void_p)]),
+    "destroy": (C.c_int, [_P]),
+    "last_error": (C.c_char_p, [_P]),
+    "set_walls": (C.c_int, [_P, _D, _D, C.c_int32]),
+    "upload_state": (C.c_int, [_P, _D, _D, _D, _D, _D, _D, _I8, _I32, C.c_int32]),
+    "download_state": (C.c_int, [_P, _D, _D, _D, _I8, C.c_int32]),
+    "download_forces": (C.c_int, [_P, _D, _D, C.c_int32]),
+    "set_ab2_history": (C.c_int, [_P, _D, _D, C.c_int32, C.c_int32]),
+    "get_ab2_history": (C.c_int, [_P, _D, _D, C.c_int32]),
+    "pair_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "download_pairs": (C.c_int, [_P, _I32, _I32, _D, C.c_int64, C.c_int32]),
+    "upload_pairs": (C.c_int, [_P, _I32, _I32, _D, C.c_int64, C.c_int32]),
+    "download_wall_history": (C.c_int, [_P, _I32, _D, C.c_int32]),
+    "download_cells": (C.c_int, [_P, _I32, C.c_int32]),
+    "desgrid_pic": (C.c_int, [_P]),
+    "neighbour": (C.c_int, [_P]),
+    "calc_force": (C.c_int, [_P]),
+    "cfnewvalues": (C.c_int, [_P]),
+    "init_neighbors": (C.c_int, [_P]),
+    "step": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "get_stats": (C.c_int, [_P, C.POINTER(DemStats)]),
+    "set_gas_fields": (C.c_int, [_P, C.POINTER(DemFluidGrid), _D, _D, _D, _D, _D]),
+    "get_mean_fields": (C.c_int, [_P, _D, _D]),
+    "comp_mean_fields": (C.c_int, [_P]),
+    "drag_gs_des0": (C.c_int, [_P]),
+    "step_coupled": (C.c_int, [_P, C.c_int32, C.c_int32]),
+}
+
+# entry points only the CUDA library has
+DEM_ONLY = {
+    "abi_version": (C.c_int, []),
+    "launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "set_stream": (C.c_int, [_P, C.c_void_p]),
+    "force_error": (C.c_int, [_P, C.POINTER(C.c_double)]),
+}
+
+
+def bind(lib, prefix, extra=None):
+    """Set restype/argtypes for every entry point present in `lib`."""
+    table = dict(SIGNATURES)
+    if extra:
+        table.update(extra)
+    for name, (res, args) in table.items():
+        fn = getattr(lib, prefix + name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib

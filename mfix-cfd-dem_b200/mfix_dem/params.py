@@ -1,0 +1,414 @@
+"""Keyword-level set-up of a DEM case: the derived tables MFiX computes before
+the DEM loop, restated for the host side of this library.
+
+A Fortran driver already holds these values in its module globals and passes
+them to dem_create().  Python users build them here from the same keywords:
+
+- reference particle size/mass per phase, GET_REF_PARTICLE_SIZE_AND_MASS
+  (model/check_data/check_solids_dem.f:1135-1223);
+- LSD and Hertz spring/damping tables and DTSOLID, CHECK_SOLIDS_DEM_COLL_LSD
+  (check_solids_dem.f:519-782) and CHECK_SOLIDS_DEM_COLL_HERTZ (798-1122);
+- DES grid sizing, CHECK_GEOMETRY (model/check_data/check_geometry.f:133-190)
+  and DESGRID_INIT (model/des/desgrid_mod.f:571-604, 833-850);
+- particle mass and inverse moment of inertia, MAKE_ARRAYS_DES
+  (model/des/make_arrays_des.f:241-244).
+
+Keyword defaults follow model/des/des_init_namelist.f.  Several of them are
+REAL(4) literals in the reference and are reproduced as such (float32 values
+widened to double): FACTOR_RLM = 1.2 (line 1169) and KT_FAC = KT_W_FAC =
+0.28571428571429 (lines 1215, 1237).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import abi
+
+PI = 4.0 * math.atan(1.0)          # parse_line.f:563
+UNDEFINED = 9.87654321e31          # param1_mod.f:20
+FLT_HUGE = float(np.finfo(np.float32).max)
+
+
+def f32(x: float) -> float:
+    """A Fortran default-REAL literal widened to DOUBLE PRECISION."""
+    return float(np.float32(x))
+
+
+FACTOR_RLM_DEFAULT = f32(1.2)
+KT_FAC_DEFAULT = f32(0.28571428571429)
+
+
+def xpow3(x):
+    """x**3.0d0 through the reference's pow wrapper (model/xpow.c): an
+    integral exponent 3 is evaluated by binary powering as x*(x*x)."""
+    return x * (x * x)
+
+
+@dataclass
+class DemCase:
+    """The DEM keywords of one case (des_init_namelist.f names in comments)."""
+    n_phases: int = 1
+    d_p0: Sequence[float] = (1e-3,)             # D_P0(M)
+    ro_s0: Sequence[float] = (2500.0,)          # RO_S0(M)
+    coll_model: str = "LSD"                      # DES_COLL_MODEL
+    intg_method: str = "EULER"                   # DES_INTG_METHOD
+    kn: float = UNDEFINED                        # KN
+    kn_w: float = UNDEFINED                      # KN_W
+    kt_fac: Optional[float] = None               # KT_FAC (default f32 2/7)
+    kt_w_fac: Optional[float] = None             # KT_W_FAC
+    des_etat_fac: Optional[float] = None         # DES_ETAT_FAC (default 1/2)
+    des_etat_w_fac: Optional[float] = None       # DES_ETAT_W_FAC
+    des_en_input: Optional[np.ndarray] = None    # (M,M) restitution
+    des_en_wall_input: Optional[Sequence[float]] = None
+    des_et_input: Optional[np.ndarray] = None    # Hertz tangential restitution
+    des_et_wall_input: Optional[Sequence[float]] = None
+    e_young: Sequence[float] = ()                # E_YOUNG(M)
+    v_poisson: Sequence[float] = ()              # V_POISSON(M)
+    ew_young: float = UNDEFINED                  # Ew_YOUNG
+    vw_poisson: float = UNDEFINED                # Vw_POISSON
+    mew: float = 0.0                             # MEW
+    mew_w: float = 0.0                           # MEW_W
+    mew_r: float = 0.0                           # MEW_R
+    mew_rw: float = 0.0                          # MEW_RW
+    grav: Sequence[float] = (0.0, -9.81, 0.0)    # GRAVITY_X/Y/Z
+    domain_lo: Sequence[float] = (0.0, 0.0, 0.0)
+    domain_hi: Sequence[float] = (1.0, 1.0, 1.0)
+    fluid_cells: Sequence[int] = (1, 1, 1)       # IMAX, JMAX, KMAX
+    no_k: bool = False
+    periodic: Sequence[bool] = (False, False, False)
+    desgridsearch: Sequence[Optional[int]] = (None, None, None)
+    neighbor_search_n: int = 25                  # NEIGHBOR_SEARCH_N
+    factor_rlm: float = FACTOR_RLM_DEFAULT       # FACTOR_RLM
+    dtsolid_factor: float = 50.0                 # DTSOLID_FACTOR
+    dtsolid: Optional[float] = None              # DTSOLID (None = derived)
+    collision_array_max: int = 8                 # COLLISION_ARRAY_MAX
+    remove_rogue: bool = True                    # REMOVE_ROGUE_PARTICLES
+    force_precision: int = abi.DEM_PREC_FP64
+
+
+def particle_props(radius: np.ndarray, rho: np.ndarray):
+    """PVOL, PMASS, OMOI as MAKE_ARRAYS_DES computes them
+    (make_arrays_des.f:241-244): PVOL = (4/3)*PI*R**3.0d0, PMASS = PVOL*RO,
+    OMOI = 2.5/(PMASS*R**2)."""
+    radius = np.asarray(radius, dtype=np.float64)
+    pvol = ((4.0 / 3.0) * PI) * xpow3(radius)
+    pmass = pvol * np.asarray(rho, dtype=np.float64)
+    with np.errstate(divide="ignore"):
+        omoi = 2.5 / (pmass * (radius * radius))
+    return pvol, pmass, omoi
+
+
+def ref_size_and_mass(case: DemCase, radius, pmass, phase, state):
+    """GET_REF_PARTICLE_SIZE_AND_MASS (check_solids_dem.f:1135-1223): the
+    minimum of the phase's nominal and actual NORMAL particle sizes/masses.
+    `phase` is 1-based."""
+    M = case.n_phases
+    ref_r = np.zeros(M)
+    ref_m = np.zeros(M)
+    for m in range(M):
+        d = case.d_p0[m]
+        ref_r[m] = 0.5 * d
+        ref_m[m] = (PI / 6.0) * (d * d * d) * case.ro_s0[m]
+    normal = np.asarray(state) == abi.DEM_STATE_NORMAL
+    ph = np.asarray(phase) - 1
+    for m in range(M):
+        sel = normal & (ph == m)
+        if sel.any():
+            ref_r[m] = min(ref_r[m], float(np.min(radius[sel])))
+            ref_m[m] = min(ref_m[m], float(np.min(pmass[sel])))
+    return ref_r, ref_m
+
+
+def _sym(x, M, name):
+    if x is None:
+        raise ValueError(f"Required input not specified: {name}")
+    a = np.asarray(x, dtype=np.float64)
+    if a.ndim == 0:
+        return np.full((M, M), float(a))
+    return a
+
+
+def contact_constants(case: DemCase, ref_r, ref_m, p: abi.DemParams):
+    """Fills the contact tables of `p` and returns TCOLL.
+
+    LSD: check_solids_dem.f:519-782.  Hertz: check_solids_dem.f:798-1122.
+    Tables are stored in the particle-agnostic form the force routines use.
+    """
+    M, S = case.n_phases, abi.DEM_MAX_PHASES
+    en = _sym(case.des_en_input, M, "DES_EN_INPUT")
+    enw = np.asarray(case.des_en_wall_input if case.des_en_wall_input is not None
+                     else [None] * M, dtype=object)
+    if any(v is None for v in enw):
+        raise ValueError("Required input not specified: DES_EN_WALL_INPUT")
+    enw = enw.astype(np.float64)
+    tcoll = UNDEFINED
+    if case.coll_model.upper() == "LSD":
+        if case.kn == UNDEFINED or case.kn_w == UNDEFINED:
+            raise ValueError("Required input not specified: KN / KN_W")
+        kt_fac = KT_FAC_DEFAULT if case.kt_fac is None else case.kt_fac
+        kt_w_fac = KT_FAC_DEFAULT if case.kt_w_fac is None else case.kt_w_fac
+        etat_fac = 0.5 if case.des_etat_fac is None else case.des_etat_fac
+        etat_w_fac = 0.5 if case.des_etat_w_fac is None else case.des_etat_w_fac
+        p.kn, p.kn_w = case.kn, case.kn_w
+        p.kt = kt_fac * case.kn
+        p.kt_w = kt_w_fac * case.kn_w
+        for m in range(M):
+            mass_m = ref_m[m]
+            for l in range(m, M):
+                e = en[m, l]
+                mass_l = ref_m[l]
+                meff = mass_m * mass_l / (mass_m + mass_l)
+                if e != 0.0:
+                    etan = 2.0 * math.sqrt(case.kn * meff) * abs(math.log(e))
+                    etan = etan / math.sqrt(PI * PI + (math.log(e) * math.log(e)))
+                    tc = PI / math.sqrt(case.kn / meff - ((etan / meff) * (etan / meff)) / 4.0)
+                else:
+                    etan = 2.0 * math.sqrt(case.kn * meff)
+                    tc = PI / math.sqrt(case.kn / meff)
+                tcoll = min(tc, tcoll)
+                etan = etan / math.sqrt(meff)
+                p.des_etan[m * S + l] = p.des_etan[l * S + m] = etan
+                p.des_etat[m * S + l] = p.des_etat[l * S + m] = etat_fac * etan
+            e = enw[m]
+            meff = mass_m
+            if e != 0.0:
+                etan = 2.0 * math.sqrt(case.kn_w * meff) * abs(math.log(e))
+                etan = etan / math.sqrt(PI * PI + (math.log(e) * math.log(e)))
+            else:
+                etan = 2.0 * math.sqrt(case.kn_w * meff)
+            etan = etan / math.sqrt(meff)
+            p.des_etan_wall[m] = etan
+            p.des_etat_wall[m] = etat_w_fac * etan
+    elif case.coll_model.upper() == "HERTZ":
+        et = _sym(case.des_et_input, M, "DES_ET_INPUT")
+        if case.des_et_wall_input is None:
+            raise ValueError("Required input not specified: DES_ET_WALL_INPUT")
+        etw = np.asarray(case.des_et_wall_input, dtype=np.float64)
+        if case.ew_young == UNDEFINED or case.vw_poisson == UNDEFINED:
+            raise ValueError("Required input not specified: Ew_YOUNG / Vw_POISSON")
+        E = np.asarray(case.e_young, dtype=np.float64)
+        nu = np.asarray(case.v_poisson, dtype=np.float64)
+        gw = 0.5 * case.ew_young / (1.0 + case.vw_poisson)
+        G = [0.5 * E[m] / (1.0 + nu[m]) for m in range(M)]
+        for m in range(M):
+            mass_m = ref_m[m]
+            for l in range(m, M):
+                e, t = en[m, l], et[m, l]
+                mass_l = ref_m[l]
+                meff = (mass_m * mass_l) / (mass_m + mass_l)
+                red = (2.0 / 7.0) * meff
+                reff = ref_r[m] * ref_r[l] / (ref_r[m] + ref_r[l])
+                eeff = E[m] * E[l] / (E[m] * (1.0 - nu[l] * nu[l]) + E[l] * (1.0 - nu[m] * nu[m]))
+                geff = G[m] * G[l] / (G[m] * (2.0 - nu[l]) + G[l] * (2.0 - nu[m]))
+                hkn = (4.0 / 3.0) * math.sqrt(reff) * eeff
+                hkt = 8.0 * math.sqrt(reff) * geff
+                if e != 0.0:
+                    etan = math.sqrt(5.0) * math.sqrt(hkn * meff) * abs(math.log(e))
+                    etan = etan / math.sqrt(PI * PI + (math.log(e) * math.log(e)))
+                    tc = PI / math.sqrt(hkn / meff - ((etan / meff) * (etan / meff)) / 5.0)
+                else:
+                    etan = math.sqrt(5.0) * math.sqrt(hkn * meff)
+                    tc = PI / math.sqrt(hkn / meff)
+                if t != 0.0:
+                    etat = math.sqrt(5.0) * math.sqrt(hkt * red) * abs(math.log(t))
+                    etat = etat / math.sqrt(PI * PI + (math.log(t) * math.log(t)))
+                else:
+                    etat = math.sqrt(5.0) * math.sqrt(hkt * red)
+                tcoll = min(tc, tcoll)
+                etan = etan / math.sqrt(hkn * meff)
+                etat = etat / math.sqrt(hkt * meff)
+                hkn = hkn / math.sqrt(reff)
+                hkt = hkt / math.sqrt(reff)
+                p.hert_kn[m * S + l] = p.hert_kn[l * S + m] = hkn
+                p.hert_kt[m * S + l] = p.hert_kt[l * S + m] = hkt
+                p.des_etan[m * S + l] = p.des_etan[l * S + m] = etan
+                p.des_etat[m * S + l] = p.des_etat[l * S + m] = etat
+            e, t = enw[m], etw[m]
+            meff = mass_m
+            red = (2.0 / 7.0) * meff
+            reff = ref_r[m]
+            eeff = E[m] * case.ew_young / (E[m] * (1.0 - case.vw_poisson * case.vw_poisson)
+                                          + case.ew_young * (1.0 - nu[m] * nu[m]))
+            geff = G[m] * gw / (G[m] * (2.0 - case.vw_poisson) + gw * (2.0 - nu[m]))
+            hkwn = (4.0 / 3.0) * math.sqrt(reff) * eeff
+            hkwt = 8.0 * math.sqrt(reff) * geff
+            if e != 0.0:
+                etan = math.sqrt(5.0) * math.sqrt(hkwn * meff) * abs(math.log(e))
+                etan = etan / math.sqrt(PI * PI + (math.log(e) * math.log(e)))
+            else:
+                etan = math.sqrt(5.0) * math.sqrt(hkwn * meff)
+            if t != 0.0:
+                etat = math.sqrt(5.0) * math.sqrt(hkwt * red) * abs(math.log(t))
+                etat = etat / math.sqrt(PI * PI + (math.log(t) * math.log(t)))
+            else:
+                etat = math.sqrt(5.0) * math.sqrt(hkwt * red)
+            p.des_etan_wall[m] = etan / math.sqrt(hkwn * meff)
+            p.des_etat_wall[m] = etat / math.sqrt(hkwt * meff)
+            p.hert_kwn[m] = hkwn / math.sqrt(reff)
+            p.hert_kwt[m] = hkwt / math.sqrt(reff)
+    else:
+        raise ValueError(f"unknown DES_COLL_MODEL {case.coll_model}")
+    return tcoll
+
+
+def desgrid_geometry(case: DemCase, max_radius: float):
+    """DES grid cells per axis and origin/inverse width for one rank.
+
+    CHECK_GEOMETRY (check_geometry.f:133-190): WIDTH = 3*max diameter, capped
+    by the smallest fluid cell; DESGRIDSEARCH_?MAX = max(int(LENGTH/WIDTH),1)
+    unless given.  DESGRID_INIT (desgrid_mod.f:833-850): dg_xstart is the west
+    face of the first interior fluid cell and dg_dxinv = cells/(xend-xstart),
+    with xend accumulated face by face over the fluid cells.
+    """
+    max_diam = 2.0 * max_radius
+    width = 3.0 * max_diam
+    lo, hi = case.domain_lo, case.domain_hi
+    ncell, starts, invs = [], [], []
+    for ax in range(3):
+        length = hi[ax] - lo[ax]
+        nfl = case.fluid_cells[ax]
+        dfl = length / nfl
+        if ax == 2 and case.no_k:
+            ncell.append(1)
+            starts.append(lo[2])
+            invs.append(1.0 / (hi[2] - lo[2]))
+            continue
+        w = min(width, dfl)
+        n = case.desgridsearch[ax]
+        if n is None:
+            n = max(int(length / w), 1)
+        if length / float(n) < max_diam:
+            raise ValueError("The des search grid is too fine (cell smaller than the max diameter)")
+        xend = lo[ax]
+        for _ in range(nfl):
+            xend = xend + dfl
+        ncell.append(n)
+        starts.append(lo[ax])
+        invs.append(n / (xend - lo[ax]))
+    return ncell, starts, invs
+
+
+def build_params(case: DemCase, radius, pmass, phase, state):
+    """dem_params for a case, plus a dict of derived scalars (tcoll, ...)."""
+    p = abi.DemParams()
+    M = case.n_phases
+    if not (1 <= M <= abi.DEM_MAX_PHASES):
+        raise ValueError("n_phases out of range")
+    p.n_phases = M
+    p.coll_model = abi.DEM_COLL_HERTZ if case.coll_model.upper() == "HERTZ" else abi.DEM_COLL_LSD
+    intg = case.intg_method.upper()
+    p.intg_method = abi.DEM_INTG_AB2 if intg in ("ADAMS_BASHFORTH", "AB2") else abi.DEM_INTG_EULER
+    p.neighbor_search_n = case.neighbor_search_n
+    p.force_precision = case.force_precision
+    p.remove_rogue = 1 if case.remove_rogue else 0
+    p.no_k = 1 if case.no_k else 0
+    for a in range(3):
+        p.periodic[a] = 1 if case.periodic[a] else 0
+        p.grav[a] = case.grav[a]
+        p.domain_lo[a] = case.domain_lo[a]
+        p.domain_hi[a] = case.domain_hi[a]
+    p.collision_array_max = case.collision_array_max
+    p.factor_rlm = case.factor_rlm
+    p.mew, p.mew_w, p.mew_r, p.mew_rw = case.mew, case.mew_w, case.mew_r, case.mew_rw
+
+    # MAX_RADIUS: largest nominal radius (check_solids_common_discrete.f:176-181)
+    max_radius = max(0.5 * d for d in case.d_p0[:M])
+    normal = np.asarray(state) == abi.DEM_STATE_NORMAL
+    if normal.any():
+        max_radius = max(max_radius, float(np.max(np.asarray(radius)[normal])))
+    p.max_radius = max_radius
+
+    ref_r, ref_m = ref_size_and_mass(case, np.asarray(radius), np.asarray(pmass), phase, state)
+    tcoll = contact_constants(case, ref_r, ref_m, p)
+    p.dtsolid = case.dtsolid if case.dtsolid is not None else tcoll / case.dtsolid_factor
+
+    ncell, starts, invs = desgrid_geometry(case, max_radius)
+    p.dg_imax, p.dg_jmax, p.dg_kmax = ncell
+    p.dg_xstart, p.dg_ystart, p.dg_zstart = starts
+    p.dg_dxinv, p.dg_dyinv, p.dg_dzinv = invs
+    for ax in range(3):
+        if case.periodic[ax] and ncell[ax] < 3:
+            raise ValueError("periodic axes need at least 3 DES grid cells")
+    return p, {"tcoll": tcoll, "ref_radius": ref_r, "ref_mass": ref_m, "max_radius": max_radius}
+
+
+# ---------------------------------------------------------------------------
+# Wall geometry in the Fortran layout VERTEX(3,3,F), NORM_FACE(3,F).
+
+def _facets(tris, norms):
+    F = len(tris)
+    vertex = np.zeros((F, 3, 3))   # [f, c, v] -> offset v + 3c + 9f
+    norm = np.zeros((F, 3))
+    for f, (t, nrm) in enumerate(zip(tris, norms)):
+        for v in range(3):
+            for c in range(3):
+                vertex[f, c, v] = t[v][c]
+        norm[f] = nrm
+    return vertex, norm
+
+
+def default_walls(lo, hi, periodic=(False, False, False), no_k=False):
+    """CONVERT_DEFAULT_WALLS_TO_STL (stl_preproc_des_mod.f:973-1046): one large
+    triangle per non-periodic domain face, normals pointing into the domain."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    xl, yl, zl = x1 - x0, y1 - y0, z1 - z0
+    tris, norms = [], []
+    if not periodic[0]:
+        tris.append([(x0, y0, z0), (x0, y1 + yl, z0), (x0, y0, z1 + zl)]); norms.append((1.0, 0.0, 0.0))
+        tris.append([(x1, y0, z0), (x1, y1 + yl, z0), (x1, y0, z1 + zl)]); norms.append((-1.0, 0.0, 0.0))
+    if not periodic[1]:
+        tris.append([(x0, y0, z0), (x1 + xl, y0, z0), (x0, y0, z1 + zl)]); norms.append((0.0, 1.0, 0.0))
+        tris.append([(x0, y1, z0), (x1 + xl, y1, z0), (x0, y1, z1 + zl)]); norms.append((0.0, -1.0, 0.0))
+    if not periodic[2] and not no_k:
+        tris.append([(x0, y0, z0), (x1 + xl, y0, z0), (x0, y1 + yl, z0)]); norms.append((0.0, 0.0, 1.0))
+        tris.append([(x0, y0, z1), (x1 + xl, y0, z1), (x0, y1 + yl, z1)]); norms.append((0.0, 0.0, -1.0))
+    return _facets(tris, norms)
+
+
+def hopper_walls(lo, hi, half_angle_deg=30.0, outlet_diam=0.012, y_cone_top=None,
+                 n_seg=64):
+    """Box walls plus a conical hopper bottom, triangulated.
+
+    Side walls are the default box faces above the cone; the cone runs from
+    the box's inscribed circle at y_cone_top down to an outlet of diameter
+    outlet_diam, with its axis along y through the box centre.  The bottom
+    face is left open below the outlet (particles that leave are removed as
+    rogue by the neighbour build).  Normals point into the particle region.
+    """
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    cx, cz = 0.5 * (x0 + x1), 0.5 * (z0 + z1)
+    R = 0.5 * min(x1 - x0, z1 - z0)
+    r_out = 0.5 * outlet_diam
+    t = math.tan(math.radians(half_angle_deg))
+    h_cone = (R - r_out) / t
+    y_out = y0 + 0.05 * (y1 - y0) if y_cone_top is None else y_cone_top - h_cone
+    y_top = y_out + h_cone
+    xl, yl, zl = x1 - x0, y1 - y0, z1 - z0
+    tris, norms = [], []
+    # side walls (x and z faces) and top
+    tris.append([(x0, y0, z0), (x0, y1 + yl, z0), (x0, y0, z1 + zl)]); norms.append((1.0, 0.0, 0.0))
+    tris.append([(x1, y0, z0), (x1, y1 + yl, z0), (x1, y0, z1 + zl)]); norms.append((-1.0, 0.0, 0.0))
+    tris.append([(x0, y1, z0), (x1 + xl, y1, z0), (x0, y1, z1 + zl)]); norms.append((0.0, -1.0, 0.0))
+    tris.append([(x0, y0, z0), (x1 + xl, y0, z0), (x0, y1 + yl, z0)]); norms.append((0.0, 0.0, 1.0))
+    tris.append([(x0, y0, z1), (x1 + xl, y0, z1), (x0, y1 + yl, z1)]); norms.append((0.0, 0.0, -1.0))
+    # cone: n_seg quads -> 2 triangles each
+    ca, sa = math.cos(math.radians(half_angle_deg)), math.sin(math.radians(half_angle_deg))
+    for s in range(n_seg):
+        a0 = 2 * math.pi * s / n_seg
+        a1 = 2 * math.pi * (s + 1) / n_seg
+        am = 0.5 * (a0 + a1)
+        P0t = (cx + R * math.cos(a0), y_top, cz + R * math.sin(a0))
+        P1t = (cx + R * math.cos(a1), y_top, cz + R * math.sin(a1))
+        P0b = (cx + r_out * math.cos(a0), y_out, cz + r_out * math.sin(a0))
+        P1b = (cx + r_out * math.cos(a1), y_out, cz + r_out * math.sin(a1))
+        # inward normal: points toward the axis and up
+        nrm = (-ca * math.cos(am), sa, -ca * math.sin(am))
+        tris.append([P0b, P1b, P1t]); norms.append(nrm)
+        tris.append([P0b, P1t, P0t]); norms.append(nrm)
+    return _facets(tris, norms), {"y_out": y_out, "y_top": y_top, "r_out": r_out, "R": R}

@@ -1,0 +1,238 @@
+"""Host-side mirror of the DES_TIME_STEP call sequence over the C ABI.
+
+`DemSystem` wraps one dem_handle of the CUDA library (include/dem_b200.h).
+Its methods are named after the reference routines they replace
+(model/des/des_time_march.f:293-460) and take/return numpy arrays in the
+Fortran layouts of the DES arrays: per-particle vectors are (3, MAX_PIP)
+arrays whose memory is the (MAX_PIP,3) column-major Fortran array, indices
+are 1-based where the reference stores indices.
+
+The same class drives any library that exports the ABI under another
+prefix (the test suite points it at the CPU restatement with prefix "orc_").
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+
+
+class DemError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        self.code = code
+        name = abi.ERROR_NAMES.get(code, str(code))
+        super().__init__(f"{where}: {name}: {msg}")
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32)) if a is not None else None
+
+
+def _bp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int8)) if a is not None else None
+
+
+def _f64(a, shape):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+class DemSystem:
+    """One DEM case resident on the device (or in the CPU restatement)."""
+
+    def __init__(self, lib, params: abi.DemParams, max_pip: int, prefix: str = "dem_"):
+        self._lib = lib
+        self._pre = prefix
+        self.params = params
+        self.n = int(max_pip)
+        h = C.c_void_p()
+        self._call("create", C.byref(params), C.c_int32(self.n), C.byref(h))
+        self._h = h
+        self.nn = 0  # last DES_TIME_STEP index executed
+
+    # ------------------------------------------------------------------
+    def _fn(self, name):
+        return getattr(self._lib, self._pre + name)
+
+    def _call(self, name, *args):
+        rc = self._fn(name)(*args)
+        if rc != 0:
+            msg = ""
+            if getattr(self, "_h", None) is not None:
+                raw = self._fn("last_error")(self._h)
+                msg = raw.decode() if raw else ""
+            raise DemError(rc, self._pre + name, msg)
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._fn("destroy")(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------
+    def set_walls(self, vertex: np.ndarray, norm_face: np.ndarray):
+        """VERTEX(3,3,F) as a (F,3,3) [f,c,v] array, NORM_FACE(3,F) as (F,3)."""
+        vertex = np.ascontiguousarray(vertex, dtype=np.float64)
+        norm_face = np.ascontiguousarray(norm_face, dtype=np.float64)
+        nf = vertex.shape[0]
+        self._call("set_walls", self._h, _dp(vertex), _dp(norm_face), C.c_int32(nf))
+
+    def upload_state(self, pos, vel, omega, radius, pmass, omoi, state, phase):
+        n = self.n
+        pos = _f64(pos, (3, n)); vel = _f64(vel, (3, n)); omega = _f64(omega, (3, n))
+        radius = _f64(radius, (n,)); pmass = _f64(pmass, (n,)); omoi = _f64(omoi, (n,))
+        state = np.ascontiguousarray(state, dtype=np.int8)
+        phase = np.ascontiguousarray(phase, dtype=np.int32)
+        self._call("upload_state", self._h, _dp(pos), _dp(vel), _dp(omega), _dp(radius),
+                   _dp(pmass), _dp(omoi), _bp(state), _ip(phase), C.c_int32(n))
+
+    def download_state(self):
+        n = self.n
+        pos = np.empty((3, n)); vel = np.empty((3, n)); omega = np.empty((3, n))
+        state = np.empty(n, dtype=np.int8)
+        self._call("download_state", self._h, _dp(pos), _dp(vel), _dp(omega), _bp(state), C.c_int32(n))
+        return {"pos": pos, "vel": vel, "omega": omega, "state": state}
+
+    def download_forces(self):
+        n = self.n
+        fc = np.empty((3, n)); tow = np.empty((3, n))
+        self._call("download_forces", self._h, _dp(fc), _dp(tow), C.c_int32(n))
+        return fc, tow
+
+    def set_ab2_history(self, acc_old=None, rot_acc_old=None, first_pass=True):
+        n = self.n
+        a = None if acc_old is None else _f64(acc_old, (3, n))
+        r = None if rot_acc_old is None else _f64(rot_acc_old, (3, n))
+        self._call("set_ab2_history", self._h, _dp(a), _dp(r), C.c_int32(1 if first_pass else 0), C.c_int32(n))
+
+    def get_ab2_history(self):
+        n = self.n
+        a = np.empty((3, n)); r = np.empty((3, n))
+        self._call("get_ab2_history", self._h, _dp(a), _dp(r), C.c_int32(n))
+        return a, r
+
+    def pair_count(self) -> int:
+        v = C.c_int64()
+        self._call("pair_count", self._h, C.byref(v))
+        return int(v.value)
+
+    def download_pairs(self):
+        """NEIGHBOR_INDEX (1-based end pointers), NEIGHBORS (1-based), PFT (P,3)."""
+        n = self.n
+        P = self.pair_count()
+        ni = np.empty(n, dtype=np.int32)
+        nb = np.empty(max(P, 1), dtype=np.int32)
+        pf = np.empty((max(P, 1), 3))
+        self._call("download_pairs", self._h, _ip(ni), _ip(nb), _dp(pf), C.c_int64(max(P, 1)), C.c_int32(n))
+        return ni, nb[:P].copy(), pf[:P].copy()
+
+    def upload_pairs(self, neighbor_index, neighbors, pft):
+        n = self.n
+        ni = np.ascontiguousarray(neighbor_index, dtype=np.int32)
+        nb = np.ascontiguousarray(neighbors, dtype=np.int32)
+        pf = np.ascontiguousarray(pft, dtype=np.float64).reshape(-1, 3)
+        P = nb.shape[0]
+        self._call("upload_pairs", self._h, _ip(ni), _ip(nb), _dp(pf), C.c_int64(P), C.c_int32(n))
+
+    def download_wall_history(self):
+        n = self.n
+        cm = self.params.collision_array_max or 8
+        fid = np.empty((n, cm), dtype=np.int32)
+        pf = np.empty((n, cm, 3))
+        self._call("download_wall_history", self._h, _ip(fid), _dp(pf), C.c_int32(n))
+        return fid, pf
+
+    def download_cells(self):
+        cells = np.empty(self.n, dtype=np.int32)
+        self._call("download_cells", self._h, _ip(cells), C.c_int32(self.n))
+        return cells
+
+    # ---- stages ------------------------------------------------------
+    def desgrid_pic(self):
+        self._call("desgrid_pic", self._h)
+
+    def neighbour(self):
+        self._call("neighbour", self._h)
+
+    def calc_force(self):
+        self._call("calc_force", self._h)
+
+    def cfnewvalues(self):
+        self._call("cfnewvalues", self._h)
+
+    def init_neighbors(self):
+        """MAKE_ARRAYS_DES tail: DESGRID_PIC + NEIGHBOUR on the uploaded state."""
+        self._call("init_neighbors", self._h)
+
+    def step(self, nsteps: int = 1, nn_first: Optional[int] = None):
+        """DES_TIME_STEP(NN) for the next nsteps values of NN."""
+        first = self.nn + 1 if nn_first is None else nn_first
+        self._call("step", self._h, C.c_int32(first), C.c_int32(nsteps))
+        self.nn = first + nsteps - 1
+
+    def stats(self) -> dict:
+        s = abi.DemStats()
+        self._call("get_stats", self._h, C.byref(s))
+        return s.as_dict()
+
+    # ---- coupling ----------------------------------------------------
+    def set_gas_fields(self, grid: abi.DemFluidGrid, ep_g, u_g, v_g, w_g, p_force=None):
+        ep_g = np.ascontiguousarray(ep_g, dtype=np.float64)
+        u_g = np.ascontiguousarray(u_g, dtype=np.float64)
+        v_g = np.ascontiguousarray(v_g, dtype=np.float64)
+        w_g = np.ascontiguousarray(w_g, dtype=np.float64)
+        pf = None if p_force is None else np.ascontiguousarray(p_force, dtype=np.float64)
+        self._keep = (ep_g, u_g, v_g, w_g, pf)
+        self._call("set_gas_fields", self._h, C.byref(grid), _dp(ep_g), _dp(u_g), _dp(v_g), _dp(w_g), _dp(pf))
+        self._ncell = ep_g.shape[0]
+
+    def get_mean_fields(self):
+        ep = np.empty(self._ncell); rop = np.empty(self._ncell)
+        self._call("get_mean_fields", self._h, _dp(ep), _dp(rop))
+        return ep, rop
+
+    def comp_mean_fields(self):
+        self._call("comp_mean_fields", self._h)
+
+    def drag_gs_des0(self):
+        self._call("drag_gs_des0", self._h)
+
+    def step_coupled(self, nsteps: int = 1, nn_first: Optional[int] = None):
+        first = self.nn + 1 if nn_first is None else nn_first
+        self._call("step_coupled", self._h, C.c_int32(first), C.c_int32(nsteps))
+        self.nn = first + nsteps - 1
+
+    # ---- CUDA-only ---------------------------------------------------
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        self._call("launch_count", self._h, C.byref(v))
+        return int(v.value)
+
+    def set_stream(self, stream_ptr: int):
+        self._call("set_stream", self._h, C.c_void_p(stream_ptr))
+
+    def force_error(self) -> float:
+        v = C.c_double()
+        self._call("force_error", self._h, C.byref(v))
+        return float(v.value)

@@ -1,0 +1,1229 @@
+// dem_oracle.cpp -- CPU restatement of the MFiX DEM particle step.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA library, never part of
+// the product path.  Each routine restates the cited Fortran of the reference
+// (paths relative to the MFiX source root) in the same floating-point
+// operation order as the serial (non-OpenMP) build, so that a compiler
+// without FMA contraction reproduces the reference's double-precision
+// results.  Build with -ffp-contract=off.
+//
+// Data layout: per-particle vectors are Fortran (MAX_PIP,3) column-major
+// (x block, y block, z block); indices are 0-based inside, 1-based at the
+// orc_* boundary.  Periodic axes use the minimum-image convention in place of
+// the reference's ghost copies (see periodic_shift()).
+
+#include "dem_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <cfloat>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr double SMALL_NUMBER = 1.0e-15;     // param1_mod.f:26
+constexpr double UNDEFINED    = 9.87654321e31; // param1_mod.f:20
+constexpr double TOL_STL      = 1.0e-6;      // cartesian_grid_init_namelist.f:748
+constexpr double TOL_EDGE     = 1.0e-9;      // stl_preproc_des_mod.f:383
+constexpr float  STL_NB_ANGLE = 5.0f;        // cartesian_grid_init_namelist.f:765 (REAL literal)
+
+inline double dot3(const double a[3], const double b[3]) {
+  // gfortran DOT_PRODUCT: accumulate left to right from zero.
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+inline void cross3(const double x[3], const double y[3], double out[3]) {
+  // CROSS, discretelement_mod.f:918-920
+  out[0] = x[1] * y[2] - x[2] * y[1];
+  out[1] = x[2] * y[0] - x[0] * y[2];
+  out[2] = x[0] * y[1] - x[1] * y[0];
+}
+
+struct FacetEntry {
+  int id;       // 0-based facet
+  int dir;      // 0-based axis of smallest extent
+  double mn, mx;
+};
+
+struct Oracle {
+  dem_params p{};
+  int n = 0;
+  int nthreads = 1;
+  std::string err;
+
+  // particle state (Fortran column blocks)
+  std::vector<double> pos, vel, omg, rad, pmass, omoi;
+  std::vector<int8_t> state;
+  std::vector<int> phase;  // 0-based
+  std::vector<double> fc, tow, acc_old, rot_acc_old;
+  bool first_pass = true;
+  bool have_state = false;
+
+  // DES grid (desgrid_mod.f:506-865, single rank)
+  int istart1, iend1, istart2, iend2, jstart1, jend1, jstart2, jend2;
+  int kstart1, kend1, kstart2, kend2;
+  int c1, c2, c3, ncell2;
+  std::vector<int> dg_pijk;              // 1-based cell, 0 = none
+  std::vector<int> cell_start, cell_list;  // dg_pic as CSR over 0-based cell
+
+  // pairs: row_end[i] = pairs in rows 0..i; nbrs 0-based; pft (3,P)
+  std::vector<int> row_end, nbrs;
+  std::vector<double> pft;
+
+  // walls
+  int nf = 0;
+  std::vector<double> vertex, norm_face;   // (3,3,F), (3,F)
+  std::vector<int8_t> ignore_edge;         // (F,4) edges 0..3
+  std::vector<int> fbin_start;             // CSR over 0-based cells
+  std::vector<FacetEntry> fbin;
+  int cmax = 8;
+  std::vector<int> wall_fid;               // (cmax, n) 0-based facet, -1 free
+  std::vector<double> wall_pft;            // (3, cmax, n)
+
+  // bookkeeping
+  double s_time = 0.0;
+  int64_t steps_done = 0, rogue_removed = 0, n_contacts = 0, n_wall_contacts = 0;
+  double max_overlap_ratio = 0.0;
+
+  // coupling
+  bool have_gas = false;
+  dem_fluid_grid g{};
+  std::vector<double> ep_g, u_g, v_g, w_g, p_force, rop_s;
+
+  int fail(int code, const std::string& m) { err = m; return code; }
+
+  // ---------------------------------------------------------------------
+  // DES grid index functions (desgrid_mod.f:184-188, 338-368, 391-419)
+  int funijk(int i, int j, int k) const { return j + i * c1 + k * c2 + c3; }
+  int jof(int ijk) const { return ((ijk - 1) % c2) % c1 + jstart2; }
+  int iof(int ijk) const { return ((ijk - jof(ijk) + jstart2 - 1) % c2) / c1 + istart2; }
+  int kof(int ijk) const { return (ijk - c3 - iof(ijk) * c1 - jof(ijk)) / c2; }
+  int iofpos(double x) const { return (int)std::floor((x - p.dg_xstart) * p.dg_dxinv) + istart1; }
+  int jofpos(double y) const { return (int)std::floor((y - p.dg_ystart) * p.dg_dyinv) + jstart1; }
+  int kofpos(double z) const { return (int)std::floor((z - p.dg_zstart) * p.dg_dzinv) + kstart1; }
+
+  void grid_init() {
+    // desgrid_init (desgrid_mod.f:571-604, 780-850) for one rank.
+    istart1 = 2; iend1 = p.dg_imax + 1; istart2 = 1; iend2 = p.dg_imax + 2;
+    jstart1 = 2; jend1 = p.dg_jmax + 1; jstart2 = 1; jend2 = p.dg_jmax + 2;
+    if (p.no_k) { kstart1 = kend1 = kstart2 = kend2 = 1; }
+    else { kstart1 = 2; kend1 = p.dg_kmax + 1; kstart2 = 1; kend2 = p.dg_kmax + 2; }
+    c1 = jend2 - jstart2 + 1;
+    c2 = c1 * (iend2 - istart2 + 1);
+    c3 = -c1 * istart2 - c2 * kstart2 - jstart2 + 1;
+    ncell2 = (iend2 - istart2 + 1) * (jend2 - jstart2 + 1) * (kend2 - kstart2 + 1);
+  }
+
+  double* X(std::vector<double>& v, int c) { return v.data() + (size_t)c * n; }
+  double  P(const std::vector<double>& v, int i, int c) const { return v[(size_t)c * n + i]; }
+
+  // Minimum-image shift for periodic axes: the displacement pos(j)-pos(i) is
+  // the one to the nearest periodic copy of j, which is the copy the
+  // reference's ghost exchange would have placed in i's stencil.
+  double periodic_shift(int c, double d) const {
+    if (!p.periodic[c]) return 0.0;
+    double L = p.domain_hi[c] - p.domain_lo[c];
+    if (d > 0.5 * L) return -L;
+    if (d < -0.5 * L) return L;
+    return 0.0;
+  }
+  void pair_dist(int i, int j, double d[3]) const {
+    // DIST = DES_POS_NEW(I,:) - DES_POS_NEW(LL,:) (calc_force_dem.f:214)
+    for (int c = 0; c < 3; ++c) {
+      double pj = P(pos, j, c);
+      double pi = P(pos, i, c);
+      double s = periodic_shift(c, pj - pi);
+      if (s != 0.0) pj = pj + s;
+      d[c] = pj - pi;
+    }
+  }
+
+  // ---------------------------------------------------------------------
+  // Periodic self-exchange of crossing particles (the serial path of
+  // DES_PAR_EXCHANGE, mpi_funs_des_mod.f:38-160): a particle whose cell
+  // index lies past the last interior cell is moved by one period.
+  void periodic_wrap() {
+    int lo[3] = {istart1, jstart1, kstart1}, hi[3] = {iend1, jend1, kend1};
+    for (int i = 0; i < n; ++i) {
+      if (state[i] == DEM_STATE_NONEXISTENT) continue;
+      for (int c = 0; c < 3; ++c) {
+        if (!p.periodic[c]) continue;
+        if (c == 2 && p.no_k) continue;
+        double x = P(pos, i, c);
+        int ci = c == 0 ? iofpos(x) : (c == 1 ? jofpos(x) : kofpos(x));
+        double L = p.domain_hi[c] - p.domain_lo[c];
+        if (ci > hi[c]) X(pos, c)[i] = x - L;
+        else if (ci < lo[c]) X(pos, c)[i] = x + L;
+      }
+    }
+  }
+
+  // DESGRID_PIC(.TRUE.) (desgrid_mod.f:877-995), serial order.
+  void desgrid_pic() {
+    bool anyper = p.periodic[0] || p.periodic[1] || (p.periodic[2] && !p.no_k);
+    if (anyper) periodic_wrap();
+    std::vector<int> cnt(ncell2, 0);
+    for (int i = 0; i < n; ++i) {
+      if (state[i] == DEM_STATE_NONEXISTENT) { dg_pijk[i] = 0; continue; }
+      int li = std::min(iend2, std::max(istart2, iofpos(P(pos, i, 0))));
+      int lj = std::min(jend2, std::max(jstart2, jofpos(P(pos, i, 1))));
+      int lk = p.no_k ? 1 : std::min(kend2, std::max(kstart2, kofpos(P(pos, i, 2))));
+      dg_pijk[i] = funijk(li, lj, lk);
+      cnt[dg_pijk[i] - 1]++;
+    }
+    cell_start.assign(ncell2 + 1, 0);
+    for (int c = 0; c < ncell2; ++c) cell_start[c + 1] = cell_start[c] + cnt[c];
+    cell_list.assign(cell_start[ncell2], 0);
+    std::vector<int> fillp(cell_start.begin(), cell_start.end() - 1);
+    for (int i = 0; i < n; ++i) {
+      if (state[i] == DEM_STATE_NONEXISTENT) continue;
+      cell_list[fillp[dg_pijk[i] - 1]++] = i;
+    }
+  }
+
+  // DELETE_PARTICLE (mass_outflow_dem.f:201-303)
+  void delete_particle(int i) {
+    for (int c = 0; c < 3; ++c) {
+      X(pos, c)[i] = 0.0; X(vel, c)[i] = 0.0; X(omg, c)[i] = 0.0;
+      X(fc, c)[i] = 0.0; X(tow, c)[i] = 0.0;
+    }
+    rad[i] = 0.0;
+    pmass[i] = (double)FLT_MAX;  // HUGE(0.0)
+    omoi[i] = 0.0;
+    for (int s = 0; s < cmax; ++s) wall_fid[(size_t)i * cmax + s] = -1;
+    state[i] = DEM_STATE_NONEXISTENT;
+  }
+
+  // DESGRID_NEIGH_BUILD (desgrid_mod.f:1002-1299), serial build with add_pair
+  // (des_allocate_mod.f:555-567).  Rows follow the (lk, lj, li) stencil order
+  // and ascending particle index inside each cell.
+  void neigh_build() {
+    row_end.assign(n, 0);
+    nbrs.clear();
+    bool do_exit = false;
+    const double fr = p.factor_rlm, mr = p.max_radius;
+    bool coarse_x = 1.0 > 2.0 * mr * fr * p.dg_dxinv;
+    bool coarse_y = 1.0 > 2.0 * mr * fr * p.dg_dyinv;
+    bool coarse_z = 1.0 > 2.0 * mr * fr * p.dg_dzinv;
+    for (int cur = 0; cur < n; ++cur) {
+      row_end[cur] = (int)nbrs.size();
+      if (state[cur] != DEM_STATE_NORMAL) continue;
+      int lijk = dg_pijk[cur];
+      int lic = iof(lijk), ljc = jof(lijk), lkc = kof(lijk);
+      if (lic < istart1 || lic > iend1 || ljc < jstart1 || ljc > jend1 ||
+          lkc < kstart1 || lkc > kend1) {
+        do_exit = true;
+        if (p.remove_rogue) { delete_particle(cur); rogue_removed++; }
+        else err = "NORMAL particle found in GHOST cell";
+      }
+      if (do_exit) continue;
+      int il = 1, iu = 1, jl = 1, ju = 1, kl = 1, ku = 1;
+      double cp[3] = {P(pos, cur, 0), P(pos, cur, 1), P(pos, cur, 2)};
+      if (coarse_x) {
+        double t = (cp[0] - p.dg_xstart) * p.dg_dxinv;
+        double off = t - (double)(long long)std::floor(t);
+        if (off >= 0.5) il = 0; else iu = 0;
+      }
+      if (coarse_y) {
+        double t = (cp[1] - p.dg_ystart) * p.dg_dyinv;
+        double off = t - (double)(long long)std::floor(t);
+        if (off >= 0.5) jl = 0; else ju = 0;
+      }
+      if (p.no_k) { kl = 0; ku = 0; }
+      else if (coarse_z) {
+        double t = (cp[2] - p.dg_zstart) * p.dg_dzinv;
+        double off = t - (double)(long long)std::floor(t);
+        if (off >= 0.5) kl = 0; else ku = 0;
+      }
+      for (int lk = lkc - kl; lk <= lkc + ku; ++lk)
+      for (int lj = ljc - jl; lj <= ljc + ju; ++lj)
+      for (int li = lic - il; li <= lic + iu; ++li) {
+        // periodic axes: the ghost layer holds copies of the opposite
+        // interior layer shifted by one period.
+        int ri = li, rj = lj, rk = lk;
+        double sh[3] = {0.0, 0.0, 0.0};
+        if (p.periodic[0]) {
+          if (li < istart1) { ri = iend1; sh[0] = -(p.domain_hi[0] - p.domain_lo[0]); }
+          else if (li > iend1) { ri = istart1; sh[0] = (p.domain_hi[0] - p.domain_lo[0]); }
+        }
+        if (p.periodic[1]) {
+          if (lj < jstart1) { rj = jend1; sh[1] = -(p.domain_hi[1] - p.domain_lo[1]); }
+          else if (lj > jend1) { rj = jstart1; sh[1] = (p.domain_hi[1] - p.domain_lo[1]); }
+        }
+        if (p.periodic[2] && !p.no_k) {
+          if (lk < kstart1) { rk = kend1; sh[2] = -(p.domain_hi[2] - p.domain_lo[2]); }
+          else if (lk > kend1) { rk = kstart1; sh[2] = (p.domain_hi[2] - p.domain_lo[2]); }
+        }
+        bool ghost = (sh[0] != 0.0 || sh[1] != 0.0 || sh[2] != 0.0);
+        int cell = funijk(ri, rj, rk) - 1;
+        for (int s = cell_start[cell]; s < cell_start[cell + 1]; ++s) {
+          int nb = cell_list[s];
+          if (nb == cur) continue;
+          if (nb < cur && state[nb] == DEM_STATE_NORMAL) continue;
+          if (state[nb] == DEM_STATE_NONEXISTENT) continue;
+          double srad = fr * (rad[cur] + rad[nb]);
+          double d[3];
+          for (int c = 0; c < 3; ++c) {
+            double pn = P(pos, nb, c);
+            if (ghost && sh[c] != 0.0) pn = pn + sh[c];
+            d[c] = cp[c] - pn;
+          }
+          double d2 = dot3(d, d);
+          if (d2 > srad * srad) continue;
+          nbrs.push_back(nb);
+        }
+      }
+      row_end[cur] = (int)nbrs.size();
+    }
+  }
+
+  // NEIGHBOUR (neighbour.f:21-126): rebuild and carry PFT over by matching
+  // the neighbour id inside the old row of the same particle.
+  void neighbour() {
+    std::vector<int> old_end = row_end, old_nbrs = nbrs;
+    std::vector<double> old_pft = pft;
+    neigh_build();
+    pft.assign((size_t)3 * nbrs.size(), 0.0);
+    for (int ll = 0; ll < n; ++ll) {
+      int s = ll ? row_end[ll - 1] : 0, e = row_end[ll];
+      int so = 0, eo = 0;
+      if (!old_end.empty()) { so = ll ? old_end[ll - 1] : 0; eo = old_end[ll]; }
+      for (int cc = s; cc < e; ++cc) {
+        bool found = false;
+        for (int co = so; co < eo; ++co) {
+          if (nbrs[cc] == old_nbrs[co]) {
+            for (int c = 0; c < 3; ++c) pft[3 * (size_t)cc + c] = old_pft[3 * (size_t)co + c];
+            found = true;
+            break;
+          }
+        }
+        if (!found) for (int c = 0; c < 3; ++c) pft[3 * (size_t)cc + c] = 0.0;
+      }
+    }
+  }
+
+  // ---------------------------------------------------------------------
+  // Walls
+  double V(int f, int v, int c) const { return vertex[(size_t)v + 3 * c + 9 * (size_t)f]; }
+
+  // TRI_BOX_OVERLAP (stl_functions_des_mod.f:280-536), Akenine-Moller test.
+  static bool tri_box_overlap(const double ctr[3], const double hs[3], const double vt[3][3]) {
+    double v0[3], v1[3], v2[3], e0[3], e1[3], e2[3];
+    for (int c = 0; c < 3; ++c) {
+      v0[c] = vt[0][c] - ctr[c]; v1[c] = vt[1][c] - ctr[c]; v2[c] = vt[2][c] - ctr[c];
+    }
+    for (int c = 0; c < 3; ++c) { e0[c] = v1[c] - v0[c]; e1[c] = v2[c] - v1[c]; e2[c] = v0[c] - v2[c]; }
+    auto axtest = [&](double pa, double pb, double rad) {
+      double lmin = pa < pb ? pa : pb, lmax = pa < pb ? pb : pa;
+      return (lmin > rad || lmax < -rad);
+    };
+    auto z12 = [&](double pa1, double pa2, double rad) {  // ATEST_Z12 orders (p2<p1)
+      double lmin, lmax;
+      if (pa2 < pa1) { lmin = pa2; lmax = pa1; } else { lmin = pa1; lmax = pa2; }
+      return (lmin > rad || lmax < -rad);
+    };
+    double fex, fey, fez;
+    // edge e0
+    fex = std::fabs(e0[0]); fey = std::fabs(e0[1]); fez = std::fabs(e0[2]);
+    { double a = e0[2], b = e0[1];  // X01
+      if (axtest(a * v0[1] - b * v0[2], a * v2[1] - b * v2[2], fez * hs[1] + fey * hs[2])) return false; }
+    { double a = e0[2], b = e0[0];  // Y02
+      if (axtest(-a * v0[0] + b * v0[2], -a * v2[0] + b * v2[2], fez * hs[0] + fex * hs[2])) return false; }
+    { double a = e0[1], b = e0[0];  // Z12
+      if (z12(a * v1[0] - b * v1[1], a * v2[0] - b * v2[1], fey * hs[0] + fex * hs[1])) return false; }
+    // edge e1
+    fex = std::fabs(e1[0]); fey = std::fabs(e1[1]); fez = std::fabs(e1[2]);
+    { double a = e1[2], b = e1[1];  // X01
+      if (axtest(a * v0[1] - b * v0[2], a * v2[1] - b * v2[2], fez * hs[1] + fey * hs[2])) return false; }
+    { double a = e1[2], b = e1[0];  // Y02
+      if (axtest(-a * v0[0] + b * v0[2], -a * v2[0] + b * v2[2], fez * hs[0] + fex * hs[2])) return false; }
+    { double a = e1[1], b = e1[0];  // Z0
+      if (axtest(a * v0[0] - b * v0[1], a * v1[0] - b * v1[1], fey * hs[0] + fex * hs[1])) return false; }
+    // edge e2
+    fex = std::fabs(e2[0]); fey = std::fabs(e2[1]); fez = std::fabs(e2[2]);
+    { double a = e2[2], b = e2[1];  // X2
+      if (axtest(a * v0[1] - b * v0[2], a * v1[1] - b * v1[2], fez * hs[1] + fey * hs[2])) return false; }
+    { double a = e2[2], b = e2[0];  // Y1
+      if (axtest(-a * v0[0] + b * v0[2], -a * v1[0] + b * v1[2], fez * hs[0] + fex * hs[2])) return false; }
+    { double a = e2[1], b = e2[0];  // Z12
+      if (z12(a * v1[0] - b * v1[1], a * v2[0] - b * v2[1], fey * hs[0] + fex * hs[1])) return false; }
+    auto fmin3 = [](double a, double b, double c) { double m = a; if (b < m) m = b; if (c < m) m = c; return m; };
+    auto fmax3 = [](double a, double b, double c) { double m = a; if (b > m) m = b; if (c > m) m = c; return m; };
+    for (int c = 0; c < 3; ++c)
+      if (fmin3(v0[c], v1[c], v2[c]) > hs[c] || fmax3(v0[c], v1[c], v2[c]) < -hs[c]) return false;
+    double nrm[3];
+    nrm[0] = e0[1] * e1[2] - e0[2] * e1[1];
+    nrm[1] = e0[2] * e1[0] - e0[0] * e1[2];
+    nrm[2] = e0[0] * e1[1] - e0[1] * e1[0];
+    double vmin[3], vmax[3];
+    for (int c = 0; c < 3; ++c) {
+      double v = v0[c];
+      if (nrm[c] > 0.0) { vmin[c] = -hs[c] - v; vmax[c] = hs[c] - v; }
+      else { vmin[c] = hs[c] - v; vmax[c] = -hs[c] - v; }
+    }
+    if (dot3(nrm, vmin) > 0.0) return false;
+    if (dot3(nrm, vmax) >= 0.0) return true;
+    return false;
+  }
+
+  // BIN_FACETS_TO_DG + ADD_FACET_FOR_DES + ADD_FACET
+  // (stl_preproc_des_mod.f:135-349) and
+  // FLAG_FACETS_WHERE_EDGE_COLLISION_IS_IGNORED (361-490).
+  void bin_facets() {
+    std::vector<std::vector<FacetEntry>> bins(ncell2);
+    const double buffer = 1.1 * p.max_radius;
+    const double ldx = 1.0 / p.dg_dxinv, ldy = 1.0 / p.dg_dyinv, ldz = 1.0 / p.dg_dzinv;
+    for (int f = 0; f < nf; ++f) {
+      double x1 = std::min({V(f,0,0), V(f,1,0), V(f,2,0)}), x2 = std::max({V(f,0,0), V(f,1,0), V(f,2,0)});
+      double y1 = std::min({V(f,0,1), V(f,1,1), V(f,2,1)}), y2 = std::max({V(f,0,1), V(f,1,1), V(f,2,1)});
+      double z1 = std::min({V(f,0,2), V(f,1,2), V(f,2,2)}), z2 = std::max({V(f,0,2), V(f,1,2), V(f,2,2)});
+      int i1 = iend2, i2 = istart2, j1 = jend2, j2 = jstart2, k1 = kend2, k2 = kstart2;
+      if (x2 >= p.domain_lo[0] - TOL_STL && x1 <= p.domain_hi[0] + TOL_STL) {
+        i1 = std::max(iofpos(x1) - 1, istart2); i2 = std::min(iofpos(x2) + 1, iend2);
+      }
+      if (y2 >= p.domain_lo[1] - TOL_STL && y1 <= p.domain_hi[1] + TOL_STL) {
+        j1 = std::max(jofpos(y1) - 1, jstart2); j2 = std::min(jofpos(y2) + 1, jend2);
+      }
+      if (!p.no_k) {
+        if (z2 >= p.domain_lo[2] - TOL_STL && z1 <= p.domain_hi[2] + TOL_STL) {
+          k1 = std::max(kofpos(z1) - 1, kstart2); k2 = std::min(kofpos(z2) + 1, kend2);
+        }
+      }
+      double vt[3][3];
+      for (int v = 0; v < 3; ++v) for (int c = 0; c < 3; ++c) vt[v][c] = V(f, v, c);
+      for (int kk = k1; kk <= k2; ++kk)
+      for (int jj = j1; jj <= j2; ++jj)
+      for (int ii = i1; ii <= i2; ++ii) {
+        double ctr[3], hs[3];
+        ctr[0] = p.dg_xstart + ((double)(ii - istart1) + 0.5) * ldx; hs[0] = 0.5 * ldx + buffer;
+        ctr[1] = p.dg_ystart + ((double)(jj - jstart1) + 0.5) * ldy; hs[1] = 0.5 * ldy + buffer;
+        if (!p.no_k) { ctr[2] = p.dg_zstart + ((double)(kk - kstart1) + 0.5) * ldz; hs[2] = 0.5 * ldz + buffer; }
+        else { ctr[2] = 0.5 * ldz; hs[2] = 0.5 * ldz; }
+        if (!tri_box_overlap(ctr, hs, vt)) continue;
+        auto& b = bins[funijk(ii, jj, kk) - 1];
+        bool dup = false;
+        for (auto& e : b) if (e.id == f) { dup = true; break; }
+        if (dup) continue;
+        FacetEntry e{f, 0, 0.0, 0.0};
+        double smallest = (double)FLT_MAX;  // HUGE(0.0)
+        for (int c = 0; c < 3; ++c) {
+          double mn = std::min({V(f,0,c), V(f,1,c), V(f,2,c)});
+          double mx = std::max({V(f,0,c), V(f,1,c), V(f,2,c)});
+          if (std::fabs(mx - mn) < smallest) { e.dir = c; e.mn = mn; e.mx = mx; smallest = std::fabs(mx - mn); }
+        }
+        b.push_back(e);
+      }
+    }
+    fbin_start.assign(ncell2 + 1, 0);
+    fbin.clear();
+    for (int c = 0; c < ncell2; ++c) {
+      fbin_start[c] = (int)fbin.size();
+      for (auto& e : bins[c]) fbin.push_back(e);
+    }
+    fbin_start[ncell2] = (int)fbin.size();
+
+    // edge flags
+    ignore_edge.assign((size_t)nf * 4, 0);
+    const double pi = 4.0 * std::atan(1.0);
+    const double cos_nb = std::cos((double)STL_NB_ANGLE / 180.0 * pi) + 1.0e-6;
+    auto edge_centers = [&](int f, double ec[3][3]) {
+      for (int c = 0; c < 3; ++c) {
+        ec[0][c] = 0.5 * (V(f,0,c) + V(f,1,c));
+        ec[1][c] = 0.5 * (V(f,0,c) + V(f,2,c));
+        ec[2][c] = 0.5 * (V(f,1,c) + V(f,2,c));
+      }
+    };
+    for (int cell = 0; cell < ncell2; ++cell) {
+      int s = fbin_start[cell], e = fbin_start[cell + 1];
+      for (int a = s; a < e; ++a) {
+        int fa = fbin[a].id; double ec[3][3]; edge_centers(fa, ec);
+        for (int ed = 0; ed < 3; ++ed)
+          for (int b = s; b < e; ++b) {
+            if (a == b) continue;
+            int fb = fbin[b].id; double nec[3][3]; edge_centers(fb, nec);
+            for (int ned = 0; ned < 3; ++ned) {
+              double d[3] = {nec[ned][0] - ec[ed][0], nec[ned][1] - ec[ed][1], nec[ned][2] - ec[ed][2]};
+              if (dot3(d, d) < TOL_EDGE) {
+                const double* na = &norm_face[3 * (size_t)fa];
+                const double* nb = &norm_face[3 * (size_t)fb];
+                double dp = na[0] * nb[0] + na[1] * nb[1] + na[2] * nb[2];
+                if (dp > cos_nb) {
+                  ignore_edge[(size_t)fa * 4 + ed + 1] = 1;
+                  ignore_edge[(size_t)fb * 4 + ned + 1] = 1;
+                }
+              }
+            }
+          }
+      }
+    }
+  }
+
+  // ClosestPtPointTriangle (stl_functions_des_mod.f:25-160)
+  void closest_pt(int f, const double pp[3], double cpt[3], bool& poe, int& edge) const {
+    poe = false; edge = 0;
+    double a[3], b[3], c[3], ab[3], ac[3], ap[3], bp[3], cp[3];
+    for (int k = 0; k < 3; ++k) { a[k] = V(f,0,k); b[k] = V(f,1,k); c[k] = V(f,2,k); }
+    for (int k = 0; k < 3; ++k) { ab[k] = b[k] - a[k]; ac[k] = c[k] - a[k]; ap[k] = pp[k] - a[k]; }
+    double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+    auto ign = [&](int e) { return ignore_edge[(size_t)f * 4 + e] != 0; };
+    if (d1 < 0.0 && d2 < 0.0) {
+      for (int k = 0; k < 3; ++k) cpt[k] = a[k];
+      poe = true; if (ign(1)) cpt[0] = UNDEFINED; edge = 1; return;
+    }
+    for (int k = 0; k < 3; ++k) bp[k] = pp[k] - b[k];
+    double d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+    if (d3 > 0.0 && d4 < d3) {
+      for (int k = 0; k < 3; ++k) cpt[k] = b[k];
+      poe = true; if (ign(1)) cpt[0] = UNDEFINED; edge = 1; return;
+    }
+    double vc = d1 * d4 - d3 * d2;
+    if (vc < 0.0 && d1 > 0.0 && d3 < 0.0) {
+      double v = d1 / (d1 - d3);
+      for (int k = 0; k < 3; ++k) cpt[k] = a[k] + v * ab[k];
+      poe = true; if (ign(1)) cpt[0] = UNDEFINED; edge = 1; return;
+    }
+    for (int k = 0; k < 3; ++k) cp[k] = pp[k] - c[k];
+    double d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+    if (d6 > 0.0 && d5 < d6) {
+      for (int k = 0; k < 3; ++k) cpt[k] = c[k];
+      poe = true; if (ign(2)) cpt[0] = UNDEFINED; edge = 2; return;
+    }
+    double vb = d5 * d2 - d1 * d6;
+    if (vb < 0.0 && d2 > 0.0 && d6 < 0.0) {
+      double w = d2 / (d2 - d6);
+      for (int k = 0; k < 3; ++k) cpt[k] = a[k] + w * ac[k];
+      poe = true; if (ign(2)) cpt[0] = UNDEFINED; edge = 2; return;
+    }
+    double va = d3 * d6 - d5 * d4;
+    if (va < 0.0 && (d4 - d3) > 0.0 && (d5 - d6) > 0.0) {
+      double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+      for (int k = 0; k < 3; ++k) cpt[k] = b[k] + w * (c[k] - b[k]);
+      poe = true; if (ign(3)) cpt[0] = UNDEFINED; edge = 3; return;
+    }
+    double denom = 1.0 / (va + vb + vc);
+    double v = vb * denom, w = vc * denom;
+    for (int k = 0; k < 3; ++k) cpt[k] = a[k] + ab[k] * v + ac[k] * w;
+    if (p.no_k) cpt[2] = pp[2];
+    poe = false; edge = 0;
+  }
+
+  // GET_COLLISION / UPDATE_COLLISION / REMOVE_COLLISION
+  // (calc_collision_wall_mod.f:651-792)
+  int get_collision(int ll, int f, double out[3]) {
+    int* fid = &wall_fid[(size_t)ll * cmax];
+    double* wp = &wall_pft[(size_t)ll * cmax * 3];
+    int free_index = -1;
+    for (int s = 0; s < cmax; ++s) {
+      if (f == fid[s]) { for (int c = 0; c < 3; ++c) out[c] = wp[3 * s + c]; return 0; }
+      else if (fid[s] == -1) free_index = s;
+    }
+    if (free_index == -1) {
+      int cell = dg_pijk[ll] - 1;
+      for (int s = 0; s < cmax && free_index == -1; ++s) {
+        bool in_cell = false;
+        for (int q = fbin_start[cell]; q < fbin_start[cell + 1]; ++q)
+          if (fid[s] == fbin[q].id) { in_cell = true; break; }
+        if (!in_cell) free_index = s;
+      }
+    }
+    if (free_index == -1) return DEM_ERR_WALL_SLOTS;
+    fid[free_index] = f;
+    for (int c = 0; c < 3; ++c) { wp[3 * free_index + c] = 0.0; out[c] = 0.0; }
+    return 0;
+  }
+  void update_collision(int ll, int f, const double v[3]) {
+    int* fid = &wall_fid[(size_t)ll * cmax];
+    double* wp = &wall_pft[(size_t)ll * cmax * 3];
+    for (int s = 0; s < cmax; ++s)
+      if (fid[s] == f) { for (int c = 0; c < 3; ++c) wp[3 * s + c] = v[c]; return; }
+  }
+  void remove_collision(int ll, int f) {
+    int* fid = &wall_fid[(size_t)ll * cmax];
+    for (int s = 0; s < cmax; ++s) if (fid[s] == f) { fid[s] = -1; return; }
+  }
+
+  // CALC_DEM_FORCE_WITH_WALL_STL (calc_collision_wall_mod.f:180-629) for one
+  // particle, spheres only, static walls (CFRELVEL_WALL 806-847 with zero
+  // wall velocity).
+  int wall_force_one(int ll) {
+    if (state[ll] != DEM_STATE_NORMAL) return 0;
+    int cell = dg_pijk[ll] - 1;
+    int fs = fbin_start[cell], fe = fbin_start[cell + 1];
+    if (fe - fs < 1) {
+      for (int s = 0; s < cmax; ++s) wall_fid[(size_t)ll * cmax + s] = -1;
+      for (int s = 0; s < 3 * cmax; ++s) wall_pft[(size_t)ll * cmax * 3 + s] = 0.0;
+      return 0;
+    }
+    const double r = rad[ll];
+    const double radsq = r * r;
+    double xp[3] = {P(pos, ll, 0), P(pos, ll, 1), P(pos, ll, 2)};
+    double v[3] = {P(vel, ll, 0), P(vel, ll, 1), P(vel, ll, 2)};
+    double w[3] = {P(omg, ll, 0), P(omg, ll, 1), P(omg, ll, 2)};
+    double pmax[3], pmin[3];
+    for (int c = 0; c < 3; ++c) { pmax[c] = xp[c] + r; pmin[c] = xp[c] - r; }
+    const int ph = phase[ll];
+    for (int q = fs; q < fe; ++q) {
+      const FacetEntry& fe_ = fbin[q];
+      int nf_ = fe_.id;
+      if (fe_.mn > pmax[fe_.dir]) { remove_collision(ll, nf_); continue; }
+      if (fe_.mx < pmin[fe_.dir]) { remove_collision(ll, nf_); continue; }
+      double d1[3] = {V(nf_,0,0) - xp[0], V(nf_,0,1) - xp[1], V(nf_,0,2) - xp[2]};
+      double line_t = dot3(d1, &norm_face[3 * (size_t)nf_]);
+      if (line_t <= -1.0001 * r) { remove_collision(ll, nf_); continue; }
+      double cpt[3]; bool poe; int edge;
+      closest_pt(nf_, xp, cpt, poe, edge);
+      double dist[3] = {cpt[0] - xp[0], cpt[1] - xp[1], cpt[2] - xp[2]};
+      double distsq = dot3(dist, dist);
+      if (distsq >= radsq - SMALL_NUMBER) { remove_collision(ll, nf_); continue; }
+      if (poe && ignore_edge[(size_t)nf_ * 4 + edge]) continue;
+      double distmod = std::sqrt(distsq);
+      double nrm[3] = {dist[0], dist[1], dist[2]};
+      if (distsq > 0) { double s = std::sqrt(distsq); for (int c = 0; c < 3; ++c) nrm[c] = dist[c] / s; }
+      double overlap_n = r - distmod;
+      double wxn[3]; cross3(w, nrm, wxn);
+      double vrot[3] = {distmod * wxn[0], distmod * wxn[1], distmod * wxn[2]};
+      double vrel[3];
+      for (int c = 0; c < 3; ++c) { vrel[c] = v[c] + vrot[c]; vrel[c] = vrel[c] - (0.0 + 0.0); }
+      double vrn = dot3(vrel, nrm);
+      double vt[3] = {vrel[0] - vrn * nrm[0], vrel[1] - vrn * nrm[1], vrel[2] - vrn * nrm[2]};
+      double kn_w, kt_w, etan_w, etat_w;
+      if (p.coll_model == DEM_COLL_HERTZ) {
+        double so = 0.0;
+        if (overlap_n > 0) so = std::sqrt(overlap_n);
+        kn_w = p.hert_kwn[ph] * so * std::sqrt(r);
+        kt_w = p.hert_kwt[ph] * so * std::sqrt(r);
+        etan_w = p.des_etan_wall[ph] * std::sqrt(so) * std::sqrt(p.hert_kwn[ph] * std::sqrt(r) * pmass[ll]);
+        etat_w = p.des_etat_wall[ph] * std::sqrt(so) * std::sqrt(p.hert_kwt[ph] * std::sqrt(r) * pmass[ll]);
+      } else {
+        kn_w = p.kn_w; kt_w = p.kt_w;
+        etan_w = p.des_etan_wall[ph] * std::sqrt(pmass[ll]);
+        etat_w = p.des_etat_wall[ph] * std::sqrt(pmass[ll]);
+      }
+      double fn[3];
+      for (int c = 0; c < 3; ++c) fn[c] = -(kn_w * overlap_n * nrm[c] + etan_w * vrn * nrm[c]);
+      double hist[3];
+      int rc = get_collision(ll, nf_, hist);
+      if (rc) return fail(rc, "COLLISION_ARRAY_MAX too small");
+      double ot[3];
+      for (int c = 0; c < 3; ++c) ot[c] = p.dtsolid * vt[c] + hist[c];
+      double mag = std::sqrt(dot3(ot, ot));
+      double ft[3];
+      if (mag > 0.0) {
+        for (int c = 0; c < 3; ++c) ft[c] = -kt_w * ot[c] - etat_w * vt[c];
+        double ftmd = std::sqrt(dot3(ft, ft));
+        double fnmd = p.mew_w * std::sqrt(dot3(fn, fn));
+        if (ftmd > fnmd) {
+          double tg[3];
+          for (int c = 0; c < 3; ++c) tg[c] = ot[c] / mag;
+          for (int c = 0; c < 3; ++c) ft[c] = -fnmd * tg[c];
+          for (int c = 0; c < 3; ++c) ot[c] = (fnmd / kt_w) * tg[c];
+        }
+      } else {
+        ft[0] = ft[1] = ft[2] = 0.0;
+      }
+      update_collision(ll, nf_, ot);
+      n_wall_contacts++;
+      for (int c = 0; c < 3; ++c) X(fc, c)[ll] = X(fc, c)[ll] + fn[c] + ft[c];
+      double nxf[3]; cross3(nrm, ft, nxf);
+      for (int c = 0; c < 3; ++c) X(tow, c)[ll] = X(tow, c)[ll] + distmod * nxf[c];
+      if (p.mew_rw > 0.0) {
+        double om = std::sqrt(dot3(w, w));
+        if (om > 0.0) {
+          for (int c = 0; c < 3; ++c) {
+            double rf = -(p.mew_rw * (2.0 * r) * kn_w * overlap_n * w[c] / om);
+            X(tow, c)[ll] = X(tow, c)[ll] + rf;
+          }
+        }
+      }
+    }
+    return 0;
+  }
+
+  // One pair of CALC_FORCE_DEM (calc_force_dem.f:204-506) with CFRELVEL
+  // (cfrelvel.f:54-77).  Returns 0 and fills outputs; *contact = false when
+  // the pair is apart (history reset).
+  struct PairOut {
+    double fc[3], tl[3], ti[3], rl[3], ri[3];
+    bool contact, roll_l, roll_i;
+  };
+  int pair_force(int ll, int i, const double* pft_in, double* pft_out, PairOut& o) const {
+    o.contact = false; o.roll_l = o.roll_i = false;
+    double rl = rad[ll], ri = rad[i];
+    double r_lm = rl + ri;
+    double dist[3];
+    pair_dist(ll, i, dist);
+    double dmag = dot3(dist, dist);
+    double fct[3] = {0.0, 0.0, 0.0};
+    if (dmag > (r_lm - SMALL_NUMBER) * (r_lm - SMALL_NUMBER)) {
+      pft_out[0] = pft_out[1] = pft_out[2] = 0.0;
+      return 0;
+    }
+    if (dmag == 0) return DEM_ERR_ZERO_DISTANCE;
+    dmag = std::sqrt(dmag);
+    double nrm[3] = {dist[0] / dmag, dist[1] / dmag, dist[2] / dmag};
+    double overlap_n = r_lm - dmag;
+    // CFRELVEL
+    double vrel[3];
+    for (int c = 0; c < 3; ++c) vrel[c] = P(vel, ll, c) - P(vel, i, c);
+    double dcl = (dmag * dmag + rl * rl - ri * ri) / (2.0 * dmag);
+    double dci = dmag - dcl;
+    double osum[3];
+    for (int c = 0; c < 3; ++c) osum[c] = P(omg, ll, c) * dcl + P(omg, i, c) * dci;
+    double vrot[3]; cross3(osum, nrm, vrot);
+    for (int c = 0; c < 3; ++c) vrel[c] = vrel[c] + vrot[c];
+    double vrn = dot3(vrel, nrm);
+    double vt[3] = {vrel[0] - vrn * nrm[0], vrel[1] - vrn * nrm[1], vrel[2] - vrn * nrm[2]};
+    int pl = phase[ll], pi_ = phase[i];
+    int ix = pl * DEM_MAX_PHASES + pi_;
+    double rad_eff = (rl * ri) / (rl + ri);
+    double m_eff = (pmass[ll] * pmass[i]) / (pmass[ll] + pmass[i]);
+    double kn, kt, etan, etat;
+    if (p.coll_model == DEM_COLL_HERTZ) {
+      double so = std::sqrt(overlap_n);
+      kn = p.hert_kn[ix] * so * std::sqrt(rad_eff);
+      kt = p.hert_kt[ix] * so * std::sqrt(rad_eff);
+      so = std::sqrt(so);
+      etan = p.des_etan[ix] * so * std::sqrt(p.hert_kn[ix] * std::sqrt(rad_eff) * m_eff);
+      etat = p.des_etat[ix] * so * std::sqrt(p.hert_kt[ix] * std::sqrt(rad_eff) * m_eff);
+    } else {
+      kn = p.kn; kt = p.kt;
+      etan = p.des_etan[ix] * std::sqrt(m_eff);
+      etat = p.des_etat[ix] * std::sqrt(m_eff);
+    }
+    double fn[3];
+    for (int c = 0; c < 3; ++c) fn[c] = -(kn * overlap_n * nrm[c] + etan * vrn * nrm[c]);
+    double ot[3];
+    for (int c = 0; c < 3; ++c) ot[c] = p.dtsolid * vt[c] + pft_in[c];
+    double mag = std::sqrt(dot3(ot, ot));
+    double ft[3];
+    if (mag > 0.0) {
+      for (int c = 0; c < 3; ++c) ft[c] = -kt * ot[c] - etat * vt[c];
+      double ftmd = std::sqrt(dot3(ft, ft));
+      double fnmd = p.mew * std::sqrt(dot3(fn, fn));
+      if (ftmd > fnmd) {
+        double tg[3];
+        for (int c = 0; c < 3; ++c) tg[c] = ot[c] / mag;
+        for (int c = 0; c < 3; ++c) ft[c] = -fnmd * tg[c];
+        for (int c = 0; c < 3; ++c) ot[c] = (fnmd / kt) * tg[c];
+      }
+    } else {
+      ft[0] = ft[1] = ft[2] = 0.0;
+    }
+    for (int c = 0; c < 3; ++c) pft_out[c] = ot[c];
+    double dcl2 = dmag / 2.0 + (rl * rl - ri * ri) / (2.0 * dmag);
+    double dci2 = dmag - dcl2;
+    double tf[3]; cross3(nrm, ft, tf);
+    for (int c = 0; c < 3; ++c) { o.tl[c] = dcl2 * tf[c]; o.ti[c] = dci2 * tf[c]; }
+    for (int c = 0; c < 3; ++c) fct[c] = fct[c] + fn[c] + ft[c];
+    for (int c = 0; c < 3; ++c) o.fc[c] = fct[c];
+    if (p.mew_r > 0.0) {
+      double wl[3] = {P(omg, ll, 0), P(omg, ll, 1), P(omg, ll, 2)};
+      double om = std::sqrt(dot3(wl, wl));
+      if (om > 0.0) {
+        o.roll_l = true;
+        for (int c = 0; c < 3; ++c) o.rl[c] = -(p.mew_r * (2.0 * rl) * kn * overlap_n * wl[c] / om);
+      }
+      double wi[3] = {P(omg, i, 0), P(omg, i, 1), P(omg, i, 2)};
+      om = std::sqrt(dot3(wi, wi));
+      if (om > 0.0) {
+        o.roll_i = true;
+        for (int c = 0; c < 3; ++c) o.ri[c] = -(p.mew_r * (2.0 * ri) * kn * overlap_n * wi[c] / om);
+      }
+    }
+    o.contact = true;
+    return 0;
+  }
+
+  // CALC_FORCE_DEM (calc_force_dem.f:18-544), serial order: walls first, then
+  // LL ascending, CC ascending, scattering into FC/TOW.
+  int calc_force() {
+    n_contacts = 0; n_wall_contacts = 0; max_overlap_ratio = 0.0;
+    for (int ll = 0; ll < n; ++ll) {
+      int rc = wall_force_one(ll);
+      if (rc) return rc;
+    }
+#ifdef _OPENMP
+    if (nthreads > 1) return calc_force_omp();
+#endif
+    for (int ll = 0; ll < n; ++ll) {
+      if (state[ll] == DEM_STATE_NONEXISTENT) continue;
+      int s = ll ? row_end[ll - 1] : 0, e = row_end[ll];
+      for (int cc = s; cc < e; ++cc) {
+        int i = nbrs[cc];
+        if (state[i] == DEM_STATE_NONEXISTENT) continue;
+        PairOut o;
+        double* pf = &pft[3 * (size_t)cc];
+        double in[3] = {pf[0], pf[1], pf[2]};
+        int rc = pair_force(ll, i, in, pf, o);
+        if (rc) { char b[96]; snprintf(b, sizeof b, "distance between particles is zero: %d %d", ll + 1, i + 1); return fail(rc, b); }
+        if (!o.contact) continue;
+        n_contacts++;
+        for (int c = 0; c < 3; ++c) { X(fc, c)[ll] = X(fc, c)[ll] + o.fc[c]; }
+        for (int c = 0; c < 3; ++c) { X(fc, c)[i] = X(fc, c)[i] - o.fc[c]; }
+        for (int c = 0; c < 3; ++c) { X(tow, c)[ll] = X(tow, c)[ll] + o.tl[c]; }
+        for (int c = 0; c < 3; ++c) { X(tow, c)[i] = X(tow, c)[i] + o.ti[c]; }
+        if (o.roll_l) for (int c = 0; c < 3; ++c) X(tow, c)[ll] = X(tow, c)[ll] + o.rl[c];
+        if (o.roll_i) for (int c = 0; c < 3; ++c) X(tow, c)[i] = X(tow, c)[i] + o.ri[c];
+      }
+    }
+    return 0;
+  }
+
+#ifdef _OPENMP
+  // OpenMP mode of the same loop (the reference's SMP build: !$omp do over
+  // LL with !$omp atomic scatter, calc_force_dem.f:139-412).  Used only to
+  // time the CPU baseline; its summation order is not deterministic.
+  int calc_force_omp() {
+    int rc_all = 0;
+    int64_t ncont = 0;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads) reduction(+ : ncont)
+    for (int ll = 0; ll < n; ++ll) {
+      if (state[ll] == DEM_STATE_NONEXISTENT) continue;
+      int s = ll ? row_end[ll - 1] : 0, e = row_end[ll];
+      for (int cc = s; cc < e; ++cc) {
+        int i = nbrs[cc];
+        if (state[i] == DEM_STATE_NONEXISTENT) continue;
+        PairOut o;
+        double* pf = &pft[3 * (size_t)cc];
+        double in[3] = {pf[0], pf[1], pf[2]};
+        int rc = pair_force(ll, i, in, pf, o);
+        if (rc) { rc_all = rc; continue; }
+        if (!o.contact) continue;
+        ncont++;
+        for (int c = 0; c < 3; ++c) {
+#pragma omp atomic
+          fc[(size_t)c * n + ll] += o.fc[c];
+#pragma omp atomic
+          fc[(size_t)c * n + i] -= o.fc[c];
+#pragma omp atomic
+          tow[(size_t)c * n + ll] += o.tl[c];
+#pragma omp atomic
+          tow[(size_t)c * n + i] += o.ti[c];
+          if (o.roll_l) {
+#pragma omp atomic
+            tow[(size_t)c * n + ll] += o.rl[c];
+          }
+          if (o.roll_i) {
+#pragma omp atomic
+            tow[(size_t)c * n + i] += o.ri[c];
+          }
+        }
+      }
+    }
+    n_contacts = ncont;
+    if (rc_all) return fail(rc_all, "distance between particles is zero");
+    return 0;
+  }
+#endif
+
+  // CFUPDATEOLD + CFNEWVALUES (cfupdateold.f:33-41, cfnewvalues.f:669-812).
+  void cfnewvalues() {
+    const double dt = p.dtsolid;
+    if (first_pass && p.intg_method == DEM_INTG_AB2) {
+      for (int l = 0; l < n; ++l) {
+        // cfnewvalues.f:672-676: skip NONEXISTENT, ENTERING(_GHOST), GHOST and
+        // RIGID_MOTION_GHOST (functions.inc:858-880).
+        int s = state[l];
+        if (s == DEM_STATE_NONEXISTENT || s == DEM_STATE_ENTERING || s == 102) continue;
+        if (s == DEM_STATE_NORMAL_GHOST || s == 110) continue;
+        for (int c = 0; c < 3; ++c) {
+          X(acc_old, c)[l] = P(fc, l, c) / pmass[l] + p.grav[c];
+          X(rot_acc_old, c)[l] = P(tow, l, c);
+        }
+      }
+    }
+    if (p.intg_method == DEM_INTG_EULER) {
+      for (int c = 0; c < 3; ++c) {
+        double* v = X(vel, c); double* x = X(pos, c); double* f = X(fc, c);
+        for (int l = 0; l < n; ++l) if (state[l] == DEM_STATE_NORMAL) v[l] = v[l] + dt * (f[l] / pmass[l] + p.grav[c]);
+        for (int l = 0; l < n; ++l) if (state[l] < DEM_STATE_NORMAL_GHOST) x[l] = x[l] + v[l] * dt;
+        for (int l = 0; l < n; ++l) f[l] = 0.0;
+      }
+      for (int c = 0; c < 3; ++c) {
+        double* w = X(omg, c); double* t = X(tow, c);
+        for (int l = 0; l < n; ++l) if (state[l] == DEM_STATE_NORMAL) w[l] = w[l] + t[l] * omoi[l] * dt;
+        for (int l = 0; l < n; ++l) t[l] = 0.0;
+      }
+    } else {
+      for (int c = 0; c < 3; ++c) {
+        double* v = X(vel, c); double* x = X(pos, c); double* f = X(fc, c); double* a = X(acc_old, c);
+        for (int l = 0; l < n; ++l) {
+          // CFUPDATEOLD copies NEW into OLD for existing non-ghost particles.
+          double vold = v[l], xold = x[l];
+          if (state[l] == DEM_STATE_NORMAL) f[l] = f[l] / pmass[l] + p.grav[c];
+          if (state[l] == DEM_STATE_NORMAL) v[l] = vold + 0.5 * (3.0 * f[l] - a[l]) * dt;
+          a[l] = f[l];
+          if (state[l] < DEM_STATE_NORMAL_GHOST) x[l] = xold + 0.5 * (vold + v[l]) * dt;
+          f[l] = 0.0;
+        }
+      }
+      for (int c = 0; c < 3; ++c) {
+        double* w = X(omg, c); double* t = X(tow, c); double* ra = X(rot_acc_old, c);
+        for (int l = 0; l < n; ++l) {
+          double wold = w[l];
+          if (state[l] == DEM_STATE_NORMAL) w[l] = wold + 0.5 * (3.0 * t[l] * omoi[l] - ra[l]) * dt;
+          if (state[l] == DEM_STATE_NORMAL) ra[l] = t[l] * omoi[l];
+          t[l] = 0.0;
+        }
+      }
+    }
+    first_pass = false;
+  }
+
+  // DES_TIME_STEP(NN) for pure DEM (des_time_march.f:342-432).
+  int step(int nn) {
+    int rc = calc_force();
+    if (rc) return rc;
+    cfnewvalues();
+    bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0);
+    bool anyper = p.periodic[0] || p.periodic[1] || (p.periodic[2] && !p.no_k);
+    if (do_nsearch || anyper) desgrid_pic();
+    if (do_nsearch) neighbour();
+    s_time = s_time + p.dtsolid;
+    steps_done++;
+    return 0;
+  }
+};
+
+}  // namespace
+
+struct orc_handle { Oracle o; };
+
+extern "C" {
+
+int orc_create(const dem_params* p, int32_t max_pip, orc_handle** out) {
+  if (!p || !out || max_pip <= 0) return DEM_ERR_ARG;
+  if (p->dg_imax < 1 || p->dg_jmax < 1 || (!p->no_k && p->dg_kmax < 1)) return DEM_ERR_ARG;
+  if (p->n_phases < 1 || p->n_phases > DEM_MAX_PHASES) return DEM_ERR_ARG;
+  auto* h = new orc_handle();
+  Oracle& o = h->o;
+  o.p = *p;
+  o.n = max_pip;
+  o.cmax = p->collision_array_max > 0 ? p->collision_array_max : 8;
+  o.grid_init();
+  size_t n3 = (size_t)3 * max_pip;
+  o.pos.assign(n3, 0.0); o.vel.assign(n3, 0.0); o.omg.assign(n3, 0.0);
+  o.fc.assign(n3, 0.0); o.tow.assign(n3, 0.0); o.acc_old.assign(n3, 0.0); o.rot_acc_old.assign(n3, 0.0);
+  o.rad.assign(max_pip, 0.0); o.pmass.assign(max_pip, 0.0); o.omoi.assign(max_pip, 0.0);
+  o.state.assign(max_pip, 0); o.phase.assign(max_pip, 0);
+  o.dg_pijk.assign(max_pip, 0);
+  o.row_end.assign(max_pip, 0);
+  o.wall_fid.assign((size_t)o.cmax * max_pip, -1);
+  o.wall_pft.assign((size_t)3 * o.cmax * max_pip, 0.0);
+  o.fbin_start.assign(o.ncell2 + 1, 0);
+  *out = h;
+  return 0;
+}
+
+int orc_destroy(orc_handle* h) { delete h; return 0; }
+const char* orc_last_error(const orc_handle* h) { return h ? h->o.err.c_str() : "null handle"; }
+int orc_set_threads(orc_handle* h, int32_t nt) { h->o.nthreads = nt < 1 ? 1 : nt; return 0; }
+
+int orc_set_walls(orc_handle* h, const double* vertex, const double* norm_face, int32_t nf) {
+  Oracle& o = h->o;
+  if (nf < 0) return DEM_ERR_ARG;
+  o.nf = nf;
+  o.vertex.assign(vertex, vertex + (size_t)9 * nf);
+  o.norm_face.assign(norm_face, norm_face + (size_t)3 * nf);
+  o.bin_facets();
+  return 0;
+}
+
+int orc_upload_state(orc_handle* h, const double* pos, const double* vel, const double* omega,
+                     const double* radius, const double* pmass, const double* omoi,
+                     const int8_t* state, const int32_t* phase, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return o.fail(DEM_ERR_ARG, "max_pip mismatch");
+  size_t n3 = (size_t)3 * o.n;
+  std::copy(pos, pos + n3, o.pos.begin());
+  std::copy(vel, vel + n3, o.vel.begin());
+  std::copy(omega, omega + n3, o.omg.begin());
+  std::copy(radius, radius + o.n, o.rad.begin());
+  std::copy(pmass, pmass + o.n, o.pmass.begin());
+  std::copy(omoi, omoi + o.n, o.omoi.begin());
+  std::copy(state, state + o.n, o.state.begin());
+  for (int i = 0; i < o.n; ++i) {
+    int ph = phase[i] - 1;
+    if (o.state[i] != DEM_STATE_NONEXISTENT && (ph < 0 || ph >= o.p.n_phases))
+      return o.fail(DEM_ERR_ARG, "phase out of range");
+    o.phase[i] = ph < 0 ? 0 : ph;
+  }
+  o.have_state = true;
+  return 0;
+}
+
+int orc_download_state(orc_handle* h, double* pos, double* vel, double* omega, int8_t* state, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return DEM_ERR_ARG;
+  size_t n3 = (size_t)3 * o.n;
+  if (pos) std::copy(o.pos.begin(), o.pos.begin() + n3, pos);
+  if (vel) std::copy(o.vel.begin(), o.vel.begin() + n3, vel);
+  if (omega) std::copy(o.omg.begin(), o.omg.begin() + n3, omega);
+  if (state) std::copy(o.state.begin(), o.state.end(), state);
+  return 0;
+}
+
+int orc_download_forces(orc_handle* h, double* fc, double* tow, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return DEM_ERR_ARG;
+  if (fc) std::copy(o.fc.begin(), o.fc.end(), fc);
+  if (tow) std::copy(o.tow.begin(), o.tow.end(), tow);
+  return 0;
+}
+
+int orc_set_ab2_history(orc_handle* h, const double* acc_old, const double* rot_acc_old,
+                        int32_t first_pass, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return DEM_ERR_ARG;
+  if (acc_old) std::copy(acc_old, acc_old + (size_t)3 * o.n, o.acc_old.begin());
+  if (rot_acc_old) std::copy(rot_acc_old, rot_acc_old + (size_t)3 * o.n, o.rot_acc_old.begin());
+  o.first_pass = first_pass != 0;
+  return 0;
+}
+
+int orc_get_ab2_history(orc_handle* h, double* acc_old, double* rot_acc_old, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return DEM_ERR_ARG;
+  if (acc_old) std::copy(o.acc_old.begin(), o.acc_old.end(), acc_old);
+  if (rot_acc_old) std::copy(o.rot_acc_old.begin(), o.rot_acc_old.end(), rot_acc_old);
+  return 0;
+}
+
+int orc_pair_count(orc_handle* h, int64_t* np) { *np = (int64_t)h->o.nbrs.size(); return 0; }
+
+int orc_download_pairs(orc_handle* h, int32_t* ni, int32_t* nb, double* pf, int64_t cap, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return DEM_ERR_ARG;
+  if ((nb || pf) && cap < (int64_t)o.nbrs.size()) return o.fail(DEM_ERR_CAPACITY, "pair capacity too small");
+  if (ni) for (int i = 0; i < o.n; ++i) ni[i] = o.row_end[i] + 1;
+  if (nb) for (size_t c = 0; c < o.nbrs.size(); ++c) nb[c] = o.nbrs[c] + 1;
+  if (pf) std::copy(o.pft.begin(), o.pft.end(), pf);
+  return 0;
+}
+
+int orc_upload_pairs(orc_handle* h, const int32_t* ni, const int32_t* nb, const double* pf,
+                     int64_t np, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return DEM_ERR_ARG;
+  o.row_end.resize(o.n);
+  for (int i = 0; i < o.n; ++i) o.row_end[i] = ni[i] - 1;
+  o.nbrs.resize(np);
+  for (int64_t c = 0; c < np; ++c) o.nbrs[c] = nb[c] - 1;
+  o.pft.assign(pf, pf + 3 * np);
+  return 0;
+}
+
+int orc_download_wall_history(orc_handle* h, int32_t* fid, double* pf, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return DEM_ERR_ARG;
+  if (fid) for (size_t s = 0; s < o.wall_fid.size(); ++s) fid[s] = o.wall_fid[s] < 0 ? -1 : o.wall_fid[s] + 1;
+  if (pf) std::copy(o.wall_pft.begin(), o.wall_pft.end(), pf);
+  return 0;
+}
+
+int orc_download_cells(orc_handle* h, int32_t* cells, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n) return DEM_ERR_ARG;
+  std::copy(o.dg_pijk.begin(), o.dg_pijk.end(), cells);
+  return 0;
+}
+
+int orc_download_facet_bins(orc_handle* h, int32_t* start, int32_t* ids, int32_t cap, int32_t* nc) {
+  Oracle& o = h->o;
+  *nc = o.ncell2;
+  if (start) for (int c = 0; c <= o.ncell2; ++c) start[c] = o.fbin_start[c];
+  if (ids) {
+    if (cap < (int32_t)o.fbin.size()) return DEM_ERR_CAPACITY;
+    for (size_t q = 0; q < o.fbin.size(); ++q) ids[q] = o.fbin[q].id + 1;
+  }
+  return 0;
+}
+
+int orc_download_edge_flags(orc_handle* h, int8_t* flags) {
+  std::copy(h->o.ignore_edge.begin(), h->o.ignore_edge.end(), flags);
+  return 0;
+}
+
+int orc_desgrid_pic(orc_handle* h) { h->o.desgrid_pic(); return 0; }
+int orc_neighbour(orc_handle* h) { h->o.neighbour(); return 0; }
+int orc_calc_force(orc_handle* h) { return h->o.calc_force(); }
+int orc_cfnewvalues(orc_handle* h) { h->o.cfnewvalues(); return 0; }
+int orc_init_neighbors(orc_handle* h) {
+  if (!h->o.have_state) return DEM_ERR_STATE;
+  h->o.desgrid_pic();
+  h->o.row_end.assign(h->o.n, 0); h->o.nbrs.clear(); h->o.pft.clear();
+  h->o.neighbour();
+  return 0;
+}
+int orc_step(orc_handle* h, int32_t nn_first, int32_t nsteps) {
+  for (int32_t k = 0; k < nsteps; ++k) {
+    int rc = h->o.step(nn_first + k);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int orc_get_stats(orc_handle* h, dem_stats* s) {
+  Oracle& o = h->o;
+  std::memset(s, 0, sizeof *s);
+  double mv[3] = {0, 0, 0}, msum = 0, ysum = 0, ke = 0;
+  int64_t nn = 0;
+  for (int i = 0; i < o.n; ++i) {
+    if (o.state[i] != DEM_STATE_NORMAL) continue;
+    nn++;
+    for (int c = 0; c < 3; ++c) mv[c] += o.P(o.vel, i, c);
+    msum += o.pmass[i]; ysum += o.pmass[i] * o.P(o.pos, i, 1);
+    double v2 = 0; for (int c = 0; c < 3; ++c) v2 += o.P(o.vel, i, c) * o.P(o.vel, i, c);
+    ke += 0.5 * o.pmass[i] * v2;
+  }
+  for (int c = 0; c < 3; ++c) mv[c] = nn ? mv[c] / nn : 0.0;
+  double gt[3] = {0, 0, 0};
+  for (int i = 0; i < o.n; ++i) {
+    if (o.state[i] != DEM_STATE_NORMAL) continue;
+    for (int c = 0; c < 3; ++c) { double d = o.P(o.vel, i, c) - mv[c]; gt[c] += d * d; }
+  }
+  for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn ? gt[c] / nn : 0.0; }
+  s->n_normal = nn;
+  s->n_pairs = (int64_t)o.nbrs.size();
+  s->n_contacts = o.n_contacts;
+  s->n_wall_contacts = o.n_wall_contacts;
+  s->n_rogue_removed = o.rogue_removed;
+  s->steps_done = o.steps_done;
+  s->kinetic_energy = ke;
+  s->bed_height = msum > 0 ? ysum / msum : 0.0;
+  s->s_time = o.s_time;
+  return 0;
+}
+
+int orc_set_gas_fields(orc_handle* h, const dem_fluid_grid*, const double*, const double*,
+                       const double*, const double*, const double*) {
+  return h->o.fail(DEM_ERR_STATE, "coupling not available in this build");
+}
+int orc_get_mean_fields(orc_handle* h, double*, double*) { return h->o.fail(DEM_ERR_STATE, "coupling not available"); }
+int orc_comp_mean_fields(orc_handle* h) { return h->o.fail(DEM_ERR_STATE, "coupling not available"); }
+int orc_drag_gs_des0(orc_handle* h) { return h->o.fail(DEM_ERR_STATE, "coupling not available"); }
+int orc_step_coupled(orc_handle* h, int32_t, int32_t) { return h->o.fail(DEM_ERR_STATE, "coupling not available"); }
+
+// CHECK_SOLIDS_DEM_COLL_LSD (check_solids_dem.f:519-782) and
+// CHECK_SOLIDS_DEM_COLL_HERTZ (798-1122), DEM phases only (MMAX = 0).
+int orc_contact_constants(dem_params* p, const double* ref_radius, const double* ref_mass,
+                          const double* e_young, const double* v_poisson,
+                          const double* en_in, const double* et_in,
+                          const double* en_w_in, const double* et_w_in,
+                          double ew_young, double vw_poisson,
+                          double kt_fac, double kt_w_fac,
+                          double des_etat_fac, double des_etat_w_fac,
+                          double dtsolid_factor, double* tcoll_out) {
+  const int M = p->n_phases, S = DEM_MAX_PHASES;
+  const double PI = 4.0 * std::atan(1.0);
+  double tcoll = UNDEFINED;
+  if (p->coll_model == DEM_COLL_LSD) {
+    p->kt = kt_fac * p->kn;
+    p->kt_w = kt_w_fac * p->kn_w;
+    for (int m = 0; m < M; ++m) {
+      double mass_m = ref_mass[m];
+      for (int l = m; l < M; ++l) {
+        double en = en_in[m * S + l];
+        double mass_l = ref_mass[l];
+        double mass_eff = mass_m * mass_l / (mass_m + mass_l);
+        double etan;
+        if (en != 0.0) {
+          etan = 2.0 * std::sqrt(p->kn * mass_eff) * std::fabs(std::log(en));
+          etan = etan / std::sqrt(PI * PI + (std::log(en) * std::log(en)));
+        } else {
+          etan = 2.0 * std::sqrt(p->kn * mass_eff);
+        }
+        double tc;
+        if (en != 0.0) tc = PI / std::sqrt(p->kn / mass_eff - ((etan / mass_eff) * (etan / mass_eff)) / 4.0);
+        else tc = PI / std::sqrt(p->kn / mass_eff);
+        tcoll = std::min(tc, tcoll);
+        etan = etan / std::sqrt(mass_eff);
+        p->des_etan[m * S + l] = etan; p->des_etat[m * S + l] = des_etat_fac * etan;
+        p->des_etan[l * S + m] = p->des_etan[m * S + l]; p->des_etat[l * S + m] = p->des_etat[m * S + l];
+      }
+      double en = en_w_in[m];
+      double mass_eff = mass_m;
+      double etan;
+      if (en != 0.0) {
+        etan = 2.0 * std::sqrt(p->kn_w * mass_eff) * std::fabs(std::log(en));
+        etan = etan / std::sqrt(PI * PI + (std::log(en) * std::log(en)));
+      } else {
+        etan = 2.0 * std::sqrt(p->kn_w * mass_eff);
+      }
+      etan = etan / std::sqrt(mass_eff);
+      p->des_etan_wall[m] = etan;
+      p->des_etat_wall[m] = des_etat_w_fac * etan;
+    }
+  } else {
+    double g_wall = 0.5 * ew_young / (1.0 + vw_poisson);
+    double gm[DEM_MAX_PHASES];
+    for (int m = 0; m < M; ++m) gm[m] = 0.5 * e_young[m] / (1.0 + v_poisson[m]);
+    for (int m = 0; m < M; ++m) {
+      double mass_m = ref_mass[m];
+      for (int l = m; l < M; ++l) {
+        double en = en_in[m * S + l], et = et_in[m * S + l];
+        double mass_l = ref_mass[l];
+        double mass_eff = (mass_m * mass_l) / (mass_m + mass_l);
+        double red = (2.0 / 7.0) * mass_eff;
+        double r_eff = ref_radius[m] * ref_radius[l] / (ref_radius[m] + ref_radius[l]);
+        double e_eff = e_young[m] * e_young[l] /
+            (e_young[m] * (1.0 - v_poisson[l] * v_poisson[l]) + e_young[l] * (1.0 - v_poisson[m] * v_poisson[m]));
+        double g_eff = gm[m] * gm[l] / (gm[m] * (2.0 - v_poisson[l]) + gm[l] * (2.0 - v_poisson[m]));
+        double hkn = (4.0 / 3.0) * std::sqrt(r_eff) * e_eff;
+        double hkt = 8.0 * std::sqrt(r_eff) * g_eff;
+        double etan, etat;
+        if (en != 0.0) {
+          etan = std::sqrt(5.0) * std::sqrt(hkn * mass_eff) * std::fabs(std::log(en));
+          etan = etan / std::sqrt(PI * PI + (std::log(en) * std::log(en)));
+        } else etan = std::sqrt(5.0) * std::sqrt(hkn * mass_eff);
+        if (et != 0.0) {
+          etat = std::sqrt(5.0) * std::sqrt(hkt * red) * std::fabs(std::log(et));
+          etat = etat / std::sqrt(PI * PI + (std::log(et) * std::log(et)));
+        } else etat = std::sqrt(5.0) * std::sqrt(hkt * red);
+        double tc;
+        if (en != 0.0) tc = PI / std::sqrt(hkn / mass_eff - ((etan / mass_eff) * (etan / mass_eff)) / 5.0);
+        else tc = PI / std::sqrt(hkn / mass_eff);
+        tcoll = std::min(tc, tcoll);
+        etan = etan / std::sqrt(hkn * mass_eff);
+        etat = etat / std::sqrt(hkt * mass_eff);
+        hkn = hkn / std::sqrt(r_eff);
+        hkt = hkt / std::sqrt(r_eff);
+        p->hert_kn[m * S + l] = p->hert_kn[l * S + m] = hkn;
+        p->hert_kt[m * S + l] = p->hert_kt[l * S + m] = hkt;
+        p->des_etan[m * S + l] = p->des_etan[l * S + m] = etan;
+        p->des_etat[m * S + l] = p->des_etat[l * S + m] = etat;
+      }
+      double en = en_w_in[m], et = et_w_in[m];
+      double mass_eff = mass_m, red = (2.0 / 7.0) * mass_eff;
+      double r_eff = ref_radius[m];
+      double e_eff = e_young[m] * ew_young /
+          (e_young[m] * (1.0 - vw_poisson * vw_poisson) + ew_young * (1.0 - v_poisson[m] * v_poisson[m]));
+      double g_eff = gm[m] * g_wall / (gm[m] * (2.0 - vw_poisson) + g_wall * (2.0 - v_poisson[m]));
+      double hkwn = (4.0 / 3.0) * std::sqrt(r_eff) * e_eff;
+      double hkwt = (double)8.0f * std::sqrt(r_eff) * g_eff;
+      double etan, etat;
+      if (en != 0.0) {
+        etan = std::sqrt(5.0) * std::sqrt(hkwn * mass_eff) * std::fabs(std::log(en));
+        etan = etan / std::sqrt(PI * PI + (std::log(en) * std::log(en)));
+      } else etan = std::sqrt(5.0) * std::sqrt(hkwn * mass_eff);
+      if (et != 0.0) {
+        etat = std::sqrt(5.0) * std::sqrt(hkwt * red) * std::fabs(std::log(et));
+        etat = etat / std::sqrt(PI * PI + (std::log(et) * std::log(et)));
+      } else etat = std::sqrt(5.0) * std::sqrt(hkwt * red);
+      p->des_etan_wall[m] = etan / std::sqrt(hkwn * mass_eff);
+      p->des_etat_wall[m] = etat / std::sqrt(hkwt * mass_eff);
+      p->hert_kwn[m] = hkwn / std::sqrt(r_eff);
+      p->hert_kwt[m] = hkwt / std::sqrt(r_eff);
+    }
+  }
+  if (tcoll_out) *tcoll_out = tcoll;
+  p->dtsolid = tcoll / dtsolid_factor;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+"""Small DEM cases shared by the oracle and GPU parity tests.
+
+Each builder returns (params, arrays, walls) where arrays holds the DES
+arrays in Fortran layout ((3, n) for vectors, 1-based phases).
+"""
+import math
+
+import numpy as np
+
+from mfix_dem import abi
+from mfix_dem import params as P
+
+
+def state_arrays(pos, vel, omega, radius, rho, phase=None):
+    n = pos.shape[1]
+    _, pmass, omoi = P.particle_props(radius, rho)
+    st = np.full(n, abi.DEM_STATE_NORMAL, dtype=np.int8)
+    ph = np.ones(n, np.int32) if phase is None else np.asarray(phase, np.int32)
+    return {"pos": pos, "vel": vel, "omega": omega, "radius": np.asarray(radius, float),
+            "pmass": pmass, "omoi": omoi, "state": st, "phase": ph}
+
+
+def dem01_case(intg, kn, en):
+    """DEM01 (tests/dem/DEM01/mfix.dat): one 0.2 m sphere dropped from
+    y = 0.5 m in a 1 m box, LSD, default walls, one DES cell."""
+    case = P.DemCase(d_p0=(0.2,), ro_s0=(2600.0,), coll_model="LSD", intg_method=intg,
+                     kn=kn, kn_w=kn, des_en_input=en, des_en_wall_input=[en],
+                     grav=(0.0, -9.80665, 0.0), neighbor_search_n=99, desgridsearch=(1, 1, 1))
+    arr = state_arrays(np.array([[0.6], [0.5], [0.6]]), np.zeros((3, 1)), np.zeros((3, 1)),
+                       np.array([0.1]), np.array([2600.0]))
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    walls = P.default_walls(case.domain_lo, case.domain_hi)
+    return case, prm, arr, walls
+
+
+def settling_case(n_side=(6, 20, 6), d=1e-3, rho=2500.0, box=(12e-3, 60e-3, 12e-3),
+                  spacing=1.1, jitter=0.04, vmax=0.1, seed=1000, coll="LSD", intg="EULER",
+                  kn=1000.0, en=0.9, mew=0.1, nsn=25, polydisperse=0.0, mew_r=0.0,
+                  periodic=(False, False, False), precision=abi.DEM_PREC_FP64):
+    """Dry granular settling: spheres on a cubic lattice of spacing `spacing`*d
+    with seeded jitter and velocities, default box walls, gravity -9.81 in y.
+    The 4,000-sphere LSD instance of this builder (n_side=(10,40,10)) is the
+    reference-runnable settling workload; smaller n_side are parity cases."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = n_side
+    n = nx * ny * nz
+    a = spacing * d
+    # order: y fastest, then x, then z (the DES cell key order, j fastest)
+    kk, ii, jj = np.meshgrid(np.arange(nz), np.arange(nx), np.arange(ny), indexing="ij")
+    x0 = np.array(box) * 0.0
+    pos = np.empty((3, n))
+    pos[0] = (ii.ravel() + 0.5) * a + (box[0] - nx * a) * 0.5
+    pos[1] = (jj.ravel() + 0.5) * a + 0.5 * a * 0.0 + 1e-5
+    pos[2] = (kk.ravel() + 0.5) * a + (box[2] - nz * a) * 0.5
+    pos += rng.uniform(-jitter * d, jitter * d, size=pos.shape)
+    vel = rng.uniform(-vmax, vmax, size=(3, n))
+    omega = np.zeros((3, n))
+    if polydisperse > 0:
+        diam = np.clip(d * np.exp(rng.normal(0.0, polydisperse, n)), 0.5 * d, 2.0 * d)
+        diam = np.minimum(diam, a * 0.95)
+    else:
+        diam = np.full(n, d)
+    radius = 0.5 * diam
+    arr = state_arrays(pos, vel, omega, radius, np.full(n, rho))
+    dmax = float(np.max(diam))
+    kw = {}
+    if coll == "HERTZ":
+        kw = dict(e_young=(1e7,), v_poisson=(0.3,), ew_young=1e7, vw_poisson=0.3,
+                  des_et_input=en, des_et_wall_input=[en])
+    case = P.DemCase(d_p0=(dmax,), ro_s0=(rho,), coll_model=coll, intg_method=intg,
+                     kn=kn, kn_w=kn, des_en_input=en, des_en_wall_input=[en],
+                     mew=mew, mew_w=mew, mew_r=mew_r, mew_rw=mew_r,
+                     grav=(0.0, -9.81, 0.0), domain_hi=box, fluid_cells=(1, 1, 1),
+                     neighbor_search_n=nsn, periodic=periodic, force_precision=precision, **kw)
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    walls = P.default_walls(case.domain_lo, case.domain_hi, periodic=periodic)
+    return case, prm, arr, walls
+
+
+def make_system(cls, prm, arr, walls, **kw):
+    s = cls(prm, arr["pos"].shape[1], **kw)
+    s.set_walls(*walls)
+    s.upload_state(arr["pos"], arr["vel"], arr["omega"], arr["radius"], arr["pmass"],
+                   arr["omoi"], arr["state"], arr["phase"])
+    s.init_neighbors()
+    return s
