@@ -244,6 +244,21 @@ int dem_get_stats(dem_handle* h, dem_stats* out);
 /* Number of kernels this handle has launched so far (for launch accounting). */
 int dem_launch_count(const dem_handle* h, int64_t* count);
 
+/* Kernel-time accounting: when on, every kernel the handle launches is
+ * bracketed by CUDA events on its stream and its time is added to one of
+ * these classes. */
+#define DEM_PROF_FORCE     0   /* contact force (+ fused integration) */
+#define DEM_PROF_NEIGHBOR  1   /* pair-list build, history carry-over, transpose */
+#define DEM_PROF_DESGRID   2   /* cell keys and per-cell lists */
+#define DEM_PROF_INTEGRATE 3   /* stand-alone CFNEWVALUES */
+#define DEM_PROF_COUPLING  4   /* drag and mean fields */
+#define DEM_PROF_OTHER     5
+#define DEM_PROF_N         6
+int dem_set_profiling(dem_handle* h, int32_t on);
+/* Milliseconds and launch counts per class since profiling was switched on
+ * (synchronizes the handle's stream). */
+int dem_get_profile(dem_handle* h, double* ms, int64_t* launches);
+
 /* Sets the CUDA stream (cudaStream_t passed as void*) used by the handle.
  * NULL selects the legacy default stream. */
 int dem_set_stream(dem_handle* h, void* stream);

@@ -1,0 +1,637 @@
+// capi.cu -- the C ABI of include/dem_b200.h.
+//
+// Owns device allocation, host<->device conversion between the Fortran
+// layouts of the DES arrays and the packed device layout, and the
+// DES_TIME_STEP sequence (model/des/des_time_march.f:342-432).
+#include "dem_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+using namespace demb;
+
+namespace demb {
+
+int set_err(dem_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int check_cuda(dem_handle* h, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return 0;
+  char b[256];
+  snprintf(b, sizeof b, "%s: %s", what, cudaGetErrorString(e));
+  return set_err(h, DEM_ERR_CUDA, b);
+}
+
+// Packs Fortran (n,3) columns + scalars into double4 arrays.
+__global__ void k_pack(int n, const double* __restrict__ v3, const double* __restrict__ s, double4* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = make_double4(v3[i], v3[(size_t)n + i], v3[2 * (size_t)n + i], s ? s[i] : 0.0);
+}
+__global__ void k_pack_keepw(int n, const double* __restrict__ v3, double4* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 o = out[i];
+  out[i] = make_double4(v3[i], v3[(size_t)n + i], v3[2 * (size_t)n + i], o.w);
+}
+__global__ void k_unpack(int n, const double4* __restrict__ in, double* __restrict__ v3) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 a = in[i];
+  v3[i] = a.x; v3[(size_t)n + i] = a.y; v3[2 * (size_t)n + i] = a.z;
+}
+__global__ void k_phase_in(int n, const int* __restrict__ ph, const int8_t* __restrict__ st, uint8_t* __restrict__ out,
+                           int nph, unsigned* __restrict__ bad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int p = ph[i] - 1;
+  if (st[i] != DEM_STATE_NONEXISTENT && (p < 0 || p >= nph)) { atomicOr(bad, 1u); p = 0; }
+  out[i] = (uint8_t)(p < 0 ? 0 : p);
+}
+
+// Per-block partial sums for statistics; the host adds the partials in
+// block order, so the result is deterministic.
+constexpr int STAT_T = 256;
+__global__ void k_stats1(int n, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+                         const int8_t* __restrict__ state, double* __restrict__ part) {
+  __shared__ double sh[8][STAT_T];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (i < n && state[i] == DEM_STATE_NORMAL) {
+    double4 p = pos4[i], u = vel4[i];
+    v[0] = 1.0; v[1] = u.x; v[2] = u.y; v[3] = u.z;
+    v[4] = u.w; v[5] = u.w * p.y;
+    v[6] = 0.5 * u.w * (u.x * u.x + u.y * u.y + u.z * u.z);
+    v[7] = 0.0;
+  }
+  for (int k = 0; k < 8; ++k) sh[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int s = STAT_T / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) for (int k = 0; k < 8; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) for (int k = 0; k < 8; ++k) part[(size_t)blockIdx.x * 8 + k] = sh[k][0];
+}
+__global__ void k_stats2(int n, const double4* __restrict__ vel4, const int8_t* __restrict__ state,
+                         double mx, double my, double mz, double* __restrict__ part) {
+  __shared__ double sh[3][STAT_T];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[3] = {0, 0, 0};
+  if (i < n && state[i] == DEM_STATE_NORMAL) {
+    double4 u = vel4[i];
+    v[0] = (u.x - mx) * (u.x - mx); v[1] = (u.y - my) * (u.y - my); v[2] = (u.z - mz) * (u.z - mz);
+  }
+  for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int s = STAT_T / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) for (int k = 0; k < 3; ++k) part[(size_t)blockIdx.x * 3 + k] = sh[k][0];
+}
+
+int fetch_errors(dem_handle* h) {
+  if (int rc = check_cuda(h, cudaMemcpyAsync(h->herr, h->derr, sizeof(DevErr), cudaMemcpyDeviceToHost, h->stream), "copy err")) return rc;
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
+  unsigned f = h->herr->flags;
+  if (!f) return 0;
+  // clear the flags for the next call
+  unsigned z = 0;
+  cudaMemcpyAsync(&h->derr->flags, &z, sizeof(unsigned), cudaMemcpyHostToDevice, h->stream);
+  cudaStreamSynchronize(h->stream);
+  char b[200];
+  if (f & EF_ZERO_DIST) {
+    snprintf(b, sizeof b, "distance between particles is zero: %d %d", h->herr->zero_a + 1, h->herr->zero_b + 1);
+    return set_err(h, DEM_ERR_ZERO_DISTANCE, b);
+  }
+  if (f & EF_WALL_SLOTS) return set_err(h, DEM_ERR_WALL_SLOTS, "Error: COLLISION_ARRAY_MAX too small.");
+  if (f & EF_ROGUE_FATAL) return set_err(h, DEM_ERR_ROGUE, "NORMAL particle found in GHOST cell (remove_rogue = 0)");
+  if (f & EF_PAIR_CAP) return set_err(h, DEM_ERR_PAIR_OVERFLOW, "pair list capacity exceeded");
+  return set_err(h, DEM_ERR_STATE, "device error flags set");
+}
+
+void* stage_buffer(dem_handle* h, size_t bytes) {
+  if (bytes > h->stage_bytes) {
+    if (h->stage) cudaFree(h->stage);
+    h->stage = nullptr;
+    h->stage_bytes = 0;
+    if (cudaMalloc(&h->stage, bytes) != cudaSuccess) return nullptr;
+    h->stage_bytes = bytes;
+  }
+  return h->stage;
+}
+
+static cudaEvent_t pool_event(dem_handle* h) {
+  if (!h->ev_pool.empty()) { cudaEvent_t e = h->ev_pool.back(); h->ev_pool.pop_back(); return e; }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+ProfScope::ProfScope(dem_handle* hh, int cls) : h(hh) {
+  if (!h->prof) return;
+  dem_handle::ProfEv ev{cls, pool_event(h), pool_event(h)};
+  cudaEventRecord(ev.a, h->stream);
+  h->prof_pending.push_back(ev);
+  idx = (int)h->prof_pending.size() - 1;
+}
+ProfScope::~ProfScope() {
+  if (idx < 0) return;
+  cudaEventRecord(h->prof_pending[idx].b, h->stream);
+}
+
+static void prof_collect(dem_handle* h) {
+  if (h->prof_pending.empty()) return;
+  cudaStreamSynchronize(h->stream);
+  for (auto& e : h->prof_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+      h->prof_ms[e.cls] += ms;
+      h->prof_n[e.cls] += 1;
+    }
+    h->ev_pool.push_back(e.a);
+    h->ev_pool.push_back(e.b);
+  }
+  h->prof_pending.clear();
+}
+
+}  // namespace demb
+
+static void fill_devparams(dem_handle* h) {
+  const dem_params& q = h->prm;
+  DevParams& p = h->dp;
+  memset(&p, 0, sizeof p);
+  p.n = h->n;
+  p.coll = q.coll_model; p.intg = q.intg_method; p.nph = q.n_phases; p.no_k = q.no_k;
+  p.cmax = q.collision_array_max > 0 ? q.collision_array_max : 8;
+  p.remove_rogue = q.remove_rogue;
+  for (int a = 0; a < 3; ++a) {
+    p.per[a] = q.periodic[a] ? 1 : 0;
+    p.grav[a] = q.grav[a];
+    p.lo[a] = q.domain_lo[a]; p.hi[a] = q.domain_hi[a];
+    p.L[a] = q.domain_hi[a] - q.domain_lo[a];
+  }
+  // desgrid_init for one rank (desgrid_mod.f:571-604, 780-850)
+  p.istart1 = 2; p.iend1 = q.dg_imax + 1; p.istart2 = 1; p.iend2 = q.dg_imax + 2;
+  p.jstart1 = 2; p.jend1 = q.dg_jmax + 1; p.jstart2 = 1; p.jend2 = q.dg_jmax + 2;
+  if (q.no_k) { p.kstart1 = p.kend1 = p.kstart2 = p.kend2 = 1; }
+  else { p.kstart1 = 2; p.kend1 = q.dg_kmax + 1; p.kstart2 = 1; p.kend2 = q.dg_kmax + 2; }
+  p.c1 = p.jend2 - p.jstart2 + 1;
+  p.c2 = p.c1 * (p.iend2 - p.istart2 + 1);
+  p.c3 = -p.c1 * p.istart2 - p.c2 * p.kstart2 - p.jstart2 + 1;
+  p.ncell2 = (p.iend2 - p.istart2 + 1) * (p.jend2 - p.jstart2 + 1) * (p.kend2 - p.kstart2 + 1);
+  p.dt = q.dtsolid;
+  p.kn = q.kn; p.kt = q.kt; p.kn_w = q.kn_w; p.kt_w = q.kt_w;
+  p.mew = q.mew; p.mew_w = q.mew_w; p.mew_r = q.mew_r; p.mew_rw = q.mew_rw;
+  p.factor_rlm = q.factor_rlm; p.max_radius = q.max_radius;
+  p.dg_start[0] = q.dg_xstart; p.dg_start[1] = q.dg_ystart; p.dg_start[2] = q.dg_zstart;
+  p.dg_inv[0] = q.dg_dxinv; p.dg_inv[1] = q.dg_dyinv; p.dg_inv[2] = q.dg_dzinv;
+  for (int k = 0; k < MAXP * MAXP; ++k) {
+    p.etan[k] = q.des_etan[k]; p.etat[k] = q.des_etat[k]; p.hkn[k] = q.hert_kn[k]; p.hkt[k] = q.hert_kt[k];
+  }
+  for (int k = 0; k < MAXP; ++k) {
+    p.etanw[k] = q.des_etan_wall[k]; p.etatw[k] = q.des_etat_wall[k];
+    p.hkwn[k] = q.hert_kwn[k]; p.hkwt[k] = q.hert_kwt[k];
+  }
+}
+
+#define API_GUARD(h) do { if (!(h)) return DEM_ERR_ARG; cudaSetDevice((h)->dev); } while (0)
+
+extern "C" {
+
+int dem_abi_version(void) { return DEM_ABI_VERSION; }
+
+const char* dem_last_error(const dem_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
+  if (!q || !out || max_pip <= 0) return DEM_ERR_ARG;
+  if (q->n_phases < 1 || q->n_phases > DEM_MAX_PHASES) return DEM_ERR_ARG;
+  if (q->dg_imax < 1 || q->dg_jmax < 1 || (!q->no_k && q->dg_kmax < 1)) return DEM_ERR_ARG;
+  if (q->neighbor_search_n < 1 || !(q->dtsolid > 0.0)) return DEM_ERR_ARG;
+  for (int a = 0; a < 3; ++a) {
+    int cells = a == 0 ? q->dg_imax : (a == 1 ? q->dg_jmax : q->dg_kmax);
+    if (q->periodic[a] && !(a == 2 && q->no_k) && cells < 3) return DEM_ERR_ARG;
+  }
+  dem_handle* h = new dem_handle();
+  h->prm = *q;
+  h->n = max_pip;
+  cudaGetDevice(&h->dev);
+  fill_devparams(h);
+  const size_t n = (size_t)max_pip;
+  const int nc = h->dp.ncell2;
+  const int cmax = h->dp.cmax;
+  bool ok = true;
+  auto A = [&](void** p, size_t bytes) {
+    if (!ok) return;
+    if (cudaMalloc(p, bytes > 0 ? bytes : 8) != cudaSuccess) ok = false;
+    else cudaMemset(*p, 0, bytes > 0 ? bytes : 8);
+  };
+  for (int b = 0; b < 2; ++b) {
+    A((void**)&h->pos4[b], sizeof(double4) * n);
+    A((void**)&h->vel4[b], sizeof(double4) * n);
+    A((void**)&h->omg4[b], sizeof(double4) * n);
+    A((void**)&h->row_end[b], sizeof(int) * n);
+  }
+  A((void**)&h->state, n);
+  A((void**)&h->phase, n);
+  A((void**)&h->fc, sizeof(double) * 3 * n);
+  A((void**)&h->tow, sizeof(double) * 3 * n);
+  A((void**)&h->acc_old, sizeof(double) * 3 * n);
+  A((void**)&h->rot_acc_old, sizeof(double) * 3 * n);
+  A((void**)&h->dg_pijk, sizeof(int) * n);
+  A((void**)&h->cell_cnt, sizeof(int) * (nc + 1));
+  A((void**)&h->cell_start, sizeof(int) * (nc + 1));
+  A((void**)&h->cell_fill, sizeof(int) * (nc + 1));
+  A((void**)&h->cell_list, sizeof(int) * n);
+  A((void**)&h->row_cnt, sizeof(int) * n);
+  A((void**)&h->in_cnt, sizeof(int) * n);
+  A((void**)&h->in_start, sizeof(int) * (n + 1));
+  A((void**)&h->in_fill, sizeof(int) * n);
+  A((void**)&h->fbin_start, sizeof(int) * (nc + 1));
+  A((void**)&h->wall_fid, sizeof(int) * cmax * n);
+  A((void**)&h->wall_pft, sizeof(double) * 3 * cmax * n);
+  A((void**)&h->derr, sizeof(DevErr));
+  if (!ok) {
+    dem_destroy(h);
+    return DEM_ERR_CUDA;
+  }
+  cudaMemset(h->wall_fid, 0xff, sizeof(int) * cmax * n);  // -1 = free slot
+  if (cudaMallocHost((void**)&h->herr, sizeof(DevErr)) != cudaSuccess) { dem_destroy(h); return DEM_ERR_CUDA; }
+  memset(h->herr, 0, sizeof(DevErr));
+  h->herr->first_rogue = max_pip;
+  cudaMemcpy(h->derr, h->herr, sizeof(DevErr), cudaMemcpyHostToDevice);
+  if (ensure_pair_capacity(h, 16 * (long long)n + 1024)) { dem_destroy(h); return DEM_ERR_CUDA; }
+  if (cudaDeviceSynchronize() != cudaSuccess) { dem_destroy(h); return DEM_ERR_CUDA; }
+  *out = h;
+  return 0;
+}
+
+int dem_destroy(dem_handle* h) {
+  if (!h) return 0;
+  cudaSetDevice(h->dev);
+  cudaStreamSynchronize(h->stream);
+  void* ptrs[] = {h->pos4[0], h->pos4[1], h->vel4[0], h->vel4[1], h->omg4[0], h->omg4[1],
+                  h->state, h->phase, h->fc, h->tow, h->acc_old, h->rot_acc_old, h->dg_pijk,
+                  h->cell_cnt, h->cell_start, h->cell_fill, h->cell_list, h->row_cnt,
+                  h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
+                  h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
+                  h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
+                  h->scan_tmp, h->derr, h->red, h->stage};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  for (auto e : h->ev_pool) cudaEventDestroy(e);
+  if (h->herr) cudaFreeHost(h->herr);
+  delete h;
+  return 0;
+}
+
+int dem_set_stream(dem_handle* h, void* stream) {
+  API_GUARD(h);
+  h->stream = (cudaStream_t)stream;
+  return 0;
+}
+
+int dem_launch_count(const dem_handle* h, int64_t* count) {
+  if (!h || !count) return DEM_ERR_ARG;
+  *count = h->launches;
+  return 0;
+}
+
+int dem_set_walls(dem_handle* h, const double* vertex, const double* norm_face, int32_t nf) {
+  API_GUARD(h);
+  if (nf < 0 || (nf > 0 && (!vertex || !norm_face))) return set_err(h, DEM_ERR_ARG, "bad facet arrays");
+  return run_bin_facets(h, vertex, norm_face, nf);
+}
+
+// Upload goes through a device staging buffer so that the layout change is a
+// kernel, not a host loop.
+int dem_upload_state(dem_handle* h, const double* pos, const double* vel, const double* omega,
+                     const double* radius, const double* pmass, const double* omoi,
+                     const int8_t* state, const int32_t* phase, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip does not match dem_create");
+  if (!pos || !vel || !omega || !radius || !pmass || !omoi || !state || !phase)
+    return set_err(h, DEM_ERR_ARG, "null array");
+  const size_t n = h->n;
+  // one staging block: pos(3n) vel(3n) omega(3n) r(n) m(n) omoi(n) + phase(n ints)
+  double* st = (double*)stage_buffer(h, sizeof(double) * 12 * n + sizeof(int) * n + 64);
+  if (!st) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
+  cudaMemcpyAsync(st, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 3 * n, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 6 * n, omega, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 9 * n, radius, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 10 * n, pmass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 11 * n, omoi, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+  int* ph = (int*)(st + 12 * n);
+  cudaMemcpyAsync(ph, phase, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->state, state, n, cudaMemcpyHostToDevice, h->stream);
+  const int T = 256, B = (int)((n + T - 1) / T);
+  const int c = h->cur;
+  k_pack<<<B, T, 0, h->stream>>>(h->n, st, st + 9 * n, h->pos4[c]);
+  k_pack<<<B, T, 0, h->stream>>>(h->n, st + 3 * n, st + 10 * n, h->vel4[c]);
+  k_pack<<<B, T, 0, h->stream>>>(h->n, st + 6 * n, st + 11 * n, h->omg4[c]);
+  unsigned* bad = (unsigned*)h->cell_fill;
+  cudaMemsetAsync(bad, 0, sizeof(unsigned), h->stream);
+  k_phase_in<<<B, T, 0, h->stream>>>(h->n, ph, h->state, h->phase, h->dp.nph, bad);
+  h->launches += 4;
+  unsigned hb = 0;
+  cudaMemcpyAsync(&hb, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "upload")) return rc;
+  if (hb) return set_err(h, DEM_ERR_ARG, "phase out of range");
+  h->have_state = true;
+  return 0;
+}
+
+int dem_download_state(dem_handle* h, double* pos, double* vel, double* omega, int8_t* state, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
+  const size_t n = h->n;
+  double* st = (double*)stage_buffer(h, sizeof(double) * 12 * n + sizeof(int) * n + 64);
+  if (!st) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
+  const int T = 256, B = (int)((n + T - 1) / T);
+  const int c = h->cur;
+  k_unpack<<<B, T, 0, h->stream>>>(h->n, h->pos4[c], st);
+  k_unpack<<<B, T, 0, h->stream>>>(h->n, h->vel4[c], st + 3 * n);
+  k_unpack<<<B, T, 0, h->stream>>>(h->n, h->omg4[c], st + 6 * n);
+  h->launches += 3;
+  if (pos) cudaMemcpyAsync(pos, st, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  if (vel) cudaMemcpyAsync(vel, st + 3 * n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  if (omega) cudaMemcpyAsync(omega, st + 6 * n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  if (state) cudaMemcpyAsync(state, h->state, n, cudaMemcpyDeviceToHost, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "download");
+}
+
+int dem_download_forces(dem_handle* h, double* fc, double* tow, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
+  const size_t n = h->n;
+  if (fc) cudaMemcpyAsync(fc, h->fc, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  if (tow) cudaMemcpyAsync(tow, h->tow, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "download forces");
+}
+
+int dem_set_ab2_history(dem_handle* h, const double* acc_old, const double* rot_acc_old,
+                        int32_t first_pass, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
+  const size_t n = h->n;
+  if (acc_old) cudaMemcpyAsync(h->acc_old, acc_old, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  if (rot_acc_old) cudaMemcpyAsync(h->rot_acc_old, rot_acc_old, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  h->first_pass = first_pass != 0;
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "ab2 history");
+}
+
+int dem_get_ab2_history(dem_handle* h, double* acc_old, double* rot_acc_old, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
+  const size_t n = h->n;
+  if (acc_old) cudaMemcpyAsync(acc_old, h->acc_old, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  if (rot_acc_old) cudaMemcpyAsync(rot_acc_old, h->rot_acc_old, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "ab2 history");
+}
+
+int dem_pair_count(dem_handle* h, int64_t* np) {
+  API_GUARD(h);
+  if (!np) return DEM_ERR_ARG;
+  *np = h->n_pairs;
+  return 0;
+}
+
+int dem_download_pairs(dem_handle* h, int32_t* ni, int32_t* nb, double* pf, int64_t cap, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
+  const long long P = h->n_pairs;
+  if ((nb || pf) && cap < P) return set_err(h, DEM_ERR_CAPACITY, "pair capacity too small");
+  if (ni) cudaMemcpyAsync(ni, h->row_end[h->rb], sizeof(int) * h->n, cudaMemcpyDeviceToHost, h->stream);
+  if (nb && P) cudaMemcpyAsync(nb, h->nbrs[h->rb], sizeof(int) * P, cudaMemcpyDeviceToHost, h->stream);
+  if (pf && P) cudaMemcpyAsync(pf, h->pft[h->pcur], sizeof(double) * 3 * P, cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "download pairs")) return rc;
+  if (ni) for (int i = 0; i < h->n; ++i) ni[i] += 1;
+  if (nb) for (long long c = 0; c < P; ++c) nb[c] += 1;
+  return 0;
+}
+
+__global__ void k_owner_from_rows(int n, const int* __restrict__ row_end, int* __restrict__ owner) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int s = i ? row_end[i - 1] : 0, e = row_end[i];
+  for (int c = s; c < e; ++c) owner[c] = i;
+}
+__global__ void k_in_count2(long long np, const int* __restrict__ nbrs, int* __restrict__ in_cnt) {
+  long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cc < np) atomicAdd(&in_cnt[nbrs[cc]], 1);
+}
+__global__ void k_in_fill2(long long np, const int* __restrict__ nbrs, const int* __restrict__ owner,
+                           const int* __restrict__ in_start, int* __restrict__ in_fill, int2* __restrict__ in_pair) {
+  long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cc >= np) return;
+  int j = nbrs[cc];
+  int slot = atomicAdd(&in_fill[j], 1);
+  in_pair[in_start[j] + slot] = make_int2(owner[cc], (int)cc);
+}
+__global__ void k_in_sort2(int n, const int* __restrict__ in_start, int2* __restrict__ in_pair) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int s = in_start[j], e = in_start[j + 1];
+  for (int a = s + 1; a < e; ++a) {
+    int2 v = in_pair[a];
+    int b = a - 1;
+    while (b >= s && in_pair[b].y > v.y) { in_pair[b + 1] = in_pair[b]; --b; }
+    in_pair[b + 1] = v;
+  }
+}
+
+int dem_upload_pairs(dem_handle* h, const int32_t* ni, const int32_t* nb, const double* pf, int64_t np, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n || np < 0 || !ni || (np > 0 && (!nb || !pf))) return set_err(h, DEM_ERR_ARG, "bad pair arrays");
+  // validate the CSR on the host: monotone end pointers, indices in range
+  long long prev = 0;
+  std::vector<int> re(h->n), nbr((size_t)np);
+  for (int i = 0; i < h->n; ++i) {
+    long long e = (long long)ni[i] - 1;
+    if (e < prev || e > np) return set_err(h, DEM_ERR_ARG, "NEIGHBOR_INDEX is not a valid CSR");
+    re[i] = (int)e;
+    prev = e;
+  }
+  if (prev != np) return set_err(h, DEM_ERR_ARG, "NEIGHBOR_INDEX(MAX_PIP) does not match the pair count");
+  for (long long c = 0; c < np; ++c) {
+    if (nb[c] < 1 || nb[c] > h->n) return set_err(h, DEM_ERR_ARG, "NEIGHBORS index out of range");
+    nbr[c] = nb[c] - 1;
+  }
+  if (int rc = ensure_pair_capacity(h, np + 1)) return rc;
+  cudaMemcpyAsync(h->row_end[h->rb], re.data(), sizeof(int) * h->n, cudaMemcpyHostToDevice, h->stream);
+  if (np) {
+    cudaMemcpyAsync(h->nbrs[h->rb], nbr.data(), sizeof(int) * np, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->pft[h->pcur], pf, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, h->stream);
+  }
+  h->n_pairs = np;
+  const int T = 256, B = (h->n + T - 1) / T;
+  k_owner_from_rows<<<B, T, 0, h->stream>>>(h->n, h->row_end[h->rb], h->pair_owner);
+  cudaMemsetAsync(h->in_cnt, 0, sizeof(int) * h->n, h->stream);
+  h->launches++;
+  if (np) {
+    unsigned BP = (unsigned)((np + T - 1) / T);
+    k_in_count2<<<BP, T, 0, h->stream>>>(np, h->nbrs[h->rb], h->in_cnt);
+    h->launches++;
+  }
+  if (int rc = exclusive_scan(h, h->in_cnt, h->in_start, h->n, h->in_start + h->n)) return rc;
+  if (np) {
+    unsigned BP = (unsigned)((np + T - 1) / T);
+    cudaMemsetAsync(h->in_fill, 0, sizeof(int) * h->n, h->stream);
+    k_in_fill2<<<BP, T, 0, h->stream>>>(np, h->nbrs[h->rb], h->pair_owner, h->in_start, h->in_fill, h->in_pair);
+    k_in_sort2<<<B, T, 0, h->stream>>>(h->n, h->in_start, h->in_pair);
+    h->launches += 2;
+  }
+  h->have_pairs = true;
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "upload pairs");
+}
+
+int dem_download_wall_history(dem_handle* h, int32_t* fid, double* pf, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
+  const size_t cnt = (size_t)h->n * h->dp.cmax;
+  if (fid) cudaMemcpyAsync(fid, h->wall_fid, sizeof(int) * cnt, cudaMemcpyDeviceToHost, h->stream);
+  if (pf) cudaMemcpyAsync(pf, h->wall_pft, sizeof(double) * 3 * cnt, cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "download wall history")) return rc;
+  if (fid) for (size_t s = 0; s < cnt; ++s) fid[s] = fid[s] < 0 ? -1 : fid[s] + 1;
+  return 0;
+}
+
+int dem_download_cells(dem_handle* h, int32_t* cells, int32_t max_pip) {
+  API_GUARD(h);
+  if (max_pip != h->n || !cells) return set_err(h, DEM_ERR_ARG, "bad arguments");
+  cudaMemcpyAsync(cells, h->dg_pijk, sizeof(int) * h->n, cudaMemcpyDeviceToHost, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "download cells");
+}
+
+int dem_desgrid_pic(dem_handle* h) {
+  API_GUARD(h);
+  if (!h->have_state) return set_err(h, DEM_ERR_STATE, "no particle state uploaded");
+  if (int rc = run_desgrid_pic(h, true)) return rc;
+  return fetch_errors(h);
+}
+
+int dem_neighbour(dem_handle* h) {
+  API_GUARD(h);
+  if (!h->have_state) return set_err(h, DEM_ERR_STATE, "no particle state uploaded");
+  if (int rc = run_neighbour(h, true)) return rc;
+  return fetch_errors(h);
+}
+
+int dem_init_neighbors(dem_handle* h) {
+  API_GUARD(h);
+  if (!h->have_state) return set_err(h, DEM_ERR_STATE, "no particle state uploaded");
+  h->have_pairs = false;
+  if (int rc = run_desgrid_pic(h, true)) return rc;
+  if (int rc = run_neighbour(h, false)) return rc;
+  return fetch_errors(h);
+}
+
+int dem_calc_force(dem_handle* h) {
+  API_GUARD(h);
+  if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
+  cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
+  if (int rc = run_force(h, false)) return rc;
+  return fetch_errors(h);
+}
+
+int dem_cfnewvalues(dem_handle* h) {
+  API_GUARD(h);
+  if (!h->have_state) return set_err(h, DEM_ERR_STATE, "no particle state uploaded");
+  if (int rc = run_cfnewvalues(h)) return rc;
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "cfnewvalues");
+}
+
+int dem_step(dem_handle* h, int32_t nn_first, int32_t nsteps) {
+  API_GUARD(h);
+  if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
+  if (nsteps < 0 || nn_first < 1) return set_err(h, DEM_ERR_ARG, "bad step range");
+  const DevParams& p = h->dp;
+  const bool anyper = p.per[0] || p.per[1] || (p.per[2] && !p.no_k);
+  for (int k = 0; k < nsteps; ++k) {
+    const int nn = nn_first + k;
+    cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
+    if (int rc = run_force(h, true)) return rc;
+    const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0);
+    if (do_nsearch || anyper) {
+      if (int rc = run_desgrid_pic(h, do_nsearch)) return rc;
+    }
+    if (do_nsearch) {
+      if (int rc = run_neighbour(h, true)) return rc;
+    }
+    h->s_time = h->s_time + h->prm.dtsolid;
+    h->steps_done++;
+  }
+  return fetch_errors(h);
+}
+
+int dem_get_stats(dem_handle* h, dem_stats* s) {
+  API_GUARD(h);
+  if (!s) return DEM_ERR_ARG;
+  memset(s, 0, sizeof *s);
+  const int T = STAT_T, B = (h->n + T - 1) / T;
+  if (h->red_elems < 8 * B) {
+    if (h->red) cudaFree(h->red);
+    h->red = nullptr;
+    if (int rc = check_cuda(h, cudaMalloc(&h->red, sizeof(double) * 8 * B), "cudaMalloc")) return rc;
+    h->red_elems = 8 * B;
+  }
+  std::vector<double> part((size_t)8 * B);
+  k_stats1<<<B, T, 0, h->stream>>>(h->n, h->pos4[h->cur], h->vel4[h->cur], h->state, h->red);
+  h->launches++;
+  cudaMemcpyAsync(part.data(), h->red, sizeof(double) * 8 * B, cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
+  double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < B; ++b) for (int k = 0; k < 8; ++k) sum[k] += part[(size_t)8 * b + k];
+  const double nn = sum[0];
+  double mv[3] = {0, 0, 0};
+  if (nn > 0) for (int c = 0; c < 3; ++c) mv[c] = sum[1 + c] / nn;
+  k_stats2<<<B, T, 0, h->stream>>>(h->n, h->vel4[h->cur], h->state, mv[0], mv[1], mv[2], h->red);
+  h->launches++;
+  cudaMemcpyAsync(part.data(), h->red, sizeof(double) * 3 * B, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(h->herr, h->derr, sizeof(DevErr), cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
+  double gt[3] = {0, 0, 0};
+  for (int b = 0; b < B; ++b) for (int k = 0; k < 3; ++k) gt[k] += part[(size_t)3 * b + k];
+  s->n_normal = (int64_t)nn;
+  for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn > 0 ? gt[c] / nn : 0.0; }
+  s->n_pairs = h->n_pairs;
+  s->n_contacts = (int64_t)h->herr->n_contacts;
+  s->n_wall_contacts = (int64_t)h->herr->n_wall_contacts;
+  s->n_rogue_removed = (int64_t)h->herr->rogue_removed;
+  s->steps_done = h->steps_done;
+  s->kinetic_energy = sum[6];
+  s->bed_height = sum[4] > 0 ? sum[5] / sum[4] : 0.0;
+  s->s_time = h->s_time;
+  return 0;
+}
+
+int dem_set_profiling(dem_handle* h, int32_t on) {
+  API_GUARD(h);
+  prof_collect(h);
+  h->prof = on != 0;
+  for (int k = 0; k < DEM_PROF_N; ++k) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
+  return 0;
+}
+
+int dem_get_profile(dem_handle* h, double* ms, int64_t* launches) {
+  API_GUARD(h);
+  prof_collect(h);
+  for (int k = 0; k < DEM_PROF_N; ++k) {
+    if (ms) ms[k] = h->prof_ms[k];
+    if (launches) launches[k] = h->prof_n[k];
+  }
+  return 0;
+}
+
+int dem_force_error(dem_handle* h, double* rel_err) {
+  API_GUARD(h);
+  if (!rel_err) return DEM_ERR_ARG;
+  return run_split_force_error(h, rel_err);
+}
+
+}  // extern "C"

@@ -1,0 +1,241 @@
+// dem_internal.cuh -- shared definitions of the CUDA DEM library.
+//
+// Device layout (n = MAX_PIP):
+//   pos4[b][i] = (x, y, z, radius)      double4, double-buffered (b = 0/1)
+//   vel4[b][i] = (u, v, w, pmass)       double4, double-buffered
+//   omg4[b][i] = (wx, wy, wz, omoi)     double4, double-buffered
+//   state[i]   int8 PARTICLE_STATE, phase[i] uint8 (0-based)
+//   fc, tow    (n,3) column blocks, as FC/TOW of discretelement_mod.f:630
+//   pairs      CSR half list: row_end[i] = pairs in rows 0..i,
+//              nbrs[P] 0-based, pft[b][3P] (3,P) like PFT_NEIGHBOR,
+//              and the transpose in_start[n+1] / in_pair[] = (owner, cc)
+//              sorted by owner so each particle can gather the forces of
+//              the pairs it does not own in the serial reference's order.
+// Packing a particle's position with its radius (and velocity with mass,
+// spin with inverse inertia) makes each neighbour gather one 32-byte sector
+// per quantity.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/dem_b200.h"
+
+namespace demb {
+
+constexpr double SMALL_NUMBER = 1.0e-15;       // param1_mod.f:26
+constexpr double UNDEFINED_D  = 9.87654321e31; // param1_mod.f:20
+constexpr int MAXP = DEM_MAX_PHASES;
+
+// Error word bits (device -> host)
+enum : unsigned {
+  EF_ZERO_DIST   = 1u << 0,
+  EF_WALL_SLOTS  = 1u << 1,
+  EF_PAIR_CAP    = 1u << 2,
+  EF_ROGUE_FATAL = 1u << 3,
+  EF_CELL_CAP    = 1u << 4,
+  EF_NONFINITE   = 1u << 5,
+};
+
+struct DevErr {
+  unsigned flags;
+  int first_rogue;   // smallest rogue particle index of the last build (n if none)
+  int zero_a, zero_b;  // particles of a zero-distance pair
+  unsigned long long n_contacts;
+  unsigned long long n_wall_contacts;
+  unsigned long long rogue_removed;
+  int pad[2];
+};
+
+// Parameters as kernels see them (passed by value).
+struct DevParams {
+  int n;
+  int coll, intg, nph, no_k, cmax, remove_rogue, first_pass;
+  int per[3];
+  int istart1, iend1, istart2, iend2;
+  int jstart1, jend1, jstart2, jend2;
+  int kstart1, kend1, kstart2, kend2;
+  int c1, c2, c3, ncell2;
+  double dt, grav[3];
+  double kn, kt, kn_w, kt_w, mew, mew_w, mew_r, mew_rw;
+  double factor_rlm, max_radius;
+  double dg_start[3], dg_inv[3];
+  double lo[3], hi[3], L[3];
+  double etan[MAXP * MAXP], etat[MAXP * MAXP], hkn[MAXP * MAXP], hkt[MAXP * MAXP];
+  double etanw[MAXP], etatw[MAXP], hkwn[MAXP], hkwt[MAXP];
+};
+
+struct FacetBinEntry {  // one entry of facets_at_dg(cell)
+  double mn, mx;        // facet extent along dir
+  int id;               // 0-based facet
+  int dir;              // 0-based axis of smallest extent
+};
+
+// ---------------------------------------------------------------------------
+// Host-side handle
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace demb
+
+struct dem_handle {
+  dem_params prm;
+  demb::DevParams dp;
+  int n = 0;
+  int dev = 0;
+  cudaStream_t stream = 0;
+  std::string err;
+  long long launches = 0;
+  bool have_state = false, have_pairs = false;
+  int cur = 0;  // current state buffer
+  int pcur = 0; // current pft buffer
+  bool first_pass = true;
+  long long steps_done = 0;
+  double s_time = 0.0;
+
+  // particle state
+  double4* pos4[2] = {nullptr, nullptr};
+  double4* vel4[2] = {nullptr, nullptr};
+  double4* omg4[2] = {nullptr, nullptr};
+  int8_t* state = nullptr;
+  uint8_t* phase = nullptr;
+  double* fc = nullptr;   // (n,3)
+  double* tow = nullptr;
+  double* acc_old = nullptr;
+  double* rot_acc_old = nullptr;
+
+  // DES grid
+  int* dg_pijk = nullptr;     // 1-based cell, 0 = none
+  int* cell_cnt = nullptr;    // ncell2
+  int* cell_start = nullptr;  // ncell2+1
+  int* cell_fill = nullptr;   // ncell2
+  int* cell_list = nullptr;   // n
+
+  // pairs
+  long long pair_cap = 0;
+  long long n_pairs = 0;
+  int* row_cnt = nullptr;     // n
+  int* row_end[2] = {nullptr, nullptr};   // n (current / previous build)
+  int* nbrs[2] = {nullptr, nullptr};      // cap
+  double* pft[2] = {nullptr, nullptr};    // 3*cap
+  int* in_cnt = nullptr;      // n
+  int* in_start = nullptr;    // n+1
+  int* in_fill = nullptr;     // n
+  int2* in_pair = nullptr;    // cap
+  int* pair_owner = nullptr;  // cap
+  int rb = 0;                 // which row_end/nbrs buffer is current
+
+  // walls
+  int nf = 0;
+  double* vertex = nullptr;   // [f][v][c]
+  double* norm_face = nullptr;// [f][c]
+  int8_t* ignore_edge = nullptr; // [f][4]
+  int* fbin_start = nullptr;  // ncell2+1
+  demb::FacetBinEntry* fbin = nullptr;
+  int n_fbin = 0;
+  int* wall_fid = nullptr;    // [i][cmax]
+  double* wall_pft = nullptr; // [i][cmax][3]
+
+  // scan scratch
+  int* scan_tmp = nullptr;
+  size_t scan_tmp_elems = 0;
+
+  // error word
+  demb::DevErr* derr = nullptr;
+  demb::DevErr* herr = nullptr;   // pinned mirror
+
+  // reductions for stats
+  double* red = nullptr;      // scratch doubles
+  int red_elems = 0;
+
+  // coupling (see coupling.cu)
+  struct Gas* gas = nullptr;
+
+  // host<->device staging (kept between calls)
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
+
+  // kernel-time accounting (dem_set_profiling)
+  bool prof = false;
+  struct ProfEv { int cls; cudaEvent_t a, b; };
+  std::vector<ProfEv> prof_pending;
+  std::vector<cudaEvent_t> ev_pool;
+  double prof_ms[DEM_PROF_N] = {0};
+  long long prof_n[DEM_PROF_N] = {0};
+};
+
+namespace demb {
+
+// set by every API entry point on failure
+int set_err(dem_handle* h, int code, const std::string& msg);
+int check_cuda(dem_handle* h, cudaError_t e, const char* what);
+
+// scan.cu: exclusive scan of n ints into out (out may alias in); total
+// written to *d_total (device pointer) when non-null.
+int exclusive_scan(dem_handle* h, const int* in, int* out, int n, int* d_total);
+
+// desgrid.cu / neighbor.cu / force.cu / walls.cu host drivers
+int run_desgrid_pic(dem_handle* h, bool sort_cells);
+int run_neighbour(dem_handle* h, bool carry_history);
+int run_force(dem_handle* h, bool fused);
+int run_cfnewvalues(dem_handle* h);
+int run_bin_facets(dem_handle* h, const double* vertex_fortran, const double* norm_fortran, int nf);
+int run_split_force_error(dem_handle* h, double* rel_err);
+int ensure_pair_capacity(dem_handle* h, long long need);
+int fetch_errors(dem_handle* h);
+void* stage_buffer(dem_handle* h, size_t bytes);
+
+// Brackets the kernels issued in its scope with CUDA events when the
+// handle's profiling is on.
+struct ProfScope {
+  dem_handle* h;
+  int idx = -1;
+  ProfScope(dem_handle* hh, int cls);
+  ~ProfScope();
+};
+
+// ---------------------------------------------------------------------------
+// Device helpers.  All FP64 arithmetic in the parity kernels is compiled
+// without FMA contraction so each expression rounds like the Fortran.
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+__device__ __forceinline__ void cross3(const double x[3], const double y[3], double o[3]) {
+  o[0] = x[1] * y[2] - x[2] * y[1];
+  o[1] = x[2] * y[0] - x[0] * y[2];
+  o[2] = x[0] * y[1] - x[1] * y[0];
+}
+
+__device__ __forceinline__ int dg_funijk(const DevParams& p, int i, int j, int k) {
+  return j + i * p.c1 + k * p.c2 + p.c3;
+}
+__device__ __forceinline__ int dg_jof(const DevParams& p, int ijk) {
+  return ((ijk - 1) % p.c2) % p.c1 + p.jstart2;
+}
+__device__ __forceinline__ int dg_iof(const DevParams& p, int ijk) {
+  return ((ijk - dg_jof(p, ijk) + p.jstart2 - 1) % p.c2) / p.c1 + p.istart2;
+}
+__device__ __forceinline__ int dg_kof(const DevParams& p, int ijk) {
+  return (ijk - p.c3 - dg_iof(p, ijk) * p.c1 - dg_jof(p, ijk)) / p.c2;
+}
+__device__ __forceinline__ int dg_ofpos(const DevParams& p, int ax, double x, int start1) {
+  return (int)floor((x - p.dg_start[ax]) * p.dg_inv[ax]) + start1;
+}
+
+// Minimum-image shift for periodic axes (the copy of j that the reference's
+// ghost exchange places next to i).
+__device__ __forceinline__ double periodic_shift(const DevParams& p, int ax, double d) {
+  if (!p.per[ax]) return 0.0;
+  double L = p.L[ax];
+  if (d > 0.5 * L) return -L;
+  if (d < -0.5 * L) return L;
+  return 0.0;
+}
+
+}  // namespace demb
+
+#define DEM_LAUNCH(h) ((h)->launches++)

@@ -1,0 +1,608 @@
+// force.cu -- contact forces and integration, FP64 (K3, K4, K5).
+//
+// Replaces CALC_FORCE_DEM (model/des/calc_force_dem.f:18-544) with CFRELVEL
+// (model/des/cfrelvel.f:54-77), the wall contacts of
+// CALC_DEM_FORCE_WITH_WALL_STL (model/des/calc_collision_wall_mod.f:180-629,
+// GET/UPDATE/REMOVE_COLLISION 651-792, CFRELVEL_WALL 806-847,
+// ClosestPtPointTriangle in stl_functions_des_mod.f:25-160), and
+// CFUPDATEOLD + CFNEWVALUES (cfupdateold.f:33-41, cfnewvalues.f:669-812).
+//
+// The reference loops over owners LL and scatters each pair's force into
+// FC(LL) and FC(I) with atomics.  Here one thread owns one particle and
+// gathers instead: walls first, then the pairs it appears in as neighbour I
+// (in ascending owner order, from the transpose), then its own row.  That is
+// exactly the order in which the serial reference adds into FC(me)/TOW(me),
+// and each pair is evaluated by both of its particles with identical
+// operands, so every particle's force is bit-identical to the serial
+// reference without atomics.  The tangential history is double-buffered:
+// both evaluations read PFT_in, only the owner writes PFT_out.
+//
+// This file is compiled with -fmad=false: every FP64 expression rounds as
+// the Fortran does (gfortran emits no FMA without -march).  sqrt and '/' are
+// IEEE round-to-nearest in CUDA, as they are on the host.
+#include "dem_internal.cuh"
+
+namespace demb {
+
+struct PairRes {
+  double fc[3], tl[3], ti[3], rl[3], ri[3];
+  bool contact, roll_l, roll_i, zero;
+};
+
+struct PState {  // one particle's gathered state
+  double x[3], v[3], w[3];
+  double r, m;
+  int ph;
+};
+
+__device__ __forceinline__ void load_p(const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+                                       const double4* __restrict__ omg4, const uint8_t* __restrict__ phase,
+                                       int i, PState& s) {
+  double4 a = pos4[i], b = vel4[i], c = omg4[i];
+  s.x[0] = a.x; s.x[1] = a.y; s.x[2] = a.z; s.r = a.w;
+  s.v[0] = b.x; s.v[1] = b.y; s.v[2] = b.z; s.m = b.w;
+  s.w[0] = c.x; s.w[1] = c.y; s.w[2] = c.z;
+  s.ph = phase[i];
+}
+
+// One CC iteration of CALC_FORCE_DEM for owner L and neighbour I.
+template <int COLL>
+__device__ __forceinline__ void pair_force(const DevParams& p, const PState& L, const PState& I,
+                                           const double pin[3], double pout[3], PairRes& o) {
+  o.contact = false; o.roll_l = false; o.roll_i = false; o.zero = false;
+  const double rl = L.r, ri = I.r;
+  const double r_lm = rl + ri;
+  double dist[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double pj = I.x[c];
+    double s = periodic_shift(p, c, pj - L.x[c]);
+    if (s != 0.0) pj = pj + s;
+    dist[c] = pj - L.x[c];
+  }
+  double dmag = dot3(dist, dist);
+  if (dmag > (r_lm - SMALL_NUMBER) * (r_lm - SMALL_NUMBER)) {
+    pout[0] = pout[1] = pout[2] = 0.0;
+    return;
+  }
+  if (dmag == 0.0) { o.zero = true; pout[0] = pin[0]; pout[1] = pin[1]; pout[2] = pin[2]; return; }
+  dmag = sqrt(dmag);
+  double nrm[3] = {dist[0] / dmag, dist[1] / dmag, dist[2] / dmag};
+  const double overlap_n = r_lm - dmag;
+  // CFRELVEL
+  double vrel[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) vrel[c] = L.v[c] - I.v[c];
+  const double dcl = (dmag * dmag + rl * rl - ri * ri) / (2.0 * dmag);
+  const double dci = dmag - dcl;
+  double osum[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) osum[c] = L.w[c] * dcl + I.w[c] * dci;
+  double vrot[3];
+  cross3(osum, nrm, vrot);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) vrel[c] = vrel[c] + vrot[c];
+  const double vrn = dot3(vrel, nrm);
+  double vt[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) vt[c] = vrel[c] - vrn * nrm[c];
+  const int ix = L.ph * MAXP + I.ph;
+  const double rad_eff = (rl * ri) / (rl + ri);
+  const double m_eff = (L.m * I.m) / (L.m + I.m);
+  double kn, kt, etan, etat;
+  if (COLL == DEM_COLL_HERTZ) {
+    double so = sqrt(overlap_n);
+    kn = p.hkn[ix] * so * sqrt(rad_eff);
+    kt = p.hkt[ix] * so * sqrt(rad_eff);
+    so = sqrt(so);
+    etan = p.etan[ix] * so * sqrt(p.hkn[ix] * sqrt(rad_eff) * m_eff);
+    etat = p.etat[ix] * so * sqrt(p.hkt[ix] * sqrt(rad_eff) * m_eff);
+  } else {
+    kn = p.kn; kt = p.kt;
+    etan = p.etan[ix] * sqrt(m_eff);
+    etat = p.etat[ix] * sqrt(m_eff);
+  }
+  double fn[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) fn[c] = -(kn * overlap_n * nrm[c] + etan * vrn * nrm[c]);
+  double ot[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) ot[c] = p.dt * vt[c] + pin[c];
+  const double mag = sqrt(dot3(ot, ot));
+  double ft[3];
+  if (mag > 0.0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ft[c] = -kt * ot[c] - etat * vt[c];
+    const double ftmd = sqrt(dot3(ft, ft));
+    const double fnmd = p.mew * sqrt(dot3(fn, fn));
+    if (ftmd > fnmd) {
+      double tg[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) tg[c] = ot[c] / mag;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ft[c] = -fnmd * tg[c];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ot[c] = (fnmd / kt) * tg[c];
+    }
+  } else {
+    ft[0] = ft[1] = ft[2] = 0.0;
+  }
+  pout[0] = ot[0]; pout[1] = ot[1]; pout[2] = ot[2];
+  const double dcl2 = dmag / 2.0 + (rl * rl - ri * ri) / (2.0 * dmag);
+  const double dci2 = dmag - dcl2;
+  double tf[3];
+  cross3(nrm, ft, tf);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) { o.tl[c] = dcl2 * tf[c]; o.ti[c] = dci2 * tf[c]; }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) o.fc[c] = 0.0 + fn[c] + ft[c];
+  if (p.mew_r > 0.0) {
+    double om = sqrt(dot3(L.w, L.w));
+    if (om > 0.0) {
+      o.roll_l = true;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o.rl[c] = -(p.mew_r * (2.0 * rl) * kn * overlap_n * L.w[c] / om);
+    }
+    om = sqrt(dot3(I.w, I.w));
+    if (om > 0.0) {
+      o.roll_i = true;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o.ri[c] = -(p.mew_r * (2.0 * ri) * kn * overlap_n * I.w[c] / om);
+    }
+  }
+  o.contact = true;
+}
+
+// ---------------------------------------------------------------------------
+// Walls
+
+struct WallCtx {
+  const double* __restrict__ vertex;   // [f][v][c]
+  const double* __restrict__ norm_face;// [f][c]
+  const int8_t* __restrict__ ignore_edge; // [f][4]
+  const int* __restrict__ fbin_start;
+  const FacetBinEntry* __restrict__ fbin;
+  const int* __restrict__ dg_pijk;
+  int* __restrict__ wall_fid;          // [i][cmax]
+  double* __restrict__ wall_pft;       // [i][cmax][3]
+  int nf;
+};
+
+__device__ __forceinline__ void closest_pt(const DevParams& p, const WallCtx& w, int f, const double pp[3],
+                                           double cpt[3], bool& poe, int& edge) {
+  poe = false; edge = 0;
+  const double* V = w.vertex + 9 * (size_t)f;
+  double a[3], b[3], c[3], ab[3], ac[3], ap[3], bp[3], cp[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) { a[k] = V[k]; b[k] = V[3 + k]; c[k] = V[6 + k]; }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) { ab[k] = b[k] - a[k]; ac[k] = c[k] - a[k]; ap[k] = pp[k] - a[k]; }
+  const double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  const int8_t* ig = w.ignore_edge + 4 * (size_t)f;
+  if (d1 < 0.0 && d2 < 0.0) {
+    for (int k = 0; k < 3; ++k) cpt[k] = a[k];
+    poe = true; if (ig[1]) cpt[0] = UNDEFINED_D; edge = 1; return;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) bp[k] = pp[k] - b[k];
+  const double d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+  if (d3 > 0.0 && d4 < d3) {
+    for (int k = 0; k < 3; ++k) cpt[k] = b[k];
+    poe = true; if (ig[1]) cpt[0] = UNDEFINED_D; edge = 1; return;
+  }
+  const double vc = d1 * d4 - d3 * d2;
+  if (vc < 0.0 && d1 > 0.0 && d3 < 0.0) {
+    const double v = d1 / (d1 - d3);
+    for (int k = 0; k < 3; ++k) cpt[k] = a[k] + v * ab[k];
+    poe = true; if (ig[1]) cpt[0] = UNDEFINED_D; edge = 1; return;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) cp[k] = pp[k] - c[k];
+  const double d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+  if (d6 > 0.0 && d5 < d6) {
+    for (int k = 0; k < 3; ++k) cpt[k] = c[k];
+    poe = true; if (ig[2]) cpt[0] = UNDEFINED_D; edge = 2; return;
+  }
+  const double vb = d5 * d2 - d1 * d6;
+  if (vb < 0.0 && d2 > 0.0 && d6 < 0.0) {
+    const double ww = d2 / (d2 - d6);
+    for (int k = 0; k < 3; ++k) cpt[k] = a[k] + ww * ac[k];
+    poe = true; if (ig[2]) cpt[0] = UNDEFINED_D; edge = 2; return;
+  }
+  const double va = d3 * d6 - d5 * d4;
+  if (va < 0.0 && (d4 - d3) > 0.0 && (d5 - d6) > 0.0) {
+    const double ww = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    for (int k = 0; k < 3; ++k) cpt[k] = b[k] + ww * (c[k] - b[k]);
+    poe = true; if (ig[3]) cpt[0] = UNDEFINED_D; edge = 3; return;
+  }
+  const double denom = 1.0 / (va + vb + vc);
+  const double v = vb * denom, ww = vc * denom;
+  for (int k = 0; k < 3; ++k) cpt[k] = a[k] + ab[k] * v + ac[k] * ww;
+  if (p.no_k) cpt[2] = pp[2];
+}
+
+__device__ __forceinline__ void remove_collision(const DevParams& p, const WallCtx& w, int me, int f) {
+  int* fid = w.wall_fid + (size_t)me * p.cmax;
+  for (int s = 0; s < p.cmax; ++s) if (fid[s] == f) { fid[s] = -1; return; }
+}
+
+// returns slot index, or -1 on overflow
+__device__ __forceinline__ int get_collision(const DevParams& p, const WallCtx& w, int me, int f, int cell,
+                                             double out[3]) {
+  int* fid = w.wall_fid + (size_t)me * p.cmax;
+  double* wp = w.wall_pft + (size_t)me * p.cmax * 3;
+  int free_index = -1;
+  for (int s = 0; s < p.cmax; ++s) {
+    int v = fid[s];
+    if (f == v) { out[0] = wp[3 * s]; out[1] = wp[3 * s + 1]; out[2] = wp[3 * s + 2]; return s; }
+    else if (v == -1) free_index = s;
+  }
+  if (free_index == -1) {
+    for (int s = 0; s < p.cmax && free_index == -1; ++s) {
+      bool in_cell = false;
+      for (int q = w.fbin_start[cell]; q < w.fbin_start[cell + 1]; ++q)
+        if (fid[s] == w.fbin[q].id) { in_cell = true; break; }
+      if (!in_cell) free_index = s;
+    }
+  }
+  if (free_index == -1) return -1;
+  fid[free_index] = f;
+  wp[3 * free_index] = 0.0; wp[3 * free_index + 1] = 0.0; wp[3 * free_index + 2] = 0.0;
+  out[0] = out[1] = out[2] = 0.0;
+  return free_index;
+}
+
+template <int COLL>
+__device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, const PState& s,
+                              double f[3], double t[3], unsigned long long& nwc, unsigned& eflags) {
+  const int cell = w.dg_pijk[me] - 1;
+  const int fs = w.fbin_start[cell], fe = w.fbin_start[cell + 1];
+  if (fe - fs < 1) {
+    int* fid = w.wall_fid + (size_t)me * p.cmax;
+    double* wp = w.wall_pft + (size_t)me * p.cmax * 3;
+    for (int q = 0; q < p.cmax; ++q) fid[q] = -1;
+    for (int q = 0; q < 3 * p.cmax; ++q) wp[q] = 0.0;
+    return;
+  }
+  const double r = s.r;
+  const double radsq = r * r;
+  double pmax[3], pmin[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) { pmax[c] = s.x[c] + r; pmin[c] = s.x[c] - r; }
+  for (int q = fs; q < fe; ++q) {
+    const FacetBinEntry e = w.fbin[q];
+    const int nf = e.id;
+    if (e.mn > pmax[e.dir]) { remove_collision(p, w, me, nf); continue; }
+    if (e.mx < pmin[e.dir]) { remove_collision(p, w, me, nf); continue; }
+    const double* V = w.vertex + 9 * (size_t)nf;
+    const double* N = w.norm_face + 3 * (size_t)nf;
+    double d1[3] = {V[0] - s.x[0], V[1] - s.x[1], V[2] - s.x[2]};
+    double nn[3] = {N[0], N[1], N[2]};
+    const double line_t = dot3(d1, nn);
+    if (line_t <= -1.0001 * r) { remove_collision(p, w, me, nf); continue; }
+    double cpt[3]; bool poe; int edge;
+    closest_pt(p, w, nf, s.x, cpt, poe, edge);
+    double dist[3] = {cpt[0] - s.x[0], cpt[1] - s.x[1], cpt[2] - s.x[2]};
+    const double distsq = dot3(dist, dist);
+    if (distsq >= radsq - SMALL_NUMBER) { remove_collision(p, w, me, nf); continue; }
+    if (poe && w.ignore_edge[4 * (size_t)nf + edge]) continue;
+    const double distmod = sqrt(distsq);
+    double nrm[3] = {dist[0], dist[1], dist[2]};
+    if (distsq > 0) { const double sq = sqrt(distsq); for (int c = 0; c < 3; ++c) nrm[c] = dist[c] / sq; }
+    const double overlap_n = r - distmod;
+    double wxn[3]; cross3(s.w, nrm, wxn);
+    double vrel[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { vrel[c] = s.v[c] + distmod * wxn[c]; vrel[c] = vrel[c] - (0.0 + 0.0); }
+    const double vrn = dot3(vrel, nrm);
+    double vt[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) vt[c] = vrel[c] - vrn * nrm[c];
+    double kn_w, kt_w, etan_w, etat_w;
+    const int ph = s.ph;
+    if (COLL == DEM_COLL_HERTZ) {
+      double so = 0.0;
+      if (overlap_n > 0) so = sqrt(overlap_n);
+      kn_w = p.hkwn[ph] * so * sqrt(r);
+      kt_w = p.hkwt[ph] * so * sqrt(r);
+      etan_w = p.etanw[ph] * sqrt(so) * sqrt(p.hkwn[ph] * sqrt(r) * s.m);
+      etat_w = p.etatw[ph] * sqrt(so) * sqrt(p.hkwt[ph] * sqrt(r) * s.m);
+    } else {
+      kn_w = p.kn_w; kt_w = p.kt_w;
+      etan_w = p.etanw[ph] * sqrt(s.m);
+      etat_w = p.etatw[ph] * sqrt(s.m);
+    }
+    double fn[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) fn[c] = -(kn_w * overlap_n * nrm[c] + etan_w * vrn * nrm[c]);
+    double hist[3];
+    const int slot = get_collision(p, w, me, nf, cell, hist);
+    if (slot < 0) { eflags |= EF_WALL_SLOTS; continue; }
+    double ot[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ot[c] = p.dt * vt[c] + hist[c];
+    const double mag = sqrt(dot3(ot, ot));
+    double ft[3];
+    if (mag > 0.0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ft[c] = -kt_w * ot[c] - etat_w * vt[c];
+      const double ftmd = sqrt(dot3(ft, ft));
+      const double fnmd = p.mew_w * sqrt(dot3(fn, fn));
+      if (ftmd > fnmd) {
+        double tg[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tg[c] = ot[c] / mag;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ft[c] = -fnmd * tg[c];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ot[c] = (fnmd / kt_w) * tg[c];
+      }
+    } else {
+      ft[0] = ft[1] = ft[2] = 0.0;
+    }
+    double* wp = w.wall_pft + ((size_t)me * p.cmax + slot) * 3;  // UPDATE_COLLISION
+    wp[0] = ot[0]; wp[1] = ot[1]; wp[2] = ot[2];
+    ++nwc;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f[c] = f[c] + fn[c] + ft[c];
+    double nxf[3]; cross3(nrm, ft, nxf);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) t[c] = t[c] + distmod * nxf[c];
+    if (p.mew_rw > 0.0) {
+      const double om = sqrt(dot3(s.w, s.w));
+      if (om > 0.0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) t[c] = t[c] + -(p.mew_rw * (2.0 * r) * kn_w * overlap_n * s.w[c] / om);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MODE 0: forces into FC/TOW.  MODE 1: fused Euler.  MODE 2: fused AB2.
+template <int COLL, int MODE>
+__global__ void __launch_bounds__(128)
+k_force(DevParams p, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
+        const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
+        double4* __restrict__ omg_n, const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
+        const int* __restrict__ row_end, const int* __restrict__ nbrs, const int* __restrict__ in_start,
+        const int2* __restrict__ in_pair, const double* __restrict__ pft_in, double* __restrict__ pft_out,
+        WallCtx w, double* __restrict__ fc, double* __restrict__ tow, double* __restrict__ acc_old,
+        double* __restrict__ rot_acc_old, DevErr* __restrict__ err) {
+  const int me = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long ncont = 0, nwc = 0;
+  unsigned eflags = 0;
+  if (me < p.n) {
+    const int8_t st = state[me];
+    PState S;
+    load_p(pos_c, vel_c, omg_c, phase, me, S);
+    double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+    if (st == DEM_STATE_NORMAL && w.nf > 0) wall_contacts<COLL>(p, w, me, S, f, t, nwc, eflags);
+    const int rs = me ? row_end[me - 1] : 0, re = row_end[me];
+    const int is = in_start[me], ie = in_start[me + 1];
+    if (st != DEM_STATE_NONEXISTENT) {
+      // pairs owned by lower-index particles, then own row, then the rest
+      int q = is;
+      for (int pass = 0; pass < 2; ++pass) {
+        for (; q < ie; ++q) {
+          const int2 e = in_pair[q];
+          if (pass == 0 && e.x > me) break;
+          if (state[e.x] == DEM_STATE_NONEXISTENT) continue;
+          PState L;
+          load_p(pos_c, vel_c, omg_c, phase, e.x, L);
+          const double* pi = pft_in + 3 * (size_t)e.y;
+          double pin[3] = {pi[0], pi[1], pi[2]}, pout[3];
+          PairRes o;
+          pair_force<COLL>(p, L, S, pin, pout, o);
+          if (!o.contact) continue;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) f[c] = f[c] - o.fc[c];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) t[c] = t[c] + o.ti[c];
+          if (o.roll_i) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) t[c] = t[c] + o.ri[c];
+          }
+        }
+        if (pass == 0) {
+          for (int cc = rs; cc < re; ++cc) {
+            const int i = nbrs[cc];
+            const double* pi = pft_in + 3 * (size_t)cc;
+            double pin[3] = {pi[0], pi[1], pi[2]};
+            double* po = pft_out + 3 * (size_t)cc;
+            if (state[i] == DEM_STATE_NONEXISTENT) { po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2]; continue; }
+            PState I;
+            load_p(pos_c, vel_c, omg_c, phase, i, I);
+            double pout[3];
+            PairRes o;
+            pair_force<COLL>(p, S, I, pin, pout, o);
+            po[0] = pout[0]; po[1] = pout[1]; po[2] = pout[2];
+            if (o.zero) {
+              eflags |= EF_ZERO_DIST;
+              err->zero_a = me; err->zero_b = i;
+            }
+            if (!o.contact) continue;
+            ++ncont;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) f[c] = f[c] + o.fc[c];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) t[c] = t[c] + o.tl[c];
+            if (o.roll_l) {
+#pragma unroll
+              for (int c = 0; c < 3; ++c) t[c] = t[c] + o.rl[c];
+            }
+          }
+        }
+      }
+    } else {
+      for (int cc = rs; cc < re; ++cc) {
+        const double* pi = pft_in + 3 * (size_t)cc;
+        double* po = pft_out + 3 * (size_t)cc;
+        po[0] = pi[0]; po[1] = pi[1]; po[2] = pi[2];
+      }
+    }
+
+    const size_t n = (size_t)p.n;
+    if (MODE == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) { fc[c * n + me] = f[c]; tow[c * n + me] = t[c]; }
+    } else {
+      const double dt = p.dt;
+      const double omoi = omg_c[me].w;
+      double xn[3], vn[3], wn[3];
+      if (MODE == 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          vn[c] = S.v[c];
+          if (st == DEM_STATE_NORMAL) vn[c] = S.v[c] + dt * (f[c] / S.m + p.grav[c]);
+          xn[c] = S.x[c];
+          if (st < DEM_STATE_NORMAL_GHOST) xn[c] = S.x[c] + vn[c] * dt;
+          wn[c] = S.w[c];
+          if (st == DEM_STATE_NORMAL) wn[c] = S.w[c] + t[c] * omoi * dt;
+        }
+      } else {
+        const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
+                             st == DEM_STATE_NORMAL_GHOST || st == 110);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
+          if (p.first_pass && fp_ok) { ao = f[c] / S.m + p.grav[c]; ro = t[c]; }
+          double a = f[c];
+          if (st == DEM_STATE_NORMAL) a = f[c] / S.m + p.grav[c];
+          vn[c] = S.v[c];
+          if (st == DEM_STATE_NORMAL) vn[c] = S.v[c] + 0.5 * (3.0 * a - ao) * dt;
+          acc_old[c * n + me] = a;
+          xn[c] = S.x[c];
+          if (st < DEM_STATE_NORMAL_GHOST) xn[c] = S.x[c] + 0.5 * (S.v[c] + vn[c]) * dt;
+          wn[c] = S.w[c];
+          if (st == DEM_STATE_NORMAL) {
+            wn[c] = S.w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
+            ro = t[c] * omoi;
+          }
+          rot_acc_old[c * n + me] = ro;
+        }
+      }
+      pos_n[me] = make_double4(xn[0], xn[1], xn[2], S.r);
+      vel_n[me] = make_double4(vn[0], vn[1], vn[2], S.m);
+      omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+    }
+  }
+  // warp-aggregated counters
+  for (int o = 16; o > 0; o >>= 1) {
+    ncont += __shfl_down_sync(0xffffffffu, ncont, o);
+    nwc += __shfl_down_sync(0xffffffffu, nwc, o);
+    eflags |= __shfl_down_sync(0xffffffffu, eflags, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (ncont) atomicAdd(&err->n_contacts, ncont);
+    if (nwc) atomicAdd(&err->n_wall_contacts, nwc);
+    if (eflags) atomicOr(&err->flags, eflags);
+  }
+}
+
+// CFUPDATEOLD + CFNEWVALUES from FC/TOW, in place; zeroes FC/TOW.
+template <int INTG>
+__global__ void k_integrate(DevParams p, double4* __restrict__ pos4, double4* __restrict__ vel4,
+                            double4* __restrict__ omg4, const int8_t* __restrict__ state,
+                            double* __restrict__ fc, double* __restrict__ tow,
+                            double* __restrict__ acc_old, double* __restrict__ rot_acc_old) {
+  const int me = blockIdx.x * blockDim.x + threadIdx.x;
+  if (me >= p.n) return;
+  const size_t n = (size_t)p.n;
+  const int8_t st = state[me];
+  double4 X = pos4[me], Vv = vel4[me], W = omg4[me];
+  double x[3] = {X.x, X.y, X.z}, v[3] = {Vv.x, Vv.y, Vv.z}, w[3] = {W.x, W.y, W.z};
+  const double m = Vv.w, omoi = W.w, dt = p.dt;
+  double f[3], t[3];
+  for (int c = 0; c < 3; ++c) { f[c] = fc[c * n + me]; t[c] = tow[c * n + me]; fc[c * n + me] = 0.0; tow[c * n + me] = 0.0; }
+  double xn[3], vn[3], wn[3];
+  if (INTG == DEM_INTG_EULER) {
+    for (int c = 0; c < 3; ++c) {
+      vn[c] = v[c];
+      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + dt * (f[c] / m + p.grav[c]);
+      xn[c] = x[c];
+      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + vn[c] * dt;
+      wn[c] = w[c];
+      if (st == DEM_STATE_NORMAL) wn[c] = w[c] + t[c] * omoi * dt;
+    }
+  } else {
+    const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
+                         st == DEM_STATE_NORMAL_GHOST || st == 110);
+    for (int c = 0; c < 3; ++c) {
+      double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
+      if (p.first_pass && fp_ok) { ao = f[c] / m + p.grav[c]; ro = t[c]; }
+      double a = f[c];
+      if (st == DEM_STATE_NORMAL) a = f[c] / m + p.grav[c];
+      vn[c] = v[c];
+      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + 0.5 * (3.0 * a - ao) * dt;
+      acc_old[c * n + me] = a;
+      xn[c] = x[c];
+      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + 0.5 * (v[c] + vn[c]) * dt;
+      wn[c] = w[c];
+      if (st == DEM_STATE_NORMAL) {
+        wn[c] = w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
+        ro = t[c] * omoi;
+      }
+      rot_acc_old[c * n + me] = ro;
+    }
+  }
+  pos4[me] = make_double4(xn[0], xn[1], xn[2], X.w);
+  vel4[me] = make_double4(vn[0], vn[1], vn[2], m);
+  omg4[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+}
+
+static WallCtx wall_ctx(dem_handle* h) {
+  WallCtx w;
+  w.vertex = h->vertex; w.norm_face = h->norm_face; w.ignore_edge = h->ignore_edge;
+  w.fbin_start = h->fbin_start; w.fbin = h->fbin; w.dg_pijk = h->dg_pijk;
+  w.wall_fid = h->wall_fid; w.wall_pft = h->wall_pft; w.nf = h->nf;
+  return w;
+}
+
+template <int COLL, int MODE>
+static void launch_force(dem_handle* h, int nb) {
+  const int T = 128, B = (h->n + T - 1) / T;
+  const int c = h->cur, pc = h->pcur;
+  k_force<COLL, MODE><<<B, T, 0, h->stream>>>(
+      h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
+      h->state, h->phase, h->row_end[h->rb], h->nbrs[h->rb], h->in_start, h->in_pair,
+      h->pft[pc], h->pft[1 - pc], wall_ctx(h), h->fc, h->tow, h->acc_old, h->rot_acc_old, h->derr);
+  DEM_LAUNCH(h);
+  (void)nb;
+}
+
+int run_force(dem_handle* h, bool fused) {
+  ProfScope ps(h, DEM_PROF_FORCE);
+  h->dp.first_pass = h->first_pass ? 1 : 0;
+  const bool hz = h->dp.coll == DEM_COLL_HERTZ;
+  const bool ab2 = h->dp.intg == DEM_INTG_AB2;
+  if (!fused) {
+    if (hz) launch_force<DEM_COLL_HERTZ, 0>(h, 0); else launch_force<DEM_COLL_LSD, 0>(h, 0);
+  } else if (ab2) {
+    if (hz) launch_force<DEM_COLL_HERTZ, 2>(h, 0); else launch_force<DEM_COLL_LSD, 2>(h, 0);
+  } else {
+    if (hz) launch_force<DEM_COLL_HERTZ, 1>(h, 0); else launch_force<DEM_COLL_LSD, 1>(h, 0);
+  }
+  if (int rc = check_cuda(h, cudaGetLastError(), "k_force")) return rc;
+  h->pcur = 1 - h->pcur;
+  if (fused) { h->cur = 1 - h->cur; h->first_pass = false; }
+  return 0;
+}
+
+int run_cfnewvalues(dem_handle* h) {
+  ProfScope ps(h, DEM_PROF_INTEGRATE);
+  h->dp.first_pass = h->first_pass ? 1 : 0;
+  const int T = 256, B = (h->n + T - 1) / T;
+  const int c = h->cur;
+  if (h->dp.intg == DEM_INTG_AB2)
+    k_integrate<DEM_INTG_AB2><<<B, T, 0, h->stream>>>(h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->state,
+                                                      h->fc, h->tow, h->acc_old, h->rot_acc_old);
+  else
+    k_integrate<DEM_INTG_EULER><<<B, T, 0, h->stream>>>(h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->state,
+                                                        h->fc, h->tow, h->acc_old, h->rot_acc_old);
+  DEM_LAUNCH(h);
+  h->first_pass = false;
+  return check_cuda(h, cudaGetLastError(), "k_integrate");
+}
+
+}  // namespace demb

@@ -1,0 +1,274 @@
+// neighbor.cu -- pair-list build and history carry-over (K2).
+//
+// Replaces NEIGHBOUR (model/des/neighbour.f:21-126) with its
+// DESGRID_NEIGH_BUILD (model/des/desgrid_mod.f:1002-1299) and ADD_PAIR
+// (model/des/des_allocate_mod.f:555-567), serial build semantics:
+//   * rows only for NORMAL particles; a NORMAL particle found in a ghost cell
+//     is rogue: it is deleted (REMOVE_ROGUE_PARTICLES) and, as in the
+//     reference where the shared do_exit flag stays set, every particle with a
+//     larger index gets an empty row in that build;
+//   * candidates are visited cell by cell in (lk, lj, li) stencil order,
+//     each cell in ascending particle index; coarse grids (cell narrower than
+//     2*FACTOR_RLM*MAX_RADIUS) scan only the nearer neighbour cell per axis;
+//   * a candidate is kept when it is not the particle itself, not a NORMAL
+//     particle of lower index, not NONEXISTENT, and
+//     |x_i - x_j|^2 <= (FACTOR_RLM*(r_i + r_j))^2 in FP64.
+// The list is built as count -> scan -> fill, so NEIGHBOR_INDEX / NEIGHBORS
+// come out bit-identical to the serial reference.  PFT_NEIGHBOR is carried
+// over by matching the neighbour id inside the particle's previous row
+// (neighbour.f:77-117).  Finally the transpose (incoming pairs per particle,
+// ascending owner) is built for the deterministic force gather.
+#include "dem_internal.cuh"
+
+namespace demb {
+
+__global__ void k_find_rogue(DevParams p, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
+                             DevErr* __restrict__ err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n || state[i] != DEM_STATE_NORMAL) return;
+  int c = dg_pijk[i];
+  int lic = dg_iof(p, c), ljc = dg_jof(p, c), lkc = dg_kof(p, c);
+  if (lic < p.istart1 || lic > p.iend1 || ljc < p.jstart1 || ljc > p.jend1 ||
+      lkc < p.kstart1 || lkc > p.kend1) {
+    atomicMin(&err->first_rogue, i);
+  }
+}
+
+// DELETE_PARTICLE (mass_outflow_dem.f:241-300) for the rogue particles.
+__global__ void k_delete_rogue(DevParams p, int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
+                               double4* __restrict__ pos4, double4* __restrict__ vel4, double4* __restrict__ omg4,
+                               double* __restrict__ fc, double* __restrict__ tow, int* __restrict__ wall_fid,
+                               DevErr* __restrict__ err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n || state[i] != DEM_STATE_NORMAL) return;
+  int c = dg_pijk[i];
+  int lic = dg_iof(p, c), ljc = dg_jof(p, c), lkc = dg_kof(p, c);
+  if (!(lic < p.istart1 || lic > p.iend1 || ljc < p.jstart1 || ljc > p.jend1 ||
+        lkc < p.kstart1 || lkc > p.kend1)) return;
+  if (!p.remove_rogue) { atomicOr(&err->flags, EF_ROGUE_FATAL); return; }
+  pos4[i] = make_double4(0.0, 0.0, 0.0, 0.0);                         // DES_RADIUS = 0
+  vel4[i] = make_double4(0.0, 0.0, 0.0, 3.4028234663852886e38);       // PMASS = HUGE(0.0)
+  omg4[i] = make_double4(0.0, 0.0, 0.0, 0.0);                         // OMOI = 0
+  for (int a = 0; a < 3; ++a) { fc[(size_t)a * p.n + i] = 0.0; tow[(size_t)a * p.n + i] = 0.0; }
+  for (int s = 0; s < p.cmax; ++s) wall_fid[(size_t)i * p.cmax + s] = -1;
+  state[i] = DEM_STATE_NONEXISTENT;
+  atomicAdd(&err->rogue_removed, 1ull);
+}
+
+// Count (FILL = false) or fill (FILL = true) one row per particle.
+template <bool FILL>
+__global__ void k_neigh(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict__ state,
+                        const int* __restrict__ dg_pijk, const int* __restrict__ cell_start,
+                        const int* __restrict__ cell_list, const DevErr* __restrict__ err,
+                        int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
+                        int* __restrict__ owner, long long cap) {
+  const int cur = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cur >= p.n) return;
+  int start = 0;
+  if (FILL) start = row_se[cur];
+  int cnt = 0;
+  if (state[cur] == DEM_STATE_NORMAL && cur < err->first_rogue) {
+    const int lijk = dg_pijk[cur];
+    const int lic = dg_iof(p, lijk), ljc = dg_jof(p, lijk), lkc = dg_kof(p, lijk);
+    const double4 cp = pos4[cur];
+    const double fr = p.factor_rlm, mr = p.max_radius;
+    int il = 1, iu = 1, jl = 1, ju = 1, kl = 1, ku = 1;
+    const double cpos[3] = {cp.x, cp.y, cp.z};
+    int* lo_off[3] = {&il, &jl, &kl};
+    int* hi_off[3] = {&iu, &ju, &ku};
+    for (int ax = 0; ax < 3; ++ax) {
+      if (ax == 2 && p.no_k) { kl = 0; ku = 0; break; }
+      bool coarse = 1.0 > 2.0 * mr * fr * p.dg_inv[ax];
+      if (coarse) {
+        double t = (cpos[ax] - p.dg_start[ax]) * p.dg_inv[ax];
+        double off = t - (double)(long long)floor(t);
+        if (off >= 0.5) *lo_off[ax] = 0; else *hi_off[ax] = 0;
+      }
+    }
+    for (int lk = lkc - kl; lk <= lkc + ku; ++lk)
+    for (int lj = ljc - jl; lj <= ljc + ju; ++lj)
+    for (int li = lic - il; li <= lic + iu; ++li) {
+      int ri = li, rj = lj, rk = lk;
+      double sh0 = 0.0, sh1 = 0.0, sh2 = 0.0;
+      if (p.per[0]) {
+        if (li < p.istart1) { ri = p.iend1; sh0 = -p.L[0]; }
+        else if (li > p.iend1) { ri = p.istart1; sh0 = p.L[0]; }
+      }
+      if (p.per[1]) {
+        if (lj < p.jstart1) { rj = p.jend1; sh1 = -p.L[1]; }
+        else if (lj > p.jend1) { rj = p.jstart1; sh1 = p.L[1]; }
+      }
+      if (p.per[2] && !p.no_k) {
+        if (lk < p.kstart1) { rk = p.kend1; sh2 = -p.L[2]; }
+        else if (lk > p.kend1) { rk = p.kstart1; sh2 = p.L[2]; }
+      }
+      const int cell = dg_funijk(p, ri, rj, rk) - 1;
+      const int s = cell_start[cell], e = cell_start[cell + 1];
+      for (int q = s; q < e; ++q) {
+        const int nb = cell_list[q];
+        if (nb == cur) continue;
+        const int8_t sn = state[nb];
+        if (nb < cur && sn == DEM_STATE_NORMAL) continue;
+        if (sn == DEM_STATE_NONEXISTENT) continue;
+        const double4 np_ = pos4[nb];
+        const double srad = fr * (cp.w + np_.w);
+        double px = np_.x, py = np_.y, pz = np_.z;
+        if (sh0 != 0.0) px = px + sh0;
+        if (sh1 != 0.0) py = py + sh1;
+        if (sh2 != 0.0) pz = pz + sh2;
+        const double d0 = cp.x - px, d1 = cp.y - py, d2 = cp.z - pz;
+        const double dd = d0 * d0 + d1 * d1 + d2 * d2;
+        if (dd > srad * srad) continue;
+        if (FILL) {
+          long long slot = (long long)start + cnt;
+          if (slot < cap) { nbrs[slot] = nb; owner[slot] = cur; }
+        }
+        ++cnt;
+      }
+    }
+  }
+  if (FILL) row_se[cur] = start + cnt;   // start -> end pointer
+  else row_cnt[cur] = cnt;
+}
+
+// neighbour.f:77-117: history of each new pair from the same neighbour id in
+// the particle's previous row, zero when the pair is new.
+__global__ void k_remap(int n, const int* __restrict__ row_end, const int* __restrict__ nbrs,
+                        const int* __restrict__ old_end, const int* __restrict__ old_nbrs,
+                        const double* __restrict__ old_pft, double* __restrict__ pft, int have_old) {
+  const int ll = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ll >= n) return;
+  const int s = ll ? row_end[ll - 1] : 0, e = row_end[ll];
+  int so = 0, eo = 0;
+  if (have_old) { so = ll ? old_end[ll - 1] : 0; eo = old_end[ll]; }
+  for (int cc = s; cc < e; ++cc) {
+    const int nb = nbrs[cc];
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int co = so; co < eo; ++co) {
+      if (old_nbrs[co] == nb) {
+        a = old_pft[3 * (size_t)co]; b = old_pft[3 * (size_t)co + 1]; c = old_pft[3 * (size_t)co + 2];
+        break;
+      }
+    }
+    pft[3 * (size_t)cc] = a; pft[3 * (size_t)cc + 1] = b; pft[3 * (size_t)cc + 2] = c;
+  }
+}
+
+__global__ void k_in_count(long long np, const int* __restrict__ nbrs, int* __restrict__ in_cnt) {
+  long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cc >= np) return;
+  atomicAdd(&in_cnt[nbrs[cc]], 1);
+}
+
+__global__ void k_in_fill(long long np, const int* __restrict__ nbrs, const int* __restrict__ owner,
+                          const int* __restrict__ in_start, int* __restrict__ in_fill, int2* __restrict__ in_pair) {
+  long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cc >= np) return;
+  int j = nbrs[cc];
+  int slot = atomicAdd(&in_fill[j], 1);
+  in_pair[in_start[j] + slot] = make_int2(owner[cc], (int)cc);
+}
+
+// incoming pairs of each particle in ascending pair index (= owner order)
+__global__ void k_in_sort(int n, const int* __restrict__ in_start, int2* __restrict__ in_pair) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int s = in_start[j], e = in_start[j + 1];
+  for (int a = s + 1; a < e; ++a) {
+    int2 v = in_pair[a];
+    int b = a - 1;
+    while (b >= s && in_pair[b].y > v.y) { in_pair[b + 1] = in_pair[b]; --b; }
+    in_pair[b + 1] = v;
+  }
+}
+
+int ensure_pair_capacity(dem_handle* h, long long need) {
+  if (need <= h->pair_cap) return 0;
+  long long cap = h->pair_cap > 0 ? h->pair_cap : 1024;
+  while (cap < need) cap *= 2;
+  const long long old = h->n_pairs;
+  int* nb[2]; double* pf[2]; int2* inp; int* own;
+  for (int b = 0; b < 2; ++b) {
+    if (int rc = check_cuda(h, cudaMalloc(&nb[b], sizeof(int) * cap), "cudaMalloc nbrs")) return rc;
+    if (int rc = check_cuda(h, cudaMalloc(&pf[b], sizeof(double) * 3 * cap), "cudaMalloc pft")) return rc;
+  }
+  if (int rc = check_cuda(h, cudaMalloc(&inp, sizeof(int2) * cap), "cudaMalloc in_pair")) return rc;
+  if (int rc = check_cuda(h, cudaMalloc(&own, sizeof(int) * cap), "cudaMalloc owner")) return rc;
+  if (old > 0) {
+    // keep the current list and history (the rebuild reads them)
+    cudaMemcpyAsync(nb[h->rb], h->nbrs[h->rb], sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(pf[h->pcur], h->pft[h->pcur], sizeof(double) * 3 * old, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(inp, h->in_pair, sizeof(int2) * old, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(own, h->pair_owner, sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
+  }
+  cudaStreamSynchronize(h->stream);
+  for (int b = 0; b < 2; ++b) { cudaFree(h->nbrs[b]); cudaFree(h->pft[b]); h->nbrs[b] = nb[b]; h->pft[b] = pf[b]; }
+  cudaFree(h->in_pair); cudaFree(h->pair_owner);
+  h->in_pair = inp; h->pair_owner = own;
+  h->pair_cap = cap;
+  return check_cuda(h, cudaGetLastError(), "grow pairs");
+}
+
+int run_neighbour(dem_handle* h, bool carry_history) {
+  ProfScope ps(h, DEM_PROF_NEIGHBOR);
+  const DevParams& p = h->dp;
+  const int n = h->n, T = 128, B = (n + T - 1) / T;
+  DevErr* e = h->derr;
+  // first_rogue := n
+  {
+    int v = n;
+    if (int rc = check_cuda(h, cudaMemcpyAsync(&e->first_rogue, &v, sizeof(int), cudaMemcpyHostToDevice, h->stream), "copy")) return rc;
+    if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
+  }
+  k_find_rogue<<<B, T, 0, h->stream>>>(p, h->state, h->dg_pijk, e);
+  DEM_LAUNCH(h);
+  const int nb = 1 - h->rb;  // new list goes into the other buffer
+  k_neigh<false><<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, h->cell_start,
+                                         h->cell_list, e, h->row_cnt, nullptr, nullptr, nullptr, 0);
+  DEM_LAUNCH(h);
+  // delete rogue particles only after every row has been counted with the
+  // states the serial loop saw
+  int* total = h->cell_fill;  // scratch int on device (cell_fill is free here)
+  if (int rc = exclusive_scan(h, h->row_cnt, h->row_end[nb], n, total)) return rc;
+  int P = 0;
+  if (int rc = check_cuda(h, cudaMemcpyAsync(&P, total, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "copy P")) return rc;
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
+  if (int rc = ensure_pair_capacity(h, (long long)P + 1)) return rc;
+  k_neigh<true><<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, h->cell_start,
+                                        h->cell_list, e, nullptr, h->row_end[nb], h->nbrs[nb],
+                                        h->pair_owner, h->pair_cap);
+  DEM_LAUNCH(h);
+  k_delete_rogue<<<B, T, 0, h->stream>>>(p, h->state, h->dg_pijk, h->pos4[h->cur], h->vel4[h->cur],
+                                         h->omg4[h->cur], h->fc, h->tow, h->wall_fid, e);
+  DEM_LAUNCH(h);
+  // history carry-over into the other pft buffer
+  const int pn = 1 - h->pcur;
+  k_remap<<<B, T, 0, h->stream>>>(n, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
+                                  h->pft[h->pcur], h->pft[pn], (carry_history && h->have_pairs) ? 1 : 0);
+  DEM_LAUNCH(h);
+  h->rb = nb;
+  h->pcur = pn;
+  h->n_pairs = P;
+  h->have_pairs = true;
+  // transpose
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->in_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
+  if (P > 0) {
+    const int TP = 256;
+    const long long BP = ((long long)P + TP - 1) / TP;
+    k_in_count<<<(unsigned)BP, TP, 0, h->stream>>>(P, h->nbrs[nb], h->in_cnt);
+    DEM_LAUNCH(h);
+  }
+  if (int rc = exclusive_scan(h, h->in_cnt, h->in_start, n, h->in_start + n)) return rc;
+  if (P > 0) {
+    const int TP = 256;
+    const long long BP = ((long long)P + TP - 1) / TP;
+    if (int rc = check_cuda(h, cudaMemsetAsync(h->in_fill, 0, sizeof(int) * n, h->stream), "memset")) return rc;
+    k_in_fill<<<(unsigned)BP, TP, 0, h->stream>>>(P, h->nbrs[nb], h->pair_owner, h->in_start, h->in_fill, h->in_pair);
+    DEM_LAUNCH(h);
+    k_in_sort<<<B, T, 0, h->stream>>>(n, h->in_start, h->in_pair);
+    DEM_LAUNCH(h);
+  }
+  return check_cuda(h, cudaGetLastError(), "neighbour");
+}
+
+}  // namespace demb

@@ -177,6 +177,8 @@ DEM_ONLY = {
     "launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "set_stream": (C.c_int, [_P, C.c_void_p]),
     "force_error": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "set_profiling": (C.c_int, [_P, C.c_int32]),
+    "get_profile": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
 }
 
 

@@ -1,0 +1,223 @@
+"""Seeded synthetic DEM workloads (no dataset is involved in the reference's
+DEM benchmarks; these follow the shapes the workloads are specified with).
+
+- `settling_4k`      4,000 monodisperse 1 mm spheres, LSD, 12x60x12 mm box,
+                     lattice 1.1 d with +-0.04 d jitter (the CPU-runnable case).
+- `hertz_rsa_1m`     1,000,000 lognormal spheres (median 1 mm, sigma 0.25,
+                     clipped 0.5-2 mm), Hertz E=1e7, periodic x/z, bottom
+                     wall, random sequential placement at 40 % solids.
+- `coupled_500k`     500,000 spheres of 0.5 mm in a 64x256x64 fluid grid.
+
+Particles are numbered in DES-cell order (k, then i, then j fastest, the
+order of DG_FUNIJK), which is a free choice of the input and gives the
+neighbour gathers spatial locality.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import abi
+from . import params as P
+
+SEED_BASE = 1000
+
+
+def _rsa_numba():
+    import numba as nb
+
+    @nb.njit(cache=False)
+    def rsa(diam, lo, hi, periodic, cell, ncell, seed, max_attempts, grow):
+        n = diam.shape[0]
+        pos = np.zeros((n, 3))
+        cap = 64
+        grid = -np.ones((ncell[0] * ncell[1] * ncell[2], cap), dtype=np.int64)
+        gcnt = np.zeros(ncell[0] * ncell[1] * ncell[2], dtype=np.int64)
+        np.random.seed(seed)
+        y_top = hi[1]
+        L = hi - lo
+        placed = 0
+        for i in range(n):
+            r = 0.5 * diam[i]
+            ok = False
+            att = 0
+            while not ok:
+                att += 1
+                if att > max_attempts:
+                    y_top = y_top + grow
+                    att = 0
+                x = np.empty(3)
+                for a in range(3):
+                    if a == 1:
+                        x[a] = lo[1] + r + np.random.random() * (min(y_top, hi[1] + 1e9) - lo[1] - 2 * r)
+                    elif periodic[a]:
+                        x[a] = lo[a] + np.random.random() * L[a]
+                    else:
+                        x[a] = lo[a] + r + np.random.random() * (L[a] - 2 * r)
+                ci = np.empty(3, dtype=np.int64)
+                for a in range(3):
+                    ci[a] = int((x[a] - lo[a]) / cell[a])
+                    if ci[a] < 0:
+                        ci[a] = 0
+                    if ci[a] >= ncell[a]:
+                        ci[a] = ncell[a] - 1
+                ok = True
+                for dk in range(-1, 2):
+                    if not ok:
+                        break
+                    for di in range(-1, 2):
+                        if not ok:
+                            break
+                        for dj in range(-1, 2):
+                            c0 = ci[0] + di
+                            c1 = ci[1] + dj
+                            c2 = ci[2] + dk
+                            if periodic[0]:
+                                c0 = (c0 + ncell[0]) % ncell[0]
+                            if periodic[2]:
+                                c2 = (c2 + ncell[2]) % ncell[2]
+                            if c0 < 0 or c0 >= ncell[0] or c1 < 0 or c1 >= ncell[1] or c2 < 0 or c2 >= ncell[2]:
+                                continue
+                            g = (c2 * ncell[0] + c0) * ncell[1] + c1
+                            for s in range(gcnt[g]):
+                                j = grid[g, s]
+                                d2 = 0.0
+                                for a in range(3):
+                                    d = x[a] - pos[j, a]
+                                    if periodic[a]:
+                                        if d > 0.5 * L[a]:
+                                            d -= L[a]
+                                        elif d < -0.5 * L[a]:
+                                            d += L[a]
+                                    d2 += d * d
+                                rr = r + 0.5 * diam[j]
+                                if d2 < rr * rr:
+                                    ok = False
+                                    break
+                            if not ok:
+                                break
+                if ok:
+                    g = (ci[2] * ncell[0] + ci[0]) * ncell[1] + ci[1]
+                    if gcnt[g] >= cap:
+                        ok = False
+                        continue
+                    for a in range(3):
+                        pos[i, a] = x[a]
+                    grid[g, gcnt[g]] = i
+                    gcnt[g] += 1
+                    placed += 1
+        return pos, y_top
+
+    return rsa
+
+
+def random_sequential_placement(diam, lo, hi, periodic, seed, region_top, max_attempts=4000, grow_frac=0.005):
+    """Places spheres (largest first) uniformly at random without overlap in
+    [lo, (hi.x, region_top, hi.z)], raising the region top by grow_frac of its
+    height whenever max_attempts consecutive tries fail.  Returns positions
+    (in the input order of `diam`) and the final region top."""
+    order = np.argsort(-diam, kind="stable")
+    d_sorted = diam[order]
+    lo = np.asarray(lo, float)
+    hi_reg = np.asarray(hi, float).copy()
+    hi_reg[1] = region_top
+    dmax = float(d_sorted[0])
+    ncell = np.maximum(((np.asarray(hi, float) - lo) / dmax).astype(np.int64), 1)
+    cell = (np.asarray(hi, float) - lo) / ncell
+    rsa = _rsa_numba()
+    pos_sorted, top = rsa(d_sorted, lo, hi_reg, np.asarray(periodic, np.bool_), cell, ncell,
+                          int(seed) % (2**31), max_attempts, grow_frac * (region_top - lo[1]))
+    pos = np.empty_like(pos_sorted)
+    pos[order] = pos_sorted
+    return pos, float(top)
+
+
+def _sort_by_des_cell(prm, pos):
+    """Permutation that orders particles by DG_FUNIJK cell (j fastest)."""
+    li = np.floor((pos[:, 0] - prm.dg_xstart) * prm.dg_dxinv).astype(np.int64)
+    lj = np.floor((pos[:, 1] - prm.dg_ystart) * prm.dg_dyinv).astype(np.int64)
+    lk = np.floor((pos[:, 2] - prm.dg_zstart) * prm.dg_dzinv).astype(np.int64)
+    key = (lk * (prm.dg_imax + 2) + li) * (prm.dg_jmax + 2) + lj
+    return np.argsort(key, kind="stable")
+
+
+def _arrays(pos, vel, omega, radius, rho):
+    n = pos.shape[0]
+    _, pmass, omoi = P.particle_props(radius, rho)
+    return {
+        "pos": np.ascontiguousarray(pos.T), "vel": np.ascontiguousarray(vel.T),
+        "omega": np.ascontiguousarray(omega.T), "radius": radius, "pmass": pmass, "omoi": omoi,
+        "state": np.full(n, abi.DEM_STATE_NORMAL, np.int8), "phase": np.ones(n, np.int32),
+    }
+
+
+def hertz_rsa(n=1_000_000, box=(0.1, 0.4, 0.1), solids=0.40, seed=SEED_BASE + 1,
+              precision=abi.DEM_PREC_FP64, nsn=25, cache_dir=None):
+    """1M polydisperse Hertzian spheres: lognormal d (median 1 mm, sigma
+    0.25, clipped to [0.5, 2] mm), rho 2500, E 1e7, nu 0.3, e_n = e_t = 0.85,
+    mu 0.3, mu_r 0.01, periodic x/z, flat bottom wall; random sequential
+    placement with the region height set for `solids` volume fraction.
+    The placement is cached as .npz in `cache_dir` when given."""
+    rng = np.random.default_rng(seed)
+    d = np.clip(1e-3 * np.exp(rng.normal(0.0, 0.25, n)), 0.5e-3, 2.0e-3)
+    vol = float(np.sum((math.pi / 6.0) * d ** 3))
+    top = vol / (solids * box[0] * box[2])
+    cache = None
+    if cache_dir is not None:
+        from pathlib import Path
+        cache = Path(cache_dir) / f"hertz_rsa_{n}_{seed}_{box[0]:.4g}_{box[2]:.4g}_{solids:.3f}.npz"
+    if cache is not None and cache.exists():
+        z = np.load(cache)
+        pos, top_final = z["pos"], float(z["top"])
+    else:
+        pos, top_final = random_sequential_placement(d, (0, 0, 0), box, (True, False, True), seed, top)
+        if cache is not None:
+            cache.parent.mkdir(parents=True, exist_ok=True)
+            np.savez(cache, pos=pos, top=top_final)
+    vel = np.zeros((n, 3)); omega = np.zeros((n, 3))
+    radius = 0.5 * d
+    case = P.DemCase(d_p0=(2e-3,), ro_s0=(2500.0,), coll_model="HERTZ", intg_method="EULER",
+                     des_en_input=0.85, des_en_wall_input=[0.85], des_et_input=0.85, des_et_wall_input=[0.85],
+                     e_young=(1e7,), v_poisson=(0.3,), ew_young=1e7, vw_poisson=0.3,
+                     mew=0.3, mew_w=0.3, mew_r=0.01, mew_rw=0.01, grav=(0.0, -9.81, 0.0),
+                     domain_hi=box, fluid_cells=(1, 1, 1), periodic=(True, False, True),
+                     neighbor_search_n=nsn, force_precision=precision)
+    arr = _arrays(pos, vel, omega, radius, np.full(n, 2500.0))
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    perm = _sort_by_des_cell(prm, pos)
+    arr = _arrays(pos[perm], vel[perm], omega[perm], radius[perm], np.full(n, 2500.0))
+    walls = P.default_walls(case.domain_lo, case.domain_hi, periodic=case.periodic)
+    info.update({"region_top": top, "region_top_final": top_final,
+                 "solids_fraction": vol / (box[0] * box[2] * top_final)})
+    return case, prm, arr, walls, info
+
+
+def settling(n_side=(10, 40, 10), d=1e-3, rho=2500.0, box=(12e-3, 60e-3, 12e-3), spacing=1.1,
+             jitter=0.04, vmax=0.1, seed=SEED_BASE, kn=1000.0, en=0.9, mew=0.1,
+             precision=abi.DEM_PREC_FP64):
+    """Dry settling: cubic lattice of spacing `spacing`*d, jitter +-`jitter`*d,
+    velocities U(+-vmax); LSD kn = kn_w, kt = 2/7 kn, e_n, friction mew;
+    default box walls; dt = t_coll/50.  n_side=(10,40,10) is the 4,000-sphere
+    case."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = n_side
+    n = nx * ny * nz
+    a = spacing * d
+    kk, ii, jj = np.meshgrid(np.arange(nz), np.arange(nx), np.arange(ny), indexing="ij")
+    pos = np.empty((n, 3))
+    pos[:, 0] = (ii.ravel() + 0.5) * a + (box[0] - nx * a) * 0.5
+    pos[:, 1] = (jj.ravel() + 0.5) * a
+    pos[:, 2] = (kk.ravel() + 0.5) * a + (box[2] - nz * a) * 0.5
+    pos += rng.uniform(-jitter * d, jitter * d, size=pos.shape)
+    vel = rng.uniform(-vmax, vmax, size=(n, 3))
+    omega = np.zeros((n, 3))
+    radius = np.full(n, 0.5 * d)
+    case = P.DemCase(d_p0=(d,), ro_s0=(rho,), coll_model="LSD", kn=kn, kn_w=kn,
+                     des_en_input=en, des_en_wall_input=[en], mew=mew, mew_w=mew,
+                     grav=(0.0, -9.81, 0.0), domain_hi=box, fluid_cells=(1, 1, 1),
+                     force_precision=precision)
+    arr = _arrays(pos, vel, omega, radius, np.full(n, rho))
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    walls = P.default_walls(case.domain_lo, case.domain_hi)
+    return case, prm, arr, walls, info

@@ -107,10 +107,15 @@ class DemSystem:
         self._call("upload_state", self._h, _dp(pos), _dp(vel), _dp(omega), _dp(radius),
                    _dp(pmass), _dp(omoi), _bp(state), _ip(phase), C.c_int32(n))
 
-    def download_state(self):
+    def download_state(self, out=None):
+        """DES_POS_NEW, DES_VEL_NEW, OMEGA_NEW, PARTICLE_STATE; `out` may hold
+        preallocated (e.g. pinned) arrays under the same keys."""
         n = self.n
-        pos = np.empty((3, n)); vel = np.empty((3, n)); omega = np.empty((3, n))
-        state = np.empty(n, dtype=np.int8)
+        if out is not None:
+            pos, vel, omega, state = out["pos"], out["vel"], out["omega"], out["state"]
+        else:
+            pos = np.empty((3, n)); vel = np.empty((3, n)); omega = np.empty((3, n))
+            state = np.empty(n, dtype=np.int8)
         self._call("download_state", self._h, _dp(pos), _dp(vel), _dp(omega), _bp(state), C.c_int32(n))
         return {"pos": pos, "vel": vel, "omega": omega, "state": state}
 
@@ -224,6 +229,17 @@ class DemSystem:
         self.nn = first + nsteps - 1
 
     # ---- CUDA-only ---------------------------------------------------
+    def set_profiling(self, on: bool):
+        self._call("set_profiling", self._h, C.c_int32(1 if on else 0))
+
+    def profile(self):
+        """{class: (ms, launches)} since profiling was switched on."""
+        ms = (C.c_double * 6)()
+        nl = (C.c_int64 * 6)()
+        self._call("get_profile", self._h, ms, nl)
+        names = ("force", "neighbor", "desgrid", "integrate", "coupling", "other")
+        return {k: (float(ms[i]), int(nl[i])) for i, k in enumerate(names)}
+
     def launch_count(self) -> int:
         v = C.c_int64()
         self._call("launch_count", self._h, C.byref(v))

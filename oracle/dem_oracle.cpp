@@ -201,84 +201,110 @@ struct Oracle {
 
   // DESGRID_NEIGH_BUILD (desgrid_mod.f:1002-1299), serial build with add_pair
   // (des_allocate_mod.f:555-567).  Rows follow the (lk, lj, li) stencil order
-  // and ascending particle index inside each cell.
-  void neigh_build() {
-    row_end.assign(n, 0);
-    nbrs.clear();
-    bool do_exit = false;
+  // and ascending particle index inside each cell.  The serial loop deletes a
+  // rogue particle when it reaches it and, because its do_exit flag stays
+  // set, gives every later particle an empty row; particles before the first
+  // rogue one still see it as NORMAL.  Rows are therefore computed with the
+  // pre-deletion states for cur < first_rogue, and the rogue particles are
+  // deleted afterwards, which is the same result.
+  int row_scan(int cur, int* out) const {
     const double fr = p.factor_rlm, mr = p.max_radius;
     bool coarse_x = 1.0 > 2.0 * mr * fr * p.dg_dxinv;
     bool coarse_y = 1.0 > 2.0 * mr * fr * p.dg_dyinv;
     bool coarse_z = 1.0 > 2.0 * mr * fr * p.dg_dzinv;
+    int cnt = 0;
+    int lijk = dg_pijk[cur];
+    int lic = iof(lijk), ljc = jof(lijk), lkc = kof(lijk);
+    int il = 1, iu = 1, jl = 1, ju = 1, kl = 1, ku = 1;
+    double cp[3] = {P(pos, cur, 0), P(pos, cur, 1), P(pos, cur, 2)};
+    if (coarse_x) {
+      double t = (cp[0] - p.dg_xstart) * p.dg_dxinv;
+      double off = t - (double)(long long)std::floor(t);
+      if (off >= 0.5) il = 0; else iu = 0;
+    }
+    if (coarse_y) {
+      double t = (cp[1] - p.dg_ystart) * p.dg_dyinv;
+      double off = t - (double)(long long)std::floor(t);
+      if (off >= 0.5) jl = 0; else ju = 0;
+    }
+    if (p.no_k) { kl = 0; ku = 0; }
+    else if (coarse_z) {
+      double t = (cp[2] - p.dg_zstart) * p.dg_dzinv;
+      double off = t - (double)(long long)std::floor(t);
+      if (off >= 0.5) kl = 0; else ku = 0;
+    }
+    for (int lk = lkc - kl; lk <= lkc + ku; ++lk)
+    for (int lj = ljc - jl; lj <= ljc + ju; ++lj)
+    for (int li = lic - il; li <= lic + iu; ++li) {
+      // periodic axes: the ghost layer holds copies of the opposite
+      // interior layer shifted by one period.
+      int ri = li, rj = lj, rk = lk;
+      double sh[3] = {0.0, 0.0, 0.0};
+      if (p.periodic[0]) {
+        if (li < istart1) { ri = iend1; sh[0] = -(p.domain_hi[0] - p.domain_lo[0]); }
+        else if (li > iend1) { ri = istart1; sh[0] = (p.domain_hi[0] - p.domain_lo[0]); }
+      }
+      if (p.periodic[1]) {
+        if (lj < jstart1) { rj = jend1; sh[1] = -(p.domain_hi[1] - p.domain_lo[1]); }
+        else if (lj > jend1) { rj = jstart1; sh[1] = (p.domain_hi[1] - p.domain_lo[1]); }
+      }
+      if (p.periodic[2] && !p.no_k) {
+        if (lk < kstart1) { rk = kend1; sh[2] = -(p.domain_hi[2] - p.domain_lo[2]); }
+        else if (lk > kend1) { rk = kstart1; sh[2] = (p.domain_hi[2] - p.domain_lo[2]); }
+      }
+      bool ghost = (sh[0] != 0.0 || sh[1] != 0.0 || sh[2] != 0.0);
+      int cell = funijk(ri, rj, rk) - 1;
+      for (int s = cell_start[cell]; s < cell_start[cell + 1]; ++s) {
+        int nb = cell_list[s];
+        if (nb == cur) continue;
+        if (nb < cur && state[nb] == DEM_STATE_NORMAL) continue;
+        if (state[nb] == DEM_STATE_NONEXISTENT) continue;
+        double srad = fr * (rad[cur] + rad[nb]);
+        double d[3];
+        for (int c = 0; c < 3; ++c) {
+          double pn = P(pos, nb, c);
+          if (ghost && sh[c] != 0.0) pn = pn + sh[c];
+          d[c] = cp[c] - pn;
+        }
+        double d2 = dot3(d, d);
+        if (d2 > srad * srad) continue;
+        if (out) out[cnt] = nb;
+        ++cnt;
+      }
+    }
+    return cnt;
+  }
+
+  bool is_rogue(int cur) const {
+    if (state[cur] != DEM_STATE_NORMAL) return false;
+    int lijk = dg_pijk[cur];
+    int lic = iof(lijk), ljc = jof(lijk), lkc = kof(lijk);
+    return (lic < istart1 || lic > iend1 || ljc < jstart1 || ljc > jend1 ||
+            lkc < kstart1 || lkc > kend1);
+  }
+
+  void neigh_build() {
+    int first_rogue = n;
+    for (int cur = 0; cur < n; ++cur) if (is_rogue(cur)) { first_rogue = cur; break; }
+    std::vector<int> cnt(n, 0);
+#pragma omp parallel for schedule(dynamic, 512) num_threads(nthreads) if (nthreads > 1)
     for (int cur = 0; cur < n; ++cur) {
-      row_end[cur] = (int)nbrs.size();
-      if (state[cur] != DEM_STATE_NORMAL) continue;
-      int lijk = dg_pijk[cur];
-      int lic = iof(lijk), ljc = jof(lijk), lkc = kof(lijk);
-      if (lic < istart1 || lic > iend1 || ljc < jstart1 || ljc > jend1 ||
-          lkc < kstart1 || lkc > kend1) {
-        do_exit = true;
-        if (p.remove_rogue) { delete_particle(cur); rogue_removed++; }
-        else err = "NORMAL particle found in GHOST cell";
-      }
-      if (do_exit) continue;
-      int il = 1, iu = 1, jl = 1, ju = 1, kl = 1, ku = 1;
-      double cp[3] = {P(pos, cur, 0), P(pos, cur, 1), P(pos, cur, 2)};
-      if (coarse_x) {
-        double t = (cp[0] - p.dg_xstart) * p.dg_dxinv;
-        double off = t - (double)(long long)std::floor(t);
-        if (off >= 0.5) il = 0; else iu = 0;
-      }
-      if (coarse_y) {
-        double t = (cp[1] - p.dg_ystart) * p.dg_dyinv;
-        double off = t - (double)(long long)std::floor(t);
-        if (off >= 0.5) jl = 0; else ju = 0;
-      }
-      if (p.no_k) { kl = 0; ku = 0; }
-      else if (coarse_z) {
-        double t = (cp[2] - p.dg_zstart) * p.dg_dzinv;
-        double off = t - (double)(long long)std::floor(t);
-        if (off >= 0.5) kl = 0; else ku = 0;
-      }
-      for (int lk = lkc - kl; lk <= lkc + ku; ++lk)
-      for (int lj = ljc - jl; lj <= ljc + ju; ++lj)
-      for (int li = lic - il; li <= lic + iu; ++li) {
-        // periodic axes: the ghost layer holds copies of the opposite
-        // interior layer shifted by one period.
-        int ri = li, rj = lj, rk = lk;
-        double sh[3] = {0.0, 0.0, 0.0};
-        if (p.periodic[0]) {
-          if (li < istart1) { ri = iend1; sh[0] = -(p.domain_hi[0] - p.domain_lo[0]); }
-          else if (li > iend1) { ri = istart1; sh[0] = (p.domain_hi[0] - p.domain_lo[0]); }
-        }
-        if (p.periodic[1]) {
-          if (lj < jstart1) { rj = jend1; sh[1] = -(p.domain_hi[1] - p.domain_lo[1]); }
-          else if (lj > jend1) { rj = jstart1; sh[1] = (p.domain_hi[1] - p.domain_lo[1]); }
-        }
-        if (p.periodic[2] && !p.no_k) {
-          if (lk < kstart1) { rk = kend1; sh[2] = -(p.domain_hi[2] - p.domain_lo[2]); }
-          else if (lk > kend1) { rk = kstart1; sh[2] = (p.domain_hi[2] - p.domain_lo[2]); }
-        }
-        bool ghost = (sh[0] != 0.0 || sh[1] != 0.0 || sh[2] != 0.0);
-        int cell = funijk(ri, rj, rk) - 1;
-        for (int s = cell_start[cell]; s < cell_start[cell + 1]; ++s) {
-          int nb = cell_list[s];
-          if (nb == cur) continue;
-          if (nb < cur && state[nb] == DEM_STATE_NORMAL) continue;
-          if (state[nb] == DEM_STATE_NONEXISTENT) continue;
-          double srad = fr * (rad[cur] + rad[nb]);
-          double d[3];
-          for (int c = 0; c < 3; ++c) {
-            double pn = P(pos, nb, c);
-            if (ghost && sh[c] != 0.0) pn = pn + sh[c];
-            d[c] = cp[c] - pn;
-          }
-          double d2 = dot3(d, d);
-          if (d2 > srad * srad) continue;
-          nbrs.push_back(nb);
-        }
-      }
-      row_end[cur] = (int)nbrs.size();
+      if (state[cur] != DEM_STATE_NORMAL || cur >= first_rogue) continue;
+      cnt[cur] = row_scan(cur, nullptr);
+    }
+    row_end.assign(n, 0);
+    long long tot = 0;
+    for (int cur = 0; cur < n; ++cur) { tot += cnt[cur]; row_end[cur] = (int)tot; }
+    nbrs.assign((size_t)tot, 0);
+#pragma omp parallel for schedule(dynamic, 512) num_threads(nthreads) if (nthreads > 1)
+    for (int cur = 0; cur < n; ++cur) {
+      if (!cnt[cur]) continue;
+      row_scan(cur, nbrs.data() + (cur ? row_end[cur - 1] : 0));
+    }
+    for (int cur = first_rogue; cur < n; ++cur) {
+      if (!is_rogue(cur)) continue;
+      if (p.remove_rogue) { delete_particle(cur); rogue_removed++; }
+      else err = "NORMAL particle found in GHOST cell";
     }
   }
 
@@ -289,6 +315,7 @@ struct Oracle {
     std::vector<double> old_pft = pft;
     neigh_build();
     pft.assign((size_t)3 * nbrs.size(), 0.0);
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads) if (nthreads > 1)
     for (int ll = 0; ll < n; ++ll) {
       int s = ll ? row_end[ll - 1] : 0, e = row_end[ll];
       int so = 0, eo = 0;
@@ -550,7 +577,7 @@ struct Oracle {
   // CALC_DEM_FORCE_WITH_WALL_STL (calc_collision_wall_mod.f:180-629) for one
   // particle, spheres only, static walls (CFRELVEL_WALL 806-847 with zero
   // wall velocity).
-  int wall_force_one(int ll) {
+  int wall_force_one(int ll, int64_t& nwc) {
     if (state[ll] != DEM_STATE_NORMAL) return 0;
     int cell = dg_pijk[ll] - 1;
     int fs = fbin_start[cell], fe = fbin_start[cell + 1];
@@ -608,7 +635,7 @@ struct Oracle {
       for (int c = 0; c < 3; ++c) fn[c] = -(kn_w * overlap_n * nrm[c] + etan_w * vrn * nrm[c]);
       double hist[3];
       int rc = get_collision(ll, nf_, hist);
-      if (rc) return fail(rc, "COLLISION_ARRAY_MAX too small");
+      if (rc) return rc;
       double ot[3];
       for (int c = 0; c < 3; ++c) ot[c] = p.dtsolid * vt[c] + hist[c];
       double mag = std::sqrt(dot3(ot, ot));
@@ -627,7 +654,7 @@ struct Oracle {
         ft[0] = ft[1] = ft[2] = 0.0;
       }
       update_collision(ll, nf_, ot);
-      n_wall_contacts++;
+      nwc++;
       for (int c = 0; c < 3; ++c) X(fc, c)[ll] = X(fc, c)[ll] + fn[c] + ft[c];
       double nxf[3]; cross3(nrm, ft, nxf);
       for (int c = 0; c < 3; ++c) X(tow, c)[ll] = X(tow, c)[ll] + distmod * nxf[c];
@@ -743,10 +770,17 @@ struct Oracle {
   // LL ascending, CC ascending, scattering into FC/TOW.
   int calc_force() {
     n_contacts = 0; n_wall_contacts = 0; max_overlap_ratio = 0.0;
+    int wrc = 0;
+    int64_t nwc = 0;
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads) if (nthreads > 1) reduction(+ : nwc)
     for (int ll = 0; ll < n; ++ll) {
-      int rc = wall_force_one(ll);
-      if (rc) return rc;
+      int64_t c0 = 0;
+      int rc = wall_force_one(ll, c0);
+      nwc += c0;
+      if (rc) wrc = rc;
     }
+    n_wall_contacts = nwc;
+    if (wrc) return fail(wrc, "COLLISION_ARRAY_MAX too small");
 #ifdef _OPENMP
     if (nthreads > 1) return calc_force_omp();
 #endif
@@ -840,14 +874,20 @@ struct Oracle {
     if (p.intg_method == DEM_INTG_EULER) {
       for (int c = 0; c < 3; ++c) {
         double* v = X(vel, c); double* x = X(pos, c); double* f = X(fc, c);
-        for (int l = 0; l < n; ++l) if (state[l] == DEM_STATE_NORMAL) v[l] = v[l] + dt * (f[l] / pmass[l] + p.grav[c]);
-        for (int l = 0; l < n; ++l) if (state[l] < DEM_STATE_NORMAL_GHOST) x[l] = x[l] + v[l] * dt;
-        for (int l = 0; l < n; ++l) f[l] = 0.0;
+#pragma omp parallel for schedule(static) num_threads(nthreads) if (nthreads > 1)
+        for (int l = 0; l < n; ++l) {
+          if (state[l] == DEM_STATE_NORMAL) v[l] = v[l] + dt * (f[l] / pmass[l] + p.grav[c]);
+          if (state[l] < DEM_STATE_NORMAL_GHOST) x[l] = x[l] + v[l] * dt;
+          f[l] = 0.0;
+        }
       }
       for (int c = 0; c < 3; ++c) {
         double* w = X(omg, c); double* t = X(tow, c);
-        for (int l = 0; l < n; ++l) if (state[l] == DEM_STATE_NORMAL) w[l] = w[l] + t[l] * omoi[l] * dt;
-        for (int l = 0; l < n; ++l) t[l] = 0.0;
+#pragma omp parallel for schedule(static) num_threads(nthreads) if (nthreads > 1)
+        for (int l = 0; l < n; ++l) {
+          if (state[l] == DEM_STATE_NORMAL) w[l] = w[l] + t[l] * omoi[l] * dt;
+          t[l] = 0.0;
+        }
       }
     } else {
       for (int c = 0; c < 3; ++c) {
