@@ -47,15 +47,17 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=125_000, help="particles in the CPU sample")
     ap.add_argument("--cpu-steps", type=int, default=25)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--inflate", type=float, default=1.0,
+                    help="grow every sphere by this factor after placement (contact-dense variant)")
     return ap.parse_args()
 
 
-def workload(n, precision):
+def workload(n, precision, inflate=1.0):
     from mfix_dem import abi, configs
     prec = abi.DEM_PREC_SPLIT if precision == "split" else abi.DEM_PREC_FP64
     scale = (n / 1_000_000) ** 0.5
     box = (0.1 * scale, 0.4, 0.1 * scale)
-    return configs.hertz_rsa(n=n, box=box, precision=prec, cache_dir=CACHE)
+    return configs.hertz_rsa(n=n, box=box, precision=prec, cache_dir=CACHE, inflate=inflate)
 
 
 def dist_env():
@@ -198,7 +200,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from mfix_dem import GpuSystem
-    case, prm, arr, walls, info = workload(args.n, args.precision)
+    case, prm, arr, walls, info = workload(args.n, args.precision, args.inflate)
     n = arr["pos"].shape[1]
     stream = torch.cuda.Stream()
     g = GpuSystem(prm, n)
@@ -318,7 +320,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": "hertz_rsa_1m", "n_particles": n_normal, "n_pairs": int(p1),
+            "config": {"workload": "hertz_rsa_1m" if args.inflate == 1.0 else f"hertz_rsa_1m_inflated_{args.inflate:g}",
+                       "n_particles": n_normal, "n_pairs": int(p1),
                        "pairs_per_particle": p1 / max(n_normal, 1), "precision": args.precision,
                        "contact": "hertz", "integrator": "euler", "periodic": "xz",
                        "neighbor_search_n": int(prm.neighbor_search_n),

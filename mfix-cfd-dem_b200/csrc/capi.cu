@@ -197,6 +197,26 @@ static void fill_devparams(dem_handle* h) {
     p.etanw[k] = q.des_etan_wall[k]; p.etatw[k] = q.des_etat_wall[k];
     p.hkwn[k] = q.hert_kwn[k]; p.hkwt[k] = q.hert_kwt[k];
   }
+  // Search grid for the pair build: cells no narrower than the largest
+  // search diameter 2*FACTOR_RLM*MAX_RADIUS (with a 1 % margin), so a 27-cell
+  // stencil holds every candidate.  An axis keeps the DES grid's division
+  // when that is not coarser, when the DES grid is coarse there, or when a
+  // periodic axis would get fewer than 3 cells.
+  const int dgn[3] = {q.dg_imax, q.dg_jmax, q.no_k ? 1 : q.dg_kmax};
+  const double target = 2.0 * q.factor_rlm * q.max_radius * 1.01;
+  for (int a = 0; a < 3; ++a) {
+    const double len = (double)dgn[a] / p.dg_inv[a];
+    int nfa = (int)std::floor(len / target);
+    const bool coarse = 1.0 > 2.0 * q.max_radius * q.factor_rlm * p.dg_inv[a];
+    if (nfa <= dgn[a] || coarse || (p.per[a] && nfa < 3) || (a == 2 && q.no_k)) nfa = dgn[a];
+    if (nfa < 1) nfa = 1;
+    p.fn[a] = nfa;
+    // same division as the DES grid -> the same inverse width, bit for bit
+    p.f_inv[a] = nfa == dgn[a] ? p.dg_inv[a] : (double)nfa / len;
+  }
+  p.fc1 = p.fn[1] + 2;
+  p.fc2 = p.fc1 * (p.fn[0] + 2);
+  p.nfcell = p.fc2 * (q.no_k ? 1 : p.fn[2] + 2);
 }
 
 #define API_GUARD(h) do { if (!(h)) return DEM_ERR_ARG; cudaSetDevice((h)->dev); } while (0)
@@ -247,6 +267,10 @@ int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
   A((void**)&h->cell_start, sizeof(int) * (nc + 1));
   A((void**)&h->cell_fill, sizeof(int) * (nc + 1));
   A((void**)&h->cell_list, sizeof(int) * n);
+  A((void**)&h->fcell_key, sizeof(int) * n);
+  A((void**)&h->fcell_cnt, sizeof(int) * (h->dp.nfcell + 1));
+  A((void**)&h->fcell_start, sizeof(int) * (h->dp.nfcell + 1));
+  A((void**)&h->fcell_list, sizeof(int) * n);
   A((void**)&h->row_cnt, sizeof(int) * n);
   A((void**)&h->in_cnt, sizeof(int) * n);
   A((void**)&h->in_start, sizeof(int) * (n + 1));
@@ -254,6 +278,8 @@ int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
   A((void**)&h->fbin_start, sizeof(int) * (nc + 1));
   A((void**)&h->wall_fid, sizeof(int) * cmax * n);
   A((void**)&h->wall_pft, sizeof(double) * 3 * cmax * n);
+  A((void**)&h->wall_live, n);
+  A((void**)&h->wf, sizeof(double) * 6 * n);
   A((void**)&h->derr, sizeof(DevErr));
   if (!ok) {
     dem_destroy(h);
@@ -280,7 +306,8 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage};
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec,
+                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (auto e : h->ev_pool) cudaEventDestroy(e);

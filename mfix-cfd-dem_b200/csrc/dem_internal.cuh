@@ -65,6 +65,18 @@ struct DevParams {
   double lo[3], hi[3], L[3];
   double etan[MAXP * MAXP], etat[MAXP * MAXP], hkn[MAXP * MAXP], hkt[MAXP * MAXP];
   double etanw[MAXP], etatw[MAXP], hkwn[MAXP], hkwt[MAXP];
+  // search grid of the pair build: fn[a] interior cells of width 1/f_inv[a]
+  // over the DES-grid interior, plus one ghost layer on each side
+  int fn[3], fc1, fc2, nfcell;
+  double f_inv[3];
+};
+
+// What the two particles of a contact pair need to add the pair's terms to
+// FC/TOW in the reference's order: FC_TMP, CROSS(NORMAL, FT) with the two
+// lever arms (the torques are DIST_CL*TOW_force and DIST_CI*TOW_force), and
+// KN_DES and OVERLAP_N for the rolling-friction torque.  80 bytes.
+struct PairRec {
+  double fc[3], tf[3], dcl2, dci2, kn, ov;
 };
 
 struct FacetBinEntry {  // one entry of facets_at_dg(cell)
@@ -114,6 +126,10 @@ struct dem_handle {
   int* cell_start = nullptr;  // ncell2+1
   int* cell_fill = nullptr;   // ncell2
   int* cell_list = nullptr;   // n
+  int* fcell_key = nullptr;   // n: search-grid cell of each particle (0-based)
+  int* fcell_cnt = nullptr;   // nfcell+1
+  int* fcell_start = nullptr; // nfcell+1
+  int* fcell_list = nullptr;  // n
 
   // pairs
   long long pair_cap = 0;
@@ -127,6 +143,8 @@ struct dem_handle {
   int* in_fill = nullptr;     // n
   int2* in_pair = nullptr;    // cap
   int* pair_owner = nullptr;  // cap
+  uint8_t* pflag = nullptr;   // cap: 1 = pair in contact at the last force pass
+  demb::PairRec* prec = nullptr; // cap: contact terms of the last force pass
   int rb = 0;                 // which row_end/nbrs buffer is current
 
   // walls
@@ -139,6 +157,8 @@ struct dem_handle {
   int n_fbin = 0;
   int* wall_fid = nullptr;    // [i][cmax]
   double* wall_pft = nullptr; // [i][cmax][3]
+  uint8_t* wall_live = nullptr; // [i] 1 when some wall slot may be in use
+  double* wf = nullptr;       // [i][6] wall force and torque of the last force pass
 
   // scan scratch
   int* scan_tmp = nullptr;

@@ -3,11 +3,10 @@
 // Replaces DESGRID_PIC(.TRUE.) (model/des/desgrid_mod.f:877-995) with the
 // cell functions IofPOS/JofPOS/KofPOS (391-419) and DG_FUNIJK (184-188):
 //   dg_pijk = dg_funijk(clamp(iofpos(x)), clamp(jofpos(y)), clamp(kofpos(z)))
-// followed by a counting sort of particle indices into per-cell lists whose
-// order is ascending particle index, the order of the serial reference.
-// The sort is: count (atomics) -> exclusive scan -> scatter (atomics) ->
-// per-cell rank sort (one warp per cell, shared memory), so the result does
-// not depend on the order in which atomics were served.
+// On neighbour-search steps the particles are also binned (count -> scan
+// -> scatter) to the finer search grid of the pair build; the order inside a
+// search cell does not matter there because every row is put into the
+// reference's stencil order when it is filled.
 //
 // For periodic axes the same pass wraps particles that crossed a periodic
 // face by one period, which is what the serial self-exchange of
@@ -49,65 +48,51 @@ __global__ void k_cell_keys(DevParams p, double4* __restrict__ pos4, const int8_
   if (cell_cnt) atomicAdd(&cell_cnt[c - 1], 1);
 }
 
-__global__ void k_cell_scatter(int n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
-                               const int* __restrict__ cell_start, int* __restrict__ cell_fill,
-                               int* __restrict__ cell_list) {
+// Search-grid cell of every existing particle (for the pair build).
+__global__ void k_fine_keys(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict__ state,
+                            int* __restrict__ fkey, int* __restrict__ fcnt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n || state[i] == DEM_STATE_NONEXISTENT) return;
+  const double4 x = pos4[i];
+  const double xx[3] = {x.x, x.y, x.z};
+  int g[3] = {0, 0, 0};
+  for (int a = 0; a < 3; ++a) {
+    if (a == 2 && p.no_k) break;
+    int v = (int)floor((xx[a] - p.dg_start[a]) * p.f_inv[a]) + 1;
+    const int lo = p.per[a] ? 1 : 0, hi = p.per[a] ? p.fn[a] : p.fn[a] + 1;
+    g[a] = min(hi, max(lo, v));
+  }
+  const int key = g[2] * p.fc2 + g[0] * p.fc1 + g[1];
+  fkey[i] = key;
+  atomicAdd(&fcnt[key], 1);
+}
+
+__global__ void k_fine_scatter(int n, const int8_t* __restrict__ state, const int* __restrict__ fkey,
+                               const int* __restrict__ fstart, int* __restrict__ ffill, int* __restrict__ flist) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || state[i] == DEM_STATE_NONEXISTENT) return;
-  int c = dg_pijk[i] - 1;
-  int slot = atomicAdd(&cell_fill[c], 1);
-  cell_list[cell_start[c] + slot] = i;
+  const int c = fkey[i];
+  const int slot = atomicAdd(&ffill[c], 1);
+  flist[fstart[c] + slot] = i;
 }
 
-constexpr int SORT_WARPS = 4;
-constexpr int SORT_CAP = 1024;  // particles per cell sorted in shared memory
-
-// One warp per cell: each lane ranks its elements by counting smaller ones
-// (indices are distinct), then writes them to their sorted slot.
-__global__ void k_cell_sort(int ncell, const int* __restrict__ cell_start, int* __restrict__ cell_list) {
-  __shared__ int buf[SORT_WARPS][SORT_CAP];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = blockIdx.x * SORT_WARPS + w;
-  if (c >= ncell) return;
-  const int s = cell_start[c], e = cell_start[c + 1];
-  const int k = e - s;
-  if (k <= 1) return;
-  if (k <= SORT_CAP) {
-    for (int t = lane; t < k; t += 32) buf[w][t] = cell_list[s + t];
-    __syncwarp();
-    for (int t = lane; t < k; t += 32) {
-      int v = buf[w][t], r = 0;
-      for (int u = 0; u < k; ++u) r += (buf[w][u] < v);
-      cell_list[s + r] = v;
-    }
-  } else if (lane == 0) {
-    // rare overfull cell: insertion sort in global memory
-    for (int a = s + 1; a < e; ++a) {
-      int v = cell_list[a], b = a - 1;
-      while (b >= s && cell_list[b] > v) { cell_list[b + 1] = cell_list[b]; --b; }
-      cell_list[b + 1] = v;
-    }
-  }
-}
-
-int run_desgrid_pic(dem_handle* h, bool sort_cells) {
+// DESGRID_PIC: cell of every particle (and the periodic wrap).  When
+// `bin_search` is set (neighbour-search steps) the particles are also binned
+// to the search grid of the pair build.
+int run_desgrid_pic(dem_handle* h, bool bin_search) {
   ProfScope ps(h, DEM_PROF_DESGRID);
   const DevParams& p = h->dp;
   const int n = h->n, T = 256, B = (n + T - 1) / T;
   const bool anyper = p.per[0] || p.per[1] || (p.per[2] && !p.no_k);
-  if (sort_cells) {
-    if (int rc = check_cuda(h, cudaMemsetAsync(h->cell_cnt, 0, sizeof(int) * p.ncell2, h->stream), "memset")) return rc;
-  }
-  k_cell_keys<<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk,
-                                      sort_cells ? h->cell_cnt : nullptr, anyper ? 1 : 0);
+  k_cell_keys<<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, nullptr, anyper ? 1 : 0);
   DEM_LAUNCH(h);
-  if (!sort_cells) return check_cuda(h, cudaGetLastError(), "k_cell_keys");
-  if (int rc = exclusive_scan(h, h->cell_cnt, h->cell_start, p.ncell2, h->cell_start + p.ncell2)) return rc;
-  if (int rc = check_cuda(h, cudaMemsetAsync(h->cell_fill, 0, sizeof(int) * p.ncell2, h->stream), "memset")) return rc;
-  k_cell_scatter<<<B, T, 0, h->stream>>>(n, h->state, h->dg_pijk, h->cell_start, h->cell_fill, h->cell_list);
+  if (!bin_search) return check_cuda(h, cudaGetLastError(), "k_cell_keys");
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * p.nfcell, h->stream), "memset")) return rc;
+  k_fine_keys<<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->fcell_key, h->fcell_cnt);
   DEM_LAUNCH(h);
-  k_cell_sort<<<(p.ncell2 + SORT_WARPS - 1) / SORT_WARPS, 32 * SORT_WARPS, 0, h->stream>>>(
-      p.ncell2, h->cell_start, h->cell_list);
+  if (int rc = exclusive_scan(h, h->fcell_cnt, h->fcell_start, p.nfcell, h->fcell_start + p.nfcell)) return rc;
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * p.nfcell, h->stream), "memset")) return rc;
+  k_fine_scatter<<<B, T, 0, h->stream>>>(n, h->state, h->fcell_key, h->fcell_start, h->fcell_cnt, h->fcell_list);
   DEM_LAUNCH(h);
   return check_cuda(h, cudaGetLastError(), "desgrid_pic");
 }

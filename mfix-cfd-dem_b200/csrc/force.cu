@@ -24,11 +24,6 @@
 
 namespace demb {
 
-struct PairRes {
-  double fc[3], tl[3], ti[3], rl[3], ri[3];
-  bool contact, roll_l, roll_i, zero;
-};
-
 struct PState {  // one particle's gathered state
   double x[3], v[3], w[3];
   double r, m;
@@ -45,28 +40,16 @@ __device__ __forceinline__ void load_p(const double4* __restrict__ pos4, const d
   s.ph = phase[i];
 }
 
-// One CC iteration of CALC_FORCE_DEM for owner L and neighbour I.
+// Contact part of one CC iteration of CALC_FORCE_DEM (calc_force_dem.f:
+// 273-363) with CFRELVEL (cfrelvel.f:54-77) for owner L and neighbour I in
+// contact; dist = x_I - x_L and d2 = |dist|^2 come from the apart test.
 template <int COLL>
-__device__ __forceinline__ void pair_force(const DevParams& p, const PState& L, const PState& I,
-                                           const double pin[3], double pout[3], PairRes& o) {
-  o.contact = false; o.roll_l = false; o.roll_i = false; o.zero = false;
+__device__ __forceinline__ void contact_force(const DevParams& p, const PState& L, const PState& I,
+                                              const double dist[3], double d2, const double pin[3],
+                                              double pout[3], PairRec& o) {
   const double rl = L.r, ri = I.r;
   const double r_lm = rl + ri;
-  double dist[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    double pj = I.x[c];
-    double s = periodic_shift(p, c, pj - L.x[c]);
-    if (s != 0.0) pj = pj + s;
-    dist[c] = pj - L.x[c];
-  }
-  double dmag = dot3(dist, dist);
-  if (dmag > (r_lm - SMALL_NUMBER) * (r_lm - SMALL_NUMBER)) {
-    pout[0] = pout[1] = pout[2] = 0.0;
-    return;
-  }
-  if (dmag == 0.0) { o.zero = true; pout[0] = pin[0]; pout[1] = pin[1]; pout[2] = pin[2]; return; }
-  dmag = sqrt(dmag);
+  const double dmag = sqrt(d2);
   double nrm[3] = {dist[0] / dmag, dist[1] / dmag, dist[2] / dmag};
   const double overlap_n = r_lm - dmag;
   // CFRELVEL
@@ -128,29 +111,13 @@ __device__ __forceinline__ void pair_force(const DevParams& p, const PState& L, 
     ft[0] = ft[1] = ft[2] = 0.0;
   }
   pout[0] = ot[0]; pout[1] = ot[1]; pout[2] = ot[2];
-  const double dcl2 = dmag / 2.0 + (rl * rl - ri * ri) / (2.0 * dmag);
-  const double dci2 = dmag - dcl2;
-  double tf[3];
-  cross3(nrm, ft, tf);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) { o.tl[c] = dcl2 * tf[c]; o.ti[c] = dci2 * tf[c]; }
+  o.dcl2 = dmag / 2.0 + (rl * rl - ri * ri) / (2.0 * dmag);
+  o.dci2 = dmag - o.dcl2;
+  cross3(nrm, ft, o.tf);
 #pragma unroll
   for (int c = 0; c < 3; ++c) o.fc[c] = 0.0 + fn[c] + ft[c];
-  if (p.mew_r > 0.0) {
-    double om = sqrt(dot3(L.w, L.w));
-    if (om > 0.0) {
-      o.roll_l = true;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) o.rl[c] = -(p.mew_r * (2.0 * rl) * kn * overlap_n * L.w[c] / om);
-    }
-    om = sqrt(dot3(I.w, I.w));
-    if (om > 0.0) {
-      o.roll_i = true;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) o.ri[c] = -(p.mew_r * (2.0 * ri) * kn * overlap_n * I.w[c] / om);
-    }
-  }
-  o.contact = true;
+  o.kn = kn;
+  o.ov = overlap_n;
 }
 
 // ---------------------------------------------------------------------------
@@ -359,145 +326,233 @@ __device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, cons
 }
 
 // ---------------------------------------------------------------------------
-// MODE 0: forces into FC/TOW.  MODE 1: fused Euler.  MODE 2: fused AB2.
-template <int COLL, int MODE>
+// Kernel 1 (per particle): wall contacts of NORMAL particles whose DES cell
+// holds facets.  Writes the particle's wall force and torque, which are the
+// first terms of FC/TOW in the reference's order (CALC_DEM_FORCE_WITH_WALL_STL
+// runs before the pair loop, calc_force_dem.f:113).
+template <int COLL>
 __global__ void __launch_bounds__(128)
-k_force(DevParams p, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
-        const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
-        double4* __restrict__ omg_n, const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
-        const int* __restrict__ row_end, const int* __restrict__ nbrs, const int* __restrict__ in_start,
-        const int2* __restrict__ in_pair, const double* __restrict__ pft_in, double* __restrict__ pft_out,
-        WallCtx w, double* __restrict__ fc, double* __restrict__ tow, double* __restrict__ acc_old,
-        double* __restrict__ rot_acc_old, DevErr* __restrict__ err) {
+k_walls(DevParams p, WallCtx w, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+        const double4* __restrict__ omg4, const uint8_t* __restrict__ phase, const int8_t* __restrict__ state,
+        uint8_t* __restrict__ wall_live, double* __restrict__ wf, DevErr* __restrict__ err) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long ncont = 0, nwc = 0;
+  unsigned long long nwc = 0;
   unsigned eflags = 0;
-  if (me < p.n) {
-    const int8_t st = state[me];
-    PState S;
-    load_p(pos_c, vel_c, omg_c, phase, me, S);
-    double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
-    if (st == DEM_STATE_NORMAL && w.nf > 0) wall_contacts<COLL>(p, w, me, S, f, t, nwc, eflags);
-    const int rs = me ? row_end[me - 1] : 0, re = row_end[me];
-    const int is = in_start[me], ie = in_start[me + 1];
-    if (st != DEM_STATE_NONEXISTENT) {
-      // pairs owned by lower-index particles, then own row, then the rest
-      int q = is;
-      for (int pass = 0; pass < 2; ++pass) {
-        for (; q < ie; ++q) {
-          const int2 e = in_pair[q];
-          if (pass == 0 && e.x > me) break;
-          if (state[e.x] == DEM_STATE_NONEXISTENT) continue;
-          PState L;
-          load_p(pos_c, vel_c, omg_c, phase, e.x, L);
-          const double* pi = pft_in + 3 * (size_t)e.y;
-          double pin[3] = {pi[0], pi[1], pi[2]}, pout[3];
-          PairRes o;
-          pair_force<COLL>(p, L, S, pin, pout, o);
-          if (!o.contact) continue;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) f[c] = f[c] - o.fc[c];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) t[c] = t[c] + o.ti[c];
-          if (o.roll_i) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) t[c] = t[c] + o.ri[c];
-          }
-        }
-        if (pass == 0) {
-          for (int cc = rs; cc < re; ++cc) {
-            const int i = nbrs[cc];
-            const double* pi = pft_in + 3 * (size_t)cc;
-            double pin[3] = {pi[0], pi[1], pi[2]};
-            double* po = pft_out + 3 * (size_t)cc;
-            if (state[i] == DEM_STATE_NONEXISTENT) { po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2]; continue; }
-            PState I;
-            load_p(pos_c, vel_c, omg_c, phase, i, I);
-            double pout[3];
-            PairRes o;
-            pair_force<COLL>(p, S, I, pin, pout, o);
-            po[0] = pout[0]; po[1] = pout[1]; po[2] = pout[2];
-            if (o.zero) {
-              eflags |= EF_ZERO_DIST;
-              err->zero_a = me; err->zero_b = i;
-            }
-            if (!o.contact) continue;
-            ++ncont;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) f[c] = f[c] + o.fc[c];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) t[c] = t[c] + o.tl[c];
-            if (o.roll_l) {
-#pragma unroll
-              for (int c = 0; c < 3; ++c) t[c] = t[c] + o.rl[c];
-            }
-          }
-        }
+  if (me < p.n && state[me] == DEM_STATE_NORMAL) {
+    const int cell = w.dg_pijk[me] - 1;
+    if (w.fbin_start[cell + 1] - w.fbin_start[cell] < 1) {
+      // no facet near: clear the history once (calc_collision_wall_mod.f:194-198)
+      if (wall_live[me]) {
+        int* fid = w.wall_fid + (size_t)me * p.cmax;
+        double* wp = w.wall_pft + (size_t)me * p.cmax * 3;
+        for (int q = 0; q < p.cmax; ++q) fid[q] = -1;
+        for (int q = 0; q < 3 * p.cmax; ++q) wp[q] = 0.0;
+        wall_live[me] = 0;
       }
     } else {
-      for (int cc = rs; cc < re; ++cc) {
-        const double* pi = pft_in + 3 * (size_t)cc;
-        double* po = pft_out + 3 * (size_t)cc;
-        po[0] = pi[0]; po[1] = pi[1]; po[2] = pi[2];
-      }
-    }
-
-    const size_t n = (size_t)p.n;
-    if (MODE == 0) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) { fc[c * n + me] = f[c]; tow[c * n + me] = t[c]; }
-    } else {
-      const double dt = p.dt;
-      const double omoi = omg_c[me].w;
-      double xn[3], vn[3], wn[3];
-      if (MODE == 1) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          vn[c] = S.v[c];
-          if (st == DEM_STATE_NORMAL) vn[c] = S.v[c] + dt * (f[c] / S.m + p.grav[c]);
-          xn[c] = S.x[c];
-          if (st < DEM_STATE_NORMAL_GHOST) xn[c] = S.x[c] + vn[c] * dt;
-          wn[c] = S.w[c];
-          if (st == DEM_STATE_NORMAL) wn[c] = S.w[c] + t[c] * omoi * dt;
-        }
-      } else {
-        const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
-                             st == DEM_STATE_NORMAL_GHOST || st == 110);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
-          if (p.first_pass && fp_ok) { ao = f[c] / S.m + p.grav[c]; ro = t[c]; }
-          double a = f[c];
-          if (st == DEM_STATE_NORMAL) a = f[c] / S.m + p.grav[c];
-          vn[c] = S.v[c];
-          if (st == DEM_STATE_NORMAL) vn[c] = S.v[c] + 0.5 * (3.0 * a - ao) * dt;
-          acc_old[c * n + me] = a;
-          xn[c] = S.x[c];
-          if (st < DEM_STATE_NORMAL_GHOST) xn[c] = S.x[c] + 0.5 * (S.v[c] + vn[c]) * dt;
-          wn[c] = S.w[c];
-          if (st == DEM_STATE_NORMAL) {
-            wn[c] = S.w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
-            ro = t[c] * omoi;
-          }
-          rot_acc_old[c * n + me] = ro;
-        }
-      }
-      pos_n[me] = make_double4(xn[0], xn[1], xn[2], S.r);
-      vel_n[me] = make_double4(vn[0], vn[1], vn[2], S.m);
-      omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+      PState S;
+      load_p(pos4, vel4, omg4, phase, me, S);
+      double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+      wall_contacts<COLL>(p, w, me, S, f, t, nwc, eflags);
+      wall_live[me] = 1;
+      double* o = wf + 6 * (size_t)me;
+      o[0] = f[0]; o[1] = f[1]; o[2] = f[2]; o[3] = t[0]; o[4] = t[1]; o[5] = t[2];
     }
   }
-  // warp-aggregated counters
   for (int o = 16; o > 0; o >>= 1) {
-    ncont += __shfl_down_sync(0xffffffffu, ncont, o);
     nwc += __shfl_down_sync(0xffffffffu, nwc, o);
     eflags |= __shfl_down_sync(0xffffffffu, eflags, o);
   }
   if ((threadIdx.x & 31) == 0) {
-    if (ncont) atomicAdd(&err->n_contacts, ncont);
     if (nwc) atomicAdd(&err->n_wall_contacts, nwc);
     if (eflags) atomicOr(&err->flags, eflags);
   }
+}
+
+// Kernel 2 (per pair): one CC iteration of CALC_FORCE_DEM, evaluated once
+// per pair.  The apart test needs only the two positions; velocities, spins
+// and masses are gathered only for pairs in contact.  PFT_out is written for
+// every pair; the contact terms go to a compact record that both particles
+// read back in kernel 3.
+template <int COLL>
+__global__ void __launch_bounds__(256)
+k_pairs(DevParams p, long long np, const int* __restrict__ owner, const int* __restrict__ nbrs,
+        const double4* __restrict__ pos4, const double4* __restrict__ vel4, const double4* __restrict__ omg4,
+        const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
+        const double* __restrict__ pft_in, double* __restrict__ pft_out,
+        uint8_t* __restrict__ pflag, PairRec* __restrict__ prec, DevErr* __restrict__ err) {
+  const long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long ncont = 0;
+  unsigned eflags = 0;
+  if (cc < np) {
+    const int ll = owner[cc], i = nbrs[cc];
+    const double* pi = pft_in + 3 * cc;
+    double pin[3] = {pi[0], pi[1], pi[2]};
+    double* po = pft_out + 3 * cc;
+    uint8_t flag = 0;
+    if (state[i] == DEM_STATE_NONEXISTENT || state[ll] == DEM_STATE_NONEXISTENT) {
+      po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2];
+    } else {
+      PState L, I;
+      const double4 a = pos4[ll], b = pos4[i];
+      L.x[0] = a.x; L.x[1] = a.y; L.x[2] = a.z; L.r = a.w;
+      I.x[0] = b.x; I.x[1] = b.y; I.x[2] = b.z; I.r = b.w;
+      const double r_lm = L.r + I.r;
+      double dist[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double pj = I.x[c];
+        double s = periodic_shift(p, c, pj - L.x[c]);
+        if (s != 0.0) pj = pj + s;
+        dist[c] = pj - L.x[c];
+      }
+      const double d2 = dot3(dist, dist);
+      if (d2 > (r_lm - SMALL_NUMBER) * (r_lm - SMALL_NUMBER)) {
+        po[0] = po[1] = po[2] = 0.0;
+      } else if (d2 == 0.0) {
+        po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2];
+        eflags |= EF_ZERO_DIST;
+        err->zero_a = ll; err->zero_b = i;
+      } else {
+        const double4 va = vel4[ll], vb = vel4[i], wa = omg4[ll], wb = omg4[i];
+        L.v[0] = va.x; L.v[1] = va.y; L.v[2] = va.z; L.m = va.w;
+        I.v[0] = vb.x; I.v[1] = vb.y; I.v[2] = vb.z; I.m = vb.w;
+        L.w[0] = wa.x; L.w[1] = wa.y; L.w[2] = wa.z;
+        I.w[0] = wb.x; I.w[1] = wb.y; I.w[2] = wb.z;
+        L.ph = phase[ll]; I.ph = phase[i];
+        double pout[3];
+        PairRec r;
+        contact_force<COLL>(p, L, I, dist, d2, pin, pout, r);
+        po[0] = pout[0]; po[1] = pout[1]; po[2] = pout[2];
+        prec[cc] = r;
+        flag = 1;
+        ++ncont;
+      }
+    }
+    pflag[cc] = flag;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ncont += __shfl_down_sync(0xffffffffu, ncont, o);
+    eflags |= __shfl_down_sync(0xffffffffu, eflags, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (ncont) atomicAdd(&err->n_contacts, ncont);
+    if (eflags) atomicOr(&err->flags, eflags);
+  }
+}
+
+// Rolling-friction torque of one particle in a pair (calc_force_dem.f:491-506):
+// -MEW_R*(2*R)*KN_DES*OVERLAP_N*OMEGA/|OMEGA|, evaluated left to right.
+__device__ __forceinline__ void add_rolling(const DevParams& p, double r, const double w[3], double om,
+                                            const PairRec& q, double t[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) t[c] = t[c] + -(p.mew_r * (2.0 * r) * q.kn * q.ov * w[c] / om);
+}
+
+// Kernel 3 (per particle): sums FC/TOW in the serial reference's order --
+// wall terms, pairs owned by lower-index particles (ascending owner), the
+// particle's own row, pairs owned by higher-index particles -- and either
+// stores them (MODE 0) or integrates them in place of CFNEWVALUES
+// (MODE 1 = Euler, MODE 2 = Adams-Bashforth).
+template <int MODE>
+__global__ void __launch_bounds__(256)
+k_gather(DevParams p, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
+         const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
+         double4* __restrict__ omg_n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
+         const int* __restrict__ fbin_start, int nf, const double* __restrict__ wf,
+         const int* __restrict__ row_end, const int* __restrict__ in_start, const int2* __restrict__ in_pair,
+         const uint8_t* __restrict__ pflag, const PairRec* __restrict__ prec,
+         double* __restrict__ fc, double* __restrict__ tow, double* __restrict__ acc_old,
+         double* __restrict__ rot_acc_old) {
+  const int me = blockIdx.x * blockDim.x + threadIdx.x;
+  if (me >= p.n) return;
+  const int8_t st = state[me];
+  const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
+  const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
+  const double r = X.w, m = V.w, omoi = W.w;
+  double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+  if (st == DEM_STATE_NORMAL && nf > 0) {
+    const int cell = dg_pijk[me] - 1;
+    if (fbin_start[cell + 1] > fbin_start[cell]) {
+      const double* o = wf + 6 * (size_t)me;
+      f[0] = o[0]; f[1] = o[1]; f[2] = o[2]; t[0] = o[3]; t[1] = o[4]; t[2] = o[5];
+    }
+  }
+  if (st != DEM_STATE_NONEXISTENT) {
+    const bool roll = p.mew_r > 0.0;
+    double om = 0.0;
+    if (roll) om = sqrt(dot3(w, w));
+    const int rs = me ? row_end[me - 1] : 0, re = row_end[me];
+    const int is = in_start[me], ie = in_start[me + 1];
+    int q = is;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (; q < ie; ++q) {
+        const int2 e = in_pair[q];
+        if (pass == 0 && e.x > me) break;
+        if (!pflag[e.y]) continue;
+        const PairRec o = prec[e.y];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) f[c] = f[c] - o.fc[c];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) t[c] = t[c] + o.dci2 * o.tf[c];
+        if (roll && om > 0.0) add_rolling(p, r, w, om, o, t);
+      }
+      if (pass == 0) {
+        for (int cc = rs; cc < re; ++cc) {
+          if (!pflag[cc]) continue;
+          const PairRec o = prec[cc];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) f[c] = f[c] + o.fc[c];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) t[c] = t[c] + o.dcl2 * o.tf[c];
+          if (roll && om > 0.0) add_rolling(p, r, w, om, o, t);
+        }
+      }
+    }
+  }
+  const size_t n = (size_t)p.n;
+  if (MODE == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { fc[c * n + me] = f[c]; tow[c * n + me] = t[c]; }
+    return;
+  }
+  const double dt = p.dt;
+  double xn[3], vn[3], wn[3];
+  if (MODE == 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      vn[c] = v[c];
+      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + dt * (f[c] / m + p.grav[c]);
+      xn[c] = x[c];
+      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + vn[c] * dt;
+      wn[c] = w[c];
+      if (st == DEM_STATE_NORMAL) wn[c] = w[c] + t[c] * omoi * dt;
+    }
+  } else {
+    const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
+                         st == DEM_STATE_NORMAL_GHOST || st == 110);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
+      if (p.first_pass && fp_ok) { ao = f[c] / m + p.grav[c]; ro = t[c]; }
+      double a = f[c];
+      if (st == DEM_STATE_NORMAL) a = f[c] / m + p.grav[c];
+      vn[c] = v[c];
+      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + 0.5 * (3.0 * a - ao) * dt;
+      acc_old[c * n + me] = a;
+      xn[c] = x[c];
+      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + 0.5 * (v[c] + vn[c]) * dt;
+      wn[c] = w[c];
+      if (st == DEM_STATE_NORMAL) {
+        wn[c] = w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
+        ro = t[c] * omoi;
+      }
+      rot_acc_old[c * n + me] = ro;
+    }
+  }
+  pos_n[me] = make_double4(xn[0], xn[1], xn[2], r);
+  vel_n[me] = make_double4(vn[0], vn[1], vn[2], m);
+  omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
 }
 
 // CFUPDATEOLD + CFNEWVALUES from FC/TOW, in place; zeroes FC/TOW.
@@ -559,31 +614,45 @@ static WallCtx wall_ctx(dem_handle* h) {
   return w;
 }
 
-template <int COLL, int MODE>
-static void launch_force(dem_handle* h, int nb) {
-  const int T = 128, B = (h->n + T - 1) / T;
+template <int COLL>
+static void launch_walls_pairs(dem_handle* h) {
   const int c = h->cur, pc = h->pcur;
-  k_force<COLL, MODE><<<B, T, 0, h->stream>>>(
-      h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
-      h->state, h->phase, h->row_end[h->rb], h->nbrs[h->rb], h->in_start, h->in_pair,
-      h->pft[pc], h->pft[1 - pc], wall_ctx(h), h->fc, h->tow, h->acc_old, h->rot_acc_old, h->derr);
+  if (h->nf > 0) {
+    const int T = 128, B = (h->n + T - 1) / T;
+    k_walls<COLL><<<B, T, 0, h->stream>>>(h->dp, wall_ctx(h), h->pos4[c], h->vel4[c], h->omg4[c], h->phase,
+                                          h->state, h->wall_live, h->wf, h->derr);
+    DEM_LAUNCH(h);
+  }
+  if (h->n_pairs > 0) {
+    const int T = 256;
+    const unsigned B = (unsigned)((h->n_pairs + T - 1) / T);
+    k_pairs<COLL><<<B, T, 0, h->stream>>>(h->dp, h->n_pairs, h->pair_owner, h->nbrs[h->rb], h->pos4[c],
+                                          h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc],
+                                          h->pft[1 - pc], h->pflag, h->prec, h->derr);
+    DEM_LAUNCH(h);
+  }
+}
+
+template <int MODE>
+static void launch_gather(dem_handle* h) {
+  const int T = 256, B = (h->n + T - 1) / T;
+  const int c = h->cur;
+  k_gather<MODE><<<B, T, 0, h->stream>>>(h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
+                                         h->vel4[1 - c], h->omg4[1 - c], h->state, h->dg_pijk, h->fbin_start,
+                                         h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
+                                         h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
   DEM_LAUNCH(h);
-  (void)nb;
 }
 
 int run_force(dem_handle* h, bool fused) {
   ProfScope ps(h, DEM_PROF_FORCE);
   h->dp.first_pass = h->first_pass ? 1 : 0;
-  const bool hz = h->dp.coll == DEM_COLL_HERTZ;
-  const bool ab2 = h->dp.intg == DEM_INTG_AB2;
-  if (!fused) {
-    if (hz) launch_force<DEM_COLL_HERTZ, 0>(h, 0); else launch_force<DEM_COLL_LSD, 0>(h, 0);
-  } else if (ab2) {
-    if (hz) launch_force<DEM_COLL_HERTZ, 2>(h, 0); else launch_force<DEM_COLL_LSD, 2>(h, 0);
-  } else {
-    if (hz) launch_force<DEM_COLL_HERTZ, 1>(h, 0); else launch_force<DEM_COLL_LSD, 1>(h, 0);
-  }
-  if (int rc = check_cuda(h, cudaGetLastError(), "k_force")) return rc;
+  if (h->dp.coll == DEM_COLL_HERTZ) launch_walls_pairs<DEM_COLL_HERTZ>(h);
+  else launch_walls_pairs<DEM_COLL_LSD>(h);
+  if (!fused) launch_gather<0>(h);
+  else if (h->dp.intg == DEM_INTG_AB2) launch_gather<2>(h);
+  else launch_gather<1>(h);
+  if (int rc = check_cuda(h, cudaGetLastError(), "force kernels")) return rc;
   h->pcur = 1 - h->pcur;
   if (fused) { h->cur = 1 - h->cur; h->first_pass = false; }
   return 0;

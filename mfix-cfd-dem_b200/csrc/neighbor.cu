@@ -56,12 +56,24 @@ __global__ void k_delete_rogue(DevParams p, int8_t* __restrict__ state, const in
 }
 
 // Count (FILL = false) or fill (FILL = true) one row per particle.
+//
+// Candidates come from the 27 search-grid cells around the particle; the
+// search grid is at least as fine as the DES grid and its cells are no
+// narrower than the largest search diameter, so every pair the reference
+// keeps is among the candidates.  A candidate is then tested exactly as the
+// reference tests it: it must lie in the particle's DES-grid stencil (the
+// coarse-grid reduction included), its periodic image is the one that
+// stencil cell holds, and the FP64 distance test is the reference's.  Each
+// kept neighbour carries its stencil rank ((lk, lj, li) order); the fill
+// pass inserts it into the row sorted by (rank, index), which is the order
+// of the reference's cell-by-cell scan.
 template <bool FILL>
-__global__ void k_neigh(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict__ state,
-                        const int* __restrict__ dg_pijk, const int* __restrict__ cell_start,
-                        const int* __restrict__ cell_list, const DevErr* __restrict__ err,
-                        int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
-                        int* __restrict__ owner, long long cap) {
+__global__ void __launch_bounds__(128)
+k_neigh(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict__ state,
+        const int* __restrict__ dg_pijk, const int* __restrict__ fkey, const int* __restrict__ fstart,
+        const int* __restrict__ flist, const DevErr* __restrict__ err, int* __restrict__ row_cnt,
+        int* __restrict__ row_se, int* __restrict__ nbrs, uint8_t* __restrict__ rank_buf,
+        int* __restrict__ owner, long long cap) {
   const int cur = blockIdx.x * blockDim.x + threadIdx.x;
   if (cur >= p.n) return;
   int start = 0;
@@ -70,58 +82,95 @@ __global__ void k_neigh(DevParams p, const double4* __restrict__ pos4, const int
   if (state[cur] == DEM_STATE_NORMAL && cur < err->first_rogue) {
     const int lijk = dg_pijk[cur];
     const int lic = dg_iof(p, lijk), ljc = dg_jof(p, lijk), lkc = dg_kof(p, lijk);
+    const int rc[3] = {lic, ljc, lkc};
+    const int s1[3] = {p.istart1, p.jstart1, p.kstart1}, e1[3] = {p.iend1, p.jend1, p.kend1};
+    const int ncl[3] = {p.iend1 - p.istart1 + 1, p.jend1 - p.jstart1 + 1, p.kend1 - p.kstart1 + 1};
     const double4 cp = pos4[cur];
-    const double fr = p.factor_rlm, mr = p.max_radius;
-    int il = 1, iu = 1, jl = 1, ju = 1, kl = 1, ku = 1;
     const double cpos[3] = {cp.x, cp.y, cp.z};
-    int* lo_off[3] = {&il, &jl, &kl};
-    int* hi_off[3] = {&iu, &ju, &ku};
+    const double fr = p.factor_rlm, mr = p.max_radius;
+    int lo_off[3] = {1, 1, 1}, hi_off[3] = {1, 1, 1};
     for (int ax = 0; ax < 3; ++ax) {
-      if (ax == 2 && p.no_k) { kl = 0; ku = 0; break; }
-      bool coarse = 1.0 > 2.0 * mr * fr * p.dg_inv[ax];
+      if (ax == 2 && p.no_k) { lo_off[2] = 0; hi_off[2] = 0; break; }
+      const bool coarse = 1.0 > 2.0 * mr * fr * p.dg_inv[ax];
       if (coarse) {
-        double t = (cpos[ax] - p.dg_start[ax]) * p.dg_inv[ax];
-        double off = t - (double)(long long)floor(t);
-        if (off >= 0.5) *lo_off[ax] = 0; else *hi_off[ax] = 0;
+        const double t = (cpos[ax] - p.dg_start[ax]) * p.dg_inv[ax];
+        const double off = t - (double)(long long)floor(t);
+        if (off >= 0.5) lo_off[ax] = 0; else hi_off[ax] = 0;
       }
     }
-    for (int lk = lkc - kl; lk <= lkc + ku; ++lk)
-    for (int lj = ljc - jl; lj <= ljc + ju; ++lj)
-    for (int li = lic - il; li <= lic + iu; ++li) {
-      int ri = li, rj = lj, rk = lk;
-      double sh0 = 0.0, sh1 = 0.0, sh2 = 0.0;
-      if (p.per[0]) {
-        if (li < p.istart1) { ri = p.iend1; sh0 = -p.L[0]; }
-        else if (li > p.iend1) { ri = p.istart1; sh0 = p.L[0]; }
+    const int key = fkey[cur];
+    const int fk = key / p.fc2, fi = (key % p.fc2) / p.fc1, fj = key % p.fc1;
+    const int kr = p.no_k ? 0 : 1;
+    for (int dk = -kr; dk <= kr; ++dk)
+    for (int dj = -1; dj <= 1; ++dj)
+    for (int di = -1; di <= 1; ++di) {
+      int g[3] = {fi + di, fj + dj, fk + dk};
+      const int d[3] = {di, dj, dk};
+      bool skip = false;
+      for (int ax = 0; ax < 3; ++ax) {
+        if (ax == 2 && p.no_k) break;
+        if (p.per[ax]) {
+          if (g[ax] < 1) g[ax] += p.fn[ax];
+          else if (g[ax] > p.fn[ax]) g[ax] -= p.fn[ax];
+        } else if (g[ax] < 0 || g[ax] > p.fn[ax] + 1) {
+          skip = true;
+        }
+        (void)d;
       }
-      if (p.per[1]) {
-        if (lj < p.jstart1) { rj = p.jend1; sh1 = -p.L[1]; }
-        else if (lj > p.jend1) { rj = p.jstart1; sh1 = p.L[1]; }
-      }
-      if (p.per[2] && !p.no_k) {
-        if (lk < p.kstart1) { rk = p.kend1; sh2 = -p.L[2]; }
-        else if (lk > p.kend1) { rk = p.kstart1; sh2 = p.L[2]; }
-      }
-      const int cell = dg_funijk(p, ri, rj, rk) - 1;
-      const int s = cell_start[cell], e = cell_start[cell + 1];
-      for (int q = s; q < e; ++q) {
-        const int nb = cell_list[q];
+      if (skip) continue;
+      const int cell = g[2] * p.fc2 + g[0] * p.fc1 + g[1];
+      const int qs = fstart[cell], qe = fstart[cell + 1];
+      for (int q = qs; q < qe; ++q) {
+        const int nb = flist[q];
         if (nb == cur) continue;
         const int8_t sn = state[nb];
         if (nb < cur && sn == DEM_STATE_NORMAL) continue;
         if (sn == DEM_STATE_NONEXISTENT) continue;
+        // position of the neighbour's DES cell in the reference stencil
+        const int nijk = dg_pijk[nb];
+        const int nc[3] = {dg_iof(p, nijk), dg_jof(p, nijk), dg_kof(p, nijk)};
+        int rel[3];
+        double sh[3] = {0.0, 0.0, 0.0};
+        bool in_stencil = true;
+        for (int ax = 0; ax < 3; ++ax) {
+          int r = nc[ax] - rc[ax];
+          if (p.per[ax] && !(ax == 2 && p.no_k)) {
+            if (r > 1) r -= ncl[ax];
+            else if (r < -1) r += ncl[ax];
+            const int l = rc[ax] + r;
+            if (l < s1[ax]) sh[ax] = -p.L[ax];
+            else if (l > e1[ax]) sh[ax] = p.L[ax];
+          }
+          if (r < -lo_off[ax] || r > hi_off[ax]) { in_stencil = false; break; }
+          rel[ax] = r;
+        }
+        if (!in_stencil) continue;
         const double4 np_ = pos4[nb];
         const double srad = fr * (cp.w + np_.w);
         double px = np_.x, py = np_.y, pz = np_.z;
-        if (sh0 != 0.0) px = px + sh0;
-        if (sh1 != 0.0) py = py + sh1;
-        if (sh2 != 0.0) pz = pz + sh2;
+        if (sh[0] != 0.0) px = px + sh[0];
+        if (sh[1] != 0.0) py = py + sh[1];
+        if (sh[2] != 0.0) pz = pz + sh[2];
         const double d0 = cp.x - px, d1 = cp.y - py, d2 = cp.z - pz;
         const double dd = d0 * d0 + d1 * d1 + d2 * d2;
         if (dd > srad * srad) continue;
         if (FILL) {
+          const int rank = ((rel[2] + 1) * 3 + (rel[1] + 1)) * 3 + (rel[0] + 1);
           long long slot = (long long)start + cnt;
-          if (slot < cap) { nbrs[slot] = nb; owner[slot] = cur; }
+          if (slot < cap) {
+            // insertion into the row kept sorted by (rank, index)
+            long long b = slot - 1;
+            while (b >= start) {
+              const int rb = rank_buf[b];
+              if (rb < rank || (rb == rank && nbrs[b] < nb)) break;
+              nbrs[b + 1] = nbrs[b];
+              rank_buf[b + 1] = (uint8_t)rb;
+              --b;
+            }
+            nbrs[b + 1] = nb;
+            rank_buf[b + 1] = (uint8_t)rank;
+            owner[slot] = cur;
+          }
         }
         ++cnt;
       }
@@ -187,13 +236,15 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   long long cap = h->pair_cap > 0 ? h->pair_cap : 1024;
   while (cap < need) cap *= 2;
   const long long old = h->n_pairs;
-  int* nb[2]; double* pf[2]; int2* inp; int* own;
+  int* nb[2]; double* pf[2]; int2* inp; int* own; uint8_t* pfl; PairRec* prc;
   for (int b = 0; b < 2; ++b) {
     if (int rc = check_cuda(h, cudaMalloc(&nb[b], sizeof(int) * cap), "cudaMalloc nbrs")) return rc;
     if (int rc = check_cuda(h, cudaMalloc(&pf[b], sizeof(double) * 3 * cap), "cudaMalloc pft")) return rc;
   }
   if (int rc = check_cuda(h, cudaMalloc(&inp, sizeof(int2) * cap), "cudaMalloc in_pair")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&own, sizeof(int) * cap), "cudaMalloc owner")) return rc;
+  if (int rc = check_cuda(h, cudaMalloc(&pfl, cap), "cudaMalloc pflag")) return rc;
+  if (int rc = check_cuda(h, cudaMalloc(&prc, sizeof(PairRec) * cap), "cudaMalloc prec")) return rc;
   if (old > 0) {
     // keep the current list and history (the rebuild reads them)
     cudaMemcpyAsync(nb[h->rb], h->nbrs[h->rb], sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
@@ -203,8 +254,8 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   }
   cudaStreamSynchronize(h->stream);
   for (int b = 0; b < 2; ++b) { cudaFree(h->nbrs[b]); cudaFree(h->pft[b]); h->nbrs[b] = nb[b]; h->pft[b] = pf[b]; }
-  cudaFree(h->in_pair); cudaFree(h->pair_owner);
-  h->in_pair = inp; h->pair_owner = own;
+  cudaFree(h->in_pair); cudaFree(h->pair_owner); cudaFree(h->pflag); cudaFree(h->prec);
+  h->in_pair = inp; h->pair_owner = own; h->pflag = pfl; h->prec = prc;
   h->pair_cap = cap;
   return check_cuda(h, cudaGetLastError(), "grow pairs");
 }
@@ -223,8 +274,9 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   k_find_rogue<<<B, T, 0, h->stream>>>(p, h->state, h->dg_pijk, e);
   DEM_LAUNCH(h);
   const int nb = 1 - h->rb;  // new list goes into the other buffer
-  k_neigh<false><<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, h->cell_start,
-                                         h->cell_list, e, h->row_cnt, nullptr, nullptr, nullptr, 0);
+  k_neigh<false><<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, h->fcell_key,
+                                         h->fcell_start, h->fcell_list, e, h->row_cnt, nullptr, nullptr,
+                                         nullptr, nullptr, 0);
   DEM_LAUNCH(h);
   // delete rogue particles only after every row has been counted with the
   // states the serial loop saw
@@ -234,9 +286,9 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   if (int rc = check_cuda(h, cudaMemcpyAsync(&P, total, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "copy P")) return rc;
   if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
   if (int rc = ensure_pair_capacity(h, (long long)P + 1)) return rc;
-  k_neigh<true><<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, h->cell_start,
-                                        h->cell_list, e, nullptr, h->row_end[nb], h->nbrs[nb],
-                                        h->pair_owner, h->pair_cap);
+  k_neigh<true><<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, h->fcell_key,
+                                        h->fcell_start, h->fcell_list, e, nullptr, h->row_end[nb],
+                                        h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
   DEM_LAUNCH(h);
   k_delete_rogue<<<B, T, 0, h->stream>>>(p, h->state, h->dg_pijk, h->pos4[h->cur], h->vel4[h->cur],
                                          h->omg4[h->cur], h->fc, h->tow, h->wall_fid, e);

@@ -153,7 +153,7 @@ def _arrays(pos, vel, omega, radius, rho):
 
 
 def hertz_rsa(n=1_000_000, box=(0.1, 0.4, 0.1), solids=0.40, seed=SEED_BASE + 1,
-              precision=abi.DEM_PREC_FP64, nsn=25, cache_dir=None):
+              precision=abi.DEM_PREC_FP64, nsn=25, cache_dir=None, inflate=1.0):
     """1M polydisperse Hertzian spheres: lognormal d (median 1 mm, sigma
     0.25, clipped to [0.5, 2] mm), rho 2500, E 1e7, nu 0.3, e_n = e_t = 0.85,
     mu 0.3, mu_r 0.01, periodic x/z, flat bottom wall; random sequential
@@ -176,8 +176,10 @@ def hertz_rsa(n=1_000_000, box=(0.1, 0.4, 0.1), solids=0.40, seed=SEED_BASE + 1,
             cache.parent.mkdir(parents=True, exist_ok=True)
             np.savez(cache, pos=pos, top=top_final)
     vel = np.zeros((n, 3)); omega = np.zeros((n, 3))
-    radius = 0.5 * d
-    case = P.DemCase(d_p0=(2e-3,), ro_s0=(2500.0,), coll_model="HERTZ", intg_method="EULER",
+    # inflate > 1 grows every sphere after placement, which turns the
+    # near-contacts of the random packing into overlapping contacts
+    radius = 0.5 * d * inflate
+    case = P.DemCase(d_p0=(2e-3 * inflate,), ro_s0=(2500.0,), coll_model="HERTZ", intg_method="EULER",
                      des_en_input=0.85, des_en_wall_input=[0.85], des_et_input=0.85, des_et_wall_input=[0.85],
                      e_young=(1e7,), v_poisson=(0.3,), ew_young=1e7, vw_poisson=0.3,
                      mew=0.3, mew_w=0.3, mew_r=0.01, mew_rw=0.01, grav=(0.0, -9.81, 0.0),

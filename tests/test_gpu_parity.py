@@ -110,3 +110,32 @@ def test_rogue_particles_removed_like_oracle():
     assert sg["state"][50] == 0 and sg["state"][120] == 0
     g.step(20); o.step(20)
     compare_state(g, o, exact=True)
+
+
+def test_coarse_des_grid_matches_oracle():
+    """DES cells narrower than 2*FACTOR_RLM*MAX_RADIUS: the reference scans only
+    the nearer neighbour cell per axis (desgrid_mod.f:1116-1152)."""
+    from mfix_dem import params as P
+    case, prm, arr, walls = settling_case(n_side=(8, 20, 8), box=(12e-3, 60e-3, 12e-3), spacing=1.0, nsn=5)
+    case.desgridsearch = (11, 55, 11)
+    prm, _ = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    assert 1.0 > 2.0 * prm.max_radius * prm.factor_rlm * prm.dg_dxinv
+    g, o = pair_both(prm, arr, walls)
+    compare_pairs(g, o)
+    for _ in range(3):
+        g.step(10); o.step(10)
+        compare_state(g, o, exact=True)
+        compare_pairs(g, o)
+
+
+def test_dense_overlapping_bed_matches_oracle():
+    """Initial overlaps everywhere (lattice spacing 0.97 d): every pair is a
+    contact from the first step, Hertz with rolling friction, AB2."""
+    case, prm, arr, walls = settling_case(n_side=(8, 12, 8), spacing=0.97, jitter=0.01, coll="HERTZ",
+                                          intg="ADAMS_BASHFORTH", mew_r=0.02, polydisperse=0.1, nsn=7)
+    g, o = pair_both(prm, arr, walls)
+    for _ in range(3):
+        g.step(11); o.step(11)
+        compare_state(g, o, exact=True)
+        compare_pairs(g, o)
+    assert g.stats()["n_contacts"] == o.stats()["n_contacts"] > 0
