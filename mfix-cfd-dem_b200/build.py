@@ -30,6 +30,7 @@ SOURCES = {
     "desgrid.cu": ["-fmad=false"],
     "neighbor.cu": ["-fmad=false"],
     "force.cu": ["-fmad=false"],
+    "force_split.cu": ["-fmad=true", "-use_fast_math"],
     "walls.cu": ["-fmad=false"],
     "coupling.cu": ["-fmad=false"],
 }

@@ -169,6 +169,7 @@ static void fill_devparams(dem_handle* h) {
   p.coll = q.coll_model; p.intg = q.intg_method; p.nph = q.n_phases; p.no_k = q.no_k;
   p.cmax = q.collision_array_max > 0 ? q.collision_array_max : 8;
   p.remove_rogue = q.remove_rogue;
+  p.prec = q.force_precision == DEM_PREC_SPLIT ? DEM_PREC_SPLIT : DEM_PREC_FP64;
   for (int a = 0; a < 3; ++a) {
     p.per[a] = q.periodic[a] ? 1 : 0;
     p.grav[a] = q.grav[a];
@@ -199,16 +200,17 @@ static void fill_devparams(dem_handle* h) {
   }
   // Search grid for the pair build: cells no narrower than the largest
   // search diameter 2*FACTOR_RLM*MAX_RADIUS (with a 1 % margin), so a 27-cell
-  // stencil holds every candidate.  An axis keeps the DES grid's division
-  // when that is not coarser, when the DES grid is coarse there, or when a
-  // periodic axis would get fewer than 3 cells.
+  // stencil holds every candidate within reach; the reference's own DES-grid
+  // stencil (reduced to the nearer cells when the DES cells are wider than
+  // that diameter) is applied to the candidates afterwards.  An axis keeps
+  // the DES grid's division when that is not coarser or when a periodic axis
+  // would get fewer than 3 cells.
   const int dgn[3] = {q.dg_imax, q.dg_jmax, q.no_k ? 1 : q.dg_kmax};
   const double target = 2.0 * q.factor_rlm * q.max_radius * 1.01;
   for (int a = 0; a < 3; ++a) {
     const double len = (double)dgn[a] / p.dg_inv[a];
     int nfa = (int)std::floor(len / target);
-    const bool coarse = 1.0 > 2.0 * q.max_radius * q.factor_rlm * p.dg_inv[a];
-    if (nfa <= dgn[a] || coarse || (p.per[a] && nfa < 3) || (a == 2 && q.no_k)) nfa = dgn[a];
+    if (nfa <= dgn[a] || (p.per[a] && nfa < 3) || (a == 2 && q.no_k)) nfa = dgn[a];
     if (nfa < 1) nfa = 1;
     p.fn[a] = nfa;
     // same division as the DES grid -> the same inverse width, bit for bit

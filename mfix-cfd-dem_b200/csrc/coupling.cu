@@ -3,12 +3,6 @@
 
 using namespace demb;
 
-namespace demb {
-int run_split_force_error(dem_handle* h, double* rel_err) {
-  (void)rel_err;
-  return set_err(h, DEM_ERR_STATE, "split-precision path not built");
-}
-}  // namespace demb
 
 extern "C" {
 int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid*, const double*, const double*, const double*,

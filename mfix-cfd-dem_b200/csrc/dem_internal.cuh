@@ -52,7 +52,7 @@ struct DevErr {
 // Parameters as kernels see them (passed by value).
 struct DevParams {
   int n;
-  int coll, intg, nph, no_k, cmax, remove_rogue, first_pass;
+  int coll, intg, nph, no_k, cmax, remove_rogue, first_pass, prec;
   int per[3];
   int istart1, iend1, istart2, iend2;
   int jstart1, jend1, jstart2, jend2;
@@ -205,6 +205,8 @@ int run_force(dem_handle* h, bool fused);
 int run_cfnewvalues(dem_handle* h);
 int run_bin_facets(dem_handle* h, const double* vertex_fortran, const double* norm_fortran, int nf);
 int run_split_force_error(dem_handle* h, double* rel_err);
+void launch_pairs_split(dem_handle* h);         // force_split.cu
+void launch_gather_split(dem_handle* h, int mode);
 int ensure_pair_capacity(dem_handle* h, long long need);
 int fetch_errors(dem_handle* h);
 void* stage_buffer(dem_handle* h, size_t bytes);

@@ -22,6 +22,9 @@
 // IEEE round-to-nearest in CUDA, as they are on the host.
 #include "dem_internal.cuh"
 
+#include <algorithm>
+#include <cmath>
+
 namespace demb {
 
 struct PState {  // one particle's gathered state
@@ -615,15 +618,15 @@ static WallCtx wall_ctx(dem_handle* h) {
 }
 
 template <int COLL>
-static void launch_walls_pairs(dem_handle* h) {
+static void launch_walls_pairs(dem_handle* h, bool walls, bool pairs) {
   const int c = h->cur, pc = h->pcur;
-  if (h->nf > 0) {
+  if (walls && h->nf > 0) {
     const int T = 128, B = (h->n + T - 1) / T;
     k_walls<COLL><<<B, T, 0, h->stream>>>(h->dp, wall_ctx(h), h->pos4[c], h->vel4[c], h->omg4[c], h->phase,
                                           h->state, h->wall_live, h->wf, h->derr);
     DEM_LAUNCH(h);
   }
-  if (h->n_pairs > 0) {
+  if (pairs && h->n_pairs > 0) {
     const int T = 256;
     const unsigned B = (unsigned)((h->n_pairs + T - 1) / T);
     k_pairs<COLL><<<B, T, 0, h->stream>>>(h->dp, h->n_pairs, h->pair_owner, h->nbrs[h->rb], h->pos4[c],
@@ -644,18 +647,75 @@ static void launch_gather(dem_handle* h) {
   DEM_LAUNCH(h);
 }
 
+static void launch_walls(dem_handle* h) {
+  if (h->dp.coll == DEM_COLL_HERTZ) launch_walls_pairs<DEM_COLL_HERTZ>(h, true, false);
+  else launch_walls_pairs<DEM_COLL_LSD>(h, true, false);
+}
+
+// Contact forces of the current state.  mode: 0 = into FC/TOW, 1/2 = fused
+// Euler/AB2 integration into the other state buffer.
+static void launch_force_kernels(dem_handle* h, int mode, bool split) {
+  launch_walls(h);
+  if (split) {
+    launch_pairs_split(h);
+    launch_gather_split(h, mode);
+    return;
+  }
+  if (h->dp.coll == DEM_COLL_HERTZ) launch_walls_pairs<DEM_COLL_HERTZ>(h, false, true);
+  else launch_walls_pairs<DEM_COLL_LSD>(h, false, true);
+  if (mode == 0) launch_gather<0>(h);
+  else if (mode == 1) launch_gather<1>(h);
+  else launch_gather<2>(h);
+}
+
 int run_force(dem_handle* h, bool fused) {
   ProfScope ps(h, DEM_PROF_FORCE);
   h->dp.first_pass = h->first_pass ? 1 : 0;
-  if (h->dp.coll == DEM_COLL_HERTZ) launch_walls_pairs<DEM_COLL_HERTZ>(h);
-  else launch_walls_pairs<DEM_COLL_LSD>(h);
-  if (!fused) launch_gather<0>(h);
-  else if (h->dp.intg == DEM_INTG_AB2) launch_gather<2>(h);
-  else launch_gather<1>(h);
+  const int mode = !fused ? 0 : (h->dp.intg == DEM_INTG_AB2 ? 2 : 1);
+  launch_force_kernels(h, mode, h->dp.prec == DEM_PREC_SPLIT);
   if (int rc = check_cuda(h, cudaGetLastError(), "force kernels")) return rc;
   h->pcur = 1 - h->pcur;
   if (fused) { h->cur = 1 - h->cur; h->first_pass = false; }
   return 0;
+}
+
+// Per-step force error of the split path: both paths evaluate FC for the
+// current state (the wall history is restored between and after them, the
+// pair history is read, not advanced); returns max|F_split - F_fp64| over
+// all components divided by max|F_fp64|.
+int run_split_force_error(dem_handle* h, double* rel_err) {
+  if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
+  const size_t n = h->n, cm = h->dp.cmax;
+  const size_t b_fid = sizeof(int) * cm * n, b_pft = sizeof(double) * 3 * cm * n;
+  char* snap = (char*)stage_buffer(h, b_fid + b_pft + n + 64);
+  if (!snap) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
+  auto save = [&]() {
+    cudaMemcpyAsync(snap, h->wall_fid, b_fid, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(snap + b_fid, h->wall_pft, b_pft, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(snap + b_fid + b_pft, h->wall_live, n, cudaMemcpyDeviceToDevice, h->stream);
+  };
+  auto restore = [&]() {
+    cudaMemcpyAsync(h->wall_fid, snap, b_fid, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->wall_pft, snap + b_fid, b_pft, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->wall_live, snap + b_fid + b_pft, n, cudaMemcpyDeviceToDevice, h->stream);
+  };
+  std::vector<double> f64(3 * n), f32(3 * n);
+  h->dp.first_pass = 0;
+  save();
+  launch_force_kernels(h, 0, false);
+  cudaMemcpyAsync(f64.data(), h->fc, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  restore();
+  launch_force_kernels(h, 0, true);
+  cudaMemcpyAsync(f32.data(), h->fc, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  restore();
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "force error")) return rc;
+  double dmax = 0.0, fmax = 0.0;
+  for (size_t k = 0; k < 3 * n; ++k) {
+    dmax = std::max(dmax, std::fabs(f32[k] - f64[k]));
+    fmax = std::max(fmax, std::fabs(f64[k]));
+  }
+  *rel_err = fmax > 0.0 ? dmax / fmax : dmax;
+  return fetch_errors(h);
 }
 
 int run_cfnewvalues(dem_handle* h) {

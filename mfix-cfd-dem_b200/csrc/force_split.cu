@@ -1,0 +1,300 @@
+// force_split.cu -- split-precision contact forces (FP32 forces, FP64
+// history and integration).
+//
+// Same structure as the FP64 path (walls -> pairs -> gather, see force.cu)
+// and the same contact law (calc_force_dem.f:204-506, cfrelvel.f:54-77), with
+// this split of the arithmetic:
+//   FP64  the displacement x_I - x_L and the velocity difference v_L - v_I
+//         (differences of large, nearly equal numbers), |x_I - x_L| and the
+//         normal overlap R_LM - |x_I - x_L|; the tangential-overlap history
+//         update (PFT + DT*V_t, its magnitude and the Coulomb rescaling) and
+//         the integration (CFNEWVALUES);
+//   FP32  the unit normal, relative velocity at the contact point, spring and
+//         damping coefficients, normal/tangential forces, torque arms and
+//         rolling friction; per-particle sums use compensated (Neumaier)
+//         FP32 accumulation.
+// Wall contacts use the FP64 wall kernel.  This file is compiled with FMA
+// contraction and fast single-precision square roots and divisions.
+#include "dem_internal.cuh"
+
+namespace demb {
+
+struct PairRec32 {  // 40 bytes, fits in a PairRec slot
+  float fc[3], tf[3], dcl2, dci2, kn, ov;
+};
+static_assert(sizeof(PairRec32) <= sizeof(PairRec), "record size");
+
+struct Comp3 {  // Neumaier-compensated FP32 sum of a 3-vector
+  float s[3], c[3];
+  __device__ void zero() { for (int k = 0; k < 3; ++k) { s[k] = 0.f; c[k] = 0.f; } }
+  __device__ __forceinline__ void add(int k, float x) {
+    const float t = s[k] + x;
+    if (fabsf(s[k]) >= fabsf(x)) c[k] += (s[k] - t) + x;
+    else c[k] += (x - t) + s[k];
+    s[k] = t;
+  }
+  __device__ __forceinline__ double value(int k) const { return (double)s[k] + (double)c[k]; }
+};
+
+template <int COLL>
+__global__ void __launch_bounds__(256)
+k_pairs_split(DevParams p, long long np, const int* __restrict__ owner, const int* __restrict__ nbrs,
+              const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+              const double4* __restrict__ omg4, const int8_t* __restrict__ state,
+              const uint8_t* __restrict__ phase, const double* __restrict__ pft_in,
+              double* __restrict__ pft_out, uint8_t* __restrict__ pflag, PairRec32* __restrict__ prec,
+              DevErr* __restrict__ err) {
+  const long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long ncont = 0;
+  unsigned eflags = 0;
+  if (cc < np) {
+    const int ll = owner[cc], i = nbrs[cc];
+    const double* pi = pft_in + 3 * cc;
+    const double pin[3] = {pi[0], pi[1], pi[2]};
+    double* po = pft_out + 3 * cc;
+    uint8_t flag = 0;
+    if (state[i] == DEM_STATE_NONEXISTENT || state[ll] == DEM_STATE_NONEXISTENT) {
+      po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2];
+    } else {
+      const double4 a = pos4[ll], b = pos4[i];
+      const double xl[3] = {a.x, a.y, a.z}, xi[3] = {b.x, b.y, b.z};
+      double dist[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double pj = xi[c];
+        const double s = periodic_shift(p, c, pj - xl[c]);
+        if (s != 0.0) pj = pj + s;
+        dist[c] = pj - xl[c];
+      }
+      const double r_lm = a.w + b.w;
+      const double d2 = dist[0] * dist[0] + dist[1] * dist[1] + dist[2] * dist[2];
+      if (d2 > (r_lm - SMALL_NUMBER) * (r_lm - SMALL_NUMBER)) {
+        po[0] = po[1] = po[2] = 0.0;
+      } else if (d2 == 0.0) {
+        po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2];
+        eflags |= EF_ZERO_DIST;
+        err->zero_a = ll; err->zero_b = i;
+      } else {
+        const double dmag64 = sqrt(d2);
+        const float dmag = (float)dmag64;
+        const float ov = (float)(r_lm - dmag64);
+        const float rl = (float)a.w, ri = (float)b.w;
+        const float nrm[3] = {(float)dist[0] / dmag, (float)dist[1] / dmag, (float)dist[2] / dmag};
+        const double4 va = vel4[ll], vb = vel4[i], wa = omg4[ll], wb = omg4[i];
+        float vrel[3] = {(float)(va.x - vb.x), (float)(va.y - vb.y), (float)(va.z - vb.z)};
+        const float dcl = (dmag * dmag + rl * rl - ri * ri) / (2.f * dmag);
+        const float dci = dmag - dcl;
+        const float osum[3] = {(float)wa.x * dcl + (float)wb.x * dci, (float)wa.y * dcl + (float)wb.y * dci,
+                               (float)wa.z * dcl + (float)wb.z * dci};
+        vrel[0] += osum[1] * nrm[2] - osum[2] * nrm[1];
+        vrel[1] += osum[2] * nrm[0] - osum[0] * nrm[2];
+        vrel[2] += osum[0] * nrm[1] - osum[1] * nrm[0];
+        const float vrn = vrel[0] * nrm[0] + vrel[1] * nrm[1] + vrel[2] * nrm[2];
+        const float vt[3] = {vrel[0] - vrn * nrm[0], vrel[1] - vrn * nrm[1], vrel[2] - vrn * nrm[2]};
+        const int ix = phase[ll] * MAXP + phase[i];
+        const float rad_eff = (rl * ri) / (rl + ri);
+        const float ml = (float)va.w, mi = (float)vb.w;
+        const float m_eff = (ml * mi) / (ml + mi);
+        float kn, kt, etan, etat;
+        if (COLL == DEM_COLL_HERTZ) {
+          float so = sqrtf(ov);
+          const float sre = sqrtf(rad_eff);
+          const float hkn = (float)p.hkn[ix], hkt = (float)p.hkt[ix];
+          kn = hkn * so * sre;
+          kt = hkt * so * sre;
+          so = sqrtf(so);
+          etan = (float)p.etan[ix] * so * sqrtf(hkn * sre * m_eff);
+          etat = (float)p.etat[ix] * so * sqrtf(hkt * sre * m_eff);
+        } else {
+          kn = (float)p.kn; kt = (float)p.kt;
+          const float sm = sqrtf(m_eff);
+          etan = (float)p.etan[ix] * sm;
+          etat = (float)p.etat[ix] * sm;
+        }
+        float fn[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fn[c] = -(kn * ov + etan * vrn) * nrm[c];
+        // tangential history in FP64
+        double ot[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ot[c] = p.dt * (double)vt[c] + pin[c];
+        const double mag = sqrt(ot[0] * ot[0] + ot[1] * ot[1] + ot[2] * ot[2]);
+        float ft[3] = {0.f, 0.f, 0.f};
+        if (mag > 0.0) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) ft[c] = -kt * (float)ot[c] - etat * vt[c];
+          const float ftmd = sqrtf(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+          const float fnmd = (float)p.mew * sqrtf(fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2]);
+          if (ftmd > fnmd) {
+            const double sc = (double)fnmd / (double)kt / mag;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const double tg = ot[c] / mag;
+              ft[c] = -fnmd * (float)tg;
+              ot[c] = sc * ot[c];
+            }
+          }
+        }
+        po[0] = ot[0]; po[1] = ot[1]; po[2] = ot[2];
+        PairRec32 r;
+        r.dcl2 = dmag * 0.5f + (rl * rl - ri * ri) / (2.f * dmag);
+        r.dci2 = dmag - r.dcl2;
+        r.tf[0] = nrm[1] * ft[2] - nrm[2] * ft[1];
+        r.tf[1] = nrm[2] * ft[0] - nrm[0] * ft[2];
+        r.tf[2] = nrm[0] * ft[1] - nrm[1] * ft[0];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) r.fc[c] = fn[c] + ft[c];
+        r.kn = kn;
+        r.ov = ov;
+        prec[cc] = r;
+        flag = 1;
+        ++ncont;
+      }
+    }
+    pflag[cc] = flag;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ncont += __shfl_down_sync(0xffffffffu, ncont, o);
+    eflags |= __shfl_down_sync(0xffffffffu, eflags, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (ncont) atomicAdd(&err->n_contacts, ncont);
+    if (eflags) atomicOr(&err->flags, eflags);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256)
+k_gather_split(DevParams p, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
+               const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
+               double4* __restrict__ omg_n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
+               const int* __restrict__ fbin_start, int nf, const double* __restrict__ wf,
+               const int* __restrict__ row_end, const int* __restrict__ in_start,
+               const int2* __restrict__ in_pair, const uint8_t* __restrict__ pflag,
+               const PairRec32* __restrict__ prec, double* __restrict__ fc, double* __restrict__ tow,
+               double* __restrict__ acc_old, double* __restrict__ rot_acc_old) {
+  const int me = blockIdx.x * blockDim.x + threadIdx.x;
+  if (me >= p.n) return;
+  const int8_t st = state[me];
+  const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
+  const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
+  const double r = X.w, m = V.w, omoi = W.w;
+  double f0[3] = {0.0, 0.0, 0.0}, t0[3] = {0.0, 0.0, 0.0};
+  if (st == DEM_STATE_NORMAL && nf > 0) {
+    const int cell = dg_pijk[me] - 1;
+    if (fbin_start[cell + 1] > fbin_start[cell]) {
+      const double* o = wf + 6 * (size_t)me;
+      f0[0] = o[0]; f0[1] = o[1]; f0[2] = o[2]; t0[0] = o[3]; t0[1] = o[4]; t0[2] = o[5];
+    }
+  }
+  Comp3 F, T;
+  F.zero(); T.zero();
+  if (st != DEM_STATE_NONEXISTENT) {
+    const float wf32[3] = {(float)w[0], (float)w[1], (float)w[2]};
+    const float om = sqrtf(wf32[0] * wf32[0] + wf32[1] * wf32[1] + wf32[2] * wf32[2]);
+    const bool roll = p.mew_r > 0.0 && om > 0.f;
+    const float rf = (float)p.mew_r * (2.f * (float)r);
+    const int rs = me ? row_end[me - 1] : 0, re = row_end[me];
+    const int is = in_start[me], ie = in_start[me + 1];
+    for (int q = is; q < ie; ++q) {
+      const int cc = in_pair[q].y;
+      if (!pflag[cc]) continue;
+      const PairRec32 o = prec[cc];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) { F.add(c, -o.fc[c]); T.add(c, o.dci2 * o.tf[c]); }
+      if (roll) {
+        const float s = -(rf * o.kn * o.ov) / om;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) T.add(c, s * wf32[c]);
+      }
+    }
+    for (int cc = rs; cc < re; ++cc) {
+      if (!pflag[cc]) continue;
+      const PairRec32 o = prec[cc];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) { F.add(c, o.fc[c]); T.add(c, o.dcl2 * o.tf[c]); }
+      if (roll) {
+        const float s = -(rf * o.kn * o.ov) / om;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) T.add(c, s * wf32[c]);
+      }
+    }
+  }
+  double f[3], t[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) { f[c] = f0[c] + F.value(c); t[c] = t0[c] + T.value(c); }
+  const size_t n = (size_t)p.n;
+  if (MODE == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { fc[c * n + me] = f[c]; tow[c * n + me] = t[c]; }
+    return;
+  }
+  const double dt = p.dt;
+  double xn[3], vn[3], wn[3];
+  if (MODE == 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      vn[c] = v[c];
+      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + dt * (f[c] / m + p.grav[c]);
+      xn[c] = x[c];
+      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + vn[c] * dt;
+      wn[c] = w[c];
+      if (st == DEM_STATE_NORMAL) wn[c] = w[c] + t[c] * omoi * dt;
+    }
+  } else {
+    const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
+                         st == DEM_STATE_NORMAL_GHOST || st == 110);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
+      if (p.first_pass && fp_ok) { ao = f[c] / m + p.grav[c]; ro = t[c]; }
+      double a = f[c];
+      if (st == DEM_STATE_NORMAL) a = f[c] / m + p.grav[c];
+      vn[c] = v[c];
+      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + 0.5 * (3.0 * a - ao) * dt;
+      acc_old[c * n + me] = a;
+      xn[c] = x[c];
+      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + 0.5 * (v[c] + vn[c]) * dt;
+      wn[c] = w[c];
+      if (st == DEM_STATE_NORMAL) {
+        wn[c] = w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
+        ro = t[c] * omoi;
+      }
+      rot_acc_old[c * n + me] = ro;
+    }
+  }
+  pos_n[me] = make_double4(xn[0], xn[1], xn[2], r);
+  vel_n[me] = make_double4(vn[0], vn[1], vn[2], m);
+  omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+}
+
+void launch_pairs_split(dem_handle* h) {
+  if (h->n_pairs <= 0) return;
+  const int c = h->cur, pc = h->pcur;
+  const int T = 256;
+  const unsigned B = (unsigned)((h->n_pairs + T - 1) / T);
+  if (h->dp.coll == DEM_COLL_HERTZ)
+    k_pairs_split<DEM_COLL_HERTZ><<<B, T, 0, h->stream>>>(h->dp, h->n_pairs, h->pair_owner, h->nbrs[h->rb],
+        h->pos4[c], h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
+        (PairRec32*)h->prec, h->derr);
+  else
+    k_pairs_split<DEM_COLL_LSD><<<B, T, 0, h->stream>>>(h->dp, h->n_pairs, h->pair_owner, h->nbrs[h->rb],
+        h->pos4[c], h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
+        (PairRec32*)h->prec, h->derr);
+  DEM_LAUNCH(h);
+}
+
+void launch_gather_split(dem_handle* h, int mode) {
+  const int T = 256, B = (h->n + T - 1) / T;
+  const int c = h->cur;
+#define GS_ARGS h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c], \
+    h->state, h->dg_pijk, h->fbin_start, h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair,         \
+    h->pflag, (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old
+  if (mode == 0) k_gather_split<0><<<B, T, 0, h->stream>>>(GS_ARGS);
+  else if (mode == 1) k_gather_split<1><<<B, T, 0, h->stream>>>(GS_ARGS);
+  else k_gather_split<2><<<B, T, 0, h->stream>>>(GS_ARGS);
+#undef GS_ARGS
+  DEM_LAUNCH(h);
+}
+
+}  // namespace demb

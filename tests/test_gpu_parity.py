@@ -112,14 +112,16 @@ def test_rogue_particles_removed_like_oracle():
     compare_state(g, o, exact=True)
 
 
-def test_coarse_des_grid_matches_oracle():
-    """DES cells narrower than 2*FACTOR_RLM*MAX_RADIUS: the reference scans only
-    the nearer neighbour cell per axis (desgrid_mod.f:1116-1152)."""
+def test_narrow_des_grid_matches_oracle():
+    """DES cells narrower than the search diameter 2*FACTOR_RLM*MAX_RADIUS:
+    the reference scans all 27 cells.  (With the default sizing of 3 max
+    diameters the cells are wider and the reference scans only the nearer
+    2x2x2 cells, desgrid_mod.f:1116-1152; the other tests cover that.)"""
     from mfix_dem import params as P
     case, prm, arr, walls = settling_case(n_side=(8, 20, 8), box=(12e-3, 60e-3, 12e-3), spacing=1.0, nsn=5)
     case.desgridsearch = (11, 55, 11)
     prm, _ = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
-    assert 1.0 > 2.0 * prm.max_radius * prm.factor_rlm * prm.dg_dxinv
+    assert not (1.0 > 2.0 * prm.max_radius * prm.factor_rlm * prm.dg_dxinv)
     g, o = pair_both(prm, arr, walls)
     compare_pairs(g, o)
     for _ in range(3):
