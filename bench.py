@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=125_000, help="particles in the CPU sample")
     ap.add_argument("--cpu-steps", type=int, default=25)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-split", action="store_true", help="skip the split-precision leg")
     ap.add_argument("--inflate", type=float, default=1.0,
                     help="grow every sphere by this factor after placement (contact-dense variant)")
     return ap.parse_args()
@@ -191,33 +192,22 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
+def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
+    """Builds one system for `prec`, runs W warm-up steps, then K timed steps
+    bracketed by CUDA events on the library's stream; returns the figures."""
     import torch
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from mfix_dem import GpuSystem
-    case, prm, arr, walls, info = workload(args.n, args.precision, args.inflate)
+    case, prm, arr, walls, info = workload(args.n, prec, args.inflate)
     n = arr["pos"].shape[1]
-    stream = torch.cuda.Stream()
     g = GpuSystem(prm, n)
     g.set_stream(stream.cuda_stream)
     g.set_walls(*walls)
     g.upload_state(arr["pos"], arr["vel"], arr["omega"], arr["radius"], arr["pmass"], arr["omoi"],
                    arr["state"], arr["phase"])
     g.init_neighbors()
-    # warm-up
     g.step(args.warmup, 1)
     torch.cuda.synchronize()
-
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
+    ferr0 = g.force_error() if prec == "split" else None
     clocks = ClockSampler(local)
     p0 = g.pair_count()
     l0 = g.launch_count()
@@ -239,16 +229,16 @@ def run_ours(args):
     launches = g.launch_count() - l0
     p1 = g.pair_count()
     st = g.stats()
+    ferr1 = g.force_error() if prec == "split" else None
     if ws > 1:
         import torch.distributed as dist
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     n_normal = int(st["n_normal"])
-    value_rank = n_normal * args.steps / (ms / 1e3)
-    value = value_rank * ws
+    value = ws * n_normal * args.steps / (ms / 1e3)
 
-    # roofline of the dominant kernel (fused contact force + integration)
+    # roofline of the dominant kernel class (contact forces + fused integration)
     f_ms, f_n = prof["force"]
     peak, peak_kind = measured_peak()
     p_avg = 0.5 * (p0 + p1)
@@ -257,20 +247,22 @@ def run_ours(args):
     traffic = None
     if PROFILE_TRAFFIC.exists():
         tr = json.loads(PROFILE_TRAFFIC.read_text())
-        if tr.get("workload") == "hertz_rsa_1m" and tr.get("precision") == args.precision:
-            traffic = tr.get("dram_bytes_per_launch")
+        key = f"{'hertz_rsa_1m' if args.inflate == 1.0 else 'hertz_rsa_1m_inflated'}:{prec}"
+        traffic = tr.get(key)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": "k_force (fused contact force + integration)", "peak_kind": peak_kind,
-                "algorithmic_bytes_per_launch": bytes_launch,
+                "kernel": "force step (k_walls + k_pairs + k_gather with fused integration)",
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_launch,
                 "avg_launch_ms": f_ms / f_n if f_n else None,
                 "share_of_step": f_ms / ms if ms else None,
                 "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]}}
+    out = {"value": value, "ms": ms, "n": n, "n_normal": n_normal, "pairs": int(p1), "launches": int(launches),
+           "roofline": roofline, "clocks": clk, "contacts": int(st["n_contacts"]), "prm": prm, "info": info,
+           "force_error": None if ferr0 is None else [ferr0, ferr1]}
 
     # e2e: per step, H2D of the particle arrays from pinned host memory, one
     # DES_TIME_STEP through the C ABI, D2H of the new positions/velocities/spins
-    e2e = None
-    if args.e2e_steps > 0:
+    if with_e2e and args.e2e_steps > 0:
         def pinned(a):
             t = torch.empty(a.shape, dtype={np.float64: torch.float64, np.int8: torch.int8,
                                             np.int32: torch.int32}[a.dtype.type], pin_memory=True)
@@ -300,12 +292,33 @@ def run_ours(args):
             t = torch.tensor([ems], device="cuda", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
-        h2d = n * (9 * 8 + 3 * 8 + 1 + 4)
-        d2h = n * (9 * 8 + 1)
-        e2e = {"value": ws * n_normal * args.e2e_steps / (ems / 1e3), "unit": METRIC,
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "steps": args.e2e_steps,
-               "note": "each step: dem_upload_state from pinned host arrays, dem_step, dem_download_state"}
+        out["e2e"] = {"value": ws * n_normal * args.e2e_steps / (ems / 1e3), "unit": METRIC,
+                      "h2d_bytes_per_step": n * (9 * 8 + 3 * 8 + 1 + 4), "d2h_bytes_per_step": n * (9 * 8 + 1),
+                      "steps": args.e2e_steps,
+                      "note": "each step: dem_upload_state from pinned host arrays, dem_step, dem_download_state"}
+    g.close()
+    return out
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    stream = torch.cuda.Stream()
+    main = _timed_run(args, args.precision, stream, barrier, ws, local, with_e2e=True)
+    other = None
+    if args.precision == "fp64" and not args.no_split:
+        other = _timed_run(args, "split", stream, barrier, ws, local, with_e2e=False)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -315,29 +328,35 @@ def run_ours(args):
             cpu = {"error": str(ex)}
 
     if rank == 0:
+        prm, info = main["prm"], main["info"]
+        wl = "hertz_rsa_1m" if args.inflate == 1.0 else f"hertz_rsa_1m_inflated_{args.inflate:g}"
         line = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "metric": METRIC, "value": main["value"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": "hertz_rsa_1m" if args.inflate == 1.0 else f"hertz_rsa_1m_inflated_{args.inflate:g}",
-                       "n_particles": n_normal, "n_pairs": int(p1),
-                       "pairs_per_particle": p1 / max(n_normal, 1), "precision": args.precision,
-                       "contact": "hertz", "integrator": "euler", "periodic": "xz",
-                       "neighbor_search_n": int(prm.neighbor_search_n),
+            "config": {"workload": wl, "n_particles": main["n_normal"], "n_pairs": main["pairs"],
+                       "pairs_per_particle": main["pairs"] / max(main["n_normal"], 1),
+                       "precision": args.precision, "contact": "hertz", "integrator": "euler",
+                       "periodic": "xz", "neighbor_search_n": int(prm.neighbor_search_n),
                        "solids_fraction": info.get("solids_fraction"), "dtsolid": prm.dtsolid,
+                       "contacts_last_step": main["contacts"],
                        "l2": "inputs larger than L2 (state and pair arrays ~%.0f MB)" % (
-                           (n * 3 * 32 * 2 + p1 * 60) / 1e6),
+                           (main["n"] * 3 * 32 * 2 + main["pairs"] * 100) / 1e6),
                        "parallelism": f"replicas x{ws}"},
-            "roofline": roofline,
+            "roofline": main["roofline"],
             "cpu_baseline": cpu,
-            "clocks": clk,
-            "e2e": e2e,
-            "gpu_launches": int(launches),
-            "contacts": int(st["n_contacts"]),
+            "clocks": main["clocks"],
+            "e2e": main.get("e2e"),
+            "gpu_launches": main["launches"],
         }
+        if other is not None:
+            line["split"] = {"value": other["value"], "ms_per_step": other["ms"] / args.steps,
+                             "speedup_vs_fp64": other["value"] / main["value"],
+                             "force_rel_error_first_last": other["force_error"],
+                             "roofline": other["roofline"], "gpu_launches": other["launches"],
+                             "clocks": other["clocks"]}
         print(json.dumps(line), flush=True)
-    g.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

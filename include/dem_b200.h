@@ -280,6 +280,7 @@ typedef struct dem_fluid_grid {
     double ro_g, mu_g;           /* gas density and viscosity (uniform) */
     double ep_star;              /* packed-bed void fraction EP_STAR (for ep_s max) */
     double ur_f_gs;              /* under-relaxation of F_GP (drag_gp_des.f), usually 1 */
+    double ro_s[DEM_MAX_PHASES]; /* RO_S0 of each solids phase (EP_S = ROP_S/RO_S) */
     double reserved[6];
 } dem_fluid_grid;
 

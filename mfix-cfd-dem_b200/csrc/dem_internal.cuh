@@ -210,6 +210,7 @@ void launch_gather_split(dem_handle* h, int mode);
 int ensure_pair_capacity(dem_handle* h, long long need);
 int fetch_errors(dem_handle* h);
 void* stage_buffer(dem_handle* h, size_t bytes);
+void free_gas(dem_handle* h);                   // coupling.cu
 
 // Brackets the kernels issued in its scope with CUDA events when the
 // handle's profiling is on.

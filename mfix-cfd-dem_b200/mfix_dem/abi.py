@@ -132,6 +132,7 @@ class DemFluidGrid(C.Structure):
         ("mu_g", C.c_double),
         ("ep_star", C.c_double),
         ("ur_f_gs", C.c_double),
+        ("ro_s", C.c_double * DEM_MAX_PHASES),
         ("reserved", C.c_double * 6),
     ]
 

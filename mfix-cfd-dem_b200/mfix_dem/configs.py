@@ -223,3 +223,69 @@ def settling(n_side=(10, 40, 10), d=1e-3, rho=2500.0, box=(12e-3, 60e-3, 12e-3),
     prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
     walls = P.default_walls(case.domain_lo, case.domain_hi)
     return case, prm, arr, walls, info
+
+
+def _smooth_noise(rng, shape, sigma_cells, std):
+    """Gaussian noise with a Gaussian correlation of sigma_cells, scaled to std."""
+    from scipy.ndimage import gaussian_filter
+    a = gaussian_filter(rng.normal(0.0, 1.0, shape), sigma=sigma_cells, mode="wrap")
+    s = a.std()
+    return a * (std / s if s > 0 else 0.0)
+
+
+def coupled(n=500_000, cells=(64, 256, 64), dx=1e-3, d=0.5e-3, rho=2600.0, kn=500.0, en=0.9, mew=0.1,
+            u_sup=1.0, u_std=0.1, corr_cells=4, ro_g=1.2, mu_g=1.8e-5, spacing=1.1, seed=SEED_BASE + 2,
+            nsn=25):
+    """CFD-DEM coupling: n spheres of diameter d on a jittered cubic lattice
+    (spacing `spacing`*d) filling the bottom of a cells[0] x cells[1] x cells[2]
+    fluid grid of cell size dx, LSD contact, default walls; frozen gas with
+    superficial velocity u_sup in y plus seeded Gaussian perturbations (std
+    u_std, correlation corr_cells cells) on every component; the interstitial
+    velocity is the superficial one divided by the initial void fraction.
+    Returns (case, prm, arr, walls, info, grid, fields)."""
+    rng = np.random.default_rng(seed)
+    box = (cells[0] * dx, cells[1] * dx, cells[2] * dx)
+    a = spacing * d
+    nx, nz = int(box[0] / a), int(box[2] / a)
+    ny = int(math.ceil(n / (nx * nz)))
+    kk, ii, jj = np.meshgrid(np.arange(nz), np.arange(nx), np.arange(ny), indexing="ij")
+    pos = np.empty((nx * ny * nz, 3))
+    pos[:, 0] = (ii.ravel() + 0.5) * a
+    pos[:, 1] = (jj.ravel() + 0.5) * a
+    pos[:, 2] = (kk.ravel() + 0.5) * a
+    pos = pos[np.argsort(pos[:, 1] * 1e6 + pos[:, 2] * 1e3 + pos[:, 0], kind="stable")][:n]
+    pos += rng.uniform(-0.04 * d, 0.04 * d, size=pos.shape)
+    vel = np.zeros((n, 3)); omega = np.zeros((n, 3))
+    radius = np.full(n, 0.5 * d)
+    case = P.DemCase(d_p0=(d,), ro_s0=(rho,), coll_model="LSD", kn=kn, kn_w=kn, des_en_input=en,
+                     des_en_wall_input=[en], mew=mew, mew_w=mew, grav=(0.0, -9.81, 0.0),
+                     domain_hi=box, fluid_cells=cells, neighbor_search_n=nsn)
+    arr = _arrays(pos, vel, omega, radius, np.full(n, rho))
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    perm = _sort_by_des_cell(prm, pos)
+    arr = _arrays(pos[perm], vel[perm], omega[perm], radius[perm], np.full(n, rho))
+    walls = P.default_walls(case.domain_lo, case.domain_hi)
+    # fluid fields on MFiX IJK (one ghost layer, i fastest)
+    gi, gj, gk = cells[0] + 2, cells[1] + 2, cells[2] + 2
+    vs_cell = np.zeros((gk, gj, gi))
+    ci = np.clip((pos[:, 0] / dx).astype(int) + 1, 1, cells[0])
+    cj = np.clip((pos[:, 1] / dx).astype(int) + 1, 1, cells[1])
+    ck = np.clip((pos[:, 2] / dx).astype(int) + 1, 1, cells[2])
+    np.add.at(vs_cell, (ck, cj, ci), (math.pi / 6.0) * d ** 3)
+    ep = 1.0 - np.minimum(1.0, vs_cell / dx ** 3)
+    ep = np.maximum(ep, 0.35)
+    shape = (gk, gj, gi)
+    u = _smooth_noise(rng, shape, corr_cells, u_std)
+    v = u_sup + _smooth_noise(rng, shape, corr_cells, u_std)
+    w = _smooth_noise(rng, shape, corr_cells, u_std)
+    fields = {"ep_g": ep.ravel().copy(), "u_g": (u / ep).ravel().copy(), "v_g": (v / ep).ravel().copy(),
+              "w_g": (w / ep).ravel().copy()}
+    grid = abi.DemFluidGrid()
+    grid.imax, grid.jmax, grid.kmax = cells
+    grid.drag_model = 0
+    grid.dx = grid.dy = grid.dz = dx
+    grid.ro_g, grid.mu_g = ro_g, mu_g
+    grid.ep_star = 0.42
+    grid.ur_f_gs = 1.0
+    grid.ro_s[0] = rho
+    return case, prm, arr, walls, info, grid, fields

@@ -90,10 +90,18 @@ struct Oracle {
   int64_t steps_done = 0, rogue_removed = 0, n_contacts = 0, n_wall_contacts = 0;
   double max_overlap_ratio = 0.0;
 
-  // coupling
+  // coupling (uniform Cartesian fluid grid; MFiX IJK with one ghost layer,
+  // i fastest)
   bool have_gas = false;
   dem_fluid_grid g{};
-  std::vector<double> ep_g, u_g, v_g, w_g, p_force, rop_s;
+  int gi2 = 0, gj2 = 0, gk2 = 0;          // imax+2, jmax+2, kmax+2
+  std::vector<double> xe, yn, zt;         // face positions, index 0..imax+2
+  std::vector<double> ep_g, u_g, v_g, w_g, p_force, rop_s, vol_surr;
+  std::vector<int> pijk;                  // (n,4): i, j, k, ijk (1-based), 0 = none
+  std::vector<double> f_gp;               // F_GP(n)
+  std::vector<int> pic_start, pic_list;   // particles per fluid cell, ascending
+  double pi_c = 4.0 * std::atan(1.0);
+  double ro_s[DEM_MAX_PHASES] = {0};
 
   int fail(int code, const std::string& m) { err = m; return code; }
 
@@ -915,6 +923,237 @@ struct Oracle {
     first_pass = false;
   }
 
+  // ---------------------------------------------------------------------
+  // CFD-DEM coupling, GARG_2012 interpolation (drag_gs_des0.f,
+  // comp_mean_fields0.f, calc_epg_des.f, particles_in_cell.f).
+  int cijk(int i, int j, int k) const { return (i - 1) + (j - 1) * gi2 + (k - 1) * gi2 * gj2; }  // 0-based
+  bool fluid_at(int i, int j, int k) const {
+    return i >= 2 && i <= g.imax + 1 && j >= 2 && j <= g.jmax + 1 &&
+           (p.no_k ? k == 1 : (k >= 2 && k <= g.kmax + 1));
+  }
+  double vol() const { return g.dx * g.dy * (p.no_k ? (p.domain_hi[2] - p.domain_lo[2]) : g.dz); }
+
+  void gas_setup() {
+    gi2 = g.imax + 2; gj2 = g.jmax + 2; gk2 = p.no_k ? 1 : g.kmax + 2;
+    auto faces = [](double lo, double d, int nc) {
+      std::vector<double> f(nc + 3);
+      f[1] = lo;
+      f[0] = lo - d;
+      for (int i = 2; i <= nc + 2; ++i) f[i] = f[i - 1] + d;
+      return f;
+    };
+    xe = faces(p.domain_lo[0], g.dx, g.imax);
+    yn = faces(p.domain_lo[1], g.dy, g.jmax);
+    zt = faces(p.domain_lo[2], g.dz, p.no_k ? 0 : g.kmax);
+    // VOL_SURR (make_arrays_des.f:78-105): fluid volume of the cells that
+    // share node (I,J,K), nodes I = ISTART2..IEND1
+    vol_surr.assign((size_t)gi2 * gj2 * gk2, 0.0);
+    const int kk0 = p.no_k ? 1 : 1, kk1 = p.no_k ? 1 : g.kmax + 1;
+    for (int k = kk0; k <= kk1; ++k)
+      for (int j = 1; j <= g.jmax + 1; ++j)
+        for (int i = 1; i <= g.imax + 1; ++i) {
+          double v = 0.0;
+          for (int kk = k; kk <= (p.no_k ? k : k + 1); ++kk)
+            for (int jj = j; jj <= j + 1; ++jj)
+              for (int ii = i; ii <= i + 1; ++ii)
+                if (fluid_at(ii, jj, kk)) v = v + vol();
+          vol_surr[cijk(i, j, k)] = v;
+        }
+    pijk.assign((size_t)4 * n, 0);
+    f_gp.assign(n, 0.0);
+  }
+
+  // PIC_SEARCH (particles_in_cell.f:347-370): first IDX in [1, nc+2] with
+  // faces[IDX-1] <= x < faces[IDX]; nc+3 when there is none.
+  static int pic_search(const std::vector<double>& f, int nc, double x) {
+    for (int idx = 1; idx <= nc + 2; ++idx)
+      if (x >= f[idx - 1] && x < f[idx]) return idx;
+    return nc + 3;
+  }
+
+  // PARTICLES_IN_CELL (particles_in_cell.f:20-234): fluid cell of every
+  // particle, per-cell lists in ascending particle order; particles outside
+  // the grid are deleted.
+  void particles_in_cell() {
+    std::vector<int> cnt(vol_surr.size(), 0);
+    for (int l = 0; l < n; ++l) {
+      if (state[l] == DEM_STATE_NONEXISTENT) continue;
+      int i = pic_search(xe, g.imax, P(pos, l, 0));
+      int j = pic_search(yn, g.jmax, P(pos, l, 1));
+      int k = p.no_k ? 1 : pic_search(zt, g.kmax, P(pos, l, 2));
+      bool on = i >= 1 && i <= gi2 && j >= 1 && j <= gj2 && k >= 1 && k <= gk2;
+      if (!on) { delete_particle(l); for (int c = 0; c < 4; ++c) pijk[4 * (size_t)l + c] = 0; continue; }
+      pijk[4 * (size_t)l] = i; pijk[4 * (size_t)l + 1] = j; pijk[4 * (size_t)l + 2] = k;
+      pijk[4 * (size_t)l + 3] = cijk(i, j, k) + 1;
+      if (state[l] < DEM_STATE_NORMAL_GHOST) cnt[cijk(i, j, k)]++;
+    }
+    pic_start.assign(cnt.size() + 1, 0);
+    for (size_t c = 0; c < cnt.size(); ++c) pic_start[c + 1] = pic_start[c] + cnt[c];
+    pic_list.assign(pic_start.back(), 0);
+    std::vector<int> fill(pic_start.begin(), pic_start.end() - 1);
+    for (int l = 0; l < n; ++l) {
+      if (state[l] == DEM_STATE_NONEXISTENT || state[l] >= DEM_STATE_NORMAL_GHOST) continue;
+      pic_list[fill[pijk[4 * (size_t)l + 3] - 1]++] = l;
+    }
+  }
+
+  // Trilinear weights in the cell whose west/south/bottom node is
+  // (xe[i-1], yn[j-1], zt[k-1]) -- DRAG_WEIGHTFACTOR (comp_mean_fields0.f:
+  // 478-530) and the weights of DRAG_INTERPOLATION (drag_gs_des0.f:507-566).
+  void weights(int i, int j, int k, const double x[3], double w[2][2][2]) const {
+    const double dxx = xe[i] - xe[i - 1], dyy = yn[j] - yn[j - 1];
+    double z0 = (x[0] - xe[i - 1]) / dxx, z1 = (x[1] - yn[j - 1]) / dyy;
+    double xx[2] = {1 - z0, z0}, yy[2] = {1 - z1, z1};
+    if (p.no_k) {
+      for (int jj = 0; jj < 2; ++jj) for (int ii = 0; ii < 2; ++ii) w[0][jj][ii] = xx[ii] * yy[jj];
+    } else {
+      const double dzz = zt[k] - zt[k - 1];
+      double z2 = (x[2] - zt[k - 1]) / dzz;
+      double zz[2] = {1 - z2, z2};
+      for (int kk = 0; kk < 2; ++kk) for (int jj = 0; jj < 2; ++jj) for (int ii = 0; ii < 2; ++ii)
+        w[kk][jj][ii] = xx[ii] * yy[jj] * zz[kk];
+    }
+  }
+
+  // DRAG_GIDASPOW (drag_gs.f:536-598) with C_DS_SN (drag_mod.f:54).
+  static double drag_gidaspow(double epg, double mug, double rog, double ropg, double vrel, double dpm) {
+    const double LARGE_NUMBER = 1.0e32;
+    double re = mug > 0.0 ? dpm * vrel * ropg / mug : LARGE_NUMBER;
+    if (re == 0.0) return 0.0;
+    if (epg <= 0.8) return 150.0 * (1.0 - epg) * mug / (epg * (dpm * dpm)) + 1.75 * rog * vrel / dpm;
+    double cd = re <= 1000.0 ? 24.0 * (1.0 + 0.15 * std::pow(re, 0.687)) / (re + SMALL_NUMBER) : 0.44;
+    return 0.75 * cd * vrel * ropg * std::pow(epg, -2.65) / dpm;
+  }
+
+  // DRAG_GS_DES0 (drag_gs_des0.f:22-219): gas velocity at the particle from
+  // the 2x2x2 node stencil of its fluid cell, DES_DRAG_GP (drag_gp_des.f:
+  // 97-257, Model A) and FC += F_GP*(u_g - v_p) + P_FORCE*PVOL.
+  void drag() {
+    const double avg = p.no_k ? 0.5 : 0.25;
+    for (int l = 0; l < n; ++l) {
+      int8_t st = state[l];
+      if (st == DEM_STATE_NONEXISTENT || st >= DEM_STATE_NORMAL_GHOST) continue;
+      int i = pijk[4 * (size_t)l], j = pijk[4 * (size_t)l + 1], k = pijk[4 * (size_t)l + 2];
+      if (!fluid_at(i, j, k)) continue;
+      const int iw = i - 1, js = j - 1, kb = p.no_k ? 1 : k - 1;
+      double vst[2][2][2][3];
+      for (int kk = 0; kk < (p.no_k ? 1 : 2); ++kk)
+        for (int jj = 0; jj < 2; ++jj)
+          for (int ii = 0; ii < 2; ++ii) {
+            int I = iw + ii, J = js + jj, K = kb + kk;
+            int c = cijk(I, J, K), ipjk = cijk(I + 1, J, K), ijpk = cijk(I, J + 1, K), ipjpk = cijk(I + 1, J + 1, K);
+            double* v = vst[kk][jj][ii];
+            v[0] = avg * (u_g[c] + u_g[ijpk]);
+            v[1] = avg * (v_g[c] + v_g[ipjk]);
+            if (!p.no_k) {
+              int ijpkp = cijk(I, J + 1, K + 1), ipjkp = cijk(I + 1, J, K + 1), ijkp = cijk(I, J, K + 1);
+              v[0] = v[0] + avg * (u_g[ijkp] + u_g[ijpkp]);
+              v[1] = v[1] + avg * (v_g[ijkp] + v_g[ipjkp]);
+              v[2] = avg * (w_g[c] + w_g[ijpk] + w_g[ipjk] + w_g[ipjpk]);
+            } else {
+              v[2] = 0.0;
+            }
+          }
+      double x[3] = {P(pos, l, 0), P(pos, l, 1), P(pos, l, 2)};
+      double w[2][2][2];
+      weights(i, j, k, x, w);
+      double velfp[3] = {0.0, 0.0, 0.0};
+      for (int kk = 0; kk < (p.no_k ? 1 : 2); ++kk)
+        for (int jj = 0; jj < 2; ++jj)
+          for (int ii = 0; ii < 2; ++ii)
+            for (int c = 0; c < (p.no_k ? 2 : 3); ++c) velfp[c] = velfp[c] + vst[kk][jj][ii][c] * w[kk][jj][ii];
+      double vp[3] = {P(vel, l, 0), P(vel, l, 1), P(vel, l, 2)};
+      const int ijk = cijk(i, j, k);
+      const double epg = ep_g[ijk];
+      double vs[3] = {velfp[0] - vp[0], velfp[1] - vp[1], velfp[2] - vp[2]};
+      double vrel = std::sqrt(dot3(vs, vs));
+      double dpm = 2.0 * rad[l];
+      double dga = drag_gidaspow(epg, g.mu_g, g.ro_g, g.ro_g * epg, vrel, dpm);
+      double pvol = ((4.0 / 3.0) * pi_c) * (rad[l] * (rad[l] * rad[l]));
+      double fgs = dga * pvol;
+      f_gp[l] = (1.0 - g.ur_f_gs) * f_gp[l] + g.ur_f_gs * fgs;
+      for (int c = 0; c < 3; ++c) X(fc, c)[l] = X(fc, c)[l] + f_gp[l] * (velfp[c] - vp[c]);
+      if (!p_force.empty())
+        for (int c = 0; c < 3; ++c) X(fc, c)[l] = X(fc, c)[l] + p_force[3 * (size_t)ijk + c] * pvol;
+    }
+  }
+
+  // COMP_MEAN_FIELDS0 (comp_mean_fields0.f:139-435) + CALC_EPG_DES
+  // (calc_epg_des.f:123-150), one solids phase per particle phase.
+  void comp_mean_fields() {
+    particles_in_cell();
+    const size_t nc = vol_surr.size();
+    const int M = p.n_phases;
+    std::vector<double> rops_node(nc * M, 0.0);
+    rop_s.assign(nc * M, 0.0);
+    for (int k = 1; k <= gk2; ++k)
+      for (int j = 1; j <= gj2; ++j)
+        for (int i = 1; i <= gi2; ++i) {
+          if (!fluid_at(i, j, k)) continue;
+          const int ijk = cijk(i, j, k);
+          const int iw = i - 1, js = j - 1, kb = p.no_k ? 1 : k - 1;
+          for (int q = pic_start[ijk]; q < pic_start[ijk + 1]; ++q) {
+            int np = pic_list[q];
+            double x[3] = {P(pos, np, 0), P(pos, np, 1), P(pos, np, 2)};
+            double w[2][2][2];
+            weights(i, j, k, x, w);
+            const int m = phase[np];
+            const double temp2 = pmass[np];
+            for (int kk = 0; kk < (p.no_k ? 1 : 2); ++kk)
+              for (int jj = 0; jj < 2; ++jj)
+                for (int ii = 0; ii < 2; ++ii) {
+                  int node = cijk(iw + ii, js + jj, kb + kk);
+                  double temp1 = w[kk][jj][ii] * temp2;
+                  rops_node[(size_t)m * nc + node] = rops_node[(size_t)m * nc + node] + temp1;
+                }
+          }
+        }
+    const int kn1 = p.no_k ? 1 : g.kmax + 1;
+    for (int k = 1; k <= kn1; ++k)
+      for (int j = 1; j <= g.jmax + 1; ++j)
+        for (int i = 1; i <= g.imax + 1; ++i) {
+          const int ijk = cijk(i, j, k);
+          if (vol_surr[ijk] == 0.0) continue;
+          for (int m = 0; m < M; ++m) {
+            double dens = rops_node[(size_t)m * nc + ijk] / vol_surr[ijk];
+            for (int kk = k; kk <= (p.no_k ? k : k + 1); ++kk)
+              for (int jj = j; jj <= j + 1; ++jj)
+                for (int ii = i; ii <= i + 1; ++ii) {
+                  int c2 = cijk(ii, jj, kk);
+                  rop_s[(size_t)m * nc + c2] = rop_s[(size_t)m * nc + c2] + dens * vol();
+                }
+          }
+        }
+    for (int k = 1; k <= gk2; ++k)
+      for (int j = 1; j <= gj2; ++j)
+        for (int i = 1; i <= gi2; ++i) {
+          if (!fluid_at(i, j, k)) continue;
+          const int ijk = cijk(i, j, k);
+          double sum_eps = 0.0;
+          for (int m = 0; m < M; ++m) {
+            double& r = rop_s[(size_t)m * nc + ijk];
+            if (r > 0.0) r = r / vol();
+            sum_eps = sum_eps + r / ro_s[m];
+          }
+          ep_g[ijk] = 1.0 - std::min(1.0, sum_eps);
+        }
+  }
+
+  int step_coupled(int nn) {
+    int rc = calc_force();
+    if (rc) return rc;
+    drag();
+    cfnewvalues();
+    bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0);
+    bool anyper = p.periodic[0] || p.periodic[1] || (p.periodic[2] && !p.no_k);
+    if (do_nsearch || anyper) desgrid_pic();
+    if (do_nsearch) neighbour();
+    comp_mean_fields();
+    s_time = s_time + p.dtsolid;
+    steps_done++;
+    return 0;
+  }
+
   // DES_TIME_STEP(NN) for pure DEM (des_time_march.f:342-432).
   int step(int nn) {
     int rc = calc_force();
@@ -1140,14 +1379,57 @@ int orc_get_stats(orc_handle* h, dem_stats* s) {
   return 0;
 }
 
-int orc_set_gas_fields(orc_handle* h, const dem_fluid_grid*, const double*, const double*,
-                       const double*, const double*, const double*) {
-  return h->o.fail(DEM_ERR_STATE, "coupling not available in this build");
+// Coupling.
+int orc_set_gas_fields(orc_handle* h, const dem_fluid_grid* g, const double* ep_g,
+                       const double* u_g, const double* v_g, const double* w_g,
+                       const double* p_force) {
+  Oracle& o = h->o;
+  if (!g || !ep_g || !u_g || !v_g || !w_g) return o.fail(DEM_ERR_ARG, "null gas field");
+  if (!o.have_state) return o.fail(DEM_ERR_STATE, "upload particles first");
+  o.g = *g;
+  o.gas_setup();
+  size_t nc = o.vol_surr.size();
+  o.ep_g.assign(ep_g, ep_g + nc);
+  o.u_g.assign(u_g, u_g + nc);
+  o.v_g.assign(v_g, v_g + nc);
+  o.w_g.assign(w_g, w_g + nc);
+  if (p_force) o.p_force.assign(p_force, p_force + 3 * nc); else o.p_force.clear();
+  for (int m = 0; m < o.p.n_phases; ++m) {
+    if (!(g->ro_s[m] > 0.0)) return o.fail(DEM_ERR_ARG, "ro_s must be positive");
+    o.ro_s[m] = g->ro_s[m];
+  }
+  o.have_gas = true;
+  o.particles_in_cell();
+  return 0;
 }
-int orc_get_mean_fields(orc_handle* h, double*, double*) { return h->o.fail(DEM_ERR_STATE, "coupling not available"); }
-int orc_comp_mean_fields(orc_handle* h) { return h->o.fail(DEM_ERR_STATE, "coupling not available"); }
-int orc_drag_gs_des0(orc_handle* h) { return h->o.fail(DEM_ERR_STATE, "coupling not available"); }
-int orc_step_coupled(orc_handle* h, int32_t, int32_t) { return h->o.fail(DEM_ERR_STATE, "coupling not available"); }
+int orc_get_mean_fields(orc_handle* h, double* ep_g, double* rop_s) {
+  Oracle& o = h->o;
+  if (!o.have_gas) return o.fail(DEM_ERR_STATE, "no gas fields");
+  if (ep_g) std::copy(o.ep_g.begin(), o.ep_g.end(), ep_g);
+  if (rop_s) {
+    if (o.rop_s.empty()) std::fill(rop_s, rop_s + o.vol_surr.size(), 0.0);
+    else std::copy(o.rop_s.begin(), o.rop_s.begin() + o.vol_surr.size(), rop_s);
+  }
+  return 0;
+}
+int orc_comp_mean_fields(orc_handle* h) {
+  if (!h->o.have_gas) return h->o.fail(DEM_ERR_STATE, "no gas fields");
+  h->o.comp_mean_fields();
+  return 0;
+}
+int orc_drag_gs_des0(orc_handle* h) {
+  if (!h->o.have_gas) return h->o.fail(DEM_ERR_STATE, "no gas fields");
+  h->o.drag();
+  return 0;
+}
+int orc_step_coupled(orc_handle* h, int32_t nn_first, int32_t nsteps) {
+  if (!h->o.have_gas) return h->o.fail(DEM_ERR_STATE, "no gas fields");
+  for (int32_t k = 0; k < nsteps; ++k) {
+    int rc = h->o.step_coupled(nn_first + k);
+    if (rc) return rc;
+  }
+  return 0;
+}
 
 // CHECK_SOLIDS_DEM_COLL_LSD (check_solids_dem.f:519-782) and
 // CHECK_SOLIDS_DEM_COLL_HERTZ (798-1122), DEM phases only (MMAX = 0).

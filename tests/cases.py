@@ -84,3 +84,16 @@ def make_system(cls, prm, arr, walls, **kw):
                    arr["omoi"], arr["state"], arr["phase"])
     s.init_neighbors()
     return s
+
+
+def coupled_case(cells=(8, 24, 8), n=1500, **kw):
+    """A small CFD-DEM case on a cells[0] x cells[1] x cells[2] grid of 1 mm cells."""
+    from mfix_dem import configs
+    return configs.coupled(n=n, cells=cells, **kw)
+
+
+def make_coupled(cls, case_tuple, **kw):
+    case, prm, arr, walls, info, grid, fields = case_tuple
+    s = make_system(cls, prm, arr, walls, **kw)
+    s.set_gas_fields(grid, fields["ep_g"], fields["u_g"], fields["v_g"], fields["w_g"])
+    return s

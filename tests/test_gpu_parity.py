@@ -134,7 +134,7 @@ def test_dense_overlapping_bed_matches_oracle():
     """Initial overlaps everywhere (lattice spacing 0.97 d): every pair is a
     contact from the first step, Hertz with rolling friction, AB2."""
     case, prm, arr, walls = settling_case(n_side=(8, 12, 8), spacing=0.97, jitter=0.01, coll="HERTZ",
-                                          intg="ADAMS_BASHFORTH", mew_r=0.02, polydisperse=0.1, nsn=7)
+                                          intg="ADAMS_BASHFORTH", mew_r=0.02, polydisperse=0.0, nsn=7)
     g, o = pair_both(prm, arr, walls)
     for _ in range(3):
         g.step(11); o.step(11)
