@@ -211,7 +211,6 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     clocks = ClockSampler(local)
     p0 = g.pair_count()
     l0 = g.launch_count()
-    g.set_profiling(True)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
@@ -224,11 +223,22 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     barrier()
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    prof = g.profile()
-    g.set_profiling(False)
     launches = g.launch_count() - l0
     p1 = g.pair_count()
     st = g.stats()
+    # kernel times: a second pass of the same length with CUDA events around
+    # every kernel class, launched step by step (events cannot sit inside the
+    # graphs the timed pass replays)
+    g.set_profiling(True)
+    ep0 = torch.cuda.Event(enable_timing=True)
+    ep1 = torch.cuda.Event(enable_timing=True)
+    ep0.record(stream)
+    g.step(args.steps, args.warmup + args.steps + 1)
+    ep1.record(stream)
+    torch.cuda.synchronize()
+    ms_eager = ep0.elapsed_time(ep1)
+    prof = g.profile()
+    g.set_profiling(False)
     ferr1 = g.force_error() if prec == "split" else None
     if ws > 1:
         import torch.distributed as dist
@@ -254,7 +264,8 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
                 "kernel": "force step (k_walls + k_pairs + k_gather with fused integration)",
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_launch,
                 "avg_launch_ms": f_ms / f_n if f_n else None,
-                "share_of_step": f_ms / ms if ms else None,
+                "share_of_step": f_ms / ms_eager if ms_eager else None,
+                "ms_per_step_eager": ms_eager / args.steps,
                 "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]}}
     out = {"value": value, "ms": ms, "n": n, "n_normal": n_normal, "pairs": int(p1), "launches": int(launches),
            "roofline": roofline, "clocks": clk, "contacts": int(st["n_contacts"]), "prm": prm, "info": info,
@@ -273,7 +284,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
                "radius": pinned(arr["radius"]), "pmass": pinned(arr["pmass"]), "omoi": pinned(arr["omoi"]),
                "state": pinned(st_now["state"]), "phase": pinned(arr["phase"])}
         hout = {"pos": hin["pos"], "vel": hin["vel"], "omega": hin["omega"], "state": hin["state"]}
-        nn0 = args.warmup + args.steps + 1
+        nn0 = args.warmup + 2 * args.steps + 1
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)

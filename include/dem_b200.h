@@ -238,6 +238,11 @@ int dem_init_neighbors(dem_handle* h);
  * dem_cfnewvalues. */
 int dem_step(dem_handle* h, int32_t nn_first, int32_t nsteps);
 
+/* dem_step replays whole NEIGHBOR_SEARCH_N-step periods as CUDA graphs when
+ * the handle has a stream of its own (the default) and profiling is off.
+ * on = 0 runs every step launch by launch. */
+int dem_set_graphs(dem_handle* h, int32_t on);
+
 /* Statistics of the current state. */
 int dem_get_stats(dem_handle* h, dem_stats* out);
 

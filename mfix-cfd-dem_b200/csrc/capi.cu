@@ -114,6 +114,13 @@ int fetch_errors(dem_handle* h) {
   return set_err(h, DEM_ERR_STATE, "device error flags set");
 }
 
+void invalidate_graphs(dem_handle* h) {
+  for (auto& g : h->graphs) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+}
+
 void* stage_buffer(dem_handle* h, size_t bytes) {
   if (bytes > h->stage_bytes) {
     if (h->stage) cudaFree(h->stage);
@@ -273,6 +280,8 @@ int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
   A((void**)&h->fcell_cnt, sizeof(int) * (h->dp.nfcell + 1));
   A((void**)&h->fcell_start, sizeof(int) * (h->dp.nfcell + 1));
   A((void**)&h->fcell_list, sizeof(int) * n);
+  A((void**)&h->spos, sizeof(double4) * n);
+  A((void**)&h->sinfo, sizeof(int4) * n);
   A((void**)&h->row_cnt, sizeof(int) * n);
   A((void**)&h->in_cnt, sizeof(int) * n);
   A((void**)&h->in_start, sizeof(int) * (n + 1));
@@ -283,6 +292,7 @@ int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
   A((void**)&h->wall_live, n);
   A((void**)&h->wf, sizeof(double) * 6 * n);
   A((void**)&h->derr, sizeof(DevErr));
+  A((void**)&h->d_np, sizeof(int));
   if (!ok) {
     dem_destroy(h);
     return DEM_ERR_CUDA;
@@ -292,6 +302,11 @@ int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
   memset(h->herr, 0, sizeof(DevErr));
   h->herr->first_rogue = max_pip;
   cudaMemcpy(h->derr, h->herr, sizeof(DevErr), cudaMemcpyHostToDevice);
+  cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, h->dev);
+  // a stream of its own, so that whole rebuild periods can be captured as
+  // CUDA graphs (the legacy default stream cannot be captured)
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) { dem_destroy(h); return DEM_ERR_CUDA; }
+  h->stream = h->own_stream;
   if (ensure_pair_capacity(h, 16 * (long long)n + 1024)) { dem_destroy(h); return DEM_ERR_CUDA; }
   if (cudaDeviceSynchronize() != cudaSuccess) { dem_destroy(h); return DEM_ERR_CUDA; }
   *out = h;
@@ -303,6 +318,7 @@ int dem_destroy(dem_handle* h) {
   cudaSetDevice(h->dev);
   cudaStreamSynchronize(h->stream);
   free_gas(h);
+  invalidate_graphs(h);
   void* ptrs[] = {h->pos4[0], h->pos4[1], h->vel4[0], h->vel4[1], h->omg4[0], h->omg4[1],
                   h->state, h->phase, h->fc, h->tow, h->acc_old, h->rot_acc_old, h->dg_pijk,
                   h->cell_cnt, h->cell_start, h->cell_fill, h->cell_list, h->row_cnt,
@@ -310,17 +326,20 @@ int dem_destroy(dem_handle* h) {
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
                   h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec,
-                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list};
+                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->d_np};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (auto e : h->ev_pool) cudaEventDestroy(e);
   if (h->herr) cudaFreeHost(h->herr);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return 0;
 }
 
 int dem_set_stream(dem_handle* h, void* stream) {
   API_GUARD(h);
+  cudaStreamSynchronize(h->stream);
+  invalidate_graphs(h);
   h->stream = (cudaStream_t)stream;
   return 0;
 }
@@ -427,14 +446,14 @@ int dem_get_ab2_history(dem_handle* h, double* acc_old, double* rot_acc_old, int
 int dem_pair_count(dem_handle* h, int64_t* np) {
   API_GUARD(h);
   if (!np) return DEM_ERR_ARG;
-  *np = h->n_pairs;
+  *np = host_pairs(h);
   return 0;
 }
 
 int dem_download_pairs(dem_handle* h, int32_t* ni, int32_t* nb, double* pf, int64_t cap, int32_t max_pip) {
   API_GUARD(h);
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
-  const long long P = h->n_pairs;
+  const long long P = host_pairs(h);
   if ((nb || pf) && cap < P) return set_err(h, DEM_ERR_CAPACITY, "pair capacity too small");
   if (ni) cudaMemcpyAsync(ni, h->row_end[h->rb], sizeof(int) * h->n, cudaMemcpyDeviceToHost, h->stream);
   if (nb && P) cudaMemcpyAsync(nb, h->nbrs[h->rb], sizeof(int) * P, cudaMemcpyDeviceToHost, h->stream);
@@ -499,6 +518,12 @@ int dem_upload_pairs(dem_handle* h, const int32_t* ni, const int32_t* nb, const 
     cudaMemcpyAsync(h->pft[h->pcur], pf, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, h->stream);
   }
   h->n_pairs = np;
+  h->np_stale = false;
+  {
+    int v = (int)np;
+    cudaMemcpyAsync(h->d_np, &v, sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+  }
   const int T = 256, B = (h->n + T - 1) / T;
   k_owner_from_rows<<<B, T, 0, h->stream>>>(h->n, h->row_end[h->rb], h->pair_owner);
   cudaMemsetAsync(h->in_cnt, 0, sizeof(int) * h->n, h->stream);
@@ -576,27 +601,111 @@ int dem_cfnewvalues(dem_handle* h) {
   return check_cuda(h, cudaStreamSynchronize(h->stream), "cfnewvalues");
 }
 
+// One DES_TIME_STEP(NN) of a pure DEM run: force + integration, then the
+// cell binning (every step with periodic axes) and the neighbour rebuild
+// when NN == 1 or mod(NN, NEIGHBOR_SEARCH_N) == 0 (des_time_march.f:398-414).
+static int step_once(dem_handle* h, int nn) {
+  const DevParams& p = h->dp;
+  const bool anyper = p.per[0] || p.per[1] || (p.per[2] && !p.no_k);
+  cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
+  if (int rc = run_force(h, true)) return rc;
+  const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0);
+  if (do_nsearch || anyper) {
+    if (int rc = run_desgrid_pic(h, do_nsearch)) return rc;
+  }
+  if (do_nsearch) {
+    if (int rc = run_neighbour(h, true)) return rc;
+  }
+  h->s_time = h->s_time + h->prm.dtsolid;
+  h->steps_done++;
+  return 0;
+}
+
+// The NEIGHBOR_SEARCH_N steps NN = m*N+1 .. (m+1)*N (m >= 1) end with the one
+// rebuild of the period and are otherwise identical, so they are captured
+// once as a CUDA graph per combination of buffer parities and replayed.  A
+// replay cannot grow the pair arrays: the capacity is kept at twice the
+// last known pair count before every replay, and a build that still
+// overflows is reported as DEM_ERR_PAIR_OVERFLOW.
+static int replay_period(dem_handle* h, int nn0) {
+  const int nsn = h->prm.neighbor_search_n;
+  const long long P = host_pairs(h);
+  if (2 * P + 1024 > h->pair_cap) {
+    if (int rc = ensure_pair_capacity(h, 2 * P + 1024)) return rc;
+    invalidate_graphs(h);
+  }
+  const int key = (h->cur << 2) | (h->pcur << 1) | h->rb;
+  if (!h->graphs[key]) {
+    cudaGraph_t graph;
+    h->capturing = true;
+    if (int rc = check_cuda(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture")) {
+      h->capturing = false;
+      return rc;
+    }
+    int rc = 0;
+    const int cur0 = h->cur, pcur0 = h->pcur, rb0 = h->rb;
+    const long long sd0 = h->steps_done;
+    const double st0 = h->s_time;
+    const long long l0 = h->launches;
+    for (int j = 0; j < nsn && !rc; ++j) rc = step_once(h, nn0 + j);
+    cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+    h->capturing = false;
+    // capture only recorded the work: restore the bookkeeping, then launch
+    h->cur = cur0; h->pcur = pcur0; h->rb = rb0; h->steps_done = sd0; h->s_time = st0;
+    h->graph_launches += h->launches - l0;
+    h->launches = l0;
+    if (rc) return rc;
+    if (int r2 = check_cuda(h, ce, "end capture")) return r2;
+    cudaGraphExec_t exec;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (int r2 = check_cuda(h, ce, "graph instantiate")) return r2;
+    h->graphs[key] = exec;
+    h->graph_kernels[key] = h->graph_launches;
+    h->graph_launches = 0;
+  }
+  if (int rc = check_cuda(h, cudaGraphLaunch(h->graphs[key], h->stream), "graph launch")) return rc;
+  h->launches += h->graph_kernels[key];
+  // buffer parities and bookkeeping after the period: N force passes flip
+  // the state and history buffers, the rebuild flips the list and history
+  for (int j = 0; j < nsn; ++j) {
+    h->cur = 1 - h->cur;
+    h->pcur = 1 - h->pcur;
+    h->s_time = h->s_time + h->prm.dtsolid;
+    h->steps_done++;
+  }
+  h->pcur = 1 - h->pcur;
+  h->rb = 1 - h->rb;
+  h->first_pass = false;
+  h->np_stale = true;
+  return 0;
+}
+
 int dem_step(dem_handle* h, int32_t nn_first, int32_t nsteps) {
   API_GUARD(h);
   if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
   if (nsteps < 0 || nn_first < 1) return set_err(h, DEM_ERR_ARG, "bad step range");
-  const DevParams& p = h->dp;
-  const bool anyper = p.per[0] || p.per[1] || (p.per[2] && !p.no_k);
-  for (int k = 0; k < nsteps; ++k) {
+  const int nsn = h->prm.neighbor_search_n;
+  const bool graphs_ok = h->stream != nullptr && !h->prof && !h->no_graphs;
+  int k = 0;
+  while (k < nsteps) {
     const int nn = nn_first + k;
-    cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
-    if (int rc = run_force(h, true)) return rc;
-    const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0);
-    if (do_nsearch || anyper) {
-      if (int rc = run_desgrid_pic(h, do_nsearch)) return rc;
+    if (graphs_ok && !h->first_pass && nn > 1 && (nn - 1) % nsn == 0 && nsteps - k >= nsn) {
+      if (int rc = replay_period(h, nn)) return rc;
+      k += nsn;
+    } else {
+      if (int rc = step_once(h, nn)) return rc;
+      ++k;
     }
-    if (do_nsearch) {
-      if (int rc = run_neighbour(h, true)) return rc;
-    }
-    h->s_time = h->s_time + h->prm.dtsolid;
-    h->steps_done++;
   }
   return fetch_errors(h);
+}
+
+int dem_set_graphs(dem_handle* h, int32_t on) {
+  API_GUARD(h);
+  h->no_graphs = on == 0;
+  if (h->no_graphs) invalidate_graphs(h);
+  return 0;
 }
 
 int dem_get_stats(dem_handle* h, dem_stats* s) {
@@ -629,7 +738,7 @@ int dem_get_stats(dem_handle* h, dem_stats* s) {
   for (int b = 0; b < B; ++b) for (int k = 0; k < 3; ++k) gt[k] += part[(size_t)3 * b + k];
   s->n_normal = (int64_t)nn;
   for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn > 0 ? gt[c] / nn : 0.0; }
-  s->n_pairs = h->n_pairs;
+  s->n_pairs = host_pairs(h);
   s->n_contacts = (int64_t)h->herr->n_contacts;
   s->n_wall_contacts = (int64_t)h->herr->n_wall_contacts;
   s->n_rogue_removed = (int64_t)h->herr->rogue_removed;

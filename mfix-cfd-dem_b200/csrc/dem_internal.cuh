@@ -130,10 +130,21 @@ struct dem_handle {
   int* fcell_cnt = nullptr;   // nfcell+1
   int* fcell_start = nullptr; // nfcell+1
   int* fcell_list = nullptr;  // n
+  double4* spos = nullptr;    // n: positions in search-cell order (pair build)
+  int4* sinfo = nullptr;      // n: (particle, DES cell, state, search cell) in that order
 
   // pairs
   long long pair_cap = 0;
-  long long n_pairs = 0;
+  long long n_pairs = 0;      // host copy of the pair count (valid when !np_stale)
+  bool np_stale = false;      // the last build ran without reading the count back
+  int* d_np = nullptr;        // device pair count (persistent pair kernels read it)
+  int n_sm = 148;             // multiprocessors of the device
+  bool capturing = false;     // inside a CUDA graph capture: no host syncs
+  cudaStream_t own_stream = nullptr;
+  cudaGraphExec_t graphs[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  long long graph_launches = 0;
+  long long graph_kernels[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // kernels per graph replay
+  bool no_graphs = false;
   int* row_cnt = nullptr;     // n
   int* row_end[2] = {nullptr, nullptr};   // n (current / previous build)
   int* nbrs[2] = {nullptr, nullptr};      // cap
@@ -211,6 +222,13 @@ int ensure_pair_capacity(dem_handle* h, long long need);
 int fetch_errors(dem_handle* h);
 void* stage_buffer(dem_handle* h, size_t bytes);
 void free_gas(dem_handle* h);                   // coupling.cu
+long long host_pairs(dem_handle* h);            // pair count on the host (syncs when stale)
+void invalidate_graphs(dem_handle* h);
+
+// Grid of the persistent pair kernels: a fixed number of resident blocks.
+inline unsigned pair_grid(const dem_handle* h, int threads) {
+  return (unsigned)(h->n_sm * (2048 / threads));
+}
 
 // Brackets the kernels issued in its scope with CUDA events when the
 // handle's profiling is on.

@@ -379,15 +379,18 @@ k_walls(DevParams p, WallCtx w, const double4* __restrict__ pos4, const double4*
 // read back in kernel 3.
 template <int COLL>
 __global__ void __launch_bounds__(256)
-k_pairs(DevParams p, long long np, const int* __restrict__ owner, const int* __restrict__ nbrs,
+k_pairs(DevParams p, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
         const double4* __restrict__ pos4, const double4* __restrict__ vel4, const double4* __restrict__ omg4,
         const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
         const double* __restrict__ pft_in, double* __restrict__ pft_out,
         uint8_t* __restrict__ pflag, PairRec* __restrict__ prec, DevErr* __restrict__ err) {
-  const long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // persistent grid-stride loop over the device-side pair count (the grid
+  // size does not depend on the list, so the launch can live in a graph)
+  const long long np = min((long long)*d_np, cap);
+  const long long stride = (long long)gridDim.x * blockDim.x;
   unsigned long long ncont = 0;
   unsigned eflags = 0;
-  if (cc < np) {
+  for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
     const int ll = owner[cc], i = nbrs[cc];
     const double* pi = pft_in + 3 * cc;
     double pin[3] = {pi[0], pi[1], pi[2]};
@@ -626,10 +629,9 @@ static void launch_walls_pairs(dem_handle* h, bool walls, bool pairs) {
                                           h->state, h->wall_live, h->wf, h->derr);
     DEM_LAUNCH(h);
   }
-  if (pairs && h->n_pairs > 0) {
+  if (pairs) {
     const int T = 256;
-    const unsigned B = (unsigned)((h->n_pairs + T - 1) / T);
-    k_pairs<COLL><<<B, T, 0, h->stream>>>(h->dp, h->n_pairs, h->pair_owner, h->nbrs[h->rb], h->pos4[c],
+    k_pairs<COLL><<<pair_grid(h, T), T, 0, h->stream>>>(h->dp, h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c],
                                           h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc],
                                           h->pft[1 - pc], h->pflag, h->prec, h->derr);
     DEM_LAUNCH(h);

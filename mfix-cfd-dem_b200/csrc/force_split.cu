@@ -38,16 +38,19 @@ struct Comp3 {  // Neumaier-compensated FP32 sum of a 3-vector
 
 template <int COLL>
 __global__ void __launch_bounds__(256)
-k_pairs_split(DevParams p, long long np, const int* __restrict__ owner, const int* __restrict__ nbrs,
+k_pairs_split(DevParams p, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
               const double4* __restrict__ pos4, const double4* __restrict__ vel4,
               const double4* __restrict__ omg4, const int8_t* __restrict__ state,
               const uint8_t* __restrict__ phase, const double* __restrict__ pft_in,
               double* __restrict__ pft_out, uint8_t* __restrict__ pflag, PairRec32* __restrict__ prec,
               DevErr* __restrict__ err) {
-  const long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // persistent grid-stride loop over the device-side pair count (the grid
+  // size does not depend on the list, so the launch can live in a graph)
+  const long long np = min((long long)*d_np, cap);
+  const long long stride = (long long)gridDim.x * blockDim.x;
   unsigned long long ncont = 0;
   unsigned eflags = 0;
-  if (cc < np) {
+  for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
     const int ll = owner[cc], i = nbrs[cc];
     const double* pi = pft_in + 3 * cc;
     const double pin[3] = {pi[0], pi[1], pi[2]};
@@ -269,16 +272,15 @@ k_gather_split(DevParams p, const double4* __restrict__ pos_c, const double4* __
 }
 
 void launch_pairs_split(dem_handle* h) {
-  if (h->n_pairs <= 0) return;
   const int c = h->cur, pc = h->pcur;
   const int T = 256;
-  const unsigned B = (unsigned)((h->n_pairs + T - 1) / T);
+  const unsigned B = pair_grid(h, T);
   if (h->dp.coll == DEM_COLL_HERTZ)
-    k_pairs_split<DEM_COLL_HERTZ><<<B, T, 0, h->stream>>>(h->dp, h->n_pairs, h->pair_owner, h->nbrs[h->rb],
+    k_pairs_split<DEM_COLL_HERTZ><<<B, T, 0, h->stream>>>(h->dp, h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb],
         h->pos4[c], h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
         (PairRec32*)h->prec, h->derr);
   else
-    k_pairs_split<DEM_COLL_LSD><<<B, T, 0, h->stream>>>(h->dp, h->n_pairs, h->pair_owner, h->nbrs[h->rb],
+    k_pairs_split<DEM_COLL_LSD><<<B, T, 0, h->stream>>>(h->dp, h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb],
         h->pos4[c], h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
         (PairRec32*)h->prec, h->derr);
   DEM_LAUNCH(h);

@@ -67,25 +67,43 @@ __global__ void k_delete_rogue(DevParams p, int8_t* __restrict__ state, const in
 // kept neighbour carries its stencil rank ((lk, lj, li) order); the fill
 // pass inserts it into the row sorted by (rank, index), which is the order
 // of the reference's cell-by-cell scan.
+// The search runs over a cell-sorted copy of the candidate data: sinfo[q] =
+// (particle, DES cell, state, search cell) and spos[q] = (x, y, z, r) in the
+// order of the search-grid cell lists.  Thread q handles particle sinfo[q].x,
+// so a warp holds spatially adjacent particles that scan the same cells, and
+// every candidate read is a contiguous run of the sorted arrays.
+__global__ void k_sorted_copy(int n, const int* __restrict__ n_exist, const int* __restrict__ flist,
+                              const double4* __restrict__ pos4, const int8_t* __restrict__ state,
+                              const int* __restrict__ dg_pijk, const int* __restrict__ fkey,
+                              double4* __restrict__ spos, int4* __restrict__ sinfo) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n || q >= *n_exist) return;
+  const int i = flist[q];
+  spos[q] = pos4[i];
+  sinfo[q] = make_int4(i, dg_pijk[i], (int)state[i], fkey[i]);
+}
+
 template <bool FILL>
 __global__ void __launch_bounds__(128)
-k_neigh(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict__ state,
-        const int* __restrict__ dg_pijk, const int* __restrict__ fkey, const int* __restrict__ fstart,
-        const int* __restrict__ flist, const DevErr* __restrict__ err, int* __restrict__ row_cnt,
-        int* __restrict__ row_se, int* __restrict__ nbrs, uint8_t* __restrict__ rank_buf,
-        int* __restrict__ owner, long long cap) {
-  const int cur = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cur >= p.n) return;
+k_neigh(DevParams p, const int* __restrict__ n_exist, const double4* __restrict__ spos,
+        const int4* __restrict__ sinfo, const int* __restrict__ fstart, const DevErr* __restrict__ err,
+        int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
+        uint8_t* __restrict__ rank_buf, int* __restrict__ owner, long long cap) {
+  const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q0 >= p.n || q0 >= *n_exist) return;
+  const int4 me = sinfo[q0];
+  const int cur = me.x;
+  if (me.z != DEM_STATE_NORMAL || cur >= err->first_rogue) return;
   int start = 0;
-  if (FILL) start = row_se[cur];
+  if (FILL) start = (int)min((long long)row_se[cur], cap);
   int cnt = 0;
-  if (state[cur] == DEM_STATE_NORMAL && cur < err->first_rogue) {
-    const int lijk = dg_pijk[cur];
+  {
+    const int lijk = me.y;
     const int lic = dg_iof(p, lijk), ljc = dg_jof(p, lijk), lkc = dg_kof(p, lijk);
     const int rc[3] = {lic, ljc, lkc};
     const int s1[3] = {p.istart1, p.jstart1, p.kstart1}, e1[3] = {p.iend1, p.jend1, p.kend1};
     const int ncl[3] = {p.iend1 - p.istart1 + 1, p.jend1 - p.jstart1 + 1, p.kend1 - p.kstart1 + 1};
-    const double4 cp = pos4[cur];
+    const double4 cp = spos[q0];
     const double cpos[3] = {cp.x, cp.y, cp.z};
     const double fr = p.factor_rlm, mr = p.max_radius;
     int lo_off[3] = {1, 1, 1}, hi_off[3] = {1, 1, 1};
@@ -98,14 +116,13 @@ k_neigh(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict_
         if (off >= 0.5) lo_off[ax] = 0; else hi_off[ax] = 0;
       }
     }
-    const int key = fkey[cur];
+    const int key = me.w;
     const int fk = key / p.fc2, fi = (key % p.fc2) / p.fc1, fj = key % p.fc1;
     const int kr = p.no_k ? 0 : 1;
     for (int dk = -kr; dk <= kr; ++dk)
     for (int dj = -1; dj <= 1; ++dj)
     for (int di = -1; di <= 1; ++di) {
       int g[3] = {fi + di, fj + dj, fk + dk};
-      const int d[3] = {di, dj, dk};
       bool skip = false;
       for (int ax = 0; ax < 3; ++ax) {
         if (ax == 2 && p.no_k) break;
@@ -115,19 +132,18 @@ k_neigh(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict_
         } else if (g[ax] < 0 || g[ax] > p.fn[ax] + 1) {
           skip = true;
         }
-        (void)d;
       }
       if (skip) continue;
       const int cell = g[2] * p.fc2 + g[0] * p.fc1 + g[1];
       const int qs = fstart[cell], qe = fstart[cell + 1];
       for (int q = qs; q < qe; ++q) {
-        const int nb = flist[q];
+        const int4 o = sinfo[q];
+        const int nb = o.x;
         if (nb == cur) continue;
-        const int8_t sn = state[nb];
-        if (nb < cur && sn == DEM_STATE_NORMAL) continue;
-        if (sn == DEM_STATE_NONEXISTENT) continue;
+        if (nb < cur && o.z == DEM_STATE_NORMAL) continue;
+        if (o.z == DEM_STATE_NONEXISTENT) continue;
         // position of the neighbour's DES cell in the reference stencil
-        const int nijk = dg_pijk[nb];
+        const int nijk = o.y;
         const int nc[3] = {dg_iof(p, nijk), dg_jof(p, nijk), dg_kof(p, nijk)};
         int rel[3];
         double sh[3] = {0.0, 0.0, 0.0};
@@ -145,7 +161,7 @@ k_neigh(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict_
           rel[ax] = r;
         }
         if (!in_stencil) continue;
-        const double4 np_ = pos4[nb];
+        const double4 np_ = spos[q];
         const double srad = fr * (cp.w + np_.w);
         double px = np_.x, py = np_.y, pz = np_.z;
         if (sh[0] != 0.0) px = px + sh[0];
@@ -176,7 +192,7 @@ k_neigh(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict_
       }
     }
   }
-  if (FILL) row_se[cur] = start + cnt;   // start -> end pointer
+  if (FILL) row_se[cur] = (int)min((long long)start + cnt, cap);   // start -> end pointer
   else row_cnt[cur] = cnt;
 }
 
@@ -203,19 +219,29 @@ __global__ void k_remap(int n, const int* __restrict__ row_end, const int* __res
   }
 }
 
-__global__ void k_in_count(long long np, const int* __restrict__ nbrs, int* __restrict__ in_cnt) {
-  long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (cc >= np) return;
-  atomicAdd(&in_cnt[nbrs[cc]], 1);
+__global__ void k_set_int(int* __restrict__ p, int v) { *p = v; }
+
+// Keeps every pair-indexed kernel inside the allocation when a build needed
+// more than the capacity (only possible inside a captured step, which cannot
+// grow the arrays); the overflow is reported as DEM_ERR_PAIR_OVERFLOW.
+__global__ void k_clamp_np(int* __restrict__ d_np, long long cap, DevErr* __restrict__ err) {
+  if (*d_np > cap) { *d_np = (int)cap; atomicOr(&err->flags, EF_PAIR_CAP); }
 }
 
-__global__ void k_in_fill(long long np, const int* __restrict__ nbrs, const int* __restrict__ owner,
+__global__ void k_in_count(const int* __restrict__ d_np, const int* __restrict__ nbrs, int* __restrict__ in_cnt) {
+  const long long np = *d_np, stride = (long long)gridDim.x * blockDim.x;
+  for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride)
+    atomicAdd(&in_cnt[nbrs[cc]], 1);
+}
+
+__global__ void k_in_fill(const int* __restrict__ d_np, const int* __restrict__ nbrs, const int* __restrict__ owner,
                           const int* __restrict__ in_start, int* __restrict__ in_fill, int2* __restrict__ in_pair) {
-  long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (cc >= np) return;
-  int j = nbrs[cc];
-  int slot = atomicAdd(&in_fill[j], 1);
-  in_pair[in_start[j] + slot] = make_int2(owner[cc], (int)cc);
+  const long long np = *d_np, stride = (long long)gridDim.x * blockDim.x;
+  for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
+    const int j = nbrs[cc];
+    const int slot = atomicAdd(&in_fill[j], 1);
+    in_pair[in_start[j] + slot] = make_int2(owner[cc], (int)cc);
+  }
 }
 
 // incoming pairs of each particle in ascending pair index (= owner order)
@@ -235,7 +261,7 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   if (need <= h->pair_cap) return 0;
   long long cap = h->pair_cap > 0 ? h->pair_cap : 1024;
   while (cap < need) cap *= 2;
-  const long long old = h->n_pairs;
+  const long long old = h->pair_cap;  // the whole old allocation (the count may be stale)
   int* nb[2]; double* pf[2]; int2* inp; int* own; uint8_t* pfl; PairRec* prc;
   for (int b = 0; b < 2; ++b) {
     if (int rc = check_cuda(h, cudaMalloc(&nb[b], sizeof(int) * cap), "cudaMalloc nbrs")) return rc;
@@ -257,6 +283,7 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   cudaFree(h->in_pair); cudaFree(h->pair_owner); cudaFree(h->pflag); cudaFree(h->prec);
   h->in_pair = inp; h->pair_owner = own; h->pflag = pfl; h->prec = prc;
   h->pair_cap = cap;
+  invalidate_graphs(h);  // captured steps point at the old arrays
   return check_cuda(h, cudaGetLastError(), "grow pairs");
 }
 
@@ -266,29 +293,35 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   const int n = h->n, T = 128, B = (n + T - 1) / T;
   DevErr* e = h->derr;
   // first_rogue := n
-  {
-    int v = n;
-    if (int rc = check_cuda(h, cudaMemcpyAsync(&e->first_rogue, &v, sizeof(int), cudaMemcpyHostToDevice, h->stream), "copy")) return rc;
-    if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
-  }
+  k_set_int<<<1, 1, 0, h->stream>>>(&e->first_rogue, n);
+  DEM_LAUNCH(h);
   k_find_rogue<<<B, T, 0, h->stream>>>(p, h->state, h->dg_pijk, e);
   DEM_LAUNCH(h);
   const int nb = 1 - h->rb;  // new list goes into the other buffer
-  k_neigh<false><<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, h->fcell_key,
-                                         h->fcell_start, h->fcell_list, e, h->row_cnt, nullptr, nullptr,
-                                         nullptr, nullptr, 0);
+  const int* n_exist = h->fcell_start + p.nfcell;
+  k_sorted_copy<<<B, T, 0, h->stream>>>(n, n_exist, h->fcell_list, h->pos4[h->cur], h->state, h->dg_pijk,
+                                        h->fcell_key, h->spos, h->sinfo);
   DEM_LAUNCH(h);
-  // delete rogue particles only after every row has been counted with the
-  // states the serial loop saw
-  int* total = h->cell_fill;  // scratch int on device (cell_fill is free here)
-  if (int rc = exclusive_scan(h, h->row_cnt, h->row_end[nb], n, total)) return rc;
-  int P = 0;
-  if (int rc = check_cuda(h, cudaMemcpyAsync(&P, total, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "copy P")) return rc;
-  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
-  if (int rc = ensure_pair_capacity(h, (long long)P + 1)) return rc;
-  k_neigh<true><<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, h->fcell_key,
-                                        h->fcell_start, h->fcell_list, e, nullptr, h->row_end[nb],
-                                        h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->row_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
+  k_neigh<false><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
+                                         nullptr, nullptr, nullptr, nullptr, 0);
+  DEM_LAUNCH(h);
+  if (int rc = exclusive_scan(h, h->row_cnt, h->row_end[nb], n, h->d_np)) return rc;
+  if (!h->capturing) {
+    // eager steps read the count back and grow the arrays when needed
+    int P = 0;
+    if (int rc = check_cuda(h, cudaMemcpyAsync(&P, h->d_np, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "copy P")) return rc;
+    if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
+    if (int rc = ensure_pair_capacity(h, (long long)P + 1)) return rc;
+    h->n_pairs = P;
+    h->np_stale = false;
+  } else {
+    h->np_stale = true;
+  }
+  k_neigh<true><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
+                                        h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+  DEM_LAUNCH(h);
+  k_clamp_np<<<1, 1, 0, h->stream>>>(h->d_np, h->pair_cap, e);
   DEM_LAUNCH(h);
   k_delete_rogue<<<B, T, 0, h->stream>>>(p, h->state, h->dg_pijk, h->pos4[h->cur], h->vel4[h->cur],
                                          h->omg4[h->cur], h->fc, h->tow, h->wall_fid, e);
@@ -300,27 +333,31 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   DEM_LAUNCH(h);
   h->rb = nb;
   h->pcur = pn;
-  h->n_pairs = P;
   h->have_pairs = true;
-  // transpose
+  // transpose: incoming pairs of every particle, ascending owner
+  const int TP = 256;
+  const unsigned BP = pair_grid(h, TP);
   if (int rc = check_cuda(h, cudaMemsetAsync(h->in_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
-  if (P > 0) {
-    const int TP = 256;
-    const long long BP = ((long long)P + TP - 1) / TP;
-    k_in_count<<<(unsigned)BP, TP, 0, h->stream>>>(P, h->nbrs[nb], h->in_cnt);
-    DEM_LAUNCH(h);
-  }
+  k_in_count<<<BP, TP, 0, h->stream>>>(h->d_np, h->nbrs[nb], h->in_cnt);
+  DEM_LAUNCH(h);
   if (int rc = exclusive_scan(h, h->in_cnt, h->in_start, n, h->in_start + n)) return rc;
-  if (P > 0) {
-    const int TP = 256;
-    const long long BP = ((long long)P + TP - 1) / TP;
-    if (int rc = check_cuda(h, cudaMemsetAsync(h->in_fill, 0, sizeof(int) * n, h->stream), "memset")) return rc;
-    k_in_fill<<<(unsigned)BP, TP, 0, h->stream>>>(P, h->nbrs[nb], h->pair_owner, h->in_start, h->in_fill, h->in_pair);
-    DEM_LAUNCH(h);
-    k_in_sort<<<B, T, 0, h->stream>>>(n, h->in_start, h->in_pair);
-    DEM_LAUNCH(h);
-  }
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->in_fill, 0, sizeof(int) * n, h->stream), "memset")) return rc;
+  k_in_fill<<<BP, TP, 0, h->stream>>>(h->d_np, h->nbrs[nb], h->pair_owner, h->in_start, h->in_fill, h->in_pair);
+  DEM_LAUNCH(h);
+  k_in_sort<<<B, T, 0, h->stream>>>(n, h->in_start, h->in_pair);
+  DEM_LAUNCH(h);
   return check_cuda(h, cudaGetLastError(), "neighbour");
+}
+
+long long host_pairs(dem_handle* h) {
+  if (h->np_stale) {
+    int P = 0;
+    cudaMemcpyAsync(&P, h->d_np, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    cudaStreamSynchronize(h->stream);
+    h->n_pairs = P;
+    h->np_stale = false;
+  }
+  return h->n_pairs;
 }
 
 }  // namespace demb

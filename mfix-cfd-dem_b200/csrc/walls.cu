@@ -161,6 +161,7 @@ __global__ void k_edge_flags(int ncell, const int* __restrict__ start, const Fac
 
 int run_bin_facets(dem_handle* h, const double* vf, const double* nfort, int nf) {
   const DevParams& p = h->dp;
+  invalidate_graphs(h);
   cudaFree(h->vertex); cudaFree(h->norm_face); cudaFree(h->ignore_edge); cudaFree(h->fbin);
   h->vertex = nullptr; h->norm_face = nullptr; h->ignore_edge = nullptr; h->fbin = nullptr;
   h->nf = nf;

@@ -179,6 +179,7 @@ DEM_ONLY = {
     "set_stream": (C.c_int, [_P, C.c_void_p]),
     "force_error": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "set_profiling": (C.c_int, [_P, C.c_int32]),
+    "set_graphs": (C.c_int, [_P, C.c_int32]),
     "get_profile": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
 }
 

@@ -229,6 +229,9 @@ class DemSystem:
         self.nn = first + nsteps - 1
 
     # ---- CUDA-only ---------------------------------------------------
+    def set_graphs(self, on: bool):
+        self._call("set_graphs", self._h, C.c_int32(1 if on else 0))
+
     def set_profiling(self, on: bool):
         self._call("set_profiling", self._h, C.c_int32(1 if on else 0))
 

@@ -141,3 +141,29 @@ def test_dense_overlapping_bed_matches_oracle():
         compare_state(g, o, exact=True)
         compare_pairs(g, o)
     assert g.stats()["n_contacts"] == o.stats()["n_contacts"] > 0
+
+
+@pytest.mark.parametrize("coll,intg,periodic", [("HERTZ", "EULER", (False, False, False)),
+                                                ("LSD", "ADAMS_BASHFORTH", (True, False, True))])
+def test_graph_replay_matches_eager_and_oracle(coll, intg, periodic):
+    """dem_step replays whole NEIGHBOR_SEARCH_N periods as CUDA graphs; the
+    result must not differ from launching step by step, nor from the oracle."""
+    from mfix_dem import GpuSystem
+    from oracle_ffi import OracleSystem
+    kw = dict(n_side=(10, 10, 10), box=(12e-3, 40e-3, 12e-3), spacing=1.0, coll=coll, intg=intg,
+              periodic=periodic, nsn=5, vmax=0.3)
+    case, prm, arr, walls = settling_case(**kw)
+    g1 = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    g2 = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    g2.set_graphs(False)
+    o = make_system(OracleSystem, prm, arr, walls)
+    for s in (g1, g2, o):
+        s.step(1)
+        s.step(33)
+    l0 = g1.launch_count()
+    g1.step(10); g2.step(10); o.step(10)
+    assert g1.launch_count() > l0
+    compare_state(g1, o, exact=True)
+    compare_state(g2, o, exact=True)
+    compare_pairs(g1, o)
+    assert g1.stats()["n_contacts"] == o.stats()["n_contacts"]
