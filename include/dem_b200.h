@@ -246,6 +246,26 @@ int dem_set_graphs(dem_handle* h, int32_t on);
 /* Statistics of the current state. */
 int dem_get_stats(dem_handle* h, dem_stats* out);
 
+/* The statistics of dem_get_stats, bit for bit, computed without allocating
+ * anything: no cudaMalloc or cudaFree and no host heap.  No counterpart in
+ * the reference.  It is for callers that must not allocate while particles
+ * are being stepped: cudaMalloc/cudaFree can synchronise the whole device and
+ * so stall the streams of other handles on the same GPU, and a caller that
+ * runs systems under a fixed device-memory budget cannot let a statistics
+ * buffer grow with the system (dem_get_stats grows its buffer on demand).
+ *
+ * Its scratch is one static device array of the library, sized for
+ * DEM_STATS_NOALLOC_MAX_PARTICLES particles (about 2 MiB, held on every GPU
+ * that loads the library until the process exits).  Handles with more
+ * particles get DEM_ERR_CAPACITY.  The first call made for a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture begins.  All calls on a device share the array:
+ * calls whose kernels overlap on the GPU (for example from two host threads
+ * on handles with different streams) race and must be serialised by the
+ * caller.  The call synchronises the handle's stream before it returns. */
+#define DEM_STATS_NOALLOC_MAX_PARTICLES (1 << 23)
+int dem_get_stats_noalloc(dem_handle* h, dem_stats* out);
+
 /* Number of kernels this handle has launched so far (for launch accounting). */
 int dem_launch_count(const dem_handle* h, int64_t* count);
 

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 using namespace demb;
 
@@ -226,6 +227,49 @@ static void fill_devparams(dem_handle* h) {
   p.fc1 = p.fn[1] + 2;
   p.fc2 = p.fc1 * (p.fn[0] + 2);
   p.nfcell = p.fc2 * (q.no_k ? 1 : p.fn[2] + 2);
+}
+
+// ---- scratch of dem_get_stats_noalloc --------------------------------------
+// Per-block partial sums of the two statistics passes (8 columns for the
+// first, 3 for the second), followed by the 8 block-ordered totals.  The
+// array is static device memory of the library: every GPU that loads it
+// holds STATS_SCRATCH_DOUBLES * 8 bytes (2 MiB for 2^23 particles) until the
+// process exits.  All calls on a device share it and it keeps what the last
+// call left there; nothing in it has to start at zero, because each call
+// writes every element it reads earlier on the same stream.
+constexpr int STATS_NOALLOC_BLOCKS = (DEM_STATS_NOALLOC_MAX_PARTICLES + STAT_T - 1) / STAT_T;
+constexpr size_t STATS_TOTAL_OFF = (size_t)8 * STATS_NOALLOC_BLOCKS;
+constexpr size_t STATS_SCRATCH_DOUBLES = STATS_TOTAL_OFF + 8;
+static __device__ __align__(256) double g_stats_scratch[STATS_SCRATCH_DOUBLES];
+
+// Adds the partials of nb blocks in block order (the order dem_get_stats
+// adds them on the host), one thread per column.
+__global__ void k_stats_total(int nb, int ncol, const double* __restrict__ part, double* __restrict__ total) {
+  const int k = threadIdx.x;
+  if (k >= ncol) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += part[(size_t)ncol * b + k];
+  total[k] = s;
+}
+
+// Device address of g_stats_scratch on each device.  In host code the name
+// g_stats_scratch is only a stand-in for the symbol, not a device address;
+// the address is looked up with cudaGetSymbolAddress, once per device, with
+// that device current, on the first call made for it.
+constexpr int STATS_MAX_DEVICES = 64;
+static std::mutex g_stats_mu;
+static double* g_stats_ptr[STATS_MAX_DEVICES] = {};
+
+static int stats_scratch(dem_handle* h, double** out) {
+  if (h->dev < 0 || h->dev >= STATS_MAX_DEVICES) return set_err(h, DEM_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_stats_mu);
+  if (!g_stats_ptr[h->dev]) {
+    void* p = nullptr;
+    if (int rc = check_cuda(h, cudaGetSymbolAddress(&p, g_stats_scratch), "cudaGetSymbolAddress(stats scratch)")) return rc;
+    g_stats_ptr[h->dev] = static_cast<double*>(p);
+  }
+  *out = g_stats_ptr[h->dev];
+  return 0;
 }
 
 #define API_GUARD(h) do { if (!(h)) return DEM_ERR_ARG; cudaSetDevice((h)->dev); } while (0)
@@ -736,6 +780,60 @@ int dem_get_stats(dem_handle* h, dem_stats* s) {
   if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
   double gt[3] = {0, 0, 0};
   for (int b = 0; b < B; ++b) for (int k = 0; k < 3; ++k) gt[k] += part[(size_t)3 * b + k];
+  s->n_normal = (int64_t)nn;
+  for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn > 0 ? gt[c] / nn : 0.0; }
+  s->n_pairs = host_pairs(h);
+  s->n_contacts = (int64_t)h->herr->n_contacts;
+  s->n_wall_contacts = (int64_t)h->herr->n_wall_contacts;
+  s->n_rogue_removed = (int64_t)h->herr->rogue_removed;
+  s->steps_done = h->steps_done;
+  s->kinetic_energy = sum[6];
+  s->bed_height = sum[4] > 0 ? sum[5] / sum[4] : 0.0;
+  s->s_time = h->s_time;
+  return 0;
+}
+
+// The same statistics as dem_get_stats from the same two kernels and the
+// same block-ordered sums, with every intermediate kept in g_stats_scratch:
+// no device or host allocation on any call.
+int dem_get_stats_noalloc(dem_handle* h, dem_stats* s) {
+  API_GUARD(h);
+  if (!s) return DEM_ERR_ARG;
+  if (h->n > DEM_STATS_NOALLOC_MAX_PARTICLES) {
+    char b[200];
+    snprintf(b, sizeof b, "dem_get_stats_noalloc: %d particles exceed its limit of %d (DEM_STATS_NOALLOC_MAX_PARTICLES)",
+             h->n, (int)DEM_STATS_NOALLOC_MAX_PARTICLES);
+    return set_err(h, DEM_ERR_CAPACITY, b);
+  }
+  double* scr = nullptr;
+  if (int rc = stats_scratch(h, &scr)) return rc;
+  memset(s, 0, sizeof *s);
+  const int T = STAT_T, B = (h->n + T - 1) / T;
+  double* tot = scr + STATS_TOTAL_OFF;
+  double sum[8];
+  if (B > 0) {
+    k_stats1<<<B, T, 0, h->stream>>>(h->n, h->pos4[h->cur], h->vel4[h->cur], h->state, scr);
+    h->launches++;
+  }
+  k_stats_total<<<1, 32, 0, h->stream>>>(B, 8, scr, tot);
+  h->launches++;
+  if (int rc = check_cuda(h, cudaGetLastError(), "stats launch")) return rc;
+  cudaMemcpyAsync(sum, tot, sizeof sum, cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
+  const double nn = sum[0];
+  double mv[3] = {0, 0, 0};
+  if (nn > 0) for (int c = 0; c < 3; ++c) mv[c] = sum[1 + c] / nn;
+  if (B > 0) {
+    k_stats2<<<B, T, 0, h->stream>>>(h->n, h->vel4[h->cur], h->state, mv[0], mv[1], mv[2], scr);
+    h->launches++;
+  }
+  k_stats_total<<<1, 32, 0, h->stream>>>(B, 3, scr, tot);
+  h->launches++;
+  if (int rc = check_cuda(h, cudaGetLastError(), "stats launch")) return rc;
+  double gt[3];
+  cudaMemcpyAsync(gt, tot, sizeof gt, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(h->herr, h->derr, sizeof(DevErr), cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
   s->n_normal = (int64_t)nn;
   for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn > 0 ? gt[c] / nn : 0.0; }
   s->n_pairs = host_pairs(h);

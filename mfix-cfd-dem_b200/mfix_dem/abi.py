@@ -181,7 +181,10 @@ DEM_ONLY = {
     "set_profiling": (C.c_int, [_P, C.c_int32]),
     "set_graphs": (C.c_int, [_P, C.c_int32]),
     "get_profile": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "get_stats_noalloc": (C.c_int, [_P, C.POINTER(DemStats)]),
 }
+
+DEM_STATS_NOALLOC_MAX_PARTICLES = 1 << 23
 
 
 def bind(lib, prefix, extra=None):

@@ -201,6 +201,13 @@ class DemSystem:
         self._call("get_stats", self._h, C.byref(s))
         return s.as_dict()
 
+    def stats_noalloc(self) -> dict:
+        """Same statistics through dem_get_stats_noalloc (static scratch,
+        no allocation; CUDA library only)."""
+        s = abi.DemStats()
+        self._call("get_stats_noalloc", self._h, C.byref(s))
+        return s.as_dict()
+
     # ---- coupling ----------------------------------------------------
     def set_gas_fields(self, grid: abi.DemFluidGrid, ep_g, u_g, v_g, w_g, p_force=None):
         ep_g = np.ascontiguousarray(ep_g, dtype=np.float64)
