@@ -331,6 +331,76 @@ int dem_drag_gs_des0(dem_handle* h);
  * particles-in-cell and mean fields. */
 int dem_step_coupled(dem_handle* h, int32_t nn_first, int32_t nsteps);
 
+/* ---- batches of independent systems ----------------------------------
+ * No counterpart in the reference, which runs one system per process.  A
+ * batch handle holds many independent dry DEM systems of any sizes; every
+ * kernel of a step runs once over all of them, each particle with its own
+ * system's parameters (DES grid, walls, contact constants, DTSOLID, NN).
+ * All systems of a batch share the collision model, the integrator, the
+ * force precision and COLLISION_ARRAY_MAX (those of the parameters given to
+ * dem_batch_create).  Each system rebuilds its pair list by its own NN rule
+ * (NN == 1 or mod(NN, NEIGHBOR_SEARCH_N) == 0), so its results are the same
+ * as in a handle of its own, whatever else runs in the batch.  Systems can
+ * be added and removed between steps (their particle, cell, facet and bin
+ * ranges are reserved from the limits below and never move while they
+ * live).  The single-system calls (dem_upload_state, dem_step, ...) refuse a
+ * batch handle; the coupling calls are not available on it. */
+typedef struct dem_batch_limits {
+    int32_t max_particles;     /* particles of all systems together */
+    int32_t max_systems;       /* system slots (at most 65535) */
+    int32_t max_cells;         /* DES-grid cells of all systems, plus 1 per system */
+    int32_t max_search_cells;  /* search-grid cells of all systems */
+    int32_t max_facets;        /* wall facets of all systems */
+    int32_t max_facet_bins;    /* facet-in-cell entries of all systems */
+    int32_t reserved[10];
+} dem_batch_limits;
+
+typedef struct dem_sys_status {
+    int32_t capacity;          /* particles reserved for the system */
+    int32_t started;           /* 1 once dem_sys_start has built its pair list */
+    int32_t next_nn;           /* NN of its next DES_TIME_STEP */
+    int32_t particle_offset;   /* first particle of its range in the handle */
+    int64_t steps_done;
+    double  s_time;
+    double  reserved[6];
+} dem_sys_status;
+
+/* Cell ranges a system with parameters p takes from a batch: DES-grid cells
+ * (with its end entry) and search-grid cells.  Host only, no device. */
+int dem_params_cells(const dem_params* p, int32_t* des_cells, int32_t* search_cells);
+
+/* Creates an empty batch handle on the current CUDA device.  `common` gives
+ * the collision model, integrator, force precision and COLLISION_ARRAY_MAX
+ * of all systems (its other fields are not used for the systems). */
+int dem_batch_create(const dem_params* common, const dem_batch_limits* lim, dem_handle** out);
+
+/* Adds a system with its own parameters and room for max_pip particles;
+ * returns its id.  DEM_ERR_CAPACITY when the limits are exhausted. */
+int dem_sys_add(dem_handle* h, const dem_params* p, int32_t max_pip, int32_t* sys);
+/* Removes a system; its ranges become free for later systems. */
+int dem_sys_remove(dem_handle* h, int32_t sys);
+/* dem_set_walls / dem_upload_state / dem_download_state of one system
+ * (arrays with max_pip rows, max_pip <= its capacity). */
+int dem_sys_set_walls(dem_handle* h, int32_t sys, const double* vertex, const double* norm_face, int32_t nf);
+int dem_sys_upload_state(dem_handle* h, int32_t sys, const double* pos, const double* vel,
+                         const double* omega, const double* radius, const double* pmass,
+                         const double* omoi, const int8_t* state, const int32_t* phase,
+                         int32_t max_pip);
+int dem_sys_download_state(dem_handle* h, int32_t sys, double* pos, double* vel, double* omega,
+                           int8_t* state, int32_t max_pip);
+/* Builds the first pair list of the given systems (dem_init_neighbors for
+ * each) in one pass; the running systems keep theirs.  They then step from
+ * NN = 1.  Every system with particles must be started before a step. */
+int dem_sys_start(dem_handle* h, const int32_t* sys, int32_t n_sys);
+/* nsteps DES_TIME_STEPs of every started system, each with its own NN. */
+int dem_batch_step(dem_handle* h, int32_t nsteps);
+/* Statistics of one system (contact counts are not kept per system: 0). */
+int dem_sys_get_stats(dem_handle* h, int32_t sys, dem_stats* out);
+/* dem_download_pairs of one system: its rows as its own 1-based CSR. */
+int dem_sys_download_pairs(dem_handle* h, int32_t sys, int32_t* neighbor_index, int32_t* neighbors,
+                           double* pft, int64_t cap, int32_t max_pip);
+int dem_sys_info(dem_handle* h, int32_t sys, dem_sys_status* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,7 @@ SOURCES = {
     "force_split.cu": ["-fmad=true", "-use_fast_math"],
     "walls.cu": ["-fmad=false"],
     "coupling.cu": ["-fmad=false"],
+    "batch.cu": ["-fmad=false"],
 }
 HEADERS = ["dem_internal.cuh"]
 

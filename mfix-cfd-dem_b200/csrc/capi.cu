@@ -167,13 +167,105 @@ static void prof_collect(dem_handle* h) {
   h->prof_pending.clear();
 }
 
+
+// Particles [off, off + cnt) from Fortran-layout host arrays with cnt rows.
+int upload_range(dem_handle* h, int off, int cnt, int nph, const double* pos, const double* vel,
+                 const double* omega, const double* radius, const double* pmass, const double* omoi,
+                 const int8_t* state, const int32_t* phase) {
+  if (!pos || !vel || !omega || !radius || !pmass || !omoi || !state || !phase)
+    return set_err(h, DEM_ERR_ARG, "null array");
+  if (cnt <= 0) return 0;
+  const size_t n = (size_t)cnt;
+  // one staging block: pos(3n) vel(3n) omega(3n) r(n) m(n) omoi(n) + phase(n ints) + flag
+  double* st = (double*)stage_buffer(h, sizeof(double) * 12 * n + sizeof(int) * n + 64);
+  if (!st) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
+  cudaMemcpyAsync(st, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 3 * n, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 6 * n, omega, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 9 * n, radius, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 10 * n, pmass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(st + 11 * n, omoi, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+  int* ph = (int*)(st + 12 * n);
+  unsigned* bad = (unsigned*)(ph + n);
+  cudaMemcpyAsync(ph, phase, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->state + off, state, n, cudaMemcpyHostToDevice, h->stream);
+  const int T = 256, B = (int)((n + T - 1) / T);
+  const int c = h->cur;
+  k_pack<<<B, T, 0, h->stream>>>(cnt, st, st + 9 * n, h->pos4[c] + off);
+  k_pack<<<B, T, 0, h->stream>>>(cnt, st + 3 * n, st + 10 * n, h->vel4[c] + off);
+  k_pack<<<B, T, 0, h->stream>>>(cnt, st + 6 * n, st + 11 * n, h->omg4[c] + off);
+  cudaMemsetAsync(bad, 0, sizeof(unsigned), h->stream);
+  k_phase_in<<<B, T, 0, h->stream>>>(cnt, ph, h->state + off, h->phase + off, nph, bad);
+  h->launches += 4;
+  unsigned hb = 0;
+  cudaMemcpyAsync(&hb, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "upload")) return rc;
+  if (hb) return set_err(h, DEM_ERR_ARG, "phase out of range");
+  return 0;
+}
+
+// Particles [off, off + cnt) into Fortran-layout host arrays with cnt rows.
+int download_range(dem_handle* h, int off, int cnt, double* pos, double* vel, double* omega, int8_t* state) {
+  if (cnt <= 0) return 0;
+  const size_t n = (size_t)cnt;
+  double* st = (double*)stage_buffer(h, sizeof(double) * 12 * n + sizeof(int) * n + 64);
+  if (!st) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
+  const int T = 256, B = (int)((n + T - 1) / T);
+  const int c = h->cur;
+  k_unpack<<<B, T, 0, h->stream>>>(cnt, h->pos4[c] + off, st);
+  k_unpack<<<B, T, 0, h->stream>>>(cnt, h->vel4[c] + off, st + 3 * n);
+  k_unpack<<<B, T, 0, h->stream>>>(cnt, h->omg4[c] + off, st + 6 * n);
+  h->launches += 3;
+  if (pos) cudaMemcpyAsync(pos, st, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  if (vel) cudaMemcpyAsync(vel, st + 3 * n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  if (omega) cudaMemcpyAsync(omega, st + 6 * n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+  if (state) cudaMemcpyAsync(state, h->state + off, n, cudaMemcpyDeviceToHost, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "download");
+}
+
+// Kinematic statistics of particles [off, off + cnt): NORMAL count, mean
+// velocity, granular temperature, kinetic energy and bed height.
+int stats_range(dem_handle* h, int off, int cnt, dem_stats* s) {
+  const int T = STAT_T, B = (cnt + T - 1) / T;
+  if (B > 0 && h->red_elems < 8 * B) {
+    if (h->red) cudaFree(h->red);
+    h->red = nullptr;
+    h->red_elems = 0;
+    if (int rc = check_cuda(h, cudaMalloc(&h->red, sizeof(double) * 8 * B), "cudaMalloc")) return rc;
+    h->red_elems = 8 * B;
+  }
+  std::vector<double> part((size_t)8 * B);
+  double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (B > 0) {
+    k_stats1<<<B, T, 0, h->stream>>>(cnt, h->pos4[h->cur] + off, h->vel4[h->cur] + off, h->state + off, h->red);
+    h->launches++;
+    cudaMemcpyAsync(part.data(), h->red, sizeof(double) * 8 * B, cudaMemcpyDeviceToHost, h->stream);
+    if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
+    for (int b = 0; b < B; ++b) for (int k = 0; k < 8; ++k) sum[k] += part[(size_t)8 * b + k];
+  }
+  const double nn = sum[0];
+  double mv[3] = {0, 0, 0};
+  if (nn > 0) for (int c = 0; c < 3; ++c) mv[c] = sum[1 + c] / nn;
+  double gt[3] = {0, 0, 0};
+  if (B > 0) {
+    k_stats2<<<B, T, 0, h->stream>>>(cnt, h->vel4[h->cur] + off, h->state + off, mv[0], mv[1], mv[2], h->red);
+    h->launches++;
+    cudaMemcpyAsync(part.data(), h->red, sizeof(double) * 3 * B, cudaMemcpyDeviceToHost, h->stream);
+    if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
+    for (int b = 0; b < B; ++b) for (int k = 0; k < 3; ++k) gt[k] += part[(size_t)3 * b + k];
+  }
+  s->n_normal = (int64_t)nn;
+  for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn > 0 ? gt[c] / nn : 0.0; }
+  s->kinetic_energy = sum[6];
+  s->bed_height = sum[4] > 0 ? sum[5] / sum[4] : 0.0;
+  return 0;
+}
+
 }  // namespace demb
 
-static void fill_devparams(dem_handle* h) {
-  const dem_params& q = h->prm;
-  DevParams& p = h->dp;
+void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
   memset(&p, 0, sizeof p);
-  p.n = h->n;
+  p.n = n;
   p.coll = q.coll_model; p.intg = q.intg_method; p.nph = q.n_phases; p.no_k = q.no_k;
   p.cmax = q.collision_array_max > 0 ? q.collision_array_max : 8;
   p.remove_rogue = q.remove_rogue;
@@ -272,30 +364,10 @@ static int stats_scratch(dem_handle* h, double** out) {
   return 0;
 }
 
-#define API_GUARD(h) do { if (!(h)) return DEM_ERR_ARG; cudaSetDevice((h)->dev); } while (0)
-
-extern "C" {
-
-int dem_abi_version(void) { return DEM_ABI_VERSION; }
-
-const char* dem_last_error(const dem_handle* h) { return h ? h->err.c_str() : "null handle"; }
-
-int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
-  if (!q || !out || max_pip <= 0) return DEM_ERR_ARG;
-  if (q->n_phases < 1 || q->n_phases > DEM_MAX_PHASES) return DEM_ERR_ARG;
-  if (q->dg_imax < 1 || q->dg_jmax < 1 || (!q->no_k && q->dg_kmax < 1)) return DEM_ERR_ARG;
-  if (q->neighbor_search_n < 1 || !(q->dtsolid > 0.0)) return DEM_ERR_ARG;
-  for (int a = 0; a < 3; ++a) {
-    int cells = a == 0 ? q->dg_imax : (a == 1 ? q->dg_jmax : q->dg_kmax);
-    if (q->periodic[a] && !(a == 2 && q->no_k) && cells < 3) return DEM_ERR_ARG;
-  }
-  dem_handle* h = new dem_handle();
-  h->prm = *q;
-  h->n = max_pip;
-  cudaGetDevice(&h->dev);
-  fill_devparams(h);
-  const size_t n = (size_t)max_pip;
-  const int nc = h->dp.ncell2;
+// Device arrays of a handle for h->n particles, nc DES cells and nfc search
+// cells, its error word, stream and an initial pair capacity.
+int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
+  const size_t n = (size_t)h->n;
   const int cmax = h->dp.cmax;
   bool ok = true;
   auto A = [&](void** p, size_t bytes) {
@@ -321,8 +393,8 @@ int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
   A((void**)&h->cell_fill, sizeof(int) * (nc + 1));
   A((void**)&h->cell_list, sizeof(int) * n);
   A((void**)&h->fcell_key, sizeof(int) * n);
-  A((void**)&h->fcell_cnt, sizeof(int) * (h->dp.nfcell + 1));
-  A((void**)&h->fcell_start, sizeof(int) * (h->dp.nfcell + 1));
+  A((void**)&h->fcell_cnt, sizeof(int) * (nfc + 1));
+  A((void**)&h->fcell_start, sizeof(int) * (nfc + 1));
   A((void**)&h->fcell_list, sizeof(int) * n);
   A((void**)&h->spos, sizeof(double4) * n);
   A((void**)&h->sinfo, sizeof(int4) * n);
@@ -337,22 +409,54 @@ int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
   A((void**)&h->wf, sizeof(double) * 6 * n);
   A((void**)&h->derr, sizeof(DevErr));
   A((void**)&h->d_np, sizeof(int));
-  if (!ok) {
-    dem_destroy(h);
-    return DEM_ERR_CUDA;
-  }
+  if (!ok) return DEM_ERR_CUDA;
   cudaMemset(h->wall_fid, 0xff, sizeof(int) * cmax * n);  // -1 = free slot
-  if (cudaMallocHost((void**)&h->herr, sizeof(DevErr)) != cudaSuccess) { dem_destroy(h); return DEM_ERR_CUDA; }
+  if (cudaMallocHost((void**)&h->herr, sizeof(DevErr)) != cudaSuccess) return DEM_ERR_CUDA;
   memset(h->herr, 0, sizeof(DevErr));
-  h->herr->first_rogue = max_pip;
+  h->herr->first_rogue = h->n;
   cudaMemcpy(h->derr, h->herr, sizeof(DevErr), cudaMemcpyHostToDevice);
   cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, h->dev);
   // a stream of its own, so that whole rebuild periods can be captured as
   // CUDA graphs (the legacy default stream cannot be captured)
-  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) { dem_destroy(h); return DEM_ERR_CUDA; }
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return DEM_ERR_CUDA;
   h->stream = h->own_stream;
-  if (ensure_pair_capacity(h, 16 * (long long)n + 1024)) { dem_destroy(h); return DEM_ERR_CUDA; }
-  if (cudaDeviceSynchronize() != cudaSuccess) { dem_destroy(h); return DEM_ERR_CUDA; }
+  if (ensure_pair_capacity(h, pairs)) return DEM_ERR_CUDA;
+  if (cudaDeviceSynchronize() != cudaSuccess) return DEM_ERR_CUDA;
+  return 0;
+}
+
+#define API_GUARD(h) do { if (!(h)) return DEM_ERR_ARG; cudaSetDevice((h)->dev); } while (0)
+// entry points of a single-system handle (a batch handle has dem_sys_* calls)
+#define SINGLE_GUARD(h)                                                                       \
+  do {                                                                                        \
+    API_GUARD(h);                                                                             \
+    if ((h)->batch()) return set_err((h), DEM_ERR_ARG, "batch handle: use the dem_sys_ calls"); \
+  } while (0)
+
+extern "C" {
+
+int dem_abi_version(void) { return DEM_ABI_VERSION; }
+
+const char* dem_last_error(const dem_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
+  if (!q || !out || max_pip <= 0) return DEM_ERR_ARG;
+  if (q->n_phases < 1 || q->n_phases > DEM_MAX_PHASES) return DEM_ERR_ARG;
+  if (q->dg_imax < 1 || q->dg_jmax < 1 || (!q->no_k && q->dg_kmax < 1)) return DEM_ERR_ARG;
+  if (q->neighbor_search_n < 1 || !(q->dtsolid > 0.0)) return DEM_ERR_ARG;
+  for (int a = 0; a < 3; ++a) {
+    int cells = a == 0 ? q->dg_imax : (a == 1 ? q->dg_jmax : q->dg_kmax);
+    if (q->periodic[a] && !(a == 2 && q->no_k) && cells < 3) return DEM_ERR_ARG;
+  }
+  dem_handle* h = new dem_handle();
+  h->prm = *q;
+  h->n = max_pip;
+  cudaGetDevice(&h->dev);
+  fill_devparams(h->prm, h->n, h->dp);
+  if (int rc = alloc_handle(h, h->dp.ncell2, h->dp.nfcell, 16 * (long long)max_pip + 1024)) {
+    dem_destroy(h);
+    return rc;
+  }
   *out = h;
   return 0;
 }
@@ -370,7 +474,8 @@ int dem_destroy(dem_handle* h) {
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
                   h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec,
-                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->d_np};
+                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->d_np,
+                  h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (auto e : h->ev_pool) cudaEventDestroy(e);
@@ -395,7 +500,7 @@ int dem_launch_count(const dem_handle* h, int64_t* count) {
 }
 
 int dem_set_walls(dem_handle* h, const double* vertex, const double* norm_face, int32_t nf) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (nf < 0 || (nf > 0 && (!vertex || !norm_face))) return set_err(h, DEM_ERR_ARG, "bad facet arrays");
   return run_bin_facets(h, vertex, norm_face, nf);
 }
@@ -405,57 +510,17 @@ int dem_set_walls(dem_handle* h, const double* vertex, const double* norm_face, 
 int dem_upload_state(dem_handle* h, const double* pos, const double* vel, const double* omega,
                      const double* radius, const double* pmass, const double* omoi,
                      const int8_t* state, const int32_t* phase, int32_t max_pip) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip does not match dem_create");
-  if (!pos || !vel || !omega || !radius || !pmass || !omoi || !state || !phase)
-    return set_err(h, DEM_ERR_ARG, "null array");
-  const size_t n = h->n;
-  // one staging block: pos(3n) vel(3n) omega(3n) r(n) m(n) omoi(n) + phase(n ints)
-  double* st = (double*)stage_buffer(h, sizeof(double) * 12 * n + sizeof(int) * n + 64);
-  if (!st) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
-  cudaMemcpyAsync(st, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 3 * n, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 6 * n, omega, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 9 * n, radius, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 10 * n, pmass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 11 * n, omoi, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
-  int* ph = (int*)(st + 12 * n);
-  cudaMemcpyAsync(ph, phase, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(h->state, state, n, cudaMemcpyHostToDevice, h->stream);
-  const int T = 256, B = (int)((n + T - 1) / T);
-  const int c = h->cur;
-  k_pack<<<B, T, 0, h->stream>>>(h->n, st, st + 9 * n, h->pos4[c]);
-  k_pack<<<B, T, 0, h->stream>>>(h->n, st + 3 * n, st + 10 * n, h->vel4[c]);
-  k_pack<<<B, T, 0, h->stream>>>(h->n, st + 6 * n, st + 11 * n, h->omg4[c]);
-  unsigned* bad = (unsigned*)h->cell_fill;
-  cudaMemsetAsync(bad, 0, sizeof(unsigned), h->stream);
-  k_phase_in<<<B, T, 0, h->stream>>>(h->n, ph, h->state, h->phase, h->dp.nph, bad);
-  h->launches += 4;
-  unsigned hb = 0;
-  cudaMemcpyAsync(&hb, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
-  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "upload")) return rc;
-  if (hb) return set_err(h, DEM_ERR_ARG, "phase out of range");
+  if (int rc = upload_range(h, 0, h->n, h->dp.nph, pos, vel, omega, radius, pmass, omoi, state, phase)) return rc;
   h->have_state = true;
   return 0;
 }
 
 int dem_download_state(dem_handle* h, double* pos, double* vel, double* omega, int8_t* state, int32_t max_pip) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
-  const size_t n = h->n;
-  double* st = (double*)stage_buffer(h, sizeof(double) * 12 * n + sizeof(int) * n + 64);
-  if (!st) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
-  const int T = 256, B = (int)((n + T - 1) / T);
-  const int c = h->cur;
-  k_unpack<<<B, T, 0, h->stream>>>(h->n, h->pos4[c], st);
-  k_unpack<<<B, T, 0, h->stream>>>(h->n, h->vel4[c], st + 3 * n);
-  k_unpack<<<B, T, 0, h->stream>>>(h->n, h->omg4[c], st + 6 * n);
-  h->launches += 3;
-  if (pos) cudaMemcpyAsync(pos, st, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
-  if (vel) cudaMemcpyAsync(vel, st + 3 * n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
-  if (omega) cudaMemcpyAsync(omega, st + 6 * n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
-  if (state) cudaMemcpyAsync(state, h->state, n, cudaMemcpyDeviceToHost, h->stream);
-  return check_cuda(h, cudaStreamSynchronize(h->stream), "download");
+  return download_range(h, 0, h->n, pos, vel, omega, state);
 }
 
 int dem_download_forces(dem_handle* h, double* fc, double* tow, int32_t max_pip) {
@@ -469,7 +534,7 @@ int dem_download_forces(dem_handle* h, double* fc, double* tow, int32_t max_pip)
 
 int dem_set_ab2_history(dem_handle* h, const double* acc_old, const double* rot_acc_old,
                         int32_t first_pass, int32_t max_pip) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
   const size_t n = h->n;
   if (acc_old) cudaMemcpyAsync(h->acc_old, acc_old, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
@@ -488,14 +553,14 @@ int dem_get_ab2_history(dem_handle* h, double* acc_old, double* rot_acc_old, int
 }
 
 int dem_pair_count(dem_handle* h, int64_t* np) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (!np) return DEM_ERR_ARG;
   *np = host_pairs(h);
   return 0;
 }
 
 int dem_download_pairs(dem_handle* h, int32_t* ni, int32_t* nb, double* pf, int64_t cap, int32_t max_pip) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
   const long long P = host_pairs(h);
   if ((nb || pf) && cap < P) return set_err(h, DEM_ERR_CAPACITY, "pair capacity too small");
@@ -514,32 +579,8 @@ __global__ void k_owner_from_rows(int n, const int* __restrict__ row_end, int* _
   int s = i ? row_end[i - 1] : 0, e = row_end[i];
   for (int c = s; c < e; ++c) owner[c] = i;
 }
-__global__ void k_in_count2(long long np, const int* __restrict__ nbrs, int* __restrict__ in_cnt) {
-  long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (cc < np) atomicAdd(&in_cnt[nbrs[cc]], 1);
-}
-__global__ void k_in_fill2(long long np, const int* __restrict__ nbrs, const int* __restrict__ owner,
-                           const int* __restrict__ in_start, int* __restrict__ in_fill, int2* __restrict__ in_pair) {
-  long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (cc >= np) return;
-  int j = nbrs[cc];
-  int slot = atomicAdd(&in_fill[j], 1);
-  in_pair[in_start[j] + slot] = make_int2(owner[cc], (int)cc);
-}
-__global__ void k_in_sort2(int n, const int* __restrict__ in_start, int2* __restrict__ in_pair) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  int s = in_start[j], e = in_start[j + 1];
-  for (int a = s + 1; a < e; ++a) {
-    int2 v = in_pair[a];
-    int b = a - 1;
-    while (b >= s && in_pair[b].y > v.y) { in_pair[b + 1] = in_pair[b]; --b; }
-    in_pair[b + 1] = v;
-  }
-}
-
 int dem_upload_pairs(dem_handle* h, const int32_t* ni, const int32_t* nb, const double* pf, int64_t np, int32_t max_pip) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (max_pip != h->n || np < 0 || !ni || (np > 0 && (!nb || !pf))) return set_err(h, DEM_ERR_ARG, "bad pair arrays");
   // validate the CSR on the host: monotone end pointers, indices in range
   long long prev = 0;
@@ -570,27 +611,14 @@ int dem_upload_pairs(dem_handle* h, const int32_t* ni, const int32_t* nb, const 
   }
   const int T = 256, B = (h->n + T - 1) / T;
   k_owner_from_rows<<<B, T, 0, h->stream>>>(h->n, h->row_end[h->rb], h->pair_owner);
-  cudaMemsetAsync(h->in_cnt, 0, sizeof(int) * h->n, h->stream);
   h->launches++;
-  if (np) {
-    unsigned BP = (unsigned)((np + T - 1) / T);
-    k_in_count2<<<BP, T, 0, h->stream>>>(np, h->nbrs[h->rb], h->in_cnt);
-    h->launches++;
-  }
-  if (int rc = exclusive_scan(h, h->in_cnt, h->in_start, h->n, h->in_start + h->n)) return rc;
-  if (np) {
-    unsigned BP = (unsigned)((np + T - 1) / T);
-    cudaMemsetAsync(h->in_fill, 0, sizeof(int) * h->n, h->stream);
-    k_in_fill2<<<BP, T, 0, h->stream>>>(np, h->nbrs[h->rb], h->pair_owner, h->in_start, h->in_fill, h->in_pair);
-    k_in_sort2<<<B, T, 0, h->stream>>>(h->n, h->in_start, h->in_pair);
-    h->launches += 2;
-  }
+  if (int rc = build_transpose(h, h->rb)) return rc;
   h->have_pairs = true;
   return check_cuda(h, cudaStreamSynchronize(h->stream), "upload pairs");
 }
 
 int dem_download_wall_history(dem_handle* h, int32_t* fid, double* pf, int32_t max_pip) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip mismatch");
   const size_t cnt = (size_t)h->n * h->dp.cmax;
   if (fid) cudaMemcpyAsync(fid, h->wall_fid, sizeof(int) * cnt, cudaMemcpyDeviceToHost, h->stream);
@@ -601,28 +629,28 @@ int dem_download_wall_history(dem_handle* h, int32_t* fid, double* pf, int32_t m
 }
 
 int dem_download_cells(dem_handle* h, int32_t* cells, int32_t max_pip) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (max_pip != h->n || !cells) return set_err(h, DEM_ERR_ARG, "bad arguments");
   cudaMemcpyAsync(cells, h->dg_pijk, sizeof(int) * h->n, cudaMemcpyDeviceToHost, h->stream);
   return check_cuda(h, cudaStreamSynchronize(h->stream), "download cells");
 }
 
 int dem_desgrid_pic(dem_handle* h) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (!h->have_state) return set_err(h, DEM_ERR_STATE, "no particle state uploaded");
   if (int rc = run_desgrid_pic(h, true)) return rc;
   return fetch_errors(h);
 }
 
 int dem_neighbour(dem_handle* h) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (!h->have_state) return set_err(h, DEM_ERR_STATE, "no particle state uploaded");
   if (int rc = run_neighbour(h, true)) return rc;
   return fetch_errors(h);
 }
 
 int dem_init_neighbors(dem_handle* h) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (!h->have_state) return set_err(h, DEM_ERR_STATE, "no particle state uploaded");
   h->have_pairs = false;
   if (int rc = run_desgrid_pic(h, true)) return rc;
@@ -631,7 +659,7 @@ int dem_init_neighbors(dem_handle* h) {
 }
 
 int dem_calc_force(dem_handle* h) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
   cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
   if (int rc = run_force(h, false)) return rc;
@@ -639,7 +667,7 @@ int dem_calc_force(dem_handle* h) {
 }
 
 int dem_cfnewvalues(dem_handle* h) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (!h->have_state) return set_err(h, DEM_ERR_STATE, "no particle state uploaded");
   if (int rc = run_cfnewvalues(h)) return rc;
   return check_cuda(h, cudaStreamSynchronize(h->stream), "cfnewvalues");
@@ -726,7 +754,7 @@ static int replay_period(dem_handle* h, int nn0) {
 }
 
 int dem_step(dem_handle* h, int32_t nn_first, int32_t nsteps) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
   if (nsteps < 0 || nn_first < 1) return set_err(h, DEM_ERR_ARG, "bad step range");
   const int nsn = h->prm.neighbor_search_n;
@@ -756,39 +784,14 @@ int dem_get_stats(dem_handle* h, dem_stats* s) {
   API_GUARD(h);
   if (!s) return DEM_ERR_ARG;
   memset(s, 0, sizeof *s);
-  const int T = STAT_T, B = (h->n + T - 1) / T;
-  if (h->red_elems < 8 * B) {
-    if (h->red) cudaFree(h->red);
-    h->red = nullptr;
-    if (int rc = check_cuda(h, cudaMalloc(&h->red, sizeof(double) * 8 * B), "cudaMalloc")) return rc;
-    h->red_elems = 8 * B;
-  }
-  std::vector<double> part((size_t)8 * B);
-  k_stats1<<<B, T, 0, h->stream>>>(h->n, h->pos4[h->cur], h->vel4[h->cur], h->state, h->red);
-  h->launches++;
-  cudaMemcpyAsync(part.data(), h->red, sizeof(double) * 8 * B, cudaMemcpyDeviceToHost, h->stream);
-  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
-  double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < B; ++b) for (int k = 0; k < 8; ++k) sum[k] += part[(size_t)8 * b + k];
-  const double nn = sum[0];
-  double mv[3] = {0, 0, 0};
-  if (nn > 0) for (int c = 0; c < 3; ++c) mv[c] = sum[1 + c] / nn;
-  k_stats2<<<B, T, 0, h->stream>>>(h->n, h->vel4[h->cur], h->state, mv[0], mv[1], mv[2], h->red);
-  h->launches++;
-  cudaMemcpyAsync(part.data(), h->red, sizeof(double) * 3 * B, cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = stats_range(h, 0, h->n, s)) return rc;
   cudaMemcpyAsync(h->herr, h->derr, sizeof(DevErr), cudaMemcpyDeviceToHost, h->stream);
   if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stats")) return rc;
-  double gt[3] = {0, 0, 0};
-  for (int b = 0; b < B; ++b) for (int k = 0; k < 3; ++k) gt[k] += part[(size_t)3 * b + k];
-  s->n_normal = (int64_t)nn;
-  for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn > 0 ? gt[c] / nn : 0.0; }
   s->n_pairs = host_pairs(h);
   s->n_contacts = (int64_t)h->herr->n_contacts;
   s->n_wall_contacts = (int64_t)h->herr->n_wall_contacts;
   s->n_rogue_removed = (int64_t)h->herr->rogue_removed;
   s->steps_done = h->steps_done;
-  s->kinetic_energy = sum[6];
-  s->bed_height = sum[4] > 0 ? sum[5] / sum[4] : 0.0;
   s->s_time = h->s_time;
   return 0;
 }
@@ -866,7 +869,7 @@ int dem_get_profile(dem_handle* h, double* ms, int64_t* launches) {
 }
 
 int dem_force_error(dem_handle* h, double* rel_err) {
-  API_GUARD(h);
+  SINGLE_GUARD(h);
   if (!rel_err) return DEM_ERR_ARG;
   return run_split_force_error(h, rel_err);
 }

@@ -337,6 +337,7 @@ extern "C" {
 int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid* g, const double* ep_g, const double* u_g,
                        const double* v_g, const double* w_g, const double* p_force) {
   API_GUARD(h);
+  if (h->batch()) return set_err(h, DEM_ERR_ARG, "coupling is not available on a batch handle");
   if (!g || !ep_g || !u_g || !v_g || !w_g) return set_err(h, DEM_ERR_ARG, "null gas field");
   if (!h->have_state) return set_err(h, DEM_ERR_STATE, "upload particles first");
   if (g->imax < 1 || g->jmax < 1 || (!h->dp.no_k && g->kmax < 1) || !(g->dx > 0) || !(g->dy > 0) ||

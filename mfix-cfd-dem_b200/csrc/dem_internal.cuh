@@ -69,7 +69,27 @@ struct DevParams {
   // over the DES-grid interior, plus one ghost layer on each side
   int fn[3], fc1, fc2, nfcell;
   double f_inv[3];
+  // place of the system in a batch handle (0 for an ordinary handle):
+  // particles [p_begin, p_end), DES cells from cell_off, search cells from
+  // fcell_off in the handle-wide cell arrays; n stays the handle-wide count
+  int p_begin, p_end, cell_off, fcell_off;
 };
+
+// Batch view of a kernel: the parameter block of every system and the
+// system of every particle.  Kernels instantiated with B = false use the
+// by-value block of the handle's single system and never touch the view.
+struct BatchView {
+  const DevParams* tab;       // [system]
+  const uint16_t* sys_of;     // [particle]
+  const uint8_t* due;         // [system] 1 = rebuild its pair list now, 2 = first build (no history)
+  int* first_rogue;           // [system] smallest rogue particle of the last build
+};
+
+template <bool B>
+__device__ __forceinline__ const DevParams& sysp(const DevParams& p, const BatchView& bv, int particle) {
+  if constexpr (B) return bv.tab[bv.sys_of[particle]];
+  else return p;
+}
 
 // What the two particles of a contact pair need to add the pair's terms to
 // FC/TOW in the reference's order: FC_TMP, CROSS(NORMAL, FT) with the two
@@ -92,12 +112,49 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+// Host bookkeeping of one system of a batch handle.
+struct SysSlot {
+  bool live = false;          // the slot holds a system
+  bool clean = true;          // no rows of an earlier occupant left under this id
+  bool started = false;       // its pair list exists and it steps
+  bool have_state = false;
+  dem_params prm;
+  DevParams dp;               // p_begin/p_end/cell_off/fcell_off filled in
+  int cap = 0;                // particles reserved (p_end - p_begin)
+  int nn = 1;                 // NN of its next DES_TIME_STEP
+  bool first_pass = true;
+  long long steps_done = 0;
+  double s_time = 0.0;
+  int fac_off = 0, nf = 0;     // its wall facets in the handle-wide facet arrays
+  int bin_off = 0, nbin = 0;   // its facet-bin entries
+};
+
+// First-fit allocator over an index range (particles or cells of a batch).
+struct RangeAlloc {
+  std::vector<std::pair<int, int>> free_;  // (begin, length), sorted by begin
+  void reset(int total) { free_.assign(1, {0, total}); }
+  int take(int len, int align);             // begin, or -1 when nothing fits
+  void give(int begin, int len);
+};
+
 }  // namespace demb
 
 struct dem_handle {
   dem_params prm;
   demb::DevParams dp;
   int n = 0;
+
+  // batch of independent systems (dem_batch_create); empty otherwise
+  std::vector<demb::SysSlot> sys;
+  demb::RangeAlloc part_alloc, cell_alloc, fcell_alloc, fac_alloc, bin_alloc;
+  int max_facets = 0, max_bins = 0;
+  demb::DevParams* d_sys = nullptr;   // device copy of sys[*].dp
+  uint16_t* sys_of = nullptr;         // [particle] system
+  uint8_t* d_due = nullptr;           // [system] rebuild mask of the current event
+  int* d_first_rogue = nullptr;       // [system]
+  int ncell_total = 0, nfcell_total = 0;
+  bool batch() const { return !sys.empty(); }
+  demb::BatchView bview() const { return demb::BatchView{d_sys, sys_of, d_due, d_first_rogue}; }
   int dev = 0;
   cudaStream_t stream = 0;
   std::string err;
@@ -154,7 +211,7 @@ struct dem_handle {
   int* in_fill = nullptr;     // n
   int2* in_pair = nullptr;    // cap
   int* pair_owner = nullptr;  // cap
-  uint8_t* pflag = nullptr;   // cap: 1 = pair in contact at the last force pass
+  uint8_t* pflag = nullptr;   // cap: 1 = pair in contact at the last force pass (rank scratch in the build)
   demb::PairRec* prec = nullptr; // cap: contact terms of the last force pass
   int rb = 0;                 // which row_end/nbrs buffer is current
 
@@ -219,13 +276,25 @@ int run_split_force_error(dem_handle* h, double* rel_err);
 void launch_pairs_split(dem_handle* h);         // force_split.cu
 void launch_gather_split(dem_handle* h, int mode);
 int ensure_pair_capacity(dem_handle* h, long long need);
+int build_transpose(dem_handle* h, int nb);    // neighbor.cu
+// capi.cu: parameter block of a system with handle-wide particle count n
+void fill_devparams(const dem_params& q, int n, DevParams& p);
+int alloc_handle(dem_handle* h, int nc, int nfc, long long pairs);
+int upload_range(dem_handle* h, int off, int cnt, int nph, const double* pos, const double* vel,
+                 const double* omega, const double* radius, const double* pmass, const double* omoi,
+                 const int8_t* state, const int32_t* phase);
+int download_range(dem_handle* h, int off, int cnt, double* pos, double* vel, double* omega, int8_t* state);
+int stats_range(dem_handle* h, int off, int cnt, dem_stats* s);
+// walls.cu: facets of batch system `sys` binned to its DES cells
+int run_bin_facets_sys(dem_handle* h, int sys, const double* vertex_fortran, const double* norm_fortran, int nf);
 int fetch_errors(dem_handle* h);
 void* stage_buffer(dem_handle* h, size_t bytes);
 void free_gas(dem_handle* h);                   // coupling.cu
 long long host_pairs(dem_handle* h);            // pair count on the host (syncs when stale)
 void invalidate_graphs(dem_handle* h);
 
-// Grid of the persistent pair kernels: a fixed number of resident blocks.
+// Grid of the persistent kernels over the pair list: a fixed number of
+// resident blocks.
 inline unsigned pair_grid(const dem_handle* h, int threads) {
   return (unsigned)(h->n_sm * (2048 / threads));
 }
@@ -275,6 +344,64 @@ __device__ __forceinline__ double periodic_shift(const DevParams& p, int ax, dou
   if (d > 0.5 * L) return -L;
   if (d < -0.5 * L) return L;
   return 0.0;
+}
+
+// Result of the force sum of one particle: either stored into FC/TOW
+// (MODE 0) or integrated as CFUPDATEOLD + CFNEWVALUES (cfupdateold.f:33-41,
+// cfnewvalues.f:700-812) into the other state buffer (MODE 1 = Euler,
+// MODE 2 = Adams-Bashforth).  Velocity updates apply to NORMAL particles,
+// position updates to states below NORMAL_GHOST.
+template <int MODE>
+__device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8_t st, const double x[3],
+                                                const double v[3], const double w[3], double r, double m,
+                                                double omoi, const double f[3], const double t[3],
+                                                double4* __restrict__ pos_n, double4* __restrict__ vel_n,
+                                                double4* __restrict__ omg_n, double* __restrict__ fc,
+                                                double* __restrict__ tow, double* __restrict__ acc_old,
+                                                double* __restrict__ rot_acc_old) {
+  const size_t n = (size_t)p.n;
+  if (MODE == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { fc[c * n + me] = f[c]; tow[c * n + me] = t[c]; }
+    return;
+  }
+  const double dt = p.dt;
+  double xn[3], vn[3], wn[3];
+  if (MODE == 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      vn[c] = v[c];
+      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + dt * (f[c] / m + p.grav[c]);
+      xn[c] = x[c];
+      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + vn[c] * dt;
+      wn[c] = w[c];
+      if (st == DEM_STATE_NORMAL) wn[c] = w[c] + t[c] * omoi * dt;
+    }
+  } else {
+    const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
+                         st == DEM_STATE_NORMAL_GHOST || st == 110);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
+      if (p.first_pass && fp_ok) { ao = f[c] / m + p.grav[c]; ro = t[c]; }
+      double a = f[c];
+      if (st == DEM_STATE_NORMAL) a = f[c] / m + p.grav[c];
+      vn[c] = v[c];
+      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + 0.5 * (3.0 * a - ao) * dt;
+      acc_old[c * n + me] = a;
+      xn[c] = x[c];
+      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + 0.5 * (v[c] + vn[c]) * dt;
+      wn[c] = w[c];
+      if (st == DEM_STATE_NORMAL) {
+        wn[c] = w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
+        ro = t[c] * omoi;
+      }
+      rot_acc_old[c * n + me] = ro;
+    }
+  }
+  pos_n[me] = make_double4(xn[0], xn[1], xn[2], r);
+  vel_n[me] = make_double4(vn[0], vn[1], vn[2], m);
+  omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
 }
 
 }  // namespace demb

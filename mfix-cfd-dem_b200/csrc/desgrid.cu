@@ -15,13 +15,22 @@
 
 namespace demb {
 
-__global__ void k_cell_keys(DevParams p, double4* __restrict__ pos4, const int8_t* __restrict__ state,
-                            int* __restrict__ dg_pijk, int* __restrict__ cell_cnt, int do_wrap) {
+// Cell of every existing particle; in a batch only for systems that rebuild
+// now or have periodic axes (the others keep the cells of their last build,
+// as the reference does between rebuilds).
+template <bool B>
+__global__ void k_cell_keys(DevParams p0, BatchView bv, double4* __restrict__ pos4,
+                            const int8_t* __restrict__ state, int* __restrict__ dg_pijk) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n) return;
+  if (i >= p0.n) return;
+  const DevParams& p = sysp<B>(p0, bv, i);
+  const bool per = p.per[0] || p.per[1] || (p.per[2] && !p.no_k);
+  if constexpr (B) {
+    if (!bv.due[bv.sys_of[i]] && !per) return;
+  }
   if (state[i] == DEM_STATE_NONEXISTENT) { dg_pijk[i] = 0; return; }
   double4 x = pos4[i];
-  if (do_wrap) {
+  if (per) {
     bool moved = false;
     if (p.per[0]) {
       int ci = dg_ofpos(p, 0, x.x, p.istart1);
@@ -43,16 +52,22 @@ __global__ void k_cell_keys(DevParams p, double4* __restrict__ pos4, const int8_
   int li = min(p.iend2, max(p.istart2, dg_ofpos(p, 0, x.x, p.istart1)));
   int lj = min(p.jend2, max(p.jstart2, dg_ofpos(p, 1, x.y, p.jstart1)));
   int lk = p.no_k ? 1 : min(p.kend2, max(p.kstart2, dg_ofpos(p, 2, x.z, p.kstart1)));
-  int c = dg_funijk(p, li, lj, lk);
-  dg_pijk[i] = c;
-  if (cell_cnt) atomicAdd(&cell_cnt[c - 1], 1);
+  dg_pijk[i] = dg_funijk(p, li, lj, lk);
 }
 
-// Search-grid cell of every existing particle (for the pair build).
-__global__ void k_fine_keys(DevParams p, const double4* __restrict__ pos4, const int8_t* __restrict__ state,
-                            int* __restrict__ fkey, int* __restrict__ fcnt) {
+// Search-grid cell of every existing particle (for the pair build), as an
+// index into the handle-wide search-cell arrays; -1 for particles of batch
+// systems that do not rebuild now.
+template <bool B>
+__global__ void k_fine_keys(DevParams p0, BatchView bv, const double4* __restrict__ pos4,
+                            const int8_t* __restrict__ state, int* __restrict__ fkey, int* __restrict__ fcnt) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n || state[i] == DEM_STATE_NONEXISTENT) return;
+  if (i >= p0.n) return;
+  const DevParams& p = sysp<B>(p0, bv, i);
+  if constexpr (B) {
+    if (!bv.due[bv.sys_of[i]]) { fkey[i] = -1; return; }
+  }
+  if (state[i] == DEM_STATE_NONEXISTENT) return;
   const double4 x = pos4[i];
   const double xx[3] = {x.x, x.y, x.z};
   int g[3] = {0, 0, 0};
@@ -62,7 +77,7 @@ __global__ void k_fine_keys(DevParams p, const double4* __restrict__ pos4, const
     const int lo = p.per[a] ? 1 : 0, hi = p.per[a] ? p.fn[a] : p.fn[a] + 1;
     g[a] = min(hi, max(lo, v));
   }
-  const int key = g[2] * p.fc2 + g[0] * p.fc1 + g[1];
+  const int key = p.fcell_off + g[2] * p.fc2 + g[0] * p.fc1 + g[1];
   fkey[i] = key;
   atomicAdd(&fcnt[key], 1);
 }
@@ -72,6 +87,7 @@ __global__ void k_fine_scatter(int n, const int8_t* __restrict__ state, const in
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || state[i] == DEM_STATE_NONEXISTENT) return;
   const int c = fkey[i];
+  if (c < 0) return;
   const int slot = atomicAdd(&ffill[c], 1);
   flist[fstart[c] + slot] = i;
 }
@@ -83,15 +99,19 @@ int run_desgrid_pic(dem_handle* h, bool bin_search) {
   ProfScope ps(h, DEM_PROF_DESGRID);
   const DevParams& p = h->dp;
   const int n = h->n, T = 256, B = (n + T - 1) / T;
-  const bool anyper = p.per[0] || p.per[1] || (p.per[2] && !p.no_k);
-  k_cell_keys<<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->dg_pijk, nullptr, anyper ? 1 : 0);
+  const bool bt = h->batch();
+  const BatchView bv = h->bview();
+  const int nfc = bt ? h->nfcell_total : p.nfcell;
+  if (bt) k_cell_keys<true><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk);
+  else k_cell_keys<false><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk);
   DEM_LAUNCH(h);
   if (!bin_search) return check_cuda(h, cudaGetLastError(), "k_cell_keys");
-  if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * p.nfcell, h->stream), "memset")) return rc;
-  k_fine_keys<<<B, T, 0, h->stream>>>(p, h->pos4[h->cur], h->state, h->fcell_key, h->fcell_cnt);
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * nfc, h->stream), "memset")) return rc;
+  if (bt) k_fine_keys<true><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->fcell_key, h->fcell_cnt);
+  else k_fine_keys<false><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->fcell_key, h->fcell_cnt);
   DEM_LAUNCH(h);
-  if (int rc = exclusive_scan(h, h->fcell_cnt, h->fcell_start, p.nfcell, h->fcell_start + p.nfcell)) return rc;
-  if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * p.nfcell, h->stream), "memset")) return rc;
+  if (int rc = exclusive_scan(h, h->fcell_cnt, h->fcell_start, nfc, h->fcell_start + nfc)) return rc;
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * nfc, h->stream), "memset")) return rc;
   k_fine_scatter<<<B, T, 0, h->stream>>>(n, h->state, h->fcell_key, h->fcell_start, h->fcell_cnt, h->fcell_list);
   DEM_LAUNCH(h);
   return check_cuda(h, cudaGetLastError(), "desgrid_pic");

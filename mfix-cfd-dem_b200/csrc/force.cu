@@ -225,7 +225,7 @@ __device__ __forceinline__ int get_collision(const DevParams& p, const WallCtx& 
 template <int COLL>
 __device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, const PState& s,
                               double f[3], double t[3], unsigned long long& nwc, unsigned& eflags) {
-  const int cell = w.dg_pijk[me] - 1;
+  const int cell = p.cell_off + w.dg_pijk[me] - 1;
   const int fs = w.fbin_start[cell], fe = w.fbin_start[cell + 1];
   if (fe - fs < 1) {
     int* fid = w.wall_fid + (size_t)me * p.cmax;
@@ -333,16 +333,17 @@ __device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, cons
 // holds facets.  Writes the particle's wall force and torque, which are the
 // first terms of FC/TOW in the reference's order (CALC_DEM_FORCE_WITH_WALL_STL
 // runs before the pair loop, calc_force_dem.f:113).
-template <int COLL>
+template <int COLL, bool B>
 __global__ void __launch_bounds__(128)
-k_walls(DevParams p, WallCtx w, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+k_walls(DevParams p0, BatchView bv, WallCtx w, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
         const double4* __restrict__ omg4, const uint8_t* __restrict__ phase, const int8_t* __restrict__ state,
         uint8_t* __restrict__ wall_live, double* __restrict__ wf, DevErr* __restrict__ err) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long nwc = 0;
   unsigned eflags = 0;
-  if (me < p.n && state[me] == DEM_STATE_NORMAL) {
-    const int cell = w.dg_pijk[me] - 1;
+  if (me < p0.n && state[me] == DEM_STATE_NORMAL) {
+    const DevParams& p = sysp<B>(p0, bv, me);
+    const int cell = p.cell_off + w.dg_pijk[me] - 1;
     if (w.fbin_start[cell + 1] - w.fbin_start[cell] < 1) {
       // no facet near: clear the history once (calc_collision_wall_mod.f:194-198)
       if (wall_live[me]) {
@@ -377,9 +378,9 @@ k_walls(DevParams p, WallCtx w, const double4* __restrict__ pos4, const double4*
 // and masses are gathered only for pairs in contact.  PFT_out is written for
 // every pair; the contact terms go to a compact record that both particles
 // read back in kernel 3.
-template <int COLL>
+template <int COLL, bool B>
 __global__ void __launch_bounds__(256)
-k_pairs(DevParams p, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
+k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
         const double4* __restrict__ pos4, const double4* __restrict__ vel4, const double4* __restrict__ omg4,
         const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
         const double* __restrict__ pft_in, double* __restrict__ pft_out,
@@ -392,6 +393,7 @@ k_pairs(DevParams p, const int* __restrict__ d_np, long long cap, const int* __r
   unsigned eflags = 0;
   for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
     const int ll = owner[cc], i = nbrs[cc];
+    const DevParams& p = sysp<B>(p0, bv, ll);
     const double* pi = pft_in + 3 * cc;
     double pin[3] = {pi[0], pi[1], pi[2]};
     double* po = pft_out + 3 * cc;
@@ -460,9 +462,9 @@ __device__ __forceinline__ void add_rolling(const DevParams& p, double r, const 
 // particle's own row, pairs owned by higher-index particles -- and either
 // stores them (MODE 0) or integrates them in place of CFNEWVALUES
 // (MODE 1 = Euler, MODE 2 = Adams-Bashforth).
-template <int MODE>
+template <int MODE, bool B>
 __global__ void __launch_bounds__(256)
-k_gather(DevParams p, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
+k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
          const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
          double4* __restrict__ omg_n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
          const int* __restrict__ fbin_start, int nf, const double* __restrict__ wf,
@@ -471,14 +473,15 @@ k_gather(DevParams p, const double4* __restrict__ pos_c, const double4* __restri
          double* __restrict__ fc, double* __restrict__ tow, double* __restrict__ acc_old,
          double* __restrict__ rot_acc_old) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
-  if (me >= p.n) return;
+  if (me >= p0.n) return;
+  const DevParams& p = sysp<B>(p0, bv, me);
   const int8_t st = state[me];
   const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
   const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
   const double r = X.w, m = V.w, omoi = W.w;
   double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
   if (st == DEM_STATE_NORMAL && nf > 0) {
-    const int cell = dg_pijk[me] - 1;
+    const int cell = p.cell_off + dg_pijk[me] - 1;
     if (fbin_start[cell + 1] > fbin_start[cell]) {
       const double* o = wf + 6 * (size_t)me;
       f[0] = o[0]; f[1] = o[1]; f[2] = o[2]; t[0] = o[3]; t[1] = o[4]; t[2] = o[5];
@@ -516,100 +519,29 @@ k_gather(DevParams p, const double4* __restrict__ pos_c, const double4* __restri
       }
     }
   }
-  const size_t n = (size_t)p.n;
-  if (MODE == 0) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) { fc[c * n + me] = f[c]; tow[c * n + me] = t[c]; }
-    return;
-  }
-  const double dt = p.dt;
-  double xn[3], vn[3], wn[3];
-  if (MODE == 1) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      vn[c] = v[c];
-      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + dt * (f[c] / m + p.grav[c]);
-      xn[c] = x[c];
-      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + vn[c] * dt;
-      wn[c] = w[c];
-      if (st == DEM_STATE_NORMAL) wn[c] = w[c] + t[c] * omoi * dt;
-    }
-  } else {
-    const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
-                         st == DEM_STATE_NORMAL_GHOST || st == 110);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
-      if (p.first_pass && fp_ok) { ao = f[c] / m + p.grav[c]; ro = t[c]; }
-      double a = f[c];
-      if (st == DEM_STATE_NORMAL) a = f[c] / m + p.grav[c];
-      vn[c] = v[c];
-      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + 0.5 * (3.0 * a - ao) * dt;
-      acc_old[c * n + me] = a;
-      xn[c] = x[c];
-      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + 0.5 * (v[c] + vn[c]) * dt;
-      wn[c] = w[c];
-      if (st == DEM_STATE_NORMAL) {
-        wn[c] = w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
-        ro = t[c] * omoi;
-      }
-      rot_acc_old[c * n + me] = ro;
-    }
-  }
-  pos_n[me] = make_double4(xn[0], xn[1], xn[2], r);
-  vel_n[me] = make_double4(vn[0], vn[1], vn[2], m);
-  omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+  finish_particle<MODE>(p, me, st, x, v, w, r, m, omoi, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
+                        rot_acc_old);
 }
 
 // CFUPDATEOLD + CFNEWVALUES from FC/TOW, in place; zeroes FC/TOW.
-template <int INTG>
-__global__ void k_integrate(DevParams p, double4* __restrict__ pos4, double4* __restrict__ vel4,
+template <int INTG, bool B>
+__global__ void k_integrate(DevParams p0, BatchView bv, double4* __restrict__ pos4, double4* __restrict__ vel4,
                             double4* __restrict__ omg4, const int8_t* __restrict__ state,
                             double* __restrict__ fc, double* __restrict__ tow,
                             double* __restrict__ acc_old, double* __restrict__ rot_acc_old) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
-  if (me >= p.n) return;
+  if (me >= p0.n) return;
+  const DevParams& p = sysp<B>(p0, bv, me);
   const size_t n = (size_t)p.n;
-  const int8_t st = state[me];
-  double4 X = pos4[me], Vv = vel4[me], W = omg4[me];
-  double x[3] = {X.x, X.y, X.z}, v[3] = {Vv.x, Vv.y, Vv.z}, w[3] = {W.x, W.y, W.z};
-  const double m = Vv.w, omoi = W.w, dt = p.dt;
+  const double4 X = pos4[me], V = vel4[me], W = omg4[me];
+  const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
   double f[3], t[3];
-  for (int c = 0; c < 3; ++c) { f[c] = fc[c * n + me]; t[c] = tow[c * n + me]; fc[c * n + me] = 0.0; tow[c * n + me] = 0.0; }
-  double xn[3], vn[3], wn[3];
-  if (INTG == DEM_INTG_EULER) {
-    for (int c = 0; c < 3; ++c) {
-      vn[c] = v[c];
-      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + dt * (f[c] / m + p.grav[c]);
-      xn[c] = x[c];
-      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + vn[c] * dt;
-      wn[c] = w[c];
-      if (st == DEM_STATE_NORMAL) wn[c] = w[c] + t[c] * omoi * dt;
-    }
-  } else {
-    const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
-                         st == DEM_STATE_NORMAL_GHOST || st == 110);
-    for (int c = 0; c < 3; ++c) {
-      double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
-      if (p.first_pass && fp_ok) { ao = f[c] / m + p.grav[c]; ro = t[c]; }
-      double a = f[c];
-      if (st == DEM_STATE_NORMAL) a = f[c] / m + p.grav[c];
-      vn[c] = v[c];
-      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + 0.5 * (3.0 * a - ao) * dt;
-      acc_old[c * n + me] = a;
-      xn[c] = x[c];
-      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + 0.5 * (v[c] + vn[c]) * dt;
-      wn[c] = w[c];
-      if (st == DEM_STATE_NORMAL) {
-        wn[c] = w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
-        ro = t[c] * omoi;
-      }
-      rot_acc_old[c * n + me] = ro;
-    }
+  for (int c = 0; c < 3; ++c) {
+    f[c] = fc[c * n + me]; t[c] = tow[c * n + me];
+    fc[c * n + me] = 0.0; tow[c * n + me] = 0.0;
   }
-  pos4[me] = make_double4(xn[0], xn[1], xn[2], X.w);
-  vel4[me] = make_double4(vn[0], vn[1], vn[2], m);
-  omg4[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+  finish_particle<INTG == DEM_INTG_AB2 ? 2 : 1>(p, me, state[me], x, v, w, X.w, V.w, W.w, f, t, pos4, vel4, omg4,
+                                                fc, tow, acc_old, rot_acc_old);
 }
 
 static WallCtx wall_ctx(dem_handle* h) {
@@ -620,42 +552,56 @@ static WallCtx wall_ctx(dem_handle* h) {
   return w;
 }
 
-template <int COLL>
-static void launch_walls_pairs(dem_handle* h, bool walls, bool pairs) {
-  const int c = h->cur, pc = h->pcur;
-  if (walls && h->nf > 0) {
-    const int T = 128, B = (h->n + T - 1) / T;
-    k_walls<COLL><<<B, T, 0, h->stream>>>(h->dp, wall_ctx(h), h->pos4[c], h->vel4[c], h->omg4[c], h->phase,
-                                          h->state, h->wall_live, h->wf, h->derr);
-    DEM_LAUNCH(h);
-  }
-  if (pairs) {
-    const int T = 256;
-    k_pairs<COLL><<<pair_grid(h, T), T, 0, h->stream>>>(h->dp, h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c],
-                                          h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc],
-                                          h->pft[1 - pc], h->pflag, h->prec, h->derr);
-    DEM_LAUNCH(h);
-  }
+template <int COLL, bool B>
+static void launch_walls_t(dem_handle* h) {
+  const int c = h->cur;
+  const int T = 128, G = (h->n + T - 1) / T;
+  k_walls<COLL, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->pos4[c], h->vel4[c], h->omg4[c],
+                                           h->phase, h->state, h->wall_live, h->wf, h->derr);
+  DEM_LAUNCH(h);
 }
 
-template <int MODE>
-static void launch_gather(dem_handle* h) {
-  const int T = 256, B = (h->n + T - 1) / T;
+template <int COLL, bool B>
+static void launch_pairs_t(dem_handle* h) {
+  const int c = h->cur, pc = h->pcur;
+  const int T = 256;
+  k_pairs<COLL, B><<<pair_grid(h, T), T, 0, h->stream>>>(h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner,
+                                                         h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
+                                                         h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
+                                                         h->prec, h->derr);
+  DEM_LAUNCH(h);
+}
+
+template <int MODE, bool B>
+static void launch_gather_t(dem_handle* h) {
+  const int T = 256, G = (h->n + T - 1) / T;
   const int c = h->cur;
-  k_gather<MODE><<<B, T, 0, h->stream>>>(h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
-                                         h->vel4[1 - c], h->omg4[1 - c], h->state, h->dg_pijk, h->fbin_start,
-                                         h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
-                                         h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
+  k_gather<MODE, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
+                                            h->vel4[1 - c], h->omg4[1 - c], h->state, h->dg_pijk, h->fbin_start,
+                                            h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
+                                            h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
   DEM_LAUNCH(h);
 }
 
 static void launch_walls(dem_handle* h) {
-  if (h->dp.coll == DEM_COLL_HERTZ) launch_walls_pairs<DEM_COLL_HERTZ>(h, true, false);
-  else launch_walls_pairs<DEM_COLL_LSD>(h, true, false);
+  if (h->nf <= 0) return;
+  const bool hz = h->dp.coll == DEM_COLL_HERTZ;
+  if (h->batch()) hz ? launch_walls_t<DEM_COLL_HERTZ, true>(h) : launch_walls_t<DEM_COLL_LSD, true>(h);
+  else hz ? launch_walls_t<DEM_COLL_HERTZ, false>(h) : launch_walls_t<DEM_COLL_LSD, false>(h);
+}
+
+template <bool B>
+static void launch_pairs_gather(dem_handle* h, int mode) {
+  if (h->dp.coll == DEM_COLL_HERTZ) launch_pairs_t<DEM_COLL_HERTZ, B>(h);
+  else launch_pairs_t<DEM_COLL_LSD, B>(h);
+  if (mode == 0) launch_gather_t<0, B>(h);
+  else if (mode == 1) launch_gather_t<1, B>(h);
+  else launch_gather_t<2, B>(h);
 }
 
 // Contact forces of the current state.  mode: 0 = into FC/TOW, 1/2 = fused
-// Euler/AB2 integration into the other state buffer.
+// Euler/AB2 integration into the other state buffer.  The collision model,
+// integrator and force precision are common to all systems of a batch.
 static void launch_force_kernels(dem_handle* h, int mode, bool split) {
   launch_walls(h);
   if (split) {
@@ -663,11 +609,8 @@ static void launch_force_kernels(dem_handle* h, int mode, bool split) {
     launch_gather_split(h, mode);
     return;
   }
-  if (h->dp.coll == DEM_COLL_HERTZ) launch_walls_pairs<DEM_COLL_HERTZ>(h, false, true);
-  else launch_walls_pairs<DEM_COLL_LSD>(h, false, true);
-  if (mode == 0) launch_gather<0>(h);
-  else if (mode == 1) launch_gather<1>(h);
-  else launch_gather<2>(h);
+  if (h->batch()) launch_pairs_gather<true>(h, mode);
+  else launch_pairs_gather<false>(h, mode);
 }
 
 int run_force(dem_handle* h, bool fused) {
@@ -720,18 +663,21 @@ int run_split_force_error(dem_handle* h, double* rel_err) {
   return fetch_errors(h);
 }
 
+template <int INTG, bool B>
+static void launch_integrate_t(dem_handle* h) {
+  const int T = 256, G = (h->n + T - 1) / T;
+  const int c = h->cur;
+  k_integrate<INTG, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->state,
+                                               h->fc, h->tow, h->acc_old, h->rot_acc_old);
+  DEM_LAUNCH(h);
+}
+
 int run_cfnewvalues(dem_handle* h) {
   ProfScope ps(h, DEM_PROF_INTEGRATE);
   h->dp.first_pass = h->first_pass ? 1 : 0;
-  const int T = 256, B = (h->n + T - 1) / T;
-  const int c = h->cur;
-  if (h->dp.intg == DEM_INTG_AB2)
-    k_integrate<DEM_INTG_AB2><<<B, T, 0, h->stream>>>(h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->state,
-                                                      h->fc, h->tow, h->acc_old, h->rot_acc_old);
-  else
-    k_integrate<DEM_INTG_EULER><<<B, T, 0, h->stream>>>(h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->state,
-                                                        h->fc, h->tow, h->acc_old, h->rot_acc_old);
-  DEM_LAUNCH(h);
+  const bool ab2 = h->dp.intg == DEM_INTG_AB2;
+  if (h->batch()) ab2 ? launch_integrate_t<DEM_INTG_AB2, true>(h) : launch_integrate_t<DEM_INTG_EULER, true>(h);
+  else ab2 ? launch_integrate_t<DEM_INTG_AB2, false>(h) : launch_integrate_t<DEM_INTG_EULER, false>(h);
   h->first_pass = false;
   return check_cuda(h, cudaGetLastError(), "k_integrate");
 }

@@ -36,9 +36,9 @@ struct Comp3 {  // Neumaier-compensated FP32 sum of a 3-vector
   __device__ __forceinline__ double value(int k) const { return (double)s[k] + (double)c[k]; }
 };
 
-template <int COLL>
+template <int COLL, bool B>
 __global__ void __launch_bounds__(256)
-k_pairs_split(DevParams p, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
+k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
               const double4* __restrict__ pos4, const double4* __restrict__ vel4,
               const double4* __restrict__ omg4, const int8_t* __restrict__ state,
               const uint8_t* __restrict__ phase, const double* __restrict__ pft_in,
@@ -52,6 +52,7 @@ k_pairs_split(DevParams p, const int* __restrict__ d_np, long long cap, const in
   unsigned eflags = 0;
   for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
     const int ll = owner[cc], i = nbrs[cc];
+    const DevParams& p = sysp<B>(p0, bv, ll);
     const double* pi = pft_in + 3 * cc;
     const double pin[3] = {pi[0], pi[1], pi[2]};
     double* po = pft_out + 3 * cc;
@@ -166,9 +167,9 @@ k_pairs_split(DevParams p, const int* __restrict__ d_np, long long cap, const in
   }
 }
 
-template <int MODE>
+template <int MODE, bool B>
 __global__ void __launch_bounds__(256)
-k_gather_split(DevParams p, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
+k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
                const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
                double4* __restrict__ omg_n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
                const int* __restrict__ fbin_start, int nf, const double* __restrict__ wf,
@@ -177,14 +178,15 @@ k_gather_split(DevParams p, const double4* __restrict__ pos_c, const double4* __
                const PairRec32* __restrict__ prec, double* __restrict__ fc, double* __restrict__ tow,
                double* __restrict__ acc_old, double* __restrict__ rot_acc_old) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
-  if (me >= p.n) return;
+  if (me >= p0.n) return;
+  const DevParams& p = sysp<B>(p0, bv, me);
   const int8_t st = state[me];
   const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
   const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
   const double r = X.w, m = V.w, omoi = W.w;
   double f0[3] = {0.0, 0.0, 0.0}, t0[3] = {0.0, 0.0, 0.0};
   if (st == DEM_STATE_NORMAL && nf > 0) {
-    const int cell = dg_pijk[me] - 1;
+    const int cell = p.cell_off + dg_pijk[me] - 1;
     if (fbin_start[cell + 1] > fbin_start[cell]) {
       const double* o = wf + 6 * (size_t)me;
       f0[0] = o[0]; f0[1] = o[1]; f0[2] = o[2]; t0[0] = o[3]; t0[1] = o[4]; t0[2] = o[5];
@@ -226,77 +228,42 @@ k_gather_split(DevParams p, const double4* __restrict__ pos_c, const double4* __
   double f[3], t[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) { f[c] = f0[c] + F.value(c); t[c] = t0[c] + T.value(c); }
-  const size_t n = (size_t)p.n;
-  if (MODE == 0) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) { fc[c * n + me] = f[c]; tow[c * n + me] = t[c]; }
-    return;
-  }
-  const double dt = p.dt;
-  double xn[3], vn[3], wn[3];
-  if (MODE == 1) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      vn[c] = v[c];
-      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + dt * (f[c] / m + p.grav[c]);
-      xn[c] = x[c];
-      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + vn[c] * dt;
-      wn[c] = w[c];
-      if (st == DEM_STATE_NORMAL) wn[c] = w[c] + t[c] * omoi * dt;
-    }
-  } else {
-    const bool fp_ok = !(st == DEM_STATE_NONEXISTENT || st == DEM_STATE_ENTERING || st == 102 ||
-                         st == DEM_STATE_NORMAL_GHOST || st == 110);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double ao = acc_old[c * n + me], ro = rot_acc_old[c * n + me];
-      if (p.first_pass && fp_ok) { ao = f[c] / m + p.grav[c]; ro = t[c]; }
-      double a = f[c];
-      if (st == DEM_STATE_NORMAL) a = f[c] / m + p.grav[c];
-      vn[c] = v[c];
-      if (st == DEM_STATE_NORMAL) vn[c] = v[c] + 0.5 * (3.0 * a - ao) * dt;
-      acc_old[c * n + me] = a;
-      xn[c] = x[c];
-      if (st < DEM_STATE_NORMAL_GHOST) xn[c] = x[c] + 0.5 * (v[c] + vn[c]) * dt;
-      wn[c] = w[c];
-      if (st == DEM_STATE_NORMAL) {
-        wn[c] = w[c] + 0.5 * (3.0 * t[c] * omoi - ro) * dt;
-        ro = t[c] * omoi;
-      }
-      rot_acc_old[c * n + me] = ro;
-    }
-  }
-  pos_n[me] = make_double4(xn[0], xn[1], xn[2], r);
-  vel_n[me] = make_double4(vn[0], vn[1], vn[2], m);
-  omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+  finish_particle<MODE>(p, me, st, x, v, w, r, m, omoi, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
+                        rot_acc_old);
+}
+
+template <int COLL, bool B>
+static void launch_pairs_split_t(dem_handle* h) {
+  const int c = h->cur, pc = h->pcur;
+  const int T = 256;
+  k_pairs_split<COLL, B><<<pair_grid(h, T), T, 0, h->stream>>>(
+      h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
+      h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag, (PairRec32*)h->prec, h->derr);
+  DEM_LAUNCH(h);
 }
 
 void launch_pairs_split(dem_handle* h) {
-  const int c = h->cur, pc = h->pcur;
-  const int T = 256;
-  const unsigned B = pair_grid(h, T);
-  if (h->dp.coll == DEM_COLL_HERTZ)
-    k_pairs_split<DEM_COLL_HERTZ><<<B, T, 0, h->stream>>>(h->dp, h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb],
-        h->pos4[c], h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
-        (PairRec32*)h->prec, h->derr);
-  else
-    k_pairs_split<DEM_COLL_LSD><<<B, T, 0, h->stream>>>(h->dp, h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb],
-        h->pos4[c], h->vel4[c], h->omg4[c], h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
-        (PairRec32*)h->prec, h->derr);
+  const bool hz = h->dp.coll == DEM_COLL_HERTZ;
+  if (h->batch()) hz ? launch_pairs_split_t<DEM_COLL_HERTZ, true>(h) : launch_pairs_split_t<DEM_COLL_LSD, true>(h);
+  else hz ? launch_pairs_split_t<DEM_COLL_HERTZ, false>(h) : launch_pairs_split_t<DEM_COLL_LSD, false>(h);
+}
+
+template <int MODE, bool B>
+static void launch_gather_split_t(dem_handle* h) {
+  const int T = 256, G = (h->n + T - 1) / T;
+  const int c = h->cur;
+  k_gather_split<MODE, B><<<G, T, 0, h->stream>>>(
+      h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
+      h->state, h->dg_pijk, h->fbin_start, h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
+      (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
   DEM_LAUNCH(h);
 }
 
 void launch_gather_split(dem_handle* h, int mode) {
-  const int T = 256, B = (h->n + T - 1) / T;
-  const int c = h->cur;
-#define GS_ARGS h->dp, h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c], \
-    h->state, h->dg_pijk, h->fbin_start, h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair,         \
-    h->pflag, (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old
-  if (mode == 0) k_gather_split<0><<<B, T, 0, h->stream>>>(GS_ARGS);
-  else if (mode == 1) k_gather_split<1><<<B, T, 0, h->stream>>>(GS_ARGS);
-  else k_gather_split<2><<<B, T, 0, h->stream>>>(GS_ARGS);
-#undef GS_ARGS
-  DEM_LAUNCH(h);
+  const bool bt = h->batch();
+  if (mode == 0) bt ? launch_gather_split_t<0, true>(h) : launch_gather_split_t<0, false>(h);
+  else if (mode == 1) bt ? launch_gather_split_t<1, true>(h) : launch_gather_split_t<1, false>(h);
+  else bt ? launch_gather_split_t<2, true>(h) : launch_gather_split_t<2, false>(h);
 }
 
 }  // namespace demb

@@ -22,25 +22,41 @@
 
 namespace demb {
 
-__global__ void k_find_rogue(DevParams p, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
-                             DevErr* __restrict__ err) {
+template <bool B>
+__global__ void k_find_rogue(DevParams p0, BatchView bv, const int8_t* __restrict__ state,
+                             const int* __restrict__ dg_pijk, DevErr* __restrict__ err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n || state[i] != DEM_STATE_NORMAL) return;
+  if (i >= p0.n || state[i] != DEM_STATE_NORMAL) return;
+  const DevParams& p = sysp<B>(p0, bv, i);
+  if constexpr (B) {
+    if (!bv.due[bv.sys_of[i]]) return;
+  }
   int c = dg_pijk[i];
   int lic = dg_iof(p, c), ljc = dg_jof(p, c), lkc = dg_kof(p, c);
   if (lic < p.istart1 || lic > p.iend1 || ljc < p.jstart1 || ljc > p.jend1 ||
       lkc < p.kstart1 || lkc > p.kend1) {
-    atomicMin(&err->first_rogue, i);
+    if constexpr (B) atomicMin(&bv.first_rogue[bv.sys_of[i]], i);
+    else atomicMin(&err->first_rogue, i);
   }
 }
 
+__global__ void k_reset_rogue(int nsys, int* __restrict__ first_rogue) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsys) first_rogue[s] = 0x7fffffff;
+}
+
 // DELETE_PARTICLE (mass_outflow_dem.f:241-300) for the rogue particles.
-__global__ void k_delete_rogue(DevParams p, int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
-                               double4* __restrict__ pos4, double4* __restrict__ vel4, double4* __restrict__ omg4,
-                               double* __restrict__ fc, double* __restrict__ tow, int* __restrict__ wall_fid,
-                               DevErr* __restrict__ err) {
+template <bool B>
+__global__ void k_delete_rogue(DevParams p0, BatchView bv, int8_t* __restrict__ state,
+                               const int* __restrict__ dg_pijk, double4* __restrict__ pos4,
+                               double4* __restrict__ vel4, double4* __restrict__ omg4, double* __restrict__ fc,
+                               double* __restrict__ tow, int* __restrict__ wall_fid, DevErr* __restrict__ err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n || state[i] != DEM_STATE_NORMAL) return;
+  if (i >= p0.n || state[i] != DEM_STATE_NORMAL) return;
+  const DevParams& p = sysp<B>(p0, bv, i);
+  if constexpr (B) {
+    if (!bv.due[bv.sys_of[i]]) return;
+  }
   int c = dg_pijk[i];
   int lic = dg_iof(p, c), ljc = dg_jof(p, c), lkc = dg_kof(p, c);
   if (!(lic < p.istart1 || lic > p.iend1 || ljc < p.jstart1 || ljc > p.jend1 ||
@@ -83,17 +99,19 @@ __global__ void k_sorted_copy(int n, const int* __restrict__ n_exist, const int*
   sinfo[q] = make_int4(i, dg_pijk[i], (int)state[i], fkey[i]);
 }
 
-template <bool FILL>
+template <bool FILL, bool B>
 __global__ void __launch_bounds__(128)
-k_neigh(DevParams p, const int* __restrict__ n_exist, const double4* __restrict__ spos,
+k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
         const int4* __restrict__ sinfo, const int* __restrict__ fstart, const DevErr* __restrict__ err,
         int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
         uint8_t* __restrict__ rank_buf, int* __restrict__ owner, long long cap) {
   const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q0 >= p.n || q0 >= *n_exist) return;
+  if (q0 >= p0.n || q0 >= *n_exist) return;
   const int4 me = sinfo[q0];
   const int cur = me.x;
-  if (me.z != DEM_STATE_NORMAL || cur >= err->first_rogue) return;
+  const DevParams& p = sysp<B>(p0, bv, cur);
+  const int first_rogue = B ? bv.first_rogue[bv.sys_of[cur]] : err->first_rogue;
+  if (me.z != DEM_STATE_NORMAL || cur >= first_rogue) return;
   int start = 0;
   if (FILL) start = (int)min((long long)row_se[cur], cap);
   int cnt = 0;
@@ -116,7 +134,7 @@ k_neigh(DevParams p, const int* __restrict__ n_exist, const double4* __restrict_
         if (off >= 0.5) lo_off[ax] = 0; else hi_off[ax] = 0;
       }
     }
-    const int key = me.w;
+    const int key = me.w - p.fcell_off;
     const int fk = key / p.fc2, fi = (key % p.fc2) / p.fc1, fj = key % p.fc1;
     const int kr = p.no_k ? 0 : 1;
     for (int dk = -kr; dk <= kr; ++dk)
@@ -134,7 +152,7 @@ k_neigh(DevParams p, const int* __restrict__ n_exist, const double4* __restrict_
         }
       }
       if (skip) continue;
-      const int cell = g[2] * p.fc2 + g[0] * p.fc1 + g[1];
+      const int cell = p.fcell_off + g[2] * p.fc2 + g[0] * p.fc1 + g[1];
       const int qs = fstart[cell], qe = fstart[cell + 1];
       for (int q = qs; q < qe; ++q) {
         const int4 o = sinfo[q];
@@ -196,13 +214,36 @@ k_neigh(DevParams p, const int* __restrict__ n_exist, const double4* __restrict_
   else row_cnt[cur] = cnt;
 }
 
+// Rows of batch systems that do not rebuild now: the count pass takes the
+// length of the particle's current row, the fill pass copies the row.
+template <bool FILL>
+__global__ void k_keep_rows(int n, BatchView bv, const int* __restrict__ old_end, const int* __restrict__ old_nbrs,
+                            int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
+                            int* __restrict__ owner, long long cap) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || bv.due[bv.sys_of[i]]) return;
+  const int s = i ? old_end[i - 1] : 0, e = old_end[i];
+  if (!FILL) { row_cnt[i] = e - s; return; }
+  const long long start = row_se[i];
+  for (int c = s; c < e; ++c) {
+    const long long slot = start + (c - s);
+    if (slot < cap) { nbrs[slot] = old_nbrs[c]; owner[slot] = i; }
+  }
+  row_se[i] = (int)min(start + (e - s), cap);
+}
+
 // neighbour.f:77-117: history of each new pair from the same neighbour id in
-// the particle's previous row, zero when the pair is new.
-__global__ void k_remap(int n, const int* __restrict__ row_end, const int* __restrict__ nbrs,
+// the particle's previous row, zero when the pair is new.  A batch system
+// built for the first time (due = 2) takes no history from its region.
+template <bool B>
+__global__ void k_remap(int n, BatchView bv, const int* __restrict__ row_end, const int* __restrict__ nbrs,
                         const int* __restrict__ old_end, const int* __restrict__ old_nbrs,
                         const double* __restrict__ old_pft, double* __restrict__ pft, int have_old) {
   const int ll = blockIdx.x * blockDim.x + threadIdx.x;
   if (ll >= n) return;
+  if constexpr (B) {
+    if (bv.due[bv.sys_of[ll]] == 2) have_old = 0;
+  }
   const int s = ll ? row_end[ll - 1] : 0, e = row_end[ll];
   int so = 0, eo = 0;
   if (have_old) { so = ll ? old_end[ll - 1] : 0; eo = old_end[ll]; }
@@ -257,6 +298,24 @@ __global__ void k_in_sort(int n, const int* __restrict__ in_start, int2* __restr
   }
 }
 
+// Transpose of the current list (buffer nb, pair count in d_np): incoming
+// pairs of every particle in ascending owner order.
+int build_transpose(dem_handle* h, int nb) {
+  const int n = h->n;
+  const int T = 256, B = (n + T - 1) / T;
+  const unsigned BP = pair_grid(h, T);
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->in_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
+  k_in_count<<<BP, T, 0, h->stream>>>(h->d_np, h->nbrs[nb], h->in_cnt);
+  DEM_LAUNCH(h);
+  if (int rc = exclusive_scan(h, h->in_cnt, h->in_start, n, h->in_start + n)) return rc;
+  if (int rc = check_cuda(h, cudaMemsetAsync(h->in_fill, 0, sizeof(int) * n, h->stream), "memset")) return rc;
+  k_in_fill<<<BP, T, 0, h->stream>>>(h->d_np, h->nbrs[nb], h->pair_owner, h->in_start, h->in_fill, h->in_pair);
+  DEM_LAUNCH(h);
+  k_in_sort<<<B, T, 0, h->stream>>>(n, h->in_start, h->in_pair);
+  DEM_LAUNCH(h);
+  return check_cuda(h, cudaGetLastError(), "transpose");
+}
+
 int ensure_pair_capacity(dem_handle* h, long long need) {
   if (need <= h->pair_cap) return 0;
   long long cap = h->pair_cap > 0 ? h->pair_cap : 1024;
@@ -291,20 +350,32 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   ProfScope ps(h, DEM_PROF_NEIGHBOR);
   const DevParams& p = h->dp;
   const int n = h->n, T = 128, B = (n + T - 1) / T;
+  const bool bt = h->batch();
+  const BatchView bv = h->bview();
   DevErr* e = h->derr;
-  // first_rogue := n
-  k_set_int<<<1, 1, 0, h->stream>>>(&e->first_rogue, n);
+  // first_rogue := none
+  if (bt) k_reset_rogue<<<((int)h->sys.size() + 127) / 128, 128, 0, h->stream>>>((int)h->sys.size(), h->d_first_rogue);
+  else k_set_int<<<1, 1, 0, h->stream>>>(&e->first_rogue, n);
   DEM_LAUNCH(h);
-  k_find_rogue<<<B, T, 0, h->stream>>>(p, h->state, h->dg_pijk, e);
+  if (bt) k_find_rogue<true><<<B, T, 0, h->stream>>>(p, bv, h->state, h->dg_pijk, e);
+  else k_find_rogue<false><<<B, T, 0, h->stream>>>(p, bv, h->state, h->dg_pijk, e);
   DEM_LAUNCH(h);
   const int nb = 1 - h->rb;  // new list goes into the other buffer
-  const int* n_exist = h->fcell_start + p.nfcell;
+  const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : p.nfcell);
   k_sorted_copy<<<B, T, 0, h->stream>>>(n, n_exist, h->fcell_list, h->pos4[h->cur], h->state, h->dg_pijk,
                                         h->fcell_key, h->spos, h->sinfo);
   DEM_LAUNCH(h);
   if (int rc = check_cuda(h, cudaMemsetAsync(h->row_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
-  k_neigh<false><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
-                                         nullptr, nullptr, nullptr, nullptr, 0);
+  if (bt) {
+    k_neigh<false, true><<<B, T, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
+                                                 nullptr, nullptr, nullptr, nullptr, 0);
+    k_keep_rows<false><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], h->row_cnt, nullptr,
+                                               nullptr, nullptr, 0);
+    DEM_LAUNCH(h);
+  } else {
+    k_neigh<false, false><<<B, T, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
+                                                  nullptr, nullptr, nullptr, nullptr, 0);
+  }
   DEM_LAUNCH(h);
   if (int rc = exclusive_scan(h, h->row_cnt, h->row_end[nb], n, h->d_np)) return rc;
   if (!h->capturing) {
@@ -318,35 +389,40 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   } else {
     h->np_stale = true;
   }
-  k_neigh<true><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
-                                        h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+  if (bt) {
+    k_neigh<true, true><<<B, T, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
+                                                h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+    k_keep_rows<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], nullptr, h->row_end[nb],
+                                              h->nbrs[nb], h->pair_owner, h->pair_cap);
+    DEM_LAUNCH(h);
+  } else {
+    k_neigh<true, false><<<B, T, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
+                                                 h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+  }
   DEM_LAUNCH(h);
   k_clamp_np<<<1, 1, 0, h->stream>>>(h->d_np, h->pair_cap, e);
   DEM_LAUNCH(h);
-  k_delete_rogue<<<B, T, 0, h->stream>>>(p, h->state, h->dg_pijk, h->pos4[h->cur], h->vel4[h->cur],
-                                         h->omg4[h->cur], h->fc, h->tow, h->wall_fid, e);
+  if (bt)
+    k_delete_rogue<true><<<B, T, 0, h->stream>>>(p, bv, h->state, h->dg_pijk, h->pos4[h->cur], h->vel4[h->cur],
+                                                  h->omg4[h->cur], h->fc, h->tow, h->wall_fid, e);
+  else
+    k_delete_rogue<false><<<B, T, 0, h->stream>>>(p, bv, h->state, h->dg_pijk, h->pos4[h->cur], h->vel4[h->cur],
+                                                   h->omg4[h->cur], h->fc, h->tow, h->wall_fid, e);
   DEM_LAUNCH(h);
   // history carry-over into the other pft buffer
   const int pn = 1 - h->pcur;
-  k_remap<<<B, T, 0, h->stream>>>(n, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
-                                  h->pft[h->pcur], h->pft[pn], (carry_history && h->have_pairs) ? 1 : 0);
+  const int have_old = (carry_history && h->have_pairs) ? 1 : 0;
+  if (bt)
+    k_remap<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
+                                          h->pft[h->pcur], h->pft[pn], have_old);
+  else
+    k_remap<false><<<B, T, 0, h->stream>>>(n, bv, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
+                                           h->pft[h->pcur], h->pft[pn], have_old);
   DEM_LAUNCH(h);
   h->rb = nb;
   h->pcur = pn;
   h->have_pairs = true;
-  // transpose: incoming pairs of every particle, ascending owner
-  const int TP = 256;
-  const unsigned BP = pair_grid(h, TP);
-  if (int rc = check_cuda(h, cudaMemsetAsync(h->in_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
-  k_in_count<<<BP, TP, 0, h->stream>>>(h->d_np, h->nbrs[nb], h->in_cnt);
-  DEM_LAUNCH(h);
-  if (int rc = exclusive_scan(h, h->in_cnt, h->in_start, n, h->in_start + n)) return rc;
-  if (int rc = check_cuda(h, cudaMemsetAsync(h->in_fill, 0, sizeof(int) * n, h->stream), "memset")) return rc;
-  k_in_fill<<<BP, TP, 0, h->stream>>>(h->d_np, h->nbrs[nb], h->pair_owner, h->in_start, h->in_fill, h->in_pair);
-  DEM_LAUNCH(h);
-  k_in_sort<<<B, T, 0, h->stream>>>(n, h->in_start, h->in_pair);
-  DEM_LAUNCH(h);
-  return check_cuda(h, cudaGetLastError(), "neighbour");
+  return build_transpose(h, nb);
 }
 
 long long host_pairs(dem_handle* h) {

@@ -85,7 +85,7 @@ __device__ void facet_range(const DevParams& p, const double* V, int rng[6]) {
 }
 
 template <bool FILL>
-__global__ void k_bin_facets(DevParams p, int nf, const double* __restrict__ vertex, double buffer,
+__global__ void k_bin_facets(DevParams p, int nf, const double* __restrict__ vertex, double buffer, int fac_off,
                              int* __restrict__ cnt, const int* __restrict__ start, FacetBinEntry* __restrict__ out) {
   const int cell = blockIdx.x * blockDim.x + threadIdx.x;  // 0-based
   if (cell >= p.ncell2) return;
@@ -107,7 +107,7 @@ __global__ void k_bin_facets(DevParams p, int nf, const double* __restrict__ ver
     if (!tri_box_overlap(ctr, hs, V)) continue;
     if (FILL) {
       FacetBinEntry e;
-      e.id = f; e.dir = 0; e.mn = 0.0; e.mx = 0.0;
+      e.id = fac_off + f; e.dir = 0; e.mn = 0.0; e.mx = 0.0;
       double smallest = (double)FLT_MAX;  // HUGE(0.0)
       for (int c = 0; c < 3; ++c) {
         double a = V[c], b = V[3 + c], d = V[6 + c];
@@ -182,7 +182,7 @@ int run_bin_facets(dem_handle* h, const double* vf, const double* nfort, int nf)
   cudaMemsetAsync(h->ignore_edge, 0, (size_t)4 * nf, h->stream);
   const int T = 128, B = (p.ncell2 + T - 1) / T;
   const double buffer = 1.1 * p.max_radius;
-  k_bin_facets<false><<<B, T, 0, h->stream>>>(p, nf, h->vertex, buffer, h->cell_cnt, nullptr, nullptr);
+  k_bin_facets<false><<<B, T, 0, h->stream>>>(p, nf, h->vertex, buffer, 0, h->cell_cnt, nullptr, nullptr);
   DEM_LAUNCH(h);
   int* total = h->cell_fill;
   if (int rc = exclusive_scan(h, h->cell_cnt, h->fbin_start, p.ncell2, total)) return rc;
@@ -192,13 +192,66 @@ int run_bin_facets(dem_handle* h, const double* vf, const double* nfort, int nf)
   cudaMemcpyAsync(h->fbin_start + p.ncell2, &nb, sizeof(int), cudaMemcpyHostToDevice, h->stream);
   if (int rc = check_cuda(h, cudaMalloc(&h->fbin, sizeof(FacetBinEntry) * (size_t)(nb > 0 ? nb : 1)), "cudaMalloc")) return rc;
   h->n_fbin = nb;
-  k_bin_facets<true><<<B, T, 0, h->stream>>>(p, nf, h->vertex, buffer, nullptr, h->fbin_start, h->fbin);
+  k_bin_facets<true><<<B, T, 0, h->stream>>>(p, nf, h->vertex, buffer, 0, nullptr, h->fbin_start, h->fbin);
   DEM_LAUNCH(h);
   // COS_STL_NB_ANGLE = DCOS(STL_NB_ANGLE/180*PI) + 1e-6, STL_NB_ANGLE = 5.0 (REAL)
   const double pi = 4.0 * std::atan(1.0);
   const double cos_nb = std::cos((double)5.0f / 180.0 * pi) + 1.0e-6;
   k_edge_flags<<<B, T, 0, h->stream>>>(p.ncell2, h->fbin_start, h->fbin, h->vertex, h->norm_face, cos_nb,
                                        h->ignore_edge);
+  DEM_LAUNCH(h);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "bin facets");
+}
+
+__global__ void k_add_int(int n, int* __restrict__ a, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] += v;
+}
+
+// Facets of one system of a batch handle.  The system owns the facet range
+// [fac_off, fac_off + nf), the bin range [bin_off, bin_off + nbin) and the
+// ncell2 + 1 entries of fbin_start from its cell_off (its own end pointer
+// included), so binning one system leaves the others untouched.  Facet ids
+// in the bins and in the wall history are handle-wide.
+int run_bin_facets_sys(dem_handle* h, int sys, const double* vf, const double* nfort, int nf) {
+  SysSlot& S = h->sys[sys];
+  const DevParams& p = S.dp;
+  invalidate_graphs(h);
+  if (S.nf > 0) h->fac_alloc.give(S.fac_off, S.nf);
+  if (S.nbin > 0) h->bin_alloc.give(S.bin_off, S.nbin);
+  S.nf = 0; S.nbin = 0; S.fac_off = 0; S.bin_off = 0;
+  int* fs = h->fbin_start + p.cell_off;
+  if (int rc = check_cuda(h, cudaMemsetAsync(fs, 0, sizeof(int) * (p.ncell2 + 1), h->stream), "memset")) return rc;
+  if (nf == 0) return check_cuda(h, cudaStreamSynchronize(h->stream), "sync");
+  const int fo = h->fac_alloc.take(nf, 1);
+  if (fo < 0) return set_err(h, DEM_ERR_CAPACITY, "batch facet capacity exhausted");
+  S.fac_off = fo; S.nf = nf;
+  std::vector<double> vx((size_t)9 * nf), nx((size_t)3 * nf);
+  for (int f = 0; f < nf; ++f)
+    for (int v = 0; v < 3; ++v)
+      for (int c = 0; c < 3; ++c) vx[(size_t)9 * f + 3 * v + c] = vf[v + 3 * c + 9 * (size_t)f];
+  for (size_t q = 0; q < nx.size(); ++q) nx[q] = nfort[q];
+  cudaMemcpyAsync(h->vertex + 9 * (size_t)fo, vx.data(), sizeof(double) * vx.size(), cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->norm_face + 3 * (size_t)fo, nx.data(), sizeof(double) * nx.size(), cudaMemcpyHostToDevice, h->stream);
+  cudaMemsetAsync(h->ignore_edge + 4 * (size_t)fo, 0, (size_t)4 * nf, h->stream);
+  const int T = 128, B = (p.ncell2 + T - 1) / T;
+  const double buffer = 1.1 * p.max_radius;
+  const double* V = h->vertex + 9 * (size_t)fo;
+  k_bin_facets<false><<<B, T, 0, h->stream>>>(p, nf, V, buffer, fo, h->cell_cnt, nullptr, nullptr);
+  DEM_LAUNCH(h);
+  if (int rc = exclusive_scan(h, h->cell_cnt, fs, p.ncell2, fs + p.ncell2)) return rc;
+  int nb = 0;
+  cudaMemcpyAsync(&nb, fs + p.ncell2, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
+  const int bo = nb > 0 ? h->bin_alloc.take(nb, 1) : 0;
+  if (bo < 0) return set_err(h, DEM_ERR_CAPACITY, "batch facet-bin capacity exhausted");
+  S.bin_off = bo; S.nbin = nb;
+  k_add_int<<<(p.ncell2 + 1 + T - 1) / T, T, 0, h->stream>>>(p.ncell2 + 1, fs, bo);
+  k_bin_facets<true><<<B, T, 0, h->stream>>>(p, nf, V, buffer, fo, nullptr, fs, h->fbin);
+  h->launches += 2;
+  const double pi = 4.0 * std::atan(1.0);
+  const double cos_nb = std::cos((double)5.0f / 180.0 * pi) + 1.0e-6;
+  k_edge_flags<<<B, T, 0, h->stream>>>(p.ncell2, fs, h->fbin, h->vertex, h->norm_face, cos_nb, h->ignore_edge);
   DEM_LAUNCH(h);
   return check_cuda(h, cudaStreamSynchronize(h->stream), "bin facets");
 }

@@ -9,9 +9,9 @@ parameters, moves arrays and sequences calls.
 """
 from . import abi, params
 from ._lib import load as load_library, LIB_PATH
-from .system import DemSystem, DemError
+from .system import DemSystem, DemError, BatchSystem
 
-__all__ = ["abi", "params", "load_library", "LIB_PATH", "DemSystem", "DemError", "GpuSystem"]
+__all__ = ["abi", "params", "load_library", "LIB_PATH", "DemSystem", "DemError", "GpuSystem", "GpuBatch"]
 
 
 def GpuSystem(prm, max_pip):
@@ -19,3 +19,10 @@ def GpuSystem(prm, max_pip):
     from ._lib import require_cuda
     require_cuda()
     return DemSystem(load_library(), prm, max_pip, prefix="dem_")
+
+
+def GpuBatch(common, limits):
+    """A BatchSystem on the CUDA library (current CUDA device)."""
+    from ._lib import require_cuda
+    require_cuda()
+    return BatchSystem(load_library(), common, limits)

@@ -137,6 +137,30 @@ class DemFluidGrid(C.Structure):
     ]
 
 
+class DemBatchLimits(C.Structure):
+    _fields_ = [
+        ("max_particles", C.c_int32),
+        ("max_systems", C.c_int32),
+        ("max_cells", C.c_int32),
+        ("max_search_cells", C.c_int32),
+        ("max_facets", C.c_int32),
+        ("max_facet_bins", C.c_int32),
+        ("reserved", C.c_int32 * 10),
+    ]
+
+
+class DemSysStatus(C.Structure):
+    _fields_ = [
+        ("capacity", C.c_int32),
+        ("started", C.c_int32),
+        ("next_nn", C.c_int32),
+        ("particle_offset", C.c_int32),
+        ("steps_done", C.c_int64),
+        ("s_time", C.c_double),
+        ("reserved", C.c_double * 6),
+    ]
+
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -182,6 +206,19 @@ DEM_ONLY = {
     "set_graphs": (C.c_int, [_P, C.c_int32]),
     "get_profile": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "get_stats_noalloc": (C.c_int, [_P, C.POINTER(DemStats)]),
+    # batches of independent systems
+    "params_cells": (C.c_int, [C.POINTER(DemParams), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "batch_create": (C.c_int, [C.POINTER(DemParams), C.POINTER(DemBatchLimits), C.POINTER(C.c_void_p)]),
+    "sys_add": (C.c_int, [_P, C.POINTER(DemParams), C.c_int32, C.POINTER(C.c_int32)]),
+    "sys_remove": (C.c_int, [_P, C.c_int32]),
+    "sys_set_walls": (C.c_int, [_P, C.c_int32, _D, _D, C.c_int32]),
+    "sys_upload_state": (C.c_int, [_P, C.c_int32, _D, _D, _D, _D, _D, _D, _I8, _I32, C.c_int32]),
+    "sys_download_state": (C.c_int, [_P, C.c_int32, _D, _D, _D, _I8, C.c_int32]),
+    "sys_start": (C.c_int, [_P, _I32, C.c_int32]),
+    "batch_step": (C.c_int, [_P, C.c_int32]),
+    "sys_get_stats": (C.c_int, [_P, C.c_int32, C.POINTER(DemStats)]),
+    "sys_download_pairs": (C.c_int, [_P, C.c_int32, _I32, _I32, _D, C.c_int64, C.c_int32]),
+    "sys_info": (C.c_int, [_P, C.c_int32, C.POINTER(DemSysStatus)]),
 }
 
 DEM_STATS_NOALLOC_MAX_PARTICLES = 1 << 23

@@ -412,3 +412,28 @@ def hopper_walls(lo, hi, half_angle_deg=30.0, outlet_diam=0.012, y_cone_top=None
         tris.append([P0b, P1b, P1t]); norms.append(nrm)
         tris.append([P0b, P1t, P0t]); norms.append(nrm)
     return _facets(tris, norms), {"y_out": y_out, "y_top": y_top, "r_out": r_out, "R": R}
+
+
+def batch_limits(lib, entries, max_systems=None, slack=1.0, bins_per_cell=8):
+    """dem_batch_limits for a batch holding `entries` = [(params, max_pip,
+    n_facets), ...] at once (times `slack` for later arrivals).  The cell
+    needs come from the library's own grid sizing (dem_params_cells)."""
+    import ctypes as C
+    des = srch = parts = facets = 0
+    for prm, n, nf in entries:
+        a, b = C.c_int32(), C.c_int32()
+        rc = lib.dem_params_cells(C.byref(prm), C.byref(a), C.byref(b))
+        if rc != 0:
+            raise ValueError("invalid system parameters")
+        des += a.value
+        srch += b.value
+        parts += ((int(n) + 63) // 64) * 64
+        facets += int(nf)
+    lim = abi.DemBatchLimits()
+    lim.max_particles = int(parts * slack) + 64
+    lim.max_systems = int(max_systems if max_systems is not None else max(1, len(entries)))
+    lim.max_cells = int(des * slack) + 1
+    lim.max_search_cells = int(srch * slack) + 1
+    lim.max_facets = int(facets * slack) + 1
+    lim.max_facet_bins = int(des * slack * bins_per_cell) + 1
+    return lim

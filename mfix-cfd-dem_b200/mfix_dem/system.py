@@ -262,3 +262,101 @@ class DemSystem:
         v = C.c_double()
         self._call("force_error", self._h, C.byref(v))
         return float(v.value)
+
+
+class BatchSystem:
+    """A batch handle of the CUDA library: many independent DEM systems
+    stepped together (dem_batch_create and the dem_sys_* calls).
+
+    Systems are added with their own parameters and particle capacity and
+    addressed by the id `add` returns; arrays use the same layouts as
+    DemSystem, with as many rows as the system's particle count."""
+
+    def __init__(self, lib, common: abi.DemParams, limits: abi.DemBatchLimits):
+        self._lib = lib
+        self._pre = "dem_"
+        self.common = common
+        self.limits = limits
+        self.n_of = {}
+        h = C.c_void_p()
+        self._call("batch_create", C.byref(common), C.byref(limits), C.byref(h))
+        self._h = h
+
+    _fn = DemSystem._fn
+    _call = DemSystem._call
+    close = DemSystem.close
+    __del__ = DemSystem.__del__
+    __enter__ = DemSystem.__enter__
+    __exit__ = DemSystem.__exit__
+
+    def add(self, params: abi.DemParams, max_pip: int) -> int:
+        sid = C.c_int32()
+        self._call("sys_add", self._h, C.byref(params), C.c_int32(int(max_pip)), C.byref(sid))
+        self.n_of[sid.value] = int(max_pip)
+        return sid.value
+
+    def remove(self, sid: int):
+        self._call("sys_remove", self._h, C.c_int32(sid))
+        self.n_of.pop(sid, None)
+
+    def set_walls(self, sid: int, vertex: np.ndarray, norm_face: np.ndarray):
+        vertex = np.ascontiguousarray(vertex, dtype=np.float64)
+        norm_face = np.ascontiguousarray(norm_face, dtype=np.float64)
+        self._call("sys_set_walls", self._h, C.c_int32(sid), _dp(vertex), _dp(norm_face),
+                   C.c_int32(vertex.shape[0]))
+
+    def upload_state(self, sid: int, pos, vel, omega, radius, pmass, omoi, state, phase):
+        n = np.asarray(radius).shape[0]
+        pos = _f64(pos, (3, n)); vel = _f64(vel, (3, n)); omega = _f64(omega, (3, n))
+        radius = _f64(radius, (n,)); pmass = _f64(pmass, (n,)); omoi = _f64(omoi, (n,))
+        state = np.ascontiguousarray(state, dtype=np.int8)
+        phase = np.ascontiguousarray(phase, dtype=np.int32)
+        self._call("sys_upload_state", self._h, C.c_int32(sid), _dp(pos), _dp(vel), _dp(omega), _dp(radius),
+                   _dp(pmass), _dp(omoi), _bp(state), _ip(phase), C.c_int32(n))
+        self.n_of[sid] = n
+
+    def download_state(self, sid: int):
+        n = self.n_of[sid]
+        pos = np.empty((3, n)); vel = np.empty((3, n)); omega = np.empty((3, n))
+        state = np.empty(n, dtype=np.int8)
+        self._call("sys_download_state", self._h, C.c_int32(sid), _dp(pos), _dp(vel), _dp(omega), _bp(state),
+                   C.c_int32(n))
+        return {"pos": pos, "vel": vel, "omega": omega, "state": state}
+
+    def start(self, sids):
+        ids = np.ascontiguousarray(list(sids), dtype=np.int32)
+        self._call("sys_start", self._h, _ip(ids), C.c_int32(ids.shape[0]))
+
+    def step(self, nsteps: int = 1):
+        self._call("batch_step", self._h, C.c_int32(int(nsteps)))
+
+    def stats(self, sid: int) -> dict:
+        s = abi.DemStats()
+        self._call("sys_get_stats", self._h, C.c_int32(sid), C.byref(s))
+        return s.as_dict()
+
+    def download_pairs(self, sid: int):
+        n = self.n_of[sid]
+        P = int(self.stats(sid)["n_pairs"])
+        ni = np.empty(n, dtype=np.int32)
+        nb = np.empty(max(P, 1), dtype=np.int32)
+        pf = np.empty((max(P, 1), 3))
+        self._call("sys_download_pairs", self._h, C.c_int32(sid), _ip(ni), _ip(nb), _dp(pf),
+                   C.c_int64(max(P, 1)), C.c_int32(n))
+        return ni, nb[:P].copy(), pf[:P].copy()
+
+    def info(self, sid: int) -> dict:
+        s = abi.DemSysStatus()
+        self._call("sys_info", self._h, C.c_int32(sid), C.byref(s))
+        return {"capacity": s.capacity, "started": bool(s.started), "next_nn": s.next_nn,
+                "particle_offset": s.particle_offset, "steps_done": s.steps_done, "s_time": s.s_time}
+
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        self._call("launch_count", self._h, C.byref(v))
+        return int(v.value)
+
+    def set_profiling(self, on: bool):
+        self._call("set_profiling", self._h, C.c_int32(1 if on else 0))
+
+    profile = DemSystem.profile
