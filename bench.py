@@ -48,6 +48,12 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=25)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision leg")
+    ap.add_argument("--batch-systems", type=int, default=256, help="systems of the batched leg (0 = skip)")
+    ap.add_argument("--batch-total", type=int, default=6_000_000, help="particles of the batched leg")
+    ap.add_argument("--serve-rates", default="5,20,50", help="request rates (1/s) of the served leg ('' = skip)")
+    ap.add_argument("--serve-requests", type=int, default=30, help="requests per rate")
+    ap.add_argument("--serve-steps", type=int, default=2000, help="DES steps per served case")
+    ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="HBM budget of the server")
     ap.add_argument("--inflate", type=float, default=1.0,
                     help="grow every sphere by this factor after placement (contact-dense variant)")
     return ap.parse_args()
@@ -205,7 +211,15 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     g.upload_state(arr["pos"], arr["vel"], arr["omega"], arr["radius"], arr["pmass"], arr["omoi"],
                    arr["state"], arr["phase"])
     g.init_neighbors()
-    g.step(args.warmup, 1)
+    # warm-up: at least W steps and up to a period boundary past the first
+    # two replayed periods, so both CUDA graphs of the period (the buffer
+    # parities alternate) are captured before the timed steps
+    nsn = int(prm.neighbor_search_n)
+    warm = max(args.warmup, 3 * nsn)
+    warm = ((warm + nsn - 1) // nsn) * nsn
+    g.step(5, 1)
+    tuning = g.autotune(reps=3)  # before the graphs are captured (a new shape drops them)
+    g.step(warm - 5, 6)
     torch.cuda.synchronize()
     ferr0 = g.force_error() if prec == "split" else None
     clocks = ClockSampler(local)
@@ -217,7 +231,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    g.step(args.steps, args.warmup + 1)
+    g.step(args.steps, warm + 1)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -233,7 +247,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     ep0 = torch.cuda.Event(enable_timing=True)
     ep1 = torch.cuda.Event(enable_timing=True)
     ep0.record(stream)
-    g.step(args.steps, args.warmup + args.steps + 1)
+    g.step(args.steps, warm + args.steps + 1)
     ep1.record(stream)
     torch.cuda.synchronize()
     ms_eager = ep0.elapsed_time(ep1)
@@ -268,6 +282,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
                 "ms_per_step_eager": ms_eager / args.steps,
                 "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]}}
     out = {"value": value, "ms": ms, "n": n, "n_normal": n_normal, "pairs": int(p1), "launches": int(launches),
+           "warmup": warm, "tuning": tuning,
            "roofline": roofline, "clocks": clk, "contacts": int(st["n_contacts"]), "prm": prm, "info": info,
            "force_error": None if ferr0 is None else [ferr0, ferr1]}
 
@@ -284,7 +299,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
                "radius": pinned(arr["radius"]), "pmass": pinned(arr["pmass"]), "omoi": pinned(arr["omoi"]),
                "state": pinned(st_now["state"]), "phase": pinned(arr["phase"])}
         hout = {"pos": hin["pos"], "vel": hin["vel"], "omega": hin["omega"], "state": hin["state"]}
-        nn0 = args.warmup + 2 * args.steps + 1
+        nn0 = warm + 2 * args.steps + 1
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -311,6 +326,118 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     return out
 
 
+def _batched_run(args, prec, stream, systems, info):
+    """The batched workload: every system of `systems` in one batch handle.
+    Warm-up up to the first period boundary (NN = 26), autotune, then K steps
+    (a multiple of NEIGHBOR_SEARCH_N, replayed as captured periods) timed with
+    CUDA events on the library's stream, and an eager pass with kernel-class
+    timing for the roofline."""
+    import torch
+    from mfix_dem import GpuBatch, abi, load_library
+    from mfix_dem import params as P
+    entries = [(s[1], s[2]["pos"].shape[1], s[3][0].shape[0]) for s in systems]
+    lim = P.batch_limits(load_library(), entries, max_systems=len(systems))
+    bt = GpuBatch(systems[0][1], lim)
+    bt.set_stream(stream.cuda_stream)
+    ids = []
+    for case, prm, arr, walls, _ in systems:
+        sid = bt.add(prm, arr["pos"].shape[1])
+        bt.set_walls(sid, *walls)
+        bt.upload_state(sid, arr["pos"], arr["vel"], arr["omega"], arr["radius"], arr["pmass"], arr["omoi"],
+                        arr["state"], arr["phase"])
+        ids.append(sid)
+    bt.start(ids)
+    nsn = int(systems[0][1].neighbor_search_n)
+    warm = max(args.warmup, 3 * nsn)
+    warm = ((warm + nsn - 1) // nsn) * nsn  # NN = m*N + 1 next, both period graphs captured
+    # tune first (a new launch shape drops the captured graphs), then warm up
+    bt.step(5)
+    tuning = bt.autotune(reps=3)
+    bt.step(warm - 5)
+    steps = ((args.steps + nsn - 1) // nsn) * nsn
+    torch.cuda.synchronize()
+    p0 = bt.pair_count()
+    l0 = bt.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    bt.step(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = bt.launch_count() - l0
+    p1 = bt.pair_count()
+    st = bt.total_stats()
+    bt.set_profiling(True)
+    bt.step(steps)
+    torch.cuda.synchronize()
+    prof = bt.profile()
+    bt.set_profiling(False)
+    n_normal = int(st["n_normal"])
+    f_ms, f_n = prof["force"]
+    peak, peak_kind = measured_peak()
+    bytes_launch = algorithmic_bytes(n_normal, 0.5 * (p0 + p1))
+    achieved = bytes_launch / (f_ms / f_n / 1e3) / 1e9 if f_n else None
+    final = {sid: bt.download_state(sid)["pos"] for sid in ids}
+    bt.close()
+    return {"value": n_normal * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps, "warmup": warm,
+            "n_normal": n_normal, "pairs": int(p1), "gpu_launches": int(launches), "tuning": tuning,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "kernel": "force step over all systems (walls + pairs + gather with fused integration)",
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_launch,
+                         "avg_launch_ms": f_ms / f_n if f_n else None,
+                         "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]}},
+            "final_pos": final}
+
+
+def run_batched(args, stream):
+    """Split-precision and FP64 runs of the same batch; the split run's
+    trajectory error is max over systems of max|x_split - x_fp64| / max|x_fp64|
+    after the same steps."""
+    from mfix_dem import abi, configs
+    out = {}
+    for prec in ("split", "fp64"):
+        systems, info = configs.batched(n_sys=args.batch_systems, total=args.batch_total,
+                                        precision=abi.DEM_PREC_SPLIT if prec == "split" else abi.DEM_PREC_FP64)
+        out[prec] = _batched_run(args, prec, stream, systems, info)
+        out["info"] = info
+    err = 0.0
+    for sid, xs in out["split"]["final_pos"].items():
+        xd = out["fp64"]["final_pos"][sid]
+        err = max(err, float(np.max(np.abs(xs - xd)) / max(np.max(np.abs(xd)), 1e-300)))
+    for prec in ("split", "fp64"):
+        out[prec].pop("final_pos")
+    out["trajectory_rel_err"] = err
+    return out
+
+
+def run_served(args):
+    """Poisson streams of hopper-discharge cases served with continuous
+    batching (mfix_dem.serve.DemServer); per rate: p50/p99 latency from
+    arrival to completion and the aggregate particle-steps/s."""
+    from mfix_dem import configs, load_library
+    from mfix_dem.serve import DemServer
+
+    def build(req):
+        return configs.hopper_case(req["n"], friction=req["friction"], outlet_d=req["outlet_d"], seed=req["seed"])
+
+    rates = [float(r) for r in args.serve_rates.split(",") if r.strip()]
+    out = []
+    template = build({"n": 5000, "friction": 0.4, "outlet_d": 8, "seed": 1})
+    for k, rate in enumerate(rates):
+        reqs = configs.hopper_requests(args.serve_requests, rate, seed=configs.SEED_BASE + 4 + 100 * k,
+                                       steps=args.serve_steps)
+        srv = DemServer(load_library(), build, template, hbm_budget_bytes=int(args.serve_budget_gb * 1e9),
+                        max_systems=64)
+        res = srv.run(reqs)
+        srv.close()
+        out.append({"rate_per_s": rate, "requests": len(reqs), "p50_s": res["p50_s"], "p99_s": res["p99_s"],
+                    "mean_s": res["mean_s"], "particle_steps_per_s": res["particle_steps_per_s"],
+                    "span_s": res["span_s"], "gpu_busy_s": res["busy_s"], "chunks": res["chunks"]})
+    return out
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -331,6 +458,14 @@ def run_ours(args):
     if args.precision == "fp64" and not args.no_split:
         other = _timed_run(args, "split", stream, barrier, ws, local, with_e2e=False)
 
+    batched = None
+    if args.batch_systems > 0:
+        batched = run_batched(args, stream)
+
+    served = None
+    if args.serve_rates.strip():
+        served = run_served(args)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
@@ -343,7 +478,7 @@ def run_ours(args):
         wl = "hertz_rsa_1m" if args.inflate == 1.0 else f"hertz_rsa_1m_inflated_{args.inflate:g}"
         line = {
             "metric": METRIC, "value": main["value"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": main["ms"] / args.steps, "higher_is_better": True,
+            "warmup": main["warmup"], "warmup_requested": args.warmup, "ms_per_step": main["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": {"workload": wl, "n_particles": main["n_normal"], "n_pairs": main["pairs"],
@@ -356,6 +491,7 @@ def run_ours(args):
                            (main["n"] * 3 * 32 * 2 + main["pairs"] * 100) / 1e6),
                        "parallelism": f"replicas x{ws}"},
             "roofline": main["roofline"],
+            "tuning": main["tuning"],
             "cpu_baseline": cpu,
             "clocks": main["clocks"],
             "e2e": main.get("e2e"),
@@ -366,7 +502,30 @@ def run_ours(args):
                              "speedup_vs_fp64": other["value"] / main["value"],
                              "force_rel_error_first_last": other["force_error"],
                              "roofline": other["roofline"], "gpu_launches": other["launches"],
+                             "tuning": other["tuning"],
                              "clocks": other["clocks"]}
+        if batched is not None:
+            b = batched
+            line["batched"] = {
+                "workload": f"batched_{b['info']['n_systems']}", "config": b["info"],
+                "value": b["split"]["value"], "unit": METRIC, "precision": "split",
+                "ms_per_step": b["split"]["ms_per_step"], "steps": b["split"]["steps"],
+                "warmup": b["split"]["warmup"], "roofline": b["split"]["roofline"],
+                "tuning": b["split"]["tuning"], "gpu_launches": b["split"]["gpu_launches"],
+                "fp64": {"value": b["fp64"]["value"], "ms_per_step": b["fp64"]["ms_per_step"],
+                         "roofline": b["fp64"]["roofline"], "tuning": b["fp64"]["tuning"]},
+                "speedup_split_vs_fp64_batched": b["split"]["value"] / b["fp64"]["value"],
+                "speedup_vs_plain_fp64_single": b["split"]["value"] / main["value"],
+                "trajectory_rel_err_vs_fp64": b["trajectory_rel_err"],
+                "n_pairs": b["split"]["pairs"]}
+        if served is not None:
+            line["served"] = {
+                "workload": "hopper_discharge_poisson", "precision": "split", "integration": "fp64",
+                "steps_per_case": args.serve_steps, "particles_per_case": "log-uniform 5,000-500,000",
+                "hbm_budget_gb": args.serve_budget_gb, "admission": "particle/cell/facet ranges of the budget",
+                "note": "steps per case reduced from the 20,000 of the workload description so that a sweep "
+                        "fits in the bench run; latency = completion - arrival, wall clock",
+                "rates": served}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

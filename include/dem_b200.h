@@ -331,6 +331,24 @@ int dem_drag_gs_des0(dem_handle* h);
  * particles-in-cell and mean fields. */
 int dem_step_coupled(dem_handle* h, int32_t nn_first, int32_t nsteps);
 
+/* ---- launch-shape autotuning (no counterpart in the reference) -------- */
+typedef struct dem_tuning {
+    int32_t pair_threads;        /* pair kernel: threads per block */
+    int32_t pair_blocks_per_sm;  /* pair kernel: blocks per SM of its persistent grid */
+    int32_t gather_threads;      /* gather kernel: threads per block */
+    int32_t neigh_threads;       /* pair-build scan: threads per block */
+    double  pair_ms, gather_ms, neigh_ms;  /* measured time of the chosen shapes (autotune only) */
+    double  reserved[4];
+} dem_tuning;
+
+/* Times the candidate launch shapes of the hot kernels on the handle's
+ * current state (reps launches each, CUDA events on its stream) and keeps
+ * the fastest; results do not depend on the shapes.  Needs a state and a
+ * pair list (after dem_init_neighbors / dem_sys_start). */
+int dem_autotune(dem_handle* h, int32_t reps, dem_tuning* out);
+int dem_get_tuning(dem_handle* h, dem_tuning* out);
+int dem_set_tuning(dem_handle* h, const dem_tuning* in);
+
 /* ---- batches of independent systems ----------------------------------
  * No counterpart in the reference, which runs one system per process.  A
  * batch handle holds many independent dry DEM systems of any sizes; every

@@ -34,6 +34,7 @@ SOURCES = {
     "walls.cu": ["-fmad=false"],
     "coupling.cu": ["-fmad=false"],
     "batch.cu": ["-fmad=false"],
+    "tune.cu": [],
 }
 HEADERS = ["dem_internal.cuh"]
 

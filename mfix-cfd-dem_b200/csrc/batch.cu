@@ -185,7 +185,7 @@ int dem_batch_create(const dem_params* q, const dem_batch_limits* lim, dem_handl
   };
   A((void**)&h->d_sys, sizeof(DevParams) * lim->max_systems);
   A((void**)&h->sys_of, sizeof(uint16_t) * h->n);
-  A((void**)&h->d_due, lim->max_systems);
+  A((void**)&h->d_due, 3 * (size_t)lim->max_systems);
   A((void**)&h->d_first_rogue, sizeof(int) * lim->max_systems);
   A((void**)&h->vertex, sizeof(double) * 9 * (size_t)lim->max_facets);
   A((void**)&h->norm_face, sizeof(double) * 3 * (size_t)lim->max_facets);
@@ -204,6 +204,7 @@ int dem_batch_create(const dem_params* q, const dem_batch_limits* lim, dem_handl
   for (int s = 0; s < lim->max_systems; ++s) upload_table(h, s);
   std::vector<uint8_t> m(lim->max_systems, 1);
   upload_due(h, m);
+  h->due_cur = h->d_due;
   h->part_alloc.reset(h->n);
   h->cell_alloc.reset(lim->max_cells);
   h->fcell_alloc.reset(lim->max_search_cells);
@@ -410,6 +411,107 @@ static int batch_step_once(dem_handle* h, std::vector<uint8_t>& last_due) {
   return 0;
 }
 
+// A whole NEIGHBOR_SEARCH_N period of a batch whose running systems are in
+// step (same NEIGHBOR_SEARCH_N, NN = m*N + 1 with m >= 1, past the first
+// Adams-Bashforth step) is the same sequence every time: N force passes with
+// the periodic rebinning, the rebuild of all of them after the last.  It is
+// captured once per combination of buffer parities and replayed; the two
+// rebuild masks it uses (idle steps, rebuild step) stay in device memory.
+static bool period_aligned(const dem_handle* h, int* nsn) {
+  int N = -1, nn = -1;
+  bool any = false;
+  for (const SysSlot& S : h->sys) {
+    if (!S.live) continue;
+    if (!S.started || S.first_pass) return false;
+    if (N < 0) { N = S.prm.neighbor_search_n; nn = S.nn; }
+    if (S.prm.neighbor_search_n != N || S.nn != nn) return false;
+    any = true;
+  }
+  if (!any || nn <= 1 || (nn - 1) % N != 0) return false;
+  *nsn = N;
+  return true;
+}
+
+static int graph_step(dem_handle* h, bool rebuild, bool anyper) {
+  cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
+  if (int rc = run_force(h, true)) return rc;
+  if (rebuild || anyper) {
+    const size_t S = h->sys.size();
+    h->due_cur = h->d_due + (rebuild ? 2 * S : S);
+    int rc = run_desgrid_pic(h, rebuild);
+    if (!rc && rebuild) rc = run_neighbour(h, true);
+    h->due_cur = h->d_due;
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+static int batch_replay_period(dem_handle* h, int N) {
+  const long long P = host_pairs(h);
+  if (2 * P + 1024 > h->pair_cap) {
+    if (int rc = ensure_pair_capacity(h, 2 * P + 1024)) return rc;
+    invalidate_graphs(h);
+  }
+  bool anyper = false;
+  for (const SysSlot& S : h->sys)
+    if (S.live) anyper = anyper || S.dp.per[0] || S.dp.per[1] || (S.dp.per[2] && !S.dp.no_k);
+  const int key = (h->cur << 2) | (h->pcur << 1) | h->rb;
+  if (!h->graphs[key]) {
+    // the idle-step and rebuild-step masks of this membership
+    const size_t S = h->sys.size();
+    std::vector<uint8_t> m(2 * S);
+    for (size_t s = 0; s < S; ++s) {
+      const bool run = h->sys[s].live && h->sys[s].started;
+      m[s] = run ? 0 : 2;
+      m[S + s] = run ? 1 : 2;
+    }
+    if (int rc = check_cuda(h, cudaMemcpyAsync(h->d_due + S, m.data(), 2 * S, cudaMemcpyHostToDevice, h->stream),
+                            "period masks")) return rc;
+    if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
+    cudaGraph_t graph;
+    h->capturing = true;
+    if (int rc = check_cuda(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture")) {
+      h->capturing = false;
+      return rc;
+    }
+    const int cur0 = h->cur, pcur0 = h->pcur, rb0 = h->rb;
+    const long long l0 = h->launches;
+    int rc = 0;
+    for (int j = 0; j < N && !rc; ++j) rc = graph_step(h, j == N - 1, anyper);
+    cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+    h->capturing = false;
+    h->cur = cur0; h->pcur = pcur0; h->rb = rb0;
+    const long long kernels = h->launches - l0;
+    h->launches = l0;
+    if (rc) return rc;
+    if (int r2 = check_cuda(h, ce, "end capture")) return r2;
+    cudaGraphExec_t exec;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (int r2 = check_cuda(h, ce, "graph instantiate")) return r2;
+    h->graphs[key] = exec;
+    h->graph_kernels[key] = kernels;
+  }
+  if (int rc = check_cuda(h, cudaGraphLaunch(h->graphs[key], h->stream), "graph launch")) return rc;
+  h->launches += h->graph_kernels[key];
+  for (int j = 0; j < N; ++j) {
+    h->cur = 1 - h->cur;
+    h->pcur = 1 - h->pcur;
+  }
+  h->pcur = 1 - h->pcur;
+  h->rb = 1 - h->rb;
+  h->np_stale = true;
+  h->steps_done += N;
+  for (SysSlot& S : h->sys) {
+    if (!S.live) continue;
+    for (int j = 0; j < N; ++j) S.s_time = S.s_time + S.prm.dtsolid;
+    S.steps_done += N;
+    S.nn += N;
+  }
+  mark_clean(h);
+  return 0;
+}
+
 int dem_batch_step(dem_handle* h, int32_t nsteps) {
   if (!h) return DEM_ERR_ARG;
   cudaSetDevice(h->dev);
@@ -419,9 +521,20 @@ int dem_batch_step(dem_handle* h, int32_t nsteps) {
     if (S.live && S.have_state && !S.started)
       return set_err(h, DEM_ERR_STATE, "a system with particles has not been started");
   if (!h->have_pairs) return set_err(h, DEM_ERR_STATE, "no system started");
+  const bool graphs_ok = h->stream != nullptr && !h->prof && !h->no_graphs;
   std::vector<uint8_t> last_due;
-  for (int k = 0; k < nsteps; ++k)
-    if (int rc = batch_step_once(h, last_due)) return rc;
+  int k = 0;
+  while (k < nsteps) {
+    int N = 0;
+    if (graphs_ok && period_aligned(h, &N) && nsteps - k >= N) {
+      if (int rc = batch_replay_period(h, N)) return rc;
+      last_due.clear();
+      k += N;
+    } else {
+      if (int rc = batch_step_once(h, last_due)) return rc;
+      ++k;
+    }
+  }
   return fetch_errors(h);
 }
 

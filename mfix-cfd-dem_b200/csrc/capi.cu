@@ -553,7 +553,7 @@ int dem_get_ab2_history(dem_handle* h, double* acc_old, double* rot_acc_old, int
 }
 
 int dem_pair_count(dem_handle* h, int64_t* np) {
-  SINGLE_GUARD(h);
+  API_GUARD(h);
   if (!np) return DEM_ERR_ARG;
   *np = host_pairs(h);
   return 0;

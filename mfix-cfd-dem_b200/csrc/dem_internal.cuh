@@ -150,11 +150,13 @@ struct dem_handle {
   int max_facets = 0, max_bins = 0;
   demb::DevParams* d_sys = nullptr;   // device copy of sys[*].dp
   uint16_t* sys_of = nullptr;         // [particle] system
-  uint8_t* d_due = nullptr;           // [system] rebuild mask of the current event
+  uint8_t* d_due = nullptr;           // 3 masks of max_systems: eager events, and the idle
+                                      // and rebuild steps of a captured period
+  const uint8_t* due_cur = nullptr;   // the mask the next kernels read
   int* d_first_rogue = nullptr;       // [system]
   int ncell_total = 0, nfcell_total = 0;
   bool batch() const { return !sys.empty(); }
-  demb::BatchView bview() const { return demb::BatchView{d_sys, sys_of, d_due, d_first_rogue}; }
+  demb::BatchView bview() const { return demb::BatchView{d_sys, sys_of, due_cur, d_first_rogue}; }
   int dev = 0;
   cudaStream_t stream = 0;
   std::string err;
@@ -196,6 +198,12 @@ struct dem_handle {
   bool np_stale = false;      // the last build ran without reading the count back
   int* d_np = nullptr;        // device pair count (persistent pair kernels read it)
   int n_sm = 148;             // multiprocessors of the device
+  // launch shapes of the hot kernels (dem_autotune picks them)
+  struct Tune {
+    int pair_threads = 256, pair_bpsm = 8;  // pair kernel: threads per block, resident blocks per SM
+    int gather_threads = 256;               // gather kernel: threads per block
+    int neigh_threads = 128;                // pair-build scan: threads per block
+  } tune;
   bool capturing = false;     // inside a CUDA graph capture: no host syncs
   cudaStream_t own_stream = nullptr;
   cudaGraphExec_t graphs[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -277,6 +285,9 @@ void launch_pairs_split(dem_handle* h);         // force_split.cu
 void launch_gather_split(dem_handle* h, int mode);
 int ensure_pair_capacity(dem_handle* h, long long need);
 int build_transpose(dem_handle* h, int nb);    // neighbor.cu
+void launch_neigh_count(dem_handle* h);        // neighbor.cu: count pass of the pair build
+void launch_pairs_only(dem_handle* h);         // force.cu: pair kernel of the handle's precision
+void launch_gather_only(dem_handle* h);        // force.cu: gather kernel, forces into FC/TOW
 // capi.cu: parameter block of a system with handle-wide particle count n
 void fill_devparams(const dem_params& q, int n, DevParams& p);
 int alloc_handle(dem_handle* h, int nc, int nfc, long long pairs);

@@ -564,8 +564,8 @@ static void launch_walls_t(dem_handle* h) {
 template <int COLL, bool B>
 static void launch_pairs_t(dem_handle* h) {
   const int c = h->cur, pc = h->pcur;
-  const int T = 256;
-  k_pairs<COLL, B><<<pair_grid(h, T), T, 0, h->stream>>>(h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner,
+  const int T = h->tune.pair_threads;
+  k_pairs<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner,
                                                          h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
                                                          h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
                                                          h->prec, h->derr);
@@ -574,7 +574,7 @@ static void launch_pairs_t(dem_handle* h) {
 
 template <int MODE, bool B>
 static void launch_gather_t(dem_handle* h) {
-  const int T = 256, G = (h->n + T - 1) / T;
+  const int T = h->tune.gather_threads, G = (h->n + T - 1) / T;
   const int c = h->cur;
   k_gather<MODE, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
                                             h->vel4[1 - c], h->omg4[1 - c], h->state, h->dg_pijk, h->fbin_start,
@@ -591,12 +591,34 @@ static void launch_walls(dem_handle* h) {
 }
 
 template <bool B>
-static void launch_pairs_gather(dem_handle* h, int mode) {
+static void launch_pairs_fp64(dem_handle* h) {
   if (h->dp.coll == DEM_COLL_HERTZ) launch_pairs_t<DEM_COLL_HERTZ, B>(h);
   else launch_pairs_t<DEM_COLL_LSD, B>(h);
+}
+
+template <bool B>
+static void launch_gather_fp64(dem_handle* h, int mode) {
   if (mode == 0) launch_gather_t<0, B>(h);
   else if (mode == 1) launch_gather_t<1, B>(h);
   else launch_gather_t<2, B>(h);
+}
+
+template <bool B>
+static void launch_pairs_gather(dem_handle* h, int mode) {
+  launch_pairs_fp64<B>(h);
+  launch_gather_fp64<B>(h, mode);
+}
+
+void launch_pairs_only(dem_handle* h) {
+  if (h->dp.prec == DEM_PREC_SPLIT) launch_pairs_split(h);
+  else if (h->batch()) launch_pairs_fp64<true>(h);
+  else launch_pairs_fp64<false>(h);
+}
+
+void launch_gather_only(dem_handle* h) {
+  if (h->dp.prec == DEM_PREC_SPLIT) launch_gather_split(h, 0);
+  else if (h->batch()) launch_gather_fp64<true>(h, 0);
+  else launch_gather_fp64<false>(h, 0);
 }
 
 // Contact forces of the current state.  mode: 0 = into FC/TOW, 1/2 = fused

@@ -235,8 +235,8 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
 template <int COLL, bool B>
 static void launch_pairs_split_t(dem_handle* h) {
   const int c = h->cur, pc = h->pcur;
-  const int T = 256;
-  k_pairs_split<COLL, B><<<pair_grid(h, T), T, 0, h->stream>>>(
+  const int T = h->tune.pair_threads;
+  k_pairs_split<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
       h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
       h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag, (PairRec32*)h->prec, h->derr);
   DEM_LAUNCH(h);
@@ -250,7 +250,7 @@ void launch_pairs_split(dem_handle* h) {
 
 template <int MODE, bool B>
 static void launch_gather_split_t(dem_handle* h) {
-  const int T = 256, G = (h->n + T - 1) / T;
+  const int T = h->tune.gather_threads, G = (h->n + T - 1) / T;
   const int c = h->cur;
   k_gather_split<MODE, B><<<G, T, 0, h->stream>>>(
       h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],

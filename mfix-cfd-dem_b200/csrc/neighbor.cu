@@ -346,6 +346,20 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   return check_cuda(h, cudaGetLastError(), "grow pairs");
 }
 
+// Count pass of the pair build over the current cell-sorted copy (row_cnt).
+void launch_neigh_count(dem_handle* h) {
+  const int n = h->n, T = h->tune.neigh_threads, B = (n + T - 1) / T;
+  const bool bt = h->batch();
+  const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : h->dp.nfcell);
+  if (bt)
+    k_neigh<false, true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sinfo, h->fcell_start,
+                                                 h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, 0);
+  else
+    k_neigh<false, false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sinfo, h->fcell_start,
+                                                  h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, 0);
+  DEM_LAUNCH(h);
+}
+
 int run_neighbour(dem_handle* h, bool carry_history) {
   ProfScope ps(h, DEM_PROF_NEIGHBOR);
   const DevParams& p = h->dp;
@@ -366,17 +380,12 @@ int run_neighbour(dem_handle* h, bool carry_history) {
                                         h->fcell_key, h->spos, h->sinfo);
   DEM_LAUNCH(h);
   if (int rc = check_cuda(h, cudaMemsetAsync(h->row_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
+  launch_neigh_count(h);
   if (bt) {
-    k_neigh<false, true><<<B, T, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
-                                                 nullptr, nullptr, nullptr, nullptr, 0);
     k_keep_rows<false><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], h->row_cnt, nullptr,
                                                nullptr, nullptr, 0);
     DEM_LAUNCH(h);
-  } else {
-    k_neigh<false, false><<<B, T, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
-                                                  nullptr, nullptr, nullptr, nullptr, 0);
   }
-  DEM_LAUNCH(h);
   if (int rc = exclusive_scan(h, h->row_cnt, h->row_end[nb], n, h->d_np)) return rc;
   if (!h->capturing) {
     // eager steps read the count back and grow the arrays when needed
@@ -389,15 +398,16 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   } else {
     h->np_stale = true;
   }
+  const int TN = h->tune.neigh_threads, BN = (n + TN - 1) / TN;
   if (bt) {
-    k_neigh<true, true><<<B, T, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
-                                                h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+    k_neigh<true, true><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
+                                                  h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
     k_keep_rows<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], nullptr, h->row_end[nb],
                                               h->nbrs[nb], h->pair_owner, h->pair_cap);
     DEM_LAUNCH(h);
   } else {
-    k_neigh<true, false><<<B, T, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
-                                                 h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+    k_neigh<true, false><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
+                                                   h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
   }
   DEM_LAUNCH(h);
   k_clamp_np<<<1, 1, 0, h->stream>>>(h->d_np, h->pair_cap, e);

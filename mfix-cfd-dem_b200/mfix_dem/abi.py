@@ -137,6 +137,22 @@ class DemFluidGrid(C.Structure):
     ]
 
 
+class DemTuning(C.Structure):
+    _fields_ = [
+        ("pair_threads", C.c_int32),
+        ("pair_blocks_per_sm", C.c_int32),
+        ("gather_threads", C.c_int32),
+        ("neigh_threads", C.c_int32),
+        ("pair_ms", C.c_double),
+        ("gather_ms", C.c_double),
+        ("neigh_ms", C.c_double),
+        ("reserved", C.c_double * 4),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class DemBatchLimits(C.Structure):
     _fields_ = [
         ("max_particles", C.c_int32),
@@ -206,6 +222,9 @@ DEM_ONLY = {
     "set_graphs": (C.c_int, [_P, C.c_int32]),
     "get_profile": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "get_stats_noalloc": (C.c_int, [_P, C.POINTER(DemStats)]),
+    "autotune": (C.c_int, [_P, C.c_int32, C.POINTER(DemTuning)]),
+    "get_tuning": (C.c_int, [_P, C.POINTER(DemTuning)]),
+    "set_tuning": (C.c_int, [_P, C.POINTER(DemTuning)]),
     # batches of independent systems
     "params_cells": (C.c_int, [C.POINTER(DemParams), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "batch_create": (C.c_int, [C.POINTER(DemParams), C.POINTER(DemBatchLimits), C.POINTER(C.c_void_p)]),

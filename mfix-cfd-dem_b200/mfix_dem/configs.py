@@ -7,6 +7,10 @@ DEM benchmarks; these follow the shapes the workloads are specified with).
                      clipped 0.5-2 mm), Hertz E=1e7, periodic x/z, bottom
                      wall, random sequential placement at 40 % solids.
 - `coupled_500k`     500,000 spheres of 0.5 mm in a 64x256x64 fluid grid.
+- `batched_256`      256 independent settling columns (the 4,000-sphere box
+                     scaled in height to each count), counts lognormal in
+                     [2,000, 200,000] summing to about 6,000,000, kn
+                     U[200, 2000] N/m and friction U[0.1, 0.5] per system.
 
 Particles are numbered in DES-cell order (k, then i, then j fastest, the
 order of DG_FUNIJK), which is a free choice of the input and gives the
@@ -289,3 +293,101 @@ def coupled(n=500_000, cells=(64, 256, 64), dx=1e-3, d=0.5e-3, rho=2600.0, kn=50
     grid.ur_f_gs = 1.0
     grid.ro_s[0] = rho
     return case, prm, arr, walls, info, grid, fields
+
+
+def batched_counts(n_sys=256, total=6_000_000, lo=2_000, hi=200_000, sigma=1.0, seed=SEED_BASE + 3):
+    """Per-system particle counts: lognormal, clipped to [lo, hi], median
+    chosen so that the clipped counts sum to about `total`; multiples of 100
+    (10 x 10 lattice columns)."""
+    rng = np.random.default_rng(seed)
+    raw = rng.lognormal(mean=0.0, sigma=sigma, size=n_sys)
+    a, b = float(lo), float(hi)
+    for _ in range(80):
+        m = 0.5 * (a + b)
+        if np.clip(m * raw, lo, hi).sum() < total:
+            a = m
+        else:
+            b = m
+    counts = np.clip(np.round(0.5 * (a + b) * raw / 100.0) * 100.0, lo, hi).astype(np.int64)
+    return counts, rng
+
+
+def batched(n_sys=256, total=6_000_000, lo=2_000, hi=200_000, sigma=1.0, seed=SEED_BASE + 3,
+            precision=abi.DEM_PREC_SPLIT):
+    """Independent dry settling systems for one batch handle.  System s has
+    counts[s] = 100 * ny spheres of 1 mm on a 10 x ny x 10 lattice of spacing
+    1.1 d (jitter +-0.04 d, velocities U(+-0.1 m/s)) in a 12 x (60 ny / 40) x
+    12 mm box with walls, LSD with its own kn and friction, e_n = 0.9, and
+    dt = t_coll/50 of its own kn.  Returns (systems, info) where systems is a
+    list of (case, prm, arr, walls, info) tuples."""
+    counts, rng = batched_counts(n_sys, total, lo, hi, sigma, seed)
+    kn = rng.uniform(200.0, 2000.0, n_sys)
+    mew = rng.uniform(0.1, 0.5, n_sys)
+    systems = []
+    for s in range(n_sys):
+        ny = int(counts[s] // 100)
+        box = (12e-3, 60e-3 * ny / 40.0, 12e-3)
+        systems.append(settling(n_side=(10, ny, 10), box=box, seed=seed * 1000 + s, kn=float(kn[s]),
+                                mew=float(mew[s]), precision=precision))
+    info = {"n_systems": n_sys, "n_particles": int(counts.sum()), "min_count": int(counts.min()),
+            "max_count": int(counts.max()), "median_count": int(np.median(counts))}
+    return systems, info
+
+
+HOPPER_BOX = (0.2, 0.6, 0.2)
+
+
+def hopper_case(n, friction=0.4, outlet_d=8, seed=SEED_BASE + 4, d=2e-3, rho=2500.0,
+                precision=abi.DEM_PREC_SPLIT, jitter=0.04, spacing=1.1, half_angle=30.0):
+    """One hopper-discharge case: a 20 x 60 x 20 cm box with a conical bottom
+    (half-angle 30 degrees) and an outlet of `outlet_d` particle diameters,
+    `n` spheres of d = 2 mm filled on a lattice of spacing 1.1 d with +-0.04 d
+    jitter above the cone, Hertz E = 1e7 Pa, nu = 0.3, e_n = e_t = 0.85,
+    friction `friction` with particles and walls.  Particles that fall out
+    through the outlet leave the domain and are removed as rogue."""
+    box = HOPPER_BOX
+    (vertex, norm), geo = P.hopper_walls((0.0, 0.0, 0.0), box, half_angle_deg=half_angle,
+                                         outlet_diam=outlet_d * d)
+    rng = np.random.default_rng(seed)
+    a = spacing * d
+    m = int((min(box[0], box[2]) - a) // a)          # lattice sites per row across the box
+    layers = -(-n // (m * m))
+    y_base = geo["y_top"] + a
+    if y_base + layers * a > box[1] - a:
+        raise ValueError("hopper fill does not fit in the box")
+    kk, ii, jj = np.meshgrid(np.arange(m), np.arange(m), np.arange(layers), indexing="ij")
+    pos = np.empty((m * m * layers, 3))
+    pos[:, 0] = (ii.ravel() + 0.5) * a + 0.5 * (box[0] - m * a)
+    pos[:, 1] = y_base + jj.ravel() * a
+    pos[:, 2] = (kk.ravel() + 0.5) * a + 0.5 * (box[2] - m * a)
+    pos = pos[np.argsort(pos[:, 1], kind="stable")][:n]      # the n lowest sites
+    pos += rng.uniform(-jitter * d, jitter * d, size=pos.shape)
+    vel = np.zeros((n, 3))
+    omega = np.zeros((n, 3))
+    radius = np.full(n, 0.5 * d)
+    case = P.DemCase(d_p0=(d,), ro_s0=(rho,), coll_model="HERTZ", intg_method="EULER",
+                     des_en_input=0.85, des_en_wall_input=[0.85], des_et_input=0.85, des_et_wall_input=[0.85],
+                     e_young=(1e7,), v_poisson=(0.3,), ew_young=1e7, vw_poisson=0.3,
+                     mew=friction, mew_w=friction, grav=(0.0, -9.81, 0.0), domain_hi=box,
+                     fluid_cells=(1, 1, 1), remove_rogue=True, force_precision=precision)
+    arr = _arrays(pos, vel, omega, radius, np.full(n, rho))
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    perm = _sort_by_des_cell(prm, pos)
+    arr = _arrays(pos[perm], vel[perm], omega[perm], radius[perm], np.full(n, rho))
+    info.update(geo)
+    info.update({"n": n, "friction": friction, "outlet_d": outlet_d})
+    return case, prm, arr, (vertex, norm), info
+
+
+def hopper_requests(n_req, rate, seed=SEED_BASE + 4, n_lo=5_000, n_hi=500_000, steps=20_000):
+    """A Poisson request stream of hopper cases: arrival times (s) with mean
+    rate `rate`, particle counts log-uniform in [n_lo, n_hi], friction
+    U[0.2, 0.6], outlet U{6..10} diameters, `steps` DES steps each."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    n = np.exp(rng.uniform(math.log(n_lo), math.log(n_hi), n_req)).astype(np.int64)
+    mu = rng.uniform(0.2, 0.6, n_req)
+    outlet = rng.integers(6, 11, n_req)
+    return [{"rid": k, "arrival": float(t[k]), "n": int(n[k]), "friction": float(mu[k]),
+             "outlet_d": int(outlet[k]), "seed": int(seed * 1000 + k), "steps": int(steps)}
+            for k in range(n_req)]

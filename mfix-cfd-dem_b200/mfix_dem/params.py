@@ -370,47 +370,76 @@ def default_walls(lo, hi, periodic=(False, False, False), no_k=False):
     return _facets(tris, norms)
 
 
-def hopper_walls(lo, hi, half_angle_deg=30.0, outlet_diam=0.012, y_cone_top=None,
-                 n_seg=64):
-    """Box walls plus a conical hopper bottom, triangulated.
+def _facet_normal(t, toward):
+    """Unit normal of triangle t (cross product of its edges), oriented to
+    have a positive component along `toward`."""
+    a, b, c = (np.asarray(v, dtype=float) for v in t)
+    n = np.cross(b - a, c - a)
+    n = n / np.linalg.norm(n)
+    if float(np.dot(n, np.asarray(toward, dtype=float))) < 0.0:
+        n = -n
+    return tuple(float(x) for x in n)
 
-    Side walls are the default box faces above the cone; the cone runs from
-    the box's inscribed circle at y_cone_top down to an outlet of diameter
-    outlet_diam, with its axis along y through the box centre.  The bottom
-    face is left open below the outlet (particles that leave are removed as
-    rogue by the neighbour build).  Normals point into the particle region.
+
+def hopper_walls(lo, hi, half_angle_deg=30.0, outlet_diam=0.012, y_out=None, n_seg=64):
+    """Box walls with a conical hopper bottom, triangulated.
+
+    The cone has its axis along y through the box centre, its wall at
+    `half_angle_deg` from the axis, an outlet of diameter `outlet_diam` at
+    height y_out (default 5 % of the box height above its floor) and its rim
+    on the circle inscribed in the box cross-section.  A flat plate at the rim
+    height closes the corners between the rim and the box walls.  The x, z
+    and top faces are the default box walls; the floor below the outlet is
+    open, so particles that leave through the outlet end up outside the
+    domain and are removed as rogue by the neighbour build.  Each facet's
+    normal is its own (cross product), pointing into the particle region.
+    n_seg must be a multiple of 8 so that the plate reaches the box corners.
     """
+    if n_seg % 8:
+        raise ValueError("n_seg must be a multiple of 8")
     x0, y0, z0 = lo
     x1, y1, z1 = hi
     cx, cz = 0.5 * (x0 + x1), 0.5 * (z0 + z1)
-    R = 0.5 * min(x1 - x0, z1 - z0)
+    hx, hz = 0.5 * (x1 - x0), 0.5 * (z1 - z0)
+    R = min(hx, hz)
     r_out = 0.5 * outlet_diam
     t = math.tan(math.radians(half_angle_deg))
     h_cone = (R - r_out) / t
-    y_out = y0 + 0.05 * (y1 - y0) if y_cone_top is None else y_cone_top - h_cone
+    if y_out is None:
+        y_out = y0 + 0.05 * (y1 - y0)
     y_top = y_out + h_cone
     xl, yl, zl = x1 - x0, y1 - y0, z1 - z0
     tris, norms = [], []
-    # side walls (x and z faces) and top
+    # x faces, top face and z faces (one large triangle each, as the default walls)
     tris.append([(x0, y0, z0), (x0, y1 + yl, z0), (x0, y0, z1 + zl)]); norms.append((1.0, 0.0, 0.0))
     tris.append([(x1, y0, z0), (x1, y1 + yl, z0), (x1, y0, z1 + zl)]); norms.append((-1.0, 0.0, 0.0))
     tris.append([(x0, y1, z0), (x1 + xl, y1, z0), (x0, y1, z1 + zl)]); norms.append((0.0, -1.0, 0.0))
     tris.append([(x0, y0, z0), (x1 + xl, y0, z0), (x0, y1 + yl, z0)]); norms.append((0.0, 0.0, 1.0))
     tris.append([(x0, y0, z1), (x1 + xl, y0, z1), (x0, y1 + yl, z1)]); norms.append((0.0, 0.0, -1.0))
-    # cone: n_seg quads -> 2 triangles each
-    ca, sa = math.cos(math.radians(half_angle_deg)), math.sin(math.radians(half_angle_deg))
-    for s in range(n_seg):
-        a0 = 2 * math.pi * s / n_seg
-        a1 = 2 * math.pi * (s + 1) / n_seg
+
+    def rim(a, r, y):
+        return (cx + r * math.cos(a), y, cz + r * math.sin(a))
+
+    def square(a):
+        c, s_ = math.cos(a), math.sin(a)
+        k = min(hx / abs(c) if abs(c) > 1e-15 else math.inf, hz / abs(s_) if abs(s_) > 1e-15 else math.inf)
+        return (cx + k * c, y_top, cz + k * s_)
+
+    for s_ in range(n_seg):
+        a0 = 2 * math.pi * s_ / n_seg
+        a1 = 2 * math.pi * (s_ + 1) / n_seg
         am = 0.5 * (a0 + a1)
-        P0t = (cx + R * math.cos(a0), y_top, cz + R * math.sin(a0))
-        P1t = (cx + R * math.cos(a1), y_top, cz + R * math.sin(a1))
-        P0b = (cx + r_out * math.cos(a0), y_out, cz + r_out * math.sin(a0))
-        P1b = (cx + r_out * math.cos(a1), y_out, cz + r_out * math.sin(a1))
-        # inward normal: points toward the axis and up
-        nrm = (-ca * math.cos(am), sa, -ca * math.sin(am))
-        tris.append([P0b, P1b, P1t]); norms.append(nrm)
-        tris.append([P0b, P1t, P0t]); norms.append(nrm)
+        P0t, P1t = rim(a0, R, y_top), rim(a1, R, y_top)
+        P0b, P1b = rim(a0, r_out, y_out), rim(a1, r_out, y_out)
+        # cone wall: the particle side is toward the axis and up
+        inward = (-math.cos(am), math.tan(math.radians(half_angle_deg)), -math.sin(am))
+        for tri in ([P0b, P1b, P1t], [P0b, P1t, P0t]):
+            tris.append(tri); norms.append(_facet_normal(tri, inward))
+        # plate between the rim and the box walls
+        Q0, Q1 = square(a0), square(a1)
+        for tri in ([P0t, P1t, Q1], [P0t, Q1, Q0]):
+            if np.linalg.norm(np.cross(np.subtract(tri[1], tri[0]), np.subtract(tri[2], tri[0]))) > 1e-18:
+                tris.append(tri); norms.append((0.0, 1.0, 0.0))
     return _facets(tris, norms), {"y_out": y_out, "y_top": y_top, "r_out": r_out, "R": R}
 
 

@@ -258,6 +258,24 @@ class DemSystem:
     def set_stream(self, stream_ptr: int):
         self._call("set_stream", self._h, C.c_void_p(stream_ptr))
 
+    def autotune(self, reps: int = 5) -> dict:
+        """Picks the launch shapes of the hot kernels by timing them on the
+        current state (dem_autotune); returns the chosen shapes and times."""
+        t = abi.DemTuning()
+        self._call("autotune", self._h, C.c_int32(int(reps)), C.byref(t))
+        return t.as_dict()
+
+    def get_tuning(self) -> dict:
+        t = abi.DemTuning()
+        self._call("get_tuning", self._h, C.byref(t))
+        return t.as_dict()
+
+    def set_tuning(self, tuning: dict):
+        t = abi.DemTuning()
+        for k in ("pair_threads", "pair_blocks_per_sm", "gather_threads", "neigh_threads"):
+            setattr(t, k, int(tuning[k]))
+        self._call("set_tuning", self._h, C.byref(t))
+
     def force_error(self) -> float:
         v = C.c_double()
         self._call("force_error", self._h, C.byref(v))
@@ -345,6 +363,12 @@ class BatchSystem:
                    C.c_int64(max(P, 1)), C.c_int32(n))
         return ni, nb[:P].copy(), pf[:P].copy()
 
+    def total_stats(self) -> dict:
+        """dem_get_stats over the whole handle (all systems together)."""
+        s = abi.DemStats()
+        self._call("get_stats", self._h, C.byref(s))
+        return s.as_dict()
+
     def info(self, sid: int) -> dict:
         s = abi.DemSysStatus()
         self._call("sys_info", self._h, C.c_int32(sid), C.byref(s))
@@ -360,3 +384,9 @@ class BatchSystem:
         self._call("set_profiling", self._h, C.c_int32(1 if on else 0))
 
     profile = DemSystem.profile
+    pair_count = DemSystem.pair_count
+    set_stream = DemSystem.set_stream
+    set_graphs = DemSystem.set_graphs
+    autotune = DemSystem.autotune
+    get_tuning = DemSystem.get_tuning
+    set_tuning = DemSystem.set_tuning
