@@ -407,6 +407,7 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
   A((void**)&h->wall_pft, sizeof(double) * 3 * cmax * n);
   A((void**)&h->wall_live, n);
   A((void**)&h->wf, sizeof(double) * 6 * n);
+  A((void**)&h->touched, n);
   A((void**)&h->derr, sizeof(DevErr));
   A((void**)&h->d_np, sizeof(int));
   if (!ok) return DEM_ERR_CUDA;
@@ -473,7 +474,7 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec,
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched,
                   h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -612,6 +613,7 @@ int dem_upload_pairs(dem_handle* h, const int32_t* ni, const int32_t* nb, const 
   const int T = 256, B = (h->n + T - 1) / T;
   k_owner_from_rows<<<B, T, 0, h->stream>>>(h->n, h->row_end[h->rb], h->pair_owner);
   h->launches++;
+  set_hist_flags(h);
   if (int rc = build_transpose(h, h->rb)) return rc;
   h->have_pairs = true;
   return check_cuda(h, cudaStreamSynchronize(h->stream), "upload pairs");
@@ -739,10 +741,9 @@ static int replay_period(dem_handle* h, int nn0) {
   if (int rc = check_cuda(h, cudaGraphLaunch(h->graphs[key], h->stream), "graph launch")) return rc;
   h->launches += h->graph_kernels[key];
   // buffer parities and bookkeeping after the period: N force passes flip
-  // the state and history buffers, the rebuild flips the list and history
+  // the state buffers, the rebuild flips the list and history buffers
   for (int j = 0; j < nsn; ++j) {
     h->cur = 1 - h->cur;
-    h->pcur = 1 - h->pcur;
     h->s_time = h->s_time + h->prm.dtsolid;
     h->steps_done++;
   }

@@ -39,6 +39,12 @@ enum : unsigned {
   EF_NONFINITE   = 1u << 5,
 };
 
+// Per-pair flag bits (pflag) between force passes.
+enum : uint8_t {
+  PF_CONTACT = 1,   // in contact at the last force pass (its record is valid)
+  PF_HIST    = 2,   // its tangential history PFT is nonzero
+};
+
 struct DevErr {
   unsigned flags;
   int first_rogue;   // smallest rogue particle index of the last build (n if none)
@@ -213,13 +219,14 @@ struct dem_handle {
   int* row_cnt = nullptr;     // n
   int* row_end[2] = {nullptr, nullptr};   // n (current / previous build)
   int* nbrs[2] = {nullptr, nullptr};      // cap
-  double* pft[2] = {nullptr, nullptr};    // 3*cap
+  double* pft[2] = {nullptr, nullptr};    // 3*cap; pft[pcur] is current, the other takes the carry-over of a rebuild
   int* in_cnt = nullptr;      // n
   int* in_start = nullptr;    // n+1
   int* in_fill = nullptr;     // n
   int2* in_pair = nullptr;    // cap
   int* pair_owner = nullptr;  // cap
-  uint8_t* pflag = nullptr;   // cap: 1 = pair in contact at the last force pass (rank scratch in the build)
+  uint8_t* pflag = nullptr;   // cap: PF_* bits of each pair (stencil-rank scratch during the build)
+  uint8_t* touched = nullptr; // n: 1 = in some contact at the current force pass
   demb::PairRec* prec = nullptr; // cap: contact terms of the last force pass
   int rb = 0;                 // which row_end/nbrs buffer is current
 
@@ -286,6 +293,7 @@ void launch_gather_split(dem_handle* h, int mode);
 int ensure_pair_capacity(dem_handle* h, long long need);
 int build_transpose(dem_handle* h, int nb);    // neighbor.cu
 void launch_neigh_count(dem_handle* h);        // neighbor.cu: count pass of the pair build
+void set_hist_flags(dem_handle* h);            // neighbor.cu: PF_HIST from the current history
 void launch_pairs_only(dem_handle* h);         // force.cu: pair kernel of the handle's precision
 void launch_gather_only(dem_handle* h);        // force.cu: gather kernel, forces into FC/TOW
 // capi.cu: parameter block of a system with handle-wide particle count n

@@ -375,16 +375,19 @@ k_walls(DevParams p0, BatchView bv, WallCtx w, const double4* __restrict__ pos4,
 
 // Kernel 2 (per pair): one CC iteration of CALC_FORCE_DEM, evaluated once
 // per pair.  The apart test needs only the two positions; velocities, spins
-// and masses are gathered only for pairs in contact.  PFT_out is written for
-// every pair; the contact terms go to a compact record that both particles
-// read back in kernel 3.
+// and masses are gathered only for pairs in contact.  The tangential history
+// PFT is updated in place (only this kernel reads it).  pflag keeps, per
+// pair, PF_CONTACT (in contact at this pass) and PF_HIST (history nonzero),
+// so a pair that stays apart with a zero history costs no history traffic.
+// The contact terms go to a record that both particles read back in
+// kernel 3, and both particles of a contact are marked in `touched`.
 template <int COLL, bool B>
 __global__ void __launch_bounds__(256)
-k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
-        const double4* __restrict__ pos4, const double4* __restrict__ vel4, const double4* __restrict__ omg4,
-        const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
-        const double* __restrict__ pft_in, double* __restrict__ pft_out,
-        uint8_t* __restrict__ pflag, PairRec* __restrict__ prec, DevErr* __restrict__ err) {
+k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner,
+        const int* __restrict__ nbrs, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+        const double4* __restrict__ omg4, const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
+        double* __restrict__ pft, uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched,
+        PairRec* __restrict__ prec, DevErr* __restrict__ err) {
   // persistent grid-stride loop over the device-side pair count (the grid
   // size does not depend on the list, so the launch can live in a graph)
   const long long np = min((long long)*d_np, cap);
@@ -393,14 +396,11 @@ k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
   unsigned eflags = 0;
   for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
     const int ll = owner[cc], i = nbrs[cc];
-    const DevParams& p = sysp<B>(p0, bv, ll);
-    const double* pi = pft_in + 3 * cc;
-    double pin[3] = {pi[0], pi[1], pi[2]};
-    double* po = pft_out + 3 * cc;
-    uint8_t flag = 0;
-    if (state[i] == DEM_STATE_NONEXISTENT || state[ll] == DEM_STATE_NONEXISTENT) {
-      po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2];
-    } else {
+    const uint8_t f0 = pflag[cc];
+    uint8_t f = f0 & PF_HIST;  // NONEXISTENT partner or zero distance: history kept
+    double* ph = pft + 3 * cc;
+    if (state[i] != DEM_STATE_NONEXISTENT && state[ll] != DEM_STATE_NONEXISTENT) {
+      const DevParams& p = sysp<B>(p0, bv, ll);
       PState L, I;
       const double4 a = pos4[ll], b = pos4[i];
       L.x[0] = a.x; L.x[1] = a.y; L.x[2] = a.z; L.r = a.w;
@@ -416,9 +416,9 @@ k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
       }
       const double d2 = dot3(dist, dist);
       if (d2 > (r_lm - SMALL_NUMBER) * (r_lm - SMALL_NUMBER)) {
-        po[0] = po[1] = po[2] = 0.0;
+        if (f0 & PF_HIST) { ph[0] = 0.0; ph[1] = 0.0; ph[2] = 0.0; }
+        f = 0;
       } else if (d2 == 0.0) {
-        po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2];
         eflags |= EF_ZERO_DIST;
         err->zero_a = ll; err->zero_b = i;
       } else {
@@ -428,16 +428,20 @@ k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
         L.w[0] = wa.x; L.w[1] = wa.y; L.w[2] = wa.z;
         I.w[0] = wb.x; I.w[1] = wb.y; I.w[2] = wb.z;
         L.ph = phase[ll]; I.ph = phase[i];
+        double pin[3] = {0.0, 0.0, 0.0};
+        if (f0 & PF_HIST) { pin[0] = ph[0]; pin[1] = ph[1]; pin[2] = ph[2]; }
         double pout[3];
         PairRec r;
         contact_force<COLL>(p, L, I, dist, d2, pin, pout, r);
-        po[0] = pout[0]; po[1] = pout[1]; po[2] = pout[2];
+        ph[0] = pout[0]; ph[1] = pout[1]; ph[2] = pout[2];
         prec[cc] = r;
-        flag = 1;
+        touched[ll] = 1;
+        touched[i] = 1;
+        f = PF_CONTACT | ((pout[0] != 0.0 || pout[1] != 0.0 || pout[2] != 0.0) ? PF_HIST : 0);
         ++ncont;
       }
     }
-    pflag[cc] = flag;
+    if (f != f0) pflag[cc] = f;
   }
   for (int o = 16; o > 0; o >>= 1) {
     ncont += __shfl_down_sync(0xffffffffu, ncont, o);
@@ -469,7 +473,7 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
          double4* __restrict__ omg_n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
          const int* __restrict__ fbin_start, int nf, const double* __restrict__ wf,
          const int* __restrict__ row_end, const int* __restrict__ in_start, const int2* __restrict__ in_pair,
-         const uint8_t* __restrict__ pflag, const PairRec* __restrict__ prec,
+         const uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched, const PairRec* __restrict__ prec,
          double* __restrict__ fc, double* __restrict__ tow, double* __restrict__ acc_old,
          double* __restrict__ rot_acc_old) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
@@ -487,7 +491,10 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
       f[0] = o[0]; f[1] = o[1]; f[2] = o[2]; t[0] = o[3]; t[1] = o[4]; t[2] = o[5];
     }
   }
-  if (st != DEM_STATE_NONEXISTENT) {
+  // a particle in no contact this pass has no pair terms to add
+  const bool hit = touched[me] != 0;
+  if (hit) touched[me] = 0;
+  if (st != DEM_STATE_NONEXISTENT && hit) {
     const bool roll = p.mew_r > 0.0;
     double om = 0.0;
     if (roll) om = sqrt(dot3(w, w));
@@ -498,7 +505,7 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
       for (; q < ie; ++q) {
         const int2 e = in_pair[q];
         if (pass == 0 && e.x > me) break;
-        if (!pflag[e.y]) continue;
+        if (!(pflag[e.y] & PF_CONTACT)) continue;
         const PairRec o = prec[e.y];
 #pragma unroll
         for (int c = 0; c < 3; ++c) f[c] = f[c] - o.fc[c];
@@ -508,7 +515,7 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
       }
       if (pass == 0) {
         for (int cc = rs; cc < re; ++cc) {
-          if (!pflag[cc]) continue;
+          if (!(pflag[cc] & PF_CONTACT)) continue;
           const PairRec o = prec[cc];
 #pragma unroll
           for (int c = 0; c < 3; ++c) f[c] = f[c] + o.fc[c];
@@ -563,12 +570,11 @@ static void launch_walls_t(dem_handle* h) {
 
 template <int COLL, bool B>
 static void launch_pairs_t(dem_handle* h) {
-  const int c = h->cur, pc = h->pcur;
+  const int c = h->cur;
   const int T = h->tune.pair_threads;
-  k_pairs<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner,
-                                                         h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
-                                                         h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag,
-                                                         h->prec, h->derr);
+  k_pairs<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
+      h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
+      h->state, h->phase, h->pft[h->pcur], h->pflag, h->touched, h->prec, h->derr);
   DEM_LAUNCH(h);
 }
 
@@ -579,7 +585,7 @@ static void launch_gather_t(dem_handle* h) {
   k_gather<MODE, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
                                             h->vel4[1 - c], h->omg4[1 - c], h->state, h->dg_pijk, h->fbin_start,
                                             h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
-                                            h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
+                                            h->touched, h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
   DEM_LAUNCH(h);
 }
 
@@ -641,30 +647,43 @@ int run_force(dem_handle* h, bool fused) {
   const int mode = !fused ? 0 : (h->dp.intg == DEM_INTG_AB2 ? 2 : 1);
   launch_force_kernels(h, mode, h->dp.prec == DEM_PREC_SPLIT);
   if (int rc = check_cuda(h, cudaGetLastError(), "force kernels")) return rc;
-  h->pcur = 1 - h->pcur;
   if (fused) { h->cur = 1 - h->cur; h->first_pass = false; }
   return 0;
 }
 
 // Per-step force error of the split path: both paths evaluate FC for the
-// current state (the wall history is restored between and after them, the
-// pair history is read, not advanced); returns max|F_split - F_fp64| over
-// all components divided by max|F_fp64|.
+// current state (the wall and pair histories are restored between and after
+// them); returns max|F_split - F_fp64| over all components divided by
+// max|F_fp64|.
 int run_split_force_error(dem_handle* h, double* rel_err) {
   if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
-  const size_t n = h->n, cm = h->dp.cmax;
+  const size_t n = h->n, cm = h->dp.cmax, P = (size_t)host_pairs(h);
   const size_t b_fid = sizeof(int) * cm * n, b_pft = sizeof(double) * 3 * cm * n;
-  char* snap = (char*)stage_buffer(h, b_fid + b_pft + n + 64);
+  const size_t b_hist = sizeof(double) * 3 * P;
+  // both passes start from the same wall and pair histories (each pass
+  // updates them in place)
+  char* snap = (char*)stage_buffer(h, b_fid + b_pft + n + b_hist + P + 64);
   if (!snap) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
+  char* s_live = snap + b_fid + b_pft;
+  char* s_hist = s_live + n;
+  char* s_flag = s_hist + b_hist;
   auto save = [&]() {
     cudaMemcpyAsync(snap, h->wall_fid, b_fid, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(snap + b_fid, h->wall_pft, b_pft, cudaMemcpyDeviceToDevice, h->stream);
-    cudaMemcpyAsync(snap + b_fid + b_pft, h->wall_live, n, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(s_live, h->wall_live, n, cudaMemcpyDeviceToDevice, h->stream);
+    if (P) {
+      cudaMemcpyAsync(s_hist, h->pft[h->pcur], b_hist, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(s_flag, h->pflag, P, cudaMemcpyDeviceToDevice, h->stream);
+    }
   };
   auto restore = [&]() {
     cudaMemcpyAsync(h->wall_fid, snap, b_fid, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(h->wall_pft, snap + b_fid, b_pft, cudaMemcpyDeviceToDevice, h->stream);
-    cudaMemcpyAsync(h->wall_live, snap + b_fid + b_pft, n, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->wall_live, s_live, n, cudaMemcpyDeviceToDevice, h->stream);
+    if (P) {
+      cudaMemcpyAsync(h->pft[h->pcur], s_hist, b_hist, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(h->pflag, s_flag, P, cudaMemcpyDeviceToDevice, h->stream);
+    }
   };
   std::vector<double> f64(3 * n), f32(3 * n);
   h->dp.first_pass = 0;

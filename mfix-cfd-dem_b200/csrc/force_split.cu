@@ -41,9 +41,8 @@ __global__ void __launch_bounds__(256)
 k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
               const double4* __restrict__ pos4, const double4* __restrict__ vel4,
               const double4* __restrict__ omg4, const int8_t* __restrict__ state,
-              const uint8_t* __restrict__ phase, const double* __restrict__ pft_in,
-              double* __restrict__ pft_out, uint8_t* __restrict__ pflag, PairRec32* __restrict__ prec,
-              DevErr* __restrict__ err) {
+              const uint8_t* __restrict__ phase, double* __restrict__ pft, uint8_t* __restrict__ pflag,
+              uint8_t* __restrict__ touched, PairRec32* __restrict__ prec, DevErr* __restrict__ err) {
   // persistent grid-stride loop over the device-side pair count (the grid
   // size does not depend on the list, so the launch can live in a graph)
   const long long np = min((long long)*d_np, cap);
@@ -53,13 +52,10 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
   for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
     const int ll = owner[cc], i = nbrs[cc];
     const DevParams& p = sysp<B>(p0, bv, ll);
-    const double* pi = pft_in + 3 * cc;
-    const double pin[3] = {pi[0], pi[1], pi[2]};
-    double* po = pft_out + 3 * cc;
-    uint8_t flag = 0;
-    if (state[i] == DEM_STATE_NONEXISTENT || state[ll] == DEM_STATE_NONEXISTENT) {
-      po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2];
-    } else {
+    const uint8_t f0 = pflag[cc];
+    uint8_t f = f0 & PF_HIST;  // NONEXISTENT partner or zero distance: history kept
+    double* po = pft + 3 * cc;  // history updated in place (see k_pairs in force.cu)
+    if (state[i] != DEM_STATE_NONEXISTENT && state[ll] != DEM_STATE_NONEXISTENT) {
       const double4 a = pos4[ll], b = pos4[i];
       const double xl[3] = {a.x, a.y, a.z}, xi[3] = {b.x, b.y, b.z};
       double dist[3];
@@ -73,9 +69,9 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
       const double r_lm = a.w + b.w;
       const double d2 = dist[0] * dist[0] + dist[1] * dist[1] + dist[2] * dist[2];
       if (d2 > (r_lm - SMALL_NUMBER) * (r_lm - SMALL_NUMBER)) {
-        po[0] = po[1] = po[2] = 0.0;
+        if (f0 & PF_HIST) { po[0] = 0.0; po[1] = 0.0; po[2] = 0.0; }
+        f = 0;
       } else if (d2 == 0.0) {
-        po[0] = pin[0]; po[1] = pin[1]; po[2] = pin[2];
         eflags |= EF_ZERO_DIST;
         err->zero_a = ll; err->zero_b = i;
       } else {
@@ -119,6 +115,8 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
 #pragma unroll
         for (int c = 0; c < 3; ++c) fn[c] = -(kn * ov + etan * vrn) * nrm[c];
         // tangential history in FP64
+        double pin[3] = {0.0, 0.0, 0.0};
+        if (f0 & PF_HIST) { pin[0] = po[0]; pin[1] = po[1]; pin[2] = po[2]; }
         double ot[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) ot[c] = p.dt * (double)vt[c] + pin[c];
@@ -151,11 +149,13 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
         r.kn = kn;
         r.ov = ov;
         prec[cc] = r;
-        flag = 1;
+        touched[ll] = 1;
+        touched[i] = 1;
+        f = PF_CONTACT | ((ot[0] != 0.0 || ot[1] != 0.0 || ot[2] != 0.0) ? PF_HIST : 0);
         ++ncont;
       }
     }
-    pflag[cc] = flag;
+    if (f != f0) pflag[cc] = f;
   }
   for (int o = 16; o > 0; o >>= 1) {
     ncont += __shfl_down_sync(0xffffffffu, ncont, o);
@@ -174,7 +174,7 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
                double4* __restrict__ omg_n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
                const int* __restrict__ fbin_start, int nf, const double* __restrict__ wf,
                const int* __restrict__ row_end, const int* __restrict__ in_start,
-               const int2* __restrict__ in_pair, const uint8_t* __restrict__ pflag,
+               const int2* __restrict__ in_pair, const uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched,
                const PairRec32* __restrict__ prec, double* __restrict__ fc, double* __restrict__ tow,
                double* __restrict__ acc_old, double* __restrict__ rot_acc_old) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
@@ -194,7 +194,10 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
   }
   Comp3 F, T;
   F.zero(); T.zero();
-  if (st != DEM_STATE_NONEXISTENT) {
+  // a particle in no contact this pass has no pair terms to add
+  const bool hit = touched[me] != 0;
+  if (hit) touched[me] = 0;
+  if (st != DEM_STATE_NONEXISTENT && hit) {
     const float wf32[3] = {(float)w[0], (float)w[1], (float)w[2]};
     const float om = sqrtf(wf32[0] * wf32[0] + wf32[1] * wf32[1] + wf32[2] * wf32[2]);
     const bool roll = p.mew_r > 0.0 && om > 0.f;
@@ -203,7 +206,7 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
     const int is = in_start[me], ie = in_start[me + 1];
     for (int q = is; q < ie; ++q) {
       const int cc = in_pair[q].y;
-      if (!pflag[cc]) continue;
+      if (!(pflag[cc] & PF_CONTACT)) continue;
       const PairRec32 o = prec[cc];
 #pragma unroll
       for (int c = 0; c < 3; ++c) { F.add(c, -o.fc[c]); T.add(c, o.dci2 * o.tf[c]); }
@@ -214,7 +217,7 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
       }
     }
     for (int cc = rs; cc < re; ++cc) {
-      if (!pflag[cc]) continue;
+      if (!(pflag[cc] & PF_CONTACT)) continue;
       const PairRec32 o = prec[cc];
 #pragma unroll
       for (int c = 0; c < 3; ++c) { F.add(c, o.fc[c]); T.add(c, o.dcl2 * o.tf[c]); }
@@ -234,11 +237,11 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
 
 template <int COLL, bool B>
 static void launch_pairs_split_t(dem_handle* h) {
-  const int c = h->cur, pc = h->pcur;
+  const int c = h->cur;
   const int T = h->tune.pair_threads;
   k_pairs_split<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
       h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
-      h->state, h->phase, h->pft[pc], h->pft[1 - pc], h->pflag, (PairRec32*)h->prec, h->derr);
+      h->state, h->phase, h->pft[h->pcur], h->pflag, h->touched, (PairRec32*)h->prec, h->derr);
   DEM_LAUNCH(h);
 }
 
@@ -255,7 +258,7 @@ static void launch_gather_split_t(dem_handle* h) {
   k_gather_split<MODE, B><<<G, T, 0, h->stream>>>(
       h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
       h->state, h->dg_pijk, h->fbin_start, h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
-      (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
+      h->touched, (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
   DEM_LAUNCH(h);
 }
 

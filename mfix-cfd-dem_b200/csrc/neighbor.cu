@@ -238,7 +238,8 @@ __global__ void k_keep_rows(int n, BatchView bv, const int* __restrict__ old_end
 template <bool B>
 __global__ void k_remap(int n, BatchView bv, const int* __restrict__ row_end, const int* __restrict__ nbrs,
                         const int* __restrict__ old_end, const int* __restrict__ old_nbrs,
-                        const double* __restrict__ old_pft, double* __restrict__ pft, int have_old) {
+                        const double* __restrict__ old_pft, double* __restrict__ pft, uint8_t* __restrict__ pflag,
+                        int have_old) {
   const int ll = blockIdx.x * blockDim.x + threadIdx.x;
   if (ll >= n) return;
   if constexpr (B) {
@@ -257,7 +258,24 @@ __global__ void k_remap(int n, BatchView bv, const int* __restrict__ row_end, co
       }
     }
     pft[3 * (size_t)cc] = a; pft[3 * (size_t)cc + 1] = b; pft[3 * (size_t)cc + 2] = c;
+    pflag[cc] = (a != 0.0 || b != 0.0 || c != 0.0) ? PF_HIST : 0;
   }
+}
+
+// PF_HIST bits of a pair list whose history was set from the host.
+__global__ void k_hist_flags(const int* __restrict__ d_np, const double* __restrict__ pft,
+                             uint8_t* __restrict__ pflag) {
+  const long long np = *d_np, stride = (long long)gridDim.x * blockDim.x;
+  for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
+    const double* q = pft + 3 * cc;
+    pflag[cc] = (q[0] != 0.0 || q[1] != 0.0 || q[2] != 0.0) ? PF_HIST : 0;
+  }
+}
+
+void set_hist_flags(dem_handle* h) {
+  const int T = 256;
+  k_hist_flags<<<pair_grid(h, T), T, 0, h->stream>>>(h->d_np, h->pft[h->pcur], h->pflag);
+  DEM_LAUNCH(h);
 }
 
 __global__ void k_set_int(int* __restrict__ p, int v) { *p = v; }
@@ -336,6 +354,7 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
     cudaMemcpyAsync(pf[h->pcur], h->pft[h->pcur], sizeof(double) * 3 * old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(inp, h->in_pair, sizeof(int2) * old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(own, h->pair_owner, sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(pfl, h->pflag, old, cudaMemcpyDeviceToDevice, h->stream);
   }
   cudaStreamSynchronize(h->stream);
   for (int b = 0; b < 2; ++b) { cudaFree(h->nbrs[b]); cudaFree(h->pft[b]); h->nbrs[b] = nb[b]; h->pft[b] = pf[b]; }
@@ -424,10 +443,10 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   const int have_old = (carry_history && h->have_pairs) ? 1 : 0;
   if (bt)
     k_remap<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
-                                          h->pft[h->pcur], h->pft[pn], have_old);
+                                          h->pft[h->pcur], h->pft[pn], h->pflag, have_old);
   else
     k_remap<false><<<B, T, 0, h->stream>>>(n, bv, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
-                                           h->pft[h->pcur], h->pft[pn], have_old);
+                                           h->pft[h->pcur], h->pft[pn], h->pflag, have_old);
   DEM_LAUNCH(h);
   h->rb = nb;
   h->pcur = pn;

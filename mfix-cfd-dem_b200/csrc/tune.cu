@@ -4,11 +4,12 @@
 // resident blocks per SM of its persistent grid), the gather kernel
 // (threads per block) and the count pass of the pair build (threads per
 // block) are timed with CUDA events on the handle's stream, on the handle's
-// own current state, and the fastest shape of each is kept.  The timed
-// launches only write scratch that the next step rewrites (the other
-// history buffer, the contact records and flags, FC/TOW, the row counts), so
-// tuning does not change any result.  The launch shape does not change the
-// arithmetic, so results are also the same under every shape.
+// own current state, and the fastest shape of each is kept.  The pair
+// history and its flags, which the pair kernel updates in place, are saved
+// before and restored after the timing; everything else the timed launches
+// write is scratch that the next step rewrites (contact records, FC/TOW, row
+// counts), so tuning does not change any result.  The launch shape does not
+// change the arithmetic, so results are also the same under every shape.
 #include "dem_internal.cuh"
 
 #include <cfloat>
@@ -58,6 +59,13 @@ int dem_autotune(dem_handle* h, int32_t reps, dem_tuning* out) {
   if (reps < 1) return set_err(h, DEM_ERR_ARG, "reps must be positive");
   if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
   invalidate_graphs(h);
+  const size_t P = (size_t)host_pairs(h);
+  char* snap = (char*)stage_buffer(h, sizeof(double) * 3 * P + P + 64);
+  if (!snap) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
+  if (P) {
+    cudaMemcpyAsync(snap, h->pft[h->pcur], sizeof(double) * 3 * P, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(snap + sizeof(double) * 3 * P, h->pflag, P, cudaMemcpyDeviceToDevice, h->stream);
+  }
   const int threads[3] = {64, 128, 256};
   const int bpsm[4] = {2, 4, 8, 16};
   float best_p = FLT_MAX, best_g = FLT_MAX, best_n = FLT_MAX;
@@ -69,11 +77,15 @@ int dem_autotune(dem_handle* h, int32_t reps, dem_tuning* out) {
       const float ms = time_launches(h, reps, [&] { launch_pairs_only(h); });
       if (ms < best_p) { best_p = ms; best.pair_threads = T; best.pair_bpsm = b; }
     }
+  // the gather reads the contact marks the pair kernel sets, so each timed
+  // gather runs behind a pair launch (at the best pair shape)
   h->tune = t;
+  h->tune.pair_threads = best.pair_threads;
+  h->tune.pair_bpsm = best.pair_bpsm;
   for (int T : threads) {
     h->tune.gather_threads = T;
-    const float ms = time_launches(h, reps, [&] { launch_gather_only(h); });
-    if (ms < best_g) { best_g = ms; best.gather_threads = T; }
+    const float ms = time_launches(h, reps, [&] { launch_pairs_only(h); launch_gather_only(h); });
+    if (ms - best_p < best_g) { best_g = ms - best_p; best.gather_threads = T; }
   }
   h->tune = t;
   const int nthreads[3] = {32, 64, 128};
@@ -83,6 +95,10 @@ int dem_autotune(dem_handle* h, int32_t reps, dem_tuning* out) {
     if (ms < best_n) { best_n = ms; best.neigh_threads = T; }
   }
   h->tune = best;
+  if (P) {
+    cudaMemcpyAsync(h->pft[h->pcur], snap, sizeof(double) * 3 * P, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->pflag, snap + sizeof(double) * 3 * P, P, cudaMemcpyDeviceToDevice, h->stream);
+  }
   // the timed pair launches added to the contact counters
   cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
   if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "autotune")) return rc;
