@@ -137,7 +137,9 @@ typedef struct dem_handle dem_handle;
 
 /* Allocates device state for max_pip particles (MAX_PIP) on the current CUDA
  * device.  Replaces the DES allocation in des_allocate_mod.f and the constant
- * set-up of CHECK_SOLIDS_DEM (the derived tables are taken from *p). */
+ * set-up of CHECK_SOLIDS_DEM (the derived tables are taken from *p).
+ * Limits: max_pip < 2^27; at most 1021 interior DES cells along x and z and
+ * 4093 along y (DEM_ERR_ARG otherwise). */
 int dem_create(const dem_params* p, int32_t max_pip, dem_handle** out);
 int dem_destroy(dem_handle* h);
 const char* dem_last_error(const dem_handle* h);

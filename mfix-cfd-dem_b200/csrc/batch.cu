@@ -153,7 +153,7 @@ extern "C" {
 
 int dem_params_cells(const dem_params* q, int32_t* des_cells, int32_t* search_cells) {
   if (!q || !des_cells || !search_cells) return DEM_ERR_ARG;
-  if (q->dg_imax < 1 || q->dg_jmax < 1 || (!q->no_k && q->dg_kmax < 1)) return DEM_ERR_ARG;
+  if (!des_grid_ok(*q)) return DEM_ERR_ARG;
   DevParams dp;
   fill_devparams(*q, 1, dp);
   *des_cells = dp.ncell2 + 1;
@@ -163,7 +163,7 @@ int dem_params_cells(const dem_params* q, int32_t* des_cells, int32_t* search_ce
 
 int dem_batch_create(const dem_params* q, const dem_batch_limits* lim, dem_handle** out) {
   if (!q || !lim || !out) return DEM_ERR_ARG;
-  if (lim->max_particles <= 0 || lim->max_systems <= 0 || lim->max_systems > 65535 || lim->max_cells <= 0 ||
+  if (lim->max_particles <= 0 || lim->max_particles > MAX_PARTICLES || lim->max_systems <= 0 || lim->max_systems > 65535 || lim->max_cells <= 0 ||
       lim->max_search_cells <= 0 || lim->max_facets < 0 || lim->max_facet_bins < 0)
     return DEM_ERR_ARG;
   if (q->n_phases < 1 || q->n_phases > DEM_MAX_PHASES || !(q->dtsolid > 0.0)) return DEM_ERR_ARG;
@@ -227,8 +227,8 @@ int dem_sys_add(dem_handle* h, const dem_params* q, int32_t max_pip, int32_t* sy
   if (!same_kind(*q, h->prm))
     return set_err(h, DEM_ERR_ARG, "collision model, integrator, force precision and COLLISION_ARRAY_MAX "
                                    "must be the same for all systems of a batch");
-  if (q->n_phases < 1 || q->n_phases > DEM_MAX_PHASES || q->dg_imax < 1 || q->dg_jmax < 1 ||
-      (!q->no_k && q->dg_kmax < 1) || q->neighbor_search_n < 1 || !(q->dtsolid > 0.0))
+  if (q->n_phases < 1 || q->n_phases > DEM_MAX_PHASES || !des_grid_ok(*q) || q->neighbor_search_n < 1 ||
+      !(q->dtsolid > 0.0))
     return set_err(h, DEM_ERR_ARG, "bad system parameters");
   for (int a = 0; a < 3; ++a) {
     const int cells = a == 0 ? q->dg_imax : (a == 1 ? q->dg_jmax : q->dg_kmax);

@@ -263,6 +263,13 @@ int stats_range(dem_handle* h, int off, int cnt, dem_stats* s) {
 
 }  // namespace demb
 
+// Interior DES cells per axis at least 1 and, with the ghost layers, within
+// the packed (i, j, k) of the pair build.
+bool demb::des_grid_ok(const dem_params& q) {
+  if (q.dg_imax < 1 || q.dg_jmax < 1 || (!q.no_k && q.dg_kmax < 1)) return false;
+  return q.dg_imax + 2 <= DG_MAX_IK && q.dg_jmax + 2 <= DG_MAX_J && (q.no_k || q.dg_kmax + 2 <= DG_MAX_IK);
+}
+
 void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
   memset(&p, 0, sizeof p);
   p.n = n;
@@ -398,6 +405,7 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
   A((void**)&h->fcell_list, sizeof(int) * n);
   A((void**)&h->spos, sizeof(double4) * n);
   A((void**)&h->sinfo, sizeof(int4) * n);
+  A((void**)&h->nslot, sizeof(uint32_t) * NSLOT * n);
   A((void**)&h->row_cnt, sizeof(int) * n);
   A((void**)&h->in_cnt, sizeof(int) * n);
   A((void**)&h->in_start, sizeof(int) * (n + 1));
@@ -441,9 +449,9 @@ int dem_abi_version(void) { return DEM_ABI_VERSION; }
 const char* dem_last_error(const dem_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
 int dem_create(const dem_params* q, int32_t max_pip, dem_handle** out) {
-  if (!q || !out || max_pip <= 0) return DEM_ERR_ARG;
+  if (!q || !out || max_pip <= 0 || max_pip > MAX_PARTICLES) return DEM_ERR_ARG;
   if (q->n_phases < 1 || q->n_phases > DEM_MAX_PHASES) return DEM_ERR_ARG;
-  if (q->dg_imax < 1 || q->dg_jmax < 1 || (!q->no_k && q->dg_kmax < 1)) return DEM_ERR_ARG;
+  if (!des_grid_ok(*q)) return DEM_ERR_ARG;
   if (q->neighbor_search_n < 1 || !(q->dtsolid > 0.0)) return DEM_ERR_ARG;
   for (int a = 0; a < 3; ++a) {
     int cells = a == 0 ? q->dg_imax : (a == 1 ? q->dg_jmax : q->dg_kmax);
@@ -475,7 +483,7 @@ int dem_destroy(dem_handle* h) {
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
                   h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched,
-                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->d_np,
+                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }

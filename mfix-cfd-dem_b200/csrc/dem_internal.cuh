@@ -196,7 +196,8 @@ struct dem_handle {
   int* fcell_start = nullptr; // nfcell+1
   int* fcell_list = nullptr;  // n
   double4* spos = nullptr;    // n: positions in search-cell order (pair build)
-  int4* sinfo = nullptr;      // n: (particle, DES cell, state, search cell) in that order
+  int4* sinfo = nullptr;      // n: (particle, packed DES cell (i,j,k), state, search cell) in that order
+  uint32_t* nslot = nullptr;  // n * NSLOT: rows kept by the count pass of the pair build
 
   // pairs
   long long pair_cap = 0;
@@ -298,6 +299,7 @@ void launch_pairs_only(dem_handle* h);         // force.cu: pair kernel of the h
 void launch_gather_only(dem_handle* h);        // force.cu: gather kernel, forces into FC/TOW
 // capi.cu: parameter block of a system with handle-wide particle count n
 void fill_devparams(const dem_params& q, int n, DevParams& p);
+bool des_grid_ok(const dem_params& q);
 int alloc_handle(dem_handle* h, int nc, int nfc, long long pairs);
 int upload_range(dem_handle* h, int off, int cnt, int nph, const double* pos, const double* vel,
                  const double* omega, const double* radius, const double* pmass, const double* omoi,
@@ -351,6 +353,20 @@ __device__ __forceinline__ int dg_iof(const DevParams& p, int ijk) {
 __device__ __forceinline__ int dg_kof(const DevParams& p, int ijk) {
   return (ijk - p.c3 - dg_iof(p, ijk) * p.c1 - dg_jof(p, ijk)) / p.c2;
 }
+// A DES cell as (i, j, k) in one int: 10 bits for i and k, 12 for j (the
+// handle set-up checks the grid fits).
+constexpr int DG_MAX_IK = 1023, DG_MAX_J = 4095;
+__device__ __forceinline__ int pack_ijk(int i, int j, int k) { return i | (j << 10) | (k << 22); }
+__device__ __forceinline__ void unpack_ijk(int c, int& i, int& j, int& k) {
+  i = c & 1023;
+  j = (c >> 10) & 4095;
+  k = (c >> 22) & 1023;
+}
+
+// Neighbours per particle kept by the count pass of the pair build.
+constexpr int NSLOT = 16;
+constexpr int MAX_PARTICLES = (1 << 27) - 1;  // particle index in 27 bits of a kept key
+
 __device__ __forceinline__ int dg_ofpos(const DevParams& p, int ax, double x, int start1) {
   return (int)floor((x - p.dg_start[ax]) * p.dg_inv[ax]) + start1;
 }

@@ -84,19 +84,28 @@ __global__ void k_delete_rogue(DevParams p0, BatchView bv, int8_t* __restrict__ 
 // pass inserts it into the row sorted by (rank, index), which is the order
 // of the reference's cell-by-cell scan.
 // The search runs over a cell-sorted copy of the candidate data: sinfo[q] =
-// (particle, DES cell, state, search cell) and spos[q] = (x, y, z, r) in the
-// order of the search-grid cell lists.  Thread q handles particle sinfo[q].x,
-// so a warp holds spatially adjacent particles that scan the same cells, and
-// every candidate read is a contiguous run of the sorted arrays.
-__global__ void k_sorted_copy(int n, const int* __restrict__ n_exist, const int* __restrict__ flist,
-                              const double4* __restrict__ pos4, const int8_t* __restrict__ state,
-                              const int* __restrict__ dg_pijk, const int* __restrict__ fkey,
-                              double4* __restrict__ spos, int4* __restrict__ sinfo) {
+// (particle, DES cell as packed (i, j, k), state, search cell) and spos[q] =
+// (x, y, z, r) in the order of the search-grid cell lists.  Thread q handles
+// particle sinfo[q].x, so a warp holds spatially adjacent particles that scan
+// the same cells, and every candidate read is a contiguous run of the sorted
+// arrays.
+//
+// The count pass also keeps the first NSLOT neighbours of each particle,
+// already in row order, as (rank << 27 | index) keys in nslot[q]; the fill
+// pass copies them, and rescans only the particles with longer rows.
+template <bool B>
+__global__ void k_sorted_copy(DevParams p0, BatchView bv, int n, const int* __restrict__ n_exist,
+                              const int* __restrict__ flist, const double4* __restrict__ pos4,
+                              const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
+                              const int* __restrict__ fkey, double4* __restrict__ spos, int4* __restrict__ sinfo) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n || q >= *n_exist) return;
   const int i = flist[q];
+  const DevParams& p = sysp<B>(p0, bv, i);
+  const int c = dg_pijk[i];
   spos[q] = pos4[i];
-  sinfo[q] = make_int4(i, dg_pijk[i], (int)state[i], fkey[i]);
+  // the DES cell as (i, j, k), unpacked by every particle that scans this one
+  sinfo[q] = make_int4(i, pack_ijk(dg_iof(p, c), dg_jof(p, c), dg_kof(p, c)), (int)state[i], fkey[i]);
 }
 
 template <bool FILL, bool B>
@@ -104,7 +113,7 @@ __global__ void __launch_bounds__(128)
 k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
         const int4* __restrict__ sinfo, const int* __restrict__ fstart, const DevErr* __restrict__ err,
         int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
-        uint8_t* __restrict__ rank_buf, int* __restrict__ owner, long long cap) {
+        uint8_t* __restrict__ rank_buf, int* __restrict__ owner, uint32_t* __restrict__ nslot, long long cap) {
   const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (q0 >= p0.n || q0 >= *n_exist) return;
   const int4 me = sinfo[q0];
@@ -112,12 +121,25 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
   const DevParams& p = sysp<B>(p0, bv, cur);
   const int first_rogue = B ? bv.first_rogue[bv.sys_of[cur]] : err->first_rogue;
   if (me.z != DEM_STATE_NORMAL || cur >= first_rogue) return;
+  uint32_t* slot = nslot + (size_t)q0 * NSLOT;
   int start = 0;
-  if (FILL) start = (int)min((long long)row_se[cur], cap);
+  if (FILL) {
+    start = (int)min((long long)row_se[cur], cap);
+    const int kept = row_cnt[cur];
+    if (kept <= NSLOT) {
+      // the count pass kept the whole row
+      for (int c = 0; c < kept; ++c) {
+        const long long s = (long long)start + c;
+        if (s < cap) { nbrs[s] = (int)(slot[c] & 0x7ffffffu); owner[s] = cur; }
+      }
+      row_se[cur] = (int)min((long long)start + kept, cap);
+      return;
+    }
+  }
   int cnt = 0;
   {
-    const int lijk = me.y;
-    const int lic = dg_iof(p, lijk), ljc = dg_jof(p, lijk), lkc = dg_kof(p, lijk);
+    int lic, ljc, lkc;
+    unpack_ijk(me.y, lic, ljc, lkc);
     const int rc[3] = {lic, ljc, lkc};
     const int s1[3] = {p.istart1, p.jstart1, p.kstart1}, e1[3] = {p.iend1, p.jend1, p.kend1};
     const int ncl[3] = {p.iend1 - p.istart1 + 1, p.jend1 - p.jstart1 + 1, p.kend1 - p.kstart1 + 1};
@@ -161,8 +183,8 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
         if (nb < cur && o.z == DEM_STATE_NORMAL) continue;
         if (o.z == DEM_STATE_NONEXISTENT) continue;
         // position of the neighbour's DES cell in the reference stencil
-        const int nijk = o.y;
-        const int nc[3] = {dg_iof(p, nijk), dg_jof(p, nijk), dg_kof(p, nijk)};
+        int nc[3];
+        unpack_ijk(o.y, nc[0], nc[1], nc[2]);
         int rel[3];
         double sh[3] = {0.0, 0.0, 0.0};
         bool in_stencil = true;
@@ -188,8 +210,15 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
         const double d0 = cp.x - px, d1 = cp.y - py, d2 = cp.z - pz;
         const double dd = d0 * d0 + d1 * d1 + d2 * d2;
         if (dd > srad * srad) continue;
+        const int rank = ((rel[2] + 1) * 3 + (rel[1] + 1)) * 3 + (rel[0] + 1);
+        if (!FILL && cnt < NSLOT) {
+          // keep the row sorted by (rank, index) in the slots
+          const uint32_t key = ((uint32_t)rank << 27) | (uint32_t)nb;
+          int b = cnt - 1;
+          while (b >= 0 && slot[b] > key) { slot[b + 1] = slot[b]; --b; }
+          slot[b + 1] = key;
+        }
         if (FILL) {
-          const int rank = ((rel[2] + 1) * 3 + (rel[1] + 1)) * 3 + (rel[0] + 1);
           long long slot = (long long)start + cnt;
           if (slot < cap) {
             // insertion into the row kept sorted by (rank, index)
@@ -372,10 +401,10 @@ void launch_neigh_count(dem_handle* h) {
   const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : h->dp.nfcell);
   if (bt)
     k_neigh<false, true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sinfo, h->fcell_start,
-                                                 h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, 0);
+                                                 h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, h->nslot, 0);
   else
     k_neigh<false, false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sinfo, h->fcell_start,
-                                                  h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, 0);
+                                                  h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, h->nslot, 0);
   DEM_LAUNCH(h);
 }
 
@@ -395,8 +424,12 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   DEM_LAUNCH(h);
   const int nb = 1 - h->rb;  // new list goes into the other buffer
   const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : p.nfcell);
-  k_sorted_copy<<<B, T, 0, h->stream>>>(n, n_exist, h->fcell_list, h->pos4[h->cur], h->state, h->dg_pijk,
-                                        h->fcell_key, h->spos, h->sinfo);
+  if (bt)
+    k_sorted_copy<true><<<B, T, 0, h->stream>>>(p, bv, n, n_exist, h->fcell_list, h->pos4[h->cur], h->state,
+                                                h->dg_pijk, h->fcell_key, h->spos, h->sinfo);
+  else
+    k_sorted_copy<false><<<B, T, 0, h->stream>>>(p, bv, n, n_exist, h->fcell_list, h->pos4[h->cur], h->state,
+                                                 h->dg_pijk, h->fcell_key, h->spos, h->sinfo);
   DEM_LAUNCH(h);
   if (int rc = check_cuda(h, cudaMemsetAsync(h->row_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
   launch_neigh_count(h);
@@ -419,14 +452,16 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   }
   const int TN = h->tune.neigh_threads, BN = (n + TN - 1) / TN;
   if (bt) {
-    k_neigh<true, true><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
-                                                  h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+    k_neigh<true, true><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
+                                                  h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->nslot,
+                                                  h->pair_cap);
     k_keep_rows<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], nullptr, h->row_end[nb],
                                               h->nbrs[nb], h->pair_owner, h->pair_cap);
     DEM_LAUNCH(h);
   } else {
-    k_neigh<true, false><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, nullptr,
-                                                   h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->pair_cap);
+    k_neigh<true, false><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
+                                                   h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->nslot,
+                                                   h->pair_cap);
   }
   DEM_LAUNCH(h);
   k_clamp_np<<<1, 1, 0, h->stream>>>(h->d_np, h->pair_cap, e);
