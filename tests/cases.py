@@ -33,6 +33,51 @@ def dem01_case(intg, kn, en):
     return case, prm, arr, walls
 
 
+def dem03_case(en, en_w):
+    """DEM03 (tests/dem/DEM03/mfix.dat): two 1 mm spheres (rho 2e4 and 1e4,
+    phases 1 and 2) stacked between the bottom and top walls of a 1 x 1.8 mm
+    x 1 m box, each overlapping its wall and the other; LSD KN = KN_W = 1e3,
+    KT_FAC = KT_W_FAC = 1, DES_ETAT_FAC = DES_ETAT_W_FAC = 1, no friction,
+    Adams-Bashforth, one DES cell."""
+    case = P.DemCase(n_phases=2, d_p0=(1e-3, 1e-3), ro_s0=(2.0e4, 1.0e4), coll_model="LSD",
+                     intg_method="ADAMS_BASHFORTH", kn=1.0e3, kn_w=1.0e3, kt_fac=1.0, kt_w_fac=1.0,
+                     des_etat_fac=1.0, des_etat_w_fac=1.0, des_en_input=en, des_en_wall_input=[en_w, en_w],
+                     mew=0.0, mew_w=0.0, grav=(0.0, -9.80665, 0.0), domain_hi=(1.0, 0.0018, 1.0),
+                     neighbor_search_n=99, desgridsearch=(1, 1, 1))
+    pos = np.array([[0.5, 0.5], [0.00045, 0.00135], [0.5, 0.5]])
+    arr = state_arrays(pos, np.zeros((3, 2)), np.zeros((3, 2)), np.array([0.0005, 0.0005]),
+                       np.array([2.0e4, 1.0e4]), phase=[1, 2])
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    walls = P.default_walls(case.domain_lo, case.domain_hi)
+    return case, prm, arr, walls
+
+
+def dem05_case(model, particle_input):
+    """DEM05 (tests/dem/DEM05/mfix.dat): 93 spheres of 5 mm in a 0.5 x 0.1 x
+    0.5 m box without gravity: 31 phase-1 spheres (rho 4000) strike the floor
+    at impact angles 0-65 degrees, 31 strike fixed phase-2 targets (rho
+    5000; particles 63-93, reset every step by USR2_DES); Adams-Bashforth,
+    friction 0.092, elastic (e_n = e_t = 1).  model: "LSD" (KN = KN_W =
+    1.72e7, KT_FAC = 1.48/1.72) or "HERTZ" (E = 380e9 / 70e9, wall 70e9,
+    nu = 0.23 / 0.25, wall 0.25)."""
+    a = np.asarray(particle_input, dtype=np.float64).reshape(-1, 8)
+    n = a.shape[0]
+    kw = dict(n_phases=2, d_p0=(5.0e-3, 5.0e-3), ro_s0=(4.0e3, 5.0e3), intg_method="ADAMS_BASHFORTH",
+              des_en_input=1.0, des_en_wall_input=[1.0, 1.0], mew=0.092, mew_w=0.092,
+              grav=(0.0, 0.0, 0.0), domain_hi=(0.5, 0.1, 0.5), fluid_cells=(5, 1, 5))
+    if model == "LSD":
+        case = P.DemCase(coll_model="LSD", kn=1.72e7, kn_w=1.72e7, kt_fac=1.48 / 1.72, kt_w_fac=1.48 / 1.72, **kw)
+    else:
+        case = P.DemCase(coll_model="HERTZ", e_young=(380.0e9, 70.0e9), v_poisson=(0.23, 0.25),
+                         ew_young=70.0e9, vw_poisson=0.25, des_et_input=1.0, des_et_wall_input=[1.0, 1.0], **kw)
+    phase = np.where(a[:, 4] > 4500.0, 2, 1)
+    arr = state_arrays(a[:, 0:3].T.copy(), a[:, 5:8].T.copy(), np.zeros((3, n)), a[:, 3].copy(), a[:, 4].copy(),
+                       phase=phase)
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    walls = P.default_walls(case.domain_lo, case.domain_hi)
+    return case, prm, arr, walls
+
+
 def settling_case(n_side=(6, 20, 6), d=1e-3, rho=2500.0, box=(12e-3, 60e-3, 12e-3),
                   spacing=1.1, jitter=0.04, vmax=0.1, seed=1000, coll="LSD", intg="EULER",
                   kn=1000.0, en=0.9, mew=0.1, nsn=25, polydisperse=0.0, mew_r=0.0,
