@@ -322,6 +322,7 @@ int dem_sys_upload_state(dem_handle* h, int32_t s, const double* pos, const doub
   if (int rc = upload_range(h, S.dp.p_begin, max_pip, S.prm.n_phases, pos, vel, omega, radius, pmass, omoi,
                             state, phase))
     return rc;
+  skin_unknown(h);
   S.have_state = true;
   return 0;
 }

@@ -416,6 +416,10 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
   A((void**)&h->wall_live, n);
   A((void**)&h->wf, sizeof(double) * 6 * n);
   A((void**)&h->touched, n);
+  A((void**)&h->wall_hit, n);
+  A((void**)&h->wall_cand, n);
+  A((void**)&h->skin, sizeof(double));
+  A((void**)&h->vslot, sizeof(unsigned) * 32);
   A((void**)&h->derr, sizeof(DevErr));
   A((void**)&h->d_np, sizeof(int));
   if (!ok) return DEM_ERR_CUDA;
@@ -482,7 +486,7 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched,
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->skin, h->vslot, h->pgap,
                   h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -522,6 +526,7 @@ int dem_upload_state(dem_handle* h, const double* pos, const double* vel, const 
   SINGLE_GUARD(h);
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip does not match dem_create");
   if (int rc = upload_range(h, 0, h->n, h->dp.nph, pos, vel, omega, radius, pmass, omoi, state, phase)) return rc;
+  skin_unknown(h);  // positions changed from outside: no pair is known apart until the next build
   h->have_state = true;
   return 0;
 }
@@ -622,6 +627,7 @@ int dem_upload_pairs(dem_handle* h, const int32_t* ni, const int32_t* nb, const 
   k_owner_from_rows<<<B, T, 0, h->stream>>>(h->n, h->row_end[h->rb], h->pair_owner);
   h->launches++;
   set_hist_flags(h);
+  skin_unknown(h);  // no gaps for an uploaded list: no pair is skipped until the next build
   if (int rc = build_transpose(h, h->rb)) return rc;
   h->have_pairs = true;
   return check_cuda(h, cudaStreamSynchronize(h->stream), "upload pairs");

@@ -227,7 +227,11 @@ struct dem_handle {
   int2* in_pair = nullptr;    // cap
   int* pair_owner = nullptr;  // cap
   uint8_t* pflag = nullptr;   // cap: PF_* bits of each pair (stencil-rank scratch during the build)
-  uint8_t* touched = nullptr; // n: 1 = in some contact at the current force pass
+  uint8_t* touched = nullptr; // n: 1 = in some pair contact at the current force pass
+  uint8_t* wall_hit = nullptr; // n: 1 = in some wall contact (its terms are in wf)
+  float* pgap = nullptr;      // cap: gap |d| - (r_i + r_j) of each pair at the last build, rounded down
+  double* skin = nullptr;     // [0]: bound on any particle's displacement since the last build
+  unsigned* vslot = nullptr;  // [32]: per-step displacement bounds, as float bits
   demb::PairRec* prec = nullptr; // cap: contact terms of the last force pass
   int rb = 0;                 // which row_end/nbrs buffer is current
 
@@ -242,7 +246,8 @@ struct dem_handle {
   int* wall_fid = nullptr;    // [i][cmax]
   double* wall_pft = nullptr; // [i][cmax][3]
   uint8_t* wall_live = nullptr; // [i] 1 when some wall slot may be in use
-  double* wf = nullptr;       // [i][6] wall force and torque of the last force pass
+  uint8_t* wall_cand = nullptr; // [i] 1 when the particle's DES cell holds facets
+  double* wf = nullptr;       // [i][6] wall force and torque of the last force pass (valid with wall_hit)
 
   // scan scratch
   int* scan_tmp = nullptr;
@@ -295,6 +300,10 @@ int ensure_pair_capacity(dem_handle* h, long long need);
 int build_transpose(dem_handle* h, int nb);    // neighbor.cu
 void launch_neigh_count(dem_handle* h);        // neighbor.cu: count pass of the pair build
 void set_hist_flags(dem_handle* h);            // neighbor.cu: PF_HIST from the current history
+void launch_pair_gaps(dem_handle* h);          // neighbor.cu: pair gaps at a build, displacement bound 0
+void launch_skin(dem_handle* h);               // force.cu: adds the step's displacement to the bound
+void skin_unknown(dem_handle* h);              // force.cu: positions changed from outside: no pair skipped
+void launch_wall_cand(dem_handle* h);          // desgrid.cu: facet-cell flag of every particle
 void launch_pairs_only(dem_handle* h);         // force.cu: pair kernel of the handle's precision
 void launch_gather_only(dem_handle* h);        // force.cu: gather kernel, forces into FC/TOW
 // capi.cu: parameter block of a system with handle-wide particle count n
@@ -381,6 +390,22 @@ __device__ __forceinline__ double periodic_shift(const DevParams& p, int ax, dou
   return 0.0;
 }
 
+// Adds a particle's displacement bound of this step (max(|v|, |v_new|)*dt,
+// as float bits rounded up) to the per-step maximum.  Called by every active
+// lane of a warp; one atomic per warp, spread over 32 slots.
+__device__ __forceinline__ void note_displacement(unsigned* __restrict__ vslot, double disp) {
+  const unsigned bits = __float_as_uint(__double2float_ru(disp));
+  const unsigned mask = __activemask();
+  const unsigned m = __reduce_max_sync(mask, bits);
+  const int lane = threadIdx.x & 31;
+  if (lane == __ffs(mask) - 1 && m)
+    atomicMax(&vslot[((blockIdx.x * blockDim.x + threadIdx.x) >> 5) & 31], m);
+}
+
+__device__ __forceinline__ double speed(const double v[3]) {
+  return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+}
+
 // Result of the force sum of one particle: either stored into FC/TOW
 // (MODE 0) or integrated as CFUPDATEOLD + CFNEWVALUES (cfupdateold.f:33-41,
 // cfnewvalues.f:700-812) into the other state buffer (MODE 1 = Euler,
@@ -393,7 +418,7 @@ __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8
                                                 double4* __restrict__ pos_n, double4* __restrict__ vel_n,
                                                 double4* __restrict__ omg_n, double* __restrict__ fc,
                                                 double* __restrict__ tow, double* __restrict__ acc_old,
-                                                double* __restrict__ rot_acc_old) {
+                                                double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot) {
   const size_t n = (size_t)p.n;
   if (MODE == 0) {
 #pragma unroll
@@ -437,6 +462,8 @@ __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8
   pos_n[me] = make_double4(xn[0], xn[1], xn[2], r);
   vel_n[me] = make_double4(vn[0], vn[1], vn[2], m);
   omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+  // |x_new - x| <= max(|v|, |v_new|) * dt for both integrators
+  note_displacement(vslot, st < DEM_STATE_NORMAL_GHOST ? fmax(speed(v), speed(vn)) * dt : 0.0);
 }
 
 }  // namespace demb

@@ -20,7 +20,8 @@ namespace demb {
 // as the reference does between rebuilds).
 template <bool B>
 __global__ void k_cell_keys(DevParams p0, BatchView bv, double4* __restrict__ pos4,
-                            const int8_t* __restrict__ state, int* __restrict__ dg_pijk) {
+                            const int8_t* __restrict__ state, int* __restrict__ dg_pijk,
+                            const int* __restrict__ fbin_start, uint8_t* __restrict__ wall_cand) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, i);
@@ -28,7 +29,7 @@ __global__ void k_cell_keys(DevParams p0, BatchView bv, double4* __restrict__ po
   if constexpr (B) {
     if (!bv.due[bv.sys_of[i]] && !per) return;
   }
-  if (state[i] == DEM_STATE_NONEXISTENT) { dg_pijk[i] = 0; return; }
+  if (state[i] == DEM_STATE_NONEXISTENT) { dg_pijk[i] = 0; wall_cand[i] = 0; return; }
   double4 x = pos4[i];
   if (per) {
     bool moved = false;
@@ -52,7 +53,34 @@ __global__ void k_cell_keys(DevParams p0, BatchView bv, double4* __restrict__ po
   int li = min(p.iend2, max(p.istart2, dg_ofpos(p, 0, x.x, p.istart1)));
   int lj = min(p.jend2, max(p.jstart2, dg_ofpos(p, 1, x.y, p.jstart1)));
   int lk = p.no_k ? 1 : min(p.kend2, max(p.kstart2, dg_ofpos(p, 2, x.z, p.kstart1)));
-  dg_pijk[i] = dg_funijk(p, li, lj, lk);
+  const int c = dg_funijk(p, li, lj, lk);
+  dg_pijk[i] = c;
+  const int fc = p.cell_off + c - 1;
+  wall_cand[i] = fbin_start[fc + 1] > fbin_start[fc] ? 1 : 0;
+}
+
+// The facet-cell flag of every particle from its current DES cell (after
+// the walls change).
+template <bool B>
+__global__ void k_wall_cand(DevParams p0, BatchView bv, const int8_t* __restrict__ state,
+                            const int* __restrict__ dg_pijk, const int* __restrict__ fbin_start,
+                            uint8_t* __restrict__ wall_cand) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p0.n) return;
+  const DevParams& p = sysp<B>(p0, bv, i);
+  const int c = dg_pijk[i];
+  if (state[i] == DEM_STATE_NONEXISTENT || c < 1) { wall_cand[i] = 0; return; }
+  const int fc = p.cell_off + c - 1;
+  wall_cand[i] = fbin_start[fc + 1] > fbin_start[fc] ? 1 : 0;
+}
+
+void launch_wall_cand(dem_handle* h) {
+  const int T = 256, B = (h->n + T - 1) / T;
+  if (h->batch())
+    k_wall_cand<true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), h->state, h->dg_pijk, h->fbin_start, h->wall_cand);
+  else
+    k_wall_cand<false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), h->state, h->dg_pijk, h->fbin_start, h->wall_cand);
+  DEM_LAUNCH(h);
 }
 
 // Search-grid cell of every existing particle (for the pair build), as an
@@ -102,8 +130,12 @@ int run_desgrid_pic(dem_handle* h, bool bin_search) {
   const bool bt = h->batch();
   const BatchView bv = h->bview();
   const int nfc = bt ? h->nfcell_total : p.nfcell;
-  if (bt) k_cell_keys<true><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk);
-  else k_cell_keys<false><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk);
+  if (bt)
+    k_cell_keys<true><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk, h->fbin_start,
+                                              h->wall_cand);
+  else
+    k_cell_keys<false><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk, h->fbin_start,
+                                               h->wall_cand);
   DEM_LAUNCH(h);
   if (!bin_search) return check_cuda(h, cudaGetLastError(), "k_cell_keys");
   if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * nfc, h->stream), "memset")) return rc;

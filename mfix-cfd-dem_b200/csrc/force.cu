@@ -222,18 +222,19 @@ __device__ __forceinline__ int get_collision(const DevParams& p, const WallCtx& 
   return free_index;
 }
 
+// The wall contacts of one particle in a cell with facets.  `live` says
+// whether any of its history slots may be in use; when none is, no slot is
+// searched for the facets it does not touch (REMOVE_COLLISION would find
+// nothing).  The particle's velocity, spin, mass and phase are read at its
+// first contact only.
 template <int COLL>
-__device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, const PState& s,
-                              double f[3], double t[3], unsigned long long& nwc, unsigned& eflags) {
+__device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, PState& s, bool live,
+                              const double4* __restrict__ vel4, const double4* __restrict__ omg4,
+                              const uint8_t* __restrict__ phase, double f[3], double t[3],
+                              unsigned long long& nwc, unsigned& eflags) {
   const int cell = p.cell_off + w.dg_pijk[me] - 1;
   const int fs = w.fbin_start[cell], fe = w.fbin_start[cell + 1];
-  if (fe - fs < 1) {
-    int* fid = w.wall_fid + (size_t)me * p.cmax;
-    double* wp = w.wall_pft + (size_t)me * p.cmax * 3;
-    for (int q = 0; q < p.cmax; ++q) fid[q] = -1;
-    for (int q = 0; q < 3 * p.cmax; ++q) wp[q] = 0.0;
-    return;
-  }
+  bool have_kin = false;
   const double r = s.r;
   const double radsq = r * r;
   double pmax[3], pmin[3];
@@ -242,20 +243,27 @@ __device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, cons
   for (int q = fs; q < fe; ++q) {
     const FacetBinEntry e = w.fbin[q];
     const int nf = e.id;
-    if (e.mn > pmax[e.dir]) { remove_collision(p, w, me, nf); continue; }
-    if (e.mx < pmin[e.dir]) { remove_collision(p, w, me, nf); continue; }
+    if (e.mn > pmax[e.dir]) { if (live) remove_collision(p, w, me, nf); continue; }
+    if (e.mx < pmin[e.dir]) { if (live) remove_collision(p, w, me, nf); continue; }
     const double* V = w.vertex + 9 * (size_t)nf;
     const double* N = w.norm_face + 3 * (size_t)nf;
     double d1[3] = {V[0] - s.x[0], V[1] - s.x[1], V[2] - s.x[2]};
     double nn[3] = {N[0], N[1], N[2]};
     const double line_t = dot3(d1, nn);
-    if (line_t <= -1.0001 * r) { remove_collision(p, w, me, nf); continue; }
+    if (line_t <= -1.0001 * r) { if (live) remove_collision(p, w, me, nf); continue; }
     double cpt[3]; bool poe; int edge;
     closest_pt(p, w, nf, s.x, cpt, poe, edge);
     double dist[3] = {cpt[0] - s.x[0], cpt[1] - s.x[1], cpt[2] - s.x[2]};
     const double distsq = dot3(dist, dist);
-    if (distsq >= radsq - SMALL_NUMBER) { remove_collision(p, w, me, nf); continue; }
+    if (distsq >= radsq - SMALL_NUMBER) { if (live) remove_collision(p, w, me, nf); continue; }
     if (poe && w.ignore_edge[4 * (size_t)nf + edge]) continue;
+    if (!have_kin) {
+      const double4 b = vel4[me], c = omg4[me];
+      s.v[0] = b.x; s.v[1] = b.y; s.v[2] = b.z; s.m = b.w;
+      s.w[0] = c.x; s.w[1] = c.y; s.w[2] = c.z;
+      s.ph = phase[me];
+      have_kin = true;
+    }
     const double distmod = sqrt(distsq);
     double nrm[3] = {dist[0], dist[1], dist[2]};
     if (distsq > 0) { const double sq = sqrt(distsq); for (int c = 0; c < 3; ++c) nrm[c] = dist[c] / sq; }
@@ -337,14 +345,14 @@ template <int COLL, bool B>
 __global__ void __launch_bounds__(128)
 k_walls(DevParams p0, BatchView bv, WallCtx w, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
         const double4* __restrict__ omg4, const uint8_t* __restrict__ phase, const int8_t* __restrict__ state,
-        uint8_t* __restrict__ wall_live, double* __restrict__ wf, DevErr* __restrict__ err) {
+        uint8_t* __restrict__ wall_live, const uint8_t* __restrict__ wall_cand, double* __restrict__ wf,
+        uint8_t* __restrict__ wall_hit, DevErr* __restrict__ err) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long nwc = 0;
   unsigned eflags = 0;
   if (me < p0.n && state[me] == DEM_STATE_NORMAL) {
     const DevParams& p = sysp<B>(p0, bv, me);
-    const int cell = p.cell_off + w.dg_pijk[me] - 1;
-    if (w.fbin_start[cell + 1] - w.fbin_start[cell] < 1) {
+    if (!wall_cand[me]) {
       // no facet near: clear the history once (calc_collision_wall_mod.f:194-198)
       if (wall_live[me]) {
         int* fid = w.wall_fid + (size_t)me * p.cmax;
@@ -355,12 +363,26 @@ k_walls(DevParams p0, BatchView bv, WallCtx w, const double4* __restrict__ pos4,
       }
     } else {
       PState S;
-      load_p(pos4, vel4, omg4, phase, me, S);
+      const double4 a = pos4[me];
+      S.x[0] = a.x; S.x[1] = a.y; S.x[2] = a.z; S.r = a.w;
       double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
-      wall_contacts<COLL>(p, w, me, S, f, t, nwc, eflags);
-      wall_live[me] = 1;
-      double* o = wf + 6 * (size_t)me;
-      o[0] = f[0]; o[1] = f[1]; o[2] = f[2]; o[3] = t[0]; o[4] = t[1]; o[5] = t[2];
+      const bool live = wall_live[me] != 0;
+      const unsigned long long nwc0 = nwc;
+      wall_contacts<COLL>(p, w, me, S, live, vel4, omg4, phase, f, t, nwc, eflags);
+      const bool hit = nwc > nwc0;
+      bool used = hit;
+      if (!hit && live) {
+        const int* fid = w.wall_fid + (size_t)me * p.cmax;
+        for (int q = 0; q < p.cmax; ++q) used = used || fid[q] != -1;
+      }
+      if (used != live) wall_live[me] = used ? 1 : 0;
+      if (hit) {
+        // the wall terms are the first terms of FC/TOW; the gather reads
+        // them only for particles marked here
+        double* o = wf + 6 * (size_t)me;
+        o[0] = f[0]; o[1] = f[1]; o[2] = f[2]; o[3] = t[0]; o[4] = t[1]; o[5] = t[2];
+        wall_hit[me] = 1;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -374,7 +396,11 @@ k_walls(DevParams p0, BatchView bv, WallCtx w, const double4* __restrict__ pos4,
 }
 
 // Kernel 2 (per pair): one CC iteration of CALC_FORCE_DEM, evaluated once
-// per pair.  The apart test needs only the two positions; velocities, spins
+// per pair.  A pair whose gap at the last build is more than twice the
+// bound on any particle's displacement since (and whose history is zero) is
+// apart without a look at the particles: the reference's apart test would
+// find it apart and leave its zero history zero, so it is skipped.  The
+// apart test of the others needs only the two positions; velocities, spins
 // and masses are gathered only for pairs in contact.  The tangential history
 // PFT is updated in place (only this kernel reads it).  pflag keeps, per
 // pair, PF_CONTACT (in contact at this pass) and PF_HIST (history nonzero),
@@ -387,16 +413,24 @@ k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
         const int* __restrict__ nbrs, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
         const double4* __restrict__ omg4, const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
         double* __restrict__ pft, uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched,
-        PairRec* __restrict__ prec, DevErr* __restrict__ err) {
+        const float* __restrict__ pgap, const double* __restrict__ skin, PairRec* __restrict__ prec,
+        DevErr* __restrict__ err) {
   // persistent grid-stride loop over the device-side pair count (the grid
   // size does not depend on the list, so the launch can live in a graph)
   const long long np = min((long long)*d_np, cap);
   const long long stride = (long long)gridDim.x * blockDim.x;
+  const double reach = 2.0 * skin[0];
   unsigned long long ncont = 0;
   unsigned eflags = 0;
   for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
-    const int ll = owner[cc], i = nbrs[cc];
     const uint8_t f0 = pflag[cc];
+    // provably apart: its gap at the build exceeds what the two particles
+    // can have closed since, and its history is zero (stays zero)
+    if (!(f0 & PF_HIST) && (double)pgap[cc] > reach) {
+      if (f0) pflag[cc] = 0;
+      continue;
+    }
+    const int ll = owner[cc], i = nbrs[cc];
     uint8_t f = f0 & PF_HIST;  // NONEXISTENT partner or zero distance: history kept
     double* ph = pft + 3 * cc;
     if (state[i] != DEM_STATE_NONEXISTENT && state[ll] != DEM_STATE_NONEXISTENT) {
@@ -470,12 +504,12 @@ template <int MODE, bool B>
 __global__ void __launch_bounds__(256)
 k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
          const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
-         double4* __restrict__ omg_n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
-         const int* __restrict__ fbin_start, int nf, const double* __restrict__ wf,
+         double4* __restrict__ omg_n, const int8_t* __restrict__ state, const double* __restrict__ wf,
          const int* __restrict__ row_end, const int* __restrict__ in_start, const int2* __restrict__ in_pair,
-         const uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched, const PairRec* __restrict__ prec,
+         const uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched, uint8_t* __restrict__ wall_hit,
+         const PairRec* __restrict__ prec,
          double* __restrict__ fc, double* __restrict__ tow, double* __restrict__ acc_old,
-         double* __restrict__ rot_acc_old) {
+         double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
   if (me >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, me);
@@ -484,17 +518,15 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
   const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
   const double r = X.w, m = V.w, omoi = W.w;
   double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
-  if (st == DEM_STATE_NORMAL && nf > 0) {
-    const int cell = p.cell_off + dg_pijk[me] - 1;
-    if (fbin_start[cell + 1] > fbin_start[cell]) {
-      const double* o = wf + 6 * (size_t)me;
-      f[0] = o[0]; f[1] = o[1]; f[2] = o[2]; t[0] = o[3]; t[1] = o[4]; t[2] = o[5];
-    }
+  // the contacts of this pass; a particle in none has no terms to add
+  const bool wh = wall_hit[me] != 0, ph = touched[me] != 0;
+  if (wh) wall_hit[me] = 0;
+  if (ph) touched[me] = 0;
+  if (wh && st == DEM_STATE_NORMAL) {
+    const double* o = wf + 6 * (size_t)me;
+    f[0] = o[0]; f[1] = o[1]; f[2] = o[2]; t[0] = o[3]; t[1] = o[4]; t[2] = o[5];
   }
-  // a particle in no contact this pass has no pair terms to add
-  const bool hit = touched[me] != 0;
-  if (hit) touched[me] = 0;
-  if (st != DEM_STATE_NONEXISTENT && hit) {
+  if (st != DEM_STATE_NONEXISTENT && ph) {
     const bool roll = p.mew_r > 0.0;
     double om = 0.0;
     if (roll) om = sqrt(dot3(w, w));
@@ -527,7 +559,7 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
     }
   }
   finish_particle<MODE>(p, me, st, x, v, w, r, m, omoi, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
-                        rot_acc_old);
+                        rot_acc_old, vslot);
 }
 
 // CFUPDATEOLD + CFNEWVALUES from FC/TOW, in place; zeroes FC/TOW.
@@ -535,7 +567,8 @@ template <int INTG, bool B>
 __global__ void k_integrate(DevParams p0, BatchView bv, double4* __restrict__ pos4, double4* __restrict__ vel4,
                             double4* __restrict__ omg4, const int8_t* __restrict__ state,
                             double* __restrict__ fc, double* __restrict__ tow,
-                            double* __restrict__ acc_old, double* __restrict__ rot_acc_old) {
+                            double* __restrict__ acc_old, double* __restrict__ rot_acc_old,
+                            unsigned* __restrict__ vslot) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
   if (me >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, me);
@@ -548,7 +581,7 @@ __global__ void k_integrate(DevParams p0, BatchView bv, double4* __restrict__ po
     fc[c * n + me] = 0.0; tow[c * n + me] = 0.0;
   }
   finish_particle<INTG == DEM_INTG_AB2 ? 2 : 1>(p, me, state[me], x, v, w, X.w, V.w, W.w, f, t, pos4, vel4, omg4,
-                                                fc, tow, acc_old, rot_acc_old);
+                                                fc, tow, acc_old, rot_acc_old, vslot);
 }
 
 static WallCtx wall_ctx(dem_handle* h) {
@@ -564,7 +597,7 @@ static void launch_walls_t(dem_handle* h) {
   const int c = h->cur;
   const int T = 128, G = (h->n + T - 1) / T;
   k_walls<COLL, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->pos4[c], h->vel4[c], h->omg4[c],
-                                           h->phase, h->state, h->wall_live, h->wf, h->derr);
+                                           h->phase, h->state, h->wall_live, h->wall_cand, h->wf, h->wall_hit, h->derr);
   DEM_LAUNCH(h);
 }
 
@@ -574,7 +607,7 @@ static void launch_pairs_t(dem_handle* h) {
   const int T = h->tune.pair_threads;
   k_pairs<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
       h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
-      h->state, h->phase, h->pft[h->pcur], h->pflag, h->touched, h->prec, h->derr);
+      h->state, h->phase, h->pft[h->pcur], h->pflag, h->touched, h->pgap, h->skin, h->prec, h->derr);
   DEM_LAUNCH(h);
 }
 
@@ -583,9 +616,9 @@ static void launch_gather_t(dem_handle* h) {
   const int T = h->tune.gather_threads, G = (h->n + T - 1) / T;
   const int c = h->cur;
   k_gather<MODE, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
-                                            h->vel4[1 - c], h->omg4[1 - c], h->state, h->dg_pijk, h->fbin_start,
-                                            h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
-                                            h->touched, h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
+                                            h->vel4[1 - c], h->omg4[1 - c], h->state, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
+                                            h->touched, h->wall_hit, h->prec, h->fc, h->tow, h->acc_old,
+                                            h->rot_acc_old, h->vslot);
   DEM_LAUNCH(h);
 }
 
@@ -641,11 +674,32 @@ static void launch_force_kernels(dem_handle* h, int mode, bool split) {
   else launch_pairs_gather<false>(h, mode);
 }
 
+// Displacement bound since the last build += this step's largest particle
+// displacement bound; the slots are cleared for the next step.
+__global__ void k_skin(double* __restrict__ skin, unsigned* __restrict__ vslot) {
+  const unsigned m = __reduce_max_sync(0xffffffffu, vslot[threadIdx.x]);
+  vslot[threadIdx.x] = 0;
+  if (threadIdx.x == 0) skin[0] = skin[0] + (double)__uint_as_float(m);
+}
+
+__global__ void k_set_skin(double* __restrict__ skin, double v) { skin[0] = v; }
+
+void launch_skin(dem_handle* h) {
+  k_skin<<<1, 32, 0, h->stream>>>(h->skin, h->vslot);
+  DEM_LAUNCH(h);
+}
+
+void skin_unknown(dem_handle* h) {
+  k_set_skin<<<1, 1, 0, h->stream>>>(h->skin, HUGE_VAL);
+  DEM_LAUNCH(h);
+}
+
 int run_force(dem_handle* h, bool fused) {
   ProfScope ps(h, DEM_PROF_FORCE);
   h->dp.first_pass = h->first_pass ? 1 : 0;
   const int mode = !fused ? 0 : (h->dp.intg == DEM_INTG_AB2 ? 2 : 1);
   launch_force_kernels(h, mode, h->dp.prec == DEM_PREC_SPLIT);
+  if (fused) launch_skin(h);
   if (int rc = check_cuda(h, cudaGetLastError(), "force kernels")) return rc;
   if (fused) { h->cur = 1 - h->cur; h->first_pass = false; }
   return 0;
@@ -709,7 +763,7 @@ static void launch_integrate_t(dem_handle* h) {
   const int T = 256, G = (h->n + T - 1) / T;
   const int c = h->cur;
   k_integrate<INTG, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->state,
-                                               h->fc, h->tow, h->acc_old, h->rot_acc_old);
+                                               h->fc, h->tow, h->acc_old, h->rot_acc_old, h->vslot);
   DEM_LAUNCH(h);
 }
 
@@ -719,6 +773,7 @@ int run_cfnewvalues(dem_handle* h) {
   const bool ab2 = h->dp.intg == DEM_INTG_AB2;
   if (h->batch()) ab2 ? launch_integrate_t<DEM_INTG_AB2, true>(h) : launch_integrate_t<DEM_INTG_EULER, true>(h);
   else ab2 ? launch_integrate_t<DEM_INTG_AB2, false>(h) : launch_integrate_t<DEM_INTG_EULER, false>(h);
+  launch_skin(h);
   h->first_pass = false;
   return check_cuda(h, cudaGetLastError(), "k_integrate");
 }

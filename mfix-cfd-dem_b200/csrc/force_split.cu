@@ -42,17 +42,24 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
               const double4* __restrict__ pos4, const double4* __restrict__ vel4,
               const double4* __restrict__ omg4, const int8_t* __restrict__ state,
               const uint8_t* __restrict__ phase, double* __restrict__ pft, uint8_t* __restrict__ pflag,
-              uint8_t* __restrict__ touched, PairRec32* __restrict__ prec, DevErr* __restrict__ err) {
+              uint8_t* __restrict__ touched, const float* __restrict__ pgap, const double* __restrict__ skin,
+              PairRec32* __restrict__ prec, DevErr* __restrict__ err) {
   // persistent grid-stride loop over the device-side pair count (the grid
   // size does not depend on the list, so the launch can live in a graph)
   const long long np = min((long long)*d_np, cap);
   const long long stride = (long long)gridDim.x * blockDim.x;
   unsigned long long ncont = 0;
   unsigned eflags = 0;
+  const double reach = 2.0 * skin[0];
   for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
+    const uint8_t f0 = pflag[cc];
+    // provably apart (see k_pairs in force.cu)
+    if (!(f0 & PF_HIST) && (double)pgap[cc] > reach) {
+      if (f0) pflag[cc] = 0;
+      continue;
+    }
     const int ll = owner[cc], i = nbrs[cc];
     const DevParams& p = sysp<B>(p0, bv, ll);
-    const uint8_t f0 = pflag[cc];
     uint8_t f = f0 & PF_HIST;  // NONEXISTENT partner or zero distance: history kept
     double* po = pft + 3 * cc;  // history updated in place (see k_pairs in force.cu)
     if (state[i] != DEM_STATE_NONEXISTENT && state[ll] != DEM_STATE_NONEXISTENT) {
@@ -171,12 +178,12 @@ template <int MODE, bool B>
 __global__ void __launch_bounds__(256)
 k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
                const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
-               double4* __restrict__ omg_n, const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
-               const int* __restrict__ fbin_start, int nf, const double* __restrict__ wf,
+               double4* __restrict__ omg_n, const int8_t* __restrict__ state, const double* __restrict__ wf,
                const int* __restrict__ row_end, const int* __restrict__ in_start,
                const int2* __restrict__ in_pair, const uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched,
+               uint8_t* __restrict__ wall_hit,
                const PairRec32* __restrict__ prec, double* __restrict__ fc, double* __restrict__ tow,
-               double* __restrict__ acc_old, double* __restrict__ rot_acc_old) {
+               double* __restrict__ acc_old, double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
   if (me >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, me);
@@ -185,19 +192,17 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
   const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
   const double r = X.w, m = V.w, omoi = W.w;
   double f0[3] = {0.0, 0.0, 0.0}, t0[3] = {0.0, 0.0, 0.0};
-  if (st == DEM_STATE_NORMAL && nf > 0) {
-    const int cell = p.cell_off + dg_pijk[me] - 1;
-    if (fbin_start[cell + 1] > fbin_start[cell]) {
-      const double* o = wf + 6 * (size_t)me;
-      f0[0] = o[0]; f0[1] = o[1]; f0[2] = o[2]; t0[0] = o[3]; t0[1] = o[4]; t0[2] = o[5];
-    }
+  // the contacts of this pass; a particle in none has no terms to add
+  const bool wh = wall_hit[me] != 0, ph = touched[me] != 0;
+  if (wh) wall_hit[me] = 0;
+  if (ph) touched[me] = 0;
+  if (wh && st == DEM_STATE_NORMAL) {
+    const double* o = wf + 6 * (size_t)me;
+    f0[0] = o[0]; f0[1] = o[1]; f0[2] = o[2]; t0[0] = o[3]; t0[1] = o[4]; t0[2] = o[5];
   }
   Comp3 F, T;
   F.zero(); T.zero();
-  // a particle in no contact this pass has no pair terms to add
-  const bool hit = touched[me] != 0;
-  if (hit) touched[me] = 0;
-  if (st != DEM_STATE_NONEXISTENT && hit) {
+  if (st != DEM_STATE_NONEXISTENT && ph) {
     const float wf32[3] = {(float)w[0], (float)w[1], (float)w[2]};
     const float om = sqrtf(wf32[0] * wf32[0] + wf32[1] * wf32[1] + wf32[2] * wf32[2]);
     const bool roll = p.mew_r > 0.0 && om > 0.f;
@@ -232,7 +237,7 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
 #pragma unroll
   for (int c = 0; c < 3; ++c) { f[c] = f0[c] + F.value(c); t[c] = t0[c] + T.value(c); }
   finish_particle<MODE>(p, me, st, x, v, w, r, m, omoi, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
-                        rot_acc_old);
+                        rot_acc_old, vslot);
 }
 
 template <int COLL, bool B>
@@ -241,7 +246,8 @@ static void launch_pairs_split_t(dem_handle* h) {
   const int T = h->tune.pair_threads;
   k_pairs_split<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
       h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
-      h->state, h->phase, h->pft[h->pcur], h->pflag, h->touched, (PairRec32*)h->prec, h->derr);
+      h->state, h->phase, h->pft[h->pcur], h->pflag, h->touched, h->pgap, h->skin, (PairRec32*)h->prec,
+      h->derr);
   DEM_LAUNCH(h);
 }
 
@@ -257,8 +263,8 @@ static void launch_gather_split_t(dem_handle* h) {
   const int c = h->cur;
   k_gather_split<MODE, B><<<G, T, 0, h->stream>>>(
       h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
-      h->state, h->dg_pijk, h->fbin_start, h->nf, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
-      h->touched, (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old);
+      h->state, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
+      h->touched, h->wall_hit, (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old, h->vslot);
   DEM_LAUNCH(h);
 }
 

@@ -301,6 +301,51 @@ __global__ void k_hist_flags(const int* __restrict__ d_np, const double* __restr
   }
 }
 
+// Gap of every pair at a build: |x_i - x_l| - (r_l + r_i), less a margin of
+// 1e-9 (r_l + r_i) for the rounding of the distance, rounded down to float;
+// -1 for pairs with a NONEXISTENT particle.  The displacement bound restarts
+// at zero.
+template <bool B>
+__global__ void k_pair_gaps(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
+                            const int* __restrict__ owner, const int* __restrict__ nbrs,
+                            const double4* __restrict__ pos4, const int8_t* __restrict__ state,
+                            float* __restrict__ pgap, double* __restrict__ skin) {
+  const long long np = min((long long)*d_np, cap), stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t0 == 0) skin[0] = 0.0;
+  for (long long cc = t0; cc < np; cc += stride) {
+    const int ll = owner[cc], i = nbrs[cc];
+    if (state[ll] == DEM_STATE_NONEXISTENT || state[i] == DEM_STATE_NONEXISTENT) { pgap[cc] = -1.0f; continue; }
+    const DevParams& p = sysp<B>(p0, bv, ll);
+    const double4 a = pos4[ll], b = pos4[i];
+    const double xl[3] = {a.x, a.y, a.z}, xi[3] = {b.x, b.y, b.z};
+    double d2 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double pj = xi[c];
+      const double s = periodic_shift(p, c, pj - xl[c]);
+      if (s != 0.0) pj = pj + s;
+      const double d = pj - xl[c];
+      d2 += d * d;
+    }
+    const double r_lm = a.w + b.w;
+    pgap[cc] = __double2float_rd(sqrt(d2) - r_lm - 1e-9 * r_lm);
+  }
+}
+
+void launch_pair_gaps(dem_handle* h) {
+  const int T = 256;
+  if (h->batch())
+    k_pair_gaps<true><<<pair_grid(h, T), T, 0, h->stream>>>(h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner,
+                                                            h->nbrs[h->rb], h->pos4[h->cur], h->state, h->pgap,
+                                                            h->skin);
+  else
+    k_pair_gaps<false><<<pair_grid(h, T), T, 0, h->stream>>>(h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner,
+                                                             h->nbrs[h->rb], h->pos4[h->cur], h->state, h->pgap,
+                                                             h->skin);
+  DEM_LAUNCH(h);
+}
+
 void set_hist_flags(dem_handle* h) {
   const int T = 256;
   k_hist_flags<<<pair_grid(h, T), T, 0, h->stream>>>(h->d_np, h->pft[h->pcur], h->pflag);
@@ -368,7 +413,7 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   long long cap = h->pair_cap > 0 ? h->pair_cap : 1024;
   while (cap < need) cap *= 2;
   const long long old = h->pair_cap;  // the whole old allocation (the count may be stale)
-  int* nb[2]; double* pf[2]; int2* inp; int* own; uint8_t* pfl; PairRec* prc;
+  int* nb[2]; double* pf[2]; int2* inp; int* own; uint8_t* pfl; PairRec* prc; float* gap;
   for (int b = 0; b < 2; ++b) {
     if (int rc = check_cuda(h, cudaMalloc(&nb[b], sizeof(int) * cap), "cudaMalloc nbrs")) return rc;
     if (int rc = check_cuda(h, cudaMalloc(&pf[b], sizeof(double) * 3 * cap), "cudaMalloc pft")) return rc;
@@ -377,6 +422,7 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   if (int rc = check_cuda(h, cudaMalloc(&own, sizeof(int) * cap), "cudaMalloc owner")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&pfl, cap), "cudaMalloc pflag")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&prc, sizeof(PairRec) * cap), "cudaMalloc prec")) return rc;
+  if (int rc = check_cuda(h, cudaMalloc(&gap, sizeof(float) * cap), "cudaMalloc pgap")) return rc;
   if (old > 0) {
     // keep the current list and history (the rebuild reads them)
     cudaMemcpyAsync(nb[h->rb], h->nbrs[h->rb], sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
@@ -384,11 +430,12 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
     cudaMemcpyAsync(inp, h->in_pair, sizeof(int2) * old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(own, h->pair_owner, sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(pfl, h->pflag, old, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(gap, h->pgap, sizeof(float) * old, cudaMemcpyDeviceToDevice, h->stream);
   }
   cudaStreamSynchronize(h->stream);
   for (int b = 0; b < 2; ++b) { cudaFree(h->nbrs[b]); cudaFree(h->pft[b]); h->nbrs[b] = nb[b]; h->pft[b] = pf[b]; }
-  cudaFree(h->in_pair); cudaFree(h->pair_owner); cudaFree(h->pflag); cudaFree(h->prec);
-  h->in_pair = inp; h->pair_owner = own; h->pflag = pfl; h->prec = prc;
+  cudaFree(h->in_pair); cudaFree(h->pair_owner); cudaFree(h->pflag); cudaFree(h->prec); cudaFree(h->pgap);
+  h->in_pair = inp; h->pair_owner = own; h->pflag = pfl; h->prec = prc; h->pgap = gap;
   h->pair_cap = cap;
   invalidate_graphs(h);  // captured steps point at the old arrays
   return check_cuda(h, cudaGetLastError(), "grow pairs");
@@ -486,6 +533,7 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   h->rb = nb;
   h->pcur = pn;
   h->have_pairs = true;
+  launch_pair_gaps(h);
   return build_transpose(h, nb);
 }
 

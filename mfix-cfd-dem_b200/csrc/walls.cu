@@ -167,7 +167,10 @@ int run_bin_facets(dem_handle* h, const double* vf, const double* nfort, int nf)
   h->nf = nf;
   h->n_fbin = 0;
   if (int rc = check_cuda(h, cudaMemsetAsync(h->fbin_start, 0, sizeof(int) * (p.ncell2 + 1), h->stream), "memset")) return rc;
-  if (nf == 0) return check_cuda(h, cudaStreamSynchronize(h->stream), "sync");
+  if (nf == 0) {
+    launch_wall_cand(h);
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "sync");
+  }
   // Fortran VERTEX(3,3,F) [v + 3c + 9f] -> device [f][v][c]
   std::vector<double> vx((size_t)9 * nf), nx((size_t)3 * nf);
   for (int f = 0; f < nf; ++f)
@@ -200,6 +203,7 @@ int run_bin_facets(dem_handle* h, const double* vf, const double* nfort, int nf)
   k_edge_flags<<<B, T, 0, h->stream>>>(p.ncell2, h->fbin_start, h->fbin, h->vertex, h->norm_face, cos_nb,
                                        h->ignore_edge);
   DEM_LAUNCH(h);
+  launch_wall_cand(h);
   return check_cuda(h, cudaStreamSynchronize(h->stream), "bin facets");
 }
 
@@ -222,7 +226,10 @@ int run_bin_facets_sys(dem_handle* h, int sys, const double* vf, const double* n
   S.nf = 0; S.nbin = 0; S.fac_off = 0; S.bin_off = 0;
   int* fs = h->fbin_start + p.cell_off;
   if (int rc = check_cuda(h, cudaMemsetAsync(fs, 0, sizeof(int) * (p.ncell2 + 1), h->stream), "memset")) return rc;
-  if (nf == 0) return check_cuda(h, cudaStreamSynchronize(h->stream), "sync");
+  if (nf == 0) {
+    launch_wall_cand(h);
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "sync");
+  }
   const int fo = h->fac_alloc.take(nf, 1);
   if (fo < 0) return set_err(h, DEM_ERR_CAPACITY, "batch facet capacity exhausted");
   S.fac_off = fo; S.nf = nf;
@@ -253,6 +260,7 @@ int run_bin_facets_sys(dem_handle* h, int sys, const double* vf, const double* n
   const double cos_nb = std::cos((double)5.0f / 180.0 * pi) + 1.0e-6;
   k_edge_flags<<<B, T, 0, h->stream>>>(p.ncell2, fs, h->fbin, h->vertex, h->norm_face, cos_nb, h->ignore_edge);
   DEM_LAUNCH(h);
+  launch_wall_cand(h);
   return check_cuda(h, cudaStreamSynchronize(h->stream), "bin facets");
 }
 
