@@ -31,6 +31,10 @@ struct Gas {
   double* vol_surr = nullptr;  // ncell
   double* rop_s = nullptr;     // (M, ncell)
   double* rops_node = nullptr; // (M, ncell)
+  double* vol_node = nullptr;  // ncell: DES_VOL_NODE
+  double* drag_am = nullptr;   // ncell: DRAG_AM per node
+  double* drag_bm = nullptr;   // (3, ncell): DRAG_BM per node
+  double* f_gds = nullptr;     // ncell: F_GDS per cell
   int* pijk = nullptr;         // (n, 4): i, j, k, ijk (1-based), 0 = none
   double* f_gp = nullptr;      // n
   int* pic_cnt = nullptr; int* pic_start = nullptr; int* pic_list = nullptr;
@@ -142,24 +146,17 @@ __device__ __forceinline__ double drag_gidaspow(double epg, double mug, double r
   return 0.75 * cd * vrel * ropg * pow(epg, -2.65) / dpm;
 }
 
-// DRAG_GS_DES0 per particle: FC += F_GP*(u_g@p - v_p) + P_FORCE*PVOL.
-__global__ void k_drag(DevParams p, GasDev G, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
-                       const int8_t* __restrict__ state, const int* __restrict__ pijk,
-                       const double* __restrict__ ep_g, const double* __restrict__ u_g,
-                       const double* __restrict__ v_g, const double* __restrict__ w_g,
-                       const double* __restrict__ p_force, double* __restrict__ f_gp, double* __restrict__ fc) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= p.n) return;
-  const int8_t st = state[l];
-  if (st == DEM_STATE_NONEXISTENT || st >= DEM_STATE_NORMAL_GHOST) return;
-  const int i = pijk[4 * (size_t)l], j = pijk[4 * (size_t)l + 1], k = pijk[4 * (size_t)l + 2];
-  if (!gfluid(G, i, j, k)) return;
+// Gas velocity at a particle of fluid cell (i,j,k): staggered face
+// velocities averaged to the cell's 2x2x2 node stencil, interpolated with the
+// trilinear weights, which are returned too (drag_gs_des0.f:117-170 and
+// 313-361, DRAG_INTERPOLATION drag_gs_des0.f:507-566).
+__device__ __forceinline__ void gas_velocity(const GasDev& G, int i, int j, int k, const double4& X,
+                                             const double* __restrict__ u_g, const double* __restrict__ v_g,
+                                             const double* __restrict__ w_g, double velfp[3], double w[2][2][2]) {
   const double avg = G.no_k ? 0.5 : 0.25;
   const int iw = i - 1, js = j - 1, kb = G.no_k ? 1 : k - 1;
-  const double4 X = pos4[l], V = vel4[l];
-  double w[2][2][2];
   cell_weights(G, i, j, k, X.x, X.y, X.z, w);
-  double velfp[3] = {0.0, 0.0, 0.0};
+  velfp[0] = velfp[1] = velfp[2] = 0.0;
   for (int kk = 0; kk < (G.no_k ? 1 : 2); ++kk)
     for (int jj = 0; jj < 2; ++jj)
       for (int ii = 0; ii < 2; ++ii) {
@@ -182,22 +179,211 @@ __global__ void k_drag(DevParams p, GasDev G, const double4* __restrict__ pos4, 
         velfp[1] = velfp[1] + v1 * wt;
         if (!G.no_k) velfp[2] = velfp[2] + v2 * wt;
       }
-  const double vp[3] = {V.x, V.y, V.z};
-  const int ijk = gijk(G, i, j, k);
-  const double epg = ep_g[ijk];
-  const double vs[3] = {velfp[0] - vp[0], velfp[1] - vp[1], velfp[2] - vp[2]};
+}
+
+// DES_DRAG_GP (drag_gp_des.f:97-257, Model A, Gidaspow): the relaxed F_GP
+// of a particle of radius r with velocity V in gas of void fraction epg;
+// PVOL through *pvol.
+__device__ __forceinline__ double relaxed_fgp(const GasDev& G, double epg, double r, const double velfp[3],
+                                              const double4& V, double f_old, double* pvol) {
+  const double vs[3] = {velfp[0] - V.x, velfp[1] - V.y, velfp[2] - V.z};
   const double vrel = sqrt(dot3(vs, vs));
-  const double r = X.w;
   const double dpm = 2.0 * r;
   const double dga = drag_gidaspow(epg, G.mu_g, G.ro_g, G.ro_g * epg, vrel, dpm);
-  const double pvol = ((4.0 / 3.0) * G.pi) * (r * (r * r));
-  const double fgs = dga * pvol;
-  const double fg = (1.0 - G.ur_f_gs) * f_gp[l] + G.ur_f_gs * fgs;
+  *pvol = ((4.0 / 3.0) * G.pi) * (r * (r * r));
+  const double fgs = dga * *pvol;
+  return (1.0 - G.ur_f_gs) * f_old + G.ur_f_gs * fgs;
+}
+
+// DES_DRAG_GP per particle of a fluid cell.  ADD_FC (DRAG_GS_DES0):
+// FC += F_GP*(u_g@p - v_p) + P_FORCE*PVOL as well; without it only F_GP is
+// updated (the first half of DRAG_GS_GAS0, whose per-particle F_GP does not
+// depend on the deposition order).
+template <bool ADD_FC>
+__global__ void k_drag(DevParams p, GasDev G, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+                       const int8_t* __restrict__ state, const int* __restrict__ pijk,
+                       const double* __restrict__ ep_g, const double* __restrict__ u_g,
+                       const double* __restrict__ v_g, const double* __restrict__ w_g,
+                       const double* __restrict__ p_force, double* __restrict__ f_gp, double* __restrict__ fc) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= p.n) return;
+  const int8_t st = state[l];
+  if (st == DEM_STATE_NONEXISTENT || st >= DEM_STATE_NORMAL_GHOST) return;
+  const int i = pijk[4 * (size_t)l], j = pijk[4 * (size_t)l + 1], k = pijk[4 * (size_t)l + 2];
+  if (!gfluid(G, i, j, k)) return;
+  const double4 X = pos4[l], V = vel4[l];
+  double w[2][2][2], velfp[3];
+  gas_velocity(G, i, j, k, X, u_g, v_g, w_g, velfp, w);
+  const int ijk = gijk(G, i, j, k);
+  double pvol;
+  const double fg = relaxed_fgp(G, ep_g[ijk], X.w, velfp, V, f_gp[l], &pvol);
   f_gp[l] = fg;
+  if (!ADD_FC) return;
+  const double vp[3] = {V.x, V.y, V.z};
   const size_t n = (size_t)p.n;
   for (int c = 0; c < 3; ++c) fc[c * n + l] = fc[c * n + l] + fg * (velfp[c] - vp[c]);
   if (p_force)
     for (int c = 0; c < 3; ++c) fc[c * n + l] = fc[c * n + l] + p_force[3 * (size_t)ijk + c] * pvol;
+}
+
+// DRAG_GS_GAS0 deposition as a gather per node: the node's cells in
+// ascending IJK, their particles in PIC order, as the reference's scatter
+// adds them; DRAG_AM += F_GP*W/DES_VOL_NODE, DRAG_BM(:,c) += F_GP*V(c)*W/
+// DES_VOL_NODE (statistical weight 1).
+__global__ void k_drag_node(GasDev G, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+                            const int* __restrict__ pic_start, const int* __restrict__ pic_list,
+                            const double* __restrict__ f_gp, const double* __restrict__ vol_node,
+                            double* __restrict__ drag_am, double* __restrict__ drag_bm) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ni = G.imax + 1, nj = G.jmax + 1, nk = G.no_k ? 1 : G.kmax + 1;
+  if (t >= ni * nj * nk) return;
+  const int I = t % ni + 1, J = (t / ni) % nj + 1, K = t / (ni * nj) + 1;
+  const int node = gijk(G, I, J, K);
+  const double ovol = 1.0 / vol_node[node];
+  double am = 0.0, bm[3] = {0.0, 0.0, 0.0};
+  for (int k = K; k <= (G.no_k ? K : K + 1); ++k)
+    for (int j = J; j <= J + 1; ++j)
+      for (int i = I; i <= I + 1; ++i) {
+        if (!gfluid(G, i, j, k)) continue;
+        const int c = gijk(G, i, j, k);
+        const int ii = I - (i - 1), jj = J - (j - 1), kk = G.no_k ? 0 : K - (k - 1);
+        for (int q = pic_start[c]; q < pic_start[c + 1]; ++q) {
+          const int np = pic_list[q];
+          const double4 X = pos4[np], V = vel4[np];
+          double w[2][2][2];
+          cell_weights(G, i, j, k, X.x, X.y, X.z, w);
+          const double wt = w[kk][jj][ii], fg = f_gp[np];
+          am = am + fg * wt * ovol;
+          bm[0] = bm[0] + fg * V.x * wt * ovol;
+          bm[1] = bm[1] + fg * V.y * wt * ovol;
+          bm[2] = bm[2] + fg * V.z * wt * ovol;
+        }
+      }
+  drag_am[node] = am;
+  for (int c = 0; c < 3; ++c) drag_bm[(size_t)c * G.ncell + node] = bm[c];
+}
+
+// F_GDS per cell: the mean of the DRAG_AM of the cell's nodes, in the
+// reference's order (drag_gs_des0.f:451-494); zero outside the fluid.
+__global__ void k_fgds(GasDev G, const double* __restrict__ drag_am, double* __restrict__ f_gds) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= G.ncell) return;
+  const int i = c % G.gi2 + 1, j = (c / G.gi2) % G.gj2 + 1, k = c / (G.gi2 * G.gj2) + 1;
+  if (!gfluid(G, i, j, k)) { f_gds[c] = 0.0; return; }
+  const double avf = G.no_k ? 0.25 : 0.125;
+  double f = avf * (drag_am[c] + drag_am[gijk(G, i, j - 1, k)] + drag_am[gijk(G, i - 1, j - 1, k)] +
+                    drag_am[gijk(G, i - 1, j, k)]);
+  if (!G.no_k)
+    f = f + avf * (drag_am[gijk(G, i, j, k - 1)] + drag_am[gijk(G, i, j - 1, k - 1)] +
+                   drag_am[gijk(G, i - 1, j - 1, k - 1)] + drag_am[gijk(G, i - 1, j, k - 1)]);
+  f_gds[c] = f;
+}
+
+// ---- DES_INTERP_SCHEME = NONE: the ...1 routines without a filter ------
+
+// CALC_CELL_CENTER_GAS_VEL (drag_gs_des1.f:313-370) on a uniform grid
+// (FX = FX_BAR = 1/2, set_geometry.f:344-345); (i,j,k) is a fluid cell.
+__device__ __forceinline__ void cell_center_vel(const GasDev& G, int i, int j, int k,
+                                                const double* __restrict__ u_g, const double* __restrict__ v_g,
+                                                const double* __restrict__ w_g, double v[3]) {
+  const int ijk = gijk(G, i, j, k);
+  v[0] = 0.5 * u_g[gijk(G, i - 1, j, k)] + 0.5 * u_g[ijk];       // AVG_X_E
+  v[1] = 0.5 * (v_g[gijk(G, i, j - 1, k)] + v_g[ijk]);           // AVG_Y_N
+  v[2] = G.no_k ? 0.0 : 0.5 * (w_g[gijk(G, i, j, k - 1)] + w_g[ijk]);   // AVG_Z_T
+}
+
+__device__ __forceinline__ double sphere_vol(const GasDev& G, double r) {
+  return ((4.0 / 3.0) * G.pi) * (r * (r * r));
+}
+
+// DRAG_GS_DES1 without a filter (drag_gs_des1.f:34-160, Model A, not
+// explicitly coupled), per NORMAL particle: cell-centre gas velocity, F_GP
+// by DES_DRAG_GP, FC += F_GP*(u_g - v_p) + P_FORCE*PVOL; F_GP = 0 outside the
+// fluid.  Without ADD_FC (the F_GP half of DRAG_GS_GAS1) only F_GP of
+// particles in fluid cells changes.
+template <bool ADD_FC>
+__global__ void k_drag1(DevParams p, GasDev G, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+                        const int8_t* __restrict__ state, const int* __restrict__ pijk,
+                        const double* __restrict__ ep_g, const double* __restrict__ u_g,
+                        const double* __restrict__ v_g, const double* __restrict__ w_g,
+                        const double* __restrict__ p_force, double* __restrict__ f_gp, double* __restrict__ fc) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= p.n || state[l] != DEM_STATE_NORMAL) return;
+  const int i = pijk[4 * (size_t)l], j = pijk[4 * (size_t)l + 1], k = pijk[4 * (size_t)l + 2];
+  if (!gfluid(G, i, j, k)) {
+    if (ADD_FC) f_gp[l] = 0.0;
+    return;
+  }
+  const double4 X = pos4[l], V = vel4[l];
+  double velfp[3];
+  cell_center_vel(G, i, j, k, u_g, v_g, w_g, velfp);
+  const int ijk = gijk(G, i, j, k);
+  double pvol;
+  const double fg = relaxed_fgp(G, ep_g[ijk], X.w, velfp, V, f_gp[l], &pvol);
+  f_gp[l] = fg;
+  if (!ADD_FC) return;
+  const double vp[3] = {V.x, V.y, V.z};
+  const size_t n = (size_t)p.n;
+  for (int c = 0; c < 3; ++c) fc[c * n + l] = fc[c * n + l] + fg * (velfp[c] - vp[c]);
+  if (p_force)
+    for (int c = 0; c < 3; ++c) fc[c * n + l] = fc[c * n + l] + p_force[3 * (size_t)ijk + c] * pvol;
+}
+
+// DRAG_GS_GAS1 deposition without a filter, per cell: its NORMAL particles in
+// ascending index (the reference's particle loop restricted to the cell),
+// DRAG_BM(IJK,:) += F_GP*V/VOL, F_GDS(IJK) += F_GP/VOL; zero outside the fluid.
+__global__ void k_gas1_cell(GasDev G, const double4* __restrict__ vel4, const int8_t* __restrict__ state,
+                            const int* __restrict__ pic_start, const int* __restrict__ pic_list,
+                            const double* __restrict__ f_gp, double* __restrict__ f_gds,
+                            double* __restrict__ drag_bm) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= G.ncell) return;
+  const int i = c % G.gi2 + 1, j = (c / G.gi2) % G.gj2 + 1, k = c / (G.gi2 * G.gj2) + 1;
+  double f = 0.0, bm[3] = {0.0, 0.0, 0.0};
+  if (gfluid(G, i, j, k)) {
+    const double weight = 1.0 / G.vol;
+    for (int q = pic_start[c]; q < pic_start[c + 1]; ++q) {
+      const int np = pic_list[q];
+      if (state[np] != DEM_STATE_NORMAL) continue;
+      const double lforce = f_gp[np];
+      const double4 V = vel4[np];
+      bm[0] = bm[0] + (lforce * V.x) * weight;
+      bm[1] = bm[1] + (lforce * V.y) * weight;
+      bm[2] = bm[2] + (lforce * V.z) * weight;
+      f = f + lforce * weight;
+    }
+  }
+  f_gds[c] = f;
+  for (int a = 0; a < 3; ++a) drag_bm[(size_t)a * G.ncell + c] = bm[a];
+}
+
+// COMP_MEAN_FIELDS1 with FILTER_SIZE = 0 (comp_mean_fields1.f:46-104) and
+// CALC_EPG_DES, per cell: SOLVOLINC = sum of PVOL of its NORMAL particles in
+// ascending index, ROP_S = RO_S*SOLVOLINC/VOL and EP_G on fluid cells.
+__global__ void k_mean_fields1(GasDev G, const double4* __restrict__ pos4, const uint8_t* __restrict__ phase,
+                               const int8_t* __restrict__ state, const int* __restrict__ pic_start,
+                               const int* __restrict__ pic_list, double* __restrict__ rop_s,
+                               double* __restrict__ ep_g) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= G.ncell) return;
+  const int i = c % G.gi2 + 1, j = (c / G.gi2) % G.gj2 + 1, k = c / (G.gi2 * G.gj2) + 1;
+  const bool fl = gfluid(G, i, j, k);
+  double sv[MAXP];
+  for (int m = 0; m < G.M; ++m) sv[m] = 0.0;
+  if (fl)
+    for (int q = pic_start[c]; q < pic_start[c + 1]; ++q) {
+      const int np = pic_list[q];
+      if (state[np] != DEM_STATE_NORMAL) continue;
+      const int m = phase[np];
+      sv[m] = sv[m] + sphere_vol(G, pos4[np].w);
+    }
+  double sum_eps = 0.0;
+  for (int m = 0; m < G.M; ++m) {
+    const double r = fl ? G.ro_s[m] * sv[m] / G.vol : 0.0;
+    rop_s[(size_t)m * G.ncell + c] = r;
+    sum_eps = sum_eps + r / G.ro_s[m];
+  }
+  if (fl) ep_g[c] = 1.0 - fmin(1.0, sum_eps);
 }
 
 // COMP_MEAN_FIELDS0 node deposition as a gather over the node's cells.
@@ -296,6 +482,13 @@ static int run_mean_fields(dem_handle* h) {
   Gas* s = h->gas;
   const GasDev G = gas_view(h);
   const int T = 256;
+  if (s->g.interp_scheme == DEM_INTERP_NONE) {   // COMP_MEAN_FIELDS1
+    k_mean_fields1<<<(G.ncell + T - 1) / T, T, 0, h->stream>>>(G, h->pos4[h->cur], h->phase, h->state,
+                                                               s->pic_start, s->pic_list, s->rop_s, s->ep_g);
+    DEM_LAUNCH(h);
+    s->have_mean = true;
+    return check_cuda(h, cudaGetLastError(), "mean fields");
+  }
   const int nnodes = (G.imax + 1) * (G.jmax + 1) * (G.no_k ? 1 : G.kmax + 1);
   const int c = h->cur;
   k_node_deposit<<<(nnodes + T - 1) / T, T, 0, h->stream>>>(G, h->pos4[c], h->vel4[c], h->phase, s->pic_start,
@@ -312,17 +505,69 @@ static int run_drag(dem_handle* h) {
   const GasDev G = gas_view(h);
   const int T = 256, B = (h->n + T - 1) / T;
   const int c = h->cur;
-  k_drag<<<B, T, 0, h->stream>>>(h->dp, G, h->pos4[c], h->vel4[c], h->state, s->pijk, s->ep_g, s->u_g, s->v_g,
-                                 s->w_g, s->p_force, s->f_gp, h->fc);
+  k_drag<true><<<B, T, 0, h->stream>>>(h->dp, G, h->pos4[c], h->vel4[c], h->state, s->pijk, s->ep_g, s->u_g,
+                                       s->v_g, s->w_g, s->p_force, s->f_gp, h->fc);
   DEM_LAUNCH(h);
   return check_cuda(h, cudaGetLastError(), "drag");
+}
+
+static int run_drag1(dem_handle* h) {
+  ProfScope ps(h, DEM_PROF_COUPLING);
+  Gas* s = h->gas;
+  const GasDev G = gas_view(h);
+  const int T = 256, B = (h->n + T - 1) / T;
+  const int c = h->cur;
+  k_drag1<true><<<B, T, 0, h->stream>>>(h->dp, G, h->pos4[c], h->vel4[c], h->state, s->pijk, s->ep_g, s->u_g,
+                                        s->v_g, s->w_g, s->p_force, s->f_gp, h->fc);
+  DEM_LAUNCH(h);
+  return check_cuda(h, cudaGetLastError(), "drag");
+}
+
+// CALC_DRAG_DES: the particle side of the drag by DES_INTERP_SCHEME.
+static int run_calc_drag(dem_handle* h) {
+  return h->gas->g.interp_scheme == DEM_INTERP_NONE ? run_drag1(h) : run_drag(h);
+}
+
+// DRAG_GS_GAS1: F_GP per particle, then the per-cell gather.
+static int run_drag_gas1(dem_handle* h) {
+  ProfScope ps(h, DEM_PROF_COUPLING);
+  Gas* s = h->gas;
+  const GasDev G = gas_view(h);
+  const int T = 256, B = (h->n + T - 1) / T;
+  const int c = h->cur;
+  k_drag1<false><<<B, T, 0, h->stream>>>(h->dp, G, h->pos4[c], h->vel4[c], h->state, s->pijk, s->ep_g, s->u_g,
+                                         s->v_g, s->w_g, nullptr, s->f_gp, nullptr);
+  k_gas1_cell<<<(G.ncell + T - 1) / T, T, 0, h->stream>>>(G, h->vel4[c], h->state, s->pic_start, s->pic_list,
+                                                          s->f_gp, s->f_gds, s->drag_bm);
+  h->launches += 2;
+  return check_cuda(h, cudaGetLastError(), "drag gas");
+}
+
+// DRAG_GS_GAS0: F_GP per particle, the node gather, F_GDS per cell.
+static int run_drag_gas(dem_handle* h) {
+  ProfScope ps(h, DEM_PROF_COUPLING);
+  Gas* s = h->gas;
+  const GasDev G = gas_view(h);
+  const int T = 256, B = (h->n + T - 1) / T;
+  const int c = h->cur;
+  k_drag<false><<<B, T, 0, h->stream>>>(h->dp, G, h->pos4[c], h->vel4[c], h->state, s->pijk, s->ep_g, s->u_g,
+                                        s->v_g, s->w_g, nullptr, s->f_gp, nullptr);
+  cudaMemsetAsync(s->drag_am, 0, sizeof(double) * s->ncell, h->stream);
+  cudaMemsetAsync(s->drag_bm, 0, sizeof(double) * 3 * s->ncell, h->stream);
+  const int nnodes = (G.imax + 1) * (G.jmax + 1) * (G.no_k ? 1 : G.kmax + 1);
+  k_drag_node<<<(nnodes + T - 1) / T, T, 0, h->stream>>>(G, h->pos4[c], h->vel4[c], s->pic_start, s->pic_list,
+                                                         s->f_gp, s->vol_node, s->drag_am, s->drag_bm);
+  k_fgds<<<(G.ncell + T - 1) / T, T, 0, h->stream>>>(G, s->drag_am, s->f_gds);
+  h->launches += 3;
+  return check_cuda(h, cudaGetLastError(), "drag gas");
 }
 
 void free_gas(dem_handle* h) {
   Gas* s = h->gas;
   if (!s) return;
   void* ptrs[] = {s->xe, s->yn, s->zt, s->ep_g, s->u_g, s->v_g, s->w_g, s->p_force, s->vol_surr, s->rop_s,
-                  s->rops_node, s->pijk, s->f_gp, s->pic_cnt, s->pic_start, s->pic_list};
+                  s->rops_node, s->vol_node, s->drag_am, s->drag_bm, s->f_gds, s->pijk, s->f_gp,
+                  s->pic_cnt, s->pic_start, s->pic_list};
   for (void* q : ptrs) if (q) cudaFree(q);
   delete s;
   h->gas = nullptr;
@@ -345,6 +590,8 @@ int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid* g, const double* ep_
     return set_err(h, DEM_ERR_ARG, "bad fluid grid");
   for (int m = 0; m < h->dp.nph; ++m)
     if (!(g->ro_s[m] > 0.0)) return set_err(h, DEM_ERR_ARG, "ro_s must be positive");
+  if (g->interp_scheme != DEM_INTERP_GARG && g->interp_scheme != DEM_INTERP_NONE)
+    return set_err(h, DEM_ERR_ARG, "unknown interp_scheme");
   free_gas(h);
   Gas* s = new Gas();
   h->gas = s;
@@ -383,6 +630,19 @@ int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid* g, const double* ep_
               if (fluid(ii, jj, kk)) v = v + s->vol;
         vs[cidx(i, j, k)] = v;
       }
+  // DES_VOL_NODE (cfassign.f:104-228): a quarter (2D) or an eighth (3D) of
+  // each fluid cell sharing the node, summed in the reference's order
+  std::vector<double> vn(nc, 0.0);
+  const double avn = h->dp.no_k ? 0.25 : 0.125;
+  auto fv = [&](int i, int j, int k) { return fluid(i, j, k) ? s->vol : 0.0; };
+  for (int k = 1; k <= nk1; ++k)
+    for (int j = 1; j <= g->jmax + 1; ++j)
+      for (int i = 1; i <= g->imax + 1; ++i) {
+        double v = avn * (fv(i, j, k) + fv(i + 1, j, k) + fv(i, j + 1, k) + fv(i + 1, j + 1, k));
+        if (!h->dp.no_k)
+          v = v + avn * (fv(i, j, k + 1) + fv(i + 1, j + 1, k + 1) + fv(i, j + 1, k + 1) + fv(i + 1, j, k + 1));
+        vn[cidx(i, j, k)] = v;
+      }
   bool ok = true;
   auto A = [&](void** p, size_t b) { if (ok && cudaMalloc(p, b ? b : 8) != cudaSuccess) ok = false; };
   A((void**)&s->xe, sizeof(double) * fx.size());
@@ -396,6 +656,10 @@ int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid* g, const double* ep_
   A((void**)&s->vol_surr, sizeof(double) * nc);
   A((void**)&s->rop_s, sizeof(double) * nc * s->M);
   A((void**)&s->rops_node, sizeof(double) * nc * s->M);
+  A((void**)&s->vol_node, sizeof(double) * nc);
+  A((void**)&s->drag_am, sizeof(double) * nc);
+  A((void**)&s->drag_bm, sizeof(double) * 3 * nc);
+  A((void**)&s->f_gds, sizeof(double) * nc);
   A((void**)&s->pijk, sizeof(int) * 4 * (size_t)h->n);
   A((void**)&s->f_gp, sizeof(double) * (size_t)h->n);
   A((void**)&s->pic_cnt, sizeof(int) * (nc + 1));
@@ -411,6 +675,10 @@ int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid* g, const double* ep_
   cudaMemcpyAsync(s->w_g, w_g, sizeof(double) * nc, cudaMemcpyHostToDevice, h->stream);
   if (p_force) cudaMemcpyAsync(s->p_force, p_force, sizeof(double) * 3 * nc, cudaMemcpyHostToDevice, h->stream);
   cudaMemcpyAsync(s->vol_surr, vs.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(s->vol_node, vn.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, h->stream);
+  cudaMemsetAsync(s->drag_am, 0, sizeof(double) * nc, h->stream);
+  cudaMemsetAsync(s->drag_bm, 0, sizeof(double) * 3 * nc, h->stream);
+  cudaMemsetAsync(s->f_gds, 0, sizeof(double) * nc, h->stream);
   cudaMemsetAsync(s->rop_s, 0, sizeof(double) * nc * s->M, h->stream);
   cudaMemsetAsync(s->f_gp, 0, sizeof(double) * (size_t)h->n, h->stream);
   if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "set gas fields")) { free_gas(h); return rc; }
@@ -441,6 +709,38 @@ int dem_drag_gs_des0(dem_handle* h) {
   return check_cuda(h, cudaStreamSynchronize(h->stream), "drag");
 }
 
+int dem_drag_gs_gas0(dem_handle* h, double* f_gds, double* drag_am, double* drag_bm, double* f_gp) {
+  API_GUARD(h);
+  if (!h->gas) return set_err(h, DEM_ERR_STATE, "no gas fields");
+  if (int rc = run_drag_gas(h)) return rc;
+  Gas* s = h->gas;
+  const size_t nc = (size_t)s->ncell;
+  if (f_gds) cudaMemcpyAsync(f_gds, s->f_gds, sizeof(double) * nc, cudaMemcpyDeviceToHost, h->stream);
+  if (drag_am) cudaMemcpyAsync(drag_am, s->drag_am, sizeof(double) * nc, cudaMemcpyDeviceToHost, h->stream);
+  if (drag_bm) cudaMemcpyAsync(drag_bm, s->drag_bm, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, h->stream);
+  if (f_gp) cudaMemcpyAsync(f_gp, s->f_gp, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "drag gas");
+}
+
+int dem_drag_gs_des1(dem_handle* h) {
+  API_GUARD(h);
+  if (!h->gas) return set_err(h, DEM_ERR_STATE, "no gas fields");
+  if (int rc = run_drag1(h)) return rc;
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "drag");
+}
+
+int dem_drag_gs_gas1(dem_handle* h, double* f_gds, double* drag_bm, double* f_gp) {
+  API_GUARD(h);
+  if (!h->gas) return set_err(h, DEM_ERR_STATE, "no gas fields");
+  if (int rc = run_drag_gas1(h)) return rc;
+  Gas* s = h->gas;
+  const size_t nc = (size_t)s->ncell;
+  if (f_gds) cudaMemcpyAsync(f_gds, s->f_gds, sizeof(double) * nc, cudaMemcpyDeviceToHost, h->stream);
+  if (drag_bm) cudaMemcpyAsync(drag_bm, s->drag_bm, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, h->stream);
+  if (f_gp) cudaMemcpyAsync(f_gp, s->f_gp, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "drag gas");
+}
+
 int dem_step_coupled(dem_handle* h, int32_t nn_first, int32_t nsteps) {
   API_GUARD(h);
   if (!h->gas) return set_err(h, DEM_ERR_STATE, "no gas fields");
@@ -452,7 +752,7 @@ int dem_step_coupled(dem_handle* h, int32_t nn_first, int32_t nsteps) {
     const int nn = nn_first + k;
     cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
     if (int rc = run_force(h, false)) return rc;              // CALC_FORCE_DEM
-    if (int rc = run_drag(h)) return rc;                      // CALC_DRAG_DES
+    if (int rc = run_calc_drag(h)) return rc;                 // CALC_DRAG_DES
     if (int rc = run_cfnewvalues(h)) return rc;               // CFUPDATEOLD + CFNEWVALUES
     const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0);
     if (do_nsearch || anyper) {

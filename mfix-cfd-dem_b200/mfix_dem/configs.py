@@ -239,13 +239,14 @@ def _smooth_noise(rng, shape, sigma_cells, std):
 
 def coupled(n=500_000, cells=(64, 256, 64), dx=1e-3, d=0.5e-3, rho=2600.0, kn=500.0, en=0.9, mew=0.1,
             u_sup=1.0, u_std=0.1, corr_cells=4, ro_g=1.2, mu_g=1.8e-5, spacing=1.1, seed=SEED_BASE + 2,
-            nsn=25):
+            nsn=25, interp="GARG_2012"):
     """CFD-DEM coupling: n spheres of diameter d on a jittered cubic lattice
     (spacing `spacing`*d) filling the bottom of a cells[0] x cells[1] x cells[2]
     fluid grid of cell size dx, LSD contact, default walls; frozen gas with
     superficial velocity u_sup in y plus seeded Gaussian perturbations (std
     u_std, correlation corr_cells cells) on every component; the interstitial
     velocity is the superficial one divided by the initial void fraction.
+    `interp` is DES_INTERP_SCHEME: "GARG_2012" or "NONE".
     Returns (case, prm, arr, walls, info, grid, fields)."""
     rng = np.random.default_rng(seed)
     box = (cells[0] * dx, cells[1] * dx, cells[2] * dx)
@@ -287,6 +288,7 @@ def coupled(n=500_000, cells=(64, 256, 64), dx=1e-3, d=0.5e-3, rho=2600.0, kn=50
     grid = abi.DemFluidGrid()
     grid.imax, grid.jmax, grid.kmax = cells
     grid.drag_model = 0
+    grid.interp_scheme = {"GARG_2012": abi.DEM_INTERP_GARG, "NONE": abi.DEM_INTERP_NONE}[interp]
     grid.dx = grid.dy = grid.dz = dx
     grid.ro_g, grid.mu_g = ro_g, mu_g
     grid.ep_star = 0.42
