@@ -252,6 +252,11 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     torch.cuda.synchronize()
     ms_eager = ep0.elapsed_time(ep1)
     prof = g.profile()
+    # the parts of the force step, timed on a short extra pass (their
+    # events split the step, so they are not used for the roofline)
+    g.set_profiling(2)
+    g.step(10, warm + 2 * args.steps + 1)
+    parts = {k: v[0] / v[1] for k, v in g.profile().items() if k in ("walls", "pairs", "gather") and v[1]}
     g.set_profiling(False)
     ferr1 = g.force_error() if prec == "split" else None
     if ws > 1:
@@ -280,7 +285,8 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
                 "avg_launch_ms": f_ms / f_n if f_n else None,
                 "share_of_step": f_ms / ms_eager if ms_eager else None,
                 "ms_per_step_eager": ms_eager / args.steps,
-                "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]}}
+                "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]},
+                "force_parts_ms_per_launch": parts}
     out = {"value": value, "ms": ms, "n": n, "n_normal": n_normal, "pairs": int(p1), "launches": int(launches),
            "warmup": warm, "tuning": tuning,
            "roofline": roofline, "clocks": clk, "contacts": int(st["n_contacts"]), "prm": prm, "info": info,
@@ -372,6 +378,9 @@ def _batched_run(args, prec, stream, systems, info):
     bt.step(steps)
     torch.cuda.synchronize()
     prof = bt.profile()
+    bt.set_profiling(2)
+    bt.step(10)
+    parts = {k: v[0] / v[1] for k, v in bt.profile().items() if k in ("walls", "pairs", "gather") and v[1]}
     bt.set_profiling(False)
     n_normal = int(st["n_normal"])
     f_ms, f_n = prof["force"]
@@ -387,7 +396,8 @@ def _batched_run(args, prec, stream, systems, info):
                          "kernel": "force step over all systems (walls + pairs + gather with fused integration)",
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_launch,
                          "avg_launch_ms": f_ms / f_n if f_n else None,
-                         "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]}},
+                         "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]},
+                         "force_parts_ms_per_launch": parts},
             "final_pos": final}
 
 

@@ -206,6 +206,62 @@ int dem_upload_pairs(dem_handle* h, const int32_t* neighbor_index,
 int dem_download_wall_history(dem_handle* h, int32_t* facet_id, double* pft,
                               int32_t max_pip);
 
+/* Restores the wall tangential history from the same arrays (a restart or a
+ * hand-over from the CPU solver).  Facet ids must be -1 or 1..n_facets of
+ * the facets installed by dem_set_walls.  Call after dem_upload_state, which
+ * keeps the previous history. */
+int dem_upload_wall_history(dem_handle* h, const int32_t* facet_id, const double* pft,
+                            int32_t max_pip);
+
+/* ---- restart files (model/des/write_res0_des.f, read_res0_des.f) -------- */
+
+/* Scalars of a DEM restart file (RES, serial layout: 512-byte big-endian
+ * records as WRITE_RES0_DES writes them). */
+typedef struct dem_res_info {
+    double  version;            /* read: the file's VERSION (written: 1.2 as a REAL(4) literal) */
+    double  dtsolid;            /* DTSOLID stored in the file */
+    int32_t vtp_findex;         /* VTP_FINDEX */
+    int32_t tecplot_findex;     /* TECPLOT_FINDEX */
+    int32_t n_particles;        /* read: existing non-ghost particles in the file */
+    int32_t n_pairs;            /* read: pair entries in the file */
+    double  ro_sol[DEM_MAX_PHASES];  /* write: RO_SOL of each phase's particles */
+    double  reserved[4];
+} dem_res_info;
+
+/* WRITE_RES0_DES (write_res0_des.f:44-208) for a DEM run without MPPIC,
+ * thermal, species, user variables, SuperDEM, glued spheres or mass
+ * inflow: particle arrays of the existing non-ghost particles in slot order
+ * (global id = 1-based slot), then the pair list.  The second pair array
+ * holds each entry's owner (the reference writes a value its reader does not
+ * use), so that dem_read_res0_des can restore the pair list exactly. */
+int dem_write_res0_des(dem_handle* h, const char* path, const dem_res_info* info);
+
+/* READ_RES0_DES (read_res0_des.f): particles into slots 1..n_particles
+ * (the rest NONEXISTENT), PMASS/OMOI from DES_RADIUS and RO_SOL as
+ * MAKE_ARRAYS_DES computes them (make_arrays_des.f:287-291), uploaded as
+ * dem_upload_state does.  restore_pairs = 1 also uploads the pair list and
+ * its tangential history (files from dem_write_res0_des); with 0 the pair
+ * section is skipped and the caller builds the list (dem_init_neighbors), as
+ * for files written by the reference.  Wall-contact and Adams-Bashforth
+ * histories are not part of the format: restore them with
+ * dem_upload_wall_history / dem_set_ab2_history when they were saved. */
+int dem_read_res0_des(dem_handle* h, const char* path, int32_t restore_pairs, dem_res_info* info);
+
+/* The record codec behind the two calls, on host arrays (no device needed).
+ * dem_res_write takes the DES arrays in Fortran layout with 1-based
+ * NEIGHBOR_INDEX/NEIGHBORS as dem_download_pairs returns them.
+ * dem_res_read with pos == NULL reads the header only (counts into *info);
+ * otherwise it fills max_pip slots and, when pair_owner is not NULL, the
+ * pair entries as 1-based local owner/neighbour indices and PFT (3,P). */
+int dem_res_write(const char* path, const dem_res_info* info, int32_t max_pip, int32_t no_k,
+                  const double* pos, const double* vel, const double* omega, const double* radius,
+                  const int8_t* state, const int32_t* phase, const int32_t* neighbor_index,
+                  const int32_t* neighbors, const double* pft, int64_t n_pairs);
+int dem_res_read(const char* path, dem_res_info* info, int32_t max_pip, int32_t no_k,
+                 double* pos, double* vel, double* omega, double* radius, double* ro_sol,
+                 int8_t* state, int32_t* phase, int32_t* pair_owner, int32_t* pair_neighbor,
+                 double* pft, int64_t pair_cap);
+
 /* ---- per-stage entry points (one per reference call site) ----------------- */
 
 /* DESGRID_PIC(.TRUE.) (desgrid_mod.f:877-995): cell of every particle and the
@@ -222,7 +278,9 @@ int dem_neighbour(dem_handle* h);
 
 /* CALC_FORCE_DEM (calc_force_dem.f:18-544) including the wall contacts
  * CALC_DEM_FORCE_WITH_WALL_STL (calc_collision_wall_mod.f:54-794).
- * Leaves FC and TOW on the device. */
+ * Stores FC and TOW on the device: the reference adds to FC/TOW, which
+ * CFNEWVALUES leaves at zero, so within DES_TIME_STEP the two agree; a
+ * second call without dem_cfnewvalues in between does not add up. */
 int dem_calc_force(dem_handle* h);
 
 /* CFUPDATEOLD + CFNEWVALUES (cfupdateold.f:15-46, cfnewvalues.f:641-864):
@@ -280,7 +338,12 @@ int dem_launch_count(const dem_handle* h, int64_t* count);
 #define DEM_PROF_INTEGRATE 3   /* stand-alone CFNEWVALUES */
 #define DEM_PROF_COUPLING  4   /* drag and mean fields */
 #define DEM_PROF_OTHER     5
-#define DEM_PROF_N         6
+#define DEM_PROF_WALLS     6   /* parts of DEM_PROF_FORCE: wall contacts, */
+#define DEM_PROF_PAIRS     7   /* pair contacts, */
+#define DEM_PROF_GATHER    8   /* per-particle sums (+ fused integration) */
+#define DEM_PROF_N         9
+/* on = 1: CUDA events around every kernel class; on = 2: also around the
+ * parts of the force step (each part's events add launch gaps to it). */
 int dem_set_profiling(dem_handle* h, int32_t on);
 /* Milliseconds and launch counts per class since profiling was switched on
  * (synchronizes the handle's stream). */
@@ -297,12 +360,21 @@ int dem_force_error(dem_handle* h, double* rel_err);
 
 /* ---- CFD-DEM coupling (model/des/drag_gs_des0.f, comp_mean_fields0.f) ---- */
 
+/* DES_INTERP_SCHEME (particle_filter.f): GARG_2012 selects COMP_MEAN_FIELDS0
+ * and DRAG_GS_DES0/GAS0; NONE (the keyword's default) selects
+ * COMP_MEAN_FIELDS1 and DRAG_GS_DES1/GAS1 without a filter (each particle
+ * sees and feeds only its own fluid cell). */
+#define DEM_INTERP_GARG 0
+#define DEM_INTERP_NONE 1
+
 /* Fluid grid description for the coupled step.  Uniform Cartesian grid of
  * imax x jmax x kmax interior cells starting at domain_lo with widths dx,dy,dz;
  * MFiX's IJK includes one ghost layer on every side. */
 typedef struct dem_fluid_grid {
     int32_t imax, jmax, kmax;
     int32_t drag_model;          /* 0 = GIDASPOW (drag_gs.f:536-598) */
+    int32_t interp_scheme;       /* DES_INTERP_SCHEME: DEM_INTERP_GARG or DEM_INTERP_NONE */
+    int32_t reserved_i;
     double dx, dy, dz;
     double ro_g, mu_g;           /* gas density and viscosity (uniform) */
     double ep_star;              /* packed-bed void fraction EP_STAR (for ep_s max) */
@@ -322,12 +394,42 @@ int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid* g,
 /* Reads the mean fields of the last deposition: EP_G and ROP_S per fluid cell. */
 int dem_get_mean_fields(dem_handle* h, double* ep_g, double* rop_s);
 
-/* PARTICLES_IN_CELL + COMP_MEAN_FIELDS0 + CALC_EPG_DES. */
+/* PARTICLES_IN_CELL + COMP_MEAN_FIELDS (comp_mean_fields.f:30-40:
+ * COMP_MEAN_FIELDS0 under DEM_INTERP_GARG, COMP_MEAN_FIELDS1 without a filter
+ * under DEM_INTERP_NONE) + CALC_EPG_DES. */
 int dem_comp_mean_fields(dem_handle* h);
 
 /* DRAG_GS_DES0 with GARG_2012 interpolation: adds the drag to FC.  Call after
  * dem_calc_force and before dem_cfnewvalues. */
 int dem_drag_gs_des0(dem_handle* h);
+
+/* DRAG_GS_GAS0 (model/des/drag_gs_des0.f:235-497), the gas-phase side of the
+ * GARG_2012 drag that CALC_DES_2FLUID (calc_des_2fluid.f:70-73) calls from
+ * the fluid solver: F_GP of every particle of a fluid cell again (with the
+ * UR_F_GS under-relaxation of DES_DRAG_GP), its deposition to the nodes of
+ * the particle's fluid cell, DRAG_AM = sum F_GP*W/DES_VOL_NODE and
+ * DRAG_BM(:,c) = sum F_GP*V(c)*W/DES_VOL_NODE, and F_GDS per fluid cell as
+ * the mean of its nodes' DRAG_AM (zero elsewhere).  Particles are binned by
+ * the last PARTICLES_IN_CELL (dem_set_gas_fields, dem_comp_mean_fields,
+ * dem_step_coupled).  Outputs, each optional (NULL = not copied): f_gds and
+ * drag_am (ncells), drag_bm (ncells, 3) column-major as DRAG_BM, f_gp
+ * (max_pip).  Serial, non-periodic fluid grid (DES_ADDNODEVALUES adds
+ * nothing there). */
+int dem_drag_gs_gas0(dem_handle* h, double* f_gds, double* drag_am, double* drag_bm, double* f_gp);
+
+/* DRAG_GS_DES1 (model/des/drag_gs_des1.f:34-160) without a filter (the
+ * DEM_INTERP_NONE case): per NORMAL particle the gas velocity at the centre
+ * of its fluid cell (CALC_CELL_CENTER_GAS_VEL, drag_gs_des1.f:313-370), F_GP
+ * by DES_DRAG_GP, FC += F_GP*(u_g - v_p) + P_FORCE*PVOL; F_GP = 0 for a
+ * particle outside the fluid cells.  Call after dem_calc_force. */
+int dem_drag_gs_des1(dem_handle* h);
+
+/* DRAG_GS_GAS1 (model/des/drag_gs_des1.f:179-301) without a filter: F_GP of
+ * every NORMAL particle of a fluid cell again, DRAG_BM(IJK,:) = sum
+ * F_GP*V/VOL and F_GDS(IJK) = sum F_GP/VOL over the cell's particles (zero
+ * elsewhere).  Outputs as dem_drag_gs_gas0 (each may be NULL); there is no
+ * DRAG_AM in this scheme. */
+int dem_drag_gs_gas1(dem_handle* h, double* f_gds, double* drag_bm, double* f_gp);
 
 /* One coupled DES_TIME_STEP sequence: force, drag, integrate, rebuild if due,
  * particles-in-cell and mean fields. */

@@ -35,6 +35,7 @@ SOURCES = {
     "coupling.cu": ["-fmad=false"],
     "batch.cu": ["-fmad=false"],
     "tune.cu": [],
+    "res_des.cu": [],
 }
 HEADERS = ["dem_internal.cuh"]
 

@@ -141,7 +141,7 @@ static cudaEvent_t pool_event(dem_handle* h) {
 }
 
 ProfScope::ProfScope(dem_handle* hh, int cls) : h(hh) {
-  if (!h->prof) return;
+  if (!h->prof || (cls >= DEM_PROF_WALLS && h->prof < 2)) return;
   dem_handle::ProfEv ev{cls, pool_event(h), pool_event(h)};
   cudaEventRecord(ev.a, h->stream);
   h->prof_pending.push_back(ev);
@@ -418,6 +418,8 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
   A((void**)&h->touched, n);
   A((void**)&h->wall_hit, n);
   A((void**)&h->wall_cand, n);
+  A((void**)&h->wall_list, sizeof(int) * (size_t)n);
+  A((void**)&h->d_nwall, sizeof(int));
   A((void**)&h->skin, sizeof(double));
   A((void**)&h->vslot, sizeof(unsigned) * 32);
   A((void**)&h->derr, sizeof(DevErr));
@@ -486,7 +488,7 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->skin, h->vslot, h->pgap,
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->skin, h->vslot, h->pgap,
                   h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -642,6 +644,23 @@ int dem_download_wall_history(dem_handle* h, int32_t* fid, double* pf, int32_t m
   if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "download wall history")) return rc;
   if (fid) for (size_t s = 0; s < cnt; ++s) fid[s] = fid[s] < 0 ? -1 : fid[s] + 1;
   return 0;
+}
+
+int dem_upload_wall_history(dem_handle* h, const int32_t* fid, const double* pf, int32_t max_pip) {
+  SINGLE_GUARD(h);
+  if (max_pip != h->n || !fid || !pf) return set_err(h, DEM_ERR_ARG, "bad wall history arrays");
+  const size_t cnt = (size_t)h->n * h->dp.cmax;
+  std::vector<int> ids(cnt);
+  for (size_t s = 0; s < cnt; ++s) {
+    if (fid[s] != -1 && (fid[s] < 1 || fid[s] > h->nf)) return set_err(h, DEM_ERR_ARG, "facet id out of range");
+    ids[s] = fid[s] < 0 ? -1 : fid[s] - 1;
+  }
+  cudaMemcpyAsync(h->wall_fid, ids.data(), sizeof(int) * cnt, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->wall_pft, pf, sizeof(double) * 3 * cnt, cudaMemcpyHostToDevice, h->stream);
+  // every particle may hold history now; the wall kernel clears the mark
+  // where no slot is in use
+  cudaMemsetAsync(h->wall_live, 1, h->n, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "upload wall history");
 }
 
 int dem_download_cells(dem_handle* h, int32_t* cells, int32_t max_pip) {
@@ -868,7 +887,7 @@ int dem_get_stats_noalloc(dem_handle* h, dem_stats* s) {
 int dem_set_profiling(dem_handle* h, int32_t on) {
   API_GUARD(h);
   prof_collect(h);
-  h->prof = on != 0;
+  h->prof = on < 0 ? 0 : (on > 2 ? 2 : on);
   for (int k = 0; k < DEM_PROF_N; ++k) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
   return 0;
 }

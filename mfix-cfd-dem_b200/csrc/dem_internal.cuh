@@ -247,6 +247,8 @@ struct dem_handle {
   double* wall_pft = nullptr; // [i][cmax][3]
   uint8_t* wall_live = nullptr; // [i] 1 when some wall slot may be in use
   uint8_t* wall_cand = nullptr; // [i] 1 when the particle's DES cell holds facets
+  int* wall_list = nullptr;     // this step's particles with wall work (arbitrary order)
+  int* d_nwall = nullptr;       // their count
   double* wf = nullptr;       // [i][6] wall force and torque of the last force pass (valid with wall_hit)
 
   // scan scratch
@@ -269,7 +271,7 @@ struct dem_handle {
   size_t stage_bytes = 0;
 
   // kernel-time accounting (dem_set_profiling)
-  bool prof = false;
+  int prof = 0;                // 0 off, 1 kernel classes, 2 also the parts of the force step
   struct ProfEv { int cls; cudaEvent_t a, b; };
   std::vector<ProfEv> prof_pending;
   std::vector<cudaEvent_t> ev_pool;

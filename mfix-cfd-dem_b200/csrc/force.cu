@@ -337,52 +337,79 @@ __device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, PSta
 }
 
 // ---------------------------------------------------------------------------
-// Kernel 1 (per particle): wall contacts of NORMAL particles whose DES cell
-// holds facets.  Writes the particle's wall force and torque, which are the
-// first terms of FC/TOW in the reference's order (CALC_DEM_FORCE_WITH_WALL_STL
-// runs before the pair loop, calc_force_dem.f:113).
+// The particles with wall work this step: NORMAL particles whose DES cell
+// holds facets, and NORMAL particles elsewhere whose history slots may be in
+// use (k_walls clears them).  Each block of WALL_LIST_T threads appends its
+// particles in index order with one atomic; blocks land in arbitrary order,
+// which does not matter: each particle's wall terms depend on it alone.
+constexpr int WALL_LIST_T = 1024;
+__global__ void __launch_bounds__(WALL_LIST_T)
+k_wall_list(int n, const int8_t* __restrict__ state, const uint8_t* __restrict__ wall_cand,
+            const uint8_t* __restrict__ wall_live, int* __restrict__ list, int* __restrict__ count) {
+  __shared__ int warp_n[WALL_LIST_T / 32];
+  __shared__ int block_base;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool need = i < n && state[i] == DEM_STATE_NORMAL && (wall_cand[i] | wall_live[i]);
+  const unsigned m = __ballot_sync(0xffffffffu, need);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) warp_n[warp] = __popc(m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int tot = 0;
+    for (int k = 0; k < WALL_LIST_T / 32; ++k) { const int c = warp_n[k]; warp_n[k] = tot; tot += c; }
+    block_base = tot ? atomicAdd(count, tot) : 0;
+  }
+  __syncthreads();
+  if (need) list[block_base + warp_n[warp] + __popc(m & ((1u << lane) - 1u))] = i;
+}
+
+// Kernel 1 (per listed particle): wall contacts of NORMAL particles whose DES
+// cell holds facets.  Writes the particle's wall force and torque, which are
+// the first terms of FC/TOW in the reference's order
+// (CALC_DEM_FORCE_WITH_WALL_STL runs before the pair loop,
+// calc_force_dem.f:113).  Persistent grid over the list built by k_wall_list.
 template <int COLL, bool B>
 __global__ void __launch_bounds__(128)
-k_walls(DevParams p0, BatchView bv, WallCtx w, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
-        const double4* __restrict__ omg4, const uint8_t* __restrict__ phase, const int8_t* __restrict__ state,
+k_walls(DevParams p0, BatchView bv, WallCtx w, const int* __restrict__ wlist, const int* __restrict__ wcount,
+        const double4* __restrict__ pos4, const double4* __restrict__ vel4,
+        const double4* __restrict__ omg4, const uint8_t* __restrict__ phase,
         uint8_t* __restrict__ wall_live, const uint8_t* __restrict__ wall_cand, double* __restrict__ wf,
         uint8_t* __restrict__ wall_hit, DevErr* __restrict__ err) {
-  const int me = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nw = *wcount;
   unsigned long long nwc = 0;
   unsigned eflags = 0;
-  if (me < p0.n && state[me] == DEM_STATE_NORMAL) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nw; q += gridDim.x * blockDim.x) {
+    const int me = wlist[q];
     const DevParams& p = sysp<B>(p0, bv, me);
     if (!wall_cand[me]) {
       // no facet near: clear the history once (calc_collision_wall_mod.f:194-198)
-      if (wall_live[me]) {
-        int* fid = w.wall_fid + (size_t)me * p.cmax;
-        double* wp = w.wall_pft + (size_t)me * p.cmax * 3;
-        for (int q = 0; q < p.cmax; ++q) fid[q] = -1;
-        for (int q = 0; q < 3 * p.cmax; ++q) wp[q] = 0.0;
-        wall_live[me] = 0;
-      }
-    } else {
-      PState S;
-      const double4 a = pos4[me];
-      S.x[0] = a.x; S.x[1] = a.y; S.x[2] = a.z; S.r = a.w;
-      double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
-      const bool live = wall_live[me] != 0;
-      const unsigned long long nwc0 = nwc;
-      wall_contacts<COLL>(p, w, me, S, live, vel4, omg4, phase, f, t, nwc, eflags);
-      const bool hit = nwc > nwc0;
-      bool used = hit;
-      if (!hit && live) {
-        const int* fid = w.wall_fid + (size_t)me * p.cmax;
-        for (int q = 0; q < p.cmax; ++q) used = used || fid[q] != -1;
-      }
-      if (used != live) wall_live[me] = used ? 1 : 0;
-      if (hit) {
-        // the wall terms are the first terms of FC/TOW; the gather reads
-        // them only for particles marked here
-        double* o = wf + 6 * (size_t)me;
-        o[0] = f[0]; o[1] = f[1]; o[2] = f[2]; o[3] = t[0]; o[4] = t[1]; o[5] = t[2];
-        wall_hit[me] = 1;
-      }
+      int* fid = w.wall_fid + (size_t)me * p.cmax;
+      double* wp = w.wall_pft + (size_t)me * p.cmax * 3;
+      for (int s = 0; s < p.cmax; ++s) fid[s] = -1;
+      for (int s = 0; s < 3 * p.cmax; ++s) wp[s] = 0.0;
+      wall_live[me] = 0;
+      continue;
+    }
+    PState S;
+    const double4 a = pos4[me];
+    S.x[0] = a.x; S.x[1] = a.y; S.x[2] = a.z; S.r = a.w;
+    double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+    const bool live = wall_live[me] != 0;
+    const unsigned long long nwc0 = nwc;
+    wall_contacts<COLL>(p, w, me, S, live, vel4, omg4, phase, f, t, nwc, eflags);
+    const bool hit = nwc > nwc0;
+    bool used = hit;
+    if (!hit && live) {
+      const int* fid = w.wall_fid + (size_t)me * p.cmax;
+      for (int s = 0; s < p.cmax; ++s) used = used || fid[s] != -1;
+    }
+    if (used != live) wall_live[me] = used ? 1 : 0;
+    if (hit) {
+      // the wall terms are the first terms of FC/TOW; the gather reads
+      // them only for particles marked here
+      double* o = wf + 6 * (size_t)me;
+      o[0] = f[0]; o[1] = f[1]; o[2] = f[2]; o[3] = t[0]; o[4] = t[1]; o[5] = t[2];
+      wall_hit[me] = 1;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -495,6 +522,82 @@ __device__ __forceinline__ void add_rolling(const DevParams& p, double r, const 
   for (int c = 0; c < 3; ++c) t[c] = t[c] + -(p.mew_r * (2.0 * r) * q.kn * q.ov * w[c] / om);
 }
 
+// One pair's terms on one of its particles: the owner adds +FC and DCL2*TF,
+// the neighbour -FC and DCI2*TF (calc_force_dem.f:466-506).
+template <bool NBR>
+__device__ __forceinline__ void add_pair_terms(const DevParams& p, const PairRec& o, bool roll, double r,
+                                               const double w[3], double om, double f[3], double t[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[c] = NBR ? f[c] - o.fc[c] : f[c] + o.fc[c];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) t[c] = t[c] + (NBR ? o.dci2 : o.dcl2) * o.tf[c];
+  if (roll && om > 0.0) add_rolling(p, r, w, om, o, t);
+}
+
+// The records of the set bits of `mask` in ascending order; each record's
+// load is issued before the previous record is added.
+template <bool NBR, class Idx>
+__device__ __forceinline__ void add_flagged(const DevParams& p, unsigned mask, Idx idx,
+                                            const PairRec* __restrict__ prec, bool roll, double r,
+                                            const double w[3], double om, double f[3], double t[3]) {
+  if (!mask) return;
+  PairRec cur = prec[idx(__ffs(mask) - 1)];
+  mask &= mask - 1u;
+  while (true) {
+    const bool more = mask != 0u;
+    PairRec nxt;
+    if (more) {
+      nxt = prec[idx(__ffs(mask) - 1)];
+      mask &= mask - 1u;
+    }
+    add_pair_terms<NBR>(p, cur, roll, r, w, om, f, t);
+    if (!more) break;
+    cur = nxt;
+  }
+}
+
+// Incoming entries from q on (sorted by owner) whose owner is at most lim,
+// 32 at a time: the window's contact flags are read first (independent
+// loads), then the flagged records.  Returns the first entry not taken.
+__device__ __forceinline__ int add_incoming(const DevParams& p, int q, int ie, int lim,
+                                            const int2* __restrict__ in_pair, const uint8_t* __restrict__ pflag,
+                                            const PairRec* __restrict__ prec, bool roll, double r,
+                                            const double w[3], double om, double f[3], double t[3]) {
+  while (q < ie) {
+    const int cnt = min(32, ie - q);
+    unsigned mask = 0u;
+    int stop = cnt;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      if (k < cnt) {
+        const int2 e = in_pair[q + k];
+        if (e.x > lim && k < stop) stop = k;
+        if (pflag[e.y] & PF_CONTACT) mask |= 1u << k;
+      }
+    }
+    if (stop < 32) mask &= (1u << stop) - 1u;
+    const int base = q;
+    add_flagged<true>(p, mask, [&](int k) { return in_pair[base + k].y; }, prec, roll, r, w, om, f, t);
+    q += stop;
+    if (stop < cnt) break;
+  }
+  return q;
+}
+
+// The particle's own row [rs, re), 32 entries at a time.
+__device__ __forceinline__ void add_own(const DevParams& p, int rs, int re, const uint8_t* __restrict__ pflag,
+                                        const PairRec* __restrict__ prec, bool roll, double r, const double w[3],
+                                        double om, double f[3], double t[3]) {
+  for (int base = rs; base < re; base += 32) {
+    const int cnt = min(32, re - base);
+    unsigned mask = 0u;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k)
+      if (k < cnt && (pflag[base + k] & PF_CONTACT)) mask |= 1u << k;
+    add_flagged<false>(p, mask, [&](int k) { return base + k; }, prec, roll, r, w, om, f, t);
+  }
+}
+
 // Kernel 3 (per particle): sums FC/TOW in the serial reference's order --
 // wall terms, pairs owned by lower-index particles (ascending owner), the
 // particle's own row, pairs owned by higher-index particles -- and either
@@ -514,9 +617,8 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
   if (me >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, me);
   const int8_t st = state[me];
-  const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
-  const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
-  const double r = X.w, m = V.w, omoi = W.w;
+  const double4 W = omg_c[me];
+  const double w[3] = {W.x, W.y, W.z};
   double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
   // the contacts of this pass; a particle in none has no terms to add
   const bool wh = wall_hit[me] != 0, ph = touched[me] != 0;
@@ -528,37 +630,18 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
   }
   if (st != DEM_STATE_NONEXISTENT && ph) {
     const bool roll = p.mew_r > 0.0;
+    const double r = pos_c[me].w;
     double om = 0.0;
     if (roll) om = sqrt(dot3(w, w));
     const int rs = me ? row_end[me - 1] : 0, re = row_end[me];
     const int is = in_start[me], ie = in_start[me + 1];
-    int q = is;
-    for (int pass = 0; pass < 2; ++pass) {
-      for (; q < ie; ++q) {
-        const int2 e = in_pair[q];
-        if (pass == 0 && e.x > me) break;
-        if (!(pflag[e.y] & PF_CONTACT)) continue;
-        const PairRec o = prec[e.y];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) f[c] = f[c] - o.fc[c];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) t[c] = t[c] + o.dci2 * o.tf[c];
-        if (roll && om > 0.0) add_rolling(p, r, w, om, o, t);
-      }
-      if (pass == 0) {
-        for (int cc = rs; cc < re; ++cc) {
-          if (!(pflag[cc] & PF_CONTACT)) continue;
-          const PairRec o = prec[cc];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) f[c] = f[c] + o.fc[c];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) t[c] = t[c] + o.dcl2 * o.tf[c];
-          if (roll && om > 0.0) add_rolling(p, r, w, om, o, t);
-        }
-      }
-    }
+    const int q = add_incoming(p, is, ie, me, in_pair, pflag, prec, roll, r, w, om, f, t);
+    add_own(p, rs, re, pflag, prec, roll, r, w, om, f, t);
+    add_incoming(p, q, ie, INT_MAX, in_pair, pflag, prec, roll, r, w, om, f, t);
   }
-  finish_particle<MODE>(p, me, st, x, v, w, r, m, omoi, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
+  const double4 X = pos_c[me], V = vel_c[me];
+  const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z};
+  finish_particle<MODE>(p, me, st, x, v, w, X.w, V.w, W.w, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
                         rot_acc_old, vslot);
 }
 
@@ -595,10 +678,15 @@ static WallCtx wall_ctx(dem_handle* h) {
 template <int COLL, bool B>
 static void launch_walls_t(dem_handle* h) {
   const int c = h->cur;
-  const int T = 128, G = (h->n + T - 1) / T;
-  k_walls<COLL, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->pos4[c], h->vel4[c], h->omg4[c],
-                                           h->phase, h->state, h->wall_live, h->wall_cand, h->wf, h->wall_hit, h->derr);
-  DEM_LAUNCH(h);
+  const int T = 128;
+  cudaMemsetAsync(h->d_nwall, 0, sizeof(int), h->stream);
+  k_wall_list<<<(h->n + WALL_LIST_T - 1) / WALL_LIST_T, WALL_LIST_T, 0, h->stream>>>(
+      h->n, h->state, h->wall_cand, h->wall_live, h->wall_list, h->d_nwall);
+  // persistent: the resident blocks of the kernel's register budget
+  k_walls<COLL, B><<<h->n_sm * 4, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->wall_list, h->d_nwall,
+                                                     h->pos4[c], h->vel4[c], h->omg4[c], h->phase, h->wall_live,
+                                                     h->wall_cand, h->wf, h->wall_hit, h->derr);
+  h->launches += 2;
 }
 
 template <int COLL, bool B>
@@ -642,12 +730,6 @@ static void launch_gather_fp64(dem_handle* h, int mode) {
   else launch_gather_t<2, B>(h);
 }
 
-template <bool B>
-static void launch_pairs_gather(dem_handle* h, int mode) {
-  launch_pairs_fp64<B>(h);
-  launch_gather_fp64<B>(h, mode);
-}
-
 void launch_pairs_only(dem_handle* h) {
   if (h->dp.prec == DEM_PREC_SPLIT) launch_pairs_split(h);
   else if (h->batch()) launch_pairs_fp64<true>(h);
@@ -664,14 +746,20 @@ void launch_gather_only(dem_handle* h) {
 // Euler/AB2 integration into the other state buffer.  The collision model,
 // integrator and force precision are common to all systems of a batch.
 static void launch_force_kernels(dem_handle* h, int mode, bool split) {
-  launch_walls(h);
-  if (split) {
-    launch_pairs_split(h);
-    launch_gather_split(h, mode);
-    return;
+  {
+    ProfScope ps(h, DEM_PROF_WALLS);
+    launch_walls(h);
   }
-  if (h->batch()) launch_pairs_gather<true>(h, mode);
-  else launch_pairs_gather<false>(h, mode);
+  {
+    ProfScope ps(h, DEM_PROF_PAIRS);
+    if (split) launch_pairs_split(h);
+    else if (h->batch()) launch_pairs_fp64<true>(h);
+    else launch_pairs_fp64<false>(h);
+  }
+  ProfScope ps(h, DEM_PROF_GATHER);
+  if (split) launch_gather_split(h, mode);
+  else if (h->batch()) launch_gather_fp64<true>(h, mode);
+  else launch_gather_fp64<false>(h, mode);
 }
 
 // Displacement bound since the last build += this step's largest particle

@@ -209,28 +209,46 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
     const float rf = (float)p.mew_r * (2.f * (float)r);
     const int rs = me ? row_end[me - 1] : 0, re = row_end[me];
     const int is = in_start[me], ie = in_start[me + 1];
-    for (int q = is; q < ie; ++q) {
-      const int cc = in_pair[q].y;
-      if (!(pflag[cc] & PF_CONTACT)) continue;
-      const PairRec32 o = prec[cc];
+    auto add = [&](const PairRec32& o, bool nbr) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) { F.add(c, -o.fc[c]); T.add(c, o.dci2 * o.tf[c]); }
+      for (int c = 0; c < 3; ++c) { F.add(c, nbr ? -o.fc[c] : o.fc[c]); T.add(c, (nbr ? o.dci2 : o.dcl2) * o.tf[c]); }
       if (roll) {
         const float s = -(rf * o.kn * o.ov) / om;
 #pragma unroll
         for (int c = 0; c < 3; ++c) T.add(c, s * wf32[c]);
       }
+    };
+    // 32 entries at a time: the window's contact flags first (independent
+    // loads), then the flagged records, each load issued before the
+    // previous record is added
+    auto flagged = [&](unsigned mask, auto idx, bool nbr) {
+      if (!mask) return;
+      PairRec32 cur = prec[idx(__ffs(mask) - 1)];
+      mask &= mask - 1u;
+      while (true) {
+        const bool more = mask != 0u;
+        PairRec32 nxt;
+        if (more) { nxt = prec[idx(__ffs(mask) - 1)]; mask &= mask - 1u; }
+        add(cur, nbr);
+        if (!more) break;
+        cur = nxt;
+      }
+    };
+    for (int base = is; base < ie; base += 32) {
+      const int cnt = min(32, ie - base);
+      unsigned mask = 0u;
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k)
+        if (k < cnt && (pflag[in_pair[base + k].y] & PF_CONTACT)) mask |= 1u << k;
+      flagged(mask, [&](int k) { return in_pair[base + k].y; }, true);
     }
-    for (int cc = rs; cc < re; ++cc) {
-      if (!(pflag[cc] & PF_CONTACT)) continue;
-      const PairRec32 o = prec[cc];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) { F.add(c, o.fc[c]); T.add(c, o.dcl2 * o.tf[c]); }
-      if (roll) {
-        const float s = -(rf * o.kn * o.ov) / om;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) T.add(c, s * wf32[c]);
-      }
+    for (int base = rs; base < re; base += 32) {
+      const int cnt = min(32, re - base);
+      unsigned mask = 0u;
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k)
+        if (k < cnt && (pflag[base + k] & PF_CONTACT)) mask |= 1u << k;
+      flagged(mask, [&](int k) { return base + k; }, false);
     }
   }
   double f[3], t[3];

@@ -16,6 +16,9 @@ DEM_INTG_AB2 = 1
 DEM_PREC_FP64 = 0
 DEM_PREC_SPLIT = 1
 
+DEM_INTERP_GARG = 0
+DEM_INTERP_NONE = 1
+
 DEM_STATE_NONEXISTENT = 0
 DEM_STATE_NORMAL = 1
 DEM_STATE_ENTERING = 2
@@ -125,6 +128,8 @@ class DemFluidGrid(C.Structure):
         ("jmax", C.c_int32),
         ("kmax", C.c_int32),
         ("drag_model", C.c_int32),
+        ("interp_scheme", C.c_int32),
+        ("reserved_i", C.c_int32),
         ("dx", C.c_double),
         ("dy", C.c_double),
         ("dz", C.c_double),
@@ -177,6 +182,19 @@ class DemSysStatus(C.Structure):
     ]
 
 
+class DemResInfo(C.Structure):
+    _fields_ = [
+        ("version", C.c_double),
+        ("dtsolid", C.c_double),
+        ("vtp_findex", C.c_int32),
+        ("tecplot_findex", C.c_int32),
+        ("n_particles", C.c_int32),
+        ("n_pairs", C.c_int32),
+        ("ro_sol", C.c_double * DEM_MAX_PHASES),
+        ("reserved", C.c_double * 4),
+    ]
+
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -197,6 +215,7 @@ SIGNATURES = {
     "download_pairs": (C.c_int, [_P, _I32, _I32, _D, C.c_int64, C.c_int32]),
     "upload_pairs": (C.c_int, [_P, _I32, _I32, _D, C.c_int64, C.c_int32]),
     "download_wall_history": (C.c_int, [_P, _I32, _D, C.c_int32]),
+    "upload_wall_history": (C.c_int, [_P, _I32, _D, C.c_int32]),
     "download_cells": (C.c_int, [_P, _I32, C.c_int32]),
     "desgrid_pic": (C.c_int, [_P]),
     "neighbour": (C.c_int, [_P]),
@@ -209,6 +228,9 @@ SIGNATURES = {
     "get_mean_fields": (C.c_int, [_P, _D, _D]),
     "comp_mean_fields": (C.c_int, [_P]),
     "drag_gs_des0": (C.c_int, [_P]),
+    "drag_gs_gas0": (C.c_int, [_P, _D, _D, _D, _D]),
+    "drag_gs_des1": (C.c_int, [_P]),
+    "drag_gs_gas1": (C.c_int, [_P, _D, _D, _D]),
     "step_coupled": (C.c_int, [_P, C.c_int32, C.c_int32]),
 }
 
@@ -235,6 +257,13 @@ DEM_ONLY = {
     "sys_download_state": (C.c_int, [_P, C.c_int32, _D, _D, _D, _I8, C.c_int32]),
     "sys_start": (C.c_int, [_P, _I32, C.c_int32]),
     "batch_step": (C.c_int, [_P, C.c_int32]),
+    # restart files
+    "write_res0_des": (C.c_int, [_P, C.c_char_p, C.POINTER(DemResInfo)]),
+    "read_res0_des": (C.c_int, [_P, C.c_char_p, C.c_int32, C.POINTER(DemResInfo)]),
+    "res_write": (C.c_int, [C.c_char_p, C.POINTER(DemResInfo), C.c_int32, C.c_int32, _D, _D, _D, _D, _I8, _I32,
+                            _I32, _I32, _D, C.c_int64]),
+    "res_read": (C.c_int, [C.c_char_p, C.POINTER(DemResInfo), C.c_int32, C.c_int32, _D, _D, _D, _D, _D, _I8, _I32,
+                           _I32, _I32, _D, C.c_int64]),
     "sys_get_stats": (C.c_int, [_P, C.c_int32, C.POINTER(DemStats)]),
     "sys_download_pairs": (C.c_int, [_P, C.c_int32, _I32, _I32, _D, C.c_int64, C.c_int32]),
     "sys_info": (C.c_int, [_P, C.c_int32, C.POINTER(DemSysStatus)]),

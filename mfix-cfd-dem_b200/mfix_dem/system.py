@@ -168,6 +168,13 @@ class DemSystem:
         self._call("download_wall_history", self._h, _ip(fid), _dp(pf), C.c_int32(n))
         return fid, pf
 
+    def upload_wall_history(self, facet_id, pft):
+        n = self.n
+        cm = self.params.collision_array_max or 8
+        fid = np.ascontiguousarray(facet_id, dtype=np.int32).reshape(n, cm)
+        pf = np.ascontiguousarray(pft, dtype=np.float64).reshape(n, cm, 3)
+        self._call("upload_wall_history", self._h, _ip(fid), _dp(pf), C.c_int32(n))
+
     def download_cells(self):
         cells = np.empty(self.n, dtype=np.int32)
         self._call("download_cells", self._h, _ip(cells), C.c_int32(self.n))
@@ -230,24 +237,61 @@ class DemSystem:
     def drag_gs_des0(self):
         self._call("drag_gs_des0", self._h)
 
+    def drag_gs_gas0(self):
+        """DRAG_GS_GAS0: returns F_GDS (ncells), DRAG_AM (ncells),
+        DRAG_BM (3, ncells) and F_GP (max_pip)."""
+        f_gds = np.empty(self._ncell); am = np.empty(self._ncell)
+        bm = np.empty((3, self._ncell)); f_gp = np.empty(self.n)
+        self._call("drag_gs_gas0", self._h, _dp(f_gds), _dp(am), _dp(bm), _dp(f_gp))
+        return f_gds, am, bm, f_gp
+
+    def drag_gs_des1(self):
+        self._call("drag_gs_des1", self._h)
+
+    def drag_gs_gas1(self):
+        """DRAG_GS_GAS1 without a filter: returns F_GDS (ncells), DRAG_BM
+        (3, ncells) and F_GP (max_pip)."""
+        f_gds = np.empty(self._ncell); bm = np.empty((3, self._ncell)); f_gp = np.empty(self.n)
+        self._call("drag_gs_gas1", self._h, _dp(f_gds), _dp(bm), _dp(f_gp))
+        return f_gds, bm, f_gp
+
     def step_coupled(self, nsteps: int = 1, nn_first: Optional[int] = None):
         first = self.nn + 1 if nn_first is None else nn_first
         self._call("step_coupled", self._h, C.c_int32(first), C.c_int32(nsteps))
         self.nn = first + nsteps - 1
 
     # ---- CUDA-only ---------------------------------------------------
+    def write_res0_des(self, path, ro_sol, vtp_findex=0, tecplot_findex=0, dtsolid=None):
+        """WRITE_RES0_DES: the DEM restart file of this system.  ro_sol is
+        RO_SOL per phase (the density the particles were generated with)."""
+        info = abi.DemResInfo()
+        info.vtp_findex, info.tecplot_findex = int(vtp_findex), int(tecplot_findex)
+        info.dtsolid = self.params.dtsolid if dtsolid is None else float(dtsolid)
+        for m, r in enumerate(ro_sol):
+            info.ro_sol[m] = float(r)
+        self._call("write_res0_des", self._h, str(path).encode(), C.byref(info))
+
+    def read_res0_des(self, path, restore_pairs=True) -> abi.DemResInfo:
+        """READ_RES0_DES into this system; with restore_pairs the pair list
+        and its history come from the file, else call init_neighbors."""
+        info = abi.DemResInfo()
+        self._call("read_res0_des", self._h, str(path).encode(), C.c_int32(1 if restore_pairs else 0),
+                   C.byref(info))
+        return info
+
     def set_graphs(self, on: bool):
         self._call("set_graphs", self._h, C.c_int32(1 if on else 0))
 
-    def set_profiling(self, on: bool):
-        self._call("set_profiling", self._h, C.c_int32(1 if on else 0))
+    def set_profiling(self, on):
+        """False/True, or 2 to time the parts of the force step as well."""
+        self._call("set_profiling", self._h, C.c_int32(int(on)))
 
     def profile(self):
         """{class: (ms, launches)} since profiling was switched on."""
-        ms = (C.c_double * 6)()
-        nl = (C.c_int64 * 6)()
+        ms = (C.c_double * 9)()
+        nl = (C.c_int64 * 9)()
         self._call("get_profile", self._h, ms, nl)
-        names = ("force", "neighbor", "desgrid", "integrate", "coupling", "other")
+        names = ("force", "neighbor", "desgrid", "integrate", "coupling", "other", "walls", "pairs", "gather")
         return {k: (float(ms[i]), int(nl[i])) for i, k in enumerate(names)}
 
     def launch_count(self) -> int:
@@ -380,8 +424,9 @@ class BatchSystem:
         self._call("launch_count", self._h, C.byref(v))
         return int(v.value)
 
-    def set_profiling(self, on: bool):
-        self._call("set_profiling", self._h, C.c_int32(1 if on else 0))
+    def set_profiling(self, on):
+        """False/True, or 2 to time the parts of the force step as well."""
+        self._call("set_profiling", self._h, C.c_int32(int(on)))
 
     profile = DemSystem.profile
     pair_count = DemSystem.pair_count

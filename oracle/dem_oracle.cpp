@@ -97,6 +97,8 @@ struct Oracle {
   int gi2 = 0, gj2 = 0, gk2 = 0;          // imax+2, jmax+2, kmax+2
   std::vector<double> xe, yn, zt;         // face positions, index 0..imax+2
   std::vector<double> ep_g, u_g, v_g, w_g, p_force, rop_s, vol_surr;
+  std::vector<double> vol_node;            // DES_VOL_NODE per node
+  std::vector<double> drag_am, drag_bm, f_gds;  // DRAG_AM, DRAG_BM(:,3), F_GDS
   std::vector<int> pijk;                  // (n,4): i, j, k, ijk (1-based), 0 = none
   std::vector<double> f_gp;               // F_GP(n)
   std::vector<int> pic_start, pic_list;   // particles per fluid cell, ascending
@@ -776,7 +778,14 @@ struct Oracle {
 
   // CALC_FORCE_DEM (calc_force_dem.f:18-544), serial order: walls first, then
   // LL ascending, CC ascending, scattering into FC/TOW.
+  // CALC_FORCE_DEM adds to FC/TOW, which CFNEWVALUES leaves at zero
+  // (cfnewvalues.f:709-723); the entry point starts from zero so that a
+  // force evaluation outside the DES_TIME_STEP sequence (forces taken and not
+  // integrated) does not carry into the next one -- the CUDA library's
+  // dem_calc_force stores the sums the same way.
   int calc_force() {
+    std::fill(fc.begin(), fc.end(), 0.0);
+    std::fill(tow.begin(), tow.end(), 0.0);
     n_contacts = 0; n_wall_contacts = 0; max_overlap_ratio = 0.0;
     int wrc = 0;
     int64_t nwc = 0;
@@ -959,6 +968,20 @@ struct Oracle {
                 if (fluid_at(ii, jj, kk)) v = v + vol();
           vol_surr[cijk(i, j, k)] = v;
         }
+    // DES_VOL_NODE (cfassign.f:104-228): a quarter (2D) or an eighth (3D)
+    // of the volume of each fluid cell sharing node (I,J,K), summed in the
+    // reference's order (the k+1 plane as ijkp, ipjpkp, ijpkp, ipjkp)
+    vol_node.assign(vol_surr.size(), 0.0);
+    const double avn = p.no_k ? 0.25 : 0.125;
+    auto fv = [&](int i, int j, int k) { return fluid_at(i, j, k) ? vol() : 0.0; };
+    for (int k = kk0; k <= kk1; ++k)
+      for (int j = 1; j <= g.jmax + 1; ++j)
+        for (int i = 1; i <= g.imax + 1; ++i) {
+          double v = avn * (fv(i, j, k) + fv(i + 1, j, k) + fv(i, j + 1, k) + fv(i + 1, j + 1, k));
+          if (!p.no_k)
+            v = v + avn * (fv(i, j, k + 1) + fv(i + 1, j + 1, k + 1) + fv(i, j + 1, k + 1) + fv(i + 1, j, k + 1));
+          vol_node[cijk(i, j, k)] = v;
+        }
     pijk.assign((size_t)4 * n, 0);
     f_gp.assign(n, 0.0);
   }
@@ -1025,56 +1048,209 @@ struct Oracle {
     return 0.75 * cd * vrel * ropg * std::pow(epg, -2.65) / dpm;
   }
 
-  // DRAG_GS_DES0 (drag_gs_des0.f:22-219): gas velocity at the particle from
-  // the 2x2x2 node stencil of its fluid cell, DES_DRAG_GP (drag_gp_des.f:
-  // 97-257, Model A) and FC += F_GP*(u_g - v_p) + P_FORCE*PVOL.
-  void drag() {
+  // Gas velocity at a particle of fluid cell (i,j,k): the staggered face
+  // velocities averaged to the 2x2x2 node stencil and interpolated with the
+  // trilinear weights (drag_gs_des0.f:117-170 and 313-361,
+  // DRAG_INTERPOLATION drag_gs_des0.f:507-566).  Returns the weights too.
+  void gas_velocity(int l, int i, int j, int k, double velfp[3], double w[2][2][2]) const {
     const double avg = p.no_k ? 0.5 : 0.25;
+    const int iw = i - 1, js = j - 1, kb = p.no_k ? 1 : k - 1;
+    double vst[2][2][2][3];
+    for (int kk = 0; kk < (p.no_k ? 1 : 2); ++kk)
+      for (int jj = 0; jj < 2; ++jj)
+        for (int ii = 0; ii < 2; ++ii) {
+          int I = iw + ii, J = js + jj, K = kb + kk;
+          int c = cijk(I, J, K), ipjk = cijk(I + 1, J, K), ijpk = cijk(I, J + 1, K), ipjpk = cijk(I + 1, J + 1, K);
+          double* v = vst[kk][jj][ii];
+          v[0] = avg * (u_g[c] + u_g[ijpk]);
+          v[1] = avg * (v_g[c] + v_g[ipjk]);
+          if (!p.no_k) {
+            int ijpkp = cijk(I, J + 1, K + 1), ipjkp = cijk(I + 1, J, K + 1), ijkp = cijk(I, J, K + 1);
+            v[0] = v[0] + avg * (u_g[ijkp] + u_g[ijpkp]);
+            v[1] = v[1] + avg * (v_g[ijkp] + v_g[ipjkp]);
+            v[2] = avg * (w_g[c] + w_g[ijpk] + w_g[ipjk] + w_g[ipjpk]);
+          } else {
+            v[2] = 0.0;
+          }
+        }
+    double x[3] = {P(pos, l, 0), P(pos, l, 1), P(pos, l, 2)};
+    weights(i, j, k, x, w);
+    velfp[0] = velfp[1] = velfp[2] = 0.0;
+    for (int kk = 0; kk < (p.no_k ? 1 : 2); ++kk)
+      for (int jj = 0; jj < 2; ++jj)
+        for (int ii = 0; ii < 2; ++ii)
+          for (int c = 0; c < (p.no_k ? 2 : 3); ++c) velfp[c] = velfp[c] + vst[kk][jj][ii][c] * w[kk][jj][ii];
+  }
+
+  // DES_DRAG_GP (drag_gp_des.f:97-257, Model A, Gidaspow): F_GP of particle
+  // l in fluid cell ijk with the under-relaxation UR_F_GS; returns PVOL.
+  double update_f_gp(int l, int ijk, const double velfp[3]) {
+    double vp[3] = {P(vel, l, 0), P(vel, l, 1), P(vel, l, 2)};
+    const double epg = ep_g[ijk];
+    double vs[3] = {velfp[0] - vp[0], velfp[1] - vp[1], velfp[2] - vp[2]};
+    double vrel = std::sqrt(dot3(vs, vs));
+    double dpm = 2.0 * rad[l];
+    double dga = drag_gidaspow(epg, g.mu_g, g.ro_g, g.ro_g * epg, vrel, dpm);
+    double pvol = ((4.0 / 3.0) * pi_c) * (rad[l] * (rad[l] * rad[l]));
+    double fgs = dga * pvol;
+    f_gp[l] = (1.0 - g.ur_f_gs) * f_gp[l] + g.ur_f_gs * fgs;
+    return pvol;
+  }
+
+  // DRAG_GS_DES0 (drag_gs_des0.f:22-219): gas velocity at the particle,
+  // DES_DRAG_GP and FC += F_GP*(u_g - v_p) + P_FORCE*PVOL.
+  void drag() {
     for (int l = 0; l < n; ++l) {
       int8_t st = state[l];
       if (st == DEM_STATE_NONEXISTENT || st >= DEM_STATE_NORMAL_GHOST) continue;
       int i = pijk[4 * (size_t)l], j = pijk[4 * (size_t)l + 1], k = pijk[4 * (size_t)l + 2];
       if (!fluid_at(i, j, k)) continue;
-      const int iw = i - 1, js = j - 1, kb = p.no_k ? 1 : k - 1;
-      double vst[2][2][2][3];
-      for (int kk = 0; kk < (p.no_k ? 1 : 2); ++kk)
-        for (int jj = 0; jj < 2; ++jj)
-          for (int ii = 0; ii < 2; ++ii) {
-            int I = iw + ii, J = js + jj, K = kb + kk;
-            int c = cijk(I, J, K), ipjk = cijk(I + 1, J, K), ijpk = cijk(I, J + 1, K), ipjpk = cijk(I + 1, J + 1, K);
-            double* v = vst[kk][jj][ii];
-            v[0] = avg * (u_g[c] + u_g[ijpk]);
-            v[1] = avg * (v_g[c] + v_g[ipjk]);
-            if (!p.no_k) {
-              int ijpkp = cijk(I, J + 1, K + 1), ipjkp = cijk(I + 1, J, K + 1), ijkp = cijk(I, J, K + 1);
-              v[0] = v[0] + avg * (u_g[ijkp] + u_g[ijpkp]);
-              v[1] = v[1] + avg * (v_g[ijkp] + v_g[ipjkp]);
-              v[2] = avg * (w_g[c] + w_g[ijpk] + w_g[ipjk] + w_g[ipjpk]);
-            } else {
-              v[2] = 0.0;
-            }
-          }
-      double x[3] = {P(pos, l, 0), P(pos, l, 1), P(pos, l, 2)};
-      double w[2][2][2];
-      weights(i, j, k, x, w);
-      double velfp[3] = {0.0, 0.0, 0.0};
-      for (int kk = 0; kk < (p.no_k ? 1 : 2); ++kk)
-        for (int jj = 0; jj < 2; ++jj)
-          for (int ii = 0; ii < 2; ++ii)
-            for (int c = 0; c < (p.no_k ? 2 : 3); ++c) velfp[c] = velfp[c] + vst[kk][jj][ii][c] * w[kk][jj][ii];
-      double vp[3] = {P(vel, l, 0), P(vel, l, 1), P(vel, l, 2)};
+      double velfp[3], w[2][2][2];
+      gas_velocity(l, i, j, k, velfp, w);
       const int ijk = cijk(i, j, k);
-      const double epg = ep_g[ijk];
-      double vs[3] = {velfp[0] - vp[0], velfp[1] - vp[1], velfp[2] - vp[2]};
-      double vrel = std::sqrt(dot3(vs, vs));
-      double dpm = 2.0 * rad[l];
-      double dga = drag_gidaspow(epg, g.mu_g, g.ro_g, g.ro_g * epg, vrel, dpm);
-      double pvol = ((4.0 / 3.0) * pi_c) * (rad[l] * (rad[l] * rad[l]));
-      double fgs = dga * pvol;
-      f_gp[l] = (1.0 - g.ur_f_gs) * f_gp[l] + g.ur_f_gs * fgs;
+      const double pvol = update_f_gp(l, ijk, velfp);
+      double vp[3] = {P(vel, l, 0), P(vel, l, 1), P(vel, l, 2)};
       for (int c = 0; c < 3; ++c) X(fc, c)[l] = X(fc, c)[l] + f_gp[l] * (velfp[c] - vp[c]);
       if (!p_force.empty())
         for (int c = 0; c < 3; ++c) X(fc, c)[l] = X(fc, c)[l] + p_force[3 * (size_t)ijk + c] * pvol;
+    }
+  }
+
+  // DRAG_GS_GAS0 (drag_gs_des0.f:235-497): per fluid cell in IJK order and
+  // per particle in PIC order, F_GP again (DES_DRAG_GP) and its deposition
+  // to the cell's 2x2x2 nodes, DRAG_AM += F_GP*W/DES_VOL_NODE and
+  // DRAG_BM(:,c) += F_GP*V_p(c)*W/DES_VOL_NODE (statistical weight 1 for
+  // DEM); then F_GDS per fluid cell as the mean of its nodes' DRAG_AM
+  // (drag_gs_des0.f:451-494), zero elsewhere.  Serial, non-periodic: the
+  // node exchange DES_ADDNODEVALUES adds nothing.
+  void drag_gas() {
+    const size_t nc = vol_surr.size();
+    drag_am.assign(nc, 0.0);
+    drag_bm.assign(3 * nc, 0.0);
+    f_gds.assign(nc, 0.0);
+    const double wtp = 1.0;
+    for (int k = 1; k <= gk2; ++k)
+      for (int j = 1; j <= gj2; ++j)
+        for (int i = 1; i <= gi2; ++i) {
+          if (!fluid_at(i, j, k)) continue;
+          const int ijk = cijk(i, j, k);
+          const int iw = i - 1, js = j - 1, kb = p.no_k ? 1 : k - 1;
+          for (int q = pic_start[ijk]; q < pic_start[ijk + 1]; ++q) {
+            const int np = pic_list[q];
+            if (state[np] == DEM_STATE_NONEXISTENT || state[np] >= DEM_STATE_NORMAL_GHOST) continue;
+            double velfp[3], w[2][2][2];
+            gas_velocity(np, i, j, k, velfp, w);
+            update_f_gp(np, ijk, velfp);
+            const double vn[3] = {P(vel, np, 0), P(vel, np, 1), P(vel, np, 2)};
+            for (int kk = 0; kk < (p.no_k ? 1 : 2); ++kk)
+              for (int jj = 0; jj < 2; ++jj)
+                for (int ii = 0; ii < 2; ++ii) {
+                  const int node = cijk(iw + ii, js + jj, kb + kk);
+                  const double ovol = 1.0 / vol_node[node];
+                  drag_am[node] = drag_am[node] + f_gp[np] * w[kk][jj][ii] * ovol * wtp;
+                  for (int c = 0; c < 3; ++c)
+                    drag_bm[c * nc + node] = drag_bm[c * nc + node] + f_gp[np] * vn[c] * w[kk][jj][ii] * ovol * wtp;
+                }
+          }
+        }
+    const double avf = p.no_k ? 0.25 : 0.125;
+    for (int k = 1; k <= gk2; ++k)
+      for (int j = 1; j <= gj2; ++j)
+        for (int i = 1; i <= gi2; ++i) {
+          const int ijk = cijk(i, j, k);
+          if (!fluid_at(i, j, k)) { f_gds[ijk] = 0.0; continue; }
+          double f = avf * (drag_am[ijk] + drag_am[cijk(i, j - 1, k)] + drag_am[cijk(i - 1, j - 1, k)] +
+                            drag_am[cijk(i - 1, j, k)]);
+          if (!p.no_k)
+            f = f + avf * (drag_am[cijk(i, j, k - 1)] + drag_am[cijk(i, j - 1, k - 1)] +
+                           drag_am[cijk(i - 1, j - 1, k - 1)] + drag_am[cijk(i - 1, j, k - 1)]);
+          f_gds[ijk] = f;
+        }
+  }
+
+  // ---- DES_INTERP_SCHEME = NONE: the ...1 routines without a filter ----
+
+  // PVOL (generate_particles_mod.f:1399): 4/3 pi r^3.
+  double pvol_of(int l) const { return ((4.0 / 3.0) * pi_c) * (rad[l] * (rad[l] * rad[l])); }
+
+  // CALC_CELL_CENTER_GAS_VEL (drag_gs_des1.f:313-370) on a uniform grid
+  // (FX = FX_BAR = 1/2, set_geometry.f:344-345): the gas velocity at the
+  // centre of fluid cell (i,j,k); zero outside the fluid.
+  void cell_center_vel(int i, int j, int k, double v[3]) const {
+    if (!fluid_at(i, j, k)) { v[0] = v[1] = v[2] = 0.0; return; }
+    const int ijk = cijk(i, j, k);
+    v[0] = 0.5 * u_g[cijk(i - 1, j, k)] + 0.5 * u_g[ijk];     // AVG_X_E
+    v[1] = 0.5 * (v_g[cijk(i, j - 1, k)] + v_g[ijk]);         // AVG_Y_N
+    v[2] = p.no_k ? 0.0 : 0.5 * (w_g[cijk(i, j, k - 1)] + w_g[ijk]);   // AVG_Z_T
+  }
+
+  // COMP_MEAN_FIELDS1 with FILTER_SIZE = 0 (comp_mean_fields1.f:46-104):
+  // SOLVOLINC(PIJK(NP,4), M) += PVOL(NP) over NORMAL particles in index
+  // order, ROP_S = RO_S*SOLVOLINC/VOL on fluid cells; then CALC_EPG_DES.
+  void comp_mean_fields1() {
+    const size_t nc = vol_surr.size();
+    const int M = p.n_phases;
+    std::vector<double> solvolinc(nc * M, 0.0);
+    rop_s.assign(nc * M, 0.0);
+    for (int l = 0; l < n; ++l) {
+      if (state[l] != DEM_STATE_NORMAL) continue;
+      const int ijk = pijk[4 * (size_t)l + 3] - 1;
+      double& sv = solvolinc[(size_t)phase[l] * nc + ijk];
+      sv = sv + pvol_of(l);
+    }
+    for (int k = 1; k <= gk2; ++k)
+      for (int j = 1; j <= gj2; ++j)
+        for (int i = 1; i <= gi2; ++i) {
+          if (!fluid_at(i, j, k)) continue;
+          const int ijk = cijk(i, j, k);
+          for (int m = 0; m < M; ++m)
+            rop_s[(size_t)m * nc + ijk] = ro_s[m] * solvolinc[(size_t)m * nc + ijk] / vol();
+          double sum_eps = 0.0;
+          for (int m = 0; m < M; ++m) sum_eps = sum_eps + rop_s[(size_t)m * nc + ijk] / ro_s[m];
+          ep_g[ijk] = 1.0 - std::min(1.0, sum_eps);
+        }
+  }
+
+  // DRAG_GS_DES1 without a filter (drag_gs_des1.f:34-160, Model A, not
+  // explicitly coupled): per NORMAL particle the cell-centre gas velocity of
+  // its cell, DES_DRAG_GP with EP_G of the cell, FC += F_GP*(u_g - v_p) +
+  // P_FORCE*PVOL; F_GP = 0 for a particle outside the fluid cells.
+  void drag_des1() {
+    for (int l = 0; l < n; ++l) {
+      if (state[l] != DEM_STATE_NORMAL) continue;
+      const int i = pijk[4 * (size_t)l], j = pijk[4 * (size_t)l + 1], k = pijk[4 * (size_t)l + 2];
+      if (!fluid_at(i, j, k)) { f_gp[l] = 0.0; continue; }
+      const int ijk = cijk(i, j, k);
+      double velfp[3];
+      cell_center_vel(i, j, k, velfp);
+      const double pvol = update_f_gp(l, ijk, velfp);
+      double vp[3] = {P(vel, l, 0), P(vel, l, 1), P(vel, l, 2)};
+      for (int c = 0; c < 3; ++c) X(fc, c)[l] = X(fc, c)[l] + f_gp[l] * (velfp[c] - vp[c]);
+      if (!p_force.empty())
+        for (int c = 0; c < 3; ++c) X(fc, c)[l] = X(fc, c)[l] + p_force[3 * (size_t)ijk + c] * pvol;
+    }
+  }
+
+  // DRAG_GS_GAS1 without a filter (drag_gs_des1.f:179-301): per NORMAL
+  // particle of a fluid cell, in index order, F_GP again and DRAG_BM(IJK,:)
+  // += F_GP*V/VOL, F_GDS(IJK) += F_GP/VOL in its own cell; zero elsewhere.
+  void drag_gas1() {
+    const size_t nc = vol_surr.size();
+    drag_bm.assign(3 * nc, 0.0);
+    f_gds.assign(nc, 0.0);
+    for (int l = 0; l < n; ++l) {
+      if (state[l] != DEM_STATE_NORMAL) continue;
+      const int i = pijk[4 * (size_t)l], j = pijk[4 * (size_t)l + 1], k = pijk[4 * (size_t)l + 2];
+      if (!fluid_at(i, j, k)) continue;
+      const int ijk = cijk(i, j, k);
+      double velfp[3];
+      cell_center_vel(i, j, k, velfp);
+      update_f_gp(l, ijk, velfp);
+      const double lforce = f_gp[l];
+      const double ldbm[3] = {lforce * P(vel, l, 0), lforce * P(vel, l, 1), lforce * P(vel, l, 2)};
+      const double weight = 1.0 / vol();
+      for (int c = 0; c < 3; ++c) drag_bm[c * nc + ijk] = drag_bm[c * nc + ijk] + ldbm[c] * weight;
+      f_gds[ijk] = f_gds[ijk] + lforce * weight;
     }
   }
 
@@ -1082,6 +1258,7 @@ struct Oracle {
   // (calc_epg_des.f:123-150), one solids phase per particle phase.
   void comp_mean_fields() {
     particles_in_cell();
+    if (g.interp_scheme == DEM_INTERP_NONE) { comp_mean_fields1(); return; }
     const size_t nc = vol_surr.size();
     const int M = p.n_phases;
     std::vector<double> rops_node(nc * M, 0.0);
@@ -1142,7 +1319,7 @@ struct Oracle {
   int step_coupled(int nn) {
     int rc = calc_force();
     if (rc) return rc;
-    drag();
+    if (g.interp_scheme == DEM_INTERP_NONE) drag_des1(); else drag();   // CALC_DRAG_DES
     cfnewvalues();
     bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0);
     bool anyper = p.periodic[0] || p.periodic[1] || (p.periodic[2] && !p.no_k);
@@ -1305,6 +1482,16 @@ int orc_download_wall_history(orc_handle* h, int32_t* fid, double* pf, int32_t m
   return 0;
 }
 
+int orc_upload_wall_history(orc_handle* h, const int32_t* fid, const double* pf, int32_t max_pip) {
+  Oracle& o = h->o;
+  if (max_pip != o.n || !fid || !pf) return o.fail(DEM_ERR_ARG, "bad wall history arrays");
+  for (size_t s = 0; s < o.wall_fid.size(); ++s)
+    if (fid[s] != -1 && (fid[s] < 1 || fid[s] > o.nf)) return o.fail(DEM_ERR_ARG, "facet id out of range");
+  for (size_t s = 0; s < o.wall_fid.size(); ++s) o.wall_fid[s] = fid[s] < 0 ? -1 : fid[s] - 1;
+  std::copy(pf, pf + o.wall_pft.size(), o.wall_pft.begin());
+  return 0;
+}
+
 int orc_download_cells(orc_handle* h, int32_t* cells, int32_t max_pip) {
   Oracle& o = h->o;
   if (max_pip != o.n) return DEM_ERR_ARG;
@@ -1386,6 +1573,8 @@ int orc_set_gas_fields(orc_handle* h, const dem_fluid_grid* g, const double* ep_
   Oracle& o = h->o;
   if (!g || !ep_g || !u_g || !v_g || !w_g) return o.fail(DEM_ERR_ARG, "null gas field");
   if (!o.have_state) return o.fail(DEM_ERR_STATE, "upload particles first");
+  if (g->interp_scheme != DEM_INTERP_GARG && g->interp_scheme != DEM_INTERP_NONE)
+    return o.fail(DEM_ERR_ARG, "unknown interp_scheme");
   o.g = *g;
   o.gas_setup();
   size_t nc = o.vol_surr.size();
@@ -1420,6 +1609,30 @@ int orc_comp_mean_fields(orc_handle* h) {
 int orc_drag_gs_des0(orc_handle* h) {
   if (!h->o.have_gas) return h->o.fail(DEM_ERR_STATE, "no gas fields");
   h->o.drag();
+  return 0;
+}
+int orc_drag_gs_gas0(orc_handle* h, double* f_gds, double* drag_am, double* drag_bm, double* f_gp) {
+  Oracle& o = h->o;
+  if (!o.have_gas) return o.fail(DEM_ERR_STATE, "no gas fields");
+  o.drag_gas();
+  if (f_gds) std::copy(o.f_gds.begin(), o.f_gds.end(), f_gds);
+  if (drag_am) std::copy(o.drag_am.begin(), o.drag_am.end(), drag_am);
+  if (drag_bm) std::copy(o.drag_bm.begin(), o.drag_bm.end(), drag_bm);
+  if (f_gp) std::copy(o.f_gp.begin(), o.f_gp.end(), f_gp);
+  return 0;
+}
+int orc_drag_gs_des1(orc_handle* h) {
+  if (!h->o.have_gas) return h->o.fail(DEM_ERR_STATE, "no gas fields");
+  h->o.drag_des1();
+  return 0;
+}
+int orc_drag_gs_gas1(orc_handle* h, double* f_gds, double* drag_bm, double* f_gp) {
+  Oracle& o = h->o;
+  if (!o.have_gas) return o.fail(DEM_ERR_STATE, "no gas fields");
+  o.drag_gas1();
+  if (f_gds) std::copy(o.f_gds.begin(), o.f_gds.end(), f_gds);
+  if (drag_bm) std::copy(o.drag_bm.begin(), o.drag_bm.end(), drag_bm);
+  if (f_gp) std::copy(o.f_gp.begin(), o.f_gp.end(), f_gp);
   return 0;
 }
 int orc_step_coupled(orc_handle* h, int32_t nn_first, int32_t nsteps) {

@@ -48,6 +48,7 @@ int  orc_download_pairs(orc_handle* h, int32_t* neighbor_index, int32_t* neighbo
 int  orc_upload_pairs(orc_handle* h, const int32_t* neighbor_index, const int32_t* neighbors,
                       const double* pft, int64_t n_pairs, int32_t max_pip);
 int  orc_download_wall_history(orc_handle* h, int32_t* facet_id, double* pft, int32_t max_pip);
+int  orc_upload_wall_history(orc_handle* h, const int32_t* facet_id, const double* pft, int32_t max_pip);
 int  orc_download_cells(orc_handle* h, int32_t* dg_pijk, int32_t max_pip);
 /* facets_at_dg as CSR over 1-based DES cells: start[ncell2+1], ids (1-based) */
 int  orc_download_facet_bins(orc_handle* h, int32_t* start, int32_t* ids, int32_t capacity,
@@ -69,6 +70,10 @@ int  orc_set_gas_fields(orc_handle* h, const dem_fluid_grid* g, const double* ep
 int  orc_get_mean_fields(orc_handle* h, double* ep_g, double* rop_s);
 int  orc_comp_mean_fields(orc_handle* h);
 int  orc_drag_gs_des0(orc_handle* h);
+int  orc_drag_gs_gas0(orc_handle* h, double* f_gds, double* drag_am, double* drag_bm,
+                      double* f_gp);
+int  orc_drag_gs_des1(orc_handle* h);
+int  orc_drag_gs_gas1(orc_handle* h, double* f_gds, double* drag_bm, double* f_gp);
 int  orc_step_coupled(orc_handle* h, int32_t nn_first, int32_t nsteps);
 
 /* Contact constants as CHECK_SOLIDS_DEM_COLL_LSD / _HERTZ derive them
