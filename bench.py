@@ -75,7 +75,10 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms.  Started
+    before the timed region (nvidia-smi needs a moment to report); the
+    samples kept are those from the last one before the region to the first
+    one after it."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -84,8 +87,9 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
 
-    def start(self):
+    def start(self, wait_s=10.0):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -94,23 +98,42 @@ class ClockSampler:
             self.t.start()
         except Exception:
             self.proc = None
+            return
+        end = time.monotonic() + wait_s
+        while not self.lines and time.monotonic() < end:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def begin(self):
+        self.t0 = time.monotonic()
+
+    def end(self):
+        self.t1 = time.monotonic()
 
     def stop(self):
         if self.proc is None:
             return None
+        t1 = self.t1 if self.t1 is not None else time.monotonic()
+        deadline = time.monotonic() + 1.0
+        while time.monotonic() < deadline and not any(t > t1 for t, _ in self.lines):
+            time.sleep(0.02)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        t0 = self.t0 if self.t0 is not None else 0.0
+        before = [i for i, (t, _) in enumerate(self.lines) if t <= t0]
+        after = [i for i, (t, _) in enumerate(self.lines) if t >= t1]
+        lo = before[-1] if before else 0
+        hi = after[0] if after else len(self.lines) - 1
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
+        for _, ln in self.lines[lo:hi + 1]:
+            parts = [q.strip() for q in ln.split(",")]
             if len(parts) < 9:
                 continue
             try:
@@ -124,7 +147,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "timed_s": round(t1 - t0, 4)}
 
 
 def measured_peak():
@@ -223,17 +246,19 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     torch.cuda.synchronize()
     ferr0 = g.force_error() if prec == "split" else None
     clocks = ClockSampler(local)
+    clocks.start()
     p0 = g.pair_count()
     l0 = g.launch_count()
     barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    clocks.begin()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     g.step(args.steps, warm + 1)
     ev1.record(stream)
     torch.cuda.synchronize()
+    clocks.end()
     barrier()
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
@@ -364,12 +389,17 @@ def _batched_run(args, prec, stream, systems, info):
     torch.cuda.synchronize()
     p0 = bt.pair_count()
     l0 = bt.launch_count()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    clocks.begin()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     bt.step(steps)
     ev1.record(stream)
     torch.cuda.synchronize()
+    clocks.end()
+    clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     launches = bt.launch_count() - l0
     p1 = bt.pair_count()
@@ -391,6 +421,7 @@ def _batched_run(args, prec, stream, systems, info):
     bt.close()
     return {"value": n_normal * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps, "warmup": warm,
             "n_normal": n_normal, "pairs": int(p1), "gpu_launches": int(launches), "tuning": tuning,
+            "clocks": clk,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": None,
                          "kernel": "force step over all systems (walls + pairs + gather with fused integration)",

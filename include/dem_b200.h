@@ -262,6 +262,33 @@ int dem_res_read(const char* path, dem_res_info* info, int32_t max_pip, int32_t 
                  int8_t* state, int32_t* phase, int32_t* pair_owner, int32_t* pair_neighbor,
                  double* pft, int64_t pair_cap);
 
+/* ---- particle output (model/des/vtp_mod.f) ------------------------------- */
+
+/* One VTK region of particle data (the VTK_* keywords of a region). */
+typedef struct dem_vtp_options {
+    double  time;               /* TIMESTAMP, written in the header comment */
+    int32_t angular_velocity;   /* VTK_PART_ANGULAR_VEL: also write Angular_velocity */
+    int32_t use_box;            /* 0: the whole domain; 1: the box below */
+    int32_t select_mode;        /* VTK_SELECT_MODE: 'C' centre inside, 'P' entirely inside, 'I' intersects */
+    uint32_t phase_mask;        /* VTK_PART_PHASE: bit m-1 selects phase m; 0 = all phases */
+    double  box_lo[3];          /* VTK_X_W, VTK_Y_S, VTK_Z_B */
+    double  box_hi[3];          /* VTK_X_E, VTK_Y_N, VTK_Z_T */
+    double  reserved[4];
+} dem_vtp_options;
+
+/* WRITE_VTP_FILE for particle data (vtp_mod.f:705-1257): a .vtp PolyData file
+ * with coordinates, Diameter, Velocity (and Angular_velocity) of the NORMAL
+ * particles the region selects, Float32 big-endian appended data as the
+ * reference writes it.  opt may be NULL (whole domain, no spin).
+ * *n_written (may be NULL) receives the number of particles written. */
+int dem_write_vtp(dem_handle* h, const char* path, const dem_vtp_options* opt, int64_t* n_written);
+
+/* The same writer on host arrays in Fortran layout (no device needed);
+ * phase (1-based) may be NULL when phase_mask is 0. */
+int dem_vtp_write(const char* path, const dem_vtp_options* opt, int32_t max_pip, const double* pos,
+                  const double* vel, const double* omega, const double* radius, const int8_t* state,
+                  const int32_t* phase, int64_t* n_written);
+
 /* ---- per-stage entry points (one per reference call site) ----------------- */
 
 /* DESGRID_PIC(.TRUE.) (desgrid_mod.f:877-995): cell of every particle and the

@@ -36,6 +36,7 @@ SOURCES = {
     "batch.cu": ["-fmad=false"],
     "tune.cu": [],
     "res_des.cu": [],
+    "vtp.cu": [],
 }
 HEADERS = ["dem_internal.cuh"]
 

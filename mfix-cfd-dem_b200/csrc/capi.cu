@@ -305,19 +305,19 @@ void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
     p.etanw[k] = q.des_etan_wall[k]; p.etatw[k] = q.des_etat_wall[k];
     p.hkwn[k] = q.hert_kwn[k]; p.hkwt[k] = q.hert_kwt[k];
   }
-  // Search grid for the pair build: cells no narrower than the largest
-  // search diameter 2*FACTOR_RLM*MAX_RADIUS (with a 1 % margin), so a 27-cell
-  // stencil holds every candidate within reach; the reference's own DES-grid
+  // Search grid for the pair build: cells about half the largest search
+  // diameter 2*FACTOR_RLM*MAX_RADIUS wide (1 % margin); each particle scans
+  // the cells within its own reach FACTOR_RLM*(r + MAX_RADIUS), so a small
+  // particle among large ones scans few.  The reference's own DES-grid
   // stencil (reduced to the nearer cells when the DES cells are wider than
-  // that diameter) is applied to the candidates afterwards.  An axis keeps
-  // the DES grid's division when that is not coarser or when a periodic axis
-  // would get fewer than 3 cells.
+  // the search diameter) is applied to the candidates afterwards.  An axis
+  // keeps the DES grid's division when that is not coarser.
   const int dgn[3] = {q.dg_imax, q.dg_jmax, q.no_k ? 1 : q.dg_kmax};
-  const double target = 2.0 * q.factor_rlm * q.max_radius * 1.01;
+  const double target = q.factor_rlm * q.max_radius * 1.01;
   for (int a = 0; a < 3; ++a) {
     const double len = (double)dgn[a] / p.dg_inv[a];
     int nfa = (int)std::floor(len / target);
-    if (nfa <= dgn[a] || (p.per[a] && nfa < 3) || (a == 2 && q.no_k)) nfa = dgn[a];
+    if (nfa <= dgn[a] || (a == 2 && q.no_k)) nfa = dgn[a];
     if (nfa < 1) nfa = 1;
     p.fn[a] = nfa;
     // same division as the DES grid -> the same inverse width, bit for bit
@@ -419,6 +419,7 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
   A((void**)&h->wall_hit, n);
   A((void**)&h->wall_cand, n);
   A((void**)&h->wall_list, sizeof(int) * (size_t)n);
+  A((void**)&h->wgap, sizeof(float) * (size_t)n);
   A((void**)&h->d_nwall, sizeof(int));
   A((void**)&h->skin, sizeof(double));
   A((void**)&h->vslot, sizeof(unsigned) * 32);
@@ -488,7 +489,7 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->skin, h->vslot, h->pgap,
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->skin, h->vslot, h->pgap,
                   h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);

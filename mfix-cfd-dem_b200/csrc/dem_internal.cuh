@@ -248,6 +248,7 @@ struct dem_handle {
   uint8_t* wall_live = nullptr; // [i] 1 when some wall slot may be in use
   uint8_t* wall_cand = nullptr; // [i] 1 when the particle's DES cell holds facets
   int* wall_list = nullptr;     // this step's particles with wall work (arbitrary order)
+  float* wgap = nullptr;        // [i] clearance from the facets of its DES cell at the last build
   int* d_nwall = nullptr;       // their count
   double* wf = nullptr;       // [i][6] wall force and torque of the last force pass (valid with wall_hit)
 
@@ -305,6 +306,7 @@ void set_hist_flags(dem_handle* h);            // neighbor.cu: PF_HIST from the 
 void launch_pair_gaps(dem_handle* h);          // neighbor.cu: pair gaps at a build, displacement bound 0
 void launch_skin(dem_handle* h);               // force.cu: adds the step's displacement to the bound
 void skin_unknown(dem_handle* h);              // force.cu: positions changed from outside: no pair skipped
+void launch_wall_gaps(dem_handle* h);          // force.cu: wall clearances at a build (with the pair gaps)
 void launch_wall_cand(dem_handle* h);          // desgrid.cu: facet-cell flag of every particle
 void launch_pairs_only(dem_handle* h);         // force.cu: pair kernel of the handle's precision
 void launch_gather_only(dem_handle* h);        // force.cu: gather kernel, forces into FC/TOW

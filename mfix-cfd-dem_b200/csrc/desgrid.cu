@@ -81,6 +81,7 @@ void launch_wall_cand(dem_handle* h) {
   else
     k_wall_cand<false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), h->state, h->dg_pijk, h->fbin_start, h->wall_cand);
   DEM_LAUNCH(h);
+  skin_unknown(h);  // the walls changed: no particle is known clear of them until the next build
 }
 
 // Search-grid cell of every existing particle (for the pair build), as an

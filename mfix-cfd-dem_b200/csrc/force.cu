@@ -23,6 +23,7 @@
 #include "dem_internal.cuh"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 
 namespace demb {
@@ -337,30 +338,111 @@ __device__ void wall_contacts(const DevParams& p, const WallCtx& w, int me, PSta
 }
 
 // ---------------------------------------------------------------------------
+// Squared distance from x to the closest point of triangle (a, b, c): the
+// Voronoi-region walk over vertices, edges and face (C. Ericson, Real-Time
+// Collision Detection, 2005, section 5.1.5), with no edge or vertex left out.
+__device__ __forceinline__ double tri_dist2(const double* __restrict__ V, const double x[3]) {
+  double a[3], ab[3], ac[3], ap[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) { a[k] = V[k]; ab[k] = V[3 + k] - a[k]; ac[k] = V[6 + k] - a[k]; ap[k] = x[k] - a[k]; }
+  const double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  double q[3];
+  auto at = [&](double u, double v) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) q[k] = a[k] + u * ab[k] + v * ac[k];
+  };
+  if (d1 <= 0.0 && d2 <= 0.0) { at(0.0, 0.0); goto done; }
+  {
+    double bp[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) bp[k] = ap[k] - ab[k];
+    const double d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3) { at(1.0, 0.0); goto done; }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) { at(d1 / (d1 - d3), 0.0); goto done; }
+    double cp[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cp[k] = ap[k] - ac[k];
+    const double d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) { at(0.0, 1.0); goto done; }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) { at(0.0, d2 / (d2 - d6)); goto done; }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+      const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+      at(1.0 - w, w);
+      goto done;
+    }
+    const double den = 1.0 / (va + vb + vc);
+    at(vb * den, vc * den);
+  }
+done:
+  double d[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) d[k] = x[k] - q[k];
+  return dot3(d, d);
+}
+
+// Clearance of every NORMAL particle in a DES cell with facets from those
+// facets at a build: min over the cell's facets of |x - closest point| - r,
+// less a margin of 1e-6 r for the rounding of the closest point, rounded
+// down to float.  A particle whose clearance exceeds the displacement bound
+// since the build touches none of them (the reference's contact test is
+// |x - c|^2 < r^2 - SMALL_NUMBER), so with no history it has no wall work.
+template <bool B>
+__global__ void k_wall_gaps(DevParams p0, BatchView bv, WallCtx w, const double4* __restrict__ pos4,
+                            const int8_t* __restrict__ state, const uint8_t* __restrict__ wall_cand,
+                            float* __restrict__ wgap) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p0.n) return;
+  if (state[i] != DEM_STATE_NORMAL || !wall_cand[i]) { wgap[i] = FLT_MAX; return; }
+  const DevParams& p = sysp<B>(p0, bv, i);
+  const int cell = p.cell_off + w.dg_pijk[i] - 1;
+  const double4 a = pos4[i];
+  const double x[3] = {a.x, a.y, a.z};
+  double dmin2 = HUGE_VAL;
+  for (int q = w.fbin_start[cell]; q < w.fbin_start[cell + 1]; ++q)
+    dmin2 = fmin(dmin2, tri_dist2(w.vertex + 9 * (size_t)w.fbin[q].id, x));
+  wgap[i] = __double2float_rd(sqrt(dmin2) - a.w - 1e-6 * a.w);
+}
+
 // The particles with wall work this step: NORMAL particles whose DES cell
-// holds facets, and NORMAL particles elsewhere whose history slots may be in
-// use (k_walls clears them).  Each block of WALL_LIST_T threads appends its
-// particles in index order with one atomic; blocks land in arbitrary order,
-// which does not matter: each particle's wall terms depend on it alone.
+// holds facets and whose clearance at the last build does not exceed the
+// displacement bound since, and NORMAL particles whose history slots may be
+// in use (k_walls clears them, or updates them).  Each block of WALL_LIST_T
+// threads appends its particles in index order with one atomic; blocks land
+// in arbitrary order, which does not matter: each particle's wall terms
+// depend on it alone.
 constexpr int WALL_LIST_T = 1024;
+static_assert(WALL_LIST_T == 32 * 32, "one warp scans the warp counts");
 __global__ void __launch_bounds__(WALL_LIST_T)
 k_wall_list(int n, const int8_t* __restrict__ state, const uint8_t* __restrict__ wall_cand,
-            const uint8_t* __restrict__ wall_live, int* __restrict__ list, int* __restrict__ count) {
+            const uint8_t* __restrict__ wall_live, const float* __restrict__ wgap, const double* __restrict__ skin,
+            int* __restrict__ list, int* __restrict__ count) {
   __shared__ int warp_n[WALL_LIST_T / 32];
-  __shared__ int block_base;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool need = i < n && state[i] == DEM_STATE_NORMAL && (wall_cand[i] | wall_live[i]);
+  const double bound = *skin;
+  const bool need = i < n && state[i] == DEM_STATE_NORMAL &&
+                    (wall_live[i] || (wall_cand[i] && !((double)wgap[i] > bound)));
   const unsigned m = __ballot_sync(0xffffffffu, need);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) warp_n[warp] = __popc(m);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int tot = 0;
-    for (int k = 0; k < WALL_LIST_T / 32; ++k) { const int c = warp_n[k]; warp_n[k] = tot; tot += c; }
-    block_base = tot ? atomicAdd(count, tot) : 0;
+  if (warp == 0) {  // the warps' offsets: a scan of their counts, and one atomic
+    const int c = warp_n[lane];
+    int incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    int base = 0;
+    if (lane == 0 && tot) base = atomicAdd(count, tot);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    warp_n[lane] = base + incl - c;
   }
   __syncthreads();
-  if (need) list[block_base + warp_n[warp] + __popc(m & ((1u << lane) - 1u))] = i;
+  if (need) list[warp_n[warp] + __popc(m & ((1u << lane) - 1u))] = i;
 }
 
 // Kernel 1 (per listed particle): wall contacts of NORMAL particles whose DES
@@ -435,7 +517,7 @@ k_walls(DevParams p0, BatchView bv, WallCtx w, const int* __restrict__ wlist, co
 // The contact terms go to a record that both particles read back in
 // kernel 3, and both particles of a contact are marked in `touched`.
 template <int COLL, bool B>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner,
         const int* __restrict__ nbrs, const double4* __restrict__ pos4, const double4* __restrict__ vel4,
         const double4* __restrict__ omg4, const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
@@ -604,7 +686,7 @@ __device__ __forceinline__ void add_own(const DevParams& p, int rs, int re, cons
 // stores them (MODE 0) or integrates them in place of CFNEWVALUES
 // (MODE 1 = Euler, MODE 2 = Adams-Bashforth).
 template <int MODE, bool B>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
          const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
          double4* __restrict__ omg_n, const int8_t* __restrict__ state, const double* __restrict__ wf,
@@ -681,7 +763,7 @@ static void launch_walls_t(dem_handle* h) {
   const int T = 128;
   cudaMemsetAsync(h->d_nwall, 0, sizeof(int), h->stream);
   k_wall_list<<<(h->n + WALL_LIST_T - 1) / WALL_LIST_T, WALL_LIST_T, 0, h->stream>>>(
-      h->n, h->state, h->wall_cand, h->wall_live, h->wall_list, h->d_nwall);
+      h->n, h->state, h->wall_cand, h->wall_live, h->wgap, h->skin, h->wall_list, h->d_nwall);
   // persistent: the resident blocks of the kernel's register budget
   k_walls<COLL, B><<<h->n_sm * 4, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->wall_list, h->d_nwall,
                                                      h->pos4[c], h->vel4[c], h->omg4[c], h->phase, h->wall_live,
@@ -707,6 +789,18 @@ static void launch_gather_t(dem_handle* h) {
                                             h->vel4[1 - c], h->omg4[1 - c], h->state, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
                                             h->touched, h->wall_hit, h->prec, h->fc, h->tow, h->acc_old,
                                             h->rot_acc_old, h->vslot);
+  DEM_LAUNCH(h);
+}
+
+void launch_wall_gaps(dem_handle* h) {
+  if (h->nf <= 0) return;
+  const int T = 256, G = (h->n + T - 1) / T;
+  if (h->batch())
+    k_wall_gaps<true><<<G, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->pos4[h->cur], h->state,
+                                              h->wall_cand, h->wgap);
+  else
+    k_wall_gaps<false><<<G, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->pos4[h->cur], h->state,
+                                               h->wall_cand, h->wgap);
   DEM_LAUNCH(h);
 }
 

@@ -37,7 +37,7 @@ struct Comp3 {  // Neumaier-compensated FP32 sum of a 3-vector
 };
 
 template <int COLL, bool B>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner, const int* __restrict__ nbrs,
               const double4* __restrict__ pos4, const double4* __restrict__ vel4,
               const double4* __restrict__ omg4, const int8_t* __restrict__ state,

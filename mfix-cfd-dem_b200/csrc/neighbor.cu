@@ -156,26 +156,43 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
         if (off >= 0.5) lo_off[ax] = 0; else hi_off[ax] = 0;
       }
     }
-    const int key = me.w - p.fcell_off;
-    const int fk = key / p.fc2, fi = (key % p.fc2) / p.fc1, fj = key % p.fc1;
-    const int kr = p.no_k ? 0 : 1;
-    for (int dk = -kr; dk <= kr; ++dk)
-    for (int dj = -1; dj <= 1; ++dj)
-    for (int di = -1; di <= 1; ++di) {
-      int g[3] = {fi + di, fj + dj, fk + dk};
-      bool skip = false;
-      for (int ax = 0; ax < 3; ++ax) {
-        if (ax == 2 && p.no_k) break;
-        if (p.per[ax]) {
-          if (g[ax] < 1) g[ax] += p.fn[ax];
-          else if (g[ax] > p.fn[ax]) g[ax] -= p.fn[ax];
-        } else if (g[ax] < 0 || g[ax] > p.fn[ax] + 1) {
-          skip = true;
-        }
+    // the search cells within reach FACTOR_RLM*(r + MAX_RADIUS) of the
+    // particle, each once: per axis a range of cells, wrapped on a periodic
+    // axis (the whole axis when the range covers it); along y (the fastest
+    // key) the cells of a range are contiguous, so each (i, k) column of the
+    // range is at most two runs of the cell-sorted copy
+    const double reach = fr * (cp.w + mr);
+    int glo[3] = {0, 0, 0}, ghi[3] = {0, 0, 0};
+    for (int ax = 0; ax < 3; ++ax) {
+      if (ax == 2 && p.no_k) break;
+      // (a margin of 1e-4 of the reach covers the rounding of the cell index)
+      const double t = (cpos[ax] - p.dg_start[ax]) * p.f_inv[ax], w = reach * p.f_inv[ax] * 1.0001;
+      int lo = (int)floor(t - w) + 1, hi = (int)floor(t + w) + 1;
+      if (p.per[ax]) {
+        if (hi - lo + 1 >= p.fn[ax]) { lo = 1; hi = p.fn[ax]; }
+      } else {
+        lo = max(lo, 0);
+        hi = min(hi, p.fn[ax] + 1);
       }
-      if (skip) continue;
-      const int cell = p.fcell_off + g[2] * p.fc2 + g[0] * p.fc1 + g[1];
-      const int qs = fstart[cell], qe = fstart[cell + 1];
+      glo[ax] = lo;
+      ghi[ax] = hi;
+    }
+    auto wrap = [&](int g, int ax) {
+      if (!p.per[ax] || (ax == 2 && p.no_k)) return g;
+      return g < 1 ? g + p.fn[ax] : (g > p.fn[ax] ? g - p.fn[ax] : g);
+    };
+    for (int gk = glo[2]; gk <= ghi[2]; ++gk)
+    for (int gi = glo[0]; gi <= ghi[0]; ++gi) {
+      const int col = p.fcell_off + wrap(gk, 2) * p.fc2 + wrap(gi, 0) * p.fc1;
+      int run_lo[2], run_hi[2], nrun = 1;
+      run_lo[0] = glo[1]; run_hi[0] = ghi[1];
+      if (p.per[1] && glo[1] < 1) {
+        run_lo[0] = glo[1] + p.fn[1]; run_hi[0] = p.fn[1]; run_lo[1] = 1; run_hi[1] = ghi[1]; nrun = 2;
+      } else if (p.per[1] && ghi[1] > p.fn[1]) {
+        run_lo[0] = glo[1]; run_hi[0] = p.fn[1]; run_lo[1] = 1; run_hi[1] = ghi[1] - p.fn[1]; nrun = 2;
+      }
+      for (int rr = 0; rr < nrun; ++rr) {
+      const int qs = fstart[col + run_lo[rr]], qe = fstart[col + run_hi[rr] + 1];
       for (int q = qs; q < qe; ++q) {
         const int4 o = sinfo[q];
         const int nb = o.x;
@@ -236,6 +253,7 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
           }
         }
         ++cnt;
+      }
       }
     }
   }
@@ -534,6 +552,7 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   h->pcur = pn;
   h->have_pairs = true;
   launch_pair_gaps(h);
+  launch_wall_gaps(h);
   return build_transpose(h, nb);
 }
 

@@ -195,6 +195,19 @@ class DemResInfo(C.Structure):
     ]
 
 
+class DemVtpOptions(C.Structure):
+    _fields_ = [
+        ("time", C.c_double),
+        ("angular_velocity", C.c_int32),
+        ("use_box", C.c_int32),
+        ("select_mode", C.c_int32),
+        ("phase_mask", C.c_uint32),
+        ("box_lo", C.c_double * 3),
+        ("box_hi", C.c_double * 3),
+        ("reserved", C.c_double * 4),
+    ]
+
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -257,6 +270,10 @@ DEM_ONLY = {
     "sys_download_state": (C.c_int, [_P, C.c_int32, _D, _D, _D, _I8, C.c_int32]),
     "sys_start": (C.c_int, [_P, _I32, C.c_int32]),
     "batch_step": (C.c_int, [_P, C.c_int32]),
+    # particle output
+    "write_vtp": (C.c_int, [_P, C.c_char_p, C.POINTER(DemVtpOptions), C.POINTER(C.c_int64)]),
+    "vtp_write": (C.c_int, [C.c_char_p, C.POINTER(DemVtpOptions), C.c_int32, _D, _D, _D, _D, _I8, _I32,
+                            C.POINTER(C.c_int64)]),
     # restart files
     "write_res0_des": (C.c_int, [_P, C.c_char_p, C.POINTER(DemResInfo)]),
     "read_res0_des": (C.c_int, [_P, C.c_char_p, C.c_int32, C.POINTER(DemResInfo)]),
@@ -282,3 +299,18 @@ def bind(lib, prefix, extra=None):
         fn.restype = res
         fn.argtypes = args
     return lib
+
+
+def vtp_options(time=0.0, angular_velocity=False, box=None, select_mode="C", phases=None) -> DemVtpOptions:
+    """A dem_vtp_options for one VTK region of particle data."""
+    o = DemVtpOptions()
+    o.time = float(time)
+    o.angular_velocity = 1 if angular_velocity else 0
+    o.select_mode = ord(select_mode)
+    if box is not None:
+        o.use_box = 1
+        for c in range(3):
+            o.box_lo[c], o.box_hi[c] = float(box[0][c]), float(box[1][c])
+    if phases:
+        o.phase_mask = sum(1 << (int(m) - 1) for m in phases)
+    return o

@@ -261,6 +261,14 @@ class DemSystem:
         self.nn = first + nsteps - 1
 
     # ---- CUDA-only ---------------------------------------------------
+    def write_vtp(self, path, time=0.0, angular_velocity=False, box=None, select_mode="C", phases=None) -> int:
+        """WRITE_VTP_FILE for particle data; box = (lo, hi) of the VTK
+        region, phases = 1-based phases to keep.  Returns the particle count."""
+        o = abi.vtp_options(time, angular_velocity, box, select_mode, phases)
+        n = C.c_int64()
+        self._call("write_vtp", self._h, str(path).encode(), C.byref(o), C.byref(n))
+        return int(n.value)
+
     def write_res0_des(self, path, ro_sol, vtp_findex=0, tecplot_findex=0, dtsolid=None):
         """WRITE_RES0_DES: the DEM restart file of this system.  ro_sol is
         RO_SOL per phase (the density the particles were generated with)."""
