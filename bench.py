@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=25)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision leg")
+    ap.add_argument("--serve-graphs", type=int, default=0,
+                    help="served leg: replay aligned periods as CUDA graphs (1) or step launch by launch (0)")
     ap.add_argument("--batch-systems", type=int, default=256, help="systems of the batched leg (0 = skip)")
     ap.add_argument("--batch-total", type=int, default=6_000_000, help="particles of the batched leg")
     ap.add_argument("--serve-rates", default="5,20,50", help="request rates (1/s) of the served leg ('' = skip)")
@@ -470,7 +472,7 @@ def run_served(args):
         reqs = configs.hopper_requests(args.serve_requests, rate, seed=configs.SEED_BASE + 4 + 100 * k,
                                        steps=args.serve_steps)
         srv = DemServer(load_library(), build, template, hbm_budget_bytes=int(args.serve_budget_gb * 1e9),
-                        max_systems=64)
+                        max_systems=64, graphs=bool(args.serve_graphs))
         res = srv.run(reqs)
         srv.close()
         out.append({"rate_per_s": rate, "requests": len(reqs), "p50_s": res["p50_s"], "p99_s": res["p99_s"],
@@ -553,8 +555,10 @@ def run_ours(args):
                 "ms_per_step": b["split"]["ms_per_step"], "steps": b["split"]["steps"],
                 "warmup": b["split"]["warmup"], "roofline": b["split"]["roofline"],
                 "tuning": b["split"]["tuning"], "gpu_launches": b["split"]["gpu_launches"],
+                "clocks": b["split"]["clocks"],
                 "fp64": {"value": b["fp64"]["value"], "ms_per_step": b["fp64"]["ms_per_step"],
-                         "roofline": b["fp64"]["roofline"], "tuning": b["fp64"]["tuning"]},
+                         "roofline": b["fp64"]["roofline"], "tuning": b["fp64"]["tuning"],
+                         "clocks": b["fp64"]["clocks"]},
                 "speedup_split_vs_fp64_batched": b["split"]["value"] / b["fp64"]["value"],
                 "speedup_vs_plain_fp64_single": b["split"]["value"] / main["value"],
                 "trajectory_rel_err_vs_fp64": b["trajectory_rel_err"],

@@ -128,7 +128,8 @@ typedef struct dem_stats {
     double  max_overlap_ratio; /* max overlap / R_LM over contacts */
     double  bed_height;      /* mass-weighted mean y of NORMAL particles */
     double  s_time;          /* accumulated solids time S_TIME */
-    double  reserved[4];
+    int64_t n_outflow_removed; /* particles deleted by outflow boundaries so far */
+    double  reserved[3];
 } dem_stats;
 
 typedef struct dem_handle dem_handle;
@@ -261,6 +262,37 @@ int dem_res_read(const char* path, dem_res_info* info, int32_t max_pip, int32_t 
                  double* pos, double* vel, double* omega, double* radius, double* ro_sol,
                  int8_t* state, int32_t* phase, int32_t* pair_owner, int32_t* pair_neighbor,
                  double* pft, int64_t pair_cap);
+
+/* ---- outflow boundaries (model/des/mass_outflow_dem.f) ------------------- */
+
+/* One DEM outflow boundary (an entry of DEM_BCMO_MAP).  The DES cells it
+ * watches are the box dg_lo..dg_hi (DES-grid indices as DG_FUNIJK takes
+ * them: I_w..I_e, J_s..J_n, K_b..K_t of SET_BC_DEM_MO, set_bc_dem_mo.f:
+ * 79-101, from IofBCPOS of the BC extents); a particle belongs to it when its
+ * DES cell of the last DESGRID_PIC is in the box (DG_PIC).  `face` is the
+ * plane the distance is measured from: YN(BC_J_s-1) for 'S', YN(BC_J_s) for
+ * 'N', XE(BC_I_w-1) for 'W', XE(BC_I_w) for 'E', ZT(BC_K_b-1) for 'B',
+ * ZT(BC_K_b) for 'T' (mass_outflow_dem.f:96-103). */
+typedef struct dem_outflow_bc {
+    int32_t plane;             /* BC_PLANE: 'N','S','E','W','T','B' */
+    int32_t mass_outflow;      /* 1: BC_TYPE MASS_OUTFLOW (exiting particles take vel); 0: P_/OUTFLOW */
+    int32_t dg_lo[3], dg_hi[3];
+    int32_t reserved_i[4];
+    double  face;
+    double  vel[DEM_MAX_PHASES][3];   /* BC_U_s, BC_V_s, BC_W_s of each phase (MASS_OUTFLOW) */
+    double  reserved_d[4];
+} dem_outflow_bc;
+
+/* Installs the outflow boundaries (n = 0 removes them).  Each DES_TIME_STEP
+ * then runs UPDATE_EXIT_DES_VEL before CFNEWVALUES (des_time_march.f:
+ * 372-375; FREEZE_EXIT_DES_VEL = .FALSE.) and MASS_OUTFLOW_DEM after it
+ * (des_time_march.f:405): particles clear of the plane by more than their
+ * radius become NORMAL, straddling ones EXITING (velocity frozen to the
+ * normal component while moving out, or set to the boundary's for
+ * MASS_OUTFLOW), and those past it are deleted, which forces the neighbour
+ * search of that step.  Steps are then taken one at a time (no CUDA graph).
+ * The boxes of the boundaries must not overlap. */
+int dem_set_outflow_bcs(dem_handle* h, const dem_outflow_bc* bcs, int32_t n);
 
 /* ---- particle output (model/des/vtp_mod.f) ------------------------------- */
 

@@ -37,6 +37,7 @@ SOURCES = {
     "tune.cu": [],
     "res_des.cu": [],
     "vtp.cu": [],
+    "outflow.cu": ["-fmad=false"],
 }
 HEADERS = ["dem_internal.cuh"]
 

@@ -412,23 +412,24 @@ static int batch_step_once(dem_handle* h, std::vector<uint8_t>& last_due) {
   return 0;
 }
 
-// A whole NEIGHBOR_SEARCH_N period of a batch whose running systems are in
-// step (same NEIGHBOR_SEARCH_N, NN = m*N + 1 with m >= 1, past the first
-// Adams-Bashforth step) is the same sequence every time: N force passes with
-// the periodic rebinning, the rebuild of all of them after the last.  It is
-// captured once per combination of buffer parities and replayed; the two
-// rebuild masks it uses (idle steps, rebuild step) stay in device memory.
+// A whole NEIGHBOR_SEARCH_N period of a batch whose running systems are all
+// at a period boundary (same NEIGHBOR_SEARCH_N, each at its own NN = m*N + 1
+// with m >= 1, past the first Adams-Bashforth step) is the same sequence
+// every time: N force passes with the periodic rebinning, the rebuild of all
+// of them after the last -- the systems' own step counts do not enter it.
+// It is captured once per combination of buffer parities and replayed; the
+// two rebuild masks it uses (idle steps, rebuild step) stay in device memory.
 static bool period_aligned(const dem_handle* h, int* nsn) {
-  int N = -1, nn = -1;
+  int N = -1;
   bool any = false;
   for (const SysSlot& S : h->sys) {
     if (!S.live) continue;
     if (!S.started || S.first_pass) return false;
-    if (N < 0) { N = S.prm.neighbor_search_n; nn = S.nn; }
-    if (S.prm.neighbor_search_n != N || S.nn != nn) return false;
+    if (N < 0) N = S.prm.neighbor_search_n;
+    if (S.prm.neighbor_search_n != N || S.nn <= 1 || (S.nn - 1) % N != 0) return false;
     any = true;
   }
-  if (!any || nn <= 1 || (nn - 1) % N != 0) return false;
+  if (!any) return false;
   *nsn = N;
   return true;
 }

@@ -489,7 +489,7 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->skin, h->vslot, h->pgap,
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->skin, h->vslot, h->pgap,
                   h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -716,8 +716,16 @@ static int step_once(dem_handle* h, int nn) {
   const DevParams& p = h->dp;
   const bool anyper = p.per[0] || p.per[1] || (p.per[2] && !p.no_k);
   cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
-  if (int rc = run_force(h, true)) return rc;
-  const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0);
+  bool force = false;
+  if (h->obc.empty()) {
+    if (int rc = run_force(h, true)) return rc;
+  } else {
+    // outflow boundaries: forces, then exit velocities + CFNEWVALUES +
+    // MASS_OUTFLOW_DEM, whose deletions force the neighbour search
+    if (int rc = run_force(h, false)) return rc;
+    if (int rc = run_cfnewvalues_outflow(h, &force)) return rc;
+  }
+  const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0) || force;
   if (do_nsearch || anyper) {
     if (int rc = run_desgrid_pic(h, do_nsearch)) return rc;
   }
@@ -793,7 +801,7 @@ int dem_step(dem_handle* h, int32_t nn_first, int32_t nsteps) {
   if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
   if (nsteps < 0 || nn_first < 1) return set_err(h, DEM_ERR_ARG, "bad step range");
   const int nsn = h->prm.neighbor_search_n;
-  const bool graphs_ok = h->stream != nullptr && !h->prof && !h->no_graphs;
+  const bool graphs_ok = h->stream != nullptr && !h->prof && !h->no_graphs && h->obc.empty();
   int k = 0;
   while (k < nsteps) {
     const int nn = nn_first + k;
@@ -826,6 +834,7 @@ int dem_get_stats(dem_handle* h, dem_stats* s) {
   s->n_contacts = (int64_t)h->herr->n_contacts;
   s->n_wall_contacts = (int64_t)h->herr->n_wall_contacts;
   s->n_rogue_removed = (int64_t)h->herr->rogue_removed;
+  s->n_outflow_removed = (int64_t)h->herr->outflow_removed;
   s->steps_done = h->steps_done;
   s->s_time = h->s_time;
   return 0;

@@ -753,8 +753,13 @@ int dem_step_coupled(dem_handle* h, int32_t nn_first, int32_t nsteps) {
     cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
     if (int rc = run_force(h, false)) return rc;              // CALC_FORCE_DEM
     if (int rc = run_calc_drag(h)) return rc;                 // CALC_DRAG_DES
-    if (int rc = run_cfnewvalues(h)) return rc;               // CFUPDATEOLD + CFNEWVALUES
-    const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0);
+    bool force = false;
+    if (h->obc.empty()) {
+      if (int rc = run_cfnewvalues(h)) return rc;             // CFUPDATEOLD + CFNEWVALUES
+    } else if (int rc = run_cfnewvalues_outflow(h, &force)) { // + exit velocities, MASS_OUTFLOW_DEM
+      return rc;
+    }
+    const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0) || force;
     if (do_nsearch || anyper) {
       if (int rc = run_desgrid_pic(h, do_nsearch)) return rc;
     }

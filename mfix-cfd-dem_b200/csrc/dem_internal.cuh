@@ -52,6 +52,7 @@ struct DevErr {
   unsigned long long n_contacts;
   unsigned long long n_wall_contacts;
   unsigned long long rogue_removed;
+  unsigned long long outflow_removed;
   int pad[2];
 };
 
@@ -249,6 +250,11 @@ struct dem_handle {
   uint8_t* wall_cand = nullptr; // [i] 1 when the particle's DES cell holds facets
   int* wall_list = nullptr;     // this step's particles with wall work (arbitrary order)
   float* wgap = nullptr;        // [i] clearance from the facets of its DES cell at the last build
+  // outflow boundaries (single handles): host copy, device copy, the
+  // FIRST_PASS of UPDATE_EXIT_DES_VEL
+  std::vector<dem_outflow_bc> obc;
+  dem_outflow_bc* d_obc = nullptr;
+  bool exit_first_pass = true;
   int* d_nwall = nullptr;       // their count
   double* wf = nullptr;       // [i][6] wall force and torque of the last force pass (valid with wall_hit)
 
@@ -307,6 +313,7 @@ void launch_pair_gaps(dem_handle* h);          // neighbor.cu: pair gaps at a bu
 void launch_skin(dem_handle* h);               // force.cu: adds the step's displacement to the bound
 void skin_unknown(dem_handle* h);              // force.cu: positions changed from outside: no pair skipped
 void launch_wall_gaps(dem_handle* h);          // force.cu: wall clearances at a build (with the pair gaps)
+int run_cfnewvalues_outflow(dem_handle* h, bool* force_nsearch);  // outflow.cu: exit velocities, CFNEWVALUES, MASS_OUTFLOW_DEM
 void launch_wall_cand(dem_handle* h);          // desgrid.cu: facet-cell flag of every particle
 void launch_pairs_only(dem_handle* h);         // force.cu: pair kernel of the handle's precision
 void launch_gather_only(dem_handle* h);        // force.cu: gather kernel, forces into FC/TOW

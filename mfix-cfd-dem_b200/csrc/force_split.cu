@@ -51,10 +51,32 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
   unsigned long long ncont = 0;
   unsigned eflags = 0;
   const double reach = 2.0 * skin[0];
-  for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
-    const uint8_t f0 = pflag[cc];
+  // four consecutive pairs per iteration (see k_pairs in force.cu)
+  const long long ng = (np + 3) / 4;
+  for (long long g4 = (long long)blockIdx.x * blockDim.x + threadIdx.x; g4 < ng; g4 += stride) {
+    const long long c0 = 4 * g4;
+    uint32_t fw = 0;  // the four flags, one per byte
+    float4 gq = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c0 + 3 < np) {
+      fw = *reinterpret_cast<const uint32_t*>(pflag + c0);
+      gq = *reinterpret_cast<const float4*>(pgap + c0);
+    } else {
+      if (c0 < np) { fw |= pflag[c0]; gq.x = pgap[c0]; }
+      if (c0 + 1 < np) { fw |= (uint32_t)pflag[c0 + 1] << 8; gq.y = pgap[c0 + 1]; }
+      if (c0 + 2 < np) { fw |= (uint32_t)pflag[c0 + 2] << 16; gq.z = pgap[c0 + 2]; }
+    }
+    // bit j: pair c0+j is provably apart
+    const unsigned apart = ((!(fw & PF_HIST) && (double)gq.x > reach) ? 1u : 0u) |
+                           ((!((fw >> 8) & PF_HIST) && (double)gq.y > reach) ? 2u : 0u) |
+                           ((!((fw >> 16) & PF_HIST) && (double)gq.z > reach) ? 4u : 0u) |
+                           ((!((fw >> 24) & PF_HIST) && (double)gq.w > reach) ? 8u : 0u);
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+    const long long cc = c0 + j;
+    if (cc >= np) break;
+    const uint8_t f0 = (uint8_t)(fw >> (8 * j));
     // provably apart (see k_pairs in force.cu)
-    if (!(f0 & PF_HIST) && (double)pgap[cc] > reach) {
+    if ((apart >> j) & 1u) {
       if (f0) pflag[cc] = 0;
       continue;
     }
@@ -163,6 +185,7 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
       }
     }
     if (f != f0) pflag[cc] = f;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     ncont += __shfl_down_sync(0xffffffffu, ncont, o);

@@ -108,6 +108,150 @@ __global__ void k_sorted_copy(DevParams p0, BatchView bv, int n, const int* __re
   sinfo[q] = make_int4(i, pack_ijk(dg_iof(p, c), dg_jof(p, c), dg_kof(p, c)), (int)state[i], fkey[i]);
 }
 
+// The scanning particle's frame for the candidate test.
+struct NeighFrame {
+  int cur;
+  int rc[3], s1[3], e1[3], ncl[3], lo_off[3], hi_off[3];
+  double4 cp;
+  double fr;
+  int glo[3], ghi[3];  // search cells within reach, per axis
+  double inv_l[3];     // 1 / period length of the periodic axes
+};
+
+template <bool B>
+__device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, const double4& cp, NeighFrame& F) {
+  F.cur = me.x;
+  F.cp = cp;
+  F.fr = p.factor_rlm;
+  unpack_ijk(me.y, F.rc[0], F.rc[1], F.rc[2]);
+  F.s1[0] = p.istart1; F.s1[1] = p.jstart1; F.s1[2] = p.kstart1;
+  F.e1[0] = p.iend1; F.e1[1] = p.jend1; F.e1[2] = p.kend1;
+  F.ncl[0] = p.iend1 - p.istart1 + 1; F.ncl[1] = p.jend1 - p.jstart1 + 1; F.ncl[2] = p.kend1 - p.kstart1 + 1;
+  for (int ax = 0; ax < 3; ++ax) F.inv_l[ax] = (p.per[ax] && !(ax == 2 && p.no_k)) ? 1.0 / p.L[ax] : 0.0;
+  const double cpos[3] = {cp.x, cp.y, cp.z};
+  const double mr = p.max_radius;
+  for (int ax = 0; ax < 3; ++ax) {
+    F.lo_off[ax] = 1; F.hi_off[ax] = 1;
+    if (ax == 2 && p.no_k) { F.lo_off[2] = 0; F.hi_off[2] = 0; continue; }
+    // the reference's stencil is the nearer 2 cells when the DES cells are
+    // wider than the search diameter (desgrid_mod.f:1116-1152)
+    const bool coarse = 1.0 > 2.0 * mr * F.fr * p.dg_inv[ax];
+    if (coarse) {
+      const double t = (cpos[ax] - p.dg_start[ax]) * p.dg_inv[ax];
+      const double off = t - (double)(long long)floor(t);
+      if (off >= 0.5) F.lo_off[ax] = 0; else F.hi_off[ax] = 0;
+    }
+  }
+  // the search cells within reach FACTOR_RLM*(r + MAX_RADIUS) of the
+  // particle, each once: per axis a range of cells, wrapped on a periodic
+  // axis (the whole axis when the range covers it); a margin of 1e-4 of the
+  // reach covers the rounding of the cell index
+  const double reach = F.fr * (cp.w + mr);
+  for (int ax = 0; ax < 3; ++ax) {
+    F.glo[ax] = 0; F.ghi[ax] = 0;
+    if (ax == 2 && p.no_k) continue;
+    const double t = (cpos[ax] - p.dg_start[ax]) * p.f_inv[ax], w = reach * p.f_inv[ax] * 1.0001;
+    int lo = (int)floor(t - w) + 1, hi = (int)floor(t + w) + 1;
+    if (p.per[ax]) {
+      if (hi - lo + 1 >= p.fn[ax]) { lo = 1; hi = p.fn[ax]; }
+    } else {
+      lo = max(lo, 0);
+      hi = min(hi, p.fn[ax] + 1);
+    }
+    F.glo[ax] = lo;
+    F.ghi[ax] = hi;
+  }
+}
+
+__device__ __forceinline__ int search_wrap(const DevParams& p, int g, int ax) {
+  if (!p.per[ax] || (ax == 2 && p.no_k)) return g;
+  return g < 1 ? g + p.fn[ax] : (g > p.fn[ax] ? g - p.fn[ax] : g);
+}
+
+// The runs of the cell-sorted copy that hold the candidates: one per (i, k)
+// column of the range, two when the y range wraps (y is the fastest key, so
+// a column's cells are contiguous).
+__device__ __forceinline__ int neigh_runs_per_col(const DevParams& p, const NeighFrame& F) {
+  return (p.per[1] && (F.glo[1] < 1 || F.ghi[1] > p.fn[1])) ? 2 : 1;
+}
+__device__ __forceinline__ int neigh_nruns(const DevParams& p, const NeighFrame& F) {
+  return (F.ghi[2] - F.glo[2] + 1) * (F.ghi[0] - F.glo[0] + 1) * neigh_runs_per_col(p, F);
+}
+__device__ __forceinline__ void neigh_run(const DevParams& p, const NeighFrame& F, const int* __restrict__ fstart,
+                                          int r, int& qs, int& qe) {
+  const int rpc = neigh_runs_per_col(p, F);
+  const int col = r / rpc, sub = r % rpc;
+  const int ni = F.ghi[0] - F.glo[0] + 1;
+  const int gk = F.glo[2] + col / ni, gi = F.glo[0] + col % ni;
+  const int base = p.fcell_off + search_wrap(p, gk, 2) * p.fc2 + search_wrap(p, gi, 0) * p.fc1;
+  int lo = F.glo[1], hi = F.ghi[1];
+  if (rpc == 2) {
+    if (F.glo[1] < 1) { if (sub == 0) { lo = F.glo[1] + p.fn[1]; hi = p.fn[1]; } else { lo = 1; hi = F.ghi[1]; } }
+    else { if (sub == 0) { lo = F.glo[1]; hi = p.fn[1]; } else { lo = 1; hi = F.ghi[1] - p.fn[1]; } }
+  }
+  qs = fstart[base + lo];
+  qe = fstart[base + hi + 1];
+}
+
+// Candidate q of the sorted copy: a neighbour of the frame's particle when it
+// is a later or non-NORMAL particle (the half list of DESGRID_NEIGH_BUILD),
+// in the reference's DES-grid stencil and within FACTOR_RLM*(r_l + r_i);
+// its row key (stencil rank << 27 | index) through *key.
+__device__ __forceinline__ bool neigh_test(const DevParams& p, const NeighFrame& F, const int4* __restrict__ sinfo,
+                                           const double4* __restrict__ spos, int q, uint32_t* key) {
+  const int4 o = sinfo[q];
+  const int nb = o.x;
+  if (nb == F.cur) return false;
+  if (nb < F.cur && o.z == DEM_STATE_NORMAL) return false;
+  if (o.z == DEM_STATE_NONEXISTENT) return false;
+  const double4 np_ = spos[q];
+  const double srad = F.fr * (F.cp.w + np_.w);
+  {
+    // most candidates are out of reach: the nearest periodic image is at
+    // least as close as the one the stencil picks, so a candidate whose
+    // nearest image is farther than the search radius (with a margin for
+    // rounding) cannot be a neighbour
+    double e[3] = {F.cp.x - np_.x, F.cp.y - np_.y, F.cp.z - np_.z};
+    for (int ax = 0; ax < 3; ++ax)
+      if (F.inv_l[ax] != 0.0) e[ax] = e[ax] - p.L[ax] * rint(e[ax] * F.inv_l[ax]);
+    if (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] > srad * srad * (1.0 + 1e-9)) return false;
+  }
+  // position of the neighbour's DES cell in the reference stencil
+  int nc[3];
+  unpack_ijk(o.y, nc[0], nc[1], nc[2]);
+  int rel[3] = {0, 0, 0};
+  double sh[3] = {0.0, 0.0, 0.0};
+  for (int ax = 0; ax < 3; ++ax) {
+    int r = nc[ax] - F.rc[ax];
+    if (p.per[ax] && !(ax == 2 && p.no_k)) {
+      if (r > 1) r -= F.ncl[ax];
+      else if (r < -1) r += F.ncl[ax];
+      const int l = F.rc[ax] + r;
+      if (l < F.s1[ax]) sh[ax] = -p.L[ax];
+      else if (l > F.e1[ax]) sh[ax] = p.L[ax];
+    }
+    if (r < -F.lo_off[ax] || r > F.hi_off[ax]) return false;
+    rel[ax] = r;
+  }
+  double px = np_.x, py = np_.y, pz = np_.z;
+  if (sh[0] != 0.0) px = px + sh[0];
+  if (sh[1] != 0.0) py = py + sh[1];
+  if (sh[2] != 0.0) pz = pz + sh[2];
+  const double d0 = F.cp.x - px, d1 = F.cp.y - py, d2 = F.cp.z - pz;
+  const double dd = d0 * d0 + d1 * d1 + d2 * d2;
+  if (dd > srad * srad) return false;
+  const int rank = ((rel[2] + 1) * 3 + (rel[1] + 1)) * 3 + (rel[0] + 1);
+  *key = ((uint32_t)rank << 27) | (uint32_t)nb;
+  return true;
+}
+
+// Count pass (FILL = false) and fill pass, a thread per particle of the
+// sorted copy.  The count pass keeps the first NSLOT neighbours of the row,
+// sorted by (rank, index), in the slots; the fill pass copies a row the
+// count pass kept whole and rescans a longer one, inserting in (rank, index)
+// order.  (A warp per particle, testing 32 candidates at a time, was
+// measured slower: the per-particle set-up and run search repeated in every
+// warp cost more than the idle lanes of this loop.)
 template <bool FILL, bool B>
 __global__ void __launch_bounds__(128)
 k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
@@ -136,125 +280,41 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
       return;
     }
   }
+  NeighFrame F;
+  neigh_frame<B>(p, me, spos[q0], F);
   int cnt = 0;
-  {
-    int lic, ljc, lkc;
-    unpack_ijk(me.y, lic, ljc, lkc);
-    const int rc[3] = {lic, ljc, lkc};
-    const int s1[3] = {p.istart1, p.jstart1, p.kstart1}, e1[3] = {p.iend1, p.jend1, p.kend1};
-    const int ncl[3] = {p.iend1 - p.istart1 + 1, p.jend1 - p.jstart1 + 1, p.kend1 - p.kstart1 + 1};
-    const double4 cp = spos[q0];
-    const double cpos[3] = {cp.x, cp.y, cp.z};
-    const double fr = p.factor_rlm, mr = p.max_radius;
-    int lo_off[3] = {1, 1, 1}, hi_off[3] = {1, 1, 1};
-    for (int ax = 0; ax < 3; ++ax) {
-      if (ax == 2 && p.no_k) { lo_off[2] = 0; hi_off[2] = 0; break; }
-      const bool coarse = 1.0 > 2.0 * mr * fr * p.dg_inv[ax];
-      if (coarse) {
-        const double t = (cpos[ax] - p.dg_start[ax]) * p.dg_inv[ax];
-        const double off = t - (double)(long long)floor(t);
-        if (off >= 0.5) lo_off[ax] = 0; else hi_off[ax] = 0;
+  const int nr = neigh_nruns(p, F);
+  for (int r = 0; r < nr; ++r) {
+    int qs, qe;
+    neigh_run(p, F, fstart, r, qs, qe);
+    for (int q = qs; q < qe; ++q) {
+      uint32_t key;
+      if (!neigh_test(p, F, sinfo, spos, q, &key)) continue;
+      const int rank = (int)(key >> 27), nb = (int)(key & 0x7ffffffu);
+      if (!FILL && cnt < NSLOT) {
+        // keep the row sorted by (rank, index) in the slots
+        int b = cnt - 1;
+        while (b >= 0 && slot[b] > key) { slot[b + 1] = slot[b]; --b; }
+        slot[b + 1] = key;
       }
-    }
-    // the search cells within reach FACTOR_RLM*(r + MAX_RADIUS) of the
-    // particle, each once: per axis a range of cells, wrapped on a periodic
-    // axis (the whole axis when the range covers it); along y (the fastest
-    // key) the cells of a range are contiguous, so each (i, k) column of the
-    // range is at most two runs of the cell-sorted copy
-    const double reach = fr * (cp.w + mr);
-    int glo[3] = {0, 0, 0}, ghi[3] = {0, 0, 0};
-    for (int ax = 0; ax < 3; ++ax) {
-      if (ax == 2 && p.no_k) break;
-      // (a margin of 1e-4 of the reach covers the rounding of the cell index)
-      const double t = (cpos[ax] - p.dg_start[ax]) * p.f_inv[ax], w = reach * p.f_inv[ax] * 1.0001;
-      int lo = (int)floor(t - w) + 1, hi = (int)floor(t + w) + 1;
-      if (p.per[ax]) {
-        if (hi - lo + 1 >= p.fn[ax]) { lo = 1; hi = p.fn[ax]; }
-      } else {
-        lo = max(lo, 0);
-        hi = min(hi, p.fn[ax] + 1);
-      }
-      glo[ax] = lo;
-      ghi[ax] = hi;
-    }
-    auto wrap = [&](int g, int ax) {
-      if (!p.per[ax] || (ax == 2 && p.no_k)) return g;
-      return g < 1 ? g + p.fn[ax] : (g > p.fn[ax] ? g - p.fn[ax] : g);
-    };
-    for (int gk = glo[2]; gk <= ghi[2]; ++gk)
-    for (int gi = glo[0]; gi <= ghi[0]; ++gi) {
-      const int col = p.fcell_off + wrap(gk, 2) * p.fc2 + wrap(gi, 0) * p.fc1;
-      int run_lo[2], run_hi[2], nrun = 1;
-      run_lo[0] = glo[1]; run_hi[0] = ghi[1];
-      if (p.per[1] && glo[1] < 1) {
-        run_lo[0] = glo[1] + p.fn[1]; run_hi[0] = p.fn[1]; run_lo[1] = 1; run_hi[1] = ghi[1]; nrun = 2;
-      } else if (p.per[1] && ghi[1] > p.fn[1]) {
-        run_lo[0] = glo[1]; run_hi[0] = p.fn[1]; run_lo[1] = 1; run_hi[1] = ghi[1] - p.fn[1]; nrun = 2;
-      }
-      for (int rr = 0; rr < nrun; ++rr) {
-      const int qs = fstart[col + run_lo[rr]], qe = fstart[col + run_hi[rr] + 1];
-      for (int q = qs; q < qe; ++q) {
-        const int4 o = sinfo[q];
-        const int nb = o.x;
-        if (nb == cur) continue;
-        if (nb < cur && o.z == DEM_STATE_NORMAL) continue;
-        if (o.z == DEM_STATE_NONEXISTENT) continue;
-        // position of the neighbour's DES cell in the reference stencil
-        int nc[3];
-        unpack_ijk(o.y, nc[0], nc[1], nc[2]);
-        int rel[3];
-        double sh[3] = {0.0, 0.0, 0.0};
-        bool in_stencil = true;
-        for (int ax = 0; ax < 3; ++ax) {
-          int r = nc[ax] - rc[ax];
-          if (p.per[ax] && !(ax == 2 && p.no_k)) {
-            if (r > 1) r -= ncl[ax];
-            else if (r < -1) r += ncl[ax];
-            const int l = rc[ax] + r;
-            if (l < s1[ax]) sh[ax] = -p.L[ax];
-            else if (l > e1[ax]) sh[ax] = p.L[ax];
+      if (FILL) {
+        long long sl = (long long)start + cnt;
+        if (sl < cap) {
+          // insertion into the row kept sorted by (rank, index)
+          long long b = sl - 1;
+          while (b >= start) {
+            const int rb = rank_buf[b];
+            if (rb < rank || (rb == rank && nbrs[b] < nb)) break;
+            nbrs[b + 1] = nbrs[b];
+            rank_buf[b + 1] = (uint8_t)rb;
+            --b;
           }
-          if (r < -lo_off[ax] || r > hi_off[ax]) { in_stencil = false; break; }
-          rel[ax] = r;
+          nbrs[b + 1] = nb;
+          rank_buf[b + 1] = (uint8_t)rank;
+          owner[sl] = cur;
         }
-        if (!in_stencil) continue;
-        const double4 np_ = spos[q];
-        const double srad = fr * (cp.w + np_.w);
-        double px = np_.x, py = np_.y, pz = np_.z;
-        if (sh[0] != 0.0) px = px + sh[0];
-        if (sh[1] != 0.0) py = py + sh[1];
-        if (sh[2] != 0.0) pz = pz + sh[2];
-        const double d0 = cp.x - px, d1 = cp.y - py, d2 = cp.z - pz;
-        const double dd = d0 * d0 + d1 * d1 + d2 * d2;
-        if (dd > srad * srad) continue;
-        const int rank = ((rel[2] + 1) * 3 + (rel[1] + 1)) * 3 + (rel[0] + 1);
-        if (!FILL && cnt < NSLOT) {
-          // keep the row sorted by (rank, index) in the slots
-          const uint32_t key = ((uint32_t)rank << 27) | (uint32_t)nb;
-          int b = cnt - 1;
-          while (b >= 0 && slot[b] > key) { slot[b + 1] = slot[b]; --b; }
-          slot[b + 1] = key;
-        }
-        if (FILL) {
-          long long slot = (long long)start + cnt;
-          if (slot < cap) {
-            // insertion into the row kept sorted by (rank, index)
-            long long b = slot - 1;
-            while (b >= start) {
-              const int rb = rank_buf[b];
-              if (rb < rank || (rb == rank && nbrs[b] < nb)) break;
-              nbrs[b + 1] = nbrs[b];
-              rank_buf[b + 1] = (uint8_t)rb;
-              --b;
-            }
-            nbrs[b + 1] = nb;
-            rank_buf[b + 1] = (uint8_t)rank;
-            owner[slot] = cur;
-          }
-        }
-        ++cnt;
       }
-      }
+      ++cnt;
     }
   }
   if (FILL) row_se[cur] = (int)min((long long)start + cnt, cap);   // start -> end pointer

@@ -109,7 +109,8 @@ class DemStats(C.Structure):
         ("max_overlap_ratio", C.c_double),
         ("bed_height", C.c_double),
         ("s_time", C.c_double),
-        ("reserved", C.c_double * 4),
+        ("n_outflow_removed", C.c_int64),
+        ("reserved", C.c_double * 3),
     ]
 
     def as_dict(self):
@@ -208,6 +209,19 @@ class DemVtpOptions(C.Structure):
     ]
 
 
+class DemOutflowBC(C.Structure):
+    _fields_ = [
+        ("plane", C.c_int32),
+        ("mass_outflow", C.c_int32),
+        ("dg_lo", C.c_int32 * 3),
+        ("dg_hi", C.c_int32 * 3),
+        ("reserved_i", C.c_int32 * 4),
+        ("face", C.c_double),
+        ("vel", (C.c_double * 3) * DEM_MAX_PHASES),
+        ("reserved_d", C.c_double * 4),
+    ]
+
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -228,6 +242,7 @@ SIGNATURES = {
     "download_pairs": (C.c_int, [_P, _I32, _I32, _D, C.c_int64, C.c_int32]),
     "upload_pairs": (C.c_int, [_P, _I32, _I32, _D, C.c_int64, C.c_int32]),
     "download_wall_history": (C.c_int, [_P, _I32, _D, C.c_int32]),
+    "set_outflow_bcs": (C.c_int, [_P, C.c_void_p, C.c_int32]),
     "upload_wall_history": (C.c_int, [_P, _I32, _D, C.c_int32]),
     "download_cells": (C.c_int, [_P, _I32, C.c_int32]),
     "desgrid_pic": (C.c_int, [_P]),

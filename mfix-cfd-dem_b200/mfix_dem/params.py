@@ -466,3 +466,34 @@ def batch_limits(lib, entries, max_systems=None, slack=1.0, bins_per_cell=8):
     lim.max_facets = int(facets * slack) + 1
     lim.max_facet_bins = int(des * slack * bins_per_cell) + 1
     return lim
+
+
+def _nint(v: float) -> int:
+    """Fortran NINT: nearest integer, halves away from zero."""
+    return int(math.floor(v + 0.5)) if v >= 0 else -int(math.floor(-v + 0.5))
+
+
+def outflow_bc(prm, plane: str, lo, hi, face: float, mass_outflow: bool = False, vel=None):
+    """A dem_outflow_bc for a boundary whose extents are BC_X_w..BC_X_e,
+    BC_Y_s..BC_Y_n, BC_Z_b..BC_Z_t = lo..hi: its DES-cell box as SET_BC_DEM_MO
+    builds it (set_bc_dem_mo.f:79-101) with IofBCPOS/JofBCPOS/KofBCPOS
+    (desgrid_mod.f:428-455: NINT of the position in DES cells, 1-based with
+    one ghost layer), `face` the plane the distance is measured from and
+    `vel` the BC_U_s/V_s/W_s per phase for MASS_OUTFLOW."""
+    from . import abi
+    b = abi.DemOutflowBC()
+    b.plane = ord(plane)
+    b.mass_outflow = 1 if mass_outflow else 0
+    start = (prm.dg_xstart, prm.dg_ystart, prm.dg_zstart)
+    inv = (prm.dg_dxinv, prm.dg_dyinv, prm.dg_dzinv)
+    for a in range(3):
+        if a == 2 and prm.no_k:
+            b.dg_lo[2] = b.dg_hi[2] = 1
+            continue
+        b.dg_lo[a] = _nint((lo[a] - start[a]) * inv[a]) + 2 - 1
+        b.dg_hi[a] = _nint((hi[a] - start[a]) * inv[a]) + 2 - 1 + 1
+    b.face = float(face)
+    for m, v in enumerate(vel or []):
+        for c in range(3):
+            b.vel[m][c] = float(v[c])
+    return b

@@ -175,6 +175,12 @@ class DemSystem:
         pf = np.ascontiguousarray(pft, dtype=np.float64).reshape(n, cm, 3)
         self._call("upload_wall_history", self._h, _ip(fid), _dp(pf), C.c_int32(n))
 
+    def set_outflow_bcs(self, bcs):
+        """The DEM outflow boundaries (abi.DemOutflowBC, e.g. from
+        params.outflow_bc); an empty list removes them."""
+        arr = (abi.DemOutflowBC * max(len(bcs), 1))(*bcs)
+        self._call("set_outflow_bcs", self._h, C.cast(arr, C.c_void_p), C.c_int32(len(bcs)))
+
     def download_cells(self):
         cells = np.empty(self.n, dtype=np.int32)
         self._call("download_cells", self._h, _ip(cells), C.c_int32(self.n))

@@ -98,6 +98,10 @@ struct Oracle {
   std::vector<double> xe, yn, zt;         // face positions, index 0..imax+2
   std::vector<double> ep_g, u_g, v_g, w_g, p_force, rop_s, vol_surr;
   std::vector<double> vol_node;            // DES_VOL_NODE per node
+  std::vector<dem_outflow_bc> obc;         // DEM outflow boundaries (DEM_BCMO_MAP order)
+  std::vector<double> vel_old;             // DES_VEL_OLD when outflow boundaries are set
+  bool exit_first_pass = true;             // UPDATE_EXIT_DES_VEL's own FIRST_PASS
+  int64_t n_outflow_deleted = 0;
   std::vector<double> drag_am, drag_bm, f_gds;  // DRAG_AM, DRAG_BM(:,3), F_GDS
   std::vector<int> pijk;                  // (n,4): i, j, k, ijk (1-based), 0 = none
   std::vector<double> f_gp;               // F_GP(n)
@@ -911,7 +915,7 @@ struct Oracle {
         double* v = X(vel, c); double* x = X(pos, c); double* f = X(fc, c); double* a = X(acc_old, c);
         for (int l = 0; l < n; ++l) {
           // CFUPDATEOLD copies NEW into OLD for existing non-ghost particles.
-          double vold = v[l], xold = x[l];
+          double vold = vel_old.empty() ? v[l] : X(vel_old, c)[l], xold = x[l];
           if (state[l] == DEM_STATE_NORMAL) f[l] = f[l] / pmass[l] + p.grav[c];
           if (state[l] == DEM_STATE_NORMAL) v[l] = vold + 0.5 * (3.0 * f[l] - a[l]) * dt;
           a[l] = f[l];
@@ -1320,8 +1324,8 @@ struct Oracle {
     int rc = calc_force();
     if (rc) return rc;
     if (g.interp_scheme == DEM_INTERP_NONE) drag_des1(); else drag();   // CALC_DRAG_DES
-    cfnewvalues();
-    bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0);
+    const bool force = integrate_with_outflow();
+    bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0) || force;
     bool anyper = p.periodic[0] || p.periodic[1] || (p.periodic[2] && !p.no_k);
     if (do_nsearch || anyper) desgrid_pic();
     if (do_nsearch) neighbour();
@@ -1332,11 +1336,110 @@ struct Oracle {
   }
 
   // DES_TIME_STEP(NN) for pure DEM (des_time_march.f:342-432).
+  // Outflow boundaries -----------------------------------------------
+  bool in_bc_box(const dem_outflow_bc& b, int l) const {
+    const int c = dg_pijk[l];
+    if (c < 1) return false;
+    const int ijk[3] = {iof(c), jof(c), kof(c)};
+    for (int a = 0; a < 3; ++a)
+      if (ijk[a] < b.dg_lo[a] || ijk[a] > b.dg_hi[a]) return false;
+    return true;
+  }
+  static void bc_plane(int plane, double freeze[3], int& idx, double& sgn) {
+    freeze[0] = freeze[1] = freeze[2] = 0.0;
+    switch (plane) {
+      case 'N': idx = 1; sgn = -1.0; break;
+      case 'S': idx = 1; sgn = 1.0; break;
+      case 'E': idx = 0; sgn = -1.0; break;
+      case 'W': idx = 0; sgn = 1.0; break;
+      case 'T': idx = 2; sgn = -1.0; break;
+      default: idx = 2; sgn = 1.0; break;  // 'B'
+    }
+    freeze[idx] = 1.0;
+  }
+
+  // UPDATE_EXIT_DES_VEL (mass_outflow_dem.f:444-514): EXITING particles in the
+  // cells of a non-MASS_OUTFLOW boundary keep integrating their force, with
+  // the velocity frozen to the boundary-normal component.  The particle loop
+  // of each boundary is a particle loop here (a particle is in one cell).
+  void update_exit_vel() {
+    const double dt = p.dtsolid;
+    for (const dem_outflow_bc& b : obc) {
+      if (b.mass_outflow) continue;
+      double fz[3]; int idx; double sgn;
+      bc_plane(b.plane, fz, idx, sgn);
+      for (int l = 0; l < n; ++l) {
+        if (state[l] != DEM_STATE_EXITING || !in_bc_box(b, l)) continue;
+        for (int c = 0; c < 3; ++c) {
+          double* v = X(vel, c); double* f = X(fc, c); double* a = X(acc_old, c);
+          if (exit_first_pass && p.intg_method == DEM_INTG_AB2) a[l] = f[l] / pmass[l] + p.grav[c];
+          if (p.intg_method == DEM_INTG_EULER) {
+            v[l] = v[l] + dt * (f[l] / pmass[l] + p.grav[c]);
+          } else {
+            f[l] = f[l] / pmass[l] + p.grav[c];
+            v[l] = X(vel_old, c)[l] + 0.5 * (3.0 * f[l] - a[l]) * dt;
+            a[l] = f[l];
+          }
+          v[l] = v[l] * fz[c];
+        }
+      }
+    }
+    exit_first_pass = false;
+  }
+
+  // MASS_OUTFLOW_DEM (mass_outflow_dem.f:13-188); returns whether a particle
+  // was deleted (FORCE_NSEARCH).
+  bool mass_outflow() {
+    bool force = false;
+    for (const dem_outflow_bc& b : obc) {
+      double fz[3]; int idx; double sgn;
+      bc_plane(b.plane, fz, idx, sgn);
+      for (int l = 0; l < n; ++l) {
+        if (!in_bc_box(b, l)) continue;
+        const int8_t st = state[l];
+        if (st == DEM_STATE_NONEXISTENT || st >= DEM_STATE_NORMAL_GHOST || st == DEM_STATE_ENTERING) continue;
+        const double x = P(pos, l, idx);
+        const double dist = (b.plane == 'N' || b.plane == 'E' || b.plane == 'T') ? x - b.face : b.face - x;
+        if (dist > rad[l]) {
+          state[l] = DEM_STATE_NORMAL;
+        } else if (dist > 0.0) {
+          if (!b.mass_outflow) {
+            if (P(vel, l, idx) * sgn > 0.0) {
+              for (int c = 0; c < 3; ++c) X(vel, c)[l] = X(vel, c)[l] * fz[c];
+              state[l] = DEM_STATE_EXITING;
+            }
+          } else {
+            const int m = phase[l];
+            for (int c = 0; c < 3; ++c) X(vel, c)[l] = b.vel[m][c];
+            state[l] = DEM_STATE_EXITING;
+          }
+        } else {
+          delete_particle(l);
+          n_outflow_deleted++;
+          force = true;
+        }
+      }
+    }
+    return force;
+  }
+
+  // The part of DES_TIME_STEP between the forces and the neighbour search
+  // with outflow boundaries: CFUPDATEOLD's DES_VEL_OLD, UPDATE_EXIT_DES_VEL,
+  // CFNEWVALUES, MASS_OUTFLOW_DEM.  Returns FORCE_NSEARCH.
+  bool integrate_with_outflow() {
+    if (obc.empty()) { cfnewvalues(); return false; }
+    vel_old = vel;
+    update_exit_vel();
+    cfnewvalues();
+    vel_old.clear();
+    return mass_outflow();
+  }
+
   int step(int nn) {
     int rc = calc_force();
     if (rc) return rc;
-    cfnewvalues();
-    bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0);
+    const bool force = integrate_with_outflow();
+    bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0) || force;
     bool anyper = p.periodic[0] || p.periodic[1] || (p.periodic[2] && !p.no_k);
     if (do_nsearch || anyper) desgrid_pic();
     if (do_nsearch) neighbour();
@@ -1492,6 +1595,27 @@ int orc_upload_wall_history(orc_handle* h, const int32_t* fid, const double* pf,
   return 0;
 }
 
+int orc_set_outflow_bcs(orc_handle* h, const dem_outflow_bc* bcs, int32_t n) {
+  Oracle& o = h->o;
+  if (n < 0 || (n > 0 && !bcs)) return o.fail(DEM_ERR_ARG, "bad outflow boundaries");
+  for (int32_t b = 0; b < n; ++b) {
+    const int pl = bcs[b].plane;
+    if (pl != 'N' && pl != 'S' && pl != 'E' && pl != 'W' && pl != 'T' && pl != 'B')
+      return o.fail(DEM_ERR_ARG, "unknown BC_PLANE");
+    for (int a = 0; a < 3; ++a)
+      if (bcs[b].dg_lo[a] > bcs[b].dg_hi[a]) return o.fail(DEM_ERR_ARG, "empty DES-cell box");
+    for (int c = 0; c < b; ++c) {
+      bool overlap = true;
+      for (int a = 0; a < 3; ++a)
+        overlap = overlap && bcs[b].dg_lo[a] <= bcs[c].dg_hi[a] && bcs[c].dg_lo[a] <= bcs[b].dg_hi[a];
+      if (overlap) return o.fail(DEM_ERR_ARG, "outflow boundary boxes overlap");
+    }
+  }
+  o.obc.assign(bcs, bcs + n);
+  o.exit_first_pass = true;
+  return 0;
+}
+
 int orc_download_cells(orc_handle* h, int32_t* cells, int32_t max_pip) {
   Oracle& o = h->o;
   if (max_pip != o.n) return DEM_ERR_ARG;
@@ -1555,6 +1679,7 @@ int orc_get_stats(orc_handle* h, dem_stats* s) {
   }
   for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn ? gt[c] / nn : 0.0; }
   s->n_normal = nn;
+  s->n_outflow_removed = o.n_outflow_deleted;
   s->n_pairs = (int64_t)o.nbrs.size();
   s->n_contacts = o.n_contacts;
   s->n_wall_contacts = o.n_wall_contacts;
