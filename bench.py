@@ -44,11 +44,11 @@ def parse():
     ap.add_argument("--n", type=int, default=1_000_000, help="particles per system")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--cpu-sample", type=int, default=125_000, help="particles in the CPU sample")
-    ap.add_argument("--cpu-steps", type=int, default=25)
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000, help="particles in the CPU sample")
+    ap.add_argument("--cpu-steps", type=int, default=200, help="timed steps of the CPU sample (about 10 s)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision leg")
-    ap.add_argument("--serve-graphs", type=int, default=0,
+    ap.add_argument("--serve-graphs", type=int, default=1,
                     help="served leg: replay aligned periods as CUDA graphs (1) or step launch by launch (0)")
     ap.add_argument("--batch-systems", type=int, default=256, help="systems of the batched leg (0 = skip)")
     ap.add_argument("--batch-total", type=int, default=6_000_000, help="particles of the batched leg")
@@ -160,9 +160,11 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes(n_normal, n_pairs):
-    # per step: N*(96 read + 72 write + 4 CSR) + P*(4 id + 24 PFT read + 24 PFT write)
-    return n_normal * 172 + n_pairs * 52
+def algorithmic_bytes(n_normal, n_pairs, periodic=True):
+    # per step: N*(96 read + 72 write + 4 CSR) + P*(4 id + 24 PFT read + 24 PFT write),
+    # and for a periodic system the DES cell and facet flag the integration
+    # writes (N*5)
+    return n_normal * (177 if periodic else 172) + n_pairs * 52
 
 
 def cpu_sample(args, threads=None):
@@ -183,7 +185,8 @@ def cpu_sample(args, threads=None):
     n = int(o.stats()["n_normal"])
     return {"value": n * args.cpu_steps / dt, "unit": METRIC, "cores": threads, "kind": "port",
             "sample": f"{n} particles of the same workload (box scaled to keep density and bed height), "
-                      f"{args.cpu_steps} steps incl. one neighbour rebuild, OpenMP oracle, {dt:.1f} s"}
+                      f"{args.cpu_steps} steps incl. {args.cpu_steps // 25} neighbour rebuilds, OpenMP oracle, "
+                      f"{dt:.1f} s"}
 
 
 def run_reference(args):
@@ -417,7 +420,7 @@ def _batched_run(args, prec, stream, systems, info):
     n_normal = int(st["n_normal"])
     f_ms, f_n = prof["force"]
     peak, peak_kind = measured_peak()
-    bytes_launch = algorithmic_bytes(n_normal, 0.5 * (p0 + p1))
+    bytes_launch = algorithmic_bytes(n_normal, 0.5 * (p0 + p1), periodic=False)
     achieved = bytes_launch / (f_ms / f_n / 1e3) / 1e9 if f_n else None
     final = {sid: bt.download_state(sid)["pos"] for sid in ids}
     bt.close()

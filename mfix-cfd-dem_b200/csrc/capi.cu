@@ -404,6 +404,7 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
   A((void**)&h->fcell_start, sizeof(int) * (nfc + 1));
   A((void**)&h->fcell_list, sizeof(int) * n);
   A((void**)&h->spos, sizeof(double4) * n);
+  A((void**)&h->sposf, sizeof(float4) * n);
   A((void**)&h->sinfo, sizeof(int4) * n);
   A((void**)&h->nslot, sizeof(uint32_t) * NSLOT * n);
   A((void**)&h->row_cnt, sizeof(int) * n);
@@ -490,7 +491,7 @@ int dem_destroy(dem_handle* h) {
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
                   h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->skin, h->vslot, h->pgap,
-                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sinfo, h->nslot, h->d_np,
+                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -726,7 +727,9 @@ static int step_once(dem_handle* h, int nn) {
     if (int rc = run_cfnewvalues_outflow(h, &force)) return rc;
   }
   const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0) || force;
-  if (do_nsearch || anyper) {
+  // the integrating gather of a periodic system already placed the particles
+  const bool placed = h->obc.empty() && cells_in_gather(h);
+  if (do_nsearch || (anyper && !placed)) {
     if (int rc = run_desgrid_pic(h, do_nsearch)) return rc;
   }
   if (do_nsearch) {

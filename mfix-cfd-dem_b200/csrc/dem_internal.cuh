@@ -197,6 +197,7 @@ struct dem_handle {
   int* fcell_start = nullptr; // nfcell+1
   int* fcell_list = nullptr;  // n
   double4* spos = nullptr;    // n: positions in search-cell order (pair build)
+  float4* sposf = nullptr;    // n: the same rounded to FP32 (conservative distance pre-check)
   int4* sinfo = nullptr;      // n: (particle, packed DES cell (i,j,k), state, search cell) in that order
   uint32_t* nslot = nullptr;  // n * NSLOT: rows kept by the count pass of the pair build
 
@@ -391,6 +392,37 @@ __device__ __forceinline__ int dg_ofpos(const DevParams& p, int ax, double x, in
   return (int)floor((x - p.dg_start[ax]) * p.dg_inv[ax]) + start1;
 }
 
+// DESGRID_PIC for one existing particle at x (desgrid_mod.f:877-995): on a
+// periodic axis a coordinate whose cell left the domain's cells moves by one
+// period (the serial self-exchange of DES_PAR_EXCHANGE,
+// mpi_funs_des_mod.f:38-160); then the clamped DES cell.  Returns whether x
+// moved.
+__device__ __forceinline__ bool dg_place(const DevParams& p, bool per, double4& x, int& cell) {
+  bool moved = false;
+  if (per) {
+    if (p.per[0]) {
+      int ci = dg_ofpos(p, 0, x.x, p.istart1);
+      if (ci > p.iend1) { x.x = x.x - p.L[0]; moved = true; }
+      else if (ci < p.istart1) { x.x = x.x + p.L[0]; moved = true; }
+    }
+    if (p.per[1]) {
+      int cj = dg_ofpos(p, 1, x.y, p.jstart1);
+      if (cj > p.jend1) { x.y = x.y - p.L[1]; moved = true; }
+      else if (cj < p.jstart1) { x.y = x.y + p.L[1]; moved = true; }
+    }
+    if (p.per[2] && !p.no_k) {
+      int ck = dg_ofpos(p, 2, x.z, p.kstart1);
+      if (ck > p.kend1) { x.z = x.z - p.L[2]; moved = true; }
+      else if (ck < p.kstart1) { x.z = x.z + p.L[2]; moved = true; }
+    }
+  }
+  int li = min(p.iend2, max(p.istart2, dg_ofpos(p, 0, x.x, p.istart1)));
+  int lj = min(p.jend2, max(p.jstart2, dg_ofpos(p, 1, x.y, p.jstart1)));
+  int lk = p.no_k ? 1 : min(p.kend2, max(p.kstart2, dg_ofpos(p, 2, x.z, p.kstart1)));
+  cell = dg_funijk(p, li, lj, lk);
+  return moved;
+}
+
 // Minimum-image shift for periodic axes (the copy of j that the reference's
 // ghost exchange places next to i).
 __device__ __forceinline__ double periodic_shift(const DevParams& p, int ax, double d) {
@@ -422,6 +454,14 @@ __device__ __forceinline__ double speed(const double v[3]) {
 // cfnewvalues.f:700-812) into the other state buffer (MODE 1 = Euler,
 // MODE 2 = Adams-Bashforth).  Velocity updates apply to NORMAL particles,
 // position updates to states below NORMAL_GHOST.
+// Outputs of DESGRID_PIC when the integration does it for the new positions
+// (a null dg_pijk: not done there).
+struct CellOut {
+  int* dg_pijk = nullptr;
+  uint8_t* wall_cand = nullptr;
+  const int* fbin_start = nullptr;
+};
+
 template <int MODE>
 __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8_t st, const double x[3],
                                                 const double v[3], const double w[3], double r, double m,
@@ -429,7 +469,8 @@ __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8
                                                 double4* __restrict__ pos_n, double4* __restrict__ vel_n,
                                                 double4* __restrict__ omg_n, double* __restrict__ fc,
                                                 double* __restrict__ tow, double* __restrict__ acc_old,
-                                                double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot) {
+                                                double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot,
+                                                CellOut cells = CellOut{}) {
   const size_t n = (size_t)p.n;
   if (MODE == 0) {
 #pragma unroll
@@ -470,7 +511,21 @@ __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8
       rot_acc_old[c * n + me] = ro;
     }
   }
-  pos_n[me] = make_double4(xn[0], xn[1], xn[2], r);
+  double4 xo = make_double4(xn[0], xn[1], xn[2], r);
+  if (cells.dg_pijk) {
+    // the step's DESGRID_PIC for a periodic system, on the new position
+    if (st == DEM_STATE_NONEXISTENT) {
+      cells.dg_pijk[me] = 0;
+      cells.wall_cand[me] = 0;
+    } else {
+      int c;
+      dg_place(p, true, xo, c);
+      cells.dg_pijk[me] = c;
+      const int fc = p.cell_off + c - 1;
+      cells.wall_cand[me] = cells.fbin_start[fc + 1] > cells.fbin_start[fc] ? 1 : 0;
+    }
+  }
+  pos_n[me] = xo;
   vel_n[me] = make_double4(vn[0], vn[1], vn[2], m);
   omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
   // |x_new - x| <= max(|v|, |v_new|) * dt for both integrators
@@ -480,3 +535,23 @@ __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8
 }  // namespace demb
 
 #define DEM_LAUNCH(h) ((h)->launches++)
+
+namespace demb {
+// A single handle with a periodic axis places its particles in their DES
+// cells in the integrating gather (the step's DESGRID_PIC then runs only on
+// neighbour-search steps, where it repeats the same placement).
+inline bool cells_in_gather(const dem_handle* h) {
+  const DevParams& p = h->dp;
+  return !h->batch() && (p.per[0] || p.per[1] || (p.per[2] && !p.no_k));
+}
+template <int MODE, bool B>
+inline CellOut gather_cells(const dem_handle* h) {
+  CellOut c;
+  if (MODE != 0 && !B && cells_in_gather(h)) {
+    c.dg_pijk = h->dg_pijk;
+    c.wall_cand = h->wall_cand;
+    c.fbin_start = h->fbin_start;
+  }
+  return c;
+}
+}  // namespace demb

@@ -29,31 +29,11 @@ __global__ void k_cell_keys(DevParams p0, BatchView bv, double4* __restrict__ po
   if constexpr (B) {
     if (!bv.due[bv.sys_of[i]] && !per) return;
   }
-  if (state[i] == DEM_STATE_NONEXISTENT) { dg_pijk[i] = 0; wall_cand[i] = 0; return; }
+  // the position is read with the state (both loads in flight at once)
   double4 x = pos4[i];
-  if (per) {
-    bool moved = false;
-    if (p.per[0]) {
-      int ci = dg_ofpos(p, 0, x.x, p.istart1);
-      if (ci > p.iend1) { x.x = x.x - p.L[0]; moved = true; }
-      else if (ci < p.istart1) { x.x = x.x + p.L[0]; moved = true; }
-    }
-    if (p.per[1]) {
-      int cj = dg_ofpos(p, 1, x.y, p.jstart1);
-      if (cj > p.jend1) { x.y = x.y - p.L[1]; moved = true; }
-      else if (cj < p.jstart1) { x.y = x.y + p.L[1]; moved = true; }
-    }
-    if (p.per[2] && !p.no_k) {
-      int ck = dg_ofpos(p, 2, x.z, p.kstart1);
-      if (ck > p.kend1) { x.z = x.z - p.L[2]; moved = true; }
-      else if (ck < p.kstart1) { x.z = x.z + p.L[2]; moved = true; }
-    }
-    if (moved) pos4[i] = x;
-  }
-  int li = min(p.iend2, max(p.istart2, dg_ofpos(p, 0, x.x, p.istart1)));
-  int lj = min(p.jend2, max(p.jstart2, dg_ofpos(p, 1, x.y, p.jstart1)));
-  int lk = p.no_k ? 1 : min(p.kend2, max(p.kstart2, dg_ofpos(p, 2, x.z, p.kstart1)));
-  const int c = dg_funijk(p, li, lj, lk);
+  if (state[i] == DEM_STATE_NONEXISTENT) { dg_pijk[i] = 0; wall_cand[i] = 0; return; }
+  int c;
+  if (dg_place(p, per, x, c)) pos4[i] = x;
   dg_pijk[i] = c;
   const int fc = p.cell_off + c - 1;
   wall_cand[i] = fbin_start[fc + 1] > fbin_start[fc] ? 1 : 0;

@@ -409,40 +409,76 @@ __global__ void k_wall_gaps(DevParams p0, BatchView bv, WallCtx w, const double4
 // The particles with wall work this step: NORMAL particles whose DES cell
 // holds facets and whose clearance at the last build does not exceed the
 // displacement bound since, and NORMAL particles whose history slots may be
-// in use (k_walls clears them, or updates them).  Each block of WALL_LIST_T
-// threads appends its particles in index order with one atomic; blocks land
-// in arbitrary order, which does not matter: each particle's wall terms
-// depend on it alone.
+// in use (k_walls clears them, or updates them).  A thread screens four
+// consecutive particles: their flags arrive in one 32-bit load per array and
+// their clearances in one float4, all issued before any is used, so the
+// kernel waits on memory about once.  Each block of WALL_LIST_T threads
+// appends its particles in index order with one atomic; blocks land in
+// arbitrary order, which does not matter: each particle's wall terms depend
+// on it alone.
 constexpr int WALL_LIST_T = 1024;
 static_assert(WALL_LIST_T == 32 * 32, "one warp scans the warp counts");
+__device__ __forceinline__ unsigned wall_need(unsigned st, unsigned live, unsigned cand, float gap, double bound) {
+  return (st == (unsigned)(uint8_t)DEM_STATE_NORMAL && (live || (cand && !((double)gap > bound)))) ? 1u : 0u;
+}
 __global__ void __launch_bounds__(WALL_LIST_T)
 k_wall_list(int n, const int8_t* __restrict__ state, const uint8_t* __restrict__ wall_cand,
             const uint8_t* __restrict__ wall_live, const float* __restrict__ wgap, const double* __restrict__ skin,
             int* __restrict__ list, int* __restrict__ count) {
   __shared__ int warp_n[WALL_LIST_T / 32];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
   const double bound = *skin;
-  const bool need = i < n && state[i] == DEM_STATE_NORMAL &&
-                    (wall_live[i] || (wall_cand[i] && !((double)wgap[i] > bound)));
-  const unsigned m = __ballot_sync(0xffffffffu, need);
+  uint32_t st = 0, lv = 0, cd = 0;
+  float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (i0 + 3 < n) {  // the arrays are separate allocations: 256-byte aligned
+    st = *reinterpret_cast<const uint32_t*>(state + i0);
+    lv = *reinterpret_cast<const uint32_t*>(wall_live + i0);
+    cd = *reinterpret_cast<const uint32_t*>(wall_cand + i0);
+    g = *reinterpret_cast<const float4*>(wgap + i0);
+  } else {
+    float gg[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (i0 + j < n) {
+        st |= (uint32_t)(uint8_t)state[i0 + j] << (8 * j);
+        lv |= (uint32_t)wall_live[i0 + j] << (8 * j);
+        cd |= (uint32_t)wall_cand[i0 + j] << (8 * j);
+        gg[j] = wgap[i0 + j];
+      }
+    g = make_float4(gg[0], gg[1], gg[2], gg[3]);
+  }
+  // bit j: particle i0+j has wall work (bytes past n are zero: state 0 is
+  // not NORMAL)
+  const unsigned need = wall_need(st & 255u, lv & 255u, cd & 255u, g.x, bound) |
+                        (wall_need((st >> 8) & 255u, (lv >> 8) & 255u, (cd >> 8) & 255u, g.y, bound) << 1) |
+                        (wall_need((st >> 16) & 255u, (lv >> 16) & 255u, (cd >> 16) & 255u, g.z, bound) << 2) |
+                        (wall_need(st >> 24, lv >> 24, cd >> 24, g.w, bound) << 3);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) warp_n[warp] = __popc(m);
+  const int mine = __popc(need);
+  int incl = mine;  // inclusive scan of the counts over the warp
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_n[warp] = incl;
   __syncthreads();
   if (warp == 0) {  // the warps' offsets: a scan of their counts, and one atomic
     const int c = warp_n[lane];
-    int incl = c;
+    int wi = c;
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
+      const int y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
     }
-    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    const int tot = __shfl_sync(0xffffffffu, wi, 31);
     int base = 0;
     if (lane == 0 && tot) base = atomicAdd(count, tot);
     base = __shfl_sync(0xffffffffu, base, 0);
-    warp_n[lane] = base + incl - c;
+    warp_n[lane] = base + wi - c;
   }
   __syncthreads();
-  if (need) list[warp_n[warp] + __popc(m & ((1u << lane) - 1u))] = i;
+  int at = warp_n[warp] + incl - mine;
+  for (int j = 0; j < 4; ++j)
+    if ((need >> j) & 1u) list[at++] = i0 + j;
 }
 
 // Kernel 1 (per listed particle): wall contacts of NORMAL particles whose DES
@@ -718,7 +754,8 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
          const uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched, uint8_t* __restrict__ wall_hit,
          const PairRec* __restrict__ prec,
          double* __restrict__ fc, double* __restrict__ tow, double* __restrict__ acc_old,
-         double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot) {
+         double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot,
+         CellOut cells) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
   if (me >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, me);
@@ -748,7 +785,7 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
   const double4 X = pos_c[me], V = vel_c[me];
   const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z};
   finish_particle<MODE>(p, me, st, x, v, w, X.w, V.w, W.w, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
-                        rot_acc_old, vslot);
+                        rot_acc_old, vslot, cells);
 }
 
 // CFUPDATEOLD + CFNEWVALUES from FC/TOW, in place; zeroes FC/TOW.
@@ -786,7 +823,8 @@ static void launch_walls_t(dem_handle* h) {
   const int c = h->cur;
   const int T = 128;
   cudaMemsetAsync(h->d_nwall, 0, sizeof(int), h->stream);
-  k_wall_list<<<(h->n + WALL_LIST_T - 1) / WALL_LIST_T, WALL_LIST_T, 0, h->stream>>>(
+  const int nq = (h->n + 3) / 4;  // four particles per thread
+  k_wall_list<<<(nq + WALL_LIST_T - 1) / WALL_LIST_T, WALL_LIST_T, 0, h->stream>>>(
       h->n, h->state, h->wall_cand, h->wall_live, h->wgap, h->skin, h->wall_list, h->d_nwall);
   // persistent: the resident blocks of the kernel's register budget
   k_walls<COLL, B><<<h->n_sm * 4, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->wall_list, h->d_nwall,
@@ -812,7 +850,7 @@ static void launch_gather_t(dem_handle* h) {
   k_gather<MODE, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
                                             h->vel4[1 - c], h->omg4[1 - c], h->state, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
                                             h->touched, h->wall_hit, h->prec, h->fc, h->tow, h->acc_old,
-                                            h->rot_acc_old, h->vslot);
+                                            h->rot_acc_old, h->vslot, gather_cells<MODE, B>(h));
   DEM_LAUNCH(h);
 }
 

@@ -206,7 +206,8 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
                const int2* __restrict__ in_pair, const uint8_t* __restrict__ pflag, uint8_t* __restrict__ touched,
                uint8_t* __restrict__ wall_hit,
                const PairRec32* __restrict__ prec, double* __restrict__ fc, double* __restrict__ tow,
-               double* __restrict__ acc_old, double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot) {
+               double* __restrict__ acc_old, double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot,
+         CellOut cells) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
   if (me >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, me);
@@ -278,7 +279,7 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
 #pragma unroll
   for (int c = 0; c < 3; ++c) { f[c] = f0[c] + F.value(c); t[c] = t0[c] + T.value(c); }
   finish_particle<MODE>(p, me, st, x, v, w, r, m, omoi, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
-                        rot_acc_old, vslot);
+                        rot_acc_old, vslot, cells);
 }
 
 template <int COLL, bool B>
@@ -305,7 +306,8 @@ static void launch_gather_split_t(dem_handle* h) {
   k_gather_split<MODE, B><<<G, T, 0, h->stream>>>(
       h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
       h->state, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
-      h->touched, h->wall_hit, (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old, h->vslot);
+      h->touched, h->wall_hit, (const PairRec32*)h->prec, h->fc, h->tow, h->acc_old, h->rot_acc_old, h->vslot,
+      gather_cells<MODE, B>(h));
   DEM_LAUNCH(h);
 }
 

@@ -97,13 +97,16 @@ template <bool B>
 __global__ void k_sorted_copy(DevParams p0, BatchView bv, int n, const int* __restrict__ n_exist,
                               const int* __restrict__ flist, const double4* __restrict__ pos4,
                               const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
-                              const int* __restrict__ fkey, double4* __restrict__ spos, int4* __restrict__ sinfo) {
+                              const int* __restrict__ fkey, double4* __restrict__ spos, float4* __restrict__ sposf,
+                              int4* __restrict__ sinfo) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n || q >= *n_exist) return;
   const int i = flist[q];
   const DevParams& p = sysp<B>(p0, bv, i);
   const int c = dg_pijk[i];
-  spos[q] = pos4[i];
+  const double4 x = pos4[i];
+  spos[q] = x;
+  sposf[q] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
   // the DES cell as (i, j, k), unpacked by every particle that scans this one
   sinfo[q] = make_int4(i, pack_ijk(dg_iof(p, c), dg_jof(p, c), dg_kof(p, c)), (int)state[i], fkey[i]);
 }
@@ -116,6 +119,9 @@ struct NeighFrame {
   double fr;
   int glo[3], ghi[3];  // search cells within reach, per axis
   double inv_l[3];     // 1 / period length of the periodic axes
+  float4 cpf;          // the particle's position and radius rounded to FP32
+  float frf, lf[3], inv_lf[3];  // FACTOR_RLM and the periods in FP32 (0: not periodic)
+  float tolf;          // rounding allowance of the FP32 pre-check (infinite: check off)
 };
 
 template <bool B>
@@ -128,6 +134,31 @@ __device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, 
   F.e1[0] = p.iend1; F.e1[1] = p.jend1; F.e1[2] = p.kend1;
   F.ncl[0] = p.iend1 - p.istart1 + 1; F.ncl[1] = p.jend1 - p.jstart1 + 1; F.ncl[2] = p.kend1 - p.kstart1 + 1;
   for (int ax = 0; ax < 3; ++ax) F.inv_l[ax] = (p.per[ax] && !(ax == 2 && p.no_k)) ? 1.0 / p.L[ax] : 0.0;
+  F.cpf = make_float4((float)cp.x, (float)cp.y, (float)cp.z, (float)cp.w);
+  F.frf = (float)p.factor_rlm;
+  // The FP32 pre-check's allowance.  For a neighbour (nearest-image distance
+  // at most the search radius sr <= FACTOR_RLM*(r + MAX_RADIUS)) each
+  // coordinate of the candidate is within sr of this particle's or of one
+  // of its periodic images k*L, so the rounding error of each axis's FP32
+  // separation -- the roundings of both coordinates, of the difference and
+  // of the image shift -- is below 2^-24 (2|x| + 4|k|L + 3 sr), under
+  // 2^-20 (|x| + sr + L) for |k| <= 4 (the wrap of every step keeps the
+  // positions within one period of the domain); the sum over the axes
+  // bounds the error of the distance.  A period below four search radii
+  // could let FP32 pick another image: the check is off there.
+  {
+    const float srm = (float)(p.factor_rlm * (cp.w + p.max_radius)) * 1.0001f;
+    float tol = 0.f;
+    bool off = false;
+    for (int ax = 0; ax < 3; ++ax) {
+      F.lf[ax] = F.inv_l[ax] != 0.0 ? (float)p.L[ax] : 0.f;
+      F.inv_lf[ax] = (float)F.inv_l[ax];
+      const float c = ax == 0 ? F.cpf.x : (ax == 1 ? F.cpf.y : F.cpf.z);
+      tol += 0x1p-20f * (fabsf(c) + srm + F.lf[ax]);
+      if (F.inv_l[ax] != 0.0 && p.L[ax] < 4.0 * (double)srm) off = true;
+    }
+    F.tolf = off ? INFINITY : tol;
+  }
   const double cpos[3] = {cp.x, cp.y, cp.z};
   const double mr = p.max_radius;
   for (int ax = 0; ax < 3; ++ax) {
@@ -198,7 +229,25 @@ __device__ __forceinline__ void neigh_run(const DevParams& p, const NeighFrame& 
 // in the reference's DES-grid stencil and within FACTOR_RLM*(r_l + r_i);
 // its row key (stencil rank << 27 | index) through *key.
 __device__ __forceinline__ bool neigh_test(const DevParams& p, const NeighFrame& F, const int4* __restrict__ sinfo,
-                                           const double4* __restrict__ spos, int q, uint32_t* key) {
+                                           const double4* __restrict__ spos, const float4* __restrict__ sposf, int q,
+                                           uint32_t* key) {
+  {
+    // most candidates are far out of reach, and FP32 copies of the two
+    // positions show it: the FP32 nearest-image distance less the frame's
+    // rounding allowance is a lower bound of the exact distance for any
+    // neighbour, so a candidate beyond the search radius by more than the
+    // allowance (and a relative 2e-5 for the FP32 radius, squares and sum)
+    // is no neighbour under any test below.  On an axis that is not
+    // periodic the image shift is 0 * 0.  A NaN compares false and falls
+    // through to the exact test.
+    const float4 f = sposf[q];
+    float e0 = F.cpf.x - f.x, e1 = F.cpf.y - f.y, e2 = F.cpf.z - f.z;
+    e0 = e0 - rintf(e0 * F.inv_lf[0]) * F.lf[0];
+    e1 = e1 - rintf(e1 * F.inv_lf[1]) * F.lf[1];
+    e2 = e2 - rintf(e2 * F.inv_lf[2]) * F.lf[2];
+    const float sr = F.frf * (F.cpf.w + f.w) + F.tolf;
+    if (e0 * e0 + e1 * e1 + e2 * e2 > sr * sr * 1.00002f) return false;
+  }
   const int4 o = sinfo[q];
   const int nb = o.x;
   if (nb == F.cur) return false;
@@ -255,6 +304,7 @@ __device__ __forceinline__ bool neigh_test(const DevParams& p, const NeighFrame&
 template <bool FILL, bool B>
 __global__ void __launch_bounds__(128)
 k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
+        const float4* __restrict__ sposf,
         const int4* __restrict__ sinfo, const int* __restrict__ fstart, const DevErr* __restrict__ err,
         int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
         uint8_t* __restrict__ rank_buf, int* __restrict__ owner, uint32_t* __restrict__ nslot, long long cap) {
@@ -289,7 +339,7 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
     neigh_run(p, F, fstart, r, qs, qe);
     for (int q = qs; q < qe; ++q) {
       uint32_t key;
-      if (!neigh_test(p, F, sinfo, spos, q, &key)) continue;
+      if (!neigh_test(p, F, sinfo, spos, sposf, q, &key)) continue;
       const int rank = (int)(key >> 27), nb = (int)(key & 0x7ffffffu);
       if (!FILL && cnt < NSLOT) {
         // keep the row sorted by (rank, index) in the slots
@@ -525,10 +575,10 @@ void launch_neigh_count(dem_handle* h) {
   const bool bt = h->batch();
   const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : h->dp.nfcell);
   if (bt)
-    k_neigh<false, true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sinfo, h->fcell_start,
+    k_neigh<false, true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start,
                                                  h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, h->nslot, 0);
   else
-    k_neigh<false, false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sinfo, h->fcell_start,
+    k_neigh<false, false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start,
                                                   h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, h->nslot, 0);
   DEM_LAUNCH(h);
 }
@@ -551,10 +601,10 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : p.nfcell);
   if (bt)
     k_sorted_copy<true><<<B, T, 0, h->stream>>>(p, bv, n, n_exist, h->fcell_list, h->pos4[h->cur], h->state,
-                                                h->dg_pijk, h->fcell_key, h->spos, h->sinfo);
+                                                h->dg_pijk, h->fcell_key, h->spos, h->sposf, h->sinfo);
   else
     k_sorted_copy<false><<<B, T, 0, h->stream>>>(p, bv, n, n_exist, h->fcell_list, h->pos4[h->cur], h->state,
-                                                 h->dg_pijk, h->fcell_key, h->spos, h->sinfo);
+                                                 h->dg_pijk, h->fcell_key, h->spos, h->sposf, h->sinfo);
   DEM_LAUNCH(h);
   if (int rc = check_cuda(h, cudaMemsetAsync(h->row_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
   launch_neigh_count(h);
@@ -577,14 +627,14 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   }
   const int TN = h->tune.neigh_threads, BN = (n + TN - 1) / TN;
   if (bt) {
-    k_neigh<true, true><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
+    k_neigh<true, true><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, e, h->row_cnt,
                                                   h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->nslot,
                                                   h->pair_cap);
     k_keep_rows<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], nullptr, h->row_end[nb],
                                               h->nbrs[nb], h->pair_owner, h->pair_cap);
     DEM_LAUNCH(h);
   } else {
-    k_neigh<true, false><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sinfo, h->fcell_start, e, h->row_cnt,
+    k_neigh<true, false><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, e, h->row_cnt,
                                                    h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->nslot,
                                                    h->pair_cap);
   }
