@@ -129,7 +129,8 @@ typedef struct dem_stats {
     double  bed_height;      /* mass-weighted mean y of NORMAL particles */
     double  s_time;          /* accumulated solids time S_TIME */
     int64_t n_outflow_removed; /* particles deleted by outflow boundaries so far */
-    double  reserved[3];
+    int64_t n_inflow_added;    /* particles seeded by mass-inflow boundaries so far */
+    double  reserved[2];
 } dem_stats;
 
 typedef struct dem_handle dem_handle;
@@ -293,6 +294,67 @@ typedef struct dem_outflow_bc {
  * search of that step.  Steps are then taken one at a time (no CUDA graph).
  * The boxes of the boundaries must not overlap. */
 int dem_set_outflow_bcs(dem_handle* h, const dem_outflow_bc* bcs, int32_t n);
+
+/* ---- mass inflow (model/des/mass_inflow_dem.f, layout_mi_dem.f) --------- */
+
+/* One mass-inflow boundary: the seeding layout LAYOUT_MI_DEM builds
+ * (DEM_MI(BCV_I), layout_mi_dem.f:96-420), the rate SET_BC_DEM_MI derives
+ * (PI_COUNT, PI_FACTOR, set_bc_dem_mi.f:180-205) and the box of DES cells
+ * SET_DEM_BCMI_IJK lists (set_bc_dem_mi.f:391-530).  The in-plane axes of
+ * P and Q are x and z for 'N'/'S', y and z for 'E'/'W', x and y for 'T'/'B'
+ * (SEED_NEW_PARTICLE, mass_inflow_dem.f:306-408). */
+typedef struct dem_inflow_bc {
+    int32_t plane;            /* BC_PLANE: 'N','S','E','W','T','B' */
+    int32_t occupants;        /* DEM_MI%OCCUPANTS: seeding windows */
+    int32_t vacancy;          /* DEM_MI%VACANCY: the next window, 1-based (1 after the layout) */
+    int32_t pi_count;         /* PI_COUNT: particles per injection (0: none) */
+    int32_t polydisperse;     /* DEM_MI%POLYDISPERSE */
+    int32_t n_layout;         /* entries of poly_layout (NUMFRAC_LIMIT = 10000 in the reference) */
+    int32_t dg_lo[3], dg_hi[3];   /* DES-cell box of the entering test (DEM_BCMI_IJK) */
+    int32_t reserved_i[4];
+    double  offset;           /* DEM_MI%OFFSET: the seeding coordinate along the normal */
+    double  window;           /* DEM_MI%WINDOW */
+    double  face;             /* plane of the entering test: YN(BC_J_s) for 'N', YN(BC_J_s-1) for 'S',
+                                 XE(BC_I_w) for 'E', XE(BC_I_w-1) for 'W', ZT(BC_K_b) for 'T',
+                                 ZT(BC_K_b-1) for 'B' (mass_inflow_dem.f:118-125) */
+    double  pi_factor;        /* PI_FACTOR: solids steps per injection */
+    double  mi_time;          /* DEM_MI_TIME: solids time of the next injection */
+    double  start_time;       /* BC_MI_START_TIME */
+    double  end_time;         /* BC_MI_END_TIME */
+    const double*  p;         /* [occupants] DEM_MI%P: window corners on the first in-plane axis */
+    const double*  q;         /* [occupants] DEM_MI%Q: on the second (ignored when NO_K) */
+    const int32_t* poly_layout;   /* [n_layout] DEM_BC_POLY_LAYOUT: solids phase (1-based) per slot */
+    double  d_p0[DEM_MAX_PHASES];   /* D_P0 of each phase */
+    double  ro_s0[DEM_MAX_PHASES];  /* RO_S0 of each phase */
+    double  vel[DEM_MAX_PHASES][3]; /* BC_U_s, BC_V_s, BC_W_s of each phase */
+    double  reserved_d[4];
+} dem_inflow_bc;
+
+/* Installs the mass-inflow boundaries (n = 0 removes them; the arrays are
+ * copied).  Each DES_TIME_STEP then runs MASS_INFLOW_DEM after CFNEWVALUES
+ * and before MASS_OUTFLOW_DEM (des_time_march.f:404-405): ENTERING
+ * particles of a boundary's cells that are clear of its plane by more than
+ * their radius become NORMAL, and, once the solids time reaches DEM_MI_TIME
+ * inside [BC_MI_START_TIME, BC_MI_END_TIME], PI_COUNT particles are seeded
+ * in successive windows of the layout (random offsets inside the window,
+ * the boundary's velocity, ENTERING) into the first NONEXISTENT slots, and
+ * DEM_MI_TIME advances by PI_FACTOR*DTSOLID.  Each boundary draws three
+ * uniform numbers per call, as RANDOM_NUMBER(RAND) does: first from the
+ * queue that dem_push_inflow_random fills, then from the handle's own
+ * generator (splitmix64 from `seed`).  DEM_ERR_CAPACITY when the handle has
+ * no NONEXISTENT slot left.  Steps are then taken one at a time (no CUDA
+ * graph); not available on a batch handle. */
+int dem_set_inflow_bcs(dem_handle* h, const dem_inflow_bc* bcs, int32_t n, uint64_t seed);
+
+/* Queues n uniform numbers in [0,1) for the inflow boundaries, in the order
+ * MASS_INFLOW_DEM draws them (three per boundary per step): a Fortran host
+ * passes the values of its own RANDOM_NUMBER stream to seed exactly as the
+ * reference does. */
+int dem_push_inflow_random(dem_handle* h, const double* r, int64_t n);
+
+/* The current DEM_MI%VACANCY and DEM_MI_TIME of inflow boundary `bc`
+ * (0-based), for restart files (read_res0_des.f:217). */
+int dem_get_inflow_state(dem_handle* h, int32_t bc, int32_t* vacancy, double* mi_time);
 
 /* ---- particle output (model/des/vtp_mod.f) ------------------------------- */
 

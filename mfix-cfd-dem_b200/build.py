@@ -38,6 +38,7 @@ SOURCES = {
     "res_des.cu": [],
     "vtp.cu": [],
     "outflow.cu": ["-fmad=false"],
+    "inflow.cu": ["-fmad=false"],
 }
 HEADERS = ["dem_internal.cuh"]
 

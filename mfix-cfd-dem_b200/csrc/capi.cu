@@ -112,6 +112,7 @@ int fetch_errors(dem_handle* h) {
   if (f & EF_WALL_SLOTS) return set_err(h, DEM_ERR_WALL_SLOTS, "Error: COLLISION_ARRAY_MAX too small.");
   if (f & EF_ROGUE_FATAL) return set_err(h, DEM_ERR_ROGUE, "NORMAL particle found in GHOST cell (remove_rogue = 0)");
   if (f & EF_PAIR_CAP) return set_err(h, DEM_ERR_PAIR_OVERFLOW, "pair list capacity exceeded");
+  if (f & EF_INFLOW_CAP) return set_err(h, DEM_ERR_CAPACITY, "no NONEXISTENT slot left for an inflow particle (MAX_PIP)");
   return set_err(h, DEM_ERR_STATE, "device error flags set");
 }
 
@@ -490,7 +491,7 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->skin, h->vslot, h->pgap,
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->d_ibc, h->pic_fresh, h->d_seed, h->skin, h->vslot, h->pgap,
                   h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -720,6 +721,7 @@ static int step_once(dem_handle* h, int nn) {
   bool force = false;
   if (h->obc.empty()) {
     if (int rc = run_force(h, true)) return rc;
+    if (int rc = run_mass_inflow(h)) return rc;  // MASS_INFLOW_DEM
   } else {
     // outflow boundaries: forces, then exit velocities + CFNEWVALUES +
     // MASS_OUTFLOW_DEM, whose deletions force the neighbour search
@@ -728,7 +730,7 @@ static int step_once(dem_handle* h, int nn) {
   }
   const bool do_nsearch = (nn == 1) || (nn % h->prm.neighbor_search_n == 0) || force;
   // the integrating gather of a periodic system already placed the particles
-  const bool placed = h->obc.empty() && cells_in_gather(h);
+  const bool placed = cells_in_gather(h);
   if (do_nsearch || (anyper && !placed)) {
     if (int rc = run_desgrid_pic(h, do_nsearch)) return rc;
   }
@@ -804,7 +806,7 @@ int dem_step(dem_handle* h, int32_t nn_first, int32_t nsteps) {
   if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
   if (nsteps < 0 || nn_first < 1) return set_err(h, DEM_ERR_ARG, "bad step range");
   const int nsn = h->prm.neighbor_search_n;
-  const bool graphs_ok = h->stream != nullptr && !h->prof && !h->no_graphs && h->obc.empty();
+  const bool graphs_ok = h->stream != nullptr && !h->prof && !h->no_graphs && h->obc.empty() && h->ibc.empty();
   int k = 0;
   while (k < nsteps) {
     const int nn = nn_first + k;
@@ -838,6 +840,7 @@ int dem_get_stats(dem_handle* h, dem_stats* s) {
   s->n_wall_contacts = (int64_t)h->herr->n_wall_contacts;
   s->n_rogue_removed = (int64_t)h->herr->rogue_removed;
   s->n_outflow_removed = (int64_t)h->herr->outflow_removed;
+  s->n_inflow_added = (int64_t)h->inflow_added;
   s->steps_done = h->steps_done;
   s->s_time = h->s_time;
   return 0;

@@ -756,6 +756,7 @@ int dem_step_coupled(dem_handle* h, int32_t nn_first, int32_t nsteps) {
     bool force = false;
     if (h->obc.empty()) {
       if (int rc = run_cfnewvalues(h)) return rc;             // CFUPDATEOLD + CFNEWVALUES
+      if (int rc = run_mass_inflow(h)) return rc;             // MASS_INFLOW_DEM
     } else if (int rc = run_cfnewvalues_outflow(h, &force)) { // + exit velocities, MASS_OUTFLOW_DEM
       return rc;
     }

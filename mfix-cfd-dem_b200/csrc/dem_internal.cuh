@@ -18,6 +18,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <deque>
 #include <string>
 #include <vector>
 
@@ -37,6 +38,7 @@ enum : unsigned {
   EF_ROGUE_FATAL = 1u << 3,
   EF_CELL_CAP    = 1u << 4,
   EF_NONFINITE   = 1u << 5,
+  EF_INFLOW_CAP  = 1u << 6,   // fewer NONEXISTENT slots than particles to seed
 };
 
 // Per-pair flag bits (pflag) between force passes.
@@ -256,6 +258,23 @@ struct dem_handle {
   std::vector<dem_outflow_bc> obc;
   dem_outflow_bc* d_obc = nullptr;
   bool exit_first_pass = true;
+  // mass-inflow boundaries (single handles): host copies with their layout
+  // arrays, the device copy (membership and entering test), the queue and
+  // generator of the uniform numbers, the particles seeded since the last
+  // DESGRID_PIC (not yet in its cell lists) and the seed records
+  struct Inflow {
+    dem_inflow_bc bc;
+    std::vector<double> p, q;
+    std::vector<int32_t> layout;
+  };
+  std::vector<Inflow> ibc;
+  dem_inflow_bc* d_ibc = nullptr;
+  std::deque<double> irand;
+  uint64_t irng = 0;
+  uint8_t* pic_fresh = nullptr;
+  void* d_seed = nullptr;
+  int seed_cap = 0;
+  long long inflow_added = 0;
   int* d_nwall = nullptr;       // their count
   double* wf = nullptr;       // [i][6] wall force and torque of the last force pass (valid with wall_hit)
 
@@ -315,6 +334,7 @@ void launch_skin(dem_handle* h);               // force.cu: adds the step's disp
 void skin_unknown(dem_handle* h);              // force.cu: positions changed from outside: no pair skipped
 void launch_wall_gaps(dem_handle* h);          // force.cu: wall clearances at a build (with the pair gaps)
 int run_cfnewvalues_outflow(dem_handle* h, bool* force_nsearch);  // outflow.cu: exit velocities, CFNEWVALUES, MASS_OUTFLOW_DEM
+int run_mass_inflow(dem_handle* h);  // inflow.cu: MASS_INFLOW_DEM (entering test, seeding)
 void launch_wall_cand(dem_handle* h);          // desgrid.cu: facet-cell flag of every particle
 void launch_pairs_only(dem_handle* h);         // force.cu: pair kernel of the handle's precision
 void launch_gather_only(dem_handle* h);        // force.cu: gather kernel, forces into FC/TOW
@@ -542,7 +562,9 @@ namespace demb {
 // neighbour-search steps, where it repeats the same placement).
 inline bool cells_in_gather(const dem_handle* h) {
   const DevParams& p = h->dp;
-  return !h->batch() && (p.per[0] || p.per[1] || (p.per[2] && !p.no_k));
+  // not with flow boundaries: their cell tests read the cells of the last
+  // DESGRID_PIC, which the placement would move ahead
+  return !h->batch() && h->obc.empty() && h->ibc.empty() && (p.per[0] || p.per[1] || (p.per[2] && !p.no_k));
 }
 template <int MODE, bool B>
 inline CellOut gather_cells(const dem_handle* h) {

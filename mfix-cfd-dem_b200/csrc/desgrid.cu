@@ -118,6 +118,8 @@ int run_desgrid_pic(dem_handle* h, bool bin_search) {
     k_cell_keys<false><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk, h->fbin_start,
                                                h->wall_cand);
   DEM_LAUNCH(h);
+  // particles seeded since the last DESGRID_PIC are in its cell lists now
+  if (h->pic_fresh && !h->ibc.empty()) cudaMemsetAsync(h->pic_fresh, 0, (size_t)n, h->stream);
   if (!bin_search) return check_cuda(h, cudaGetLastError(), "k_cell_keys");
   if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * nfc, h->stream), "memset")) return rc;
   if (bt) k_fine_keys<true><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->fcell_key, h->fcell_cnt);

@@ -180,6 +180,7 @@ int run_cfnewvalues_outflow(dem_handle* h, bool* force_nsearch) {
   launch_skin(h);
   h->first_pass = false;
   h->exit_first_pass = false;
+  if (int rc = run_mass_inflow(h)) return rc;  // MASS_INFLOW_DEM comes before MASS_OUTFLOW_DEM
   unsigned long long before = 0, after = 0;
   cudaMemcpyAsync(&before, &h->derr->outflow_removed, sizeof before, cudaMemcpyDeviceToHost, h->stream);
   k_mass_outflow<<<G, T, 0, h->stream>>>(h->dp, h->d_obc, nbc, h->dg_pijk, h->pos4[c], h->vel4[c], h->omg4[c],

@@ -110,7 +110,8 @@ class DemStats(C.Structure):
         ("bed_height", C.c_double),
         ("s_time", C.c_double),
         ("n_outflow_removed", C.c_int64),
-        ("reserved", C.c_double * 3),
+        ("n_inflow_added", C.c_int64),
+        ("reserved", C.c_double * 2),
     ]
 
     def as_dict(self):
@@ -222,6 +223,34 @@ class DemOutflowBC(C.Structure):
     ]
 
 
+class DemInflowBC(C.Structure):
+    _fields_ = [
+        ("plane", C.c_int32),
+        ("occupants", C.c_int32),
+        ("vacancy", C.c_int32),
+        ("pi_count", C.c_int32),
+        ("polydisperse", C.c_int32),
+        ("n_layout", C.c_int32),
+        ("dg_lo", C.c_int32 * 3),
+        ("dg_hi", C.c_int32 * 3),
+        ("reserved_i", C.c_int32 * 4),
+        ("offset", C.c_double),
+        ("window", C.c_double),
+        ("face", C.c_double),
+        ("pi_factor", C.c_double),
+        ("mi_time", C.c_double),
+        ("start_time", C.c_double),
+        ("end_time", C.c_double),
+        ("p", C.POINTER(C.c_double)),
+        ("q", C.POINTER(C.c_double)),
+        ("poly_layout", C.POINTER(C.c_int32)),
+        ("d_p0", C.c_double * DEM_MAX_PHASES),
+        ("ro_s0", C.c_double * DEM_MAX_PHASES),
+        ("vel", (C.c_double * 3) * DEM_MAX_PHASES),
+        ("reserved_d", C.c_double * 4),
+    ]
+
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -243,6 +272,9 @@ SIGNATURES = {
     "upload_pairs": (C.c_int, [_P, _I32, _I32, _D, C.c_int64, C.c_int32]),
     "download_wall_history": (C.c_int, [_P, _I32, _D, C.c_int32]),
     "set_outflow_bcs": (C.c_int, [_P, C.c_void_p, C.c_int32]),
+    "set_inflow_bcs": (C.c_int, [_P, C.c_void_p, C.c_int32, C.c_uint64]),
+    "push_inflow_random": (C.c_int, [_P, _D, C.c_int64]),
+    "get_inflow_state": (C.c_int, [_P, C.c_int32, _I32, _D]),
     "upload_wall_history": (C.c_int, [_P, _I32, _D, C.c_int32]),
     "download_cells": (C.c_int, [_P, _I32, C.c_int32]),
     "desgrid_pic": (C.c_int, [_P]),

@@ -20,6 +20,7 @@ widened to double): FACTOR_RLM = 1.2 (line 1169) and KT_FAC = KT_W_FAC =
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
@@ -496,4 +497,109 @@ def outflow_bc(prm, plane: str, lo, hi, face: float, mass_outflow: bool = False,
     for m, v in enumerate(vel or []):
         for c in range(3):
             b.vel[m][c] = float(v[c])
+    return b
+
+
+def inflow_bc(prm, plane: str, lo, hi, d_p0, ro_s0, vel, pi_count: int, pi_factor: float,
+              min_radius: float, max_radius: float, face=None, phases=(1,), mi_time: float = 0.0,
+              start_time: float = 0.0, end_time: float = 1.0e30, layout_seed: int = 0):
+    """A dem_inflow_bc for a boundary with extents lo..hi (BC_X_w/BC_Y_s/BC_Z_b ..
+    BC_X_e/BC_Y_n/BC_Z_t) on plane `plane`.
+
+    The seeding layout follows LAYOUT_DEM_MI_NS/_EW (layout_mi_dem.f:96-420)
+    for a boundary with no excluded cells and no STL facets across it: WMAX x
+    HMAX windows of width WINDOW = min(PLEN/WMAX, QLEN/HMAX), centred on the
+    boundary, OFFSET one largest diameter off the plane; the windows are
+    visited in a seeded random order (the reference draws that permutation
+    with RANDOM_NUMBER).  The DES-cell box of the entering test is
+    SET_DEM_BCMI_IJK's (set_bc_dem_mi.f:466-522).  d_p0, ro_s0 and vel are per
+    phase (vel: BC_U_s, BC_V_s, BC_W_s); `phases` are the 1-based phases
+    injected (one entry: monodisperse; several: a DEM_BC_POLY_LAYOUT of 10000
+    slots split equally).  `face` defaults to the plane's coordinate.  The
+    returned structure keeps its layout arrays alive."""
+    import numpy as np
+    from . import abi
+    b = abi.DemInflowBC()
+    b.plane = ord(plane)
+    normal = {"N": 1, "S": 1, "E": 0, "W": 0, "T": 2, "B": 2}[plane]
+    pa, qa = {1: (0, 2), 0: (1, 2), 2: (0, 1)}[normal]
+    do_k = not prm.no_k
+    max_dia = max(float(d_p0[m - 1]) for m in phases)
+    plen = float(hi[pa] - lo[pa])
+    wmax = int(math.floor(float(np.float32(plen / max_dia))))
+    if qa == 2 and not do_k:
+        qlen = max_dia
+    else:
+        qlen = float(hi[qa] - lo[qa])
+    hmax = int(math.floor(float(np.float32(qlen / max_dia))))
+    if wmax < 1 or hmax < 1:
+        raise ValueError("inflow boundary narrower than the largest diameter")
+    shift = -1.0 if plane in ("N", "E", "T") else 1.0
+    b.offset = float(lo[normal]) + max_dia * shift
+    window = min(plen / wmax, qlen / hmax)
+    b.window = window
+    mp0 = float(lo[pa]) + 0.5 * (plen - wmax * window)
+    mesh_p = [mp0 + (lc - 1) * window for lc in range(1, wmax + 1)]
+    if qa == 2 and not do_k:
+        mesh_q = [0.0]
+    else:
+        mq0 = float(lo[qa]) + 0.5 * (qlen - hmax * window)
+        mesh_q = [mq0 + (lc - 1) * window for lc in range(1, hmax + 1)]
+    occ = wmax * hmax
+    perm = np.random.default_rng(layout_seed).permutation(occ)  # RAND_MAP, 0-based
+    P = np.zeros(occ)
+    Q = np.zeros(occ)
+    lc = 0
+    for h in range(hmax):
+        for w in range(wmax):
+            ll = perm[lc]
+            P[ll] = mesh_p[w]
+            Q[ll] = mesh_q[h] if len(mesh_q) > h else mesh_q[0]
+            lc += 1
+    b.occupants = occ
+    b.vacancy = 1
+    b.pi_count = int(pi_count)
+    b.pi_factor = float(pi_factor)
+    b.mi_time = float(mi_time)
+    b.start_time = float(start_time)
+    b.end_time = float(end_time)
+    if len(phases) > 1:
+        layout = np.repeat(np.asarray(phases, dtype=np.int32), -(-10000 // len(phases)))[:10000].copy()
+        b.polydisperse = 1
+    else:
+        layout = np.asarray([phases[0]], dtype=np.int32)
+        b.polydisperse = 0
+    b.n_layout = int(layout.size)
+    P = np.ascontiguousarray(P)
+    Q = np.ascontiguousarray(Q)
+    b.p = P.ctypes.data_as(C.POINTER(C.c_double))
+    b.q = Q.ctypes.data_as(C.POINTER(C.c_double))
+    b.poly_layout = layout.ctypes.data_as(C.POINTER(C.c_int32))
+    b._keep = (P, Q, layout)
+    for m in range(len(d_p0)):
+        b.d_p0[m] = float(d_p0[m])
+        b.ro_s0[m] = float(ro_s0[m])
+        for c in range(3):
+            b.vel[m][c] = float(vel[m][c])
+    # SET_DEM_BCMI_IJK: IofbcPOS is NINT-based, IofPOS FLOOR-based; 1-based
+    # with one ghost layer (interior 2..dg_imax+1)
+    start = (prm.dg_xstart, prm.dg_ystart, prm.dg_zstart)
+    inv = (prm.dg_dxinv, prm.dg_dyinv, prm.dg_dzinv)
+    nmax = (prm.dg_imax, prm.dg_jmax, prm.dg_kmax)
+    for a in range(3):
+        if a == 2 and not do_k:
+            b.dg_lo[2] = b.dg_hi[2] = 1
+            continue
+        if a == normal:
+            ofpos = lambda x: int(math.floor((x - start[a]) * inv[a])) + 2
+            if shift < 0:   # 'N', 'E', 'T'
+                b.dg_lo[a] = ofpos(lo[a] + min_radius)
+                b.dg_hi[a] = ofpos(hi[a] + max_radius)
+            else:
+                b.dg_lo[a] = ofpos(lo[a] - max_radius)
+                b.dg_hi[a] = ofpos(hi[a] - min_radius)
+        else:
+            b.dg_lo[a] = max(_nint((lo[a] - start[a]) * inv[a]) + 1 - 1, 2)
+            b.dg_hi[a] = min(_nint((hi[a] - start[a]) * inv[a]) + 1 + 1, nmax[a] + 1)
+    b.face = float(lo[normal] if face is None else face)
     return b

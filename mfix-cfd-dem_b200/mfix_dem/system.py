@@ -181,6 +181,26 @@ class DemSystem:
         arr = (abi.DemOutflowBC * max(len(bcs), 1))(*bcs)
         self._call("set_outflow_bcs", self._h, C.cast(arr, C.c_void_p), C.c_int32(len(bcs)))
 
+    def set_inflow_bcs(self, bcs, seed: int = 0):
+        """The DEM mass-inflow boundaries (abi.DemInflowBC, e.g. from
+        params.inflow_bc); `seed` starts the handle's generator of the
+        uniform numbers MASS_INFLOW_DEM draws.  An empty list removes them."""
+        arr = (abi.DemInflowBC * max(len(bcs), 1))(*bcs)
+        self._call("set_inflow_bcs", self._h, C.cast(arr, C.c_void_p), C.c_int32(len(bcs)), C.c_uint64(seed))
+
+    def push_inflow_random(self, r):
+        """Queue uniform numbers for the inflow boundaries (three per
+        boundary per step, in boundary order), used before the generator."""
+        a = np.ascontiguousarray(r, dtype=np.float64).ravel()
+        self._call("push_inflow_random", self._h, _dp(a), C.c_int64(a.size))
+
+    def inflow_state(self, bc: int):
+        """(DEM_MI%VACANCY, DEM_MI_TIME) of inflow boundary `bc` (0-based)."""
+        v = C.c_int32()
+        t = C.c_double()
+        self._call("get_inflow_state", self._h, C.c_int32(bc), C.byref(v), C.byref(t))
+        return int(v.value), float(t.value)
+
     def download_cells(self):
         cells = np.empty(self.n, dtype=np.int32)
         self._call("download_cells", self._h, _ip(cells), C.c_int32(self.n))

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <deque>
 #include <vector>
 #include <cfloat>
 #ifdef _OPENMP
@@ -102,6 +103,11 @@ struct Oracle {
   std::vector<double> vel_old;             // DES_VEL_OLD when outflow boundaries are set
   bool exit_first_pass = true;             // UPDATE_EXIT_DES_VEL's own FIRST_PASS
   int64_t n_outflow_deleted = 0;
+  struct Inflow { dem_inflow_bc bc; std::vector<double> p, q; std::vector<int32_t> layout; };
+  std::vector<Inflow> ibc;                 // DEM mass-inflow boundaries (DEM_BCMI_MAP order)
+  std::deque<double> irand;                // queued RANDOM_NUMBER values
+  uint64_t irng = 0;                       // splitmix64 state when the queue is empty
+  int64_t n_inflow_added = 0;
   std::vector<double> drag_am, drag_bm, f_gds;  // DRAG_AM, DRAG_BM(:,3), F_GDS
   std::vector<int> pijk;                  // (n,4): i, j, k, ijk (1-based), 0 = none
   std::vector<double> f_gp;               // F_GP(n)
@@ -1324,7 +1330,9 @@ struct Oracle {
     int rc = calc_force();
     if (rc) return rc;
     if (g.interp_scheme == DEM_INTERP_NONE) drag_des1(); else drag();   // CALC_DRAG_DES
-    const bool force = integrate_with_outflow();
+    bool ok = true;
+    const bool force = integrate_with_outflow(&ok);
+    if (!ok) return fail(DEM_ERR_CAPACITY, "no NONEXISTENT slot left for an inflow particle (MAX_PIP)");
     bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0) || force;
     bool anyper = p.periodic[0] || p.periodic[1] || (p.periodic[2] && !p.no_k);
     if (do_nsearch || anyper) desgrid_pic();
@@ -1423,22 +1431,124 @@ struct Oracle {
     return force;
   }
 
+  // Inflow boundaries ------------------------------------------------
+  double next_rand() {
+    if (!irand.empty()) { const double r = irand.front(); irand.pop_front(); return r; }
+    // splitmix64, 53 bits in [0,1)
+    uint64_t z = (irng += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * 0x1.0p-53;
+  }
+
+  // MASS_INFLOW_DEM (mass_inflow_dem.f:44-293) for plain spheres: per
+  // boundary, the entering test over the DG_PIC lists of its cells
+  // (82-140), RAND(3), the time window, then PI_COUNT particles from
+  // SEED_NEW_PARTICLE (306-408) and SET_NEW_PARTICLE_PROPS (419-642) into
+  // the first NONEXISTENT slots from LS = 1 on, and DEM_MI_TIME advanced.
+  // Returns false when no NONEXISTENT slot is left.
+  bool mass_inflow() {
+    int ls = 0;
+    for (Inflow& I : ibc) {
+      dem_inflow_bc& b = I.bc;
+      const int idx = (b.plane == 'N' || b.plane == 'S') ? 1 : ((b.plane == 'E' || b.plane == 'W') ? 0 : 2);
+      for (int lk = b.dg_lo[2]; lk <= b.dg_hi[2]; ++lk)
+        for (int li = b.dg_lo[0]; li <= b.dg_hi[0]; ++li)
+          for (int lj = b.dg_lo[1]; lj <= b.dg_hi[1]; ++lj) {
+            const int c = funijk(li, lj, lk) - 1;
+            if (c < 0 || c >= ncell2 || cell_start.empty()) continue;
+            for (int e = cell_start[c]; e < cell_start[c + 1]; ++e) {
+              const int np = cell_list[e];
+              if (state[np] == DEM_STATE_EXITING) continue;
+              const double x = P(pos, np, idx);
+              const double dist = (b.plane == 'N' || b.plane == 'E' || b.plane == 'T') ? x - b.face : b.face - x;
+              if (dist > rad[np] && state[np] == DEM_STATE_ENTERING) state[np] = DEM_STATE_NORMAL;
+            }
+          }
+      double rnd[3];
+      for (double& r : rnd) r = next_rand();
+      if (b.mi_time > s_time) continue;
+      if (s_time < b.start_time || s_time > b.end_time) continue;
+      for (int ip = 0; ip < b.pi_count; ++ip) {
+        const int vac = b.vacancy;
+        b.vacancy = vac % b.occupants + 1;
+        int m1;
+        if (b.polydisperse) {
+          int ri = (int)std::ceil((double)b.n_layout * rnd[0]);
+          ri = std::min(std::max(ri, 1), b.n_layout);
+          m1 = I.layout[ri - 1];
+        } else {
+          m1 = I.layout[0];
+        }
+        const int m = m1 - 1;
+        const double d = b.d_p0[m];
+        const double rand1 = 0.5 * d + (b.window - d) * rnd[0];
+        const double rand2 = 0.5 * d + (b.window - d) * rnd[1];
+        double x[3];
+        const double pv = I.p[vac - 1] + rand1, qv = I.q[vac - 1] + rand2;
+        switch (b.plane) {
+          case 'N': case 'S': x[0] = pv; x[2] = qv; x[1] = b.offset; break;
+          case 'E': case 'W': x[1] = pv; x[2] = qv; x[0] = b.offset; break;
+          default: x[0] = pv; x[1] = qv; x[2] = b.offset; break;
+        }
+        if (p.no_k) x[2] = 0.0;
+        const int li = iofpos(x[0]), lj = jofpos(x[1]), lk = kofpos(x[2]);
+        // one rank: DG_ISTART..DG_IEND span the ghost layers (desgrid_mod.f:756-761)
+        bool owns = istart2 <= li && li <= iend2 && jstart2 <= lj && lj <= jend2;
+        if (!p.no_k) owns = owns && kstart2 <= lk && lk <= kend2;
+        if (!owns) continue;
+        while (ls < n && state[ls] != DEM_STATE_NONEXISTENT) ++ls;
+        if (ls >= n) return false;
+        const int np = ls;
+        state[np] = DEM_STATE_ENTERING;
+        for (int c = 0; c < 3; ++c) {
+          X(pos, c)[np] = x[c];
+          X(vel, c)[np] = b.vel[m][c];
+          X(omg, c)[np] = 0.0;
+        }
+        rad[np] = d * 0.5;
+        const double pvol = (4.0 / 3.0) * M_PI * (rad[np] * rad[np] * rad[np]);
+        pmass[np] = pvol * b.ro_s0[m];
+        omoi[np] = 2.5 / (pmass[np] * (rad[np] * rad[np]));
+        phase[np] = m;
+        const int ci = std::min(iend2, std::max(istart2, li));
+        const int cj = std::min(jend2, std::max(jstart2, lj));
+        const int ck = p.no_k ? 1 : std::min(kend2, std::max(kstart2, lk));
+        dg_pijk[np] = funijk(ci, cj, ck);
+        n_inflow_added++;
+      }
+      b.mi_time = b.mi_time + b.pi_factor * p.dtsolid;
+    }
+    return true;
+  }
+
   // The part of DES_TIME_STEP between the forces and the neighbour search
-  // with outflow boundaries: CFUPDATEOLD's DES_VEL_OLD, UPDATE_EXIT_DES_VEL,
-  // CFNEWVALUES, MASS_OUTFLOW_DEM.  Returns FORCE_NSEARCH.
-  bool integrate_with_outflow() {
-    if (obc.empty()) { cfnewvalues(); return false; }
+  // with flow boundaries: CFUPDATEOLD's DES_VEL_OLD, UPDATE_EXIT_DES_VEL,
+  // CFNEWVALUES, MASS_INFLOW_DEM, MASS_OUTFLOW_DEM.  Returns FORCE_NSEARCH;
+  // *ok turns false when an inflow particle found no slot.
+  bool integrate_with_outflow(bool* ok = nullptr) {
+    if (obc.empty()) {
+      cfnewvalues();
+      const bool seeded = ibc.empty() || mass_inflow();
+      if (ok) *ok = seeded;
+      return false;
+    }
     vel_old = vel;
     update_exit_vel();
     cfnewvalues();
     vel_old.clear();
+    const bool seeded = ibc.empty() || mass_inflow();
+    if (ok) *ok = seeded;
     return mass_outflow();
   }
 
   int step(int nn) {
     int rc = calc_force();
     if (rc) return rc;
-    const bool force = integrate_with_outflow();
+    bool ok = true;
+    const bool force = integrate_with_outflow(&ok);
+    if (!ok) return fail(DEM_ERR_CAPACITY, "no NONEXISTENT slot left for an inflow particle (MAX_PIP)");
     bool do_nsearch = (nn == 1) || (nn % p.neighbor_search_n == 0) || force;
     bool anyper = p.periodic[0] || p.periodic[1] || (p.periodic[2] && !p.no_k);
     if (do_nsearch || anyper) desgrid_pic();
@@ -1616,6 +1726,56 @@ int orc_set_outflow_bcs(orc_handle* h, const dem_outflow_bc* bcs, int32_t n) {
   return 0;
 }
 
+int orc_set_inflow_bcs(orc_handle* h, const dem_inflow_bc* bcs, int32_t n, uint64_t seed) {
+  Oracle& o = h->o;
+  if (n < 0 || (n > 0 && !bcs)) return o.fail(DEM_ERR_ARG, "bad inflow boundaries");
+  for (int32_t i = 0; i < n; ++i) {
+    const dem_inflow_bc& b = bcs[i];
+    const int pl = b.plane;
+    if (pl != 'N' && pl != 'S' && pl != 'E' && pl != 'W' && pl != 'T' && pl != 'B')
+      return o.fail(DEM_ERR_ARG, "unknown BC_PLANE");
+    if (b.pi_count < 0 || (b.pi_count > 0 && (b.occupants < 1 || !b.p || !b.q)))
+      return o.fail(DEM_ERR_ARG, "inflow layout missing");
+    if (b.vacancy < 1 || (b.occupants > 0 && b.vacancy > b.occupants))
+      return o.fail(DEM_ERR_ARG, "inflow vacancy out of range");
+    if (b.n_layout < 1 || !b.poly_layout) return o.fail(DEM_ERR_ARG, "inflow phase layout missing");
+    for (int32_t j = 0; j < b.n_layout; ++j)
+      if (b.poly_layout[j] < 1 || b.poly_layout[j] > o.p.n_phases) return o.fail(DEM_ERR_ARG, "inflow phase out of range");
+    for (int a = 0; a < 3; ++a)
+      if (b.dg_lo[a] > b.dg_hi[a]) return o.fail(DEM_ERR_ARG, "empty DES-cell box");
+    if (!(b.pi_factor > 0.0) && b.pi_count > 0) return o.fail(DEM_ERR_ARG, "PI_FACTOR must be positive");
+  }
+  o.ibc.clear();
+  o.irand.clear();
+  o.irng = seed;
+  for (int32_t i = 0; i < n; ++i) {
+    Oracle::Inflow I;
+    I.bc = bcs[i];
+    const int occ = bcs[i].pi_count > 0 ? bcs[i].occupants : 0;
+    I.p.assign(bcs[i].p, bcs[i].p + occ);
+    I.q.assign(bcs[i].q, bcs[i].q + occ);
+    I.layout.assign(bcs[i].poly_layout, bcs[i].poly_layout + bcs[i].n_layout);
+    I.bc.p = nullptr; I.bc.q = nullptr; I.bc.poly_layout = nullptr;
+    o.ibc.push_back(std::move(I));
+  }
+  return 0;
+}
+
+int orc_push_inflow_random(orc_handle* h, const double* r, int64_t n) {
+  Oracle& o = h->o;
+  if (n < 0 || (n > 0 && !r)) return o.fail(DEM_ERR_ARG, "bad random numbers");
+  o.irand.insert(o.irand.end(), r, r + n);
+  return 0;
+}
+
+int orc_get_inflow_state(orc_handle* h, int32_t bc, int32_t* vacancy, double* mi_time) {
+  Oracle& o = h->o;
+  if (bc < 0 || bc >= (int32_t)o.ibc.size()) return o.fail(DEM_ERR_ARG, "no such inflow boundary");
+  if (vacancy) *vacancy = o.ibc[bc].bc.vacancy;
+  if (mi_time) *mi_time = o.ibc[bc].bc.mi_time;
+  return 0;
+}
+
 int orc_download_cells(orc_handle* h, int32_t* cells, int32_t max_pip) {
   Oracle& o = h->o;
   if (max_pip != o.n) return DEM_ERR_ARG;
@@ -1680,6 +1840,7 @@ int orc_get_stats(orc_handle* h, dem_stats* s) {
   for (int c = 0; c < 3; ++c) { s->mean_vel[c] = mv[c]; s->gran_temp[c] = nn ? gt[c] / nn : 0.0; }
   s->n_normal = nn;
   s->n_outflow_removed = o.n_outflow_deleted;
+  s->n_inflow_added = o.n_inflow_added;
   s->n_pairs = (int64_t)o.nbrs.size();
   s->n_contacts = o.n_contacts;
   s->n_wall_contacts = o.n_wall_contacts;

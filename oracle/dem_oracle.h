@@ -50,6 +50,9 @@ int  orc_upload_pairs(orc_handle* h, const int32_t* neighbor_index, const int32_
 int  orc_download_wall_history(orc_handle* h, int32_t* facet_id, double* pft, int32_t max_pip);
 int  orc_upload_wall_history(orc_handle* h, const int32_t* facet_id, const double* pft, int32_t max_pip);
 int  orc_set_outflow_bcs(orc_handle* h, const dem_outflow_bc* bcs, int32_t n);
+int  orc_set_inflow_bcs(orc_handle* h, const dem_inflow_bc* bcs, int32_t n, uint64_t seed);
+int  orc_push_inflow_random(orc_handle* h, const double* r, int64_t n);
+int  orc_get_inflow_state(orc_handle* h, int32_t bc, int32_t* vacancy, double* mi_time);
 int  orc_download_cells(orc_handle* h, int32_t* dg_pijk, int32_t max_pip);
 /* facets_at_dg as CSR over 1-based DES cells: start[ncell2+1], ids (1-based) */
 int  orc_download_facet_bins(orc_handle* h, int32_t* start, int32_t* ids, int32_t capacity,
