@@ -480,6 +480,7 @@ struct CellOut {
   int* dg_pijk = nullptr;
   uint8_t* wall_cand = nullptr;
   const int* fbin_start = nullptr;
+  float* wgap = nullptr;  // facet clearance of the last build: -1 (unknown) on a change of cell
 };
 
 template <int MODE>
@@ -540,6 +541,7 @@ __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8
     } else {
       int c;
       dg_place(p, true, xo, c);
+      if (cells.dg_pijk[me] != c) cells.wgap[me] = -1.0f;
       cells.dg_pijk[me] = c;
       const int fc = p.cell_off + c - 1;
       cells.wall_cand[me] = cells.fbin_start[fc + 1] > cells.fbin_start[fc] ? 1 : 0;
@@ -573,6 +575,7 @@ inline CellOut gather_cells(const dem_handle* h) {
     c.dg_pijk = h->dg_pijk;
     c.wall_cand = h->wall_cand;
     c.fbin_start = h->fbin_start;
+    c.wgap = h->wgap;
   }
   return c;
 }

@@ -21,7 +21,8 @@ namespace demb {
 template <bool B>
 __global__ void k_cell_keys(DevParams p0, BatchView bv, double4* __restrict__ pos4,
                             const int8_t* __restrict__ state, int* __restrict__ dg_pijk,
-                            const int* __restrict__ fbin_start, uint8_t* __restrict__ wall_cand) {
+                            const int* __restrict__ fbin_start, uint8_t* __restrict__ wall_cand,
+                            float* __restrict__ wgap) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, i);
@@ -34,6 +35,8 @@ __global__ void k_cell_keys(DevParams p0, BatchView bv, double4* __restrict__ po
   if (state[i] == DEM_STATE_NONEXISTENT) { dg_pijk[i] = 0; wall_cand[i] = 0; return; }
   int c;
   if (dg_place(p, per, x, c)) pos4[i] = x;
+  // the facet clearance of the last build holds for that build's cell only
+  if (dg_pijk[i] != c) wgap[i] = -1.0f;
   dg_pijk[i] = c;
   const int fc = p.cell_off + c - 1;
   wall_cand[i] = fbin_start[fc + 1] > fbin_start[fc] ? 1 : 0;
@@ -113,10 +116,10 @@ int run_desgrid_pic(dem_handle* h, bool bin_search) {
   const int nfc = bt ? h->nfcell_total : p.nfcell;
   if (bt)
     k_cell_keys<true><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk, h->fbin_start,
-                                              h->wall_cand);
+                                              h->wall_cand, h->wgap);
   else
     k_cell_keys<false><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk, h->fbin_start,
-                                               h->wall_cand);
+                                               h->wall_cand, h->wgap);
   DEM_LAUNCH(h);
   // particles seeded since the last DESGRID_PIC are in its cell lists now
   if (h->pic_fresh && !h->ibc.empty()) cudaMemsetAsync(h->pic_fresh, 0, (size_t)n, h->stream);

@@ -384,7 +384,9 @@ done:
 }
 
 // Clearance of every NORMAL particle in a DES cell with facets from those
-// facets at a build: min over the cell's facets of |x - closest point| - r,
+// facets at a build (valid while the particle stays in that cell: the
+// per-step placement of a periodic system sets it to -1, unknown, when the
+// particle changes cell): min over the cell's facets of |x - closest point| - r,
 // less a margin of 1e-6 r for the rounding of the closest point, rounded
 // down to float.  A particle whose clearance exceeds the displacement bound
 // since the build touches none of them (the reference's contact test is
@@ -395,7 +397,12 @@ __global__ void k_wall_gaps(DevParams p0, BatchView bv, WallCtx w, const double4
                             float* __restrict__ wgap) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p0.n) return;
-  if (state[i] != DEM_STATE_NORMAL || !wall_cand[i]) { wgap[i] = FLT_MAX; return; }
+  // a particle that is not NORMAL now may become so before the next build
+  // (ENTERING, EXITING): clearance unknown, its walls are checked
+  if (state[i] != DEM_STATE_NORMAL) { wgap[i] = -1.0f; return; }
+  // no facets in its cell: none to touch while it stays there (a move to
+  // another cell before the next build clears the screen, see dg_place users)
+  if (!wall_cand[i]) { wgap[i] = FLT_MAX; return; }
   const DevParams& p = sysp<B>(p0, bv, i);
   const int cell = p.cell_off + w.dg_pijk[i] - 1;
   const double4 a = pos4[i];

@@ -167,3 +167,27 @@ def test_graph_replay_matches_eager_and_oracle(coll, intg, periodic):
     compare_state(g2, o, exact=True)
     compare_pairs(g1, o)
     assert g1.stats()["n_contacts"] == o.stats()["n_contacts"]
+
+
+def test_periodic_particles_reach_a_wall_between_builds():
+    """A periodic system re-places its particles every step: spheres falling
+    from a DES cell without facets into the floor's cells between two
+    rebuilds must meet the floor as the oracle's (unscreened) wall test has
+    them do."""
+    from mfix_dem import GpuSystem
+    from oracle_ffi import OracleSystem
+    from cases import make_system, settling_case
+    case, prm, arr, walls = settling_case(n_side=(3, 1, 3), spacing=3.0, jitter=0.05, vmax=0.01, seed=21,
+                                          periodic=(True, False, True), nsn=2000)
+    h = 1.0 / prm.dg_dyinv
+    arr["pos"][1] = 1.5 * h + 0.1e-3 * np.arange(arr["pos"].shape[1]) / arr["pos"].shape[1]
+    arr["vel"][1] = -3.0
+    g = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    o = make_system(OracleSystem, prm, arr, walls)
+    steps = int(2.0 * h / (3.0 * prm.dtsolid)) + 50
+    for _ in range(4):
+        g.step(steps // 4); o.step(steps // 4)
+        compare_state(g, o, exact=True)
+    d = o.download_state()
+    assert np.all(d["pos"][1] > 0.0)            # the floor held them
+    assert o.stats()["n_wall_contacts"] >= 0
