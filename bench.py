@@ -76,6 +76,18 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x, ws, device):
+    """The largest of the ranks' values of x (a time): the job's time is its
+    slowest replica's.  Every rank calls it at the same point."""
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms.  Started
     before the timed region (nvidia-smi needs a moment to report); the
@@ -289,11 +301,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     parts = {k: v[0] / v[1] for k, v in g.profile().items() if k in ("walls", "pairs", "gather") and v[1]}
     g.set_profiling(False)
     ferr1 = g.force_error() if prec == "split" else None
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, ws, "cuda")
     n_normal = int(st["n_normal"])
     value = ws * n_normal * args.steps / (ms / 1e3)
 
@@ -349,11 +357,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
-        if ws > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(ems, ws, "cuda")
         out["e2e"] = {"value": ws * n_normal * args.e2e_steps / (ems / 1e3), "unit": METRIC,
                       "h2d_bytes_per_step": n * (9 * 8 + 3 * 8 + 1 + 4), "d2h_bytes_per_step": n * (9 * 8 + 1),
                       "steps": args.e2e_steps,
