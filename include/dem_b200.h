@@ -311,7 +311,8 @@ typedef struct dem_inflow_bc {
     int32_t polydisperse;     /* DEM_MI%POLYDISPERSE */
     int32_t n_layout;         /* entries of poly_layout (NUMFRAC_LIMIT = 10000 in the reference) */
     int32_t dg_lo[3], dg_hi[3];   /* DES-cell box of the entering test (DEM_BCMI_IJK) */
-    int32_t reserved_i[4];
+    int32_t l_index;          /* DEM_MI%L: fluid-cell index along the normal (restart records only) */
+    int32_t reserved_i[3];
     double  offset;           /* DEM_MI%OFFSET: the seeding coordinate along the normal */
     double  window;           /* DEM_MI%WINDOW */
     double  face;             /* plane of the entering test: YN(BC_J_s) for 'N', YN(BC_J_s-1) for 'S',
@@ -324,6 +325,8 @@ typedef struct dem_inflow_bc {
     const double*  p;         /* [occupants] DEM_MI%P: window corners on the first in-plane axis */
     const double*  q;         /* [occupants] DEM_MI%Q: on the second (ignored when NO_K) */
     const int32_t* poly_layout;   /* [n_layout] DEM_BC_POLY_LAYOUT: solids phase (1-based) per slot */
+    const int32_t* w_cell;    /* [occupants] DEM_MI%W, or NULL (restart records only: written as 0) */
+    const int32_t* h_cell;    /* [occupants] DEM_MI%H, or NULL (likewise) */
     double  d_p0[DEM_MAX_PHASES];   /* D_P0 of each phase */
     double  ro_s0[DEM_MAX_PHASES];  /* RO_S0 of each phase */
     double  vel[DEM_MAX_PHASES][3]; /* BC_U_s, BC_V_s, BC_W_s of each phase */
@@ -355,6 +358,30 @@ int dem_push_inflow_random(dem_handle* h, const double* r, int64_t n);
 /* The current DEM_MI%VACANCY and DEM_MI_TIME of inflow boundary `bc`
  * (0-based), for restart files (read_res0_des.f:217). */
 int dem_get_inflow_state(dem_handle* h, int32_t bc, int32_t* vacancy, double* mi_time);
+
+/* One mass-inflow record of a RES file (write_res0_des.f:197-210,
+ * read_res0_des.f:205-234): DEM_MI_TIME and DEM_MI's VACANCY, OCCUPANTS,
+ * WINDOW, OFFSET and L; its W, H, P, Q arrays have `occupants` entries. */
+typedef struct dem_res_inflow {
+    double  mi_time;
+    double  window;
+    double  offset;
+    int32_t vacancy;
+    int32_t occupants;
+    int32_t l_index;
+    int32_t reserved;
+} dem_res_inflow;
+
+/* Reads the mass-inflow section at the end of a RES file: *n_bc receives
+ * DEM_BCMI (0 for files without inflow); the records of the first max_bc
+ * boundaries go to mi[], and, where w/hh/p/q are not NULL, their arrays to
+ * row b of w/hh/p/q (max_occ entries per row; DEM_ERR_CAPACITY when a
+ * boundary has more).  dem_write_res0_des writes the section of the
+ * handle's inflow boundaries; dem_read_res0_des restores DEM_MI_TIME and
+ * VACANCY into the boundaries installed on the handle when their number
+ * matches the file's (RESTART_1 semantics). */
+int dem_res_read_inflow(const char* path, int32_t no_k, int32_t* n_bc, dem_res_inflow* mi, int32_t max_bc,
+                        int32_t* w, int32_t* hh, double* p, double* q, int32_t max_occ);
 
 /* ---- particle output (model/des/vtp_mod.f) ------------------------------- */
 

@@ -266,6 +266,7 @@ struct dem_handle {
     dem_inflow_bc bc;
     std::vector<double> p, q;
     std::vector<int32_t> layout;
+    std::vector<int32_t> w, hh;  // DEM_MI%W, %H for restart records (zeros when not given)
   };
   std::vector<Inflow> ibc;
   dem_inflow_bc* d_ibc = nullptr;

@@ -263,7 +263,12 @@ int dem_set_inflow_bcs(dem_handle* h, const dem_inflow_bc* bcs, int32_t n, uint6
     I.p.assign(bcs[i].p, bcs[i].p + occ);
     I.q.assign(bcs[i].q, bcs[i].q + occ);
     I.layout.assign(bcs[i].poly_layout, bcs[i].poly_layout + bcs[i].n_layout);
-    I.bc.p = nullptr; I.bc.q = nullptr; I.bc.poly_layout = nullptr;  // the device copy holds no host pointers
+    I.w.assign((size_t)occ, 0);
+    I.hh.assign((size_t)occ, 0);
+    if (bcs[i].w_cell) I.w.assign(bcs[i].w_cell, bcs[i].w_cell + occ);
+    if (bcs[i].h_cell) I.hh.assign(bcs[i].h_cell, bcs[i].h_cell + occ);
+    // the device copy holds no host pointers
+    I.bc.p = nullptr; I.bc.q = nullptr; I.bc.poly_layout = nullptr; I.bc.w_cell = nullptr; I.bc.h_cell = nullptr;
     h->ibc.push_back(std::move(I));
   }
   if (!h->pic_fresh) {

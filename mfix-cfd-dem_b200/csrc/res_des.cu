@@ -162,10 +162,10 @@ inline bool exists(int8_t s) { return s != DEM_STATE_NONEXISTENT && s < DEM_STAT
 
 extern "C" {
 
-int dem_res_write(const char* path, const dem_res_info* info, int32_t max_pip, int32_t no_k, const double* pos,
-                  const double* vel, const double* omega, const double* radius, const int8_t* state,
-                  const int32_t* phase, const int32_t* neighbor_index, const int32_t* neighbors, const double* pft,
-                  int64_t n_pairs) {
+static int res_write(const char* path, const dem_res_info* info, int32_t max_pip, int32_t no_k, const double* pos,
+                     const double* vel, const double* omega, const double* radius, const int8_t* state,
+                     const int32_t* phase, const int32_t* neighbor_index, const int32_t* neighbors, const double* pft,
+                     int64_t n_pairs, const std::vector<dem_handle::Inflow>* mi) {
   if (!path || !info || max_pip < 0 || !pos || !vel || !omega || !radius || !state || !phase) return DEM_ERR_ARG;
   if (n_pairs < 0 || (n_pairs > 0 && (!neighbor_index || !neighbors || !pft))) return DEM_ERR_ARG;
   const int dimn = no_k ? 2 : 3;
@@ -218,7 +218,24 @@ int dem_res_write(const char* path, const dem_res_info* info, int32_t max_pip, i
   w.put_ii(nc, [&](int64_t k) { return gid[neighbors[keep[k]] - 1]; });
   w.put_ii(nc, [&](int64_t k) { return gid[owner[k]]; });
   for (int c = 0; c < dimn; ++c) w.put_di(nc, [&](int64_t k) { return pft[3 * keep[k] + c]; });
-  w.put_i(0);                                      // DEM_BCMI
+  // DEM_BCMI, then per boundary DEM_MI_TIME and DEM_MI's VACANCY, OCCUPANTS,
+  // WINDOW, OFFSET, L, W, H, P, Q (write_res0_des.f:197-210)
+  const int32_t nbc = mi ? (int32_t)mi->size() : 0;
+  w.put_i(nbc);
+  for (int32_t b = 0; b < nbc; ++b) {
+    const dem_handle::Inflow& I = (*mi)[b];
+    const int32_t occ = (int32_t)I.p.size();
+    w.put_d(I.bc.mi_time);
+    w.put_i(I.bc.vacancy);
+    w.put_i(occ);
+    w.put_d(I.bc.window);
+    w.put_d(I.bc.offset);
+    w.put_i(I.bc.l_index);
+    w.put_ii(occ, [&](int64_t k) { return I.w[k]; });
+    w.put_ii(occ, [&](int64_t k) { return I.hh[k]; });
+    w.put_di(occ, [&](int64_t k) { return I.p[k]; });
+    w.put_di(occ, [&](int64_t k) { return I.q[k]; });
+  }
   const bool ok = w.ok;
   if (fclose(w.f) != 0 || !ok) return DEM_ERR_ARG;
   return 0;
@@ -288,6 +305,68 @@ int dem_res_read(const char* path, dem_res_info* info, int32_t max_pip, int32_t 
   return bad ? DEM_ERR_STATE : 0;
 }
 
+int dem_res_write(const char* path, const dem_res_info* info, int32_t max_pip, int32_t no_k, const double* pos,
+                  const double* vel, const double* omega, const double* radius, const int8_t* state,
+                  const int32_t* phase, const int32_t* neighbor_index, const int32_t* neighbors, const double* pft,
+                  int64_t n_pairs) {
+  return res_write(path, info, max_pip, no_k, pos, vel, omega, radius, state, phase, neighbor_index, neighbors, pft,
+                   n_pairs, nullptr);
+}
+
+int dem_res_read_inflow(const char* path, int32_t no_k, int32_t* n_bc, dem_res_inflow* mi, int32_t max_bc,
+                        int32_t* wc, int32_t* hc, double* pc, double* qc, int32_t max_occ) {
+  if (!path || !n_bc || max_bc < 0 || (max_bc > 0 && !mi) || max_occ < 0) return DEM_ERR_ARG;
+  const int dimn = no_k ? 2 : 3;
+  RecFile r;
+  r.f = fopen(path, "rb");
+  if (!r.f) return DEM_ERR_ARG;
+  struct Closer { FILE* f; ~Closer() { fclose(f); } } closer{r.f};
+  r.get_d();
+  const int32_t np = r.get_i();
+  r.get_i();
+  const int32_t nc = r.get_i();
+  if (!r.ok || np < 0 || nc < 0) return DEM_ERR_ARG;
+  // skip the particle and pair sections record by record
+  auto skip_d = [&](int64_t m) { r.get_di(m, [](int64_t, double) {}); };
+  auto skip_i = [&](int64_t m) { r.get_ii(m, [](int64_t, int32_t) {}); };
+  r.get_i(); r.get_i(); r.get_d();
+  for (int c = 0; c < dimn; ++c) skip_d(np);
+  skip_i(np); skip_i(np);
+  for (int c = 0; c < dimn; ++c) skip_d(np);
+  for (int c = 0; c < (no_k ? 1 : 3); ++c) skip_d(np);
+  skip_d(np); skip_d(np); skip_i(np);
+  const int32_t nusr = r.get_i();
+  if (!r.ok || nusr < 0) return DEM_ERR_ARG;
+  for (int32_t u = 0; u < nusr; ++u) skip_d(np);
+  skip_d(np);
+  skip_i(nc); skip_i(nc);
+  for (int c = 0; c < dimn; ++c) skip_d(nc);
+  const int32_t nbc = r.get_i();
+  if (!r.ok || nbc < 0) return DEM_ERR_ARG;
+  *n_bc = nbc;
+  for (int32_t b = 0; b < nbc; ++b) {
+    dem_res_inflow rec{};
+    rec.mi_time = r.get_d();
+    rec.vacancy = r.get_i();
+    rec.occupants = r.get_i();
+    rec.window = r.get_d();
+    rec.offset = r.get_d();
+    rec.l_index = r.get_i();
+    if (!r.ok || rec.occupants < 0) return DEM_ERR_ARG;
+    const int32_t occ = rec.occupants;
+    const bool keep = b < max_bc;
+    if (keep) mi[b] = rec;
+    if (keep && (wc || hc || pc || qc) && occ > max_occ) return DEM_ERR_CAPACITY;
+    const size_t row = (size_t)b * (size_t)max_occ;
+    r.get_ii(occ, [&](int64_t k, int32_t v) { if (keep && wc) wc[row + k] = v; });
+    r.get_ii(occ, [&](int64_t k, int32_t v) { if (keep && hc) hc[row + k] = v; });
+    r.get_di(occ, [&](int64_t k, double v) { if (keep && pc) pc[row + k] = v; });
+    r.get_di(occ, [&](int64_t k, double v) { if (keep && qc) qc[row + k] = v; });
+    if (!r.ok) return DEM_ERR_ARG;
+  }
+  return 0;
+}
+
 int dem_write_res0_des(dem_handle* h, const char* path, const dem_res_info* info) {
   if (!h) return DEM_ERR_ARG;
   cudaSetDevice(h->dev);
@@ -314,9 +393,9 @@ int dem_write_res0_des(dem_handle* h, const char* path, const dem_res_info* info
     pf.resize(3 * (size_t)(P ? P : 1));
     if (int rc = dem_download_pairs(h, ni.data(), nb.data(), pf.data(), P ? P : 1, h->n)) return rc;
   }
-  const int rc = dem_res_write(path, info, h->n, h->dp.no_k, pos.data(), vel.data(), omega.data(), radius.data(),
-                               state.data(), phase.data(), P ? ni.data() : nullptr, P ? nb.data() : nullptr,
-                               P ? pf.data() : nullptr, P);
+  const int rc = res_write(path, info, h->n, h->dp.no_k, pos.data(), vel.data(), omega.data(), radius.data(),
+                           state.data(), phase.data(), P ? ni.data() : nullptr, P ? nb.data() : nullptr,
+                           P ? pf.data() : nullptr, P, &h->ibc);
   if (rc) return set_err(h, rc, "restart file write failed");
   return 0;
 }
@@ -353,6 +432,22 @@ int dem_read_res0_des(dem_handle* h, const char* path, int32_t restore_pairs, de
   if ((rc = dem_upload_state(h, pos.data(), vel.data(), omega.data(), radius.data(), pmass.data(), omoi.data(),
                              state.data(), phase.data(), h->n)))
     return rc;
+  if (!h->ibc.empty()) {
+    // DEM_MI_TIME and VACANCY of the installed inflow boundaries, when the
+    // file holds as many (read_res0_des.f:205-221)
+    std::vector<dem_res_inflow> mi(h->ibc.size());
+    int32_t nbc = 0;
+    if (dem_res_read_inflow(path, h->dp.no_k, &nbc, mi.data(), (int32_t)mi.size(), nullptr, nullptr, nullptr,
+                            nullptr, 0) == 0 && nbc == (int32_t)h->ibc.size()) {
+      for (size_t b = 0; b < mi.size(); ++b) {
+        if (mi[b].occupants != h->ibc[b].bc.occupants || mi[b].vacancy < 1 ||
+            (mi[b].occupants > 0 && mi[b].vacancy > mi[b].occupants))
+          return set_err(h, DEM_ERR_ARG, "inflow layout in the restart file differs from the installed one");
+        h->ibc[b].bc.vacancy = mi[b].vacancy;
+        h->ibc[b].bc.mi_time = mi[b].mi_time;
+      }
+    }
+  }
   if (!restore_pairs) return 0;
   // entries grouped by owner in the file's order -> CSR with 1-based ends
   std::vector<int32_t> ni(n, 0);

@@ -233,7 +233,8 @@ class DemInflowBC(C.Structure):
         ("n_layout", C.c_int32),
         ("dg_lo", C.c_int32 * 3),
         ("dg_hi", C.c_int32 * 3),
-        ("reserved_i", C.c_int32 * 4),
+        ("l_index", C.c_int32),
+        ("reserved_i", C.c_int32 * 3),
         ("offset", C.c_double),
         ("window", C.c_double),
         ("face", C.c_double),
@@ -244,10 +245,24 @@ class DemInflowBC(C.Structure):
         ("p", C.POINTER(C.c_double)),
         ("q", C.POINTER(C.c_double)),
         ("poly_layout", C.POINTER(C.c_int32)),
+        ("w_cell", C.POINTER(C.c_int32)),
+        ("h_cell", C.POINTER(C.c_int32)),
         ("d_p0", C.c_double * DEM_MAX_PHASES),
         ("ro_s0", C.c_double * DEM_MAX_PHASES),
         ("vel", (C.c_double * 3) * DEM_MAX_PHASES),
         ("reserved_d", C.c_double * 4),
+    ]
+
+
+class DemResInflow(C.Structure):
+    _fields_ = [
+        ("mi_time", C.c_double),
+        ("window", C.c_double),
+        ("offset", C.c_double),
+        ("vacancy", C.c_int32),
+        ("occupants", C.c_int32),
+        ("l_index", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -326,6 +341,7 @@ DEM_ONLY = {
     "read_res0_des": (C.c_int, [_P, C.c_char_p, C.c_int32, C.POINTER(DemResInfo)]),
     "res_write": (C.c_int, [C.c_char_p, C.POINTER(DemResInfo), C.c_int32, C.c_int32, _D, _D, _D, _D, _I8, _I32,
                             _I32, _I32, _D, C.c_int64]),
+    "res_read_inflow": (C.c_int, [C.c_char_p, C.c_int32, _I32, C.c_void_p, C.c_int32, _I32, _I32, _D, _D, C.c_int32]),
     "res_read": (C.c_int, [C.c_char_p, C.POINTER(DemResInfo), C.c_int32, C.c_int32, _D, _D, _D, _D, _D, _I8, _I32,
                            _I32, _I32, _D, C.c_int64]),
     "sys_get_stats": (C.c_int, [_P, C.c_int32, C.POINTER(DemStats)]),

@@ -87,3 +87,29 @@ def res_read(lib, path, max_pip: int, no_k: bool, pairs: bool = True) -> dict:
     if pairs:
         out["owner"], out["neighbor"], out["pft"] = own[:P].copy(), nbr[:P].copy(), pft[:P].copy()
     return out
+
+
+def res_read_inflow(lib, path, no_k: bool, max_bc: int = 8, max_occ: int = 4096) -> list:
+    """The mass-inflow records at the end of a RES file: one dict per
+    boundary with mi_time, vacancy, occupants, window, offset, l_index and
+    the W, H, P, Q arrays."""
+    mi = (abi.DemResInflow * max(max_bc, 1))()
+    nbc = C.c_int32()
+    w = np.zeros((max_bc, max_occ), np.int32)
+    hh = np.zeros((max_bc, max_occ), np.int32)
+    p = np.zeros((max_bc, max_occ))
+    q = np.zeros((max_bc, max_occ))
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    rc = lib.dem_res_read_inflow(str(path).encode(), 1 if no_k else 0, C.byref(nbc), C.cast(mi, C.c_void_p),
+                                 max_bc, ip(w), ip(hh), dp(p), dp(q), max_occ)
+    if rc:
+        raise OSError(f"dem_res_read_inflow failed ({abi.ERROR_NAMES.get(rc, rc)})")
+    out = []
+    for b in range(min(nbc.value, max_bc)):
+        r = mi[b]
+        o = int(r.occupants)
+        out.append(dict(mi_time=r.mi_time, vacancy=r.vacancy, occupants=o, window=r.window, offset=r.offset,
+                        l_index=r.l_index, w=w[b, :o].copy(), h=hh[b, :o].copy(), p=p[b, :o].copy(),
+                        q=q[b, :o].copy()))
+    return out

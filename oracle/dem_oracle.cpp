@@ -1755,7 +1755,7 @@ int orc_set_inflow_bcs(orc_handle* h, const dem_inflow_bc* bcs, int32_t n, uint6
     I.p.assign(bcs[i].p, bcs[i].p + occ);
     I.q.assign(bcs[i].q, bcs[i].q + occ);
     I.layout.assign(bcs[i].poly_layout, bcs[i].poly_layout + bcs[i].n_layout);
-    I.bc.p = nullptr; I.bc.q = nullptr; I.bc.poly_layout = nullptr;
+    I.bc.p = nullptr; I.bc.q = nullptr; I.bc.poly_layout = nullptr; I.bc.w_cell = nullptr; I.bc.h_cell = nullptr;
     o.ibc.push_back(std::move(I));
   }
   return 0;

@@ -48,3 +48,29 @@ def test_queued_numbers_match_oracle():
     g.step(60); o.step(60)
     compare_state(g, o, exact=True)
     assert g.stats()["n_inflow_added"] == o.stats()["n_inflow_added"] > 0
+
+
+def test_restart_file_carries_the_inflow_state(tmp_path):
+    """dem_write_res0_des writes the inflow records (DEM_MI_TIME, VACANCY and
+    the layout); dem_read_res0_des into a handle with the same boundaries
+    installed restores DEM_MI_TIME and VACANCY, and the two handles then seed
+    the same particles."""
+    from mfix_dem import GpuSystem
+    from mfix_dem import restart
+    from mfix_dem._lib import load
+    case, prm, arr, walls, bc, _ = inflow_case()
+    a = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    a.set_inflow_bcs([bc], seed=2)
+    a.step(60)
+    path = tmp_path / "inflow.RES"
+    a.write_res0_des(path, ro_sol=[case.ro_s0[0]])
+    rec = restart.res_read_inflow(load(), path, no_k=False)
+    vac, mi_time = a.inflow_state(0)
+    assert len(rec) == 1 and rec[0]["vacancy"] == vac and rec[0]["mi_time"] == mi_time
+    P, Q, _ = bc._keep
+    assert np.array_equal(rec[0]["p"], P) and np.array_equal(rec[0]["q"], Q)
+    assert rec[0]["occupants"] == bc.occupants and rec[0]["window"] == bc.window
+    b = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    b.set_inflow_bcs([bc], seed=2)
+    b.read_res0_des(path, restore_pairs=True)
+    assert b.inflow_state(0) == (vac, mi_time)
