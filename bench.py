@@ -1,12 +1,18 @@
 #!/usr/bin/env python3
 """bench.py -- DEM particle step throughput on B200.
 
-Workload: 1,000,000 polydisperse Hertzian spheres (lognormal d, median 1 mm,
-sigma 0.25, clipped to 0.5-2 mm; rho 2500; E 1e7, nu 0.3; e_n = e_t = 0.85;
-friction 0.3, rolling friction 0.01) in a 0.1 x 0.4 x 0.1 m box, periodic in x
-and z with a flat bottom wall, seeded random sequential placement at 40 %
-solids.  One step = one DES_TIME_STEP (contact forces, walls, integration, and
-the neighbour rebuild every NEIGHBOR_SEARCH_N = 25 steps).
+Workload (`--workload dense`, the headline): 1,000,000 polydisperse
+Hertzian spheres (lognormal d, median 1 mm, sigma 0.25, clipped to 0.5-2 mm;
+rho 2500; E 1e7, nu 0.3; e_n = e_t = 0.85; friction 0.3, rolling friction
+0.01) in a 0.1 x 0.4 x 0.1 m box, periodic in x and z with a flat bottom
+wall, placed by seeded random sequential placement at 40 % solids and then
+every diameter grown by 1.15 (61 % solids, about two contacts per particle),
+so that the bed carries contacts like a settled bed.  `--workload rsa40`
+is the placement as placed (40 % solids, no contacts within the timed
+steps).  One step = one DES_TIME_STEP (contact forces, walls, integration,
+and the neighbour rebuild every NEIGHBOR_SEARCH_N = 25 steps).  The timed
+window of K steps ends on a rebuild step, so it holds ceil(K / 25) rebuilds:
+at least their natural rate.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -56,9 +62,39 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=30, help="requests per rate")
     ap.add_argument("--serve-steps", type=int, default=2000, help="DES steps per served case")
     ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="HBM budget of the server")
-    ap.add_argument("--inflate", type=float, default=1.0,
-                    help="grow every sphere by this factor after placement (contact-dense variant)")
-    return ap.parse_args()
+    ap.add_argument("--workload", default="dense", choices=["dense", "rsa40"],
+                    help="dense: the placement with every diameter grown by --inflate; rsa40: as placed")
+    ap.add_argument("--inflate", type=float, default=1.15,
+                    help="diameter growth after placement of the dense workload")
+    ap.add_argument("--no-rsa40", action="store_true", help="skip the FP64 leg on the bed as placed")
+    a = ap.parse_args()
+    if a.workload == "rsa40":
+        a.inflate = 1.0
+    return a
+
+
+def workload_name(inflate):
+    return "hertz_rsa_1m" if inflate == 1.0 else f"hertz_rsa_1m_dense_x{inflate:g}"
+
+
+def timed_window(warm_min, steps, nsn):
+    """First NN of a window of `steps` steps that starts after at least
+    warm_min warm-up steps and ends on a neighbour-search step (NN a multiple
+    of nsn), and the number of rebuilds inside it: ceil(steps / nsn), the
+    natural rate or above it."""
+    end = -(-(warm_min + steps) // nsn) * nsn
+    nn0 = end - steps + 1
+    rebuilds = sum(1 for nn in range(nn0, end + 1) if nn % nsn == 0)
+    return nn0, rebuilds
+
+
+def bench_config(args, info, prm):
+    """The `config` object shared by both arms."""
+    return {"workload": workload_name(args.inflate), "n_particles_requested": args.n,
+            "inflate": args.inflate, "contact": "hertz", "integrator": "euler", "periodic": "xz",
+            "neighbor_search_n": int(prm.neighbor_search_n),
+            "solids_fraction": round(float(info.get("solids_fraction")) * args.inflate ** 3, 4),
+            "dtsolid": prm.dtsolid, "steps_timed": args.steps}
 
 
 def workload(n, precision, inflate=1.0):
@@ -184,8 +220,8 @@ def cpu_sample(args, threads=None):
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle_ffi import OracleSystem
     threads = threads or os.cpu_count() or 1
-    case, prm, arr, walls, info = workload(args.cpu_sample, args.precision if args.precision == "fp64" else "fp64")
-    o = OracleSystem(prm, arr["pos"].shape[1], openmp=True, threads=threads)
+    case, prm, arr, walls, info = workload(args.cpu_sample, "fp64", args.inflate)
+    o = OracleSystem(prm, arr["pos"].shape[1], openmp=True, threads=threads, native=True)
     o.set_walls(*walls)
     o.upload_state(arr["pos"], arr["vel"], arr["omega"], arr["radius"], arr["pmass"], arr["omoi"],
                    arr["state"], arr["phase"])
@@ -197,8 +233,8 @@ def cpu_sample(args, threads=None):
     n = int(o.stats()["n_normal"])
     return {"value": n * args.cpu_steps / dt, "unit": METRIC, "cores": threads, "kind": "port",
             "sample": f"{n} particles of the same workload (box scaled to keep density and bed height), "
-                      f"{args.cpu_steps} steps incl. {args.cpu_steps // 25} neighbour rebuilds, OpenMP oracle, "
-                      f"{dt:.1f} s"}
+                      f"{args.cpu_steps} steps incl. {args.cpu_steps // 25} neighbour rebuilds, OpenMP oracle "
+                      f"(-O3 -march=native), {dt:.1f} s"}
 
 
 def run_reference(args):
@@ -209,15 +245,19 @@ def run_reference(args):
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle_ffi import OracleSystem
     threads = os.cpu_count() or 1
-    case, prm, arr, walls, info = workload(args.cpu_sample, "fp64")
-    o = OracleSystem(prm, arr["pos"].shape[1], openmp=True, threads=threads)
+    case, prm, arr, walls, info = workload(args.cpu_sample, "fp64", args.inflate)
+    o = OracleSystem(prm, arr["pos"].shape[1], openmp=True, threads=threads, native=True)
     o.set_walls(*walls)
     o.upload_state(arr["pos"], arr["vel"], arr["omega"], arr["radius"], arr["pmass"], arr["omoi"],
                    arr["state"], arr["phase"])
     o.init_neighbors()
-    o.step(max(args.warmup, 1), 1)
+    # the same window placement as the GPU arm: W warm-up steps or more, and
+    # K timed steps ending on a rebuild step
+    nsn = int(prm.neighbor_search_n)
+    nn0, rebuilds = timed_window(max(args.warmup, 1), args.steps, nsn)
+    o.step(nn0 - 1, 1)
     t0 = time.perf_counter()
-    o.step(args.steps, max(args.warmup, 1) + 1)
+    o.step(args.steps, nn0)
     dt = time.perf_counter() - t0
     n = int(o.stats()["n_normal"])
     value = n * args.steps / dt
@@ -226,12 +266,14 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "hertz_rsa_1m (sampled)", "n_particles": n, "periodic": "xz",
-                   "contact": "hertz", "integrator": "euler"},
+        "config": bench_config(args, info, prm) | {"n_particles": n, "precision": "fp64",
+                                                   "timed_window_nn": [nn0, nn0 + args.steps - 1],
+                                                   "rebuilds_timed": rebuilds},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
-                         "sample": f"{n} particles of the 1M workload (same density/bed height), "
-                                   f"{args.steps} timed steps, OpenMP C++ restatement of the Fortran "
-                                   "reference (the Fortran reference cannot be compiled here)"},
+                         "sample": f"{n} particles of the {workload_name(args.inflate)} workload, "
+                                   f"{args.steps} timed steps incl. {rebuilds} neighbour rebuilds, OpenMP "
+                                   "C++ restatement of the Fortran reference (-O3 -march=native; the "
+                                   "Fortran reference cannot be compiled here)"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.perf_counter() - t_all,
     }
@@ -251,12 +293,12 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     g.upload_state(arr["pos"], arr["vel"], arr["omega"], arr["radius"], arr["pmass"], arr["omoi"],
                    arr["state"], arr["phase"])
     g.init_neighbors()
-    # warm-up: at least W steps and up to a period boundary past the first
-    # two replayed periods, so both CUDA graphs of the period (the buffer
-    # parities alternate) are captured before the timed steps
+    # warm-up: at least W steps and at least three periods, so that both
+    # CUDA graphs of a period (the buffer parities alternate) are captured;
+    # the timed window then ends on a rebuild step
     nsn = int(prm.neighbor_search_n)
-    warm = max(args.warmup, 3 * nsn)
-    warm = ((warm + nsn - 1) // nsn) * nsn
+    nn0, rebuilds = timed_window(max(args.warmup, 3 * nsn), args.steps, nsn)
+    warm = nn0 - 1
     g.step(5, 1)
     tuning = g.autotune(reps=3)  # before the graphs are captured (a new shape drops them)
     g.step(warm - 5, 6)
@@ -314,7 +356,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     traffic = None
     if PROFILE_TRAFFIC.exists():
         tr = json.loads(PROFILE_TRAFFIC.read_text())
-        key = f"{'hertz_rsa_1m' if args.inflate == 1.0 else 'hertz_rsa_1m_inflated'}:{prec}"
+        key = f"{workload_name(args.inflate)}:{prec}"
         traffic = tr.get(key)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
@@ -326,7 +368,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
                 "kernel_ms": {k: v[0] for k, v in prof.items() if v[1]},
                 "force_parts_ms_per_launch": parts}
     out = {"value": value, "ms": ms, "n": n, "n_normal": n_normal, "pairs": int(p1), "launches": int(launches),
-           "warmup": warm, "tuning": tuning,
+           "warmup": warm, "tuning": tuning, "window": [warm + 1, warm + args.steps], "rebuilds_timed": rebuilds,
            "roofline": roofline, "clocks": clk, "contacts": int(st["n_contacts"]), "prm": prm, "info": info,
            "force_error": None if ferr0 is None else [ferr0, ferr1]}
 
@@ -338,12 +380,14 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
                                             np.int32: torch.int32}[a.dtype.type], pin_memory=True)
             t.numpy()[...] = a
             return t.numpy()
+        nn_e0, e2e_rebuilds = timed_window(warm + 2 * args.steps + 10, args.e2e_steps, nsn)
+        g.step(nn_e0 - (warm + 2 * args.steps + 11), warm + 2 * args.steps + 11)
         st_now = g.download_state()
         hin = {"pos": pinned(st_now["pos"]), "vel": pinned(st_now["vel"]), "omega": pinned(st_now["omega"]),
                "radius": pinned(arr["radius"]), "pmass": pinned(arr["pmass"]), "omoi": pinned(arr["omoi"]),
                "state": pinned(st_now["state"]), "phase": pinned(arr["phase"])}
         hout = {"pos": hin["pos"], "vel": hin["vel"], "omega": hin["omega"], "state": hin["state"]}
-        nn0 = warm + 2 * args.steps + 1
+        nn0 = nn_e0
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -360,7 +404,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
         ems = max_over_ranks(ems, ws, "cuda")
         out["e2e"] = {"value": ws * n_normal * args.e2e_steps / (ems / 1e3), "unit": METRIC,
                       "h2d_bytes_per_step": n * (9 * 8 + 3 * 8 + 1 + 4), "d2h_bytes_per_step": n * (9 * 8 + 1),
-                      "steps": args.e2e_steps,
+                      "steps": args.e2e_steps, "rebuilds_timed": e2e_rebuilds,
                       "note": "each step: dem_upload_state from pinned host arrays, dem_step, dem_download_state"}
     g.close()
     return out
@@ -507,6 +551,12 @@ def run_ours(args):
     other = None
     if args.precision == "fp64" and not args.no_split:
         other = _timed_run(args, "split", stream, barrier, ws, local, with_e2e=False)
+    rsa40 = None
+    if args.inflate != 1.0 and not args.no_rsa40:
+        import copy
+        a40 = copy.copy(args)
+        a40.inflate = 1.0
+        rsa40 = _timed_run(a40, "fp64", stream, barrier, ws, local, with_e2e=False)
 
     batched = None
     if args.batch_systems > 0:
@@ -525,18 +575,17 @@ def run_ours(args):
 
     if rank == 0:
         prm, info = main["prm"], main["info"]
-        wl = "hertz_rsa_1m" if args.inflate == 1.0 else f"hertz_rsa_1m_inflated_{args.inflate:g}"
         line = {
             "metric": METRIC, "value": main["value"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": main["warmup"], "warmup_requested": args.warmup, "ms_per_step": main["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": wl, "n_particles": main["n_normal"], "n_pairs": main["pairs"],
+            "config": bench_config(args, main["info"], main["prm"]) | {
+                       "n_particles": main["n_normal"], "n_pairs": main["pairs"],
                        "pairs_per_particle": main["pairs"] / max(main["n_normal"], 1),
-                       "precision": args.precision, "contact": "hertz", "integrator": "euler",
-                       "periodic": "xz", "neighbor_search_n": int(prm.neighbor_search_n),
-                       "solids_fraction": info.get("solids_fraction"), "dtsolid": prm.dtsolid,
+                       "precision": args.precision,
                        "contacts_last_step": main["contacts"],
+                       "timed_window_nn": main["window"], "rebuilds_timed": main["rebuilds_timed"],
                        "l2": "inputs larger than L2 (state and pair arrays ~%.0f MB)" % (
                            (main["n"] * 3 * 32 * 2 + main["pairs"] * 100) / 1e6),
                        "parallelism": f"replicas x{ws}"},
@@ -551,9 +600,17 @@ def run_ours(args):
             line["split"] = {"value": other["value"], "ms_per_step": other["ms"] / args.steps,
                              "speedup_vs_fp64": other["value"] / main["value"],
                              "force_rel_error_first_last": other["force_error"],
+                             "contacts_last_step": other["contacts"], "rebuilds_timed": other["rebuilds_timed"],
                              "roofline": other["roofline"], "gpu_launches": other["launches"],
                              "tuning": other["tuning"],
                              "clocks": other["clocks"]}
+        if rsa40 is not None:
+            line["rsa40"] = {"workload": workload_name(1.0), "precision": "fp64",
+                             "note": "the placement as placed (40 % solids): no contacts within the timed steps",
+                             "value": rsa40["value"], "ms_per_step": rsa40["ms"] / args.steps,
+                             "contacts_last_step": rsa40["contacts"], "n_pairs": rsa40["pairs"],
+                             "rebuilds_timed": rsa40["rebuilds_timed"], "roofline": rsa40["roofline"],
+                             "gpu_launches": rsa40["launches"], "clocks": rsa40["clocks"]}
         if batched is not None:
             b = batched
             line["batched"] = {

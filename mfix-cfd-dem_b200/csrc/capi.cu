@@ -893,6 +893,8 @@ int dem_get_stats_noalloc(dem_handle* h, dem_stats* s) {
   s->n_contacts = (int64_t)h->herr->n_contacts;
   s->n_wall_contacts = (int64_t)h->herr->n_wall_contacts;
   s->n_rogue_removed = (int64_t)h->herr->rogue_removed;
+  s->n_outflow_removed = (int64_t)h->herr->outflow_removed;
+  s->n_inflow_added = (int64_t)h->inflow_added;
   s->steps_done = h->steps_done;
   s->kinetic_energy = sum[6];
   s->bed_height = sum[4] > 0 ? sum[5] / sum[4] : 0.0;

@@ -26,13 +26,43 @@ def build():
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
 
 
-def load(openmp: bool = False):
-    name = "liboracle_omp.so" if openmp else "liboracle.so"
+def host_cpu_key() -> str:
+    """A short key for this host's CPU (model name and feature flags), so a
+    -march=native build made on one host is never loaded on another."""
+    import hashlib
+    text = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    text += line
+                if line.strip() == "":
+                    break
+    except OSError:
+        text = os.uname().machine
+    return hashlib.sha1(text.encode()).hexdigest()[:12]
+
+
+def native_path() -> Path:
+    """The OpenMP timing build with -march=native for this host's CPU,
+    compiled here on first use (a few seconds of g++)."""
+    d = HERE / "_build" / f"native_{host_cpu_key()}"
+    path = d / "liboracle_omp.so"
+    if not path.exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "native", f"NATIVE_DIR={d}"], check=True)
+    return path
+
+
+def load(openmp: bool = False, native: bool = False):
+    name = ("liboracle_native.so" if native else "liboracle_omp.so") if openmp else "liboracle.so"
     if name in _LIBS:
         return _LIBS[name]
-    path = HERE / "_build" / name
-    if not path.exists():
-        build()
+    if openmp and native:
+        path = native_path()
+    else:
+        path = HERE / "_build" / name
+        if not path.exists():
+            build()
     lib = C.CDLL(str(path))
     abi.bind(lib, "orc_")
     lib.orc_set_threads.restype = C.c_int
@@ -49,8 +79,8 @@ def load(openmp: bool = False):
 class OracleSystem(DemSystem):
     """The CPU restatement behind the same host interface as the CUDA library."""
 
-    def __init__(self, params, max_pip, openmp=False, threads=1):
-        super().__init__(load(openmp), params, max_pip, prefix="orc_")
+    def __init__(self, params, max_pip, openmp=False, threads=1, native=False):
+        super().__init__(load(openmp, native), params, max_pip, prefix="orc_")
         if threads != 1:
             self._lib.orc_set_threads(self._h, int(threads))
 

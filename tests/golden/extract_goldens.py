@@ -1,9 +1,9 @@
 """Extracts the reference's DEM regression tables into small JSON fixtures.
 
-Run in a container that holds the MFiX sources (default root below); the
+Run where the MFiX sources are checked out, passing their root; the
 fixtures it writes are committed so the tests run without the reference:
 
-    python tests/golden/extract_goldens.py [/path/to/mfix]
+    python tests/golden/extract_goldens.py /path/to/mfix
 
 Sources (relative to the MFiX root):
   tests/dem/DEM01/AUTOTEST/POST_POS.dat, POST_VEL.dat   free fall + wall bounce
@@ -112,4 +112,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/extract_goldens.py <reference checkout>")
+    main(sys.argv[1])

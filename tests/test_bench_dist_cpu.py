@@ -37,7 +37,7 @@ def test_reference_arm_two_ranks(tmp_path):
     port = 30500 + os.getpid() % 1000
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"), "--impl", "reference",
-           "--gpus", "2", "--steps", "3", "--warmup", "1", "--cpu-sample", "40000"]
+           "--gpus", "2", "--steps", "3", "--warmup", "1", "--cpu-sample", "60000"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]

@@ -4,17 +4,22 @@ The no-allocation entry point keeps its partial sums in a static device
 array shared by every call on the device; two calls in a row must each give
 the statistics of dem_get_stats (same kernels, same block-ordered sums, so
 the agreement is expected to be exact; the test allows 1e-12 relative).
+The first call on each handle comes before any dem_get_stats call, so a
+fallback to the allocating path would find no buffer to reuse; the device's
+free memory is checked across that call as well.
 """
 import numpy as np
 import pytest
 
 from mfix_dem import GpuSystem
 from cases import settling_case, make_system
+from inflow_cases import inflow_case
 
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
-KEYS_EXACT = ("n_normal", "n_pairs", "n_contacts", "n_wall_contacts", "n_rogue_removed", "steps_done")
+KEYS_EXACT = ("n_normal", "n_pairs", "n_contacts", "n_wall_contacts", "n_rogue_removed", "n_outflow_removed",
+              "n_inflow_added", "steps_done")
 KEYS_FLOAT = ("mean_vel", "gran_temp", "kinetic_energy", "bed_height", "s_time")
 
 
@@ -28,6 +33,30 @@ def _check(a, b):
         assert float(np.max(np.abs(x - y))) <= TOL * scale, (k, x, y)
 
 
+@pytest.fixture(scope="module", autouse=True)
+def _kernels_loaded():
+    # the driver loads a kernel's code at its first launch in the process
+    # (lazy module loading), which can take device memory; a throwaway
+    # handle launches both statistics paths once before any check
+    case, prm, arr, walls = settling_case(n_side=(4, 4, 4), spacing=1.05)
+    g = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    g.stats_noalloc()
+    g.stats()
+    g.close()
+    yield
+
+
+def _first_call_allocates_nothing(g):
+    import torch
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    s = g.stats_noalloc()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    return s
+
+
 def test_noalloc_stats_match_get_stats_twice():
     # 16,000 spheres in contact with the walls and with each other: 63
     # partial-sum blocks, so the block-ordered total is exercised
@@ -35,11 +64,11 @@ def test_noalloc_stats_match_get_stats_twice():
                                         box=(22e-3, 60e-3, 22e-3))
     g = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
     g.step(5)
+    first = _first_call_allocates_nothing(g)
+    second = g.stats_noalloc()
     ref = g.stats()
     assert ref["n_normal"] == arr["pos"].shape[1]
     assert ref["n_contacts"] > 0 and ref["kinetic_energy"] > 0
-    first = g.stats_noalloc()
-    second = g.stats_noalloc()
     _check(first, ref)
     _check(second, ref)
     # after more steps the shared scratch holds the previous call's sums;
@@ -49,4 +78,21 @@ def test_noalloc_stats_match_get_stats_twice():
     assert ref2["kinetic_energy"] != ref["kinetic_energy"]
     _check(g.stats_noalloc(), ref2)
     _check(g.stats_noalloc(), ref2)
+    g.close()
+
+
+def test_noalloc_stats_count_inflow_and_outflow():
+    # a box filled through its top while its floor lets particles out: the
+    # seeded and deleted counts must agree with dem_get_stats
+    case, prm, arr, walls, bc, obc = inflow_case(outflow=True, spare=220)
+    g = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    g.set_inflow_bcs([bc], seed=9)
+    g.set_outflow_bcs([obc])
+    g.step(300)
+    first = _first_call_allocates_nothing(g)
+    second = g.stats_noalloc()
+    ref = g.stats()
+    assert ref["n_inflow_added"] > 0 and ref["n_outflow_removed"] > 0
+    _check(first, ref)
+    _check(second, ref)
     g.close()
