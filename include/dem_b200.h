@@ -155,6 +155,13 @@ int dem_abi_version(void);
  * in stl_functions_des_mod.f:280-536) and flags edges shared by near-coplanar
  * facets as FLAG_FACETS_WHERE_EDGE_COLLISION_IS_IGNORED (stl_preproc_des_mod.f:
  * 361-490) does.  n_facets may be 0. */
+/* DTSOLID of the following steps.  A coupled driver shortens the last DEM
+ * step of each fluid step so the solids time lands on the fluid time
+ * (DTSOLID = TIME + DT - S_TIME, des_time_march.f:308-314) and puts the
+ * original value back after the fluid step (DES_TIME_END,
+ * des_time_march.f:470-476).  Single-system handles; dt > 0. */
+int dem_set_dtsolid(dem_handle* h, double dtsolid);
+
 int dem_set_walls(dem_handle* h, const double* vertex, const double* norm_face,
                   int32_t n_facets);
 
@@ -515,12 +522,23 @@ int dem_force_error(dem_handle* h, double* rel_err);
 #define DEM_INTERP_GARG 0
 #define DEM_INTERP_NONE 1
 
+/* DRAG_TYPE of DES_DRAG_GP (drag_gp_des.f:97-257).  GIDASPOW is the
+ * reference's DRAG_GIDASPOW (drag_gs.f:536-598).  SINGLE_SPHERE is the
+ * user drag law (DRAG_TYPE = 'USER_DRAG', drag_gp_des.f:169-171) that the
+ * reference's terminal-velocity regression compiles in (tests/dem/DEM06,
+ * usr_drag.f and usr_mod.f): DgA = 0.75*(RO_g*|u|/d_p)*Cd(Re) with the
+ * Schiller-Naumann Cd = (24/Re)*(1 + 0.15*Re**0.687) (0 for Re = 0) and
+ * Re = RO_g*usr_d_p0*|u|/MU_g from a fixed diameter usr_d_p0 (D_p0 of the
+ * phase); independent of EP_g. */
+#define DEM_DRAG_GIDASPOW      0
+#define DEM_DRAG_SINGLE_SPHERE 1
+
 /* Fluid grid description for the coupled step.  Uniform Cartesian grid of
  * imax x jmax x kmax interior cells starting at domain_lo with widths dx,dy,dz;
  * MFiX's IJK includes one ghost layer on every side. */
 typedef struct dem_fluid_grid {
     int32_t imax, jmax, kmax;
-    int32_t drag_model;          /* 0 = GIDASPOW (drag_gs.f:536-598) */
+    int32_t drag_model;          /* DEM_DRAG_GIDASPOW or DEM_DRAG_SINGLE_SPHERE */
     int32_t interp_scheme;       /* DES_INTERP_SCHEME: DEM_INTERP_GARG or DEM_INTERP_NONE */
     int32_t reserved_i;
     double dx, dy, dz;
@@ -528,7 +546,8 @@ typedef struct dem_fluid_grid {
     double ep_star;              /* packed-bed void fraction EP_STAR (for ep_s max) */
     double ur_f_gs;              /* under-relaxation of F_GP (drag_gp_des.f), usually 1 */
     double ro_s[DEM_MAX_PHASES]; /* RO_S0 of each solids phase (EP_S = ROP_S/RO_S) */
-    double reserved[6];
+    double usr_d_p0;             /* Re diameter of DEM_DRAG_SINGLE_SPHERE */
+    double reserved[5];
 } dem_fluid_grid;
 
 /* Installs the fluid grid and the gas fields on fluid cells (including
@@ -546,6 +565,16 @@ int dem_get_mean_fields(dem_handle* h, double* ep_g, double* rop_s);
  * COMP_MEAN_FIELDS0 under DEM_INTERP_GARG, COMP_MEAN_FIELDS1 without a filter
  * under DEM_INTERP_NONE) + CALC_EPG_DES. */
 int dem_comp_mean_fields(dem_handle* h);
+
+/* CALC_DES_BEDHEIGHT (model/des/des_granular_temperature.f:201-267, the
+ * formulation of Goldschmidt et al., Powder Technol. 138 (2003) 135-159):
+ * per solids phase, sum(EP_S*h*VOL) / sum(EP_S*VOL) over the fluid cells
+ * (ghost layers included) whose ROP_S of that phase is positive, h the
+ * cell-centre height 0.5*(YN(J)+YN(J-1)) and EP_S = ROP_S/RO_S from the last
+ * dem_comp_mean_fields (or coupled step).  Writes n_phases values; a phase
+ * with no solids gives 0/0 as in the reference.  Needs dem_set_gas_fields
+ * (a pure granular run installs its fluid grid with zero gas velocity). */
+int dem_calc_des_bedheight(dem_handle* h, double* bed_height);
 
 /* DRAG_GS_DES0 with GARG_2012 interpolation: adds the drag to FC.  Call after
  * dem_calc_force and before dem_cfnewvalues. */
@@ -590,7 +619,9 @@ typedef struct dem_tuning {
     int32_t gather_threads;      /* gather kernel: threads per block */
     int32_t neigh_threads;       /* pair-build scan: threads per block */
     double  pair_ms, gather_ms, neigh_ms;  /* measured time of the chosen shapes (autotune only) */
-    double  reserved[4];
+    int32_t split_lanes;         /* split-precision pass: lanes per particle (1, 2, 4 or 8; 0 = keep) */
+    int32_t reserved_i;
+    double  reserved[3];
 } dem_tuning;
 
 /* Times the candidate launch shapes of the hot kernels on the handle's

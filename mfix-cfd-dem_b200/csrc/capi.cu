@@ -265,10 +265,14 @@ int stats_range(dem_handle* h, int off, int cnt, dem_stats* s) {
 }  // namespace demb
 
 // Interior DES cells per axis at least 1 and, with the ghost layers, within
-// the packed (i, j, k) of the pair build.
+// the packed (i, j, k) of the pair build; at most MAX_GRID_CELLS cells in
+// all, so that every cell index fits an int.
 bool demb::des_grid_ok(const dem_params& q) {
   if (q.dg_imax < 1 || q.dg_jmax < 1 || (!q.no_k && q.dg_kmax < 1)) return false;
-  return q.dg_imax + 2 <= DG_MAX_IK && q.dg_jmax + 2 <= DG_MAX_J && (q.no_k || q.dg_kmax + 2 <= DG_MAX_IK);
+  if (!(q.dg_imax + 2 <= DG_MAX_IK && q.dg_jmax + 2 <= DG_MAX_J && (q.no_k || q.dg_kmax + 2 <= DG_MAX_IK)))
+    return false;
+  const long long cells = (long long)(q.dg_imax + 2) * (q.dg_jmax + 2) * (q.no_k ? 1 : q.dg_kmax + 2);
+  return cells <= MAX_GRID_CELLS;
 }
 
 void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
@@ -312,17 +316,39 @@ void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
   // particle among large ones scans few.  The reference's own DES-grid
   // stencil (reduced to the nearer cells when the DES cells are wider than
   // the search diameter) is applied to the candidates afterwards.  An axis
-  // keeps the DES grid's division when that is not coarser.
+  // keeps the DES grid's division when that is not coarser.  The grid is an
+  // acceleration structure, so it may be coarser than that and stay exact:
+  // its cell count is held to max(DES cells, 8 n + 65536) and to
+  // MAX_GRID_CELLS (a few small spheres in a large box would otherwise ask
+  // for billions of cells), scaling every refined axis down together.
   const int dgn[3] = {q.dg_imax, q.dg_jmax, q.no_k ? 1 : q.dg_kmax};
   const double target = q.factor_rlm * q.max_radius * 1.01;
+  double len[3], want[3];
   for (int a = 0; a < 3; ++a) {
-    const double len = (double)dgn[a] / p.dg_inv[a];
-    int nfa = (int)std::floor(len / target);
+    len[a] = (double)dgn[a] / p.dg_inv[a];
+    want[a] = (a == 2 && q.no_k) ? (double)dgn[a] : std::max((double)dgn[a], std::floor(len[a] / target));
+  }
+  const long long ndes = (long long)(dgn[0] + 2) * (dgn[1] + 2) * (q.no_k ? 1 : dgn[2] + 2);
+  const long long cap = std::min<long long>(MAX_GRID_CELLS, std::max<long long>(ndes, 8LL * n + 65536));
+  for (int it = 0; it < 64; ++it) {
+    const double cells = (want[0] + 2) * (want[1] + 2) * (q.no_k ? 1.0 : want[2] + 2);
+    if (cells <= (double)cap) break;
+    const double sc = std::max(0.5, std::cbrt((double)cap / cells) * 0.99);
+    bool shrunk = false;
+    for (int a = 0; a < 3; ++a) {
+      if ((a == 2 && q.no_k) || want[a] <= dgn[a]) continue;
+      want[a] = std::max((double)dgn[a], std::floor(want[a] * sc));
+      shrunk = true;
+    }
+    if (!shrunk) break;
+  }
+  for (int a = 0; a < 3; ++a) {
+    int nfa = (int)want[a];
     if (nfa <= dgn[a] || (a == 2 && q.no_k)) nfa = dgn[a];
     if (nfa < 1) nfa = 1;
     p.fn[a] = nfa;
     // same division as the DES grid -> the same inverse width, bit for bit
-    p.f_inv[a] = nfa == dgn[a] ? p.dg_inv[a] : (double)nfa / len;
+    p.f_inv[a] = nfa == dgn[a] ? p.dg_inv[a] : (double)nfa / len[a];
   }
   p.fc1 = p.fn[1] + 2;
   p.fc2 = p.fc1 * (p.fn[0] + 2);
@@ -491,7 +517,7 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->d_ibc, h->pic_fresh, h->d_seed, h->skin, h->vslot, h->pgap,
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflagb[0], h->pflagb[1], h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->d_ibc, h->pic_fresh, h->d_seed, h->skin, h->vslot, h->pgap,
                   h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -514,6 +540,17 @@ int dem_set_stream(dem_handle* h, void* stream) {
 int dem_launch_count(const dem_handle* h, int64_t* count) {
   if (!h || !count) return DEM_ERR_ARG;
   *count = h->launches;
+  return 0;
+}
+
+int dem_set_dtsolid(dem_handle* h, double dtsolid) {
+  SINGLE_GUARD(h);
+  if (!(dtsolid > 0.0) || !std::isfinite(dtsolid)) return set_err(h, DEM_ERR_ARG, "DTSOLID must be positive");
+  if (h->prm.dtsolid != dtsolid) {
+    h->prm.dtsolid = dtsolid;
+    h->dp.dt = dtsolid;
+    invalidate_graphs(h);  // captured steps hold the old DTSOLID
+  }
   return 0;
 }
 
@@ -789,8 +826,10 @@ static int replay_period(dem_handle* h, int nn0) {
   h->launches += h->graph_kernels[key];
   // buffer parities and bookkeeping after the period: N force passes flip
   // the state buffers, the rebuild flips the list and history buffers
+  const bool split = h->dp.prec == DEM_PREC_SPLIT;
   for (int j = 0; j < nsn; ++j) {
     h->cur = 1 - h->cur;
+    if (split) h->pcur = 1 - h->pcur;  // each split pass writes the other history buffer
     h->s_time = h->s_time + h->prm.dtsolid;
     h->steps_done++;
   }

@@ -44,8 +44,8 @@ struct Gas {
 namespace demb {
 
 struct GasDev {  // by-value kernel view
-  int imax, jmax, kmax, gi2, gj2, gk2, ncell, M, no_k;
-  double vol, pi, ro_g, mu_g, ur_f_gs;
+  int imax, jmax, kmax, gi2, gj2, gk2, ncell, M, no_k, drag_model;
+  double vol, pi, ro_g, mu_g, ur_f_gs, usr_d_p0;
   double ro_s[MAXP];
   const double *xe, *yn, *zt;
 };
@@ -146,6 +146,17 @@ __device__ __forceinline__ double drag_gidaspow(double epg, double mug, double r
   return 0.75 * cd * vrel * ropg * pow(epg, -2.65) / dpm;
 }
 
+// The single-sphere user drag of DEM_DRAG_SINGLE_SPHERE (tests/dem/DEM06:
+// usr_drag.f, usr_mod.f Re and Cd): 0.75*(RO_g*|u|/d_p)*Cd(Re) with
+// Re = RO_g*d_ref*|u|/MU_g and Cd = (24/Re)*(1 + 0.15*Re**0.687), the
+// exponent a default-real literal widened to double.
+__device__ __forceinline__ double drag_single_sphere(double mug, double rog, double vrel, double dpm, double dref) {
+  const double re = (rog * dref * vrel) / mug;
+  double cd = 0.0;
+  if (re > 0.0) cd = (24.0 / re) * (1.0 + 0.15 * pow(re, (double)0.687f));
+  return 0.75 * (rog * vrel / dpm) * cd;
+}
+
 // Gas velocity at a particle of fluid cell (i,j,k): staggered face
 // velocities averaged to the cell's 2x2x2 node stencil, interpolated with the
 // trilinear weights, which are returned too (drag_gs_des0.f:117-170 and
@@ -189,7 +200,9 @@ __device__ __forceinline__ double relaxed_fgp(const GasDev& G, double epg, doubl
   const double vs[3] = {velfp[0] - V.x, velfp[1] - V.y, velfp[2] - V.z};
   const double vrel = sqrt(dot3(vs, vs));
   const double dpm = 2.0 * r;
-  const double dga = drag_gidaspow(epg, G.mu_g, G.ro_g, G.ro_g * epg, vrel, dpm);
+  const double dga = G.drag_model == DEM_DRAG_SINGLE_SPHERE
+                         ? drag_single_sphere(G.mu_g, G.ro_g, vrel, dpm, G.usr_d_p0)
+                         : drag_gidaspow(epg, G.mu_g, G.ro_g, G.ro_g * epg, vrel, dpm);
   *pvol = ((4.0 / 3.0) * G.pi) * (r * (r * r));
   const double fgs = dga * *pvol;
   return (1.0 - G.ur_f_gs) * f_old + G.ur_f_gs * fgs;
@@ -448,12 +461,48 @@ __global__ void k_cell_fields(GasDev G, const double* __restrict__ vol_surr, con
   for (int m = 0; m < G.M; ++m) rop_s[(size_t)m * G.ncell + c] = acc[m];
 }
 
+// CALC_DES_BEDHEIGHT (des_granular_temperature.f:201-267) partial sums:
+// thread per fluid cell in IJK order, its (EP_S*h*VOL, EP_S*VOL) per phase
+// when ROP_S > 0, added over the block in a fixed tree order; the host adds
+// the blocks in order.  part[(block * M + m) * 2 + {0, 1}].
+constexpr int BED_T = 256;
+__global__ void k_bed_partials(GasDev G, const double* __restrict__ rop_s, double* __restrict__ part) {
+  __shared__ double sn[BED_T], sd[BED_T];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = c < G.ncell ? (c / G.gi2) % G.gj2 + 1 : 1;
+  const double hcell = 0.5 * (G.yn[j] + G.yn[j - 1]);
+  for (int m = 0; m < G.M; ++m) {
+    double a = 0.0, b = 0.0;
+    if (c < G.ncell) {
+      const double r = rop_s[(size_t)m * G.ncell + c];
+      if (r > 0.0) {
+        const double ep = r / G.ro_s[m];
+        a = ep * hcell * G.vol;
+        b = ep * G.vol;
+      }
+    }
+    sn[threadIdx.x] = a;
+    sd[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = BED_T / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) { sn[threadIdx.x] += sn[threadIdx.x + s]; sd[threadIdx.x] += sd[threadIdx.x + s]; }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      part[((size_t)blockIdx.x * G.M + m) * 2] = sn[0];
+      part[((size_t)blockIdx.x * G.M + m) * 2 + 1] = sd[0];
+    }
+    __syncthreads();
+  }
+}
+
 static GasDev gas_view(dem_handle* h) {
   Gas* s = h->gas;
   GasDev G;
   G.imax = s->g.imax; G.jmax = s->g.jmax; G.kmax = s->g.kmax;
   G.gi2 = s->gi2; G.gj2 = s->gj2; G.gk2 = s->gk2; G.ncell = s->ncell; G.M = s->M; G.no_k = h->dp.no_k;
   G.vol = s->vol; G.pi = s->pi; G.ro_g = s->g.ro_g; G.mu_g = s->g.mu_g; G.ur_f_gs = s->g.ur_f_gs;
+  G.drag_model = s->g.drag_model; G.usr_d_p0 = s->g.usr_d_p0;
   for (int m = 0; m < MAXP; ++m) G.ro_s[m] = s->g.ro_s[m];
   G.xe = s->xe; G.yn = s->yn; G.zt = s->zt;
   return G;
@@ -592,6 +641,10 @@ int dem_set_gas_fields(dem_handle* h, const dem_fluid_grid* g, const double* ep_
     if (!(g->ro_s[m] > 0.0)) return set_err(h, DEM_ERR_ARG, "ro_s must be positive");
   if (g->interp_scheme != DEM_INTERP_GARG && g->interp_scheme != DEM_INTERP_NONE)
     return set_err(h, DEM_ERR_ARG, "unknown interp_scheme");
+  if (g->drag_model != DEM_DRAG_GIDASPOW && g->drag_model != DEM_DRAG_SINGLE_SPHERE)
+    return set_err(h, DEM_ERR_ARG, "unknown drag_model");
+  if (g->drag_model == DEM_DRAG_SINGLE_SPHERE && !(g->usr_d_p0 > 0.0))
+    return set_err(h, DEM_ERR_ARG, "usr_d_p0 must be positive for the single-sphere drag");
   free_gas(h);
   Gas* s = new Gas();
   h->gas = s;
@@ -700,6 +753,40 @@ int dem_comp_mean_fields(dem_handle* h) {
   if (!h->gas) return set_err(h, DEM_ERR_STATE, "no gas fields");
   if (int rc = run_mean_fields(h)) return rc;
   return fetch_errors(h);
+}
+
+int dem_calc_des_bedheight(dem_handle* h, double* bed_height) {
+  API_GUARD(h);
+  if (!h->gas) return set_err(h, DEM_ERR_STATE, "no gas fields");
+  if (!bed_height) return set_err(h, DEM_ERR_ARG, "null output");
+  Gas* s = h->gas;
+  const GasDev G = gas_view(h);
+  const int M = s->M, nb = (s->ncell + BED_T - 1) / BED_T;
+  double* part = (double*)stage_buffer(h, sizeof(double) * 2 * M * (size_t)nb + 64);
+  if (!part) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
+  k_bed_partials<<<nb, BED_T, 0, h->stream>>>(G, s->rop_s, part);
+  DEM_LAUNCH(h);
+  std::vector<double> hp((size_t)2 * M * nb);
+  cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(h->herr, h->derr, sizeof(DevErr), cudaMemcpyDeviceToHost, h->stream);
+  if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "bed height")) return rc;
+  // the block partials in block order
+  std::vector<double> num(M, 0.0), den(M, 0.0);
+  for (int b = 0; b < nb; ++b)
+    for (int m = 0; m < M; ++m) {
+      num[m] += hp[((size_t)b * M + m) * 2];
+      den[m] += hp[((size_t)b * M + m) * 2 + 1];
+    }
+  // PIP > 0: some particle exists
+  int pip = 0;
+  {
+    std::vector<int8_t> st(h->n);
+    cudaMemcpyAsync(st.data(), h->state, h->n, cudaMemcpyDeviceToHost, h->stream);
+    if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "bed height")) return rc;
+    for (int8_t v : st) pip += v != DEM_STATE_NONEXISTENT;
+  }
+  for (int m = 0; m < M; ++m) bed_height[m] = pip > 0 ? num[m] / den[m] : 0.0;
+  return 0;
 }
 
 int dem_drag_gs_des0(dem_handle* h) {

@@ -214,6 +214,7 @@ struct dem_handle {
     int pair_threads = 256, pair_bpsm = 8;  // pair kernel: threads per block, resident blocks per SM
     int gather_threads = 256;               // gather kernel: threads per block
     int neigh_threads = 128;                // pair-build scan: threads per block
+    int split_lanes = 4;                    // split-precision pass: lanes per particle
   } tune;
   bool capturing = false;     // inside a CUDA graph capture: no host syncs
   cudaStream_t own_stream = nullptr;
@@ -230,7 +231,11 @@ struct dem_handle {
   int* in_fill = nullptr;     // n
   int2* in_pair = nullptr;    // cap
   int* pair_owner = nullptr;  // cap
-  uint8_t* pflag = nullptr;   // cap: PF_* bits of each pair (stencil-rank scratch during the build)
+  // cap: PF_* bits of each pair, one array per history buffer: pflagb[pcur]
+  // goes with pft[pcur] (the other is stencil-rank scratch during a build
+  // and the output of a split-precision force pass)
+  uint8_t* pflagb[2] = {nullptr, nullptr};
+  uint8_t* pflag() const { return pflagb[pcur]; }
   uint8_t* touched = nullptr; // n: 1 = in some pair contact at the current force pass
   uint8_t* wall_hit = nullptr; // n: 1 = in some wall contact (its terms are in wf)
   float* pgap = nullptr;      // cap: gap |d| - (r_i + r_j) of each pair at the last build, rounded down
@@ -324,8 +329,7 @@ int run_force(dem_handle* h, bool fused);
 int run_cfnewvalues(dem_handle* h);
 int run_bin_facets(dem_handle* h, const double* vertex_fortran, const double* norm_fortran, int nf);
 int run_split_force_error(dem_handle* h, double* rel_err);
-void launch_pairs_split(dem_handle* h);         // force_split.cu
-void launch_gather_split(dem_handle* h, int mode);
+void launch_force_split(dem_handle* h, int mode);  // force_split.cu: fused split-precision pass
 int ensure_pair_capacity(dem_handle* h, long long need);
 int build_transpose(dem_handle* h, int nb);    // neighbor.cu
 void launch_neigh_count(dem_handle* h);        // neighbor.cu: count pass of the pair build
@@ -404,6 +408,10 @@ __device__ __forceinline__ void unpack_ijk(int c, int& i, int& j, int& k) {
   j = (c >> 10) & 4095;
   k = (c >> 22) & 1023;
 }
+
+// Cells of the DES grid, and of the search grid of the pair build, at most
+// (with their ghost layers): every cell index and count fits an int.
+constexpr long long MAX_GRID_CELLS = 1LL << 28;
 
 // Neighbours per particle kept by the count pass of the pair build.
 constexpr int NSLOT = 16;

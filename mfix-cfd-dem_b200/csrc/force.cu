@@ -846,7 +846,7 @@ static void launch_pairs_t(dem_handle* h) {
   const int T = h->tune.pair_threads;
   k_pairs<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
       h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->pos4[c], h->vel4[c], h->omg4[c],
-      h->state, h->phase, h->pft[h->pcur], h->pflag, h->touched, h->pgap, h->skin, h->prec, h->derr);
+      h->state, h->phase, h->pft[h->pcur], h->pflag(), h->touched, h->pgap, h->skin, h->prec, h->derr);
   DEM_LAUNCH(h);
 }
 
@@ -855,7 +855,7 @@ static void launch_gather_t(dem_handle* h) {
   const int T = h->tune.gather_threads, G = (h->n + T - 1) / T;
   const int c = h->cur;
   k_gather<MODE, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
-                                            h->vel4[1 - c], h->omg4[1 - c], h->state, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag,
+                                            h->vel4[1 - c], h->omg4[1 - c], h->state, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag(),
                                             h->touched, h->wall_hit, h->prec, h->fc, h->tow, h->acc_old,
                                             h->rot_acc_old, h->vslot, gather_cells<MODE, B>(h));
   DEM_LAUNCH(h);
@@ -893,35 +893,42 @@ static void launch_gather_fp64(dem_handle* h, int mode) {
   else launch_gather_t<2, B>(h);
 }
 
+// The two timed parts of the force step for the autotuner.  The split path
+// has no separate pair kernel: its fused pass is the "gather" part.
 void launch_pairs_only(dem_handle* h) {
-  if (h->dp.prec == DEM_PREC_SPLIT) launch_pairs_split(h);
-  else if (h->batch()) launch_pairs_fp64<true>(h);
+  if (h->dp.prec == DEM_PREC_SPLIT) return;
+  if (h->batch()) launch_pairs_fp64<true>(h);
   else launch_pairs_fp64<false>(h);
 }
 
 void launch_gather_only(dem_handle* h) {
-  if (h->dp.prec == DEM_PREC_SPLIT) launch_gather_split(h, 0);
+  if (h->dp.prec == DEM_PREC_SPLIT) launch_force_split(h, 0);
   else if (h->batch()) launch_gather_fp64<true>(h, 0);
   else launch_gather_fp64<false>(h, 0);
 }
 
 // Contact forces of the current state.  mode: 0 = into FC/TOW, 1/2 = fused
 // Euler/AB2 integration into the other state buffer.  The collision model,
-// integrator and force precision are common to all systems of a batch.
+// integrator and force precision are common to all systems of a batch.  The
+// split pass reads history buffer pcur and writes the other one (run_force
+// flips pcur after it).
 static void launch_force_kernels(dem_handle* h, int mode, bool split) {
   {
     ProfScope ps(h, DEM_PROF_WALLS);
     launch_walls(h);
   }
+  if (split) {
+    ProfScope ps(h, DEM_PROF_GATHER);
+    launch_force_split(h, mode);
+    return;
+  }
   {
     ProfScope ps(h, DEM_PROF_PAIRS);
-    if (split) launch_pairs_split(h);
-    else if (h->batch()) launch_pairs_fp64<true>(h);
+    if (h->batch()) launch_pairs_fp64<true>(h);
     else launch_pairs_fp64<false>(h);
   }
   ProfScope ps(h, DEM_PROF_GATHER);
-  if (split) launch_gather_split(h, mode);
-  else if (h->batch()) launch_gather_fp64<true>(h, mode);
+  if (h->batch()) launch_gather_fp64<true>(h, mode);
   else launch_gather_fp64<false>(h, mode);
 }
 
@@ -949,9 +956,11 @@ int run_force(dem_handle* h, bool fused) {
   ProfScope ps(h, DEM_PROF_FORCE);
   h->dp.first_pass = h->first_pass ? 1 : 0;
   const int mode = !fused ? 0 : (h->dp.intg == DEM_INTG_AB2 ? 2 : 1);
-  launch_force_kernels(h, mode, h->dp.prec == DEM_PREC_SPLIT);
+  const bool split = h->dp.prec == DEM_PREC_SPLIT;
+  launch_force_kernels(h, mode, split);
   if (fused) launch_skin(h);
   if (int rc = check_cuda(h, cudaGetLastError(), "force kernels")) return rc;
+  if (split) h->pcur = 1 - h->pcur;  // the pass wrote the other history buffer
   if (fused) { h->cur = 1 - h->cur; h->first_pass = false; }
   return 0;
 }
@@ -978,7 +987,7 @@ int run_split_force_error(dem_handle* h, double* rel_err) {
     cudaMemcpyAsync(s_live, h->wall_live, n, cudaMemcpyDeviceToDevice, h->stream);
     if (P) {
       cudaMemcpyAsync(s_hist, h->pft[h->pcur], b_hist, cudaMemcpyDeviceToDevice, h->stream);
-      cudaMemcpyAsync(s_flag, h->pflag, P, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(s_flag, h->pflag(), P, cudaMemcpyDeviceToDevice, h->stream);
     }
   };
   auto restore = [&]() {
@@ -987,7 +996,7 @@ int run_split_force_error(dem_handle* h, double* rel_err) {
     cudaMemcpyAsync(h->wall_live, s_live, n, cudaMemcpyDeviceToDevice, h->stream);
     if (P) {
       cudaMemcpyAsync(h->pft[h->pcur], s_hist, b_hist, cudaMemcpyDeviceToDevice, h->stream);
-      cudaMemcpyAsync(h->pflag, s_flag, P, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(h->pflag(), s_flag, P, cudaMemcpyDeviceToDevice, h->stream);
     }
   };
   std::vector<double> f64(3 * n), f32(3 * n);

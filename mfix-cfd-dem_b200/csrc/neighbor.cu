@@ -476,7 +476,7 @@ void launch_pair_gaps(dem_handle* h) {
 
 void set_hist_flags(dem_handle* h) {
   const int T = 256;
-  k_hist_flags<<<pair_grid(h, T), T, 0, h->stream>>>(h->d_np, h->pft[h->pcur], h->pflag);
+  k_hist_flags<<<pair_grid(h, T), T, 0, h->stream>>>(h->d_np, h->pft[h->pcur], h->pflag());
   DEM_LAUNCH(h);
 }
 
@@ -541,14 +541,14 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   long long cap = h->pair_cap > 0 ? h->pair_cap : 1024;
   while (cap < need) cap *= 2;
   const long long old = h->pair_cap;  // the whole old allocation (the count may be stale)
-  int* nb[2]; double* pf[2]; int2* inp; int* own; uint8_t* pfl; PairRec* prc; float* gap;
+  int* nb[2]; double* pf[2]; int2* inp; int* own; uint8_t* pfl[2]; PairRec* prc; float* gap;
   for (int b = 0; b < 2; ++b) {
     if (int rc = check_cuda(h, cudaMalloc(&nb[b], sizeof(int) * cap), "cudaMalloc nbrs")) return rc;
     if (int rc = check_cuda(h, cudaMalloc(&pf[b], sizeof(double) * 3 * cap), "cudaMalloc pft")) return rc;
+    if (int rc = check_cuda(h, cudaMalloc(&pfl[b], cap), "cudaMalloc pflag")) return rc;
   }
   if (int rc = check_cuda(h, cudaMalloc(&inp, sizeof(int2) * cap), "cudaMalloc in_pair")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&own, sizeof(int) * cap), "cudaMalloc owner")) return rc;
-  if (int rc = check_cuda(h, cudaMalloc(&pfl, cap), "cudaMalloc pflag")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&prc, sizeof(PairRec) * cap), "cudaMalloc prec")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&gap, sizeof(float) * cap), "cudaMalloc pgap")) return rc;
   if (old > 0) {
@@ -557,13 +557,16 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
     cudaMemcpyAsync(pf[h->pcur], h->pft[h->pcur], sizeof(double) * 3 * old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(inp, h->in_pair, sizeof(int2) * old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(own, h->pair_owner, sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
-    cudaMemcpyAsync(pfl, h->pflag, old, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(pfl[h->pcur], h->pflag(), old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(gap, h->pgap, sizeof(float) * old, cudaMemcpyDeviceToDevice, h->stream);
   }
   cudaStreamSynchronize(h->stream);
-  for (int b = 0; b < 2; ++b) { cudaFree(h->nbrs[b]); cudaFree(h->pft[b]); h->nbrs[b] = nb[b]; h->pft[b] = pf[b]; }
-  cudaFree(h->in_pair); cudaFree(h->pair_owner); cudaFree(h->pflag); cudaFree(h->prec); cudaFree(h->pgap);
-  h->in_pair = inp; h->pair_owner = own; h->pflag = pfl; h->prec = prc; h->pgap = gap;
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(h->nbrs[b]); cudaFree(h->pft[b]); cudaFree(h->pflagb[b]);
+    h->nbrs[b] = nb[b]; h->pft[b] = pf[b]; h->pflagb[b] = pfl[b];
+  }
+  cudaFree(h->in_pair); cudaFree(h->pair_owner); cudaFree(h->prec); cudaFree(h->pgap);
+  h->in_pair = inp; h->pair_owner = own; h->prec = prc; h->pgap = gap;
   h->pair_cap = cap;
   invalidate_graphs(h);  // captured steps point at the old arrays
   return check_cuda(h, cudaGetLastError(), "grow pairs");
@@ -628,14 +631,14 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   const int TN = h->tune.neigh_threads, BN = (n + TN - 1) / TN;
   if (bt) {
     k_neigh<true, true><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, e, h->row_cnt,
-                                                  h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->nslot,
+                                                  h->row_end[nb], h->nbrs[nb], h->pflagb[1 - h->pcur], h->pair_owner, h->nslot,
                                                   h->pair_cap);
     k_keep_rows<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], nullptr, h->row_end[nb],
                                               h->nbrs[nb], h->pair_owner, h->pair_cap);
     DEM_LAUNCH(h);
   } else {
     k_neigh<true, false><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, e, h->row_cnt,
-                                                   h->row_end[nb], h->nbrs[nb], h->pflag, h->pair_owner, h->nslot,
+                                                   h->row_end[nb], h->nbrs[nb], h->pflagb[1 - h->pcur], h->pair_owner, h->nslot,
                                                    h->pair_cap);
   }
   DEM_LAUNCH(h);
@@ -653,10 +656,10 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   const int have_old = (carry_history && h->have_pairs) ? 1 : 0;
   if (bt)
     k_remap<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
-                                          h->pft[h->pcur], h->pft[pn], h->pflag, have_old);
+                                          h->pft[h->pcur], h->pft[pn], h->pflagb[pn], have_old);
   else
     k_remap<false><<<B, T, 0, h->stream>>>(n, bv, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
-                                           h->pft[h->pcur], h->pft[pn], h->pflag, have_old);
+                                           h->pft[h->pcur], h->pft[pn], h->pflagb[pn], have_old);
   DEM_LAUNCH(h);
   h->rb = nb;
   h->pcur = pn;

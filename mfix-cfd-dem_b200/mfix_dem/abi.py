@@ -18,6 +18,8 @@ DEM_PREC_SPLIT = 1
 
 DEM_INTERP_GARG = 0
 DEM_INTERP_NONE = 1
+DEM_DRAG_GIDASPOW = 0
+DEM_DRAG_SINGLE_SPHERE = 1
 
 DEM_STATE_NONEXISTENT = 0
 DEM_STATE_NORMAL = 1
@@ -140,7 +142,8 @@ class DemFluidGrid(C.Structure):
         ("ep_star", C.c_double),
         ("ur_f_gs", C.c_double),
         ("ro_s", C.c_double * DEM_MAX_PHASES),
-        ("reserved", C.c_double * 6),
+        ("usr_d_p0", C.c_double),
+        ("reserved", C.c_double * 5),
     ]
 
 
@@ -153,11 +156,13 @@ class DemTuning(C.Structure):
         ("pair_ms", C.c_double),
         ("gather_ms", C.c_double),
         ("neigh_ms", C.c_double),
-        ("reserved", C.c_double * 4),
+        ("split_lanes", C.c_int32),
+        ("reserved_i", C.c_int32),
+        ("reserved", C.c_double * 3),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 
 class DemBatchLimits(C.Structure):
@@ -302,6 +307,8 @@ SIGNATURES = {
     "set_gas_fields": (C.c_int, [_P, C.POINTER(DemFluidGrid), _D, _D, _D, _D, _D]),
     "get_mean_fields": (C.c_int, [_P, _D, _D]),
     "comp_mean_fields": (C.c_int, [_P]),
+    "set_dtsolid": (C.c_int, [_P, C.c_double]),
+    "calc_des_bedheight": (C.c_int, [_P, _D]),
     "drag_gs_des0": (C.c_int, [_P]),
     "drag_gs_gas0": (C.c_int, [_P, _D, _D, _D, _D]),
     "drag_gs_des1": (C.c_int, [_P]),

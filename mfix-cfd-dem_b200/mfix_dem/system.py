@@ -223,6 +223,11 @@ class DemSystem:
         """MAKE_ARRAYS_DES tail: DESGRID_PIC + NEIGHBOUR on the uploaded state."""
         self._call("init_neighbors", self._h)
 
+    def set_dtsolid(self, dt: float):
+        """DTSOLID of the following steps (a coupled driver's shortened last
+        DEM step of a fluid step, and its restore)."""
+        self._call("set_dtsolid", self._h, C.c_double(float(dt)))
+
     def step(self, nsteps: int = 1, nn_first: Optional[int] = None):
         """DES_TIME_STEP(NN) for the next nsteps values of NN."""
         first = self.nn + 1 if nn_first is None else nn_first
@@ -259,6 +264,12 @@ class DemSystem:
 
     def comp_mean_fields(self):
         self._call("comp_mean_fields", self._h)
+
+    def calc_des_bedheight(self) -> np.ndarray:
+        """CALC_DES_BEDHEIGHT per solids phase from the last mean fields."""
+        out = np.zeros(self.params.n_phases)
+        self._call("calc_des_bedheight", self._h, _dp(out))
+        return out
 
     def drag_gs_des0(self):
         self._call("drag_gs_des0", self._h)
@@ -352,6 +363,7 @@ class DemSystem:
         t = abi.DemTuning()
         for k in ("pair_threads", "pair_blocks_per_sm", "gather_threads", "neigh_threads"):
             setattr(t, k, int(tuning[k]))
+        t.split_lanes = int(tuning.get("split_lanes", 0))
         self._call("set_tuning", self._h, C.byref(t))
 
     def force_error(self) -> float:

@@ -1058,6 +1058,16 @@ struct Oracle {
     return 0.75 * cd * vrel * ropg * std::pow(epg, -2.65) / dpm;
   }
 
+  // The DEM06 regression's user drag (usr_drag.f with usr_mod.f Re, Cd):
+  // 0.75*(RO_g*VREL/DPM)*Cd(Re), Re = (RO_g0*D_p0*Vs)/MU_g0,
+  // Cd = (24/Re)*(1 + 0.15*Re**0.687) with a default-real exponent.
+  static double drag_single_sphere(double mug, double rog, double vrel, double dpm, double dref) {
+    const double re = (rog * dref * vrel) / mug;
+    double cd = 0.0;
+    if (re > 0.0) cd = (24.0 / re) * (1.0 + 0.15 * std::pow(re, (double)0.687f));
+    return 0.75 * (rog * vrel / dpm) * cd;
+  }
+
   // Gas velocity at a particle of fluid cell (i,j,k): the staggered face
   // velocities averaged to the 2x2x2 node stencil and interpolated with the
   // trilinear weights (drag_gs_des0.f:117-170 and 313-361,
@@ -1100,7 +1110,8 @@ struct Oracle {
     double vs[3] = {velfp[0] - vp[0], velfp[1] - vp[1], velfp[2] - vp[2]};
     double vrel = std::sqrt(dot3(vs, vs));
     double dpm = 2.0 * rad[l];
-    double dga = drag_gidaspow(epg, g.mu_g, g.ro_g, g.ro_g * epg, vrel, dpm);
+    double dga = g.drag_model == DEM_DRAG_SINGLE_SPHERE ? drag_single_sphere(g.mu_g, g.ro_g, vrel, dpm, g.usr_d_p0)
+                                                        : drag_gidaspow(epg, g.mu_g, g.ro_g, g.ro_g * epg, vrel, dpm);
     double pvol = ((4.0 / 3.0) * pi_c) * (rad[l] * (rad[l] * rad[l]));
     double fgs = dga * pvol;
     f_gp[l] = (1.0 - g.ur_f_gs) * f_gp[l] + g.ur_f_gs * fgs;
@@ -1593,6 +1604,13 @@ int orc_destroy(orc_handle* h) { delete h; return 0; }
 const char* orc_last_error(const orc_handle* h) { return h ? h->o.err.c_str() : "null handle"; }
 int orc_set_threads(orc_handle* h, int32_t nt) { h->o.nthreads = nt < 1 ? 1 : nt; return 0; }
 
+// DTSOLID of the following steps (des_time_march.f:308-314, 470-476).
+int orc_set_dtsolid(orc_handle* h, double dtsolid) {
+  if (!(dtsolid > 0.0) || !std::isfinite(dtsolid)) return h->o.fail(DEM_ERR_ARG, "DTSOLID must be positive");
+  h->o.p.dtsolid = dtsolid;
+  return 0;
+}
+
 int orc_set_walls(orc_handle* h, const double* vertex, const double* norm_face, int32_t nf) {
   Oracle& o = h->o;
   if (nf < 0) return DEM_ERR_ARG;
@@ -1861,6 +1879,10 @@ int orc_set_gas_fields(orc_handle* h, const dem_fluid_grid* g, const double* ep_
   if (!o.have_state) return o.fail(DEM_ERR_STATE, "upload particles first");
   if (g->interp_scheme != DEM_INTERP_GARG && g->interp_scheme != DEM_INTERP_NONE)
     return o.fail(DEM_ERR_ARG, "unknown interp_scheme");
+  if (g->drag_model != DEM_DRAG_GIDASPOW && g->drag_model != DEM_DRAG_SINGLE_SPHERE)
+    return o.fail(DEM_ERR_ARG, "unknown drag_model");
+  if (g->drag_model == DEM_DRAG_SINGLE_SPHERE && !(g->usr_d_p0 > 0.0))
+    return o.fail(DEM_ERR_ARG, "usr_d_p0 must be positive for the single-sphere drag");
   o.g = *g;
   o.gas_setup();
   size_t nc = o.vol_surr.size();
@@ -1885,6 +1907,34 @@ int orc_get_mean_fields(orc_handle* h, double* ep_g, double* rop_s) {
     if (o.rop_s.empty()) std::fill(rop_s, rop_s + o.vol_surr.size(), 0.0);
     else std::copy(o.rop_s.begin(), o.rop_s.begin() + o.vol_surr.size(), rop_s);
   }
+  return 0;
+}
+// CALC_DES_BEDHEIGHT (des_granular_temperature.f:201-267): the serial loop
+// over IJKSTART3..IJKEND3 with EP_S = ROP_S/RO_S and the cell-centre height.
+int orc_calc_des_bedheight(orc_handle* h, double* bed_height) {
+  Oracle& o = h->o;
+  if (!o.have_gas) return o.fail(DEM_ERR_STATE, "no gas fields");
+  if (!bed_height) return o.fail(DEM_ERR_ARG, "null output");
+  const int M = o.p.n_phases;
+  const size_t nc = o.vol_surr.size();
+  std::vector<double> num(M, 0.0), den(M, 0.0);
+  if (!o.rop_s.empty()) {
+    for (size_t ijk = 0; ijk < nc; ++ijk) {
+      const int j = (int)((ijk / (size_t)o.gi2) % (size_t)o.gj2) + 1;
+      for (int m = 0; m < M; ++m) {
+        const double r = o.rop_s[(size_t)m * nc + ijk];
+        if (r > 0.0) {
+          const double hcell = 0.5 * (o.yn[j] + o.yn[j - 1]);
+          const double ep = r / o.ro_s[m];
+          num[m] = num[m] + ep * hcell * o.vol();
+          den[m] = den[m] + ep * o.vol();
+        }
+      }
+    }
+  }
+  int pip = 0;
+  for (int l = 0; l < o.n; ++l) pip += o.state[l] != DEM_STATE_NONEXISTENT;
+  for (int m = 0; m < M; ++m) bed_height[m] = pip > 0 ? num[m] / den[m] : 0.0;
   return 0;
 }
 int orc_comp_mean_fields(orc_handle* h) {

@@ -43,10 +43,19 @@ def host_cpu_key() -> str:
     return hashlib.sha1(text.encode()).hexdigest()[:12]
 
 
+def source_key() -> str:
+    """A short key for the oracle's sources, so a stale build is not loaded."""
+    import hashlib
+    h = hashlib.sha1()
+    for f in (HERE / "dem_oracle.cpp", HERE / "dem_oracle.h", ROOT / "include" / "dem_b200.h"):
+        h.update(f.read_bytes())
+    return h.hexdigest()[:10]
+
+
 def native_path() -> Path:
-    """The OpenMP timing build with -march=native for this host's CPU,
-    compiled here on first use (a few seconds of g++)."""
-    d = HERE / "_build" / f"native_{host_cpu_key()}"
+    """The OpenMP timing build with -march=native for this host's CPU and
+    the current sources, compiled here on first use (a few seconds of g++)."""
+    d = HERE / "_build" / f"native_{host_cpu_key()}_{source_key()}"
     path = d / "liboracle_omp.so"
     if not path.exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "native", f"NATIVE_DIR={d}"], check=True)

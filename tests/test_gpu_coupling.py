@@ -32,6 +32,26 @@ def test_mean_fields_bitwise():
     assert np.array_equal(rg, ro)
 
 
+@pytest.mark.parametrize("interp", ["GARG_2012", "NONE"])
+def test_bed_height_matches_oracle(interp):
+    """CALC_DES_BEDHEIGHT from the mean fields of both interpolation
+    schemes: the GPU adds its cells in blocks, the oracle in the serial IJK
+    order, so the two agree to rounding (1e-12 relative), after a few
+    coupled steps as well."""
+    from oracle_ffi import OracleSystem
+    ct = coupled_case(interp=interp)
+    g = make_coupled(_gpu_system, ct)
+    o = make_coupled(OracleSystem, ct)
+    for s in (g, o):
+        s.comp_mean_fields()
+    hg, ho = g.calc_des_bedheight(), o.calc_des_bedheight()
+    assert np.all(np.isfinite(ho)) and ho[0] > 0
+    assert rel_err(hg, ho) <= 1e-12, (hg, ho)
+    g.step_coupled(30); o.step_coupled(30)
+    hg, ho = g.calc_des_bedheight(), o.calc_des_bedheight()
+    assert rel_err(hg, ho) <= 1e-12, (hg, ho)
+
+
 def test_drag_force_matches():
     from oracle_ffi import OracleSystem
     ct = coupled_case()

@@ -13,7 +13,9 @@ restitution at the end of the run to 4 decimals.  The AUTOTEST
 tables print MFiX's values with 8 decimals at the first DEM step past each
 output time; the oracle must reproduce every printed value to within the
 print resolution (5e-9, plus a small allowance for the rounding of the last
-digit).
+digit).  DEM02 (bounce heights on the floor), DEM04 (slip to roll on a rough
+floor) and the homogeneous cooling system (fully periodic, a neighbour
+search every step) are described at their tests below.
 """
 import json
 import math
@@ -22,6 +24,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
+import golden_runs as G
 from cases import dem01_case, dem03_case, dem05_case, make_system
 from oracle_ffi import OracleSystem
 
@@ -138,3 +141,111 @@ def test_dem05_matches_mfix_table(model):
             _, c_pp, c_pw = tab["coeff"][lc - 2]
             assert abs(vxz[pp] / init_vt[pp] - c_pp) <= tol, (lc, "coeff pp")
             assert abs(vxz[pw] / init_vt[pw] - c_pw) <= tol, (lc, "coeff pw")
+
+
+# ---- DEM02, DEM04, homogeneous cooling -------------------------------------
+# Tables extracted by tests/golden/extract_goldens.py; drivers in golden_runs.py.
+PRINT_8 = 5e-9 + 1e-12   # half a unit of the 8th decimal (F15.8 columns)
+
+
+def _load(name):
+    return json.loads((GOLD / name).read_text())
+
+
+@pytest.mark.parametrize("run_idx", range(18))
+def test_dem02_bounce_heights_match_mfix_table(run_idx):
+    """Every bounce height MFiX printed (POST_HEIGHT.dat: KN = KN_W in
+    {5e4, 5e5, 5e6}, e = 1.0 ... 0.5, Adams-Bashforth) to its 8 decimals."""
+    run = _load("dem02.json")["runs"][run_idx]
+    assert run["intg"] == "ADAMS_BASHFORTH" and run["en"] == run["en_w"] and run["kn"] == run["kn_w"]
+    case, prm, arr, walls = G.dem02_case(run["kn"], run["en"])
+    s = make_system(OracleSystem, prm, arr, walls)
+    last = run["rows"][-1][0]
+    h = G.dem02_heights(s, prm, last_bounce=last)
+    assert len(h) == last + 1
+    for k, hk in run["rows"]:
+        assert abs(h[k] - hk) <= PRINT_8, (k, h[k], hk)
+
+
+@pytest.mark.parametrize("run_idx", range(9))
+def test_dem04_slip_to_roll_matches_mfix_table(run_idx):
+    """The end of slip of a sphere launched along the floor (MEW = MEW_W =
+    0.2 ... 1.0): the scaled time matches MFiX's table to its 8 decimals.
+    The scaled velocities agree within 2e-5 (the AUTOTEST tolerance of the
+    reference is 1e-6 absolute or 5 % relative); at the end of slip the
+    sphere sits in the floor by mg/KN_W, 1e-5 of its radius, the size of
+    that difference, which therefore looks like a lever-arm convention of
+    the build that printed the table (this restatement uses DISTMOD,
+    calc_collision_wall_mod.f:476,606)."""
+    mew, t_nd, tvel, avel = _load("dem04.json")["rows"][run_idx]
+    case, prm, arr, walls = G.dem04_case(mew)
+    s = make_system(OracleSystem, prm, arr, walls)
+    r = G.dem04_roll(s, prm, mew)
+    assert r is not None, "no end of slip within TSTOP"
+    assert abs(r[0] - t_nd) <= PRINT_8, (r[0], t_nd)
+    assert abs(r[1] - tvel) <= 2e-5, (r[1], tvel)
+    assert abs(r[2] - avel) <= 2e-5, (r[2], avel)
+
+
+def _sig5(x, ref):
+    """x printed with G11.5 (5 significant digits) reads as ref."""
+    if ref == 0.0:
+        return abs(x) < 5e-6
+    e = math.floor(math.log10(abs(ref)))
+    return abs(x - ref) <= 0.5 * 10.0 ** (e - 4) + 1e-12
+
+
+HCS_EXACT_ROWS = 31   # output times up to 1.5 s
+
+
+def test_homogeneous_cooling_matches_mfix_table():
+    """195 elastic spheres in a fully periodic cube, a neighbour search every
+    step (legacy_tests/dem-tests/homogeneous-cooling-system): the pairs across
+    the periodic faces come from the minimum image here and from ghost
+    copies (DES_PAR_EXCHANGE) in MFiX.  Every printed value of the first 31
+    outputs (t <= 1.5 s: solids time, granular temperature, kinetic energy,
+    mean velocity) matches to its 5 significant digits.  The system is
+    chaotic, so later rows are compared as statistics: the mean velocity
+    (momentum) stays exact to print, the kinetic energy between collisions
+    returns to the same maximum, and the mean granular temperature over the
+    remaining rows agrees within 1 %."""
+    d = _load("hcs.json")
+    case, prm, arr, walls = G.hcs_case(d["particle_input"])
+    s = make_system(OracleSystem, prm, arr, walls)
+    rows = np.asarray(G.hcs_rows(s, prm, arr["pmass"]))
+    gold = np.asarray(d["rows"])
+    assert rows.shape == gold.shape == (101, 4)
+    for i in range(HCS_EXACT_ROWS):
+        for c in range(4):
+            assert _sig5(rows[i, c], gold[i, c]), (i, c, rows[i, c], gold[i, c])
+    for i in range(rows.shape[0]):
+        assert _sig5(rows[i, 0], gold[i, 0]) and _sig5(rows[i, 3], gold[i, 3]), i
+    assert _sig5(rows[:, 2].max(), gold[:, 2].max())
+    tail = slice(HCS_EXACT_ROWS, None)
+    assert abs(rows[tail, 1].mean() / gold[tail, 1].mean() - 1.0) <= 0.01
+
+
+@pytest.mark.parametrize("run_idx,interp", [(0, "NONE"), (1, "GARG_2012")])
+def test_dem06_terminal_velocity_matches_mfix_table(run_idx, interp):
+    """DEM06's one-way coupled runs (DES_INTERP_ON = .F., i.e. the
+    unfiltered NONE scheme, and GARG_2012): a 0.1 mm sphere falling against
+    a 0.4 m/s upflow with the case's user drag (Schiller-Naumann,
+    DEM_DRAG_SINGLE_SPHERE), DRAG_GS_DES1/DRAG_GS_DES0 with the buoyancy
+    term P_FORCE*PVOL, DEM sub-steps inside 1 ms fluid steps.  Positions
+    and velocities match MFiX's table within 1e-6 absolute, the tolerance
+    of the reference's own runtest (numdiff -a 1e-6).  The gas here is the
+    exact uniform hydrostatic state; MFiX solves it, and its two runs
+    differ from each other by up to 2.2e-7 in velocity, the size of the
+    remaining difference (4.4e-7 in v, 1.4e-7 in y)."""
+    d = _load("dem06.json")
+    run = d["runs"][run_idx]
+    assert run["oneway"] and run["scheme"] == interp
+    case, prm, arr, walls, grid, f = G.dem06_case(interp)
+    s = make_system(OracleSystem, prm, arr, walls)
+    s.set_gas_fields(grid, f["ep_g"], f["u_g"], f["v_g"], f["w_g"], f["p_force"])
+    rows = G.dem06_rows(s, prm)
+    assert len(rows) == len(run["rows"]) == 36
+    for (t, y, v), (tg, yg, vg) in zip(rows, run["rows"]):
+        assert abs(t - tg) <= PRINT_8
+        assert abs(y - yg) <= 1e-6, (t, y, yg)
+        assert abs(v - vg) <= 1e-6, (t, v, vg)
