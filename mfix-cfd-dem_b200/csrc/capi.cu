@@ -318,9 +318,11 @@ void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
   // the search diameter) is applied to the candidates afterwards.  An axis
   // keeps the DES grid's division when that is not coarser.  The grid is an
   // acceleration structure, so it may be coarser than that and stay exact:
-  // its cell count is held to max(DES cells, 8 n + 65536) and to
-  // MAX_GRID_CELLS (a few small spheres in a large box would otherwise ask
-  // for billions of cells), scaling every refined axis down together.
+  // its cell count is held to max(DES cells, SEARCH_CELLS_CAP) (small
+  // spheres in a large box would otherwise ask for billions of cells),
+  // scaling every refined axis down together.  The bound depends on the
+  // system's grid alone, so batch limits sized from the parameters
+  // (dem_params_cells) fit the system when it is added.
   const int dgn[3] = {q.dg_imax, q.dg_jmax, q.no_k ? 1 : q.dg_kmax};
   const double target = q.factor_rlm * q.max_radius * 1.01;
   double len[3], want[3];
@@ -329,7 +331,7 @@ void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
     want[a] = (a == 2 && q.no_k) ? (double)dgn[a] : std::max((double)dgn[a], std::floor(len[a] / target));
   }
   const long long ndes = (long long)(dgn[0] + 2) * (dgn[1] + 2) * (q.no_k ? 1 : dgn[2] + 2);
-  const long long cap = std::min<long long>(MAX_GRID_CELLS, std::max<long long>(ndes, 8LL * n + 65536));
+  const long long cap = std::min<long long>(MAX_GRID_CELLS, std::max<long long>(ndes, SEARCH_CELLS_CAP));
   for (int it = 0; it < 64; ++it) {
     const double cells = (want[0] + 2) * (want[1] + 2) * (q.no_k ? 1.0 : want[2] + 2);
     if (cells <= (double)cap) break;

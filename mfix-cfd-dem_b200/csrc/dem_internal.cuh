@@ -412,6 +412,8 @@ __device__ __forceinline__ void unpack_ijk(int c, int& i, int& j, int& k) {
 // Cells of the DES grid, and of the search grid of the pair build, at most
 // (with their ghost layers): every cell index and count fits an int.
 constexpr long long MAX_GRID_CELLS = 1LL << 28;
+// Cells of the search grid of one system when it is finer than its DES grid.
+constexpr long long SEARCH_CELLS_CAP = 1LL << 22;
 
 // Neighbours per particle kept by the count pass of the pair build.
 constexpr int NSLOT = 16;

@@ -142,3 +142,57 @@ def make_coupled(cls, case_tuple, **kw):
     s = make_system(cls, prm, arr, walls, **kw)
     s.set_gas_fields(grid, fields["ep_g"], fields["u_g"], fields["v_g"], fields["w_g"])
     return s
+
+
+def hopper_wall_case(n=1500, d=2e-3, rho=2500.0, friction=0.4, outlet_d=8, seed=44, precision=abi.DEM_PREC_FP64):
+    """Spheres against the cone of a hopper-discharge case (the 20 x 60 x 20 cm
+    box with a 30 degree conical bottom, mfix_dem.configs.hopper_case): each
+    sits off a random interior point of a random cone facet, at a gap from
+    the facet's plane drawn from [-0.01, 0.05] mm (some overlap it at the
+    start), moving toward it at up to 0.5 m/s with a random tangential
+    velocity up to 0.5 m/s, so wall contacts with tangential history and
+    Coulomb slip start within a few steps, on the slanted facets binned by
+    TRI_BOX_OVERLAP.  Spheres closer than a diameter to an earlier one are
+    dropped."""
+    from mfix_dem import configs
+    box = configs.HOPPER_BOX
+    (vertex, norm), geo = P.hopper_walls((0.0, 0.0, 0.0), box, half_angle_deg=30.0, outlet_diam=outlet_d * d)
+    rng = np.random.default_rng(seed)
+    axis = np.array([0.5 * box[0], 0.0, 0.5 * box[2]])
+    r = 0.5 * d
+    cone = np.array([f for f in range(vertex.shape[0]) if 0.1 < abs(norm[f, 1]) < 0.99])
+    pos, vel = [], []
+    for _ in range(20 * n):
+        if len(pos) >= n:
+            break
+        f = cone[rng.integers(cone.shape[0])]
+        a, b, c = vertex[f].T                 # vertex[f][c][v]: a column per vertex
+        u, v = rng.uniform(0.1, 0.8, 2)
+        if u + v > 0.9:
+            u, v = 0.9 - v, 0.9 - u
+        q = a + u * (b - a) + v * (c - a)
+        nrm = np.cross(b - a, c - a)
+        nrm /= np.linalg.norm(nrm)
+        to_axis = axis - q
+        to_axis[1] = 0.0
+        if nrm @ to_axis < 0:                 # orient toward the inside of the cone
+            nrm = -nrm
+        x = q + nrm * (r + rng.uniform(-1e-5, 5e-5))
+        if x[1] < geo["y_out"] + 2 * d or x[1] > geo["y_top"] - 2 * d:
+            continue
+        if pos and np.min(np.linalg.norm(np.asarray(pos) - x, axis=1)) < d * 1.001:
+            continue
+        tang = rng.uniform(-0.5, 0.5, 3)
+        tang -= (tang @ nrm) * nrm
+        pos.append(x)
+        vel.append(-nrm * rng.uniform(0.0, 0.5) + tang)
+    pos, vel = np.asarray(pos), np.asarray(vel)
+    n = pos.shape[0]
+    case = P.DemCase(d_p0=(d,), ro_s0=(rho,), coll_model="HERTZ", intg_method="EULER",
+                     des_en_input=0.85, des_en_wall_input=[0.85], des_et_input=0.85, des_et_wall_input=[0.85],
+                     e_young=(1e7,), v_poisson=(0.3,), ew_young=1e7, vw_poisson=0.3,
+                     mew=friction, mew_w=friction, grav=(0.0, -9.81, 0.0), domain_hi=box,
+                     fluid_cells=(1, 1, 1), remove_rogue=True, force_precision=precision, neighbor_search_n=25)
+    arr = state_arrays(pos.T.copy(), vel.T.copy(), np.zeros((3, n)), np.full(n, r), np.full(n, rho))
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    return case, prm, arr, (vertex, norm)
