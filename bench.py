@@ -410,7 +410,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     return out
 
 
-def _batched_run(args, prec, stream, systems, info):
+def _batched_run(args, prec, stream, systems, info, barrier):
     """The batched workload: every system of `systems` in one batch handle.
     Warm-up up to the first period boundary (NN = 26), autotune, then K steps
     (a multiple of NEIGHBOR_SEARCH_N, replayed as captured periods) timed with
@@ -444,6 +444,8 @@ def _batched_run(args, prec, stream, systems, info):
     l0 = bt.launch_count()
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
+    barrier()
+    torch.cuda.synchronize()
     clocks.begin()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -485,16 +487,29 @@ def _batched_run(args, prec, stream, systems, info):
             "final_pos": final}
 
 
-def run_batched(args, stream):
+def run_batched(args, stream, barrier, ws, rank):
     """Split-precision and FP64 runs of the same batch; the split run's
     trajectory error is max over systems of max|x_split - x_fp64| / max|x_fp64|
-    after the same steps."""
+    after the same steps.  With N ranks the systems are spread by a greedy
+    size balance (mfix_dem.partition), one batch handle per GPU; the job's
+    time is the slowest rank's and its particle-steps the sum over ranks."""
     from mfix_dem import abi, configs
+    from mfix_dem.partition import gather_metrics, partition_work
     out = {}
     for prec in ("split", "fp64"):
         systems, info = configs.batched(n_sys=args.batch_systems, total=args.batch_total,
                                         precision=abi.DEM_PREC_SPLIT if prec == "split" else abi.DEM_PREC_FP64)
-        out[prec] = _batched_run(args, prec, stream, systems, info)
+        part = partition_work([s[2]["pos"].shape[1] for s in systems], ws)
+        mine = [systems[i] for i in part[rank]]
+        r = _batched_run(args, prec, stream, mine, info, barrier)
+        m = gather_metrics({"ms": r["ms_per_step"] * r["steps"], "ps": r["value"] * r["ms_per_step"] * r["steps"] / 1e3},
+                           ws, "cuda")
+        r["rank_particle_steps_per_s"] = r["value"]
+        r["ms_per_step"] = max(m["ms"]) / r["steps"]
+        r["value"] = sum(m["ps"]) / (max(m["ms"]) / 1e3)
+        r["partition"] = {"ranks": ws, "systems_per_rank": [len(p) for p in part],
+                          "particles_per_rank": [sum(systems[i][2]["pos"].shape[1] for i in p) for p in part]}
+        out[prec] = r
         out["info"] = info
     err = 0.0
     for sid, xs in out["split"]["final_pos"].items():
@@ -502,15 +517,19 @@ def run_batched(args, stream):
         err = max(err, float(np.max(np.abs(xs - xd)) / max(np.max(np.abs(xd)), 1e-300)))
     for prec in ("split", "fp64"):
         out[prec].pop("final_pos")
-    out["trajectory_rel_err"] = err
+    out["trajectory_rel_err"] = max(gather_metrics({"e": err}, ws, "cuda")["e"])
     return out
 
 
-def run_served(args):
+def run_served(args, barrier, ws, rank):
     """Poisson streams of hopper-discharge cases served with continuous
     batching (mfix_dem.serve.DemServer); per rate: p50/p99 latency from
-    arrival to completion and the aggregate particle-steps/s."""
+    arrival to completion and the aggregate particle-steps/s.  With N ranks
+    each request goes, in arrival order, to the rank with the least
+    particle-steps assigned so far (mfix_dem.partition); each rank serves its
+    share on its own GPU and the latencies are gathered."""
     from mfix_dem import configs, load_library
+    from mfix_dem.partition import gather_list, gather_metrics, partition_requests
     from mfix_dem.serve import DemServer
 
     def build(req):
@@ -520,15 +539,23 @@ def run_served(args):
     out = []
     template = build({"n": 5000, "friction": 0.4, "outlet_d": 8, "seed": 1})
     for k, rate in enumerate(rates):
-        reqs = configs.hopper_requests(args.serve_requests, rate, seed=configs.SEED_BASE + 4 + 100 * k,
-                                       steps=args.serve_steps)
+        reqs_all = configs.hopper_requests(args.serve_requests, rate, seed=configs.SEED_BASE + 4 + 100 * k,
+                                           steps=args.serve_steps)
+        reqs = partition_requests(reqs_all, ws)[rank]
         srv = DemServer(load_library(), build, template, hbm_budget_bytes=int(args.serve_budget_gb * 1e9),
                         max_systems=64, graphs=bool(args.serve_graphs))
+        barrier()
         res = srv.run(reqs)
         srv.close()
-        out.append({"rate_per_s": rate, "requests": len(reqs), "p50_s": res["p50_s"], "p99_s": res["p99_s"],
-                    "mean_s": res["mean_s"], "particle_steps_per_s": res["particle_steps_per_s"],
-                    "span_s": res["span_s"], "gpu_busy_s": res["busy_s"], "chunks": res["chunks"]})
+        lat = gather_list([r.latency for r in res["results"]], ws, "cuda")
+        m = gather_metrics({"work": res["particle_steps"], "span": res["span_s"], "busy": res["busy_s"],
+                            "chunks": res["chunks"]}, ws, "cuda")
+        span = max(m["span"])
+        out.append({"rate_per_s": rate, "requests": len(reqs_all), "p50_s": float(np.percentile(lat, 50)),
+                    "p99_s": float(np.percentile(lat, 99)), "mean_s": float(np.mean(lat)),
+                    "particle_steps_per_s": sum(m["work"]) / span if span > 0 else 0.0,
+                    "span_s": span, "gpu_busy_s": max(m["busy"]), "chunks": int(sum(m["chunks"])),
+                    "ranks": ws})
     return out
 
 
@@ -560,11 +587,11 @@ def run_ours(args):
 
     batched = None
     if args.batch_systems > 0:
-        batched = run_batched(args, stream)
+        batched = run_batched(args, stream, barrier, ws, rank)
 
     served = None
     if args.serve_rates.strip():
-        served = run_served(args)
+        served = run_served(args, barrier, ws, rank)
 
     cpu = None
     if rank == 0 and not args.no_cpu:

@@ -619,9 +619,7 @@ typedef struct dem_tuning {
     int32_t gather_threads;      /* gather kernel: threads per block */
     int32_t neigh_threads;       /* pair-build scan: threads per block */
     double  pair_ms, gather_ms, neigh_ms;  /* measured time of the chosen shapes (autotune only) */
-    int32_t split_lanes;         /* split-precision pass: lanes per particle (1, 2, 4 or 8; 0 = keep) */
-    int32_t reserved_i;
-    double  reserved[3];
+    double  reserved[4];
 } dem_tuning;
 
 /* Times the candidate launch shapes of the hot kernels on the handle's

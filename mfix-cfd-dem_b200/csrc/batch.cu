@@ -496,10 +496,7 @@ static int batch_replay_period(dem_handle* h, int N) {
   }
   if (int rc = check_cuda(h, cudaGraphLaunch(h->graphs[key], h->stream), "graph launch")) return rc;
   h->launches += h->graph_kernels[key];
-  for (int j = 0; j < N; ++j) {
-    h->cur = 1 - h->cur;
-    if (h->dp.prec == DEM_PREC_SPLIT) h->pcur = 1 - h->pcur;  // each split pass writes the other history buffer
-  }
+  for (int j = 0; j < N; ++j) h->cur = 1 - h->cur;
   h->pcur = 1 - h->pcur;
   h->rb = 1 - h->rb;
   h->np_stale = true;

@@ -310,6 +310,13 @@ void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
     p.etanw[k] = q.des_etan_wall[k]; p.etatw[k] = q.des_etat_wall[k];
     p.hkwn[k] = q.hert_kwn[k]; p.hkwt[k] = q.hert_kwt[k];
   }
+  for (int k = 0; k < MAXP * MAXP; ++k) {
+    p.hkn32[k] = (float)p.hkn[k]; p.hkt32[k] = (float)p.hkt[k];
+    p.etan_sq32[k] = (float)(p.etan[k] * std::sqrt(std::max(p.hkn[k], 0.0)));
+    p.etat_sq32[k] = (float)(p.etat[k] * std::sqrt(std::max(p.hkt[k], 0.0)));
+    p.etan32[k] = (float)p.etan[k]; p.etat32[k] = (float)p.etat[k];
+  }
+  p.kn32 = (float)p.kn; p.kt32 = (float)p.kt; p.mew32 = (float)p.mew;
   // Search grid for the pair build: cells about half the largest search
   // diameter 2*FACTOR_RLM*MAX_RADIUS wide (1 % margin); each particle scans
   // the cells within its own reach FACTOR_RLM*(r + MAX_RADIUS), so a small
@@ -519,7 +526,7 @@ int dem_destroy(dem_handle* h) {
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
-                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflagb[0], h->pflagb[1], h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->d_ibc, h->pic_fresh, h->d_seed, h->skin, h->vslot, h->pgap,
+                  h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflagb[0], h->pflagb[1], h->in_pos, h->in_flag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->d_ibc, h->pic_fresh, h->d_seed, h->skin, h->vslot, h->pgap,
                   h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -828,10 +835,8 @@ static int replay_period(dem_handle* h, int nn0) {
   h->launches += h->graph_kernels[key];
   // buffer parities and bookkeeping after the period: N force passes flip
   // the state buffers, the rebuild flips the list and history buffers
-  const bool split = h->dp.prec == DEM_PREC_SPLIT;
   for (int j = 0; j < nsn; ++j) {
     h->cur = 1 - h->cur;
-    if (split) h->pcur = 1 - h->pcur;  // each split pass writes the other history buffer
     h->s_time = h->s_time + h->prm.dtsolid;
     h->steps_done++;
   }

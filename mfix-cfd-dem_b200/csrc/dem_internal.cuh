@@ -74,6 +74,12 @@ struct DevParams {
   double lo[3], hi[3], L[3];
   double etan[MAXP * MAXP], etat[MAXP * MAXP], hkn[MAXP * MAXP], hkt[MAXP * MAXP];
   double etanw[MAXP], etatw[MAXP], hkwn[MAXP], hkwt[MAXP];
+  // FP32 copies for the split-precision pair force: HERT_KN, HERT_KT,
+  // DES_ETAN*sqrt(HERT_KN), DES_ETAT*sqrt(HERT_KT) (Hertz), DES_ETAN,
+  // DES_ETAT, KN, KT (linear spring-dashpot), MEW
+  float hkn32[MAXP * MAXP], hkt32[MAXP * MAXP], etan_sq32[MAXP * MAXP], etat_sq32[MAXP * MAXP];
+  float etan32[MAXP * MAXP], etat32[MAXP * MAXP];
+  float kn32, kt32, mew32;
   // search grid of the pair build: fn[a] interior cells of width 1/f_inv[a]
   // over the DES-grid interior, plus one ghost layer on each side
   int fn[3], fc1, fc2, nfcell;
@@ -214,7 +220,6 @@ struct dem_handle {
     int pair_threads = 256, pair_bpsm = 8;  // pair kernel: threads per block, resident blocks per SM
     int gather_threads = 256;               // gather kernel: threads per block
     int neigh_threads = 128;                // pair-build scan: threads per block
-    int split_lanes = 4;                    // split-precision pass: lanes per particle
   } tune;
   bool capturing = false;     // inside a CUDA graph capture: no host syncs
   cudaStream_t own_stream = nullptr;
@@ -230,6 +235,8 @@ struct dem_handle {
   int* in_start = nullptr;    // n+1
   int* in_fill = nullptr;     // n
   int2* in_pair = nullptr;    // cap
+  int* in_pos = nullptr;      // cap: slot of each pair in its neighbour's incoming list (inverse of in_pair)
+  uint8_t* in_flag = nullptr; // cap: PF_CONTACT of the pair at each incoming slot (split-precision records)
   int* pair_owner = nullptr;  // cap
   // cap: PF_* bits of each pair, one array per history buffer: pflagb[pcur]
   // goes with pft[pcur] (the other is stencil-rank scratch during a build
@@ -329,7 +336,8 @@ int run_force(dem_handle* h, bool fused);
 int run_cfnewvalues(dem_handle* h);
 int run_bin_facets(dem_handle* h, const double* vertex_fortran, const double* norm_fortran, int nf);
 int run_split_force_error(dem_handle* h, double* rel_err);
-void launch_force_split(dem_handle* h, int mode);  // force_split.cu: fused split-precision pass
+void launch_pairs_split(dem_handle* h);         // force_split.cu
+void launch_gather_split(dem_handle* h, int mode);
 int ensure_pair_capacity(dem_handle* h, long long need);
 int build_transpose(dem_handle* h, int nb);    // neighbor.cu
 void launch_neigh_count(dem_handle* h);        // neighbor.cu: count pass of the pair build

@@ -893,42 +893,36 @@ static void launch_gather_fp64(dem_handle* h, int mode) {
   else launch_gather_t<2, B>(h);
 }
 
-// The two timed parts of the force step for the autotuner.  The split path
-// has no separate pair kernel: its fused pass is the "gather" part.
+// The two timed parts of the force step for the autotuner.
 void launch_pairs_only(dem_handle* h) {
-  if (h->dp.prec == DEM_PREC_SPLIT) return;
-  if (h->batch()) launch_pairs_fp64<true>(h);
+  if (h->dp.prec == DEM_PREC_SPLIT) launch_pairs_split(h);
+  else if (h->batch()) launch_pairs_fp64<true>(h);
   else launch_pairs_fp64<false>(h);
 }
 
 void launch_gather_only(dem_handle* h) {
-  if (h->dp.prec == DEM_PREC_SPLIT) launch_force_split(h, 0);
+  if (h->dp.prec == DEM_PREC_SPLIT) launch_gather_split(h, 0);
   else if (h->batch()) launch_gather_fp64<true>(h, 0);
   else launch_gather_fp64<false>(h, 0);
 }
 
 // Contact forces of the current state.  mode: 0 = into FC/TOW, 1/2 = fused
 // Euler/AB2 integration into the other state buffer.  The collision model,
-// integrator and force precision are common to all systems of a batch.  The
-// split pass reads history buffer pcur and writes the other one (run_force
-// flips pcur after it).
+// integrator and force precision are common to all systems of a batch.
 static void launch_force_kernels(dem_handle* h, int mode, bool split) {
   {
     ProfScope ps(h, DEM_PROF_WALLS);
     launch_walls(h);
   }
-  if (split) {
-    ProfScope ps(h, DEM_PROF_GATHER);
-    launch_force_split(h, mode);
-    return;
-  }
   {
     ProfScope ps(h, DEM_PROF_PAIRS);
-    if (h->batch()) launch_pairs_fp64<true>(h);
+    if (split) launch_pairs_split(h);
+    else if (h->batch()) launch_pairs_fp64<true>(h);
     else launch_pairs_fp64<false>(h);
   }
   ProfScope ps(h, DEM_PROF_GATHER);
-  if (h->batch()) launch_gather_fp64<true>(h, mode);
+  if (split) launch_gather_split(h, mode);
+  else if (h->batch()) launch_gather_fp64<true>(h, mode);
   else launch_gather_fp64<false>(h, mode);
 }
 
@@ -956,11 +950,9 @@ int run_force(dem_handle* h, bool fused) {
   ProfScope ps(h, DEM_PROF_FORCE);
   h->dp.first_pass = h->first_pass ? 1 : 0;
   const int mode = !fused ? 0 : (h->dp.intg == DEM_INTG_AB2 ? 2 : 1);
-  const bool split = h->dp.prec == DEM_PREC_SPLIT;
-  launch_force_kernels(h, mode, split);
+  launch_force_kernels(h, mode, h->dp.prec == DEM_PREC_SPLIT);
   if (fused) launch_skin(h);
   if (int rc = check_cuda(h, cudaGetLastError(), "force kernels")) return rc;
-  if (split) h->pcur = 1 - h->pcur;  // the pass wrote the other history buffer
   if (fused) { h->cur = 1 - h->cur; h->first_pass = false; }
   return 0;
 }
@@ -976,11 +968,12 @@ int run_split_force_error(dem_handle* h, double* rel_err) {
   const size_t b_hist = sizeof(double) * 3 * P;
   // both passes start from the same wall and pair histories (each pass
   // updates them in place)
-  char* snap = (char*)stage_buffer(h, b_fid + b_pft + n + b_hist + P + 64);
+  char* snap = (char*)stage_buffer(h, b_fid + b_pft + n + b_hist + 2 * P + 64);
   if (!snap) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
   char* s_live = snap + b_fid + b_pft;
   char* s_hist = s_live + n;
   char* s_flag = s_hist + b_hist;
+  char* s_inflag = s_flag + P;
   auto save = [&]() {
     cudaMemcpyAsync(snap, h->wall_fid, b_fid, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(snap + b_fid, h->wall_pft, b_pft, cudaMemcpyDeviceToDevice, h->stream);
@@ -988,6 +981,7 @@ int run_split_force_error(dem_handle* h, double* rel_err) {
     if (P) {
       cudaMemcpyAsync(s_hist, h->pft[h->pcur], b_hist, cudaMemcpyDeviceToDevice, h->stream);
       cudaMemcpyAsync(s_flag, h->pflag(), P, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(s_inflag, h->in_flag, P, cudaMemcpyDeviceToDevice, h->stream);
     }
   };
   auto restore = [&]() {
@@ -997,6 +991,7 @@ int run_split_force_error(dem_handle* h, double* rel_err) {
     if (P) {
       cudaMemcpyAsync(h->pft[h->pcur], s_hist, b_hist, cudaMemcpyDeviceToDevice, h->stream);
       cudaMemcpyAsync(h->pflag(), s_flag, P, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(h->in_flag, s_inflag, P, cudaMemcpyDeviceToDevice, h->stream);
     }
   };
   std::vector<double> f64(3 * n), f32(3 * n);

@@ -1,5 +1,5 @@
 // force_split.cu -- split-precision contact forces (FP32 forces, FP64
-// history and integration), one fused pass per step.
+// history and integration).
 //
 // Same contact law as the FP64 path (calc_force_dem.f:204-506 with
 // CFRELVEL, cfrelvel.f:54-77) with this split of the arithmetic:
@@ -14,19 +14,19 @@
 //         rolling friction; per-particle sums use compensated (Neumaier)
 //         FP32 accumulation.
 //
-// Structure: a group of lanes per particle walks every pair the particle is
-// in -- the incoming entries of the transpose (pairs owned by other
-// particles) and its own row -- and evaluates each contact itself, with the
-// owner as L and the neighbour as I, through a single code path, so both
-// particles of a pair compute bit-identical pair forces (equal and
-// opposite).  No
-// per-pair record goes through memory.  The history is double-buffered:
-// both particles read PFT and the flags from buffer pcur, only the owner
-// writes buffer 1 - pcur (flags of every row entry, PFT of pairs whose new
-// history is nonzero), and the caller flips pcur after the pass.  The sum
-// order differs from the serial reference (split results are compared with
-// the FP64 path by the stated force tolerance, not bit for bit).  Wall terms
-// come from the FP64 wall kernel (force.cu).
+// Structure: the pair kernel evaluates every contact once (a thread per
+// pair, consecutive pairs of the half list) and writes each particle's terms
+// as a 32-byte FP32 record: the owner's at the pair index (rec_own, in row
+// order) and the neighbour's at the pair's slot of the neighbour's incoming
+// list (rec_in[in_pos[cc]], the transpose order).  The neighbour-side writes
+// are scattered but never waited on; the per-particle kernel then reads its
+// own row and its incoming list as two contiguous ranges, with no random
+// load.  Contact flags: PF_CONTACT of pflag for the owner's records (row
+// order), and in_flag (transpose order) for the neighbour's, written only
+// when a pair's contact state changes.  Wall terms come from the FP64 wall
+// kernel (force.cu).  The sum order differs from the serial reference;
+// split results are compared with the FP64 path by the stated force
+// tolerance, not bit for bit.
 //
 // This file is compiled with FMA contraction and fast single-precision
 // square roots and divisions.
@@ -61,9 +61,10 @@ __device__ __forceinline__ void split_contact(const DevParams& p, const double4&
                                               const double4& wi, int phi, const double dist[3], double d2,
                                               double ovd, const double pin[3], double ot[3], PairTerms& o) {
   const float rl = (float)xl.w, ri = (float)xi.w;
-  const float dmag = sqrtf((float)d2);
+  const float d2f = (float)d2;
+  const float inv = rsqrtf(d2f);
+  const float dmag = d2f * inv;
   const float ov = (float)ovd / ((rl + ri) + dmag);
-  const float inv = 1.f / dmag;
   const float nrm[3] = {(float)dist[0] * inv, (float)dist[1] * inv, (float)dist[2] * inv};
   float vrel[3] = {(float)(vl.x - vi.x), (float)(vl.y - vi.y), (float)(vl.z - vi.z)};
   const float dcl = 0.5f * dmag + (rl - ri) * (rl + ri) * (0.5f * inv);
@@ -81,19 +82,20 @@ __device__ __forceinline__ void split_contact(const DevParams& p, const double4&
   const float m_eff = (ml * mi) / (ml + mi);
   float kn, kt, etan, etat;
   if (COLL == DEM_COLL_HERTZ) {
-    float so = sqrtf(ov);
-    const float sre = sqrtf(rad_eff);
-    const float hkn = (float)p.hkn[ix], hkt = (float)p.hkt[ix];
-    kn = hkn * so * sre;
-    kt = hkt * so * sre;
-    so = sqrtf(so);
-    etan = (float)p.etan[ix] * so * sqrtf(hkn * sre * m_eff);
-    etat = (float)p.etat[ix] * so * sqrtf(hkt * sre * m_eff);
+    // KN = HERT_KN*sqrt(ov)*sqrt(R_eff) = HERT_KN*q with q = sqrt(ov*R_eff);
+    // ETA_N = DES_ETAN*ov^(1/4)*sqrt(HERT_KN*sqrt(R_eff)*M_eff)
+    //       = DES_ETAN*sqrt(HERT_KN)*sqrt(q*M_eff), and the same for t
+    const float q = sqrtf(ov * rad_eff);
+    const float sqm = sqrtf(q * m_eff);
+    kn = p.hkn32[ix] * q;
+    kt = p.hkt32[ix] * q;
+    etan = p.etan_sq32[ix] * sqm;
+    etat = p.etat_sq32[ix] * sqm;
   } else {
-    kn = (float)p.kn; kt = (float)p.kt;
+    kn = p.kn32; kt = p.kt32;
     const float sm = sqrtf(m_eff);
-    etan = (float)p.etan[ix] * sm;
-    etat = (float)p.etat[ix] * sm;
+    etan = p.etan32[ix] * sm;
+    etat = p.etat32[ix] * sm;
   }
   float fn[3];
 #pragma unroll
@@ -102,16 +104,18 @@ __device__ __forceinline__ void split_contact(const DevParams& p, const double4&
 #pragma unroll
   for (int c = 0; c < 3; ++c) ot[c] = p.dt * (double)vt[c] + pin[c];
   const float o32[3] = {(float)ot[0], (float)ot[1], (float)ot[2]};
-  const float mag = sqrtf(o32[0] * o32[0] + o32[1] * o32[1] + o32[2] * o32[2]);
+  const float mag2 = o32[0] * o32[0] + o32[1] * o32[1] + o32[2] * o32[2];
   float ft[3] = {0.f, 0.f, 0.f};
-  if (mag > 0.f) {
+  if (mag2 > 0.f) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) ft[c] = -kt * o32[c] - etat * vt[c];
-    const float ftmd = sqrtf(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
-    const float fnmd = (float)p.mew * sqrtf(fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2]);
-    if (ftmd > fnmd) {
-      // Coulomb slip: Ft = -|Fn|*mu t, history (|Fn|*mu/Kt) t with t = ot/|ot|
-      const float im = 1.f / mag;
+    const float ft2 = ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2];
+    const float fn2 = fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2];
+    // |Ft| > MEW*|Fn|, compared squared
+    if (ft2 > p.mew32 * p.mew32 * fn2) {
+      // Coulomb slip: Ft = -MEW*|Fn| t, history (MEW*|Fn|/KT) t, t = ot/|ot|
+      const float fnmd = p.mew32 * sqrtf(fn2);
+      const float im = rsqrtf(mag2);
 #pragma unroll
       for (int c = 0; c < 3; ++c) ft[c] = -fnmd * (o32[c] * im);
       const double sc = (double)(fnmd / kt * im);
@@ -130,169 +134,107 @@ __device__ __forceinline__ void split_contact(const DevParams& p, const double4&
   o.ov = ov;
 }
 
-// G lanes per particle (G = 1, 2, 4 or 8, consecutive lanes of a warp): lane
-// j of the group takes entries j, j + G, ... of the particle's list -- k < nin:
-// incoming entry in_pair[is + k] = (owner, pair); otherwise the particle's
-// own row -- so the group has G entries' loads in flight at a time.  Each
-// lane keeps compensated FP32 sums of its entries; the group adds the lanes'
-// sums in FP64 in a fixed shuffle order, so results do not depend on timing.
-// Lane 0 adds the wall terms (k_walls) and integrates (MODE 1 Euler, 2
-// Adams-Bashforth) or stores the forces into FC/TOW (MODE 0).  Pairs that the
-// build's gap and the displacement bound since prove apart (with no history)
-// are skipped after reading their flag and gap, by both particles alike.
-// The owner of a pair writes its output flag and keeps its output history
-// slot exact: the new history where it is nonzero, zeros where the slot held
-// history (its old output flag says so) and no longer does.
-template <int COLL, int MODE, bool B, int G>
-__global__ void __launch_bounds__(256)
-k_force_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
-              const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
-              double4* __restrict__ omg_n, const int8_t* __restrict__ state, const uint8_t* __restrict__ phase,
-              const double* __restrict__ wf, uint8_t* __restrict__ wall_hit, const int* __restrict__ row_end,
-              const int* __restrict__ nbrs, const int* __restrict__ in_start, const int2* __restrict__ in_pair,
-              const double* __restrict__ pft_in, double* __restrict__ pft_out, const uint8_t* __restrict__ flag_in,
-              uint8_t* __restrict__ flag_out, const float* __restrict__ pgap, const double* __restrict__ skin,
-              double* __restrict__ fc, double* __restrict__ tow, double* __restrict__ acc_old,
-              double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot, DevErr* __restrict__ err,
-              CellOut cells) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int me = (int)(t / G);
-  const int lane = (int)(t % G);
+// One particle's terms of a contact: (force, KN*OVERLAP) and (torque, 0).
+struct Rec32 {
+  float4 a, b;
+};
+
+// Kernel 1 (per pair): one CC iteration of CALC_FORCE_DEM, evaluated once.
+// A pair that the build's gap and the displacement bound since prove apart
+// (history zero) is skipped after reading its flag and gap.  Four
+// consecutive pairs per thread-iteration: their flags and gaps arrive in one
+// load each.
+template <int COLL, bool B>
+__global__ void __launch_bounds__(256, 4)
+k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap, const int* __restrict__ owner,
+              const int* __restrict__ nbrs, const int* __restrict__ in_pos, const double4* __restrict__ pos4,
+              const double4* __restrict__ vel4, const double4* __restrict__ omg4, const int8_t* __restrict__ state,
+              const uint8_t* __restrict__ phase, double* __restrict__ pft, uint8_t* __restrict__ pflag,
+              uint8_t* __restrict__ in_flag, const float* __restrict__ pgap, const double* __restrict__ skin,
+              Rec32* __restrict__ rec_own, Rec32* __restrict__ rec_in, DevErr* __restrict__ err) {
+  const long long np = min((long long)*d_np, cap);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  // the bound in FP32, rounded up: a pair is skipped only when its gap
+  // (rounded down at the build) exceeds it
+  const float reach = __double2float_ru(2.0 * skin[0]);
   unsigned long long ncont = 0;
   unsigned eflags = 0;
-  if (me < p0.n) {
-    const DevParams& p = sysp<B>(p0, bv, me);
-    const int8_t st = state[me];
-    const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
-    const int ph = phase[me];
-    Comp3 F, T;
-    F.zero(); T.zero();
-    const float w32[3] = {(float)W.x, (float)W.y, (float)W.z};
-    const float om = sqrtf(w32[0] * w32[0] + w32[1] * w32[1] + w32[2] * w32[2]);
-    const bool roll = p.mew_r > 0.0 && om > 0.f;
-    const float rf = (float)p.mew_r * (2.f * (float)X.w) / (om > 0.f ? om : 1.f);
-    const double reach = 2.0 * skin[0];
-    const int rs = me ? row_end[me - 1] : 0, re = row_end[me];
-    // a NONEXISTENT particle adds no force, but it still carries its own
-    // row's history and flags into the output buffers
-    const int is = st != DEM_STATE_NONEXISTENT ? in_start[me] : 0;
-    const int nin = st != DEM_STATE_NONEXISTENT ? in_start[me + 1] - is : 0;
-    const int ntot = nin + (re - rs);
-    for (int k = lane; k < ntot; k += G) {
-      int other, cc;
-      bool own;
-      if (k < nin) {
-        const int2 e = in_pair[is + k];
-        other = e.x; cc = e.y; own = false;
+  const long long ng = (np + 3) / 4;
+  for (long long g4 = (long long)blockIdx.x * blockDim.x + threadIdx.x; g4 < ng; g4 += stride) {
+    const long long c0 = 4 * g4;
+    uint32_t fw = 0;
+    float4 gq = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c0 + 3 < np) {
+      fw = *reinterpret_cast<const uint32_t*>(pflag + c0);
+      gq = *reinterpret_cast<const float4*>(pgap + c0);
+    } else {
+      if (c0 < np) { fw |= pflag[c0]; gq.x = pgap[c0]; }
+      if (c0 + 1 < np) { fw |= (uint32_t)pflag[c0 + 1] << 8; gq.y = pgap[c0 + 1]; }
+      if (c0 + 2 < np) { fw |= (uint32_t)pflag[c0 + 2] << 16; gq.z = pgap[c0 + 2]; }
+    }
+    const unsigned apart = ((!(fw & PF_HIST) && gq.x > reach) ? 1u : 0u) |
+                           ((!((fw >> 8) & PF_HIST) && gq.y > reach) ? 2u : 0u) |
+                           ((!((fw >> 16) & PF_HIST) && gq.z > reach) ? 4u : 0u) |
+                           ((!((fw >> 24) & PF_HIST) && gq.w > reach) ? 8u : 0u);
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+      const long long cc = c0 + j;
+      if (cc >= np) break;
+      const uint8_t f0 = (uint8_t)(fw >> (8 * j));
+      uint8_t f;
+      if ((apart >> j) & 1u) {
+        f = 0;
       } else {
-        cc = rs + (k - nin); other = nbrs[cc]; own = true;
-      }
-      const uint8_t f0b = flag_in[cc];
-      uint8_t fnew = 0;
-      bool carry = false;
-      double ot[3] = {0.0, 0.0, 0.0};
-      // provably apart, history zero (stays zero): nothing to add or carry
-      if ((f0b & PF_HIST) || !((double)pgap[cc] > reach)) {
-        const int8_t so = state[other];
-        fnew = f0b & PF_HIST;  // NONEXISTENT partner or zero distance: history kept
-        carry = true;
-        if (st != DEM_STATE_NONEXISTENT && so != DEM_STATE_NONEXISTENT) {
-          const double4 xo = pos_c[other];
-          // L is the owner, I the neighbour, for both particles of the pair
-          const double4& xl = own ? X : xo;
-          const double4& xi = own ? xo : X;
+        const int ll = owner[cc], i = nbrs[cc];
+        f = f0 & PF_HIST;  // NONEXISTENT partner or zero distance: history kept
+        double* po = pft + 3 * cc;
+        if (state[i] != DEM_STATE_NONEXISTENT && state[ll] != DEM_STATE_NONEXISTENT) {
+          const DevParams& p = sysp<B>(p0, bv, ll);
+          const double4 a = pos4[ll], b = pos4[i];
+          const double xl[3] = {a.x, a.y, a.z}, xi[3] = {b.x, b.y, b.z};
           double dist[3];
-          {
-            const double a[3] = {xl.x, xl.y, xl.z}, b[3] = {xi.x, xi.y, xi.z};
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              double pj = b[c];
-              const double sh = periodic_shift(p, c, pj - a[c]);
-              if (sh != 0.0) pj = pj + sh;
-              dist[c] = pj - a[c];
-            }
+          for (int c = 0; c < 3; ++c) {
+            double pj = xi[c];
+            const double s = periodic_shift(p, c, pj - xl[c]);
+            if (s != 0.0) pj = pj + s;
+            dist[c] = pj - xl[c];
           }
-          const double r_lm = xl.w + xi.w;
+          const double r_lm = a.w + b.w;
           const double d2 = dist[0] * dist[0] + dist[1] * dist[1] + dist[2] * dist[2];
           if (d2 > (r_lm - SMALL_NUMBER) * (r_lm - SMALL_NUMBER)) {
-            fnew = 0;  // apart: history reset
-            carry = false;
+            if (f0 & PF_HIST) { po[0] = 0.0; po[1] = 0.0; po[2] = 0.0; }
+            f = 0;
           } else if (d2 == 0.0) {
-            if (own) {
-              eflags |= EF_ZERO_DIST;
-              err->zero_a = me; err->zero_b = other;
-            }
+            eflags |= EF_ZERO_DIST;
+            err->zero_a = ll; err->zero_b = i;
           } else {
-            const double4 vo = vel_c[other], wo = omg_c[other];
-            const int pho = phase[other];
+            const double4 va = vel4[ll], vb = vel4[i], wa = omg4[ll], wb = omg4[i];
             double pin[3] = {0.0, 0.0, 0.0};
-            if (f0b & PF_HIST) {
-              const double* q = pft_in + 3 * (size_t)cc;
-              pin[0] = q[0]; pin[1] = q[1]; pin[2] = q[2];
-            }
+            if (f0 & PF_HIST) { pin[0] = po[0]; pin[1] = po[1]; pin[2] = po[2]; }
+            double ot[3];
             PairTerms o;
-            if (own) split_contact<COLL>(p, X, V, W, ph, xo, vo, wo, pho, dist, d2, r_lm * r_lm - d2, pin, ot, o);
-            else split_contact<COLL>(p, xo, vo, wo, pho, X, V, W, ph, dist, d2, r_lm * r_lm - d2, pin, ot, o);
-            const float sg = own ? 1.f : -1.f;
-            const float arm = own ? o.dcl2 : o.dci2;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) { F.add(c, sg * o.fc[c]); T.add(c, arm * o.tf[c]); }
-            if (roll) {
-              const float sr = -(rf * o.kn * o.ov);
-#pragma unroll
-              for (int c = 0; c < 3; ++c) T.add(c, sr * w32[c]);
-            }
-            fnew = PF_CONTACT | ((ot[0] != 0.0 || ot[1] != 0.0 || ot[2] != 0.0) ? PF_HIST : 0);
-            carry = false;
-            if (own) ++ncont;
+            split_contact<COLL>(p, a, va, wa, phase[ll], b, vb, wb, phase[i], dist, d2, r_lm * r_lm - d2, pin, ot,
+                                o);
+            po[0] = ot[0]; po[1] = ot[1]; po[2] = ot[2];
+            const float rol = o.kn * o.ov;
+            Rec32 ro, ri;
+            ro.a = make_float4(o.fc[0], o.fc[1], o.fc[2], rol);
+            ro.b = make_float4(o.dcl2 * o.tf[0], o.dcl2 * o.tf[1], o.dcl2 * o.tf[2], 0.f);
+            ri.a = make_float4(-o.fc[0], -o.fc[1], -o.fc[2], rol);
+            ri.b = make_float4(o.dci2 * o.tf[0], o.dci2 * o.tf[1], o.dci2 * o.tf[2], 0.f);
+            rec_own[cc] = ro;
+            rec_in[in_pos[cc]] = ri;
+            f = PF_CONTACT | ((ot[0] != 0.0 || ot[1] != 0.0 || ot[2] != 0.0) ? PF_HIST : 0);
+            ++ncont;
           }
         }
       }
-      if (own) {
-        const uint8_t fold = flag_out[cc];
-        flag_out[cc] = fnew;
-        double* q = pft_out + 3 * (size_t)cc;
-        if (fnew & PF_HIST) {
-          if (carry) {
-            const double* a = pft_in + 3 * (size_t)cc;
-            q[0] = a[0]; q[1] = a[1]; q[2] = a[2];
-          } else {
-            q[0] = ot[0]; q[1] = ot[1]; q[2] = ot[2];
-          }
-        } else if (fold & PF_HIST) {
-          q[0] = 0.0; q[1] = 0.0; q[2] = 0.0;
-        }
+      if (f != f0) {
+        pflag[cc] = f;
+        // the neighbour's view of the contact, in transpose order
+        if ((f ^ f0) & PF_CONTACT) in_flag[in_pos[cc]] = f & PF_CONTACT;
       }
-    }
-    // the group's sums in FP64, lanes added in a fixed order
-    double f[3], tq[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) { f[c] = F.value(c); tq[c] = T.value(c); }
-    if constexpr (G > 1) {
-      const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << ((threadIdx.x & 31) & ~(G - 1));
-#pragma unroll
-      for (int o = G / 2; o > 0; o >>= 1) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          f[c] += __shfl_down_sync(gmask, f[c], o, G);
-          tq[c] += __shfl_down_sync(gmask, tq[c], o, G);
-        }
-      }
-    }
-    if (lane == 0) {
-      double f0[3] = {0.0, 0.0, 0.0}, t0[3] = {0.0, 0.0, 0.0};
-      if (wall_hit[me]) {
-        wall_hit[me] = 0;
-        if (st == DEM_STATE_NORMAL) {
-          const double* o = wf + 6 * (size_t)me;
-          f0[0] = o[0]; f0[1] = o[1]; f0[2] = o[2]; t0[0] = o[3]; t0[1] = o[4]; t0[2] = o[5];
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) { f[c] = f0[c] + f[c]; tq[c] = t0[c] + tq[c]; }
-      const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
-      finish_particle<MODE>(p, me, st, x, v, w, X.w, V.w, W.w, f, tq, pos_n, vel_n, omg_n, fc, tow, acc_old,
-                            rot_acc_old, vslot, cells);
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -305,42 +247,132 @@ k_force_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, con
   }
 }
 
-template <int COLL, int MODE, bool B, int L>
-static void launch_force_split_t(dem_handle* h) {
-  const int T = h->tune.gather_threads;
-  const unsigned G = (unsigned)(((long long)h->n * L + T - 1) / T);
-  const int c = h->cur, pc = h->pcur;
-  k_force_split<COLL, MODE, B, L><<<G, T, 0, h->stream>>>(
-      h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
-      h->state, h->phase, h->wf, h->wall_hit, h->row_end[h->rb], h->nbrs[h->rb], h->in_start, h->in_pair,
-      h->pft[pc], h->pft[1 - pc], h->pflagb[pc], h->pflagb[1 - pc], h->pgap, h->skin, h->fc, h->tow, h->acc_old,
-      h->rot_acc_old, h->vslot, h->derr, gather_cells<MODE, B>(h));
-  DEM_LAUNCH(h);
-}
-
-template <int MODE, int L>
-static void launch_force_split_l(dem_handle* h) {
-  const bool hz = h->dp.coll == DEM_COLL_HERTZ;
-  if (h->batch()) hz ? launch_force_split_t<DEM_COLL_HERTZ, MODE, true, L>(h) : launch_force_split_t<DEM_COLL_LSD, MODE, true, L>(h);
-  else hz ? launch_force_split_t<DEM_COLL_HERTZ, MODE, false, L>(h) : launch_force_split_t<DEM_COLL_LSD, MODE, false, L>(h);
-}
-
-template <int MODE>
-static void launch_force_split_m(dem_handle* h) {
-  switch (h->tune.split_lanes) {
-    case 1: launch_force_split_l<MODE, 1>(h); break;
-    case 2: launch_force_split_l<MODE, 2>(h); break;
-    case 8: launch_force_split_l<MODE, 8>(h); break;
-    default: launch_force_split_l<MODE, 4>(h); break;
+// The records of one contiguous range [a, e) whose flag bytes say contact,
+// a window of up to 32 at a time: the window's flags first (independent
+// loads), then the flagged records, each issued before the previous one is
+// added.
+__device__ __forceinline__ void add_range(int a, int e, const uint8_t* __restrict__ flags,
+                                          const Rec32* __restrict__ rec, Comp3& F, Comp3& T, float& rs,
+                                          float& rc) {
+  for (int base = a; base < e; base += 32) {
+    const int cnt = min(32, e - base);
+    unsigned mask = 0u;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k)
+      if (k < cnt && (flags[base + k] & PF_CONTACT)) mask |= 1u << k;
+    if (!mask) continue;
+    Rec32 cur = rec[base + __ffs(mask) - 1];
+    mask &= mask - 1u;
+    while (true) {
+      const bool more = mask != 0u;
+      Rec32 nxt;
+      if (more) {
+        nxt = rec[base + __ffs(mask) - 1];
+        mask &= mask - 1u;
+      }
+      F.add(0, cur.a.x); F.add(1, cur.a.y); F.add(2, cur.a.z);
+      T.add(0, cur.b.x); T.add(1, cur.b.y); T.add(2, cur.b.z);
+      const float x = cur.a.w, t = rs + x;
+      if (fabsf(rs) >= fabsf(x)) rc += (rs - t) + x;
+      else rc += (x - t) + rs;
+      rs = t;
+      if (!more) break;
+      cur = nxt;
+    }
   }
 }
 
-// The fused split pass: reads history buffer pcur, writes 1 - pcur (the
-// caller flips pcur when the pass counts as a step).
-void launch_force_split(dem_handle* h, int mode) {
-  if (mode == 0) launch_force_split_m<0>(h);
-  else if (mode == 1) launch_force_split_m<1>(h);
-  else launch_force_split_m<2>(h);
+// Kernel 2 (per particle): wall terms (k_walls), the particle's incoming
+// records (transpose order) and its own row's, compensated FP32 sums, the
+// rolling-friction torque -MEW_R*(2R)*sum(KN*OVERLAP_N)*OMEGA/|OMEGA|, and
+// the integration (MODE 1 Euler, 2 Adams-Bashforth) or FC/TOW (MODE 0).
+template <int MODE, bool B>
+__global__ void __launch_bounds__(256)
+k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
+               const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
+               double4* __restrict__ omg_n, const int8_t* __restrict__ state, const double* __restrict__ wf,
+               uint8_t* __restrict__ wall_hit, const int* __restrict__ row_end, const int* __restrict__ in_start,
+               const uint8_t* __restrict__ pflag, const uint8_t* __restrict__ in_flag,
+               const Rec32* __restrict__ rec_own, const Rec32* __restrict__ rec_in, double* __restrict__ fc,
+               double* __restrict__ tow, double* __restrict__ acc_old, double* __restrict__ rot_acc_old,
+               unsigned* __restrict__ vslot, CellOut cells) {
+  const int me = blockIdx.x * blockDim.x + threadIdx.x;
+  if (me >= p0.n) return;
+  const DevParams& p = sysp<B>(p0, bv, me);
+  const int8_t st = state[me];
+  const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
+  double f0[3] = {0.0, 0.0, 0.0}, t0[3] = {0.0, 0.0, 0.0};
+  if (wall_hit[me]) {
+    wall_hit[me] = 0;
+    if (st == DEM_STATE_NORMAL) {
+      const double* o = wf + 6 * (size_t)me;
+      f0[0] = o[0]; f0[1] = o[1]; f0[2] = o[2]; t0[0] = o[3]; t0[1] = o[4]; t0[2] = o[5];
+    }
+  }
+  Comp3 F, T;
+  F.zero(); T.zero();
+  float rs = 0.f, rc = 0.f;
+  if (st != DEM_STATE_NONEXISTENT) {
+    add_range(in_start[me], in_start[me + 1], in_flag, rec_in, F, T, rs, rc);
+    add_range(me ? row_end[me - 1] : 0, row_end[me], pflag, rec_own, F, T, rs, rc);
+  }
+  double f[3], t[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) { f[c] = f0[c] + F.value(c); t[c] = t0[c] + T.value(c); }
+  if (p.mew_r > 0.0) {
+    const float w32[3] = {(float)W.x, (float)W.y, (float)W.z};
+    const float om = sqrtf(w32[0] * w32[0] + w32[1] * w32[1] + w32[2] * w32[2]);
+    if (om > 0.f) {
+      const double sc = -(p.mew_r * (2.0 * X.w) * ((double)rs + (double)rc)) / (double)om;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) t[c] += sc * (double)w32[c];
+    }
+  }
+  const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
+  finish_particle<MODE>(p, me, st, x, v, w, X.w, V.w, W.w, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
+                        rot_acc_old, vslot, cells);
+}
+
+// The split records live in the handle's record array: the owner records
+// in its first 32*cap bytes, the neighbour records in the next 32*cap (the
+// array holds 80*cap bytes, the FP64 record size).
+static Rec32* rec_own_of(dem_handle* h) { return reinterpret_cast<Rec32*>(h->prec); }
+static Rec32* rec_in_of(dem_handle* h) { return reinterpret_cast<Rec32*>(h->prec) + h->pair_cap; }
+static_assert(2 * sizeof(Rec32) <= sizeof(PairRec), "split records fit the record array");
+
+template <int COLL, bool B>
+static void launch_pairs_split_t(dem_handle* h) {
+  const int c = h->cur;
+  const int T = h->tune.pair_threads;
+  k_pairs_split<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
+      h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->in_pos, h->pos4[c], h->vel4[c],
+      h->omg4[c], h->state, h->phase, h->pft[h->pcur], h->pflag(), h->in_flag, h->pgap, h->skin, rec_own_of(h),
+      rec_in_of(h), h->derr);
+  DEM_LAUNCH(h);
+}
+
+void launch_pairs_split(dem_handle* h) {
+  const bool hz = h->dp.coll == DEM_COLL_HERTZ;
+  if (h->batch()) hz ? launch_pairs_split_t<DEM_COLL_HERTZ, true>(h) : launch_pairs_split_t<DEM_COLL_LSD, true>(h);
+  else hz ? launch_pairs_split_t<DEM_COLL_HERTZ, false>(h) : launch_pairs_split_t<DEM_COLL_LSD, false>(h);
+}
+
+template <int MODE, bool B>
+static void launch_gather_split_t(dem_handle* h) {
+  const int T = h->tune.gather_threads, G = (h->n + T - 1) / T;
+  const int c = h->cur;
+  k_gather_split<MODE, B><<<G, T, 0, h->stream>>>(
+      h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
+      h->state, h->wf, h->wall_hit, h->row_end[h->rb], h->in_start, h->pflag(), h->in_flag, rec_own_of(h),
+      rec_in_of(h), h->fc, h->tow, h->acc_old, h->rot_acc_old, h->vslot, gather_cells<MODE, B>(h));
+  DEM_LAUNCH(h);
+}
+
+void launch_gather_split(dem_handle* h, int mode) {
+  const bool bt = h->batch();
+  if (mode == 0) bt ? launch_gather_split_t<0, true>(h) : launch_gather_split_t<0, false>(h);
+  else if (mode == 1) bt ? launch_gather_split_t<1, true>(h) : launch_gather_split_t<1, false>(h);
+  else bt ? launch_gather_split_t<2, true>(h) : launch_gather_split_t<2, false>(h);
 }
 
 }  // namespace demb

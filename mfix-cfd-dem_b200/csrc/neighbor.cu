@@ -505,8 +505,12 @@ __global__ void k_in_fill(const int* __restrict__ d_np, const int* __restrict__ 
   }
 }
 
-// incoming pairs of each particle in ascending pair index (= owner order)
-__global__ void k_in_sort(int n, const int* __restrict__ in_start, int2* __restrict__ in_pair) {
+// incoming pairs of each particle in ascending pair index (= owner order);
+// each pair's slot in the list (in_pos) and a cleared contact flag of the
+// slot (in_flag: no pair of a new list is in contact before its first force
+// pass)
+__global__ void k_in_sort(int n, const int* __restrict__ in_start, int2* __restrict__ in_pair,
+                          int* __restrict__ in_pos, uint8_t* __restrict__ in_flag) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   int s = in_start[j], e = in_start[j + 1];
@@ -515,6 +519,10 @@ __global__ void k_in_sort(int n, const int* __restrict__ in_start, int2* __restr
     int b = a - 1;
     while (b >= s && in_pair[b].y > v.y) { in_pair[b + 1] = in_pair[b]; --b; }
     in_pair[b + 1] = v;
+  }
+  for (int a = s; a < e; ++a) {
+    in_pos[in_pair[a].y] = a;
+    in_flag[a] = 0;
   }
 }
 
@@ -531,7 +539,7 @@ int build_transpose(dem_handle* h, int nb) {
   if (int rc = check_cuda(h, cudaMemsetAsync(h->in_fill, 0, sizeof(int) * n, h->stream), "memset")) return rc;
   k_in_fill<<<BP, T, 0, h->stream>>>(h->d_np, h->nbrs[nb], h->pair_owner, h->in_start, h->in_fill, h->in_pair);
   DEM_LAUNCH(h);
-  k_in_sort<<<B, T, 0, h->stream>>>(n, h->in_start, h->in_pair);
+  k_in_sort<<<B, T, 0, h->stream>>>(n, h->in_start, h->in_pair, h->in_pos, h->in_flag);
   DEM_LAUNCH(h);
   return check_cuda(h, cudaGetLastError(), "transpose");
 }
@@ -542,6 +550,7 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   while (cap < need) cap *= 2;
   const long long old = h->pair_cap;  // the whole old allocation (the count may be stale)
   int* nb[2]; double* pf[2]; int2* inp; int* own; uint8_t* pfl[2]; PairRec* prc; float* gap;
+  int* ipos; uint8_t* ifl;
   for (int b = 0; b < 2; ++b) {
     if (int rc = check_cuda(h, cudaMalloc(&nb[b], sizeof(int) * cap), "cudaMalloc nbrs")) return rc;
     if (int rc = check_cuda(h, cudaMalloc(&pf[b], sizeof(double) * 3 * cap), "cudaMalloc pft")) return rc;
@@ -551,6 +560,8 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   if (int rc = check_cuda(h, cudaMalloc(&own, sizeof(int) * cap), "cudaMalloc owner")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&prc, sizeof(PairRec) * cap), "cudaMalloc prec")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&gap, sizeof(float) * cap), "cudaMalloc pgap")) return rc;
+  if (int rc = check_cuda(h, cudaMalloc(&ipos, sizeof(int) * cap), "cudaMalloc in_pos")) return rc;
+  if (int rc = check_cuda(h, cudaMalloc(&ifl, cap), "cudaMalloc in_flag")) return rc;
   if (old > 0) {
     // keep the current list and history (the rebuild reads them)
     cudaMemcpyAsync(nb[h->rb], h->nbrs[h->rb], sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
@@ -559,6 +570,8 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
     cudaMemcpyAsync(own, h->pair_owner, sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(pfl[h->pcur], h->pflag(), old, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(gap, h->pgap, sizeof(float) * old, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(ipos, h->in_pos, sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(ifl, h->in_flag, old, cudaMemcpyDeviceToDevice, h->stream);
   }
   cudaStreamSynchronize(h->stream);
   for (int b = 0; b < 2; ++b) {
@@ -566,7 +579,9 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
     h->nbrs[b] = nb[b]; h->pft[b] = pf[b]; h->pflagb[b] = pfl[b];
   }
   cudaFree(h->in_pair); cudaFree(h->pair_owner); cudaFree(h->prec); cudaFree(h->pgap);
+  cudaFree(h->in_pos); cudaFree(h->in_flag);
   h->in_pair = inp; h->pair_owner = own; h->prec = prc; h->pgap = gap;
+  h->in_pos = ipos; h->in_flag = ifl;
   h->pair_cap = cap;
   invalidate_graphs(h);  // captured steps point at the old arrays
   return check_cuda(h, cudaGetLastError(), "grow pairs");

@@ -44,7 +44,6 @@ static void fill_out(const dem_handle* h, dem_tuning* o, double pms, double gms,
   o->pair_blocks_per_sm = h->tune.pair_bpsm;
   o->gather_threads = h->tune.gather_threads;
   o->neigh_threads = h->tune.neigh_threads;
-  o->split_lanes = h->tune.split_lanes;
   o->pair_ms = pms;
   o->gather_ms = gms;
   o->neigh_ms = nms;
@@ -61,11 +60,12 @@ int dem_autotune(dem_handle* h, int32_t reps, dem_tuning* out) {
   if (!h->have_state || !h->have_pairs) return set_err(h, DEM_ERR_STATE, "state or pair list missing");
   invalidate_graphs(h);
   const size_t P = (size_t)host_pairs(h);
-  char* snap = (char*)stage_buffer(h, sizeof(double) * 3 * P + P + 64);
+  char* snap = (char*)stage_buffer(h, sizeof(double) * 3 * P + 2 * P + 64);
   if (!snap) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
   if (P) {
     cudaMemcpyAsync(snap, h->pft[h->pcur], sizeof(double) * 3 * P, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(snap + sizeof(double) * 3 * P, h->pflag(), P, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(snap + sizeof(double) * 3 * P + P, h->in_flag, P, cudaMemcpyDeviceToDevice, h->stream);
   }
   const int threads[3] = {64, 128, 256};
   const int bpsm[4] = {2, 4, 8, 16};
@@ -83,18 +83,10 @@ int dem_autotune(dem_handle* h, int32_t reps, dem_tuning* out) {
   h->tune = t;
   h->tune.pair_threads = best.pair_threads;
   h->tune.pair_bpsm = best.pair_bpsm;
-  // the split pass has no pair kernel: its fused pass is timed over the
-  // threads per block and the lanes per particle
-  const bool split = h->dp.prec == DEM_PREC_SPLIT;
-  const int lanes[4] = {1, 2, 4, 8};
-  for (int L : lanes) {
-    if (!split && L != t.split_lanes) continue;
-    for (int T : threads) {
-      h->tune.gather_threads = T;
-      h->tune.split_lanes = L;
-      const float ms = time_launches(h, reps, [&] { launch_pairs_only(h); launch_gather_only(h); });
-      if (ms - best_p < best_g) { best_g = ms - best_p; best.gather_threads = T; best.split_lanes = L; }
-    }
+  for (int T : threads) {
+    h->tune.gather_threads = T;
+    const float ms = time_launches(h, reps, [&] { launch_pairs_only(h); launch_gather_only(h); });
+    if (ms - best_p < best_g) { best_g = ms - best_p; best.gather_threads = T; }
   }
   h->tune = t;
   const int nthreads[3] = {32, 64, 128};
@@ -107,6 +99,7 @@ int dem_autotune(dem_handle* h, int32_t reps, dem_tuning* out) {
   if (P) {
     cudaMemcpyAsync(h->pft[h->pcur], snap, sizeof(double) * 3 * P, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(h->pflag(), snap + sizeof(double) * 3 * P, P, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->in_flag, snap + sizeof(double) * 3 * P + P, P, cudaMemcpyDeviceToDevice, h->stream);
   }
   // the timed pair launches added to the contact counters
   cudaMemsetAsync(&h->derr->n_contacts, 0, 2 * sizeof(unsigned long long), h->stream);
@@ -126,11 +119,8 @@ int dem_set_tuning(dem_handle* h, const dem_tuning* in) {
   cudaSetDevice(h->dev);
   auto ok = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v % 32) == 0; };
   if (!ok(in->pair_threads, 32, 256) || !ok(in->gather_threads, 32, 256) || !ok(in->neigh_threads, 32, 128) ||
-      in->pair_blocks_per_sm < 1 || in->pair_blocks_per_sm > 64 ||
-      !(in->split_lanes == 0 || in->split_lanes == 1 || in->split_lanes == 2 || in->split_lanes == 4 ||
-        in->split_lanes == 8))
+      in->pair_blocks_per_sm < 1 || in->pair_blocks_per_sm > 64)
     return set_err(h, DEM_ERR_ARG, "launch shape out of range");
-  if (in->split_lanes) h->tune.split_lanes = in->split_lanes;
   h->tune.pair_threads = in->pair_threads;
   h->tune.pair_bpsm = in->pair_blocks_per_sm;
   h->tune.gather_threads = in->gather_threads;

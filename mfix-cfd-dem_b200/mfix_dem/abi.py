@@ -156,9 +156,7 @@ class DemTuning(C.Structure):
         ("pair_ms", C.c_double),
         ("gather_ms", C.c_double),
         ("neigh_ms", C.c_double),
-        ("split_lanes", C.c_int32),
-        ("reserved_i", C.c_int32),
-        ("reserved", C.c_double * 3),
+        ("reserved", C.c_double * 4),
     ]
 
     def as_dict(self):

@@ -363,7 +363,6 @@ class DemSystem:
         t = abi.DemTuning()
         for k in ("pair_threads", "pair_blocks_per_sm", "gather_threads", "neigh_threads"):
             setattr(t, k, int(tuning[k]))
-        t.split_lanes = int(tuning.get("split_lanes", 0))
         self._call("set_tuning", self._h, C.byref(t))
 
     def force_error(self) -> float:
