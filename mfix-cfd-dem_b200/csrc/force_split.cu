@@ -247,19 +247,31 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
   }
 }
 
+// Contact bits (PF_CONTACT, bit 0 of each flag byte) of flags[base,
+// base + cnt), cnt <= 32, as a mask: the bytes are read as aligned 32-bit
+// words (the flag arrays carry 16 bytes of padding past their capacity).
+__device__ __forceinline__ unsigned contact_mask(const uint8_t* __restrict__ flags, int base, int cnt) {
+  static_assert(PF_CONTACT == 1, "contact bit is bit 0");
+  unsigned mask = 0u;
+  const int w0 = base & ~3;
+  for (int w = w0; w < base + cnt; w += 4) {
+    const uint32_t v = *reinterpret_cast<const uint32_t*>(flags + w) & 0x01010101u;
+    const unsigned b4 = (v | (v >> 7) | (v >> 14) | (v >> 21)) & 0xFu;  // byte k -> bit k
+    const int sh = w - base;
+    mask |= sh >= 0 ? (b4 << sh) : (b4 >> -sh);
+  }
+  return cnt >= 32 ? mask : (mask & ((1u << cnt) - 1u));
+}
+
 // The records of one contiguous range [a, e) whose flag bytes say contact,
-// a window of up to 32 at a time: the window's flags first (independent
-// loads), then the flagged records, each issued before the previous one is
-// added.
+// a window of up to 32 at a time: the window's flags first, then the flagged
+// records, each issued before the previous one is added.
 __device__ __forceinline__ void add_range(int a, int e, const uint8_t* __restrict__ flags,
                                           const Rec32* __restrict__ rec, Comp3& F, Comp3& T, float& rs,
                                           float& rc) {
   for (int base = a; base < e; base += 32) {
     const int cnt = min(32, e - base);
-    unsigned mask = 0u;
-#pragma unroll 8
-    for (int k = 0; k < 32; ++k)
-      if (k < cnt && (flags[base + k] & PF_CONTACT)) mask |= 1u << k;
+    unsigned mask = contact_mask(flags, base, cnt);
     if (!mask) continue;
     Rec32 cur = rec[base + __ffs(mask) - 1];
     mask &= mask - 1u;
@@ -300,6 +312,15 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
   if (me >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, me);
   const int8_t st = state[me];
+  // the sums first, the particle's own state and wall terms after them (few
+  // registers live across the record loops)
+  Comp3 F, T;
+  F.zero(); T.zero();
+  float rs = 0.f, rc = 0.f;
+  if (st != DEM_STATE_NONEXISTENT) {
+    add_range(in_start[me], in_start[me + 1], in_flag, rec_in, F, T, rs, rc);
+    add_range(me ? row_end[me - 1] : 0, row_end[me], pflag, rec_own, F, T, rs, rc);
+  }
   const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
   double f0[3] = {0.0, 0.0, 0.0}, t0[3] = {0.0, 0.0, 0.0};
   if (wall_hit[me]) {
@@ -308,13 +329,6 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
       const double* o = wf + 6 * (size_t)me;
       f0[0] = o[0]; f0[1] = o[1]; f0[2] = o[2]; t0[0] = o[3]; t0[1] = o[4]; t0[2] = o[5];
     }
-  }
-  Comp3 F, T;
-  F.zero(); T.zero();
-  float rs = 0.f, rc = 0.f;
-  if (st != DEM_STATE_NONEXISTENT) {
-    add_range(in_start[me], in_start[me + 1], in_flag, rec_in, F, T, rs, rc);
-    add_range(me ? row_end[me - 1] : 0, row_end[me], pflag, rec_own, F, T, rs, rc);
   }
   double f[3], t[3];
 #pragma unroll

@@ -554,14 +554,15 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   for (int b = 0; b < 2; ++b) {
     if (int rc = check_cuda(h, cudaMalloc(&nb[b], sizeof(int) * cap), "cudaMalloc nbrs")) return rc;
     if (int rc = check_cuda(h, cudaMalloc(&pf[b], sizeof(double) * 3 * cap), "cudaMalloc pft")) return rc;
-    if (int rc = check_cuda(h, cudaMalloc(&pfl[b], cap), "cudaMalloc pflag")) return rc;
+    // flag arrays carry 16 bytes of padding: the gather reads them as aligned words
+    if (int rc = check_cuda(h, cudaMalloc(&pfl[b], cap + 16), "cudaMalloc pflag")) return rc;
   }
   if (int rc = check_cuda(h, cudaMalloc(&inp, sizeof(int2) * cap), "cudaMalloc in_pair")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&own, sizeof(int) * cap), "cudaMalloc owner")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&prc, sizeof(PairRec) * cap), "cudaMalloc prec")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&gap, sizeof(float) * cap), "cudaMalloc pgap")) return rc;
   if (int rc = check_cuda(h, cudaMalloc(&ipos, sizeof(int) * cap), "cudaMalloc in_pos")) return rc;
-  if (int rc = check_cuda(h, cudaMalloc(&ifl, cap), "cudaMalloc in_flag")) return rc;
+  if (int rc = check_cuda(h, cudaMalloc(&ifl, cap + 16), "cudaMalloc in_flag")) return rc;
   if (old > 0) {
     // keep the current list and history (the rebuild reads them)
     cudaMemcpyAsync(nb[h->rb], h->nbrs[h->rb], sizeof(int) * old, cudaMemcpyDeviceToDevice, h->stream);
