@@ -150,8 +150,9 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
               const int* __restrict__ nbrs, const int* __restrict__ in_pos, const double4* __restrict__ pos4,
               const double4* __restrict__ vel4, const double4* __restrict__ omg4, const int8_t* __restrict__ state,
               const uint8_t* __restrict__ phase, double* __restrict__ pft, uint8_t* __restrict__ pflag,
-              uint8_t* __restrict__ in_flag, const float* __restrict__ pgap, const double* __restrict__ skin,
-              Rec32* __restrict__ rec_own, Rec32* __restrict__ rec_in, DevErr* __restrict__ err) {
+              uint8_t* __restrict__ in_flag, uint8_t* __restrict__ touched, const float* __restrict__ pgap,
+              const double* __restrict__ skin, Rec32* __restrict__ rec_own, Rec32* __restrict__ rec_in,
+              DevErr* __restrict__ err) {
   const long long np = min((long long)*d_np, cap);
   const long long stride = (long long)gridDim.x * blockDim.x;
   // the bound in FP32, rounded up: a pair is skipped only when its gap
@@ -214,8 +215,9 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
             if (f0 & PF_HIST) { pin[0] = po[0]; pin[1] = po[1]; pin[2] = po[2]; }
             double ot[3];
             PairTerms o;
-            split_contact<COLL>(p, a, va, wa, phase[ll], b, vb, wb, phase[i], dist, d2, r_lm * r_lm - d2, pin, ot,
-                                o);
+            // one solids phase: no phase to look up
+            const int phl = p.nph > 1 ? phase[ll] : 0, phi = p.nph > 1 ? phase[i] : 0;
+            split_contact<COLL>(p, a, va, wa, phl, b, vb, wb, phi, dist, d2, r_lm * r_lm - d2, pin, ot, o);
             po[0] = ot[0]; po[1] = ot[1]; po[2] = ot[2];
             const float rol = o.kn * o.ov;
             Rec32 ro, ri;
@@ -225,6 +227,8 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
             ri.b = make_float4(o.dci2 * o.tf[0], o.dci2 * o.tf[1], o.dci2 * o.tf[2], 0.f);
             rec_own[cc] = ro;
             rec_in[in_pos[cc]] = ri;
+            touched[ll] = 1;
+            touched[i] = 1;
             f = PF_CONTACT | ((ot[0] != 0.0 || ot[1] != 0.0 || ot[2] != 0.0) ? PF_HIST : 0);
             ++ncont;
           }
@@ -295,7 +299,8 @@ __device__ __forceinline__ void add_range(int a, int e, const uint8_t* __restric
 }
 
 // Kernel 2 (per particle): wall terms (k_walls), the particle's incoming
-// records (transpose order) and its own row's, compensated FP32 sums, the
+// records (transpose order) and its own row's -- only for particles the
+// pair kernel marked as in some contact --, compensated FP32 sums, the
 // rolling-friction torque -MEW_R*(2R)*sum(KN*OVERLAP_N)*OMEGA/|OMEGA|, and
 // the integration (MODE 1 Euler, 2 Adams-Bashforth) or FC/TOW (MODE 0).
 template <int MODE, bool B>
@@ -303,8 +308,8 @@ __global__ void __launch_bounds__(256)
 k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const double4* __restrict__ vel_c,
                const double4* __restrict__ omg_c, double4* __restrict__ pos_n, double4* __restrict__ vel_n,
                double4* __restrict__ omg_n, const int8_t* __restrict__ state, const double* __restrict__ wf,
-               uint8_t* __restrict__ wall_hit, const int* __restrict__ row_end, const int* __restrict__ in_start,
-               const uint8_t* __restrict__ pflag, const uint8_t* __restrict__ in_flag,
+               uint8_t* __restrict__ wall_hit, uint8_t* __restrict__ touched, const int* __restrict__ row_end,
+               const int* __restrict__ in_start, const uint8_t* __restrict__ pflag, const uint8_t* __restrict__ in_flag,
                const Rec32* __restrict__ rec_own, const Rec32* __restrict__ rec_in, double* __restrict__ fc,
                double* __restrict__ tow, double* __restrict__ acc_old, double* __restrict__ rot_acc_old,
                unsigned* __restrict__ vslot, CellOut cells) {
@@ -317,7 +322,10 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
   Comp3 F, T;
   F.zero(); T.zero();
   float rs = 0.f, rc = 0.f;
-  if (st != DEM_STATE_NONEXISTENT) {
+  // a particle in no contact of this pass has no record to add
+  const bool ph = touched[me] != 0;
+  if (ph) touched[me] = 0;
+  if (st != DEM_STATE_NONEXISTENT && ph) {
     add_range(in_start[me], in_start[me + 1], in_flag, rec_in, F, T, rs, rc);
     add_range(me ? row_end[me - 1] : 0, row_end[me], pflag, rec_own, F, T, rs, rc);
   }
@@ -360,8 +368,8 @@ static void launch_pairs_split_t(dem_handle* h) {
   const int T = h->tune.pair_threads;
   k_pairs_split<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
       h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->in_pos, h->pos4[c], h->vel4[c],
-      h->omg4[c], h->state, h->phase, h->pft[h->pcur], h->pflag(), h->in_flag, h->pgap, h->skin, rec_own_of(h),
-      rec_in_of(h), h->derr);
+      h->omg4[c], h->state, h->phase, h->pft[h->pcur], h->pflag(), h->in_flag, h->touched, h->pgap, h->skin,
+      rec_own_of(h), rec_in_of(h), h->derr);
   DEM_LAUNCH(h);
 }
 
@@ -377,8 +385,8 @@ static void launch_gather_split_t(dem_handle* h) {
   const int c = h->cur;
   k_gather_split<MODE, B><<<G, T, 0, h->stream>>>(
       h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],
-      h->state, h->wf, h->wall_hit, h->row_end[h->rb], h->in_start, h->pflag(), h->in_flag, rec_own_of(h),
-      rec_in_of(h), h->fc, h->tow, h->acc_old, h->rot_acc_old, h->vslot, gather_cells<MODE, B>(h));
+      h->state, h->wf, h->wall_hit, h->touched, h->row_end[h->rb], h->in_start, h->pflag(), h->in_flag,
+      rec_own_of(h), rec_in_of(h), h->fc, h->tow, h->acc_old, h->rot_acc_old, h->vslot, gather_cells<MODE, B>(h));
   DEM_LAUNCH(h);
 }
 

@@ -224,13 +224,9 @@ __device__ __forceinline__ void neigh_run(const DevParams& p, const NeighFrame& 
   qe = fstart[base + hi + 1];
 }
 
-// Candidate q of the sorted copy: a neighbour of the frame's particle when it
-// is a later or non-NORMAL particle (the half list of DESGRID_NEIGH_BUILD),
-// in the reference's DES-grid stencil and within FACTOR_RLM*(r_l + r_i);
-// its row key (stencil rank << 27 | index) through *key.
-__device__ __forceinline__ bool neigh_test(const DevParams& p, const NeighFrame& F, const int4* __restrict__ sinfo,
-                                           const double4* __restrict__ spos, const float4* __restrict__ sposf, int q,
-                                           uint32_t* key) {
+// The conservative FP32 pre-check of candidate q (see neigh_test): false
+// only for a candidate the exact test rejects.
+__device__ __forceinline__ bool neigh_pre(const NeighFrame& F, const float4* __restrict__ sposf, int q) {
   {
     // most candidates are far out of reach, and FP32 copies of the two
     // positions show it: the FP32 nearest-image distance less the frame's
@@ -246,8 +242,17 @@ __device__ __forceinline__ bool neigh_test(const DevParams& p, const NeighFrame&
     e1 = e1 - rintf(e1 * F.inv_lf[1]) * F.lf[1];
     e2 = e2 - rintf(e2 * F.inv_lf[2]) * F.lf[2];
     const float sr = F.frf * (F.cpf.w + f.w) + F.tolf;
-    if (e0 * e0 + e1 * e1 + e2 * e2 > sr * sr * 1.00002f) return false;
+    return !(e0 * e0 + e1 * e1 + e2 * e2 > sr * sr * 1.00002f);
   }
+}
+
+// Candidate q of the sorted copy (past the pre-check): a neighbour of the
+// frame's particle when it is a later or non-NORMAL particle (the half list
+// of DESGRID_NEIGH_BUILD), in the reference's DES-grid stencil and within
+// FACTOR_RLM*(r_l + r_i); its row key (stencil rank << 27 | index) through
+// *key.
+__device__ __forceinline__ bool neigh_exact(const DevParams& p, const NeighFrame& F, const int4* __restrict__ sinfo,
+                                            const double4* __restrict__ spos, int q, uint32_t* key) {
   const int4 o = sinfo[q];
   const int nb = o.x;
   if (nb == F.cur) return false;
@@ -301,6 +306,7 @@ __device__ __forceinline__ bool neigh_test(const DevParams& p, const NeighFrame&
 // order.  (A warp per particle, testing 32 candidates at a time, was
 // measured slower: the per-particle set-up and run search repeated in every
 // warp cost more than the idle lanes of this loop.)
+constexpr int NSURV = 24;  // pre-checked candidates buffered per thread
 template <bool FILL, bool B>
 __global__ void __launch_bounds__(128)
 k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
@@ -308,6 +314,7 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
         const int4* __restrict__ sinfo, const int* __restrict__ fstart, const DevErr* __restrict__ err,
         int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
         uint8_t* __restrict__ rank_buf, int* __restrict__ owner, uint32_t* __restrict__ nslot, long long cap) {
+  __shared__ int s_surv[NSURV * 128];
   const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (q0 >= p0.n || q0 >= *n_exist) return;
   const int4 me = sinfo[q0];
@@ -333,13 +340,14 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
   NeighFrame F;
   neigh_frame<B>(p, me, spos[q0], F);
   int cnt = 0;
-  const int nr = neigh_nruns(p, F);
-  for (int r = 0; r < nr; ++r) {
-    int qs, qe;
-    neigh_run(p, F, fstart, r, qs, qe);
-    for (int q = qs; q < qe; ++q) {
+  // Candidates that pass the FP32 pre-check (a few per row) wait in this
+  // thread's column of s_surv and get the exact test in a second loop, so
+  // the long exact path runs with every lane holding work instead of one
+  // lane at a time inside the candidate scan.
+  int ns = 0;
+  auto exact = [&](int q) {
       uint32_t key;
-      if (!neigh_test(p, F, sinfo, spos, sposf, q, &key)) continue;
+      if (!neigh_exact(p, F, sinfo, spos, q, &key)) return;
       const int rank = (int)(key >> 27), nb = (int)(key & 0x7ffffffu);
       if (!FILL && cnt < NSLOT) {
         // keep the row sorted by (rank, index) in the slots
@@ -365,8 +373,22 @@ k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const doubl
         }
       }
       ++cnt;
+  };
+  auto flush = [&]() {
+    for (int s = 0; s < ns; ++s) exact(s_surv[s * blockDim.x + threadIdx.x]);
+    ns = 0;
+  };
+  const int nr = neigh_nruns(p, F);
+  for (int r = 0; r < nr; ++r) {
+    int qs, qe;
+    neigh_run(p, F, fstart, r, qs, qe);
+    for (int q = qs; q < qe; ++q) {
+      if (!neigh_pre(F, sposf, q)) continue;
+      s_surv[ns * blockDim.x + threadIdx.x] = q;
+      if (++ns == NSURV) flush();
     }
   }
+  flush();
   if (FILL) row_se[cur] = (int)min((long long)start + cnt, cap);   // start -> end pointer
   else row_cnt[cur] = cnt;
 }
