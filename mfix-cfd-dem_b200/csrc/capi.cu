@@ -287,6 +287,7 @@ void demb::fill_devparams(const dem_params& q, int n, DevParams& p) {
     p.grav[a] = q.grav[a];
     p.lo[a] = q.domain_lo[a]; p.hi[a] = q.domain_hi[a];
     p.L[a] = q.domain_hi[a] - q.domain_lo[a];
+    p.inv_L[a] = 1.0 / p.L[a];
   }
   // desgrid_init for one rank (desgrid_mod.f:571-604, 780-850)
   p.istart1 = 2; p.iend1 = q.dg_imax + 1; p.istart2 = 1; p.iend2 = q.dg_imax + 2;
@@ -443,6 +444,7 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
   A((void**)&h->sposf, sizeof(float4) * n);
   A((void**)&h->sinfo, sizeof(int4) * n);
   A((void**)&h->nslot, sizeof(uint32_t) * NSLOT * n);
+  A((void**)&h->long_rows, sizeof(int) * (n + 1));
   A((void**)&h->row_cnt, sizeof(int) * n);
   A((void**)&h->in_cnt, sizeof(int) * n);
   A((void**)&h->in_start, sizeof(int) * (n + 1));
@@ -527,7 +529,7 @@ int dem_destroy(dem_handle* h) {
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
                   h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflagb[0], h->pflagb[1], h->in_pos, h->in_flag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->d_ibc, h->pic_fresh, h->d_seed, h->skin, h->vslot, h->pgap,
-                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->d_np,
+                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->long_rows, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }

@@ -71,7 +71,7 @@ struct DevParams {
   double kn, kt, kn_w, kt_w, mew, mew_w, mew_r, mew_rw;
   double factor_rlm, max_radius;
   double dg_start[3], dg_inv[3];
-  double lo[3], hi[3], L[3];
+  double lo[3], hi[3], L[3], inv_L[3];  // inv_L = 1 / L
   double etan[MAXP * MAXP], etat[MAXP * MAXP], hkn[MAXP * MAXP], hkt[MAXP * MAXP];
   double etanw[MAXP], etatw[MAXP], hkwn[MAXP], hkwt[MAXP];
   // FP32 copies for the split-precision pair force: HERT_KN, HERT_KT,
@@ -207,7 +207,8 @@ struct dem_handle {
   double4* spos = nullptr;    // n: positions in search-cell order (pair build)
   float4* sposf = nullptr;    // n: the same rounded to FP32 (conservative distance pre-check)
   int4* sinfo = nullptr;      // n: (particle, packed DES cell (i,j,k), state, search cell) in that order
-  uint32_t* nslot = nullptr;  // n * NSLOT: rows kept by the count pass of the pair build
+  uint32_t* nslot = nullptr;  // n * NSLOT: rows kept by the count pass of the pair build, by particle
+  int* long_rows = nullptr;   // n + 1: sorted-copy places of the rows longer than NSLOT, count at [n]
 
   // pairs
   long long pair_cap = 0;

@@ -71,18 +71,17 @@ __global__ void k_delete_rogue(DevParams p0, BatchView bv, int8_t* __restrict__ 
   atomicAdd(&err->rogue_removed, 1ull);
 }
 
-// Count (FILL = false) or fill (FILL = true) one row per particle.
+// Count and fill passes of the rows.
 //
-// Candidates come from the 27 search-grid cells around the particle; the
-// search grid is at least as fine as the DES grid and its cells are no
-// narrower than the largest search diameter, so every pair the reference
-// keeps is among the candidates.  A candidate is then tested exactly as the
-// reference tests it: it must lie in the particle's DES-grid stencil (the
-// coarse-grid reduction included), its periodic image is the one that
-// stencil cell holds, and the FP64 distance test is the reference's.  Each
-// kept neighbour carries its stencil rank ((lk, lj, li) order); the fill
-// pass inserts it into the row sorted by (rank, index), which is the order
-// of the reference's cell-by-cell scan.
+// Candidates come from the search-grid cells within the particle's reach
+// FACTOR_RLM*(r + MAX_RADIUS); the search grid is at least as fine as the
+// DES grid, so every pair the reference keeps is among the candidates.  A
+// candidate is then tested exactly as the reference tests it: it must lie
+// in the particle's DES-grid stencil (the coarse-grid reduction included),
+// its periodic image is the one that stencil cell holds, and the FP64
+// distance test is the reference's.  Each kept neighbour carries its
+// stencil rank ((lk, lj, li) order); the row is sorted by (rank, index),
+// which is the order of the reference's cell-by-cell scan.
 // The search runs over a cell-sorted copy of the candidate data: sinfo[q] =
 // (particle, DES cell as packed (i, j, k), state, search cell) and spos[q] =
 // (x, y, z, r) in the order of the search-grid cell lists.  Thread q handles
@@ -90,9 +89,9 @@ __global__ void k_delete_rogue(DevParams p0, BatchView bv, int8_t* __restrict__ 
 // the same cells, and every candidate read is a contiguous run of the sorted
 // arrays.
 //
-// The count pass also keeps the first NSLOT neighbours of each particle,
-// already in row order, as (rank << 27 | index) keys in nslot[q]; the fill
-// pass copies them, and rescans only the particles with longer rows.
+// The count pass also keeps the first NSLOT neighbours of each particle as
+// (rank << 27 | index) keys in nslot[q]; the fill pass writes them in row
+// order, and rescans only the particles with longer rows.
 template <bool B>
 __global__ void k_sorted_copy(DevParams p0, BatchView bv, int n, const int* __restrict__ n_exist,
                               const int* __restrict__ flist, const double4* __restrict__ pos4,
@@ -122,10 +121,13 @@ struct NeighFrame {
   float4 cpf;          // the particle's position and radius rounded to FP32
   float frf, lf[3], inv_lf[3];  // FACTOR_RLM and the periods in FP32 (0: not periodic)
   float tolf;          // rounding allowance of the FP32 pre-check (infinite: check off)
+  bool wrap;           // the search range reaches a cell at a periodic boundary
 };
 
-template <bool B>
-__device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, const double4& cp, NeighFrame& F) {
+// The part of the frame the exact test reads: the particle, its DES cell
+// and stencil, and the periods.
+__device__ __forceinline__ void neigh_frame_exact(const DevParams& p, const int4& me, const double4& cp,
+                                                  NeighFrame& F) {
   F.cur = me.x;
   F.cp = cp;
   F.fr = p.factor_rlm;
@@ -133,7 +135,26 @@ __device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, 
   F.s1[0] = p.istart1; F.s1[1] = p.jstart1; F.s1[2] = p.kstart1;
   F.e1[0] = p.iend1; F.e1[1] = p.jend1; F.e1[2] = p.kend1;
   F.ncl[0] = p.iend1 - p.istart1 + 1; F.ncl[1] = p.jend1 - p.jstart1 + 1; F.ncl[2] = p.kend1 - p.kstart1 + 1;
-  for (int ax = 0; ax < 3; ++ax) F.inv_l[ax] = (p.per[ax] && !(ax == 2 && p.no_k)) ? 1.0 / p.L[ax] : 0.0;
+  for (int ax = 0; ax < 3; ++ax) F.inv_l[ax] = (p.per[ax] && !(ax == 2 && p.no_k)) ? p.inv_L[ax] : 0.0;
+  const double cpos[3] = {cp.x, cp.y, cp.z};
+  const double mr = p.max_radius;
+  for (int ax = 0; ax < 3; ++ax) {
+    F.lo_off[ax] = 1; F.hi_off[ax] = 1;
+    if (ax == 2 && p.no_k) { F.lo_off[2] = 0; F.hi_off[2] = 0; continue; }
+    // the reference's stencil is the nearer 2 cells when the DES cells are
+    // wider than the search diameter (desgrid_mod.f:1116-1152)
+    const bool coarse = 1.0 > 2.0 * mr * F.fr * p.dg_inv[ax];
+    if (coarse) {
+      const double t = (cpos[ax] - p.dg_start[ax]) * p.dg_inv[ax];
+      const double off = t - (double)(long long)floor(t);
+      if (off >= 0.5) F.lo_off[ax] = 0; else F.hi_off[ax] = 0;
+    }
+  }
+}
+
+// The whole frame of a particle that scans candidates.
+__device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, const double4& cp, NeighFrame& F) {
+  neigh_frame_exact(p, me, cp, F);
   F.cpf = make_float4((float)cp.x, (float)cp.y, (float)cp.z, (float)cp.w);
   F.frf = (float)p.factor_rlm;
   // The FP32 pre-check's allowance.  For a neighbour (nearest-image distance
@@ -159,25 +180,13 @@ __device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, 
     }
     F.tolf = off ? INFINITY : tol;
   }
-  const double cpos[3] = {cp.x, cp.y, cp.z};
-  const double mr = p.max_radius;
-  for (int ax = 0; ax < 3; ++ax) {
-    F.lo_off[ax] = 1; F.hi_off[ax] = 1;
-    if (ax == 2 && p.no_k) { F.lo_off[2] = 0; F.hi_off[2] = 0; continue; }
-    // the reference's stencil is the nearer 2 cells when the DES cells are
-    // wider than the search diameter (desgrid_mod.f:1116-1152)
-    const bool coarse = 1.0 > 2.0 * mr * F.fr * p.dg_inv[ax];
-    if (coarse) {
-      const double t = (cpos[ax] - p.dg_start[ax]) * p.dg_inv[ax];
-      const double off = t - (double)(long long)floor(t);
-      if (off >= 0.5) F.lo_off[ax] = 0; else F.hi_off[ax] = 0;
-    }
-  }
   // the search cells within reach FACTOR_RLM*(r + MAX_RADIUS) of the
   // particle, each once: per axis a range of cells, wrapped on a periodic
   // axis (the whole axis when the range covers it); a margin of 1e-4 of the
   // reach covers the rounding of the cell index
-  const double reach = F.fr * (cp.w + mr);
+  const double cpos[3] = {cp.x, cp.y, cp.z};
+  const double reach = F.fr * (cp.w + p.max_radius);
+  F.wrap = false;
   for (int ax = 0; ax < 3; ++ax) {
     F.glo[ax] = 0; F.ghi[ax] = 0;
     if (ax == 2 && p.no_k) continue;
@@ -185,6 +194,14 @@ __device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, 
     int lo = (int)floor(t - w) + 1, hi = (int)floor(t + w) + 1;
     if (p.per[ax]) {
       if (hi - lo + 1 >= p.fn[ax]) { lo = 1; hi = p.fn[ax]; }
+      // Search cells 2..fn-1 of a periodic axis hold particles inside the
+      // domain at least one cell from its ends (a particle outside is
+      // binned to cell 1 or fn).  When the range lies within them, the
+      // particle and every candidate are such, and a candidate's image
+      // within reach is its own position: another image would put the
+      // particle within reach of a domain end, and the range into cell 1 or
+      // fn.  Only a range that reaches cell 1 or fn needs the image shift.
+      if (lo <= 1 || hi >= p.fn[ax]) F.wrap = true;
     } else {
       lo = max(lo, 0);
       hi = min(hi, p.fn[ax] + 1);
@@ -199,51 +216,77 @@ __device__ __forceinline__ int search_wrap(const DevParams& p, int g, int ax) {
   return g < 1 ? g + p.fn[ax] : (g > p.fn[ax] ? g - p.fn[ax] : g);
 }
 
-// The runs of the cell-sorted copy that hold the candidates: one per (i, k)
-// column of the range, two when the y range wraps (y is the fastest key, so
-// a column's cells are contiguous).
-__device__ __forceinline__ int neigh_runs_per_col(const DevParams& p, const NeighFrame& F) {
-  return (p.per[1] && (F.glo[1] < 1 || F.ghi[1] > p.fn[1])) ? 2 : 1;
-}
-__device__ __forceinline__ int neigh_nruns(const DevParams& p, const NeighFrame& F) {
-  return (F.ghi[2] - F.glo[2] + 1) * (F.ghi[0] - F.glo[0] + 1) * neigh_runs_per_col(p, F);
-}
-__device__ __forceinline__ void neigh_run(const DevParams& p, const NeighFrame& F, const int* __restrict__ fstart,
-                                          int r, int& qs, int& qe) {
-  const int rpc = neigh_runs_per_col(p, F);
-  const int col = r / rpc, sub = r % rpc;
-  const int ni = F.ghi[0] - F.glo[0] + 1;
-  const int gk = F.glo[2] + col / ni, gi = F.glo[0] + col % ni;
-  const int base = p.fcell_off + search_wrap(p, gk, 2) * p.fc2 + search_wrap(p, gi, 0) * p.fc1;
-  int lo = F.glo[1], hi = F.ghi[1];
-  if (rpc == 2) {
-    if (F.glo[1] < 1) { if (sub == 0) { lo = F.glo[1] + p.fn[1]; hi = p.fn[1]; } else { lo = 1; hi = F.ghi[1]; } }
-    else { if (sub == 0) { lo = F.glo[1]; hi = p.fn[1]; } else { lo = 1; hi = F.ghi[1] - p.fn[1]; } }
+// Calls run(qs, qe) for each run [qs, qe) of the sorted copy that holds the
+// frame's candidates: one per (i, k) column of the range, two when the y
+// range wraps (y is the fastest key, so a column's cells are contiguous).
+// HALF keeps only the candidates after the particle's place q0 in the copy
+// (in search cell c_own): a run that ends before c_own is skipped unread.
+template <bool HALF, class Run>
+__device__ __forceinline__ void for_runs(const DevParams& p, const NeighFrame& F, const int* __restrict__ fstart,
+                                         int q0, int c_own, Run&& run) {
+  int ylo0 = F.glo[1], yhi0 = F.ghi[1], ylo1 = 0, yhi1 = -1;
+  if (p.per[1] && (F.glo[1] < 1 || F.ghi[1] > p.fn[1])) {
+    if (F.glo[1] < 1) { ylo0 = F.glo[1] + p.fn[1]; yhi0 = p.fn[1]; ylo1 = 1; yhi1 = F.ghi[1]; }
+    else { ylo0 = F.glo[1]; yhi0 = p.fn[1]; ylo1 = 1; yhi1 = F.ghi[1] - p.fn[1]; }
   }
-  qs = fstart[base + lo];
-  qe = fstart[base + hi + 1];
+  for (int gk = F.glo[2]; gk <= F.ghi[2]; ++gk) {
+    const int bk = p.fcell_off + search_wrap(p, gk, 2) * p.fc2;
+    for (int gi = F.glo[0]; gi <= F.ghi[0]; ++gi) {
+      const int base = bk + search_wrap(p, gi, 0) * p.fc1;
+#pragma unroll
+      for (int sg = 0; sg < 2; ++sg) {
+        const int lo = sg ? ylo1 : ylo0, hi = sg ? yhi1 : yhi0;
+        if (hi < lo) continue;
+        const int c0 = base + lo, c1 = base + hi;
+        int qs;
+        if (HALF) {
+          if (c1 < c_own) continue;
+          qs = c0 > c_own ? fstart[c0] : q0 + 1;
+        } else {
+          qs = fstart[c0];
+        }
+        run(qs, fstart[c1 + 1]);
+      }
+    }
+  }
 }
 
-// The conservative FP32 pre-check of candidate q (see neigh_test): false
-// only for a candidate the exact test rejects.
-__device__ __forceinline__ bool neigh_pre(const NeighFrame& F, const float4* __restrict__ sposf, int q) {
-  {
-    // most candidates are far out of reach, and FP32 copies of the two
-    // positions show it: the FP32 nearest-image distance less the frame's
-    // rounding allowance is a lower bound of the exact distance for any
-    // neighbour, so a candidate beyond the search radius by more than the
-    // allowance (and a relative 2e-5 for the FP32 radius, squares and sum)
-    // is no neighbour under any test below.  On an axis that is not
-    // periodic the image shift is 0 * 0.  A NaN compares false and falls
-    // through to the exact test.
-    const float4 f = sposf[q];
-    float e0 = F.cpf.x - f.x, e1 = F.cpf.y - f.y, e2 = F.cpf.z - f.z;
-    e0 = e0 - rintf(e0 * F.inv_lf[0]) * F.lf[0];
-    e1 = e1 - rintf(e1 * F.inv_lf[1]) * F.lf[1];
-    e2 = e2 - rintf(e2 * F.inv_lf[2]) * F.lf[2];
-    const float sr = F.frf * (F.cpf.w + f.w) + F.tolf;
-    return !(e0 * e0 + e1 * e1 + e2 * e2 > sr * sr * 1.00002f);
-  }
+// The FP32 part of a frame as three float4: a = the particle's position
+// and radius, b = (FACTOR_RLM, allowance, period x, period y), c = (period
+// z, 1/period x, y, z); 0 for an axis that is not periodic.
+struct PreFrame {
+  float4 a, b, c;
+};
+__device__ __forceinline__ PreFrame pre_frame(const NeighFrame& F) {
+  return {F.cpf, make_float4(F.frf, F.tolf, F.lf[0], F.lf[1]), make_float4(F.lf[2], F.inv_lf[0], F.inv_lf[1], F.inv_lf[2])};
+}
+
+// The conservative FP32 pre-check of a candidate at f (see neigh_exact):
+// false only for a candidate the exact test rejects.  Most candidates are
+// far out of reach, and FP32 copies of the two positions show it: the FP32
+// nearest-image distance less the frame's rounding allowance is a lower
+// bound of the exact distance for any neighbour, so a candidate beyond the
+// search radius by more than the allowance (and a relative 2e-5 for the
+// FP32 radius, squares and sum) is no neighbour under any test below.  On
+// an axis that is not periodic the image shift is 0 * 0.  A NaN compares
+// false and falls through to the exact test.
+__device__ __forceinline__ bool pre_test(const PreFrame& G, const float4 f) {
+  float e0 = G.a.x - f.x, e1 = G.a.y - f.y, e2 = G.a.z - f.z;
+  e0 = e0 - rintf(e0 * G.c.y) * G.b.z;
+  e1 = e1 - rintf(e1 * G.c.z) * G.b.w;
+  e2 = e2 - rintf(e2 * G.c.w) * G.c.x;
+  const float sr = G.b.x * (G.a.w + f.w) + G.b.y;
+  return !(e0 * e0 + e1 * e1 + e2 * e2 > sr * sr * 1.00002f);
+}
+// The same test for a frame whose range needs no image shift (wrap false):
+// the separation is the difference of the two positions.  Fused
+// multiply-adds round less than the separate operations the margin allows
+// for.
+__device__ __forceinline__ bool pre_direct(const PreFrame& G, const float4 f) {
+  const float e0 = G.a.x - f.x, e1 = G.a.y - f.y, e2 = G.a.z - f.z;
+  const float d2 = __fmaf_rn(e2, e2, __fmaf_rn(e1, e1, __fmul_rn(e0, e0)));
+  const float sr = __fmaf_rn(G.b.x, G.a.w + f.w, G.b.y);
+  return !(d2 > sr * sr * 1.00002f);
 }
 
 // Candidate q of the sorted copy (past the pre-check): a neighbour of the
@@ -299,98 +342,202 @@ __device__ __forceinline__ bool neigh_exact(const DevParams& p, const NeighFrame
   return true;
 }
 
-// Count pass (FILL = false) and fill pass, a thread per particle of the
-// sorted copy.  The count pass keeps the first NSLOT neighbours of the row,
-// sorted by (rank, index), in the slots; the fill pass copies a row the
-// count pass kept whole and rescans a longer one, inserting in (rank, index)
-// order.  (A warp per particle, testing 32 candidates at a time, was
-// measured slower: the per-particle set-up and run search repeated in every
-// warp cost more than the idle lanes of this loop.)
 constexpr int NSURV = 24;  // pre-checked candidates buffered per thread
-template <bool FILL, bool B>
+
+// Count pass of the pair build, a half scan: each particle of the sorted
+// copy tests only the candidates after it in the copy, so each pair of
+// particles within reach of one another is examined once, by the one that
+// comes first.  (Each is in the other's search range: a neighbour lies
+// within FACTOR_RLM*(r_l + r_i) of the particle, inside the reach
+// FACTOR_RLM*(r + MAX_RADIUS) of either.)  The pair goes to the row of its
+// owner -- the NORMAL particle of lower index, or the NORMAL one of a
+// NORMAL / non-NORMAL pair, as DESGRID_NEIGH_BUILD keeps it -- and is given
+// the exact test in the owner's FP64 frame, so the row is the full scan's.
+// The owner's count is an atomic add; its first NSLOT keys go to its slots
+// nslot[owner] in the order found, and a row that grows past NSLOT enters
+// the long-row list (long_rows[0 .. long_rows[n]), sorted-copy places) once.
+// Candidates that pass the FP32 pre-check (a few per row) wait in this
+// thread's column of s_surv and get the exact test in a second loop, so the
+// long exact path runs with every lane holding work instead of one lane at
+// a time inside the candidate scan.
+template <bool B>
 __global__ void __launch_bounds__(128)
-k_neigh(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
-        const float4* __restrict__ sposf,
-        const int4* __restrict__ sinfo, const int* __restrict__ fstart, const DevErr* __restrict__ err,
-        int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
-        uint8_t* __restrict__ rank_buf, int* __restrict__ owner, uint32_t* __restrict__ nslot, long long cap) {
+k_neigh_count(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
+              const float4* __restrict__ sposf, const int4* __restrict__ sinfo, const int* __restrict__ fstart,
+              const DevErr* __restrict__ err, int* __restrict__ row_cnt, uint32_t* __restrict__ nslot,
+              int* __restrict__ long_rows) {
   __shared__ int s_surv[NSURV * 128];
   const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (q0 >= p0.n || q0 >= *n_exist) return;
   const int4 me = sinfo[q0];
+  if (me.z == DEM_STATE_NONEXISTENT) return;
   const int cur = me.x;
   const DevParams& p = sysp<B>(p0, bv, cur);
   const int first_rogue = B ? bv.first_rogue[bv.sys_of[cur]] : err->first_rogue;
-  if (me.z != DEM_STATE_NORMAL || cur >= first_rogue) return;
-  uint32_t* slot = nslot + (size_t)q0 * NSLOT;
-  int start = 0;
-  if (FILL) {
-    start = (int)min((long long)row_se[cur], cap);
-    const int kept = row_cnt[cur];
-    if (kept <= NSLOT) {
-      // the count pass kept the whole row
-      for (int c = 0; c < kept; ++c) {
-        const long long s = (long long)start + c;
-        if (s < cap) { nbrs[s] = (int)(slot[c] & 0x7ffffffu); owner[s] = cur; }
-      }
-      row_se[cur] = (int)min((long long)start + kept, cap);
-      return;
-    }
-  }
+  const bool me_normal = me.z == DEM_STATE_NORMAL;
   NeighFrame F;
-  neigh_frame<B>(p, me, spos[q0], F);
-  int cnt = 0;
-  // Candidates that pass the FP32 pre-check (a few per row) wait in this
-  // thread's column of s_surv and get the exact test in a second loop, so
-  // the long exact path runs with every lane holding work instead of one
-  // lane at a time inside the candidate scan.
-  int ns = 0;
+  neigh_frame(p, me, spos[q0], F);
   auto exact = [&](int q) {
-      uint32_t key;
-      if (!neigh_exact(p, F, sinfo, spos, q, &key)) return;
-      const int rank = (int)(key >> 27), nb = (int)(key & 0x7ffffffu);
-      if (!FILL && cnt < NSLOT) {
-        // keep the row sorted by (rank, index) in the slots
-        int b = cnt - 1;
-        while (b >= 0 && slot[b] > key) { slot[b + 1] = slot[b]; --b; }
-        slot[b + 1] = key;
-      }
-      if (FILL) {
-        long long sl = (long long)start + cnt;
-        if (sl < cap) {
-          // insertion into the row kept sorted by (rank, index)
-          long long b = sl - 1;
-          while (b >= start) {
-            const int rb = rank_buf[b];
-            if (rb < rank || (rb == rank && nbrs[b] < nb)) break;
-            nbrs[b + 1] = nbrs[b];
-            rank_buf[b + 1] = (uint8_t)rb;
-            --b;
-          }
-          nbrs[b + 1] = nb;
-          rank_buf[b + 1] = (uint8_t)rank;
-          owner[sl] = cur;
-        }
-      }
-      ++cnt;
+    const int4 o = sinfo[q];
+    if (o.z == DEM_STATE_NONEXISTENT) return;
+    const bool o_normal = o.z == DEM_STATE_NORMAL;
+    bool mine;
+    if (me_normal && o_normal) mine = cur < o.x;
+    else if (me_normal || o_normal) mine = me_normal;
+    else return;  // two non-NORMAL particles: no row holds the pair
+    uint32_t key;
+    int oq, oi;
+    if (mine) {
+      if (cur >= first_rogue || !neigh_exact(p, F, sinfo, spos, q, &key)) return;
+      oq = q0; oi = cur;
+    } else {
+      if (o.x >= first_rogue) return;
+      NeighFrame Fo;
+      neigh_frame_exact(p, o, spos[q], Fo);
+      if (!neigh_exact(p, Fo, sinfo, spos, q0, &key)) return;
+      oq = q; oi = o.x;
+    }
+    const int s = atomicAdd(&row_cnt[oi], 1);
+    if (s < NSLOT) nslot[(size_t)oi * NSLOT + s] = key;
+    else if (s == NSLOT) {
+      const int t = atomicAdd(&long_rows[p0.n], 1);
+      if (t < p0.n) long_rows[t] = oq;
+    }
   };
+  int ns = 0;
   auto flush = [&]() {
     for (int s = 0; s < ns; ++s) exact(s_surv[s * blockDim.x + threadIdx.x]);
     ns = 0;
   };
-  const int nr = neigh_nruns(p, F);
-  for (int r = 0; r < nr; ++r) {
-    int qs, qe;
-    neigh_run(p, F, fstart, r, qs, qe);
-    for (int q = qs; q < qe; ++q) {
-      if (!neigh_pre(F, sposf, q)) continue;
-      s_surv[ns * blockDim.x + threadIdx.x] = q;
-      if (++ns == NSURV) flush();
+  const PreFrame G = pre_frame(F);
+  for_runs<true>(p, F, fstart, q0, me.w, [&](int qs, int qe) {
+    if (F.wrap) {
+      for (int q = qs; q < qe; ++q) {
+        if (!pre_test(G, sposf[q])) continue;
+        s_surv[ns * blockDim.x + threadIdx.x] = q;
+        if (++ns == NSURV) flush();
+      }
+    } else {
+      for (int q = qs; q < qe; ++q) {
+        if (!pre_direct(G, sposf[q])) continue;
+        s_surv[ns * blockDim.x + threadIdx.x] = q;
+        if (++ns == NSURV) flush();
+      }
+    }
+  });
+  flush();
+}
+
+// Fill pass of the rows the count pass kept whole (at most NSLOT
+// neighbours, in the order found), a thread per particle: each key goes to
+// the place given by the number of smaller keys (the keys of a row are
+// distinct), which is (rank, index) order.  Consecutive threads write
+// consecutive rows.
+template <bool B>
+__global__ void k_fill_kept(int n, BatchView bv, const int* __restrict__ row_cnt, int* __restrict__ row_se,
+                            int* __restrict__ nbrs, int* __restrict__ owner, const uint32_t* __restrict__ nslot,
+                            long long cap) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if constexpr (B) {
+    if (!bv.due[bv.sys_of[i]]) return;
+  }
+  const int kept = row_cnt[i];
+  if (kept == 0 || kept > NSLOT) return;
+  const long long start = min((long long)row_se[i], cap);
+  const uint32_t* slot = nslot + (size_t)i * NSLOT;
+  uint32_t k[NSLOT];
+#pragma unroll
+  for (int c = 0; c < NSLOT; ++c) k[c] = c < kept ? slot[c] : 0xffffffffu;
+#pragma unroll
+  for (int c = 0; c < NSLOT; ++c) {
+    if (c < kept) {
+      int r = 0;
+#pragma unroll
+      for (int d = 0; d < NSLOT; ++d) r += k[d] < k[c];
+      const long long s = start + r;
+      if (s < cap) { nbrs[s] = (int)(k[c] & 0x7ffffffu); owner[s] = i; }
     }
   }
-  flush();
-  if (FILL) row_se[cur] = (int)min((long long)start + cnt, cap);   // start -> end pointer
-  else row_cnt[cur] = cnt;
+  row_se[i] = (int)min(start + kept, cap);   // start -> end pointer
+}
+
+// Fill pass of the rows longer than NSLOT (the long-row list), a warp per
+// row: the lanes share out each run of the particle's candidates for a
+// full rescan, collect the row's keys in shared memory and write each key
+// at the place given by the number of smaller keys, which is (rank, index)
+// order.  A row of more than LONG_KCAP neighbours is written by one lane,
+// inserting each neighbour into the row kept sorted.  Warps stride over the
+// list.
+constexpr int LONG_KCAP = 128;
+template <bool B>
+__global__ void __launch_bounds__(128)
+k_fill_long(DevParams p0, BatchView bv, const double4* __restrict__ spos, const float4* __restrict__ sposf,
+            const int4* __restrict__ sinfo, const int* __restrict__ fstart, const int* __restrict__ row_cnt,
+            int* __restrict__ row_se, int* __restrict__ nbrs, uint8_t* __restrict__ rank_buf,
+            int* __restrict__ owner, const int* __restrict__ long_rows, long long cap) {
+  __shared__ uint32_t s_key[4][LONG_KCAP];
+  __shared__ int s_n[4];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nl = min(long_rows[p0.n], p0.n);
+  for (int t = blockIdx.x * 4 + w; t < nl; t += gridDim.x * 4) {
+    const int q0 = long_rows[t];
+    const int4 me = sinfo[q0];
+    const int cur = me.x;
+    const DevParams& p = sysp<B>(p0, bv, cur);
+    const long long start = min((long long)row_se[cur], cap);
+    NeighFrame F;
+    neigh_frame(p, me, spos[q0], F);
+    const PreFrame G = pre_frame(F);
+    if (row_cnt[cur] <= LONG_KCAP) {
+      if (lane == 0) s_n[w] = 0;
+      __syncwarp();
+      for_runs<false>(p, F, fstart, q0, me.w, [&](int qs, int qe) {
+        for (int q = qs + lane; q < qe; q += 32) {
+          uint32_t key;
+          if (!pre_test(G, sposf[q]) || !neigh_exact(p, F, sinfo, spos, q, &key)) continue;
+          const int c = atomicAdd(&s_n[w], 1);
+          if (c < LONG_KCAP) s_key[w][c] = key;
+        }
+      });
+      __syncwarp();
+      const int m = min(s_n[w], LONG_KCAP);
+      for (int c = lane; c < m; c += 32) {
+        const uint32_t kc = s_key[w][c];
+        int r = 0;
+        for (int d = 0; d < m; ++d) r += s_key[w][d] < kc;
+        const long long sl = start + r;
+        if (sl < cap) { nbrs[sl] = (int)(kc & 0x7ffffffu); owner[sl] = cur; }
+      }
+      if (lane == 0) row_se[cur] = (int)min(start + m, cap);   // start -> end pointer
+    } else if (lane == 0) {
+      int cnt = 0;
+      for_runs<false>(p, F, fstart, q0, me.w, [&](int qs, int qe) {
+        for (int q = qs; q < qe; ++q) {
+          uint32_t key;
+          if (!pre_test(G, sposf[q]) || !neigh_exact(p, F, sinfo, spos, q, &key)) continue;
+          const int rank = (int)(key >> 27), nb = (int)(key & 0x7ffffffu);
+          const long long sl = start + cnt;
+          if (sl < cap) {
+            long long b = sl - 1;
+            while (b >= start) {
+              const int rb = rank_buf[b];
+              if (rb < rank || (rb == rank && nbrs[b] < nb)) break;
+              nbrs[b + 1] = nbrs[b];
+              rank_buf[b + 1] = (uint8_t)rb;
+              --b;
+            }
+            nbrs[b + 1] = nb;
+            rank_buf[b + 1] = (uint8_t)rank;
+            owner[sl] = cur;
+          }
+          ++cnt;
+        }
+      });
+      row_se[cur] = (int)min(start + cnt, cap);   // start -> end pointer
+    }
+    __syncwarp();
+  }
 }
 
 // Rows of batch systems that do not rebuild now: the count pass takes the
@@ -610,17 +757,21 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
   return check_cuda(h, cudaGetLastError(), "grow pairs");
 }
 
-// Count pass of the pair build over the current cell-sorted copy (row_cnt).
+// Count pass of the pair build over the current cell-sorted copy: row_cnt
+// and the long-row list start from zero, so the pass can be launched again
+// on its own (the autotuner times it).
 void launch_neigh_count(dem_handle* h) {
   const int n = h->n, T = h->tune.neigh_threads, B = (n + T - 1) / T;
   const bool bt = h->batch();
   const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : h->dp.nfcell);
+  cudaMemsetAsync(h->row_cnt, 0, sizeof(int) * n, h->stream);
+  cudaMemsetAsync(h->long_rows + n, 0, sizeof(int), h->stream);
   if (bt)
-    k_neigh<false, true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start,
-                                                 h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, h->nslot, 0);
+    k_neigh_count<true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo,
+                                                h->fcell_start, h->derr, h->row_cnt, h->nslot, h->long_rows);
   else
-    k_neigh<false, false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start,
-                                                  h->derr, h->row_cnt, nullptr, nullptr, nullptr, nullptr, h->nslot, 0);
+    k_neigh_count<false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo,
+                                                 h->fcell_start, h->derr, h->row_cnt, h->nslot, h->long_rows);
   DEM_LAUNCH(h);
 }
 
@@ -647,7 +798,6 @@ int run_neighbour(dem_handle* h, bool carry_history) {
     k_sorted_copy<false><<<B, T, 0, h->stream>>>(p, bv, n, n_exist, h->fcell_list, h->pos4[h->cur], h->state,
                                                  h->dg_pijk, h->fcell_key, h->spos, h->sposf, h->sinfo);
   DEM_LAUNCH(h);
-  if (int rc = check_cuda(h, cudaMemsetAsync(h->row_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
   launch_neigh_count(h);
   if (bt) {
     k_keep_rows<false><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], h->row_cnt, nullptr,
@@ -666,18 +816,27 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   } else {
     h->np_stale = true;
   }
-  const int TN = h->tune.neigh_threads, BN = (n + TN - 1) / TN;
+  // rows kept whole by the count pass, then the long rows (a fixed grid
+  // striding over the list, whose length is on the device)
+  const int BL = 4 * 148;
   if (bt) {
-    k_neigh<true, true><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, e, h->row_cnt,
-                                                  h->row_end[nb], h->nbrs[nb], h->pflagb[1 - h->pcur], h->pair_owner, h->nslot,
-                                                  h->pair_cap);
+    k_fill_kept<true><<<B, T, 0, h->stream>>>(n, bv, h->row_cnt, h->row_end[nb], h->nbrs[nb], h->pair_owner,
+                                              h->nslot, h->pair_cap);
+    DEM_LAUNCH(h);
+    k_fill_long<true><<<BL, 128, 0, h->stream>>>(p, bv, h->spos, h->sposf, h->sinfo, h->fcell_start, h->row_cnt,
+                                                 h->row_end[nb],
+                                                 h->nbrs[nb], h->pflagb[1 - h->pcur], h->pair_owner, h->long_rows,
+                                                 h->pair_cap);
+    DEM_LAUNCH(h);
     k_keep_rows<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], nullptr, h->row_end[nb],
                                               h->nbrs[nb], h->pair_owner, h->pair_cap);
-    DEM_LAUNCH(h);
   } else {
-    k_neigh<true, false><<<BN, TN, 0, h->stream>>>(p, bv, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, e, h->row_cnt,
-                                                   h->row_end[nb], h->nbrs[nb], h->pflagb[1 - h->pcur], h->pair_owner, h->nslot,
-                                                   h->pair_cap);
+    k_fill_kept<false><<<B, T, 0, h->stream>>>(n, bv, h->row_cnt, h->row_end[nb], h->nbrs[nb], h->pair_owner,
+                                               h->nslot, h->pair_cap);
+    DEM_LAUNCH(h);
+    k_fill_long<false><<<BL, 128, 0, h->stream>>>(p, bv, h->spos, h->sposf, h->sinfo, h->fcell_start,
+                                                  h->row_cnt, h->row_end[nb], h->nbrs[nb], h->pflagb[1 - h->pcur], h->pair_owner,
+                                                  h->long_rows, h->pair_cap);
   }
   DEM_LAUNCH(h);
   k_clamp_np<<<1, 1, 0, h->stream>>>(h->d_np, h->pair_cap, e);
