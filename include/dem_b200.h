@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define DEM_ABI_VERSION 1
+#define DEM_ABI_VERSION 2
 
 /* Maximum number of DEM solids phases (MFiX DIM_M is 10; DEM cases use few). */
 #define DEM_MAX_PHASES 8
@@ -651,8 +651,22 @@ typedef struct dem_batch_limits {
     int32_t max_search_cells;  /* search-grid cells of all systems */
     int32_t max_facets;        /* wall facets of all systems */
     int32_t max_facet_bins;    /* facet-in-cell entries of all systems */
-    int32_t reserved[10];
+    int32_t pairs_per_particle;/* pair-list room reserved per particle (0: 6); the
+                                  list grows past it only when a build needs more */
+    int32_t reserved[9];
 } dem_batch_limits;
+
+/* Device memory of a handle (dem_memory_info) or of a batch handle before
+ * it is made (dem_batch_footprint).  No counterpart in the reference. */
+typedef struct dem_memory {
+    int64_t array_bytes;       /* the arrays sized by the particle, cell, facet and system
+                                  counts (state, histories, grids, work arrays, tables) */
+    int64_t pair_bytes;        /* the pair-list arrays at their capacity */
+    int64_t scratch_bytes;     /* scan and staging scratch held now (grows on demand) */
+    int64_t pair_capacity;     /* pairs the pair-list arrays hold */
+    int64_t pairs;             /* pairs of the current list */
+    int64_t reserved[3];
+} dem_memory;
 
 typedef struct dem_sys_status {
     int32_t capacity;          /* particles reserved for the system */
@@ -667,6 +681,14 @@ typedef struct dem_sys_status {
 /* Cell ranges a system with parameters p takes from a batch: DES-grid cells
  * (with its end entry) and search-grid cells.  Host only, no device. */
 int dem_params_cells(const dem_params* p, int32_t* des_cells, int32_t* search_cells);
+
+/* The device memory dem_batch_create allocates for `common` and `lim`
+ * (array_bytes + pair_bytes; scratch_bytes and pairs are 0).  Host only: it
+ * counts the same arrays, in the same sizes, that creation allocates. */
+int dem_batch_footprint(const dem_params* common, const dem_batch_limits* lim, dem_memory* out);
+/* The device memory a handle holds now (any handle).  For a single-system
+ * handle the wall, gas-field and boundary tables are not counted. */
+int dem_memory_info(dem_handle* h, dem_memory* out);
 
 /* Creates an empty batch handle on the current CUDA device.  `common` gives
  * the collision model, integrator, force precision and COLLISION_ARRAY_MAX

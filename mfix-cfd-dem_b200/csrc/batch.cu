@@ -147,6 +147,47 @@ static int total_facets(const dem_handle* h) {
       return set_err((h), DEM_ERR_ARG, "no such system in the batch");                    \
   } while (0)
 
+// The extent of the live systems' particle and search-cell ranges, which the
+// step kernels cover (ranges are taken first-fit from the low end, so the
+// extent follows what is running, not the capacity).
+static void update_extent(dem_handle* h) {
+  int np = 0, nf = 0;
+  for (const SysSlot& S : h->sys) {
+    if (!S.live) continue;
+    np = std::max(np, S.dp.p_end);
+    nf = std::max(nf, S.dp.fcell_off + S.dp.nfcell);
+  }
+  h->n_act = std::min(h->n, std::max(np, 64));
+  h->nfc_act = std::min(h->nfcell_total, std::max(nf, 1));
+}
+
+// The tables of a batch handle past handle_arrays, each given to
+// A(&pointer, bytes) as in handle_arrays.
+template <class F>
+static void batch_arrays(dem_handle* h, const dem_batch_limits* lim, F&& A) {
+  A((void**)&h->d_sys, sizeof(DevParams) * lim->max_systems);
+  A((void**)&h->sys_of, sizeof(uint16_t) * (size_t)lim->max_particles);
+  A((void**)&h->d_due, 3 * (size_t)lim->max_systems);
+  A((void**)&h->d_first_rogue, sizeof(int) * lim->max_systems);
+  A((void**)&h->vertex, sizeof(double) * 9 * (size_t)lim->max_facets);
+  A((void**)&h->norm_face, sizeof(double) * 3 * (size_t)lim->max_facets);
+  A((void**)&h->ignore_edge, (size_t)4 * lim->max_facets);
+  A((void**)&h->fbin, sizeof(FacetBinEntry) * (size_t)lim->max_facet_bins);
+}
+
+static bool limits_ok(const dem_params* q, const dem_batch_limits* lim) {
+  return lim->max_particles > 0 && lim->max_particles <= MAX_PARTICLES && lim->max_systems > 0 &&
+         lim->max_systems <= 65535 && lim->max_cells > 0 && lim->max_search_cells > 0 && lim->max_facets >= 0 &&
+         lim->max_facet_bins >= 0 && lim->pairs_per_particle >= 0 && q->n_phases >= 1 &&
+         q->n_phases <= DEM_MAX_PHASES && q->dtsolid > 0.0;
+}
+
+// Pair-list room a batch handle starts with.
+static long long batch_pair_reserve(const dem_batch_limits* lim) {
+  const long long per = lim->pairs_per_particle > 0 ? lim->pairs_per_particle : 6;
+  return per * (long long)lim->max_particles + 1024;
+}
+
 }  // namespace demb
 
 extern "C" {
@@ -161,12 +202,27 @@ int dem_params_cells(const dem_params* q, int32_t* des_cells, int32_t* search_ce
   return 0;
 }
 
+int dem_batch_footprint(const dem_params* q, const dem_batch_limits* lim, dem_memory* out) {
+  if (!q || !lim || !out) return DEM_ERR_ARG;
+  if (!limits_ok(q, lim)) return DEM_ERR_ARG;
+  dem_handle tmp;
+  tmp.prm = *q;
+  tmp.n = lim->max_particles;
+  fill_devparams(tmp.prm, tmp.n, tmp.dp);
+  long long bytes = 0;
+  auto S = [&](void**, size_t b) { bytes += (long long)(b > 0 ? b : 8); };
+  handle_arrays(&tmp, (size_t)tmp.n, (size_t)lim->max_cells, (size_t)lim->max_search_cells, S);
+  batch_arrays(&tmp, lim, S);
+  memset(out, 0, sizeof *out);
+  out->array_bytes = bytes;
+  out->pair_capacity = batch_pair_reserve(lim);
+  out->pair_bytes = pair_array_bytes(out->pair_capacity);
+  return 0;
+}
+
 int dem_batch_create(const dem_params* q, const dem_batch_limits* lim, dem_handle** out) {
   if (!q || !lim || !out) return DEM_ERR_ARG;
-  if (lim->max_particles <= 0 || lim->max_particles > MAX_PARTICLES || lim->max_systems <= 0 || lim->max_systems > 65535 || lim->max_cells <= 0 ||
-      lim->max_search_cells <= 0 || lim->max_facets < 0 || lim->max_facet_bins < 0)
-    return DEM_ERR_ARG;
-  if (q->n_phases < 1 || q->n_phases > DEM_MAX_PHASES || !(q->dtsolid > 0.0)) return DEM_ERR_ARG;
+  if (!limits_ok(q, lim)) return DEM_ERR_ARG;
   dem_handle* h = new dem_handle();
   h->prm = *q;
   h->n = lim->max_particles;
@@ -177,20 +233,14 @@ int dem_batch_create(const dem_params* q, const dem_batch_limits* lim, dem_handl
   h->nfcell_total = lim->max_search_cells;
   h->max_facets = lim->max_facets;
   h->max_bins = lim->max_facet_bins;
-  int rc = alloc_handle(h, lim->max_cells, lim->max_search_cells, 6 * (long long)h->n + 1024);
+  int rc = alloc_handle(h, lim->max_cells, lim->max_search_cells, batch_pair_reserve(lim));
   auto A = [&](void** p, size_t bytes) {
     if (rc) return;
     if (cudaMalloc(p, bytes > 0 ? bytes : 8) != cudaSuccess) rc = DEM_ERR_CUDA;
     else cudaMemset(*p, 0, bytes > 0 ? bytes : 8);
+    h->arr_bytes += (long long)(bytes > 0 ? bytes : 8);
   };
-  A((void**)&h->d_sys, sizeof(DevParams) * lim->max_systems);
-  A((void**)&h->sys_of, sizeof(uint16_t) * h->n);
-  A((void**)&h->d_due, 3 * (size_t)lim->max_systems);
-  A((void**)&h->d_first_rogue, sizeof(int) * lim->max_systems);
-  A((void**)&h->vertex, sizeof(double) * 9 * (size_t)lim->max_facets);
-  A((void**)&h->norm_face, sizeof(double) * 3 * (size_t)lim->max_facets);
-  A((void**)&h->ignore_edge, (size_t)4 * lim->max_facets);
-  A((void**)&h->fbin, sizeof(FacetBinEntry) * (size_t)lim->max_facet_bins);
+  batch_arrays(h, lim, A);
   if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = DEM_ERR_CUDA;
   if (rc) {
     dem_destroy(h);
@@ -210,6 +260,7 @@ int dem_batch_create(const dem_params* q, const dem_batch_limits* lim, dem_handl
   h->fcell_alloc.reset(lim->max_search_cells);
   h->fac_alloc.reset(lim->max_facets);
   h->bin_alloc.reset(lim->max_facet_bins);
+  update_extent(h);
   h->have_state = true;
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
     dem_destroy(h);
@@ -280,6 +331,7 @@ int dem_sys_add(dem_handle* h, const dem_params* q, int32_t max_pip, int32_t* sy
   cudaMemsetAsync(h->wall_pft + pb * cm * 3, 0, sizeof(double) * 3 * cm * n, h->stream);
   cudaMemsetAsync(h->fbin_start + cb, 0, sizeof(int) * (dp.ncell2 + 1), h->stream);
   if (int rc = upload_table(h, id)) return rc;
+  update_extent(h);
   invalidate_graphs(h);
   *sys = id;
   return check_cuda(h, cudaStreamSynchronize(h->stream), "add system");
@@ -300,6 +352,7 @@ int dem_sys_remove(dem_handle* h, int32_t s) {
   S.clean = false;
   if (int rc = upload_table(h, s)) return rc;
   h->nf = total_facets(h);
+  update_extent(h);
   invalidate_graphs(h);
   return check_cuda(h, cudaStreamSynchronize(h->stream), "remove system");
 }

@@ -418,52 +418,9 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
     if (!ok) return;
     if (cudaMalloc(p, bytes > 0 ? bytes : 8) != cudaSuccess) ok = false;
     else cudaMemset(*p, 0, bytes > 0 ? bytes : 8);
+    h->arr_bytes += (long long)(bytes > 0 ? bytes : 8);
   };
-  for (int b = 0; b < 2; ++b) {
-    A((void**)&h->pos4[b], sizeof(double4) * n);
-    A((void**)&h->vel4[b], sizeof(double4) * n);
-    A((void**)&h->omg4[b], sizeof(double4) * n);
-    A((void**)&h->row_end[b], sizeof(int) * n);
-  }
-  A((void**)&h->state, n);
-  A((void**)&h->phase, n);
-  A((void**)&h->fc, sizeof(double) * 3 * n);
-  A((void**)&h->tow, sizeof(double) * 3 * n);
-  A((void**)&h->acc_old, sizeof(double) * 3 * n);
-  A((void**)&h->rot_acc_old, sizeof(double) * 3 * n);
-  A((void**)&h->dg_pijk, sizeof(int) * n);
-  A((void**)&h->cell_cnt, sizeof(int) * (nc + 1));
-  A((void**)&h->cell_start, sizeof(int) * (nc + 1));
-  A((void**)&h->cell_fill, sizeof(int) * (nc + 1));
-  A((void**)&h->cell_list, sizeof(int) * n);
-  A((void**)&h->fcell_key, sizeof(int) * n);
-  A((void**)&h->fcell_cnt, sizeof(int) * (nfc + 1));
-  A((void**)&h->fcell_start, sizeof(int) * (nfc + 1));
-  A((void**)&h->fcell_list, sizeof(int) * n);
-  A((void**)&h->spos, sizeof(double4) * n);
-  A((void**)&h->sposf, sizeof(float4) * n);
-  A((void**)&h->sinfo, sizeof(int4) * n);
-  A((void**)&h->nslot, sizeof(uint32_t) * NSLOT * n);
-  A((void**)&h->long_rows, sizeof(int) * (n + 1));
-  A((void**)&h->row_cnt, sizeof(int) * n);
-  A((void**)&h->in_cnt, sizeof(int) * n);
-  A((void**)&h->in_start, sizeof(int) * (n + 1));
-  A((void**)&h->in_fill, sizeof(int) * n);
-  A((void**)&h->fbin_start, sizeof(int) * (nc + 1));
-  A((void**)&h->wall_fid, sizeof(int) * cmax * n);
-  A((void**)&h->wall_pft, sizeof(double) * 3 * cmax * n);
-  A((void**)&h->wall_live, n);
-  A((void**)&h->wf, sizeof(double) * 6 * n);
-  A((void**)&h->touched, n);
-  A((void**)&h->wall_hit, n);
-  A((void**)&h->wall_cand, n);
-  A((void**)&h->wall_list, sizeof(int) * (size_t)n);
-  A((void**)&h->wgap, sizeof(float) * (size_t)n);
-  A((void**)&h->d_nwall, sizeof(int));
-  A((void**)&h->skin, sizeof(double));
-  A((void**)&h->vslot, sizeof(unsigned) * 32);
-  A((void**)&h->derr, sizeof(DevErr));
-  A((void**)&h->d_np, sizeof(int));
+  handle_arrays(h, n, (size_t)nc, (size_t)nfc, A);
   if (!ok) return DEM_ERR_CUDA;
   cudaMemset(h->wall_fid, 0xff, sizeof(int) * cmax * n);  // -1 = free slot
   if (cudaMallocHost((void**)&h->herr, sizeof(DevErr)) != cudaSuccess) return DEM_ERR_CUDA;
@@ -491,6 +448,18 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
 extern "C" {
 
 int dem_abi_version(void) { return DEM_ABI_VERSION; }
+
+int dem_memory_info(dem_handle* h, dem_memory* out) {
+  API_GUARD(h);
+  if (!out) return DEM_ERR_ARG;
+  memset(out, 0, sizeof *out);
+  out->array_bytes = h->arr_bytes;
+  out->pair_capacity = h->pair_cap;
+  out->pair_bytes = pair_array_bytes(h->pair_cap);
+  out->scratch_bytes = (int64_t)(h->scan_tmp_elems * sizeof(int) + h->stage_bytes);
+  out->pairs = host_pairs(h);
+  return fetch_errors(h);
+}
 
 const char* dem_last_error(const dem_handle* h) { return h ? h->err.c_str() : "null handle"; }
 

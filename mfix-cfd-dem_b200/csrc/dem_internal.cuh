@@ -26,6 +26,8 @@
 
 namespace demb {
 
+// Neighbours per particle kept by the count pass of the pair build.
+constexpr int NSLOT = 16;
 constexpr double SMALL_NUMBER = 1.0e-15;       // param1_mod.f:26
 constexpr double UNDEFINED_D  = 9.87654321e31; // param1_mod.f:20
 constexpr int MAXP = DEM_MAX_PHASES;
@@ -170,7 +172,14 @@ struct dem_handle {
   const uint8_t* due_cur = nullptr;   // the mask the next kernels read
   int* d_first_rogue = nullptr;       // [system]
   int ncell_total = 0, nfcell_total = 0;
+  int n_act = 0, nfc_act = 0;         // extent of the live systems' particle and search-cell ranges
+  int n_built = 0;                    // the particle extent of the current pair list's build
   bool batch() const { return !sys.empty(); }
+  // The particles and search cells the step kernels cover: for a batch the
+  // extent of its live systems (the ranges past it belong to no system: no
+  // particle exists there and no cell is read), else all of them.
+  int nl() const { return batch() ? n_act : n; }
+  int nfl() const { return batch() ? nfc_act : dp.nfcell; }
   demb::BatchView bview() const { return demb::BatchView{d_sys, sys_of, due_cur, d_first_rogue}; }
   int dev = 0;
   cudaStream_t stream = 0;
@@ -212,6 +221,7 @@ struct dem_handle {
 
   // pairs
   long long pair_cap = 0;
+  long long arr_bytes = 0;    // device bytes of the arrays sized by the counts (handle_arrays and the batch tables)
   long long n_pairs = 0;      // host copy of the pair count (valid when !np_stale)
   bool np_stale = false;      // the last build ran without reading the count back
   int* d_np = nullptr;        // device pair count (persistent pair kernels read it)
@@ -356,6 +366,61 @@ void launch_gather_only(dem_handle* h);        // force.cu: gather kernel, force
 void fill_devparams(const dem_params& q, int n, DevParams& p);
 bool des_grid_ok(const dem_params& q);
 int alloc_handle(dem_handle* h, int nc, int nfc, long long pairs);
+// Device bytes of the pair-list arrays for cap pairs (ensure_pair_capacity).
+long long pair_array_bytes(long long cap);
+
+// The arrays of a handle for n particles, nc DES cells and nfc search cells
+// (COLLISION_ARRAY_MAX from h->dp), each given to A(&pointer, bytes): the
+// allocation list of alloc_handle, and what dem_batch_footprint counts.
+template <class F>
+void handle_arrays(dem_handle* h, size_t n, size_t nc, size_t nfc, F&& A) {
+  const size_t cmax = (size_t)h->dp.cmax;
+  for (int b = 0; b < 2; ++b) {
+    A((void**)&h->pos4[b], sizeof(double4) * n);
+    A((void**)&h->vel4[b], sizeof(double4) * n);
+    A((void**)&h->omg4[b], sizeof(double4) * n);
+    A((void**)&h->row_end[b], sizeof(int) * n);
+  }
+  A((void**)&h->state, n);
+  A((void**)&h->phase, n);
+  A((void**)&h->fc, sizeof(double) * 3 * n);
+  A((void**)&h->tow, sizeof(double) * 3 * n);
+  A((void**)&h->acc_old, sizeof(double) * 3 * n);
+  A((void**)&h->rot_acc_old, sizeof(double) * 3 * n);
+  A((void**)&h->dg_pijk, sizeof(int) * n);
+  A((void**)&h->cell_cnt, sizeof(int) * (nc + 1));
+  A((void**)&h->cell_start, sizeof(int) * (nc + 1));
+  A((void**)&h->cell_fill, sizeof(int) * (nc + 1));
+  A((void**)&h->cell_list, sizeof(int) * n);
+  A((void**)&h->fcell_key, sizeof(int) * n);
+  A((void**)&h->fcell_cnt, sizeof(int) * (nfc + 1));
+  A((void**)&h->fcell_start, sizeof(int) * (nfc + 1));
+  A((void**)&h->fcell_list, sizeof(int) * n);
+  A((void**)&h->spos, sizeof(double4) * n);
+  A((void**)&h->sposf, sizeof(float4) * n);
+  A((void**)&h->sinfo, sizeof(int4) * n);
+  A((void**)&h->nslot, sizeof(uint32_t) * NSLOT * n);
+  A((void**)&h->long_rows, sizeof(int) * (n + 1));
+  A((void**)&h->row_cnt, sizeof(int) * n);
+  A((void**)&h->in_cnt, sizeof(int) * n);
+  A((void**)&h->in_start, sizeof(int) * (n + 1));
+  A((void**)&h->in_fill, sizeof(int) * n);
+  A((void**)&h->fbin_start, sizeof(int) * (nc + 1));
+  A((void**)&h->wall_fid, sizeof(int) * cmax * n);
+  A((void**)&h->wall_pft, sizeof(double) * 3 * cmax * n);
+  A((void**)&h->wall_live, n);
+  A((void**)&h->wf, sizeof(double) * 6 * n);
+  A((void**)&h->touched, n);
+  A((void**)&h->wall_hit, n);
+  A((void**)&h->wall_cand, n);
+  A((void**)&h->wall_list, sizeof(int) * n);
+  A((void**)&h->wgap, sizeof(float) * n);
+  A((void**)&h->d_nwall, sizeof(int));
+  A((void**)&h->skin, sizeof(double));
+  A((void**)&h->vslot, sizeof(unsigned) * 32);
+  A((void**)&h->derr, sizeof(DevErr));
+  A((void**)&h->d_np, sizeof(int));
+}
 int upload_range(dem_handle* h, int off, int cnt, int nph, const double* pos, const double* vel,
                  const double* omega, const double* radius, const double* pmass, const double* omoi,
                  const int8_t* state, const int32_t* phase);
@@ -424,8 +489,6 @@ constexpr long long MAX_GRID_CELLS = 1LL << 28;
 // Cells of the search grid of one system when it is finer than its DES grid.
 constexpr long long SEARCH_CELLS_CAP = 1LL << 22;
 
-// Neighbours per particle kept by the count pass of the pair build.
-constexpr int NSLOT = 16;
 constexpr int MAX_PARTICLES = (1 << 27) - 1;  // particle index in 27 bits of a kept key
 
 __device__ __forceinline__ int dg_ofpos(const DevParams& p, int ax, double x, int start1) {

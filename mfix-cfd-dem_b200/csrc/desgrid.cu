@@ -58,7 +58,7 @@ __global__ void k_wall_cand(DevParams p0, BatchView bv, const int8_t* __restrict
 }
 
 void launch_wall_cand(dem_handle* h) {
-  const int T = 256, B = (h->n + T - 1) / T;
+  const int T = 256, B = (h->nl() + T - 1) / T;
   if (h->batch())
     k_wall_cand<true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), h->state, h->dg_pijk, h->fbin_start, h->wall_cand);
   else
@@ -110,10 +110,14 @@ __global__ void k_fine_scatter(int n, const int8_t* __restrict__ state, const in
 int run_desgrid_pic(dem_handle* h, bool bin_search) {
   ProfScope ps(h, DEM_PROF_DESGRID);
   const DevParams& p = h->dp;
-  const int n = h->n, T = 256, B = (n + T - 1) / T;
+  const int n = h->nl(), T = 256, B = (n + T - 1) / T;
   const bool bt = h->batch();
   const BatchView bv = h->bview();
-  const int nfc = bt ? h->nfcell_total : p.nfcell;
+  // the live systems' cells (one more, empty, ends the last range); the
+  // count of binned particles also goes to the end of the cell arrays,
+  // where the pair build reads it
+  const int nfc = h->nfl() + 1;
+  int* n_binned = h->fcell_start + (bt ? h->nfcell_total : p.nfcell);
   if (bt)
     k_cell_keys<true><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->dg_pijk, h->fbin_start,
                                               h->wall_cand, h->wgap);
@@ -128,7 +132,7 @@ int run_desgrid_pic(dem_handle* h, bool bin_search) {
   if (bt) k_fine_keys<true><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->fcell_key, h->fcell_cnt);
   else k_fine_keys<false><<<B, T, 0, h->stream>>>(p, bv, h->pos4[h->cur], h->state, h->fcell_key, h->fcell_cnt);
   DEM_LAUNCH(h);
-  if (int rc = exclusive_scan(h, h->fcell_cnt, h->fcell_start, nfc, h->fcell_start + nfc)) return rc;
+  if (int rc = exclusive_scan(h, h->fcell_cnt, h->fcell_start, nfc, n_binned)) return rc;
   if (int rc = check_cuda(h, cudaMemsetAsync(h->fcell_cnt, 0, sizeof(int) * nfc, h->stream), "memset")) return rc;
   k_fine_scatter<<<B, T, 0, h->stream>>>(n, h->state, h->fcell_key, h->fcell_start, h->fcell_cnt, h->fcell_list);
   DEM_LAUNCH(h);

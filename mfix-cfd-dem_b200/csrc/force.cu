@@ -830,9 +830,9 @@ static void launch_walls_t(dem_handle* h) {
   const int c = h->cur;
   const int T = 128;
   cudaMemsetAsync(h->d_nwall, 0, sizeof(int), h->stream);
-  const int nq = (h->n + 3) / 4;  // four particles per thread
+  const int nq = (h->nl() + 3) / 4;  // four particles per thread
   k_wall_list<<<(nq + WALL_LIST_T - 1) / WALL_LIST_T, WALL_LIST_T, 0, h->stream>>>(
-      h->n, h->state, h->wall_cand, h->wall_live, h->wgap, h->skin, h->wall_list, h->d_nwall);
+      h->nl(), h->state, h->wall_cand, h->wall_live, h->wgap, h->skin, h->wall_list, h->d_nwall);
   // persistent: the resident blocks of the kernel's register budget
   k_walls<COLL, B><<<h->n_sm * 4, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->wall_list, h->d_nwall,
                                                      h->pos4[c], h->vel4[c], h->omg4[c], h->phase, h->wall_live,
@@ -852,7 +852,7 @@ static void launch_pairs_t(dem_handle* h) {
 
 template <int MODE, bool B>
 static void launch_gather_t(dem_handle* h) {
-  const int T = h->tune.gather_threads, G = (h->n + T - 1) / T;
+  const int T = h->tune.gather_threads, G = (h->nl() + T - 1) / T;
   const int c = h->cur;
   k_gather<MODE, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c],
                                             h->vel4[1 - c], h->omg4[1 - c], h->state, h->wf, h->row_end[h->rb], h->in_start, h->in_pair, h->pflag(),
@@ -863,7 +863,7 @@ static void launch_gather_t(dem_handle* h) {
 
 void launch_wall_gaps(dem_handle* h) {
   if (h->nf <= 0) return;
-  const int T = 256, G = (h->n + T - 1) / T;
+  const int T = 256, G = (h->nl() + T - 1) / T;
   if (h->batch())
     k_wall_gaps<true><<<G, T, 0, h->stream>>>(h->dp, h->bview(), wall_ctx(h), h->pos4[h->cur], h->state,
                                               h->wall_cand, h->wgap);
@@ -1015,7 +1015,7 @@ int run_split_force_error(dem_handle* h, double* rel_err) {
 
 template <int INTG, bool B>
 static void launch_integrate_t(dem_handle* h) {
-  const int T = 256, G = (h->n + T - 1) / T;
+  const int T = 256, G = (h->nl() + T - 1) / T;
   const int c = h->cur;
   k_integrate<INTG, B><<<G, T, 0, h->stream>>>(h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->state,
                                                h->fc, h->tow, h->acc_old, h->rot_acc_old, h->vslot);

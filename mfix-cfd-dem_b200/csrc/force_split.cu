@@ -381,7 +381,7 @@ void launch_pairs_split(dem_handle* h) {
 
 template <int MODE, bool B>
 static void launch_gather_split_t(dem_handle* h) {
-  const int T = h->tune.gather_threads, G = (h->n + T - 1) / T;
+  const int T = h->tune.gather_threads, G = (h->nl() + T - 1) / T;
   const int c = h->cur;
   k_gather_split<MODE, B><<<G, T, 0, h->stream>>>(
       h->dp, h->bview(), h->pos4[c], h->vel4[c], h->omg4[c], h->pos4[1 - c], h->vel4[1 - c], h->omg4[1 - c],

@@ -251,6 +251,31 @@ __device__ __forceinline__ void for_runs(const DevParams& p, const NeighFrame& F
   }
 }
 
+// The runs of for_runs<false> by number, for scans that share them out:
+// their count, and run r (column r / rpc of the range in (k, i) order, y
+// segment r % rpc).
+__device__ __forceinline__ int runs_per_col(const DevParams& p, const NeighFrame& F) {
+  return (p.per[1] && (F.glo[1] < 1 || F.ghi[1] > p.fn[1])) ? 2 : 1;
+}
+__device__ __forceinline__ int run_count(const DevParams& p, const NeighFrame& F) {
+  return (F.ghi[2] - F.glo[2] + 1) * (F.ghi[0] - F.glo[0] + 1) * runs_per_col(p, F);
+}
+__device__ __forceinline__ void run_at(const DevParams& p, const NeighFrame& F, const int* __restrict__ fstart,
+                                       int r, int& qs, int& qe) {
+  const int rpc = runs_per_col(p, F);
+  const int col = r / rpc, sub = r % rpc;
+  const int ni = F.ghi[0] - F.glo[0] + 1;
+  const int gk = F.glo[2] + col / ni, gi = F.glo[0] + col % ni;
+  const int base = p.fcell_off + search_wrap(p, gk, 2) * p.fc2 + search_wrap(p, gi, 0) * p.fc1;
+  int lo = F.glo[1], hi = F.ghi[1];
+  if (rpc == 2) {
+    if (F.glo[1] < 1) { if (sub == 0) { lo = F.glo[1] + p.fn[1]; hi = p.fn[1]; } else { lo = 1; hi = F.ghi[1]; } }
+    else { if (sub == 0) { lo = F.glo[1]; hi = p.fn[1]; } else { lo = 1; hi = F.ghi[1] - p.fn[1]; } }
+  }
+  qs = fstart[base + lo];
+  qe = fstart[base + hi + 1];
+}
+
 // The FP32 part of a frame as three float4: a = the particle's position
 // and radius, b = (FACTOR_RLM, allowance, period x, period y), c = (period
 // z, 1/period x, y, z); 0 for an axis that is not periodic.
@@ -361,7 +386,7 @@ constexpr int NSURV = 24;  // pre-checked candidates buffered per thread
 // long exact path runs with every lane holding work instead of one lane at
 // a time inside the candidate scan.
 template <bool B>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 8)
 k_neigh_count(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
               const float4* __restrict__ sposf, const int4* __restrict__ sinfo, const int* __restrict__ fstart,
               const DevErr* __restrict__ err, int* __restrict__ row_cnt, uint32_t* __restrict__ nslot,
@@ -428,6 +453,26 @@ k_neigh_count(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const
   flush();
 }
 
+// Writes the kept <= R keys of slot at start + (number of smaller keys),
+// the keys held in registers.
+template <int R>
+__device__ __forceinline__ void place_keys(const uint32_t* __restrict__ slot, int kept, long long start,
+                                           long long cap, int i, int* __restrict__ nbrs, int* __restrict__ owner) {
+  uint32_t k[R];
+#pragma unroll
+  for (int c = 0; c < R; ++c) k[c] = c < kept ? slot[c] : 0xffffffffu;
+#pragma unroll
+  for (int c = 0; c < R; ++c) {
+    if (c < kept) {
+      int r = 0;
+#pragma unroll
+      for (int d = 0; d < R; ++d) r += k[d] < k[c];
+      const long long s = start + r;
+      if (s < cap) { nbrs[s] = (int)(k[c] & 0x7ffffffu); owner[s] = i; }
+    }
+  }
+}
+
 // Fill pass of the rows the count pass kept whole (at most NSLOT
 // neighbours, in the order found), a thread per particle: each key goes to
 // the place given by the number of smaller keys (the keys of a row are
@@ -446,25 +491,14 @@ __global__ void k_fill_kept(int n, BatchView bv, const int* __restrict__ row_cnt
   if (kept == 0 || kept > NSLOT) return;
   const long long start = min((long long)row_se[i], cap);
   const uint32_t* slot = nslot + (size_t)i * NSLOT;
-  uint32_t k[NSLOT];
-#pragma unroll
-  for (int c = 0; c < NSLOT; ++c) k[c] = c < kept ? slot[c] : 0xffffffffu;
-#pragma unroll
-  for (int c = 0; c < NSLOT; ++c) {
-    if (c < kept) {
-      int r = 0;
-#pragma unroll
-      for (int d = 0; d < NSLOT; ++d) r += k[d] < k[c];
-      const long long s = start + r;
-      if (s < cap) { nbrs[s] = (int)(k[c] & 0x7ffffffu); owner[s] = i; }
-    }
-  }
+  if (kept <= NSLOT / 2) place_keys<NSLOT / 2>(slot, kept, start, cap, i, nbrs, owner);
+  else place_keys<NSLOT>(slot, kept, start, cap, i, nbrs, owner);
   row_se[i] = (int)min(start + kept, cap);   // start -> end pointer
 }
 
 // Fill pass of the rows longer than NSLOT (the long-row list), a warp per
-// row: the lanes share out each run of the particle's candidates for a
-// full rescan, collect the row's keys in shared memory and write each key
+// row: the lanes share out the runs of the particle's candidates (a run per
+// lane) for a full rescan, collect the row's keys in shared memory and write each key
 // at the place given by the number of smaller keys, which is (rank, index)
 // order.  A row of more than LONG_KCAP neighbours is written by one lane,
 // inserting each neighbour into the row kept sorted.  Warps stride over the
@@ -492,14 +526,17 @@ k_fill_long(DevParams p0, BatchView bv, const double4* __restrict__ spos, const 
     if (row_cnt[cur] <= LONG_KCAP) {
       if (lane == 0) s_n[w] = 0;
       __syncwarp();
-      for_runs<false>(p, F, fstart, q0, me.w, [&](int qs, int qe) {
-        for (int q = qs + lane; q < qe; q += 32) {
+      const int nr = run_count(p, F);
+      for (int r = lane; r < nr; r += 32) {
+        int qs, qe;
+        run_at(p, F, fstart, r, qs, qe);
+        for (int q = qs; q < qe; ++q) {
           uint32_t key;
           if (!pre_test(G, sposf[q]) || !neigh_exact(p, F, sinfo, spos, q, &key)) continue;
           const int c = atomicAdd(&s_n[w], 1);
           if (c < LONG_KCAP) s_key[w][c] = key;
         }
-      });
+      }
       __syncwarp();
       const int m = min(s_n[w], LONG_KCAP);
       for (int c = lane; c < m; c += 32) {
@@ -541,13 +578,16 @@ k_fill_long(DevParams p0, BatchView bv, const double4* __restrict__ spos, const 
 }
 
 // Rows of batch systems that do not rebuild now: the count pass takes the
-// length of the particle's current row, the fill pass copies the row.
+// length of the particle's current row, the fill pass copies the row.  The
+// current rows end at n_old, the extent of the build that made them: a
+// particle past it has none (a system placed there since is built now, and
+// the slots between systems' ranges belong to none).
 template <bool FILL>
-__global__ void k_keep_rows(int n, BatchView bv, const int* __restrict__ old_end, const int* __restrict__ old_nbrs,
-                            int* __restrict__ row_cnt, int* __restrict__ row_se, int* __restrict__ nbrs,
-                            int* __restrict__ owner, long long cap) {
+__global__ void k_keep_rows(int n, int n_old, BatchView bv, const int* __restrict__ old_end,
+                            const int* __restrict__ old_nbrs, int* __restrict__ row_cnt, int* __restrict__ row_se,
+                            int* __restrict__ nbrs, int* __restrict__ owner, long long cap) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || bv.due[bv.sys_of[i]]) return;
+  if (i >= n || i >= n_old || bv.due[bv.sys_of[i]]) return;
   const int s = i ? old_end[i - 1] : 0, e = old_end[i];
   if (!FILL) { row_cnt[i] = e - s; return; }
   const long long start = row_se[i];
@@ -559,31 +599,32 @@ __global__ void k_keep_rows(int n, BatchView bv, const int* __restrict__ old_end
 }
 
 // neighbour.f:77-117: history of each new pair from the same neighbour id in
-// the particle's previous row, zero when the pair is new.  A batch system
-// built for the first time (due = 2) takes no history from its region.
+// the owner's previous row, zero when the pair is new.  A thread per pair of
+// the new list (its owner from pair_owner); a batch system built for the
+// first time (due = 2) takes no history from its region.
 template <bool B>
-__global__ void k_remap(int n, BatchView bv, const int* __restrict__ row_end, const int* __restrict__ nbrs,
-                        const int* __restrict__ old_end, const int* __restrict__ old_nbrs,
-                        const double* __restrict__ old_pft, double* __restrict__ pft, uint8_t* __restrict__ pflag,
-                        int have_old) {
-  const int ll = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ll >= n) return;
-  if constexpr (B) {
-    if (bv.due[bv.sys_of[ll]] == 2) have_old = 0;
-  }
-  const int s = ll ? row_end[ll - 1] : 0, e = row_end[ll];
-  int so = 0, eo = 0;
-  if (have_old) { so = ll ? old_end[ll - 1] : 0; eo = old_end[ll]; }
-  for (int cc = s; cc < e; ++cc) {
-    const int nb = nbrs[cc];
+__global__ void k_remap(const int* __restrict__ d_np, BatchView bv, const int* __restrict__ nbrs,
+                        const int* __restrict__ owner, const int* __restrict__ old_end,
+                        const int* __restrict__ old_nbrs, const double* __restrict__ old_pft,
+                        double* __restrict__ pft, uint8_t* __restrict__ pflag, int have_old) {
+  const long long np = *d_np, stride = (long long)gridDim.x * blockDim.x;
+  for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
+    const int ll = owner[cc], nb = nbrs[cc];
+    bool carry = have_old != 0;
+    if constexpr (B) {
+      if (bv.due[bv.sys_of[ll]] == 2) carry = false;
+    }
     double a = 0.0, b = 0.0, c = 0.0;
-    for (int co = so; co < eo; ++co) {
-      if (old_nbrs[co] == nb) {
-        a = old_pft[3 * (size_t)co]; b = old_pft[3 * (size_t)co + 1]; c = old_pft[3 * (size_t)co + 2];
-        break;
+    if (carry) {
+      const int so = ll ? old_end[ll - 1] : 0, eo = old_end[ll];
+      for (int co = so; co < eo; ++co) {
+        if (old_nbrs[co] == nb) {
+          a = old_pft[3 * (size_t)co]; b = old_pft[3 * (size_t)co + 1]; c = old_pft[3 * (size_t)co + 2];
+          break;
+        }
       }
     }
-    pft[3 * (size_t)cc] = a; pft[3 * (size_t)cc + 1] = b; pft[3 * (size_t)cc + 2] = c;
+    pft[3 * cc] = a; pft[3 * cc + 1] = b; pft[3 * cc + 2] = c;
     pflag[cc] = (a != 0.0 || b != 0.0 || c != 0.0) ? PF_HIST : 0;
   }
 }
@@ -682,7 +723,27 @@ __global__ void k_in_sort(int n, const int* __restrict__ in_start, int2* __restr
                           int* __restrict__ in_pos, uint8_t* __restrict__ in_flag) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
-  int s = in_start[j], e = in_start[j + 1];
+  const int s = in_start[j], e = in_start[j + 1], m = e - s;
+  constexpr int R = 16;  // lists up to R long are sorted in registers
+  if (m <= R) {
+    // each entry goes to the place given by the number of smaller pair
+    // indices (distinct within a list)
+    int2 v[R];
+#pragma unroll
+    for (int c = 0; c < R; ++c) v[c] = c < m ? in_pair[s + c] : make_int2(0, 0x7fffffff);
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      if (c < m) {
+        int r = 0;
+#pragma unroll
+        for (int d = 0; d < R; ++d) r += v[d].y < v[c].y;
+        in_pair[s + r] = v[c];
+        in_pos[v[c].y] = s + r;
+        in_flag[s + r] = 0;
+      }
+    }
+    return;
+  }
   for (int a = s + 1; a < e; ++a) {
     int2 v = in_pair[a];
     int b = a - 1;
@@ -698,7 +759,7 @@ __global__ void k_in_sort(int n, const int* __restrict__ in_start, int2* __restr
 // Transpose of the current list (buffer nb, pair count in d_np): incoming
 // pairs of every particle in ascending owner order.
 int build_transpose(dem_handle* h, int nb) {
-  const int n = h->n;
+  const int n = h->nl();
   const int T = 256, B = (n + T - 1) / T;
   const unsigned BP = pair_grid(h, T);
   if (int rc = check_cuda(h, cudaMemsetAsync(h->in_cnt, 0, sizeof(int) * n, h->stream), "memset")) return rc;
@@ -713,9 +774,18 @@ int build_transpose(dem_handle* h, int nb) {
   return check_cuda(h, cudaGetLastError(), "transpose");
 }
 
+long long pair_array_bytes(long long cap) {
+  // nbrs, pft and pflag double-buffered; in_pair, pair_owner, the contact
+  // records, gaps, in_pos and in_flag (the flag arrays padded by 16 bytes)
+  return 2 * ((long long)sizeof(int) * cap + (long long)sizeof(double) * 3 * cap + cap + 16) +
+         (long long)(sizeof(int2) + sizeof(int) + sizeof(PairRec) + sizeof(float) + sizeof(int)) * cap + cap + 16;
+}
+
+// Pair-list arrays for at least `need` pairs: the first allocation takes
+// exactly `need`, a later one doubles the capacity until it fits.
 int ensure_pair_capacity(dem_handle* h, long long need) {
   if (need <= h->pair_cap) return 0;
-  long long cap = h->pair_cap > 0 ? h->pair_cap : 1024;
+  long long cap = h->pair_cap > 0 ? h->pair_cap : need;
   while (cap < need) cap *= 2;
   const long long old = h->pair_cap;  // the whole old allocation (the count may be stale)
   int* nb[2]; double* pf[2]; int2* inp; int* own; uint8_t* pfl[2]; PairRec* prc; float* gap;
@@ -761,11 +831,11 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
 // and the long-row list start from zero, so the pass can be launched again
 // on its own (the autotuner times it).
 void launch_neigh_count(dem_handle* h) {
-  const int n = h->n, T = h->tune.neigh_threads, B = (n + T - 1) / T;
+  const int n = h->nl(), T = h->tune.neigh_threads, B = (n + T - 1) / T;
   const bool bt = h->batch();
   const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : h->dp.nfcell);
   cudaMemsetAsync(h->row_cnt, 0, sizeof(int) * n, h->stream);
-  cudaMemsetAsync(h->long_rows + n, 0, sizeof(int), h->stream);
+  cudaMemsetAsync(h->long_rows + h->n, 0, sizeof(int), h->stream);  // the count, at [capacity]
   if (bt)
     k_neigh_count<true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo,
                                                 h->fcell_start, h->derr, h->row_cnt, h->nslot, h->long_rows);
@@ -778,7 +848,7 @@ void launch_neigh_count(dem_handle* h) {
 int run_neighbour(dem_handle* h, bool carry_history) {
   ProfScope ps(h, DEM_PROF_NEIGHBOR);
   const DevParams& p = h->dp;
-  const int n = h->n, T = 128, B = (n + T - 1) / T;
+  const int n = h->nl(), T = 128, B = (n + T - 1) / T;
   const bool bt = h->batch();
   const BatchView bv = h->bview();
   DevErr* e = h->derr;
@@ -800,7 +870,7 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   DEM_LAUNCH(h);
   launch_neigh_count(h);
   if (bt) {
-    k_keep_rows<false><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], h->row_cnt, nullptr,
+    k_keep_rows<false><<<B, T, 0, h->stream>>>(n, h->n_built, bv, h->row_end[h->rb], h->nbrs[h->rb], h->row_cnt, nullptr,
                                                nullptr, nullptr, 0);
     DEM_LAUNCH(h);
   }
@@ -828,7 +898,7 @@ int run_neighbour(dem_handle* h, bool carry_history) {
                                                  h->nbrs[nb], h->pflagb[1 - h->pcur], h->pair_owner, h->long_rows,
                                                  h->pair_cap);
     DEM_LAUNCH(h);
-    k_keep_rows<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[h->rb], h->nbrs[h->rb], nullptr, h->row_end[nb],
+    k_keep_rows<true><<<B, T, 0, h->stream>>>(n, h->n_built, bv, h->row_end[h->rb], h->nbrs[h->rb], nullptr, h->row_end[nb],
                                               h->nbrs[nb], h->pair_owner, h->pair_cap);
   } else {
     k_fill_kept<false><<<B, T, 0, h->stream>>>(n, bv, h->row_cnt, h->row_end[nb], h->nbrs[nb], h->pair_owner,
@@ -852,13 +922,16 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   const int pn = 1 - h->pcur;
   const int have_old = (carry_history && h->have_pairs) ? 1 : 0;
   if (bt)
-    k_remap<true><<<B, T, 0, h->stream>>>(n, bv, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
-                                          h->pft[h->pcur], h->pft[pn], h->pflagb[pn], have_old);
+    k_remap<true><<<pair_grid(h, 256), 256, 0, h->stream>>>(h->d_np, bv, h->nbrs[nb], h->pair_owner,
+                                                            h->row_end[h->rb], h->nbrs[h->rb], h->pft[h->pcur],
+                                                            h->pft[pn], h->pflagb[pn], have_old);
   else
-    k_remap<false><<<B, T, 0, h->stream>>>(n, bv, h->row_end[nb], h->nbrs[nb], h->row_end[h->rb], h->nbrs[h->rb],
-                                           h->pft[h->pcur], h->pft[pn], h->pflagb[pn], have_old);
+    k_remap<false><<<pair_grid(h, 256), 256, 0, h->stream>>>(h->d_np, bv, h->nbrs[nb], h->pair_owner,
+                                                             h->row_end[h->rb], h->nbrs[h->rb], h->pft[h->pcur],
+                                                             h->pft[pn], h->pflagb[pn], have_old);
   DEM_LAUNCH(h);
   h->rb = nb;
+  h->n_built = n;
   h->pcur = pn;
   h->have_pairs = true;
   launch_pair_gaps(h);

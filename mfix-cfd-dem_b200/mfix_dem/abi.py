@@ -6,7 +6,7 @@ round-trip of dem_params.
 """
 import ctypes as C
 
-DEM_ABI_VERSION = 1
+DEM_ABI_VERSION = 2
 DEM_MAX_PHASES = 8
 
 DEM_COLL_LSD = 0
@@ -171,8 +171,23 @@ class DemBatchLimits(C.Structure):
         ("max_search_cells", C.c_int32),
         ("max_facets", C.c_int32),
         ("max_facet_bins", C.c_int32),
-        ("reserved", C.c_int32 * 10),
+        ("pairs_per_particle", C.c_int32),
+        ("reserved", C.c_int32 * 9),
     ]
+
+
+class DemMemory(C.Structure):
+    _fields_ = [
+        ("array_bytes", C.c_int64),
+        ("pair_bytes", C.c_int64),
+        ("scratch_bytes", C.c_int64),
+        ("pair_capacity", C.c_int64),
+        ("pairs", C.c_int64),
+        ("reserved", C.c_int64 * 3),
+    ]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
 
 
 class DemSysStatus(C.Structure):
@@ -337,6 +352,8 @@ DEM_ONLY = {
     "sys_download_state": (C.c_int, [_P, C.c_int32, _D, _D, _D, _I8, C.c_int32]),
     "sys_start": (C.c_int, [_P, _I32, C.c_int32]),
     "batch_step": (C.c_int, [_P, C.c_int32]),
+    "batch_footprint": (C.c_int, [C.POINTER(DemParams), C.POINTER(DemBatchLimits), C.POINTER(DemMemory)]),
+    "memory_info": (C.c_int, [_P, C.POINTER(DemMemory)]),
     # particle output
     "write_vtp": (C.c_int, [_P, C.c_char_p, C.POINTER(DemVtpOptions), C.POINTER(C.c_int64)]),
     "vtp_write": (C.c_int, [C.c_char_p, C.POINTER(DemVtpOptions), C.c_int32, _D, _D, _D, _D, _I8, _I32,

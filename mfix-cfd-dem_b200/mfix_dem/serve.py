@@ -1,13 +1,18 @@
 """Serving DEM cases with continuous batching (no counterpart in the
 reference, which runs one case per process).
 
-`DemServer` keeps one batch handle resident on the device.  Requests arrive
-over time; each is built on the host (in worker threads), admitted into the
-batch as soon as its HBM footprint fits -- its particle, cell, facet and bin
-ranges are reserved from the batch limits, which are sized from the HBM
-budget -- and then steps with everything else already running.  Admission
-and retirement happen between chunks of NEIGHBOR_SEARCH_N steps; a finished
-case is downloaded and removed, and its ranges go to the next arrivals.
+`DemServer` keeps one batch handle resident on the device.  Its limits are
+sized from the HBM budget with the library's own count of the arrays a
+batch allocates (dem_batch_footprint): cell, facet and bin ranges for
+`max_systems` cases of the template's box, pair-list room of
+`pairs_per_particle` per particle, and the rest of the budget to particles.
+Requests arrive over time; each is built on the host (in worker threads),
+admitted into the batch as soon as its footprint fits -- its particle, cell,
+facet and bin ranges are taken from the free ranges of the limits, and the
+pairs of the running cases plus its own estimate fit the pair-list room --
+and then steps with everything else already running.  Admission and
+retirement happen between chunks of NEIGHBOR_SEARCH_N steps; a finished case
+is downloaded and removed, and its ranges go to the next arrivals.
 Because every system of a batch keeps its own step numbering and rebuild
 cadence, a case's result does not depend on what else was running
 (tests/test_gpu_serve.py checks it against the case served alone).
@@ -28,12 +33,47 @@ from . import abi
 from . import params as P
 from .system import BatchSystem, DemError
 
-# Device bytes one particle takes in a batch handle: state (double-buffered
-# position, velocity and spin: 192), FC/TOW and the Adams-Bashforth history
-# (96), binning and sort copies (~90), wall history with 8 slots (~290),
-# and about 6 half-list pairs at ~150 bytes each (index, history x2,
-# transpose, owner, contact record) -- rounded up.
-BYTES_PER_PARTICLE = 1700
+
+def footprint(lib, prm, lim) -> dict:
+    """dem_batch_footprint: device bytes of a batch handle with limits lim
+    (array_bytes, pair_bytes, pair_capacity)."""
+    import ctypes as C
+    m = abi.DemMemory()
+    rc = lib.dem_batch_footprint(C.byref(prm), C.byref(lim), C.byref(m))
+    if rc != 0:
+        raise ValueError("invalid batch limits")
+    d = m.as_dict()
+    d["bytes"] = d["array_bytes"] + d["pair_bytes"]
+    return d
+
+
+def limits_for_budget(lib, prm, n_facets: int, budget_bytes: int, max_systems: int, pairs_per_particle: int = 6):
+    """Batch limits whose footprint fits budget_bytes: the cell, facet and
+    bin ranges of max_systems systems like `prm` (with n_facets facets), and
+    the particle capacity the rest of the budget pays for.  The footprint is
+    affine in the particle capacity, so two evaluations give the bytes per
+    particle (its arrays and its pair-list room).  Returns (limits,
+    bytes_per_particle)."""
+    per = P.batch_limits(lib, [(prm, 64, n_facets)], max_systems=1)
+    lim = abi.DemBatchLimits()
+    lim.max_systems = int(max_systems)
+    lim.max_cells = int(per.max_cells) * max_systems
+    lim.max_search_cells = int(per.max_search_cells) * max_systems
+    lim.max_facets = int(per.max_facets) * max_systems
+    lim.max_facet_bins = int(per.max_facet_bins) * max_systems
+    lim.pairs_per_particle = int(pairs_per_particle)
+    step = 1 << 20
+    lim.max_particles = 64
+    f0 = footprint(lib, prm, lim)["bytes"]
+    lim.max_particles = 64 + step
+    per_particle = (footprint(lib, prm, lim)["bytes"] - f0) / step
+    n = int((budget_bytes - f0) // per_particle) + 64
+    n = min(n, (1 << 27) - 64) // 64 * 64
+    if n < 64:
+        raise ValueError(f"{budget_bytes} bytes do not hold the cell ranges of {max_systems} systems")
+    lim.max_particles = n
+    assert footprint(lib, prm, lim)["bytes"] <= budget_bytes
+    return lim, per_particle
 
 
 @dataclass
@@ -69,21 +109,16 @@ class DemServer:
     """
 
     def __init__(self, lib, build: Callable, template, hbm_budget_bytes: int, max_systems: int = 64,
-                 chunk: int = 25, builders: int = 2, graphs: bool = False, batch=None):
+                 chunk: int = 25, builders: int = 2, graphs: bool = False, batch=None, pairs_per_particle: int = 6):
         self.lib = lib
         self.build = build
         self.chunk = int(chunk)
+        self.pairs_per_particle = int(pairs_per_particle)
         _, prm, arr, walls, _ = template
-        max_particles = int(hbm_budget_bytes // BYTES_PER_PARTICLE)
-        per = P.batch_limits(lib, [(prm, 64, walls[0].shape[0])], max_systems=1)
-        lim = abi.DemBatchLimits()
-        lim.max_particles = max_particles
-        lim.max_systems = int(max_systems)
-        lim.max_cells = int(per.max_cells) * max_systems
-        lim.max_search_cells = int(per.max_search_cells) * max_systems
-        lim.max_facets = int(per.max_facets) * max_systems
-        lim.max_facet_bins = int(per.max_facet_bins) * max_systems
+        lim, self.bytes_per_particle = limits_for_budget(lib, prm, walls[0].shape[0], hbm_budget_bytes,
+                                                         max_systems, pairs_per_particle)
         self.limits = lim
+        self.footprint = footprint(lib, prm, lim)
         # `batch` replaces the device batch (the CPU tests pass a model of it)
         self.batch = batch if batch is not None else BatchSystem(lib, prm, lim)
         self.batch.set_graphs(graphs)
@@ -95,9 +130,23 @@ class DemServer:
             self.pool.shutdown(wait=False)
         self.batch.close()
 
-    def _admit(self, req, case, now) -> Optional[_Running]:
+    def request_footprint(self, case) -> int:
+        """Device bytes a case takes: the footprint of a batch holding it
+        alone (its particle, cell, facet and bin ranges and its pair-list
+        room)."""
+        _, prm, arr, walls, _ = case
+        lim = P.batch_limits(self.lib, [(prm, arr["pos"].shape[1], walls[0].shape[0])], max_systems=1)
+        lim.pairs_per_particle = self.pairs_per_particle
+        return footprint(self.lib, prm, lim)["bytes"]
+
+    def _admit(self, req, case, now, pairs_pending: int) -> Optional[_Running]:
         _, prm, arr, walls, _ = case
         bt = self.batch
+        # the pairs of the running cases (last build), those admitted in this
+        # round and this case's estimate must fit the pair-list room
+        mem = bt.memory_info()
+        if mem["pairs"] + pairs_pending + self.pairs_per_particle * arr["pos"].shape[1] > mem["pair_capacity"]:
+            return None
         try:
             sid = bt.add(prm, arr["pos"].shape[1])
         except DemError as e:
@@ -142,15 +191,17 @@ class DemServer:
             # admit every built request that fits, in arrival order
             new = []
             keep = deque()
+            pending = 0
             for r, fut in building:
                 if self.pool is not None and not fut.done():
                     keep.append((r, fut))
                     continue
                 case = fut.result() if self.pool is not None else fut
-                rec = self._admit(r, case, now)
+                rec = self._admit(r, case, now, pending)
                 if rec is None:
                     keep.append((r, case if self.pool is None else fut))
                     continue
+                pending += self.pairs_per_particle * r["n"]
                 running[rec.sid] = rec
                 new.append(rec.sid)
             building = keep

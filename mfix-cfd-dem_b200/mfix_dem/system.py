@@ -339,6 +339,13 @@ class DemSystem:
         names = ("force", "neighbor", "desgrid", "integrate", "coupling", "other", "walls", "pairs", "gather")
         return {k: (float(ms[i]), int(nl[i])) for i, k in enumerate(names)}
 
+    def memory_info(self) -> dict:
+        """dem_memory_info: device bytes the handle holds (array_bytes,
+        pair_bytes, scratch_bytes), its pair capacity and its pairs."""
+        m = abi.DemMemory()
+        self._call("memory_info", self._h, C.byref(m))
+        return m.as_dict()
+
     def launch_count(self) -> int:
         v = C.c_int64()
         self._call("launch_count", self._h, C.byref(v))
@@ -477,6 +484,7 @@ class BatchSystem:
     pair_count = DemSystem.pair_count
     set_stream = DemSystem.set_stream
     set_graphs = DemSystem.set_graphs
+    memory_info = DemSystem.memory_info
     autotune = DemSystem.autotune
     get_tuning = DemSystem.get_tuning
     set_tuning = DemSystem.set_tuning

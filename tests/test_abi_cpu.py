@@ -40,12 +40,13 @@ def test_abi_version_and_struct_sizes(lib_path):
     lib = load_library()
     assert lib.dem_abi_version() == abi.DEM_ABI_VERSION
     # sizes of the structs as the C compiler lays them out
-    src = f'#include "{HEADER}"\n#include <stdio.h>\nint main(){{printf("%zu %zu %zu\\n", sizeof(dem_params), sizeof(dem_stats), sizeof(dem_fluid_grid));}}'
+    src = f'#include "{HEADER}"\n#include <stdio.h>\nint main(){{printf("%zu %zu %zu %zu %zu\\n", sizeof(dem_params), sizeof(dem_stats), sizeof(dem_fluid_grid), sizeof(dem_batch_limits), sizeof(dem_memory));}}'
     exe = ROOT / "oracle" / "_build" / "abi_sizes"
     exe.parent.mkdir(exist_ok=True)
     subprocess.run(["gcc", "-x", "c", "-o", str(exe), "-"], input=src, text=True, check=True)
     sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
-    assert sizes == [C.sizeof(abi.DemParams), C.sizeof(abi.DemStats), C.sizeof(abi.DemFluidGrid)]
+    assert sizes == [C.sizeof(abi.DemParams), C.sizeof(abi.DemStats), C.sizeof(abi.DemFluidGrid),
+                     C.sizeof(abi.DemBatchLimits), C.sizeof(abi.DemMemory)]
 
 
 def test_create_without_device_fails_cleanly(lib_path):

@@ -49,3 +49,38 @@ def test_served_results_same_alone_and_in_the_mix():
         for k in ("pos", "vel", "omega", "state"):
             assert np.array_equal(got.state[k], alone.state[k]), (req["rid"], k)
         assert got.stats["steps_done"] == req["steps"]
+
+
+def test_batch_memory_is_its_footprint():
+    """The device memory a batch handle takes is what dem_batch_footprint
+    counts for its limits (the same arrays, the same sizes): dem_memory_info
+    reports it exactly, and the device's free memory drops by it (within the
+    allocation granularity); served cases then stay within the pair room."""
+    import torch
+    from mfix_dem.serve import footprint, limits_for_budget
+    from mfix_dem.system import BatchSystem
+    lib = load_library()
+    _, prm, arr, walls, _ = _build(REQS[1])
+    lim, per = limits_for_budget(lib, prm, walls[0].shape[0], 2 << 30, 8)
+    f = footprint(lib, prm, lim)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    b = BatchSystem(lib, prm, lim)
+    m = b.memory_info()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    try:
+        for k in ("array_bytes", "pair_bytes", "pair_capacity"):
+            assert m[k] == f[k], k
+        used = free0 - free1
+        assert abs(used - f["bytes"]) <= 0.05 * f["bytes"] + (64 << 20), (used, f["bytes"])
+        sid = b.add(prm, arr["pos"].shape[1])
+        b.set_walls(sid, *walls)
+        b.upload_state(sid, arr["pos"], arr["vel"], arr["omega"], arr["radius"], arr["pmass"], arr["omoi"],
+                       arr["state"], arr["phase"])
+        b.start([sid])
+        b.step(50)
+        m2 = b.memory_info()
+        assert 0 < m2["pairs"] <= m2["pair_capacity"] == f["pair_capacity"]
+    finally:
+        b.close()

@@ -22,6 +22,10 @@ class FakeBatch:
     def set_graphs(self, on):
         pass
 
+    def memory_info(self):
+        # the pair room never binds here: admission is by particle ranges
+        return {"pairs": 0, "pair_capacity": 1 << 40}
+
     def add(self, prm, n):
         if sum(self.used.values()) + n > self.capacity:
             raise DemError(abi.DEM_ERR_CAPACITY, "dem_sys_add", "full")
@@ -59,16 +63,18 @@ class FakeBatch:
         pass
 
 
+TEMPLATE = configs.hopper_case(2000)
+
+
 def _build(req):
     n = req["n"]
     arr = {k: None for k in ("vel", "omega", "radius", "pmass", "omoi", "state", "phase")}
     arr["pos"] = np.zeros((3, n))
-    return (None, None, arr, (np.zeros((1, 3, 3)), np.zeros((1, 3))), {})
+    return (None, TEMPLATE[1], arr, (np.zeros((1, 3, 3)), np.zeros((1, 3))), {})
 
 
 def _server(capacity):
-    tmpl = configs.hopper_case(2000)
-    return DemServer(load_library(), _build, tmpl, hbm_budget_bytes=1 << 30, max_systems=8, builders=0,
+    return DemServer(load_library(), _build, TEMPLATE, hbm_budget_bytes=1 << 30, max_systems=8, builders=0,
                      batch=FakeBatch(capacity))
 
 
@@ -98,3 +104,32 @@ def test_steps_must_be_whole_chunks():
     srv = _server(capacity=5000)
     with pytest.raises(ValueError):
         srv.run([{"rid": 0, "arrival": 0.0, "n": 100, "steps": 30}], clock=lambda: 0.0)
+
+
+def test_limits_fill_the_budget_by_the_library_footprint():
+    """The server's limits: the footprint the library counts for them is
+    within the budget and within one particle row of it; the bytes per
+    particle cover the state and the pair-list room."""
+    from mfix_dem.serve import footprint, limits_for_budget
+    lib = load_library()
+    _, prm, _, walls, _ = TEMPLATE
+    for budget, nsys in ((1 << 30, 8), (4 << 30, 16), (40 * 10**9, 64)):
+        lim, per = limits_for_budget(lib, prm, walls[0].shape[0], budget, nsys, pairs_per_particle=6)
+        f = footprint(lib, prm, lim)
+        assert f["bytes"] <= budget < f["bytes"] + 64 * per + 1
+        assert f["pair_capacity"] == 6 * lim.max_particles + 1024
+        # state and histories (> 500 B), plus 6 pairs of > 100 B each
+        assert 500 + 6 * 100 < per < 3000
+        # the pair-list room is the one term that grows with pairs_per_particle
+        lim8 = abi.DemBatchLimits.from_buffer_copy(lim)
+        lim8.pairs_per_particle = 8
+        assert footprint(lib, prm, lim8)["bytes"] > f["bytes"]
+
+
+def test_request_footprint_grows_with_the_case():
+    srv = _server(capacity=10**6)
+    small, big = _build({"n": 10_000}), _build({"n": 100_000})
+    fs, fb = srv.request_footprint(small), srv.request_footprint(big)
+    assert fs < fb
+    # the difference is 90,000 particles at the server's bytes per particle
+    assert abs((fb - fs) - 90_000 * srv.bytes_per_particle) < 0.01 * (fb - fs)
