@@ -58,9 +58,10 @@ def parse():
                     help="served leg: replay aligned periods as CUDA graphs (1) or step launch by launch (0)")
     ap.add_argument("--batch-systems", type=int, default=256, help="systems of the batched leg (0 = skip)")
     ap.add_argument("--batch-total", type=int, default=6_000_000, help="particles of the batched leg")
-    ap.add_argument("--serve-rates", default="5,20,50", help="request rates (1/s) of the served leg ('' = skip)")
+    ap.add_argument("--serve-rates", default="5,10,20,50,100,200",
+                    help="request rates (1/s) of the served leg ('' = skip)")
     ap.add_argument("--serve-requests", type=int, default=30, help="requests per rate")
-    ap.add_argument("--serve-steps", type=int, default=2000, help="DES steps per served case")
+    ap.add_argument("--serve-steps", type=int, default=20000, help="DES steps per served case")
     ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="HBM budget of the server")
     ap.add_argument("--workload", default="dense", choices=["dense", "rsa40"],
                     help="dense: the placement with every diameter grown by --inflate; rsa40: as placed")
@@ -438,7 +439,9 @@ def _batched_run(args, prec, stream, systems, info, barrier):
     bt.step(5)
     tuning = bt.autotune(reps=3)
     bt.step(warm - 5)
-    steps = ((args.steps + nsn - 1) // nsn) * nsn
+    # at least four periods: one period is ~15 ms, short enough for a host
+    # hiccup (clock sampling, the per-period pair-count read) to show
+    steps = max(((args.steps + nsn - 1) // nsn) * nsn, 4 * nsn)
     torch.cuda.synchronize()
     p0 = bt.pair_count()
     l0 = bt.launch_count()
@@ -544,17 +547,21 @@ def run_served(args, barrier, ws, rank):
         reqs = partition_requests(reqs_all, ws)[rank]
         srv = DemServer(load_library(), build, template, hbm_budget_bytes=int(args.serve_budget_gb * 1e9),
                         max_systems=64, graphs=bool(args.serve_graphs))
+        server_bytes = srv.footprint["bytes"]
         barrier()
         res = srv.run(reqs)
         srv.close()
         lat = gather_list([r.latency for r in res["results"]], ws, "cuda")
+        # particles that left through the outlet (deleted as rogue)
+        gone = sum(r.n - int(r.stats["n_normal"]) for r in res["results"])
         m = gather_metrics({"work": res["particle_steps"], "span": res["span_s"], "busy": res["busy_s"],
-                            "chunks": res["chunks"]}, ws, "cuda")
+                            "chunks": res["chunks"], "gone": float(gone)}, ws, "cuda")
         span = max(m["span"])
         out.append({"rate_per_s": rate, "requests": len(reqs_all), "p50_s": float(np.percentile(lat, 50)),
                     "p99_s": float(np.percentile(lat, 99)), "mean_s": float(np.mean(lat)),
                     "particle_steps_per_s": sum(m["work"]) / span if span > 0 else 0.0,
                     "span_s": span, "gpu_busy_s": max(m["busy"]), "chunks": int(sum(m["chunks"])),
+                    "particles_discharged": int(sum(m["gone"])), "server_footprint_gb": server_bytes / 1e9,
                     "ranks": ws})
     return out
 
@@ -655,12 +662,20 @@ def run_ours(args):
                 "trajectory_rel_err_vs_fp64": b["trajectory_rel_err"],
                 "n_pairs": b["split"]["pairs"]}
         if served is not None:
+            from mfix_dem import configs as _cfg
+            dt = float(_cfg.hopper_case(5000)[1].dtsolid)
             line["served"] = {
                 "workload": "hopper_discharge_poisson", "precision": "split", "integration": "fp64",
                 "steps_per_case": args.serve_steps, "particles_per_case": "log-uniform 5,000-500,000",
-                "hbm_budget_gb": args.serve_budget_gb, "admission": "particle/cell/facet ranges of the budget",
-                "note": "steps per case reduced from the 20,000 of the workload description so that a sweep "
-                        "fits in the bench run; latency = completion - arrival, wall clock",
+                "hbm_budget_gb": args.serve_budget_gb,
+                "admission": "footprint counted by the library (dem_batch_footprint): limits sized to the budget, "
+                             "a case admitted when its particle/cell/facet ranges and its pair-list room are free",
+                "physical_time_per_case_s": dt * args.serve_steps,
+                "note": "latency = completion - arrival (case built on the host after arrival), wall clock; at "
+                        "DTSOLID %.3g s the steps per case cover %.3g s, in which the fill (starting at rest "
+                        "about 0.19 m above the outlet) falls under a millimetre: no particle reaches the "
+                        "outlet, which would take about 0.2 s (~%d k steps) per case" % (
+                            dt, dt * args.serve_steps, int(0.2 / dt / 1000)),
                 "rates": served}
         print(json.dumps(line), flush=True)
     if ws > 1:
