@@ -594,6 +594,20 @@ k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
                            ((!((fw >> 8) & PF_HIST) && (double)gq.y > reach) ? 2u : 0u) |
                            ((!((fw >> 16) & PF_HIST) && (double)gq.z > reach) ? 4u : 0u) |
                            ((!((fw >> 24) & PF_HIST) && (double)gq.w > reach) ? 8u : 0u);
+    // the particles of the group's pairs in one load each, when any pair
+    // needs them (a group past the list's end has fewer than four)
+    int4 o4 = make_int4(0, 0, 0, 0), n4 = make_int4(0, 0, 0, 0);
+    const unsigned live = c0 + 3 < np ? 15u : (1u << (unsigned)(np - c0)) - 1u;
+    if (~apart & live) {
+      if (c0 + 3 < np) {
+        o4 = *reinterpret_cast<const int4*>(owner + c0);
+        n4 = *reinterpret_cast<const int4*>(nbrs + c0);
+      } else {
+        o4.x = owner[c0]; n4.x = nbrs[c0];
+        if (c0 + 1 < np) { o4.y = owner[c0 + 1]; n4.y = nbrs[c0 + 1]; }
+        if (c0 + 2 < np) { o4.z = owner[c0 + 2]; n4.z = nbrs[c0 + 2]; }
+      }
+    }
 #pragma unroll 1
     for (int j = 0; j < 4; ++j) {
     const long long cc = c0 + j;
@@ -605,13 +619,17 @@ k_pairs(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
       if (f0) pflag[cc] = 0;
       continue;
     }
-    const int ll = owner[cc], i = nbrs[cc];
+    const int ll = j == 0 ? o4.x : (j == 1 ? o4.y : (j == 2 ? o4.z : o4.w));
+    const int i = j == 0 ? n4.x : (j == 1 ? n4.y : (j == 2 ? n4.z : n4.w));
     uint8_t f = f0 & PF_HIST;  // NONEXISTENT partner or zero distance: history kept
     double* ph = pft + 3 * cc;
-    if (state[i] != DEM_STATE_NONEXISTENT && state[ll] != DEM_STATE_NONEXISTENT) {
+    // the states and the positions in one round of loads (any slot's
+    // position can be read; it is used only for existing particles)
+    const double4 a = pos4[ll], b = pos4[i];
+    const int8_t sl = state[ll], si = state[i];
+    if (si != DEM_STATE_NONEXISTENT && sl != DEM_STATE_NONEXISTENT) {
       const DevParams& p = sysp<B>(p0, bv, ll);
       PState L, I;
-      const double4 a = pos4[ll], b = pos4[i];
       L.x[0] = a.x; L.x[1] = a.y; L.x[2] = a.z; L.r = a.w;
       I.x[0] = b.x; I.x[1] = b.y; I.x[2] = b.z; I.r = b.w;
       const double r_lm = L.r + I.r;
