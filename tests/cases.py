@@ -196,3 +196,51 @@ def hopper_wall_case(n=1500, d=2e-3, rho=2500.0, friction=0.4, outlet_d=8, seed=
     arr = state_arrays(pos.T.copy(), vel.T.copy(), np.zeros((3, n)), np.full(n, r), np.full(n, rho))
     prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
     return case, prm, arr, (vertex, norm)
+
+
+def bimodal_case(periodic=(False, False, False), seed=77, coll="LSD"):
+    """Three 8 mm spheres among ~11,000 1 mm spheres in a 24 mm box (36 x 24
+    x 36 mm when x and z are periodic, which needs three DES cells): the
+    first two large ones have the lowest indices, so their half-list rows
+    hold every small neighbour (a few hundred, past any fixed row length),
+    and the last has the highest, so hundreds of rows end in it (a long
+    incoming list).  Small spheres on a lattice of spacing 1.02 d with
+    jitter, none overlapping a large one; LSD, default walls."""
+    rng = np.random.default_rng(seed)
+    d, D = 1e-3, 8e-3
+    box = (36e-3, 24e-3, 36e-3) if periodic[0] else (24e-3, 24e-3, 24e-3)
+    a = 1.02 * d
+    axes = []
+    for L in box:
+        m = int(L // a)
+        axes.append((np.arange(m) + 0.5) * a + 0.5 * (L - m * a))
+    small = np.stack(np.meshgrid(*axes, indexing="ij"), 0).reshape(3, -1)
+    # with periodic x and z the first large sphere straddles the periodic
+    # faces, so its neighbours come through the image shift
+    big = (np.array([[1.0, 12.0, 1.0], [18.0, 12.0, 18.0], [12.0, 12.0, 30.0]]) if periodic[0] else
+           np.array([[6.0, 12.0, 6.0], [18.0, 12.0, 18.0], [12.0, 12.0, 12.0]])).T * 1e-3
+    sep = small[:, :, None] - big[:, None, :]
+    for ax in range(3):
+        if periodic[ax]:
+            sep[ax] -= box[ax] * np.round(sep[ax] / box[ax])
+    dist = np.sqrt((sep ** 2).sum(axis=0)).min(axis=1)
+    small = small[:, dist > 0.5 * (D + d) * 1.01]
+    small = small + rng.uniform(-0.01 * d, 0.01 * d, size=small.shape)
+    pos = np.concatenate([big[:, :2], small, big[:, 2:]], axis=1)
+    n = pos.shape[1]
+    radius = np.full(n, 0.5 * d)
+    radius[[0, 1, n - 1]] = 0.5 * D
+    vel = rng.uniform(-0.05, 0.05, size=(3, n))
+    arr = state_arrays(pos, vel, np.zeros((3, n)), radius, np.full(n, 2500.0))
+    kw = {}
+    if coll == "HERTZ":
+        kw = dict(e_young=(1e7,), v_poisson=(0.3,), ew_young=1e7, vw_poisson=0.3,
+                  des_et_input=0.9, des_et_wall_input=[0.9])
+    case = P.DemCase(d_p0=(D,), ro_s0=(2500.0,), coll_model=coll, intg_method="EULER",
+                     kn=1000.0, kn_w=1000.0, des_en_input=0.9, des_en_wall_input=[0.9],
+                     mew=0.2, mew_w=0.2, grav=(0.0, -9.81, 0.0), domain_hi=box, fluid_cells=(1, 1, 1),
+                     neighbor_search_n=25, periodic=periodic,
+                     desgridsearch=(3, 2, 3) if periodic[0] else (None, None, None), **kw)
+    prm, info = P.build_params(case, arr["radius"], arr["pmass"], arr["phase"], arr["state"])
+    walls = P.default_walls(case.domain_lo, case.domain_hi, periodic=periodic)
+    return case, prm, arr, walls

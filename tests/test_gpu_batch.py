@@ -145,3 +145,36 @@ def test_batch_refuses_single_system_calls():
     with pytest.raises(Exception):
         bt.step(1)  # a system with particles has not been started
     bt.close()
+
+
+def test_extent_grows_and_shrinks_with_long_rows():
+    """The step kernels of a batch cover the extent of the live systems'
+    ranges.  A small system (its range ends inside a 64-particle block, so
+    padding slots follow it) runs alone; a system with rows of a few hundred
+    neighbours (three large spheres among small ones) joins past it, runs,
+    and leaves from the top of the extent; a third joins where it was.
+    Each system matches its own handle bit for bit."""
+    from cases import bimodal_case
+    a = settling_case(n_side=(5, 10, 5), seed=41, kn=900.0, mew=0.2)
+    big = bimodal_case()
+    c = settling_case(n_side=(4, 10, 4), seed=43, kn=700.0, mew=0.3, spacing=0.98)
+    bt = _batch([a, big, c], max_systems=3, slack=1.0)
+    ia = _add(bt, a)
+    bt.start([ia])
+    bt.step(30)
+    ib = _add(bt, big)
+    bt.start([ib])
+    bt.step(30)
+    g = _alone(big, 30)
+    _compare(bt, ib, g)
+    g.close()
+    bt.remove(ib)
+    bt.step(25)
+    ic = _add(bt, c)
+    bt.start([ic])
+    bt.step(30)
+    for sid, case, steps in ((ia, a, 115), (ic, c, 30)):
+        g = _alone(case, steps)
+        _compare(bt, sid, g)
+        g.close()
+    bt.close()

@@ -191,3 +191,25 @@ def test_periodic_particles_reach_a_wall_between_builds():
     d = o.download_state()
     assert np.all(d["pos"][1] > 0.0)            # the floor held them
     assert o.stats()["n_wall_contacts"] >= 0
+
+
+@pytest.mark.parametrize("periodic", [(False, False, False), (True, False, True)])
+def test_long_rows_and_long_incoming_lists_match_oracle(periodic):
+    """Large spheres among small ones: rows of a few hundred neighbours (past
+    the 16 slots the count pass keeps and the 128 keys a warp ranks, so the
+    fill pass takes its one-lane insertion path) and an incoming list of a
+    few hundred pairs (past the 16 the transpose sorts in registers); with
+    periodic x and z the first large sphere straddles the periodic faces.
+    Cells, NEIGHBOR_INDEX / NEIGHBORS and the state stay bit-identical to the
+    oracle through a rebuild."""
+    from cases import bimodal_case
+    case, prm, arr, walls = bimodal_case(periodic=periodic)
+    g, o = pair_both(prm, arr, walls)
+    ni = np.asarray(o.download_pairs()[0])
+    rows = np.diff(np.concatenate([[1], ni]))
+    assert rows.max() > 128
+    assert np.array_equal(g.download_cells(), o.download_cells())
+    compare_pairs(g, o)
+    g.step(30); o.step(30)
+    compare_state(g, o, exact=True)
+    assert compare_pairs(g, o) == 0.0
