@@ -353,7 +353,6 @@ int ensure_pair_capacity(dem_handle* h, long long need);
 int build_transpose(dem_handle* h, int nb);    // neighbor.cu
 void launch_neigh_count(dem_handle* h);        // neighbor.cu: count pass of the pair build
 void set_hist_flags(dem_handle* h);            // neighbor.cu: PF_HIST from the current history
-void launch_pair_gaps(dem_handle* h);          // neighbor.cu: pair gaps at a build, displacement bound 0
 void launch_skin(dem_handle* h);               // force.cu: adds the step's displacement to the bound
 void skin_unknown(dem_handle* h);              // force.cu: positions changed from outside: no pair skipped
 void launch_wall_gaps(dem_handle* h);          // force.cu: wall clearances at a build (with the pair gaps)

@@ -598,17 +598,45 @@ __global__ void k_keep_rows(int n, int n_old, BatchView bv, const int* __restric
   row_se[i] = (int)min(start + (e - s), cap);
 }
 
+// Gap of a pair at a build: |x_i - x_l| - (r_l + r_i), less a margin of
+// 1e-9 (r_l + r_i) for the rounding of the distance, rounded down to float;
+// -1 for a pair with a NONEXISTENT particle.
+template <bool B>
+__device__ __forceinline__ float pair_gap(const DevParams& p0, const BatchView& bv, int ll, int i,
+                                          const double4* __restrict__ pos4, const int8_t* __restrict__ state) {
+  if (state[ll] == DEM_STATE_NONEXISTENT || state[i] == DEM_STATE_NONEXISTENT) return -1.0f;
+  const DevParams& p = sysp<B>(p0, bv, ll);
+  const double4 a = pos4[ll], b = pos4[i];
+  const double xl[3] = {a.x, a.y, a.z}, xi[3] = {b.x, b.y, b.z};
+  double d2 = 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double pj = xi[c];
+    const double s = periodic_shift(p, c, pj - xl[c]);
+    if (s != 0.0) pj = pj + s;
+    const double d = pj - xl[c];
+    d2 += d * d;
+  }
+  const double r_lm = a.w + b.w;
+  return __double2float_rd(sqrt(d2) - r_lm - 1e-9 * r_lm);
+}
+
 // neighbour.f:77-117: history of each new pair from the same neighbour id in
 // the owner's previous row, zero when the pair is new.  A thread per pair of
 // the new list (its owner from pair_owner); a batch system built for the
-// first time (due = 2) takes no history from its region.
+// first time (due = 2) takes no history from its region.  The same pass sets
+// the pair's gap (pair_gap) and restarts the displacement bound.
 template <bool B>
-__global__ void k_remap(const int* __restrict__ d_np, BatchView bv, const int* __restrict__ nbrs,
-                        const int* __restrict__ owner, const int* __restrict__ old_end,
-                        const int* __restrict__ old_nbrs, const double* __restrict__ old_pft,
-                        double* __restrict__ pft, uint8_t* __restrict__ pflag, int have_old) {
-  const long long np = *d_np, stride = (long long)gridDim.x * blockDim.x;
-  for (long long cc = (long long)blockIdx.x * blockDim.x + threadIdx.x; cc < np; cc += stride) {
+__global__ void k_remap(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
+                        const int* __restrict__ nbrs, const int* __restrict__ owner,
+                        const int* __restrict__ old_end, const int* __restrict__ old_nbrs,
+                        const double* __restrict__ old_pft, double* __restrict__ pft, uint8_t* __restrict__ pflag,
+                        int have_old, const double4* __restrict__ pos4, const int8_t* __restrict__ state,
+                        float* __restrict__ pgap, double* __restrict__ skin) {
+  const long long np = min((long long)*d_np, cap), stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t0 == 0) skin[0] = 0.0;
+  for (long long cc = t0; cc < np; cc += stride) {
     const int ll = owner[cc], nb = nbrs[cc];
     bool carry = have_old != 0;
     if constexpr (B) {
@@ -626,6 +654,7 @@ __global__ void k_remap(const int* __restrict__ d_np, BatchView bv, const int* _
     }
     pft[3 * cc] = a; pft[3 * cc + 1] = b; pft[3 * cc + 2] = c;
     pflag[cc] = (a != 0.0 || b != 0.0 || c != 0.0) ? PF_HIST : 0;
+    pgap[cc] = pair_gap<B>(p0, bv, ll, nb, pos4, state);
   }
 }
 
@@ -639,50 +668,7 @@ __global__ void k_hist_flags(const int* __restrict__ d_np, const double* __restr
   }
 }
 
-// Gap of every pair at a build: |x_i - x_l| - (r_l + r_i), less a margin of
-// 1e-9 (r_l + r_i) for the rounding of the distance, rounded down to float;
-// -1 for pairs with a NONEXISTENT particle.  The displacement bound restarts
-// at zero.
-template <bool B>
-__global__ void k_pair_gaps(DevParams p0, BatchView bv, const int* __restrict__ d_np, long long cap,
-                            const int* __restrict__ owner, const int* __restrict__ nbrs,
-                            const double4* __restrict__ pos4, const int8_t* __restrict__ state,
-                            float* __restrict__ pgap, double* __restrict__ skin) {
-  const long long np = min((long long)*d_np, cap), stride = (long long)gridDim.x * blockDim.x;
-  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t0 == 0) skin[0] = 0.0;
-  for (long long cc = t0; cc < np; cc += stride) {
-    const int ll = owner[cc], i = nbrs[cc];
-    if (state[ll] == DEM_STATE_NONEXISTENT || state[i] == DEM_STATE_NONEXISTENT) { pgap[cc] = -1.0f; continue; }
-    const DevParams& p = sysp<B>(p0, bv, ll);
-    const double4 a = pos4[ll], b = pos4[i];
-    const double xl[3] = {a.x, a.y, a.z}, xi[3] = {b.x, b.y, b.z};
-    double d2 = 0.0;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double pj = xi[c];
-      const double s = periodic_shift(p, c, pj - xl[c]);
-      if (s != 0.0) pj = pj + s;
-      const double d = pj - xl[c];
-      d2 += d * d;
-    }
-    const double r_lm = a.w + b.w;
-    pgap[cc] = __double2float_rd(sqrt(d2) - r_lm - 1e-9 * r_lm);
-  }
-}
 
-void launch_pair_gaps(dem_handle* h) {
-  const int T = 256;
-  if (h->batch())
-    k_pair_gaps<true><<<pair_grid(h, T), T, 0, h->stream>>>(h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner,
-                                                            h->nbrs[h->rb], h->pos4[h->cur], h->state, h->pgap,
-                                                            h->skin);
-  else
-    k_pair_gaps<false><<<pair_grid(h, T), T, 0, h->stream>>>(h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner,
-                                                             h->nbrs[h->rb], h->pos4[h->cur], h->state, h->pgap,
-                                                             h->skin);
-  DEM_LAUNCH(h);
-}
 
 void set_hist_flags(dem_handle* h) {
   const int T = 256;
@@ -922,19 +908,20 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   const int pn = 1 - h->pcur;
   const int have_old = (carry_history && h->have_pairs) ? 1 : 0;
   if (bt)
-    k_remap<true><<<pair_grid(h, 256), 256, 0, h->stream>>>(h->d_np, bv, h->nbrs[nb], h->pair_owner,
-                                                            h->row_end[h->rb], h->nbrs[h->rb], h->pft[h->pcur],
-                                                            h->pft[pn], h->pflagb[pn], have_old);
+    k_remap<true><<<pair_grid(h, 256), 256, 0, h->stream>>>(p, bv, h->d_np, h->pair_cap, h->nbrs[nb],
+                                                            h->pair_owner, h->row_end[h->rb], h->nbrs[h->rb],
+                                                            h->pft[h->pcur], h->pft[pn], h->pflagb[pn], have_old,
+                                                            h->pos4[h->cur], h->state, h->pgap, h->skin);
   else
-    k_remap<false><<<pair_grid(h, 256), 256, 0, h->stream>>>(h->d_np, bv, h->nbrs[nb], h->pair_owner,
-                                                             h->row_end[h->rb], h->nbrs[h->rb], h->pft[h->pcur],
-                                                             h->pft[pn], h->pflagb[pn], have_old);
+    k_remap<false><<<pair_grid(h, 256), 256, 0, h->stream>>>(p, bv, h->d_np, h->pair_cap, h->nbrs[nb],
+                                                             h->pair_owner, h->row_end[h->rb], h->nbrs[h->rb],
+                                                             h->pft[h->pcur], h->pft[pn], h->pflagb[pn], have_old,
+                                                             h->pos4[h->cur], h->state, h->pgap, h->skin);
   DEM_LAUNCH(h);
   h->rb = nb;
   h->n_built = n;
   h->pcur = pn;
   h->have_pairs = true;
-  launch_pair_gaps(h);
   launch_wall_gaps(h);
   return build_transpose(h, nb);
 }
