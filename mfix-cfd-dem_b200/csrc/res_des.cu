@@ -429,24 +429,43 @@ int dem_read_res0_des(dem_handle* h, const char* path, int32_t restore_pairs, de
     pmass[l] = pvol * ro[l];
     omoi[l] = 2.5 / (pmass[l] * (r * r));
   }
+  // DEM_MI_TIME and VACANCY of the installed inflow boundaries come from the
+  // file (read_res0_des.f:205-221).  The boundaries' layout is installed by
+  // the caller, so the file must hold the same boundaries: as many, each
+  // with the same OCCUPANTS and the same seeding offsets P and Q.  Checked
+  // before anything is uploaded.
+  const size_t nbi = h->ibc.size();
+  std::vector<dem_res_inflow> mi(nbi ? nbi : 1);
+  if (nbi) {
+    int32_t mocc = 1;
+    for (const auto& I : h->ibc) mocc = std::max<int32_t>(mocc, I.bc.occupants);
+    std::vector<double> fp(nbi * (size_t)mocc), fq(nbi * (size_t)mocc);
+    int32_t nbc = 0;
+    const int rr = dem_res_read_inflow(path, h->dp.no_k, &nbc, mi.data(), (int32_t)nbi, nullptr, nullptr,
+                                       fp.data(), fq.data(), mocc);
+    if (rr == DEM_ERR_CAPACITY)
+      return set_err(h, DEM_ERR_ARG, "inflow layout in the restart file differs from the installed one");
+    if (rr) return set_err(h, DEM_ERR_STATE, "restart file has no readable mass-inflow section");
+    if (nbc != (int32_t)nbi) {
+      char b[160];
+      snprintf(b, sizeof b, "restart file holds %d mass-inflow boundaries, the handle has %zu", nbc, nbi);
+      return set_err(h, DEM_ERR_STATE, b);
+    }
+    for (size_t b = 0; b < nbi; ++b) {
+      const auto& I = h->ibc[b];
+      bool same = mi[b].occupants == I.bc.occupants && mi[b].vacancy >= 1 &&
+                  !(mi[b].occupants > 0 && mi[b].vacancy > mi[b].occupants);
+      for (int k = 0; same && k < I.bc.occupants; ++k)
+        same = fp[b * (size_t)mocc + k] == I.p[k] && fq[b * (size_t)mocc + k] == I.q[k];
+      if (!same) return set_err(h, DEM_ERR_ARG, "inflow layout in the restart file differs from the installed one");
+    }
+  }
   if ((rc = dem_upload_state(h, pos.data(), vel.data(), omega.data(), radius.data(), pmass.data(), omoi.data(),
                              state.data(), phase.data(), h->n)))
     return rc;
-  if (!h->ibc.empty()) {
-    // DEM_MI_TIME and VACANCY of the installed inflow boundaries, when the
-    // file holds as many (read_res0_des.f:205-221)
-    std::vector<dem_res_inflow> mi(h->ibc.size());
-    int32_t nbc = 0;
-    if (dem_res_read_inflow(path, h->dp.no_k, &nbc, mi.data(), (int32_t)mi.size(), nullptr, nullptr, nullptr,
-                            nullptr, 0) == 0 && nbc == (int32_t)h->ibc.size()) {
-      for (size_t b = 0; b < mi.size(); ++b) {
-        if (mi[b].occupants != h->ibc[b].bc.occupants || mi[b].vacancy < 1 ||
-            (mi[b].occupants > 0 && mi[b].vacancy > mi[b].occupants))
-          return set_err(h, DEM_ERR_ARG, "inflow layout in the restart file differs from the installed one");
-        h->ibc[b].bc.vacancy = mi[b].vacancy;
-        h->ibc[b].bc.mi_time = mi[b].mi_time;
-      }
-    }
+  for (size_t b = 0; b < nbi; ++b) {
+    h->ibc[b].bc.vacancy = mi[b].vacancy;
+    h->ibc[b].bc.mi_time = mi[b].mi_time;
   }
   if (!restore_pairs) return 0;
   // entries grouped by owner in the file's order -> CSR with 1-based ends

@@ -7,6 +7,7 @@ import pytest
 from cases import make_system
 from gpu_util import compare_pairs, compare_state
 from inflow_cases import inflow_case
+from mfix_dem import abi
 
 pytestmark = pytest.mark.gpu
 
@@ -53,8 +54,10 @@ def test_queued_numbers_match_oracle():
 def test_restart_file_carries_the_inflow_state(tmp_path):
     """dem_write_res0_des writes the inflow records (DEM_MI_TIME, VACANCY and
     the layout); dem_read_res0_des into a handle with the same boundaries
-    installed restores DEM_MI_TIME and VACANCY, and the two handles then seed
-    the same particles."""
+    installed restores DEM_MI_TIME and VACANCY.  (The uniform numbers the
+    boundaries draw are not part of the file: a restarted run seeds from its
+    own generator or from the numbers its driver queues.)  A file without the
+    inflow section, read into a handle with inflow boundaries, is refused."""
     from mfix_dem import GpuSystem
     from mfix_dem import restart
     from mfix_dem._lib import load
@@ -73,4 +76,13 @@ def test_restart_file_carries_the_inflow_state(tmp_path):
     b = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
     b.set_inflow_bcs([bc], seed=2)
     b.read_res0_des(path, restore_pairs=True)
+    assert b.inflow_state(0) == (vac, mi_time)
+    # a file written by a handle with no inflow boundaries (DEM_BCMI = 0)
+    from mfix_dem.system import DemError
+    c = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    plain = tmp_path / "plain.RES"
+    c.write_res0_des(plain, ro_sol=[case.ro_s0[0]])
+    with pytest.raises(DemError) as e:
+        b.read_res0_des(plain, restore_pairs=True)
+    assert e.value.code == abi.DEM_ERR_STATE
     assert b.inflow_state(0) == (vac, mi_time)
