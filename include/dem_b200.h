@@ -169,7 +169,11 @@ int dem_set_walls(dem_handle* h, const double* vertex, const double* norm_face,
 
 /* Copies the DES arrays in: DES_POS_NEW, DES_VEL_NEW, OMEGA_NEW (max_pip,3),
  * DES_RADIUS, PMASS, OMOI (max_pip), PARTICLE_STATE (int8) and the 1-based
- * solids phase PIJK(:,5). (model/des/discretelement_mod.f:387-391,579-588) */
+ * solids phase PIJK(:,5). (model/des/discretelement_mod.f:387-391,579-588)
+ * After a first full upload, radius, pmass, omoi, state and phase may each
+ * be NULL: the handle keeps its own (a driver that changed only positions,
+ * velocities and spins sends those).  The host arrays may be reused when
+ * the call returns. */
 int dem_upload_state(dem_handle* h, const double* pos, const double* vel,
                      const double* omega, const double* radius,
                      const double* pmass, const double* omoi,

@@ -371,6 +371,7 @@ int dem_sys_upload_state(dem_handle* h, int32_t s, const double* pos, const doub
   SYS_GUARD(h, s);
   SysSlot& S = h->sys[s];
   if (max_pip < 0 || max_pip > S.cap) return set_err(h, DEM_ERR_ARG, "more particles than the system reserved");
+  if (!radius || !pmass || !omoi || !state || !phase) return set_err(h, DEM_ERR_ARG, "null array");
   cudaMemsetAsync(h->state + S.dp.p_begin, 0, (size_t)S.cap, h->stream);
   if (int rc = upload_range(h, S.dp.p_begin, max_pip, S.prm.n_phases, pos, vel, omega, radius, pmass, omoi,
                             state, phase))

@@ -173,33 +173,41 @@ static void prof_collect(dem_handle* h) {
 int upload_range(dem_handle* h, int off, int cnt, int nph, const double* pos, const double* vel,
                  const double* omega, const double* radius, const double* pmass, const double* omoi,
                  const int8_t* state, const int32_t* phase) {
-  if (!pos || !vel || !omega || !radius || !pmass || !omoi || !state || !phase)
-    return set_err(h, DEM_ERR_ARG, "null array");
+  // radius, pmass, omoi, state and phase may be NULL: the device keeps its
+  // values of those (the callers check that there are some)
+  if (!pos || !vel || !omega) return set_err(h, DEM_ERR_ARG, "null array");
   if (cnt <= 0) return 0;
   const size_t n = (size_t)cnt;
   // one staging block: pos(3n) vel(3n) omega(3n) r(n) m(n) omoi(n) + phase(n ints) + flag
   double* st = (double*)stage_buffer(h, sizeof(double) * 12 * n + sizeof(int) * n + 64);
   if (!st) return set_err(h, DEM_ERR_CUDA, "cudaMalloc stage");
-  cudaMemcpyAsync(st, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 3 * n, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 6 * n, omega, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 9 * n, radius, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 10 * n, pmass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(st + 11 * n, omoi, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
-  int* ph = (int*)(st + 12 * n);
-  unsigned* bad = (unsigned*)(ph + n);
-  cudaMemcpyAsync(ph, phase, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(h->state + off, state, n, cudaMemcpyHostToDevice, h->stream);
   const int T = 256, B = (int)((n + T - 1) / T);
   const int c = h->cur;
-  k_pack<<<B, T, 0, h->stream>>>(cnt, st, st + 9 * n, h->pos4[c] + off);
-  k_pack<<<B, T, 0, h->stream>>>(cnt, st + 3 * n, st + 10 * n, h->vel4[c] + off);
-  k_pack<<<B, T, 0, h->stream>>>(cnt, st + 6 * n, st + 11 * n, h->omg4[c] + off);
-  cudaMemsetAsync(bad, 0, sizeof(unsigned), h->stream);
-  k_phase_in<<<B, T, 0, h->stream>>>(cnt, ph, h->state + off, h->phase + off, nph, bad);
-  h->launches += 4;
+  const double* src[3] = {pos, vel, omega};
+  const double* scal[3] = {radius, pmass, omoi};
+  double4* dst[3] = {h->pos4[c] + off, h->vel4[c] + off, h->omg4[c] + off};
+  for (int a = 0; a < 3; ++a) {
+    cudaMemcpyAsync(st + 3 * n * a, src[a], sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+    if (scal[a]) {
+      cudaMemcpyAsync(st + 9 * n + n * a, scal[a], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+      k_pack<<<B, T, 0, h->stream>>>(cnt, st + 3 * n * a, st + 9 * n + n * a, dst[a]);
+    } else {
+      k_pack_keepw<<<B, T, 0, h->stream>>>(cnt, st + 3 * n * a, dst[a]);
+    }
+    h->launches++;
+  }
+  if (state) cudaMemcpyAsync(h->state + off, state, n, cudaMemcpyHostToDevice, h->stream);
   unsigned hb = 0;
-  cudaMemcpyAsync(&hb, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+  if (phase) {
+    int* ph = (int*)(st + 12 * n);
+    unsigned* bad = (unsigned*)(ph + n);
+    cudaMemcpyAsync(ph, phase, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
+    cudaMemsetAsync(bad, 0, sizeof(unsigned), h->stream);
+    k_phase_in<<<B, T, 0, h->stream>>>(cnt, ph, h->state + off, h->phase + off, nph, bad);
+    h->launches++;
+    cudaMemcpyAsync(&hb, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+  }
+  // the host arrays may be reused when the call returns
   if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "upload")) return rc;
   if (hb) return set_err(h, DEM_ERR_ARG, "phase out of range");
   return 0;
@@ -547,6 +555,8 @@ int dem_upload_state(dem_handle* h, const double* pos, const double* vel, const 
                      const int8_t* state, const int32_t* phase, int32_t max_pip) {
   SINGLE_GUARD(h);
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip does not match dem_create");
+  if ((!radius || !pmass || !omoi || !state || !phase) && !h->have_state)
+    return set_err(h, DEM_ERR_ARG, "the first upload needs every array");
   if (int rc = upload_range(h, 0, h->n, h->dp.nph, pos, vel, omega, radius, pmass, omoi, state, phase)) return rc;
   skin_unknown(h);  // positions changed from outside: no pair is known apart until the next build
   h->have_state = true;

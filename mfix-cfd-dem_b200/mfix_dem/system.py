@@ -98,14 +98,18 @@ class DemSystem:
         nf = vertex.shape[0]
         self._call("set_walls", self._h, _dp(vertex), _dp(norm_face), C.c_int32(nf))
 
-    def upload_state(self, pos, vel, omega, radius, pmass, omoi, state, phase):
+    def upload_state(self, pos, vel, omega, radius=None, pmass=None, omoi=None, state=None, phase=None):
+        """dem_upload_state; after a first full upload, radius, pmass, omoi,
+        state and phase may be None (the handle keeps its own)."""
         n = self.n
         pos = _f64(pos, (3, n)); vel = _f64(vel, (3, n)); omega = _f64(omega, (3, n))
-        radius = _f64(radius, (n,)); pmass = _f64(pmass, (n,)); omoi = _f64(omoi, (n,))
-        state = np.ascontiguousarray(state, dtype=np.int8)
-        phase = np.ascontiguousarray(phase, dtype=np.int32)
-        self._call("upload_state", self._h, _dp(pos), _dp(vel), _dp(omega), _dp(radius),
-                   _dp(pmass), _dp(omoi), _bp(state), _ip(phase), C.c_int32(n))
+        radius = None if radius is None else _f64(radius, (n,))
+        pmass = None if pmass is None else _f64(pmass, (n,))
+        omoi = None if omoi is None else _f64(omoi, (n,))
+        state = None if state is None else np.ascontiguousarray(state, dtype=np.int8)
+        phase = None if phase is None else np.ascontiguousarray(phase, dtype=np.int32)
+        self._call("upload_state", self._h, _dp(pos), _dp(vel), _dp(omega), _dp(radius), _dp(pmass), _dp(omoi),
+                   _bp(state), _ip(phase), C.c_int32(n))
 
     def download_state(self, out=None):
         """DES_POS_NEW, DES_VEL_NEW, OMEGA_NEW, PARTICLE_STATE; `out` may hold

@@ -213,3 +213,31 @@ def test_long_rows_and_long_incoming_lists_match_oracle(periodic):
     g.step(30); o.step(30)
     compare_state(g, o, exact=True)
     assert compare_pairs(g, o) == 0.0
+
+
+def test_upload_of_the_moving_state_only():
+    """dem_upload_state with only positions, velocities and spins (the
+    other arrays NULL) keeps the handle's radius, mass, inertia, state and
+    phase: a run that re-sends its own moving state every step stays
+    bit-identical to one that does not.  The first upload needs every
+    array."""
+    from mfix_dem import GpuSystem
+    from mfix_dem.system import DemError
+    from mfix_dem import abi
+    case, prm, arr, walls = settling_case(n_side=(6, 16, 6), spacing=0.98, jitter=0.03)
+    fresh = GpuSystem(prm, arr["pos"].shape[1])
+    with pytest.raises(DemError) as e:
+        fresh.upload_state(arr["pos"], arr["vel"], arr["omega"])
+    assert e.value.code == abi.DEM_ERR_ARG
+    fresh.close()
+    a = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    b = make_system(lambda p, n: GpuSystem(p, n), prm, arr, walls)
+    for k in range(40):
+        a.step(1)
+        b.step(1)
+        s = b.download_state()
+        b.upload_state(s["pos"], s["vel"], s["omega"])
+    sa, sb = a.download_state(), b.download_state()
+    for key in ("pos", "vel", "omega", "state"):
+        assert np.array_equal(sa[key], sb[key]), key
+    assert a.stats()["n_contacts"] == b.stats()["n_contacts"] > 0
