@@ -8,14 +8,15 @@
 // CFUPDATEOLD + CFNEWVALUES (cfupdateold.f:33-41, cfnewvalues.f:669-812).
 //
 // The reference loops over owners LL and scatters each pair's force into
-// FC(LL) and FC(I) with atomics.  Here one thread owns one particle and
-// gathers instead: walls first, then the pairs it appears in as neighbour I
-// (in ascending owner order, from the transpose), then its own row.  That is
-// exactly the order in which the serial reference adds into FC(me)/TOW(me),
-// and each pair is evaluated by both of its particles with identical
-// operands, so every particle's force is bit-identical to the serial
-// reference without atomics.  The tangential history is double-buffered:
-// both evaluations read PFT_in, only the owner writes PFT_out.
+// FC(LL) and FC(I).  Here each pair is evaluated once (k_pairs, a thread per
+// pair), which updates its tangential history in place and writes the
+// terms of both particles into a contact record; then one thread per
+// particle gathers (k_gather): walls first, then the records of the pairs
+// it appears in as neighbour I owned by lower-index particles (ascending
+// owner, from the transpose), its own row, then the remaining incoming
+// pairs.  That is exactly the order in which the serial reference adds into
+// FC(me)/TOW(me), so every particle's force is bit-identical to the serial
+// reference without atomics.
 //
 // This file is compiled with -fmad=false: every FP64 expression rounds as
 // the Fortran does (gfortran emits no FMA without -march).  sqrt and '/' are
