@@ -209,11 +209,25 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes(n_normal, n_pairs, periodic=True):
-    # per step: N*(96 read + 72 write + 4 CSR) + P*(4 id + 24 PFT read + 24 PFT write),
-    # and for a periodic system the DES cell and facet flag the integration
-    # writes (N*5)
-    return n_normal * (177 if periodic else 172) + n_pairs * 52
+def algorithmic_bytes(n_normal, n_pairs, periodic=True, n_torque=None):
+    # per step: N*(64 read + 48 write + 4 CSR) for positions and velocities,
+    # T*(32 read + 24 write) for the spins of the T particles with a torque
+    # (in contact with a particle or a wall: at most 2 per contact and 1 per
+    # wall contact; under Euler the others keep theirs untouched, all of
+    # them otherwise), P*(4 id + 24 PFT read + 24 PFT write), and for a
+    # periodic system the DES cell and facet flag the integration writes
+    # (N*5)
+    t = n_normal if n_torque is None else min(n_normal, n_torque)
+    return n_normal * (121 if periodic else 116) + t * 56 + n_pairs * 52
+
+
+def torqued(stats, integrator):
+    """The particles whose spin the integration must read and write: with
+    Euler at most two per particle contact and one per wall contact, with
+    Adams-Bashforth all."""
+    if integrator != "euler":
+        return None
+    return 2 * int(stats["n_contacts"]) + int(stats["n_wall_contacts"])
 
 
 def cpu_sample(args, threads=None):
@@ -352,7 +366,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     f_ms, f_n = prof["force"]
     peak, peak_kind = measured_peak()
     p_avg = 0.5 * (p0 + p1)
-    bytes_launch = algorithmic_bytes(n_normal, p_avg)
+    bytes_launch = algorithmic_bytes(n_normal, p_avg, n_torque=torqued(st, "euler"))
     achieved = bytes_launch / (f_ms / f_n / 1e3) / 1e9 if f_n else None
     traffic = None
     if PROFILE_TRAFFIC.exists():
@@ -475,7 +489,7 @@ def _batched_run(args, prec, stream, systems, info, barrier):
     n_normal = int(st["n_normal"])
     f_ms, f_n = prof["force"]
     peak, peak_kind = measured_peak()
-    bytes_launch = algorithmic_bytes(n_normal, 0.5 * (p0 + p1), periodic=False)
+    bytes_launch = algorithmic_bytes(n_normal, 0.5 * (p0 + p1), periodic=False, n_torque=torqued(st, "euler"))
     achieved = bytes_launch / (f_ms / f_n / 1e3) / 1e9 if f_n else None
     final = {sid: bt.download_state(sid)["pos"] for sid in ids}
     bt.close()

@@ -499,7 +499,7 @@ int dem_destroy(dem_handle* h) {
   cudaStreamSynchronize(h->stream);
   free_gas(h);
   invalidate_graphs(h);
-  void* ptrs[] = {h->pos4[0], h->pos4[1], h->vel4[0], h->vel4[1], h->omg4[0], h->omg4[1],
+  void* ptrs[] = {h->pos4[0], h->pos4[1], h->vel4[0], h->vel4[1], h->omg4[0],
                   h->state, h->phase, h->fc, h->tow, h->acc_old, h->rot_acc_old, h->dg_pijk,
                   h->cell_cnt, h->cell_start, h->cell_fill, h->cell_list, h->row_cnt,
                   h->row_end[0], h->row_end[1], h->nbrs[0], h->nbrs[1], h->pft[0], h->pft[1],

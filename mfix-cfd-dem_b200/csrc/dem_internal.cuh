@@ -3,7 +3,10 @@
 // Device layout (n = MAX_PIP):
 //   pos4[b][i] = (x, y, z, radius)      double4, double-buffered (b = 0/1)
 //   vel4[b][i] = (u, v, w, pmass)       double4, double-buffered
-//   omg4[b][i] = (wx, wy, wz, omoi)     double4, double-buffered
+//   omg4[b][i] = (wx, wy, wz, omoi)     double4, one array (omg4[0] and
+//                                       omg4[1] are the same): the spin is
+//                                       updated in place, and a particle with
+//                                       no torque under Euler is not touched
 //   state[i]   int8 PARTICLE_STATE, phase[i] uint8 (0-based)
 //   fc, tow    (n,3) column blocks, as FC/TOW of discretelement_mod.f:630
 //   pairs      CSR half list: row_end[i] = pairs in rows 0..i,
@@ -377,9 +380,12 @@ void handle_arrays(dem_handle* h, size_t n, size_t nc, size_t nfc, F&& A) {
   for (int b = 0; b < 2; ++b) {
     A((void**)&h->pos4[b], sizeof(double4) * n);
     A((void**)&h->vel4[b], sizeof(double4) * n);
-    A((void**)&h->omg4[b], sizeof(double4) * n);
     A((void**)&h->row_end[b], sizeof(int) * n);
   }
+  // the spin is one array under both buffer names: only the integrating
+  // gather of a particle writes it, after every kernel that reads it
+  A((void**)&h->omg4[0], sizeof(double4) * n);
+  h->omg4[1] = h->omg4[0];
   A((void**)&h->state, n);
   A((void**)&h->phase, n);
   A((void**)&h->fc, sizeof(double) * 3 * n);
@@ -573,7 +579,7 @@ __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8
                                                 double4* __restrict__ omg_n, double* __restrict__ fc,
                                                 double* __restrict__ tow, double* __restrict__ acc_old,
                                                 double* __restrict__ rot_acc_old, unsigned* __restrict__ vslot,
-                                                CellOut cells = CellOut{}) {
+                                                CellOut cells = CellOut{}, bool keep_w = false) {
   const size_t n = (size_t)p.n;
   if (MODE == 0) {
 #pragma unroll
@@ -631,7 +637,8 @@ __device__ __forceinline__ void finish_particle(const DevParams& p, int me, int8
   }
   pos_n[me] = xo;
   vel_n[me] = make_double4(vn[0], vn[1], vn[2], m);
-  omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
+  // keep_w: the spin stays as it is (the gather did not read it)
+  if (!keep_w) omg_n[me] = make_double4(wn[0], wn[1], wn[2], omoi);
   // |x_new - x| <= max(|v|, |v_new|) * dt for both integrators
   note_displacement(vslot, st < DEM_STATE_NORMAL_GHOST ? fmax(speed(v), speed(vn)) * dt : 0.0);
 }

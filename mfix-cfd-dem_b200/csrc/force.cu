@@ -786,13 +786,16 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
   if (me >= p0.n) return;
   const DevParams& p = sysp<B>(p0, bv, me);
   const int8_t st = state[me];
-  const double4 W = omg_c[me];
-  const double w[3] = {W.x, W.y, W.z};
-  double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
   // the contacts of this pass; a particle in none has no terms to add
   const bool wh = wall_hit[me] != 0, ph = touched[me] != 0;
   if (wh) wall_hit[me] = 0;
   if (ph) touched[me] = 0;
+  // no torque and Euler: the spin stays (OMEGA_NEW = OMEGA_NEW + 0), so it
+  // is neither read nor written (the spin array is updated in place)
+  const bool keep_w = MODE == 1 && !wh && !ph;
+  const double4 W = keep_w ? make_double4(0.0, 0.0, 0.0, 0.0) : omg_c[me];
+  const double w[3] = {W.x, W.y, W.z};
+  double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
   if (wh && st == DEM_STATE_NORMAL) {
     const double* o = wf + 6 * (size_t)me;
     f[0] = o[0]; f[1] = o[1]; f[2] = o[2]; t[0] = o[3]; t[1] = o[4]; t[2] = o[5];
@@ -811,7 +814,7 @@ k_gather(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, const do
   const double4 X = pos_c[me], V = vel_c[me];
   const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z};
   finish_particle<MODE>(p, me, st, x, v, w, X.w, V.w, W.w, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
-                        rot_acc_old, vslot, cells);
+                        rot_acc_old, vslot, cells, keep_w);
 }
 
 // CFUPDATEOLD + CFNEWVALUES from FC/TOW, in place; zeroes FC/TOW.

@@ -341,15 +341,18 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
   F.zero(); T.zero();
   float rs = 0.f, rc = 0.f;
   // a particle in no contact of this pass has no record to add
-  const bool ph = touched[me] != 0;
+  const bool ph = touched[me] != 0, wh = wall_hit[me] != 0;
   if (ph) touched[me] = 0;
+  // no torque and Euler: the spin stays (OMEGA_NEW = OMEGA_NEW + 0), so it
+  // is neither read nor written (the spin array is updated in place)
+  const bool keep_w = MODE == 1 && !wh && !ph;
   if (st != DEM_STATE_NONEXISTENT && ph) {
     add_range(in_start[me], in_start[me + 1], in_flag, rec_in, F, T, rs, rc);
     add_range(me ? row_end[me - 1] : 0, row_end[me], pflag, rec_own, F, T, rs, rc);
   }
-  const double4 X = pos_c[me], V = vel_c[me], W = omg_c[me];
+  const double4 X = pos_c[me], V = vel_c[me], W = keep_w ? make_double4(0.0, 0.0, 0.0, 0.0) : omg_c[me];
   double f0[3] = {0.0, 0.0, 0.0}, t0[3] = {0.0, 0.0, 0.0};
-  if (wall_hit[me]) {
+  if (wh) {
     wall_hit[me] = 0;
     if (st == DEM_STATE_NORMAL) {
       const double* o = wf + 6 * (size_t)me;
@@ -370,7 +373,7 @@ k_gather_split(DevParams p0, BatchView bv, const double4* __restrict__ pos_c, co
   }
   const double x[3] = {X.x, X.y, X.z}, v[3] = {V.x, V.y, V.z}, w[3] = {W.x, W.y, W.z};
   finish_particle<MODE>(p, me, st, x, v, w, X.w, V.w, W.w, f, t, pos_n, vel_n, omg_n, fc, tow, acc_old,
-                        rot_acc_old, vslot, cells);
+                        rot_acc_old, vslot, cells, keep_w);
 }
 
 // The split records live in the handle's record array: the owner records
