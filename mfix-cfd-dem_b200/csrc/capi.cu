@@ -440,6 +440,10 @@ int demb::alloc_handle(dem_handle* h, int nc, int nfc, long long pairs) {
   // CUDA graphs (the legacy default stream cannot be captured)
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return DEM_ERR_CUDA;
   h->stream = h->own_stream;
+  if (cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return DEM_ERR_CUDA;
   if (ensure_pair_capacity(h, pairs)) return DEM_ERR_CUDA;
   if (cudaDeviceSynchronize() != cudaSuccess) return DEM_ERR_CUDA;
   return 0;
@@ -513,6 +517,9 @@ int dem_destroy(dem_handle* h) {
   for (auto e : h->ev_pool) cudaEventDestroy(e);
   if (h->herr) cudaFreeHost(h->herr);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  if (h->side_stream) cudaStreamDestroy(h->side_stream);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   delete h;
   return 0;
 }

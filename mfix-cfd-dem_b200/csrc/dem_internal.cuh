@@ -237,6 +237,10 @@ struct dem_handle {
   } tune;
   bool capturing = false;     // inside a CUDA graph capture: no host syncs
   cudaStream_t own_stream = nullptr;
+  // the wall kernels of a force pass run on side_stream beside the pair
+  // kernel (they write disjoint arrays); ev_fork / ev_join order them
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraphExec_t graphs[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   long long graph_launches = 0;
   long long graph_kernels[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // kernels per graph replay

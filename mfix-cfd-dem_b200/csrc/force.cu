@@ -932,7 +932,22 @@ void launch_gather_only(dem_handle* h) {
 // Euler/AB2 integration into the other state buffer.  The collision model,
 // integrator and force precision are common to all systems of a batch.
 static void launch_force_kernels(dem_handle* h, int mode, bool split) {
-  {
+  // The wall kernels and the pair kernel read the same state and write
+  // disjoint arrays (walls: wall_hit, wf and the wall histories; pairs: the
+  // pair histories, flags, records and touched marks), so the wall work runs
+  // on the side stream beside the pair kernel and the gather waits for both
+  // (in a captured step, two branches of the graph).  With the parts of the
+  // step timed (profiling), they run one after the other.
+  const bool side = h->nf > 0 && h->side_stream && !h->prof;
+  if (side) {
+    cudaEventRecord(h->ev_fork, h->stream);
+    cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0);
+    cudaStream_t main = h->stream;
+    h->stream = h->side_stream;
+    launch_walls(h);
+    h->stream = main;
+    cudaEventRecord(h->ev_join, h->side_stream);
+  } else {
     ProfScope ps(h, DEM_PROF_WALLS);
     launch_walls(h);
   }
@@ -942,6 +957,7 @@ static void launch_force_kernels(dem_handle* h, int mode, bool split) {
     else if (h->batch()) launch_pairs_fp64<true>(h);
     else launch_pairs_fp64<false>(h);
   }
+  if (side) cudaStreamWaitEvent(h->stream, h->ev_join, 0);
   ProfScope ps(h, DEM_PROF_GATHER);
   if (split) launch_gather_split(h, mode);
   else if (h->batch()) launch_gather_fp64<true>(h, mode);
