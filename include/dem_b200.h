@@ -509,7 +509,10 @@ int dem_set_profiling(dem_handle* h, int32_t on);
 int dem_get_profile(dem_handle* h, double* ms, int64_t* launches);
 
 /* Sets the CUDA stream (cudaStream_t passed as void*) used by the handle.
- * NULL selects the legacy default stream. */
+ * NULL selects the legacy default stream.  The wall kernels of a force pass
+ * run on a second stream of the handle's own, forked from and joined back
+ * into this stream by events, so work ordered on this stream sees all of a
+ * step's results. */
 int dem_set_stream(dem_handle* h, void* stream);
 
 /* Per-step force error of the split-precision path: max over particles of
