@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=30, help="requests per rate")
     ap.add_argument("--serve-steps", type=int, default=20000, help="DES steps per served case")
     ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="HBM budget of the server")
+    ap.add_argument("--serve-profile", action="store_true",
+                    help="only the per-chunk cost of a fixed served mix (three hopper cases), by kernel class")
     ap.add_argument("--workload", default="dense", choices=["dense", "rsa40"],
                     help="dense: the placement with every diameter grown by --inflate; rsa40: as placed")
     ap.add_argument("--inflate", type=float, default=1.15,
@@ -582,6 +584,45 @@ def run_served(args, barrier, ws, rank):
     return out
 
 
+def serve_profile(args):
+    """Per-chunk cost of the served pattern: three hopper cases (20k, 60k and
+    150k particles) admitted together and run 500 steps (20 chunks of 25),
+    on servers of two sizes (40 GB / 64 system slots and 4 GB / 8 slots),
+    once with graph replay (wall time per chunk) and once eagerly with the
+    kernel classes timed by CUDA events (ms per chunk and launches)."""
+    import torch
+    from mfix_dem import configs, load_library
+    from mfix_dem.serve import DemServer
+    torch.cuda.set_device(0)
+    cases = {}
+
+    def build(req):
+        if req["n"] not in cases:
+            cases[req["n"]] = configs.hopper_case(req["n"], friction=req["friction"], outlet_d=req["outlet_d"],
+                                                  seed=req["seed"])
+        return cases[req["n"]]
+
+    template = configs.hopper_case(5000)
+    out = []
+    for budget, msys, prof in ((40, 64, False), (4, 8, False), (40, 64, True), (4, 8, True)):
+        reqs = [dict(rid=k, arrival=0.0, n=n, friction=0.4, outlet_d=8, seed=k, steps=500)
+                for k, n in enumerate((20_000, 60_000, 150_000))]
+        srv = DemServer(load_library(), build, template, hbm_budget_bytes=int(budget * 1e9), max_systems=msys,
+                        graphs=True, builders=0)
+        if prof:
+            srv.batch.set_profiling(1)
+        res = srv.run(reqs)
+        row = {"budget_gb": budget, "system_slots": msys, "timed_classes": prof, "chunks": res["chunks"],
+               "ms_per_chunk": 1e3 * res["busy_s"] / res["chunks"], "particles": 230_000,
+               "server_footprint_gb": srv.footprint["bytes"] / 1e9}
+        if prof:
+            row["classes_ms_per_chunk"] = {k: v[0] / res["chunks"] for k, v in srv.batch.profile().items() if v[1]}
+            row["launches_per_chunk"] = {k: v[1] / res["chunks"] for k, v in srv.batch.profile().items() if v[1]}
+        srv.close()
+        out.append(row)
+    print(json.dumps({"serve_profile": out}), flush=True)
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -703,6 +744,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.serve_profile:
+        serve_profile(args)
     else:
         run_ours(args)
 
