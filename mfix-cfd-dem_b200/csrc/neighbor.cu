@@ -904,6 +904,21 @@ int run_neighbour(dem_handle* h, bool carry_history) {
     k_delete_rogue<false><<<B, T, 0, h->stream>>>(p, bv, h->state, h->dg_pijk, h->pos4[h->cur], h->vel4[h->cur],
                                                    h->omg4[h->cur], h->fc, h->tow, h->wall_fid, e);
   DEM_LAUNCH(h);
+  // The transpose of the new list and the history carry-over with the gaps
+  // read the list and write disjoint arrays: the transpose runs on the side
+  // stream beside them and is joined before the build returns (in sequence
+  // when the kernel classes are timed).
+  const bool side = h->side_stream && !h->prof;
+  int trc = 0;
+  if (side) {
+    cudaEventRecord(h->ev_fork, h->stream);
+    cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0);
+    cudaStream_t main = h->stream;
+    h->stream = h->side_stream;
+    trc = build_transpose(h, nb);
+    h->stream = main;
+    cudaEventRecord(h->ev_join, h->side_stream);
+  }
   // history carry-over into the other pft buffer
   const int pn = 1 - h->pcur;
   const int have_old = (carry_history && h->have_pairs) ? 1 : 0;
@@ -923,6 +938,10 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   h->pcur = pn;
   h->have_pairs = true;
   launch_wall_gaps(h);
+  if (side) {
+    cudaStreamWaitEvent(h->stream, h->ev_join, 0);
+    return trc;
+  }
   return build_transpose(h, nb);
 }
 
