@@ -325,6 +325,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     clocks.start()
     p0 = g.pair_count()
     l0 = g.launch_count()
+    f0 = g.stats()["n_builds_filtered"]
     barrier()
     torch.cuda.synchronize()
     clocks.begin()
@@ -386,6 +387,7 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
                 "force_parts_ms_per_launch": parts}
     out = {"value": value, "ms": ms, "n": n, "n_normal": n_normal, "pairs": int(p1), "launches": int(launches),
            "warmup": warm, "tuning": tuning, "window": [warm + 1, warm + args.steps], "rebuilds_timed": rebuilds,
+           "rebuilds_timed_filtered": int(st["n_builds_filtered"] - f0),
            "roofline": roofline, "clocks": clk, "contacts": int(st["n_contacts"]), "prm": prm, "info": info,
            "force_error": None if ferr0 is None else [ferr0, ferr1]}
 
@@ -677,6 +679,7 @@ def run_ours(args):
                        "precision": args.precision,
                        "contacts_last_step": main["contacts"],
                        "timed_window_nn": main["window"], "rebuilds_timed": main["rebuilds_timed"],
+                       "rebuilds_timed_from_candidate_list": main["rebuilds_timed_filtered"],
                        "l2": "inputs larger than L2 (state and pair arrays ~%.0f MB)" % (
                            (main["n"] * 3 * 32 * 2 + main["pairs"] * 100) / 1e6),
                        "parallelism": f"replicas x{ws}"},
@@ -692,6 +695,7 @@ def run_ours(args):
                              "speedup_vs_fp64": other["value"] / main["value"],
                              "force_rel_error_first_last": other["force_error"],
                              "contacts_last_step": other["contacts"], "rebuilds_timed": other["rebuilds_timed"],
+                             "rebuilds_timed_from_candidate_list": other["rebuilds_timed_filtered"],
                              "roofline": other["roofline"], "gpu_launches": other["launches"],
                              "tuning": other["tuning"],
                              "clocks": other["clocks"]}
@@ -700,7 +704,9 @@ def run_ours(args):
                              "note": "the placement as placed (40 % solids): no contacts within the timed steps",
                              "value": rsa40["value"], "ms_per_step": rsa40["ms"] / args.steps,
                              "contacts_last_step": rsa40["contacts"], "n_pairs": rsa40["pairs"],
-                             "rebuilds_timed": rsa40["rebuilds_timed"], "roofline": rsa40["roofline"],
+                             "rebuilds_timed": rsa40["rebuilds_timed"],
+                             "rebuilds_timed_from_candidate_list": rsa40["rebuilds_timed_filtered"],
+                             "roofline": rsa40["roofline"],
                              "gpu_launches": rsa40["launches"], "clocks": rsa40["clocks"]}
         if batched is not None:
             b = batched

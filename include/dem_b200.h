@@ -130,7 +130,10 @@ typedef struct dem_stats {
     double  s_time;          /* accumulated solids time S_TIME */
     int64_t n_outflow_removed; /* particles deleted by outflow boundaries so far */
     int64_t n_inflow_added;    /* particles seeded by mass-inflow boundaries so far */
-    double  reserved[2];
+    int64_t n_candidate_lists; /* candidate lists the pair build made so far (single
+                                  systems without flow boundaries; no counterpart) */
+    int64_t n_builds_filtered; /* pair builds that filtered a candidate list instead
+                                  of scanning the DES grid (no counterpart) */
 } dem_stats;
 
 typedef struct dem_handle dem_handle;
@@ -172,8 +175,10 @@ int dem_set_walls(dem_handle* h, const double* vertex, const double* norm_face,
  * solids phase PIJK(:,5). (model/des/discretelement_mod.f:387-391,579-588)
  * After a first full upload, radius, pmass, omoi, state and phase may each
  * be NULL: the handle keeps its own (a driver that changed only positions,
- * velocities and spins sends those).  The host arrays may be reused when
- * the call returns. */
+ * velocities and spins sends those).  Such a motion-only upload adds the
+ * largest move of a particle to the bound the pair build and the gap
+ * screens keep; any other upload clears them until the next build.  The
+ * host arrays may be reused when the call returns. */
 int dem_upload_state(dem_handle* h, const double* pos, const double* vel,
                      const double* omega, const double* radius,
                      const double* pmass, const double* omoi,
@@ -668,7 +673,8 @@ typedef struct dem_batch_limits {
 typedef struct dem_memory {
     int64_t array_bytes;       /* the arrays sized by the particle, cell, facet and system
                                   counts (state, histories, grids, work arrays, tables) */
-    int64_t pair_bytes;        /* the pair-list arrays at their capacity */
+    int64_t pair_bytes;        /* the pair-list arrays at their capacity (with the
+                                  pair build's candidate list on a single system) */
     int64_t scratch_bytes;     /* scan and staging scratch held now (grows on demand) */
     int64_t pair_capacity;     /* pairs the pair-list arrays hold */
     int64_t pairs;             /* pairs of the current list */

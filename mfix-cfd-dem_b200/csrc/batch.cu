@@ -208,6 +208,7 @@ int dem_batch_footprint(const dem_params* q, const dem_batch_limits* lim, dem_me
   dem_handle tmp;
   tmp.prm = *q;
   tmp.n = lim->max_particles;
+  tmp.sys.resize(lim->max_systems);  // a batch: its arrays, not a single handle's
   fill_devparams(tmp.prm, tmp.n, tmp.dp);
   long long bytes = 0;
   auto S = [&](void**, size_t b) { bytes += (long long)(b > 0 ? b : 8); };

@@ -39,6 +39,22 @@ __global__ void k_pack_keepw(int n, const double* __restrict__ v3, double4* __re
   double4 o = out[i];
   out[i] = make_double4(v3[i], v3[(size_t)n + i], v3[2 * (size_t)n + i], o.w);
 }
+// Positions of a motion-only upload: as k_pack_keepw, and each existing
+// particle's move notes its length in the displacement bound's slots, so
+// the bound (pair and wall gaps, candidate list) stays valid without a
+// rebuild.
+__global__ void k_pack_moved(int n, const double* __restrict__ v3, double4* __restrict__ out,
+                             const int8_t* __restrict__ state, unsigned* __restrict__ vslot) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 o = out[i];
+  const double x = v3[i], y = v3[(size_t)n + i], z = v3[2 * (size_t)n + i];
+  out[i] = make_double4(x, y, z, o.w);
+  if (state[i] != DEM_STATE_NONEXISTENT) {
+    const double dx = x - o.x, dy = y - o.y, dz = z - o.z;
+    note_displacement(vslot, sqrt(dx * dx + dy * dy + dz * dz));
+  }
+}
 __global__ void k_unpack(int n, const double4* __restrict__ in, double* __restrict__ v3) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -172,9 +188,10 @@ static void prof_collect(dem_handle* h) {
 // Particles [off, off + cnt) from Fortran-layout host arrays with cnt rows.
 int upload_range(dem_handle* h, int off, int cnt, int nph, const double* pos, const double* vel,
                  const double* omega, const double* radius, const double* pmass, const double* omoi,
-                 const int8_t* state, const int32_t* phase) {
+                 const int8_t* state, const int32_t* phase, bool note_moves) {
   // radius, pmass, omoi, state and phase may be NULL: the device keeps its
-  // values of those (the callers check that there are some)
+  // values of those (the callers check that there are some); note_moves
+  // (with radius and state NULL) notes the moves in the displacement slots
   if (!pos || !vel || !omega) return set_err(h, DEM_ERR_ARG, "null array");
   if (cnt <= 0) return 0;
   const size_t n = (size_t)cnt;
@@ -191,6 +208,8 @@ int upload_range(dem_handle* h, int off, int cnt, int nph, const double* pos, co
     if (scal[a]) {
       cudaMemcpyAsync(st + 9 * n + n * a, scal[a], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
       k_pack<<<B, T, 0, h->stream>>>(cnt, st + 3 * n * a, st + 9 * n + n * a, dst[a]);
+    } else if (a == 0 && note_moves && !state) {
+      k_pack_moved<<<B, T, 0, h->stream>>>(cnt, st, dst[0], h->state + off, h->vslot);
     } else {
       k_pack_keepw<<<B, T, 0, h->stream>>>(cnt, st + 3 * n * a, dst[a]);
     }
@@ -467,7 +486,7 @@ int dem_memory_info(dem_handle* h, dem_memory* out) {
   memset(out, 0, sizeof *out);
   out->array_bytes = h->arr_bytes;
   out->pair_capacity = h->pair_cap;
-  out->pair_bytes = pair_array_bytes(h->pair_cap);
+  out->pair_bytes = pair_array_bytes(h->pair_cap) + (long long)sizeof(int) * h->cand_cap;
   out->scratch_bytes = (int64_t)(h->scan_tmp_elems * sizeof(int) + h->stage_bytes);
   out->pairs = host_pairs(h);
   return fetch_errors(h);
@@ -510,7 +529,7 @@ int dem_destroy(dem_handle* h) {
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
                   h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflagb[0], h->pflagb[1], h->in_pos, h->in_flag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->d_ibc, h->pic_fresh, h->d_seed, h->skin, h->vslot, h->pgap,
-                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->long_rows, h->d_np,
+                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->long_rows, h->cand_end, h->cand_cnt, h->cand_start, h->cand_fill, h->qof, h->cand_nb, h->cand, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -564,8 +583,14 @@ int dem_upload_state(dem_handle* h, const double* pos, const double* vel, const 
   if (max_pip != h->n) return set_err(h, DEM_ERR_ARG, "max_pip does not match dem_create");
   if ((!radius || !pmass || !omoi || !state || !phase) && !h->have_state)
     return set_err(h, DEM_ERR_ARG, "the first upload needs every array");
-  if (int rc = upload_range(h, 0, h->n, h->dp.nph, pos, vel, omega, radius, pmass, omoi, state, phase)) return rc;
-  skin_unknown(h);  // positions changed from outside: no pair is known apart until the next build
+  // A motion-only upload (radius, mass, inertia, state and phase kept) adds
+  // the largest move to the displacement bound; any other upload leaves no
+  // pair known apart until the next build.
+  const bool motion = h->have_state && !radius && !pmass && !omoi && !state && !phase;
+  if (int rc = upload_range(h, 0, h->n, h->dp.nph, pos, vel, omega, radius, pmass, omoi, state, phase, motion))
+    return rc;
+  if (motion) launch_skin(h);
+  else skin_unknown(h);
   h->have_state = true;
   return 0;
 }
@@ -875,6 +900,8 @@ int dem_get_stats(dem_handle* h, dem_stats* s) {
   s->n_rogue_removed = (int64_t)h->herr->rogue_removed;
   s->n_outflow_removed = (int64_t)h->herr->outflow_removed;
   s->n_inflow_added = (int64_t)h->inflow_added;
+  s->n_candidate_lists = (int64_t)h->herr->cand_lists;
+  s->n_builds_filtered = (int64_t)h->herr->cand_filtered;
   s->steps_done = h->steps_done;
   s->s_time = h->s_time;
   return 0;
@@ -929,6 +956,8 @@ int dem_get_stats_noalloc(dem_handle* h, dem_stats* s) {
   s->n_rogue_removed = (int64_t)h->herr->rogue_removed;
   s->n_outflow_removed = (int64_t)h->herr->outflow_removed;
   s->n_inflow_added = (int64_t)h->inflow_added;
+  s->n_candidate_lists = (int64_t)h->herr->cand_lists;
+  s->n_builds_filtered = (int64_t)h->herr->cand_filtered;
   s->steps_done = h->steps_done;
   s->kinetic_energy = sum[6];
   s->bed_height = sum[4] > 0 ? sum[5] / sum[4] : 0.0;

@@ -52,6 +52,19 @@ enum : uint8_t {
   PF_HIST    = 2,   // its tangential history PFT is nonzero
 };
 
+// The candidate list of a single-system handle's pair build (neighbor.cu):
+// pairs within the search radius plus a skin, kept while the displacement
+// bound since its build stays within half the skin.
+struct CandState {
+  double disp;  // displacement bound since the list was built
+  int have;     // the list is complete (built, within its capacity)
+  int ok;       // this build filters the list (set at the start of each build)
+  int build;    // this build makes a new list
+  int total;    // entries of the last list build
+  int uses;     // builds that filtered the current list
+  int cool;     // builds left before the next list is made (after one expired unused)
+};
+
 struct DevErr {
   unsigned flags;
   int first_rogue;   // smallest rogue particle index of the last build (n if none)
@@ -60,7 +73,8 @@ struct DevErr {
   unsigned long long n_wall_contacts;
   unsigned long long rogue_removed;
   unsigned long long outflow_removed;
-  int pad[2];
+  int cand_lists;     // candidate lists built (complete) so far
+  int cand_filtered;  // pair builds that filtered a candidate list so far
 };
 
 // Parameters as kernels see them (passed by value).
@@ -221,6 +235,18 @@ struct dem_handle {
   int4* sinfo = nullptr;      // n: (particle, packed DES cell (i,j,k), state, search cell) in that order
   uint32_t* nslot = nullptr;  // n * NSLOT: rows kept by the count pass of the pair build, by particle
   int* long_rows = nullptr;   // n + 1: sorted-copy places of the rows longer than NSLOT, count at [n]
+  // candidate list (single-system handles): cand_end[i] ends particle i's
+  // candidates in cand_nb (particle indices); cand_cnt / cand_start /
+  // cand_fill are build scratch, qof[i] the particle's place in the sorted
+  // copy (-1 when not in it)
+  int* cand_end = nullptr;
+  int* cand_cnt = nullptr;
+  int* cand_start = nullptr;
+  int* cand_fill = nullptr;
+  int* qof = nullptr;
+  int* cand_nb = nullptr;
+  long long cand_cap = 0;
+  demb::CandState* cand = nullptr;
 
   // pairs
   long long pair_cap = 0;
@@ -358,7 +384,7 @@ void launch_pairs_split(dem_handle* h);         // force_split.cu
 void launch_gather_split(dem_handle* h, int mode);
 int ensure_pair_capacity(dem_handle* h, long long need);
 int build_transpose(dem_handle* h, int nb);    // neighbor.cu
-void launch_neigh_count(dem_handle* h);        // neighbor.cu: count pass of the pair build
+void launch_neigh_count(dem_handle* h, const int* skip = nullptr);        // neighbor.cu: count pass of the pair build
 void set_hist_flags(dem_handle* h);            // neighbor.cu: PF_HIST from the current history
 void launch_skin(dem_handle* h);               // force.cu: adds the step's displacement to the bound
 void skin_unknown(dem_handle* h);              // force.cu: positions changed from outside: no pair skipped
@@ -429,10 +455,18 @@ void handle_arrays(dem_handle* h, size_t n, size_t nc, size_t nfc, F&& A) {
   A((void**)&h->vslot, sizeof(unsigned) * 32);
   A((void**)&h->derr, sizeof(DevErr));
   A((void**)&h->d_np, sizeof(int));
+  if (!h->batch()) {
+    A((void**)&h->cand_end, sizeof(int) * n);
+    A((void**)&h->cand_cnt, sizeof(int) * n);
+    A((void**)&h->cand_start, sizeof(int) * (n + 1));
+    A((void**)&h->cand_fill, sizeof(int) * n);
+    A((void**)&h->qof, sizeof(int) * n);
+    A((void**)&h->cand, sizeof(CandState));
+  }
 }
 int upload_range(dem_handle* h, int off, int cnt, int nph, const double* pos, const double* vel,
                  const double* omega, const double* radius, const double* pmass, const double* omoi,
-                 const int8_t* state, const int32_t* phase);
+                 const int8_t* state, const int32_t* phase, bool note_moves = false);
 int download_range(dem_handle* h, int off, int cnt, double* pos, double* vel, double* omega, int8_t* state);
 int stats_range(dem_handle* h, int off, int cnt, dem_stats* s);
 // walls.cu: facets of batch system `sys` binned to its DES cells

@@ -966,22 +966,27 @@ static void launch_force_kernels(dem_handle* h, int mode, bool split) {
 
 // Displacement bound since the last build += this step's largest particle
 // displacement bound; the slots are cleared for the next step.
-__global__ void k_skin(double* __restrict__ skin, unsigned* __restrict__ vslot) {
+__global__ void k_skin(double* __restrict__ skin, unsigned* __restrict__ vslot, CandState* __restrict__ cand) {
   const unsigned m = __reduce_max_sync(0xffffffffu, vslot[threadIdx.x]);
   vslot[threadIdx.x] = 0;
-  if (threadIdx.x == 0) skin[0] = skin[0] + (double)__uint_as_float(m);
+  if (threadIdx.x == 0) {
+    skin[0] = skin[0] + (double)__uint_as_float(m);
+    if (cand) cand->disp = cand->disp + (double)__uint_as_float(m);  // the candidate list's bound too
+  }
 }
 
 __global__ void k_set_skin(double* __restrict__ skin, double v) { skin[0] = v; }
 
 void launch_skin(dem_handle* h) {
-  k_skin<<<1, 32, 0, h->stream>>>(h->skin, h->vslot);
+  k_skin<<<1, 32, 0, h->stream>>>(h->skin, h->vslot, h->cand);
   DEM_LAUNCH(h);
 }
 
 void skin_unknown(dem_handle* h) {
   k_set_skin<<<1, 1, 0, h->stream>>>(h->skin, HUGE_VAL);
   DEM_LAUNCH(h);
+  // positions (or walls) changed from outside: the candidate list starts over
+  if (h->cand) cudaMemsetAsync(&h->cand->have, 0, sizeof(int), h->stream);
 }
 
 int run_force(dem_handle* h, bool fused) {

@@ -97,10 +97,11 @@ __global__ void k_sorted_copy(DevParams p0, BatchView bv, int n, const int* __re
                               const int* __restrict__ flist, const double4* __restrict__ pos4,
                               const int8_t* __restrict__ state, const int* __restrict__ dg_pijk,
                               const int* __restrict__ fkey, double4* __restrict__ spos, float4* __restrict__ sposf,
-                              int4* __restrict__ sinfo) {
+                              int4* __restrict__ sinfo, int* __restrict__ qof) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n || q >= *n_exist) return;
   const int i = flist[q];
+  if (qof) qof[i] = q;
   const DevParams& p = sysp<B>(p0, bv, i);
   const int c = dg_pijk[i];
   const double4 x = pos4[i];
@@ -153,7 +154,8 @@ __device__ __forceinline__ void neigh_frame_exact(const DevParams& p, const int4
 }
 
 // The whole frame of a particle that scans candidates.
-__device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, const double4& cp, NeighFrame& F) {
+__device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, const double4& cp, NeighFrame& F,
+                                            double extra = 0.0) {
   neigh_frame_exact(p, me, cp, F);
   F.cpf = make_float4((float)cp.x, (float)cp.y, (float)cp.z, (float)cp.w);
   F.frf = (float)p.factor_rlm;
@@ -168,7 +170,7 @@ __device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, 
   // bounds the error of the distance.  A period below four search radii
   // could let FP32 pick another image: the check is off there.
   {
-    const float srm = (float)(p.factor_rlm * (cp.w + p.max_radius)) * 1.0001f;
+    const float srm = (float)(p.factor_rlm * (cp.w + p.max_radius) + extra) * 1.0001f;
     float tol = 0.f;
     bool off = false;
     for (int ax = 0; ax < 3; ++ax) {
@@ -185,7 +187,7 @@ __device__ __forceinline__ void neigh_frame(const DevParams& p, const int4& me, 
   // axis (the whole axis when the range covers it); a margin of 1e-4 of the
   // reach covers the rounding of the cell index
   const double cpos[3] = {cp.x, cp.y, cp.z};
-  const double reach = F.fr * (cp.w + p.max_radius);
+  const double reach = F.fr * (cp.w + p.max_radius) + extra;
   F.wrap = false;
   for (int ax = 0; ax < 3; ++ax) {
     F.glo[ax] = 0; F.ghi[ax] = 0;
@@ -390,8 +392,9 @@ __global__ void __launch_bounds__(128, 8)
 k_neigh_count(DevParams p0, BatchView bv, const int* __restrict__ n_exist, const double4* __restrict__ spos,
               const float4* __restrict__ sposf, const int4* __restrict__ sinfo, const int* __restrict__ fstart,
               const DevErr* __restrict__ err, int* __restrict__ row_cnt, uint32_t* __restrict__ nslot,
-              int* __restrict__ long_rows) {
+              int* __restrict__ long_rows, const int* __restrict__ skip) {
   __shared__ int s_surv[NSURV * 128];
+  if (skip && *skip) return;  // this build filters the candidate list instead
   const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (q0 >= p0.n || q0 >= *n_exist) return;
   const int4 me = sinfo[q0];
@@ -470,6 +473,164 @@ __device__ __forceinline__ void place_keys(const uint32_t* __restrict__ slot, in
       const long long s = start + r;
       if (s < cap) { nbrs[s] = (int)(k[c] & 0x7ffffffu); owner[s] = i; }
     }
+  }
+}
+
+// ---- candidate list (single-system handles) --------------------------------
+// Between two builds of the list, a build filters it instead of scanning the
+// grid.  The list holds, for each particle's row, every particle within the
+// search radius FACTOR_RLM*(r_l + r_i) plus the skin at the time it was
+// built (nearest image, the half-list rules of DESGRID_NEIGH_BUILD, no
+// stencil).  A pair in the reference's list now is within the search radius
+// now, and each of its particles has moved at most the displacement bound
+// since the list was built, so while twice that bound stays within the skin
+// the pair is in the list.  The filter gives each entry the exact test of
+// the scan (neigh_exact, in the owner's frame: stencil, periodic image, FP64
+// distance, stencil rank), so the rows are the scan's.  The choice is made
+// on the device at the start of each build (k_cand_decide), so a captured
+// period holds both paths: the count pass and the list build return at once
+// when the list is filtered, the filter when it is not.
+
+// A list that expires before any build filtered it (particles moving fast)
+// cost two scans for nothing: the next CAND_COOL builds make none.
+constexpr int CAND_COOL = 4;
+__global__ void k_cand_decide(CandState* __restrict__ cs, DevErr* __restrict__ err, double half_skin) {
+  if (cs->have && cs->disp <= half_skin) {
+    cs->ok = 1;
+    cs->build = 0;
+    cs->uses += 1;
+    err->cand_filtered += 1;
+    return;
+  }
+  cs->ok = 0;
+  if (cs->have && cs->uses == 0) cs->cool = CAND_COOL;
+  if (cs->cool > 0) {
+    cs->cool -= 1;
+    cs->build = 0;
+  } else {
+    cs->build = 1;
+  }
+  cs->have = 0;
+  cs->uses = 0;
+}
+
+// The rows from the candidate list: row count, the first NSLOT keys in the
+// slots, longer rows into the long-row list (as the count pass leaves them).
+__global__ void __launch_bounds__(128)
+k_cand_filter(DevParams p, const int* __restrict__ n_exist, const double4* __restrict__ spos,
+              const int4* __restrict__ sinfo, const int* __restrict__ qof, const DevErr* __restrict__ err,
+              const int* __restrict__ cand_end, const int* __restrict__ cand_nb, const CandState* __restrict__ cs,
+              int* __restrict__ row_cnt, uint32_t* __restrict__ nslot, int* __restrict__ long_rows) {
+  if (!cs->ok) return;
+  const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q0 >= p.n || q0 >= *n_exist) return;
+  const int4 me = sinfo[q0];
+  const int cur = me.x;
+  if (me.z != DEM_STATE_NORMAL || cur >= err->first_rogue) return;
+  NeighFrame F;
+  neigh_frame_exact(p, me, spos[q0], F);
+  const int s = cur ? cand_end[cur - 1] : 0, e = cand_end[cur];
+  int cnt = 0;
+  for (int c = s; c < e; ++c) {
+    const int q = qof[cand_nb[c]];
+    if (q < 0) continue;  // not in the sorted copy: NONEXISTENT
+    uint32_t key;
+    if (!neigh_exact(p, F, sinfo, spos, q, &key)) continue;
+    if (cnt < NSLOT) nslot[(size_t)cur * NSLOT + cnt] = key;
+    ++cnt;
+  }
+  row_cnt[cur] = cnt;
+  if (cnt > NSLOT) {
+    const int t = atomicAdd(&long_rows[p.n], 1);
+    if (t < p.n) long_rows[t] = q0;
+  }
+}
+
+// Count (FILL = false) and fill pass of a list build (when k_cand_decide
+// asks for one): the half scan of
+// k_neigh_count over a reach widened by the skin, each pair within the
+// search radius plus the skin of its nearest image entered in its owner's
+// row (any NORMAL owner: the rogue limit of a build is applied when the
+// list is filtered).  The fill places entries at cand_start[owner] + an
+// atomic slot; their order within a row does not matter.
+template <bool FILL>
+__global__ void __launch_bounds__(128, 8)
+k_cand_build(DevParams p, const int* __restrict__ n_exist, const double4* __restrict__ spos,
+             const float4* __restrict__ sposf, const int4* __restrict__ sinfo, const int* __restrict__ fstart,
+             const CandState* __restrict__ cs, double skin, int* __restrict__ cand_cnt, int* __restrict__ cand_fill,
+             const int* __restrict__ cand_start, int* __restrict__ cand_nb, long long cap) {
+  __shared__ int s_surv[NSURV * 128];
+  if (!cs->build) return;
+  const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q0 >= p.n || q0 >= *n_exist) return;
+  const int4 me = sinfo[q0];
+  if (me.z == DEM_STATE_NONEXISTENT) return;
+  const int cur = me.x;
+  const bool me_normal = me.z == DEM_STATE_NORMAL;
+  NeighFrame F;
+  neigh_frame(p, me, spos[q0], F, skin);
+  PreFrame G = pre_frame(F);
+  G.b.y = __fadd_ru(G.b.y, __double2float_ru(skin));  // the allowance also covers the skin
+  auto enter = [&](int q) {
+    const int4 o = sinfo[q];
+    if (o.z == DEM_STATE_NONEXISTENT) return;
+    const bool o_normal = o.z == DEM_STATE_NORMAL;
+    bool mine;
+    if (me_normal && o_normal) mine = cur < o.x;
+    else if (me_normal || o_normal) mine = me_normal;
+    else return;
+    const double4 b = spos[q];
+    double e[3] = {F.cp.x - b.x, F.cp.y - b.y, F.cp.z - b.z};
+    for (int ax = 0; ax < 3; ++ax)
+      if (F.inv_l[ax] != 0.0) e[ax] = e[ax] - p.L[ax] * rint(e[ax] * F.inv_l[ax]);
+    const double r = F.fr * (F.cp.w + b.w) + skin;
+    if (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] > r * r * (1.0 + 1e-9)) return;
+    const int oi = mine ? cur : o.x;
+    if (!FILL) {
+      atomicAdd(&cand_cnt[oi], 1);
+    } else {
+      const long long at = (long long)cand_start[oi] + atomicAdd(&cand_fill[oi], 1);
+      if (at < cap) cand_nb[at] = mine ? o.x : cur;
+    }
+  };
+  int ns = 0;
+  auto flush = [&]() {
+    for (int s = 0; s < ns; ++s) enter(s_surv[s * blockDim.x + threadIdx.x]);
+    ns = 0;
+  };
+  for_runs<true>(p, F, fstart, q0, me.w, [&](int qs, int qe) {
+    if (F.wrap) {
+      for (int q = qs; q < qe; ++q) {
+        if (!pre_test(G, sposf[q])) continue;
+        s_surv[ns * blockDim.x + threadIdx.x] = q;
+        if (++ns == NSURV) flush();
+      }
+    } else {
+      for (int q = qs; q < qe; ++q) {
+        if (!pre_direct(G, sposf[q])) continue;
+        s_surv[ns * blockDim.x + threadIdx.x] = q;
+        if (++ns == NSURV) flush();
+      }
+    }
+  });
+  flush();
+}
+
+// The list's row ends from the counts and the scan; it is complete when its
+// entries fit the capacity, and the displacement bound restarts.
+__global__ void k_cand_commit(int n, const int* __restrict__ cand_cnt, const int* __restrict__ cand_start,
+                              int* __restrict__ cand_end, CandState* __restrict__ cs, DevErr* __restrict__ err,
+                              long long cap) {
+  if (!cs->build) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) cand_end[i] = cand_start[i] + cand_cnt[i];
+  if (i == 0) {
+    const int total = cand_start[n];
+    cs->total = total;
+    cs->have = (long long)total <= cap ? 1 : 0;
+    if (!cs->have) cs->cool = CAND_COOL;  // no retry at every build
+    else err->cand_lists += 1;
+    cs->disp = 0.0;
   }
 }
 
@@ -767,6 +928,21 @@ long long pair_array_bytes(long long cap) {
          (long long)(sizeof(int2) + sizeof(int) + sizeof(PairRec) + sizeof(float) + sizeof(int)) * cap + cap + 16;
 }
 
+// The candidate list's array for at least `need` entries, a quarter over
+// so that a list that grows a little does not reallocate at every build.
+static int ensure_cand_capacity(dem_handle* h, long long need) {
+  if (need <= h->cand_cap) return 0;
+  const long long cap = need + need / 4 + 1024;
+  int* cnb = nullptr;
+  if (int rc = check_cuda(h, cudaMalloc(&cnb, sizeof(int) * cap), "cudaMalloc candidates")) return rc;
+  cudaStreamSynchronize(h->stream);
+  cudaFree(h->cand_nb);
+  h->cand_nb = cnb;
+  h->cand_cap = cap;
+  invalidate_graphs(h);  // captured builds point at the old array
+  return check_cuda(h, cudaGetLastError(), "grow candidates");
+}
+
 // Pair-list arrays for at least `need` pairs: the first allocation takes
 // exactly `need`, a later one doubles the capacity until it fits.
 int ensure_pair_capacity(dem_handle* h, long long need) {
@@ -816,7 +992,7 @@ int ensure_pair_capacity(dem_handle* h, long long need) {
 // Count pass of the pair build over the current cell-sorted copy: row_cnt
 // and the long-row list start from zero, so the pass can be launched again
 // on its own (the autotuner times it).
-void launch_neigh_count(dem_handle* h) {
+void launch_neigh_count(dem_handle* h, const int* skip) {
   const int n = h->nl(), T = h->tune.neigh_threads, B = (n + T - 1) / T;
   const bool bt = h->batch();
   const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : h->dp.nfcell);
@@ -824,10 +1000,10 @@ void launch_neigh_count(dem_handle* h) {
   cudaMemsetAsync(h->long_rows + h->n, 0, sizeof(int), h->stream);  // the count, at [capacity]
   if (bt)
     k_neigh_count<true><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo,
-                                                h->fcell_start, h->derr, h->row_cnt, h->nslot, h->long_rows);
+                                                h->fcell_start, h->derr, h->row_cnt, h->nslot, h->long_rows, skip);
   else
     k_neigh_count<false><<<B, T, 0, h->stream>>>(h->dp, h->bview(), n_exist, h->spos, h->sposf, h->sinfo,
-                                                 h->fcell_start, h->derr, h->row_cnt, h->nslot, h->long_rows);
+                                                 h->fcell_start, h->derr, h->row_cnt, h->nslot, h->long_rows, skip);
   DEM_LAUNCH(h);
 }
 
@@ -847,14 +1023,31 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   DEM_LAUNCH(h);
   const int nb = 1 - h->rb;  // new list goes into the other buffer
   const int* n_exist = h->fcell_start + (bt ? h->nfcell_total : p.nfcell);
+  // the candidate list serves single systems without flow boundaries (their
+  // seeding and deletion change particle states, and with them the rules of
+  // the half list); with them it is dropped
+  const bool cand = !bt && h->cand && h->obc.empty() && h->ibc.empty();
+  const double skin_c = 0.1 * p.factor_rlm * p.max_radius;
+  if (cand) {
+    k_cand_decide<<<1, 1, 0, h->stream>>>(h->cand, e, 0.5 * skin_c);
+    DEM_LAUNCH(h);
+  } else if (h->cand) {
+    cudaMemsetAsync(&h->cand->have, 0, sizeof(int), h->stream);
+  }
+  if (h->qof) cudaMemsetAsync(h->qof, 0xff, sizeof(int) * n, h->stream);
   if (bt)
     k_sorted_copy<true><<<B, T, 0, h->stream>>>(p, bv, n, n_exist, h->fcell_list, h->pos4[h->cur], h->state,
-                                                h->dg_pijk, h->fcell_key, h->spos, h->sposf, h->sinfo);
+                                                h->dg_pijk, h->fcell_key, h->spos, h->sposf, h->sinfo, nullptr);
   else
     k_sorted_copy<false><<<B, T, 0, h->stream>>>(p, bv, n, n_exist, h->fcell_list, h->pos4[h->cur], h->state,
-                                                 h->dg_pijk, h->fcell_key, h->spos, h->sposf, h->sinfo);
+                                                 h->dg_pijk, h->fcell_key, h->spos, h->sposf, h->sinfo, h->qof);
   DEM_LAUNCH(h);
-  launch_neigh_count(h);
+  launch_neigh_count(h, cand ? &h->cand->ok : nullptr);
+  if (cand) {
+    k_cand_filter<<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sinfo, h->qof, e, h->cand_end, h->cand_nb, h->cand,
+                                          h->row_cnt, h->nslot, h->long_rows);
+    DEM_LAUNCH(h);
+  }
   if (bt) {
     k_keep_rows<false><<<B, T, 0, h->stream>>>(n, h->n_built, bv, h->row_end[h->rb], h->nbrs[h->rb], h->row_cnt, nullptr,
                                                nullptr, nullptr, 0);
@@ -938,6 +1131,33 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   h->pcur = pn;
   h->have_pairs = true;
   launch_wall_gaps(h);
+  if (cand) {
+    // a new candidate list when k_cand_decide asks for one (each kernel
+    // returns at once otherwise)
+    cudaMemsetAsync(h->cand_cnt, 0, sizeof(int) * n, h->stream);
+    k_cand_build<false><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, h->cand,
+                                                skin_c, h->cand_cnt, h->cand_fill, h->cand_start, h->cand_nb,
+                                                h->cand_cap);
+    DEM_LAUNCH(h);
+    if (int rc = exclusive_scan(h, h->cand_cnt, h->cand_start, n, h->cand_start + n)) return rc;
+    if (!h->capturing) {
+      // eager builds read the list's length back (0 when none is made) and
+      // grow its array when needed; a captured build that overflows leaves
+      // the list incomplete, unused
+      int total = 0;
+      if (int rc = check_cuda(h, cudaMemcpyAsync(&total, h->cand_start + n, sizeof(int), cudaMemcpyDeviceToHost,
+                                                 h->stream), "copy candidates")) return rc;
+      if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
+      if (int rc = ensure_cand_capacity(h, total)) return rc;
+    }
+    const long long cap = h->cand_cap;
+    cudaMemsetAsync(h->cand_fill, 0, sizeof(int) * n, h->stream);
+    k_cand_build<true><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, h->cand,
+                                               skin_c, h->cand_cnt, h->cand_fill, h->cand_start, h->cand_nb, cap);
+    DEM_LAUNCH(h);
+    k_cand_commit<<<B, T, 0, h->stream>>>(n, h->cand_cnt, h->cand_start, h->cand_end, h->cand, e, cap);
+    DEM_LAUNCH(h);
+  }
   if (side) {
     cudaStreamWaitEvent(h->stream, h->ev_join, 0);
     return trc;

@@ -113,7 +113,8 @@ class DemStats(C.Structure):
         ("s_time", C.c_double),
         ("n_outflow_removed", C.c_int64),
         ("n_inflow_added", C.c_int64),
-        ("reserved", C.c_double * 2),
+        ("n_candidate_lists", C.c_int64),
+        ("n_builds_filtered", C.c_int64),
     ]
 
     def as_dict(self):

@@ -1626,19 +1626,26 @@ int orc_upload_state(orc_handle* h, const double* pos, const double* vel, const 
                      const int8_t* state, const int32_t* phase, int32_t max_pip) {
   Oracle& o = h->o;
   if (max_pip != o.n) return o.fail(DEM_ERR_ARG, "max_pip mismatch");
+  if (!pos || !vel || !omega) return o.fail(DEM_ERR_ARG, "null array");
+  // after a first full upload, radius, pmass, omoi, state and phase may be
+  // NULL: the handle keeps its own (as dem_upload_state)
+  if ((!radius || !pmass || !omoi || !state || !phase) && !o.have_state)
+    return o.fail(DEM_ERR_ARG, "the first upload needs every array");
   size_t n3 = (size_t)3 * o.n;
   std::copy(pos, pos + n3, o.pos.begin());
   std::copy(vel, vel + n3, o.vel.begin());
   std::copy(omega, omega + n3, o.omg.begin());
-  std::copy(radius, radius + o.n, o.rad.begin());
-  std::copy(pmass, pmass + o.n, o.pmass.begin());
-  std::copy(omoi, omoi + o.n, o.omoi.begin());
-  std::copy(state, state + o.n, o.state.begin());
-  for (int i = 0; i < o.n; ++i) {
-    int ph = phase[i] - 1;
-    if (o.state[i] != DEM_STATE_NONEXISTENT && (ph < 0 || ph >= o.p.n_phases))
-      return o.fail(DEM_ERR_ARG, "phase out of range");
-    o.phase[i] = ph < 0 ? 0 : ph;
+  if (radius) std::copy(radius, radius + o.n, o.rad.begin());
+  if (pmass) std::copy(pmass, pmass + o.n, o.pmass.begin());
+  if (omoi) std::copy(omoi, omoi + o.n, o.omoi.begin());
+  if (state) std::copy(state, state + o.n, o.state.begin());
+  if (phase) {
+    for (int i = 0; i < o.n; ++i) {
+      int ph = phase[i] - 1;
+      if (o.state[i] != DEM_STATE_NONEXISTENT && (ph < 0 || ph >= o.p.n_phases))
+        return o.fail(DEM_ERR_ARG, "phase out of range");
+      o.phase[i] = ph < 0 ? 0 : ph;
+    }
   }
   o.have_state = true;
   return 0;

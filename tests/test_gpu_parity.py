@@ -215,6 +215,27 @@ def test_long_rows_and_long_incoming_lists_match_oracle(periodic):
     assert compare_pairs(g, o) == 0.0
 
 
+@pytest.mark.parametrize("periodic", [(False, False, False), (True, False, True)])
+def test_pair_builds_from_the_candidate_list_match_oracle(periodic):
+    """Between two grid scans a pair build filters the candidate list (the
+    pairs within the search radius plus a skin of 0.1 FACTOR_RLM MAX_RADIUS
+    when the list was made) until the particles may have moved half the
+    skin; then a build scans the grid and makes a new list.  Spheres at up to
+    1.7 m/s, rebuilt every 5 steps for 300 steps under captured periods:
+    builds of both kinds, and NEIGHBOR_INDEX / NEIGHBORS and the state stay
+    the oracle's, bit for bit, after every fifth build."""
+    case, prm, arr, walls = settling_case(n_side=(8, 12, 8), spacing=1.0, jitter=0.03, coll="HERTZ",
+                                          intg="EULER", nsn=5, vmax=1.0, periodic=periodic)
+    g, o = pair_both(prm, arr, walls)
+    for _ in range(12):
+        g.step(25); o.step(25)
+        compare_state(g, o, exact=True)
+        assert compare_pairs(g, o) == 0.0
+    st = g.stats()
+    assert st["n_builds_filtered"] > 10
+    assert st["n_candidate_lists"] >= 2
+
+
 def test_upload_of_the_moving_state_only():
     """dem_upload_state with only positions, velocities and spins (the
     other arrays NULL) keeps the handle's radius, mass, inertia, state and
@@ -241,3 +262,29 @@ def test_upload_of_the_moving_state_only():
     for key in ("pos", "vel", "omega", "state"):
         assert np.array_equal(sa[key], sb[key]), key
     assert a.stats()["n_contacts"] == b.stats()["n_contacts"] > 0
+
+
+def test_motion_only_uploads_move_the_bound_not_the_list():
+    """A motion-only upload that moves the particles adds the largest move
+    to the displacement bound: small moves keep the candidate list (the
+    build after each filters it), a move past half the skin makes the next
+    build scan the grid for a new list.  The oracle gets the same uploads;
+    state and NEIGHBOR_INDEX / NEIGHBORS stay its own, bit for bit."""
+    case, prm, arr, walls = settling_case(n_side=(8, 12, 8), spacing=1.0, jitter=0.03, coll="HERTZ",
+                                          intg="EULER", nsn=5, vmax=0.1)
+    g, o = pair_both(prm, arr, walls)
+    rng = np.random.default_rng(7)
+    skin = 0.1 * prm.factor_rlm * float(arr["radius"].max())
+    for shift, new_list in ((0.02, 0), (0.02, 0), (0.6, 1), (0.02, 0)):
+        st0 = g.stats()
+        s = o.download_state()
+        # every particle moves by at most shift * skin
+        pos = s["pos"] + rng.uniform(-1.0, 1.0, s["pos"].shape) * (shift * skin / np.sqrt(3.0))
+        g.upload_state(pos, s["vel"], s["omega"])
+        o.upload_state(pos, s["vel"], s["omega"])
+        g.step(5); o.step(5)  # one or two builds
+        compare_state(g, o, exact=True)
+        assert compare_pairs(g, o) == 0.0
+        st1 = g.stats()
+        assert st1["n_candidate_lists"] - st0["n_candidate_lists"] == new_list, shift
+        assert st1["n_builds_filtered"] - st0["n_builds_filtered"] >= 1 - new_list, shift

@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
 KEYS_EXACT = ("n_normal", "n_pairs", "n_contacts", "n_wall_contacts", "n_rogue_removed", "n_outflow_removed",
-              "n_inflow_added", "steps_done")
+              "n_inflow_added", "steps_done", "n_candidate_lists", "n_builds_filtered")
 KEYS_FLOAT = ("mean_vel", "gran_temp", "kinetic_energy", "bed_height", "s_time")
 
 
