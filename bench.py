@@ -388,6 +388,8 @@ def _timed_run(args, prec, stream, barrier, ws, local, with_e2e):
     out = {"value": value, "ms": ms, "n": n, "n_normal": n_normal, "pairs": int(p1), "launches": int(launches),
            "warmup": warm, "tuning": tuning, "window": [warm + 1, warm + args.steps], "rebuilds_timed": rebuilds,
            "rebuilds_timed_filtered": int(st["n_builds_filtered"] - f0),
+           "candidate_list": {"lists_made": int(st["n_candidate_lists"]),
+                              "builds_filtered": int(st["n_builds_filtered"])},
            "roofline": roofline, "clocks": clk, "contacts": int(st["n_contacts"]), "prm": prm, "info": info,
            "force_error": None if ferr0 is None else [ferr0, ferr1]}
 
@@ -680,6 +682,7 @@ def run_ours(args):
                        "contacts_last_step": main["contacts"],
                        "timed_window_nn": main["window"], "rebuilds_timed": main["rebuilds_timed"],
                        "rebuilds_timed_from_candidate_list": main["rebuilds_timed_filtered"],
+                       "candidate_list_since_start": main["candidate_list"],
                        "l2": "inputs larger than L2 (state and pair arrays ~%.0f MB)" % (
                            (main["n"] * 3 * 32 * 2 + main["pairs"] * 100) / 1e6),
                        "parallelism": f"replicas x{ws}"},

@@ -1097,10 +1097,39 @@ int run_neighbour(dem_handle* h, bool carry_history) {
     k_delete_rogue<false><<<B, T, 0, h->stream>>>(p, bv, h->state, h->dg_pijk, h->pos4[h->cur], h->vel4[h->cur],
                                                    h->omg4[h->cur], h->fc, h->tow, h->wall_fid, e);
   DEM_LAUNCH(h);
+  if (cand) {
+    // a new candidate list when k_cand_decide asks for one (each kernel
+    // returns at once otherwise)
+    cudaMemsetAsync(h->cand_cnt, 0, sizeof(int) * n, h->stream);
+    k_cand_build<false><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, h->cand,
+                                                skin_c, h->cand_cnt, h->cand_fill, h->cand_start, h->cand_nb,
+                                                h->cand_cap);
+    DEM_LAUNCH(h);
+    if (int rc = exclusive_scan(h, h->cand_cnt, h->cand_start, n, h->cand_start + n)) return rc;
+    if (!h->capturing) {
+      // eager builds read the list's length back (0 when none is made) and
+      // grow its array when needed; a captured build that overflows leaves
+      // the list incomplete, unused
+      int total = 0;
+      if (int rc = check_cuda(h, cudaMemcpyAsync(&total, h->cand_start + n, sizeof(int), cudaMemcpyDeviceToHost,
+                                                 h->stream), "copy candidates")) return rc;
+      if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
+      if (int rc = ensure_cand_capacity(h, total)) return rc;
+    }
+    const long long cap = h->cand_cap;
+    cudaMemsetAsync(h->cand_fill, 0, sizeof(int) * n, h->stream);
+    k_cand_build<true><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, h->cand,
+                                               skin_c, h->cand_cnt, h->cand_fill, h->cand_start, h->cand_nb, cap);
+    DEM_LAUNCH(h);
+    k_cand_commit<<<B, T, 0, h->stream>>>(n, h->cand_cnt, h->cand_start, h->cand_end, h->cand, e, cap);
+    DEM_LAUNCH(h);
+  }
   // The transpose of the new list and the history carry-over with the gaps
   // read the list and write disjoint arrays: the transpose runs on the side
   // stream beside them and is joined before the build returns (in sequence
-  // when the kernel classes are timed).
+  // when the kernel classes are timed).  Its scan uses the handle's scan
+  // scratch, so nothing on this stream between the fork and the join scans
+  // (the candidate list above is made before the fork).
   const bool side = h->side_stream && !h->prof;
   int trc = 0;
   if (side) {
@@ -1131,33 +1160,6 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   h->pcur = pn;
   h->have_pairs = true;
   launch_wall_gaps(h);
-  if (cand) {
-    // a new candidate list when k_cand_decide asks for one (each kernel
-    // returns at once otherwise)
-    cudaMemsetAsync(h->cand_cnt, 0, sizeof(int) * n, h->stream);
-    k_cand_build<false><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, h->cand,
-                                                skin_c, h->cand_cnt, h->cand_fill, h->cand_start, h->cand_nb,
-                                                h->cand_cap);
-    DEM_LAUNCH(h);
-    if (int rc = exclusive_scan(h, h->cand_cnt, h->cand_start, n, h->cand_start + n)) return rc;
-    if (!h->capturing) {
-      // eager builds read the list's length back (0 when none is made) and
-      // grow its array when needed; a captured build that overflows leaves
-      // the list incomplete, unused
-      int total = 0;
-      if (int rc = check_cuda(h, cudaMemcpyAsync(&total, h->cand_start + n, sizeof(int), cudaMemcpyDeviceToHost,
-                                                 h->stream), "copy candidates")) return rc;
-      if (int rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync")) return rc;
-      if (int rc = ensure_cand_capacity(h, total)) return rc;
-    }
-    const long long cap = h->cand_cap;
-    cudaMemsetAsync(h->cand_fill, 0, sizeof(int) * n, h->stream);
-    k_cand_build<true><<<B, T, 0, h->stream>>>(p, n_exist, h->spos, h->sposf, h->sinfo, h->fcell_start, h->cand,
-                                               skin_c, h->cand_cnt, h->cand_fill, h->cand_start, h->cand_nb, cap);
-    DEM_LAUNCH(h);
-    k_cand_commit<<<B, T, 0, h->stream>>>(n, h->cand_cnt, h->cand_start, h->cand_end, h->cand, e, cap);
-    DEM_LAUNCH(h);
-  }
   if (side) {
     cudaStreamWaitEvent(h->stream, h->ev_join, 0);
     return trc;

@@ -288,3 +288,23 @@ def test_motion_only_uploads_move_the_bound_not_the_list():
         st1 = g.stats()
         assert st1["n_candidate_lists"] - st0["n_candidate_lists"] == new_list, shift
         assert st1["n_builds_filtered"] - st0["n_builds_filtered"] >= 1 - new_list, shift
+
+
+@pytest.mark.parametrize("periodic", [(False, False, False), (True, False, True)])
+def test_candidate_lists_at_multi_tile_sizes_match_oracle(periodic):
+    """4,096 spheres at up to 1.7 m/s (scans of more than one tile, whose
+    scratch the list build and the transpose of the new pair list both
+    use), rebuilt every 5 steps for 200 steps: candidate lists made and
+    filtered, and the state and NEIGHBOR_INDEX / NEIGHBORS stay the
+    oracle's, bit for bit."""
+    case, prm, arr, walls = settling_case(n_side=(16, 16, 16), box=(20e-3, 40e-3, 20e-3), spacing=1.0,
+                                          jitter=0.03, coll="HERTZ", intg="EULER", nsn=5, vmax=1.0,
+                                          periodic=periodic)
+    g, o = pair_both(prm, arr, walls)
+    for _ in range(8):
+        g.step(25); o.step(25)
+        compare_state(g, o, exact=True)
+        assert compare_pairs(g, o) == 0.0
+    st = g.stats()
+    assert st["n_builds_filtered"] > 10
+    assert st["n_candidate_lists"] >= 2
