@@ -1027,7 +1027,7 @@ int run_neighbour(dem_handle* h, bool carry_history) {
   // seeding and deletion change particle states, and with them the rules of
   // the half list); with them it is dropped
   const bool cand = !bt && h->cand && h->obc.empty() && h->ibc.empty();
-  const double skin_c = 0.1 * p.factor_rlm * p.max_radius;
+  const double skin_c = 0.3 * p.factor_rlm * p.max_radius;
   if (cand) {
     k_cand_decide<<<1, 1, 0, h->stream>>>(h->cand, e, 0.5 * skin_c);
     DEM_LAUNCH(h);
