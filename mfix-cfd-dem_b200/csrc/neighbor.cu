@@ -17,7 +17,11 @@
 // come out bit-identical to the serial reference.  PFT_NEIGHBOR is carried
 // over by matching the neighbour id inside the particle's previous row
 // (neighbour.f:77-117).  Finally the transpose (incoming pairs per particle,
-// ascending owner) is built for the deterministic force gather.
+// ascending owner) is built for the deterministic force gather.  On a
+// single system without flow boundaries most builds filter a candidate list
+// (pairs within the search radius plus a skin, made by an earlier scan)
+// instead of scanning the grid, with the same exact test, so the rows are
+// the scan's (section "candidate list" below).
 #include "dem_internal.cuh"
 
 namespace demb {
