@@ -529,7 +529,7 @@ int dem_destroy(dem_handle* h) {
                   h->in_cnt, h->in_start, h->in_fill, h->in_pair, h->pair_owner, h->vertex,
                   h->norm_face, h->ignore_edge, h->fbin_start, h->fbin, h->wall_fid, h->wall_pft,
                   h->scan_tmp, h->derr, h->red, h->stage, h->wall_live, h->wf, h->pflagb[0], h->pflagb[1], h->in_pos, h->in_flag, h->prec, h->touched, h->wall_hit, h->wall_cand, h->wall_list, h->d_nwall, h->wgap, h->d_obc, h->d_ibc, h->pic_fresh, h->d_seed, h->skin, h->vslot, h->pgap,
-                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->long_rows, h->cand_end, h->cand_cnt, h->cand_start, h->cand_fill, h->qof, h->cand_nb, h->cand, h->d_np,
+                  h->fcell_key, h->fcell_cnt, h->fcell_start, h->fcell_list, h->spos, h->sposf, h->sinfo, h->nslot, h->long_rows, h->cand_end, h->cand_cnt, h->cand_start, h->cand_fill, h->qof, h->cand_nb, h->cand, h->slipfix, h->d_np,
                   h->d_sys, h->sys_of, h->d_due, h->d_first_rogue};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (auto& e : h->prof_pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }

@@ -65,6 +65,18 @@ struct CandState {
   int cool;     // builds left before the next list is made (after one expired unused)
 };
 
+// Contacts of a split-precision pair pass whose onset-of-slip test lies
+// near its threshold (force_split.cu): 2 * pair index + 1 when the pair
+// had a history.  The count starts at zero and k_slip_fix, which follows
+// every pass, clears it; past SLIP_FIX_CAP a contact keeps its FP32
+// decision.
+constexpr int SLIP_FIX_CAP = 4096;
+struct SlipFix {
+  unsigned count;
+  unsigned pad;
+  long long pair[SLIP_FIX_CAP];
+};
+
 struct DevErr {
   unsigned flags;
   int first_rogue;   // smallest rogue particle index of the last build (n if none)
@@ -247,6 +259,7 @@ struct dem_handle {
   int* cand_nb = nullptr;
   long long cand_cap = 0;
   demb::CandState* cand = nullptr;
+  demb::SlipFix* slipfix = nullptr;  // split pair pass: contacts near the onset of slip
 
   // pairs
   long long pair_cap = 0;
@@ -455,6 +468,7 @@ void handle_arrays(dem_handle* h, size_t n, size_t nc, size_t nfc, F&& A) {
   A((void**)&h->vslot, sizeof(unsigned) * 32);
   A((void**)&h->derr, sizeof(DevErr));
   A((void**)&h->d_np, sizeof(int));
+  A((void**)&h->slipfix, sizeof(SlipFix));
   if (!h->batch()) {
     A((void**)&h->cand_end, sizeof(int) * n);
     A((void**)&h->cand_cnt, sizeof(int) * n);

@@ -53,9 +53,66 @@ struct Comp3 {  // Neumaier-compensated FP32 sum of a 3-vector
 // ovd = R_LM^2 - d2 come from the contact test in FP64.
 struct PairTerms {
   float fc[3], tf[3], dcl2, dci2, kn, ov;
+  bool near;  // the FP32 onset-of-slip test lies within 1e-4 of its threshold
 };
 
+// The onset-of-slip test of calc_force_dem.f:330-337 in FP64, evaluated as
+// the FP64 kernels do (contact_force), for owner state (xl, vl, wl) and
+// neighbour state (xi, vi, wi) with dist = x_I - x_L and history pin.  The
+// friction law turns the tangential force at the onset of slip (below it
+// -KT*OVERLAP_T - ETAT*VREL_T, above it MEW*|FN| along OVERLAP_T), so a
+// contact whose FP32 test lies within the FP32 error of the threshold takes
+// its branch from this test (k_slip_fix).
 template <int COLL>
+__device__ __forceinline__ bool slip_fp64(const DevParams& p, const double4& xl, const double4& vl,
+                                          const double4& wl, const double4& xi, const double4& vi,
+                                          const double4& wi, int ix, const double dist[3], double d2,
+                                          const double pin[3]) {
+  const double rl = xl.w, ri = xi.w;
+  const double dmag = sqrt(d2);
+  const double nrm[3] = {dist[0] / dmag, dist[1] / dmag, dist[2] / dmag};
+  const double overlap_n = (rl + ri) - dmag;
+  const double dcl = (dmag * dmag + rl * rl - ri * ri) / (2.0 * dmag);
+  const double dci = dmag - dcl;
+  const double osum[3] = {wl.x * dcl + wi.x * dci, wl.y * dcl + wi.y * dci, wl.z * dcl + wi.z * dci};
+  const double vrel[3] = {vl.x - vi.x + (osum[1] * nrm[2] - osum[2] * nrm[1]),
+                          vl.y - vi.y + (osum[2] * nrm[0] - osum[0] * nrm[2]),
+                          vl.z - vi.z + (osum[0] * nrm[1] - osum[1] * nrm[0])};
+  const double vrn = vrel[0] * nrm[0] + vrel[1] * nrm[1] + vrel[2] * nrm[2];
+  const double vt[3] = {vrel[0] - vrn * nrm[0], vrel[1] - vrn * nrm[1], vrel[2] - vrn * nrm[2]};
+  const double rad_eff = (rl * ri) / (rl + ri);
+  const double m_eff = (vl.w * vi.w) / (vl.w + vi.w);
+  double kn, kt, etan, etat;
+  if (COLL == DEM_COLL_HERTZ) {
+    double so = sqrt(overlap_n);
+    kn = p.hkn[ix] * so * sqrt(rad_eff);
+    kt = p.hkt[ix] * so * sqrt(rad_eff);
+    so = sqrt(so);
+    etan = p.etan[ix] * so * sqrt(p.hkn[ix] * sqrt(rad_eff) * m_eff);
+    etat = p.etat[ix] * so * sqrt(p.hkt[ix] * sqrt(rad_eff) * m_eff);
+  } else {
+    kn = p.kn; kt = p.kt;
+    etan = p.etan[ix] * sqrt(m_eff);
+    etat = p.etat[ix] * sqrt(m_eff);
+  }
+  double fn2 = 0.0, ft2 = 0.0, ot2 = 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double fn = -(kn * overlap_n * nrm[c] + etan * vrn * nrm[c]);
+    const double ot = p.dt * vt[c] + pin[c];
+    const double ft = -kt * ot - etat * vt[c];
+    fn2 += fn * fn;
+    ot2 += ot * ot;
+    ft2 += ft * ft;
+  }
+  if (!(ot2 > 0.0)) return false;
+  return sqrt(ft2) > p.mew * sqrt(fn2);
+}
+
+// FIX false: the pair kernel's evaluation, the onset of slip decided in
+// FP32 and o.near set near its threshold; FIX true: the same evaluation
+// with the onset of slip decided by slip_fp64 (k_slip_fix).
+template <int COLL, bool FIX>
 __device__ __forceinline__ void split_contact(const DevParams& p, const double4& xl, const double4& vl,
                                               const double4& wl, int phl, const double4& xi, const double4& vi,
                                               const double4& wi, int phi, const double dist[3], double d2,
@@ -106,13 +163,22 @@ __device__ __forceinline__ void split_contact(const DevParams& p, const double4&
   const float o32[3] = {(float)ot[0], (float)ot[1], (float)ot[2]};
   const float mag2 = o32[0] * o32[0] + o32[1] * o32[1] + o32[2] * o32[2];
   float ft[3] = {0.f, 0.f, 0.f};
+  o.near = false;
   if (mag2 > 0.f) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) ft[c] = -kt * o32[c] - etat * vt[c];
     const float ft2 = ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2];
     const float fn2 = fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2];
     // |Ft| > MEW*|Fn|, compared squared
-    if (ft2 > p.mew32 * p.mew32 * fn2) {
+    const float thr = p.mew32 * p.mew32 * fn2;
+    bool slip;
+    if (FIX) {
+      slip = slip_fp64<COLL>(p, xl, vl, wl, xi, vi, wi, ix, dist, d2, pin);
+    } else {
+      slip = ft2 > thr;
+      o.near = fabsf(ft2 - thr) <= 1e-4f * thr;
+    }
+    if (slip) {
       // Coulomb slip: Ft = -MEW*|Fn| t, history (MEW*|Fn|/KT) t, t = ot/|ot|
       const float fnmd = p.mew32 * sqrtf(fn2);
       const float im = rsqrtf(mag2);
@@ -139,6 +205,20 @@ struct Rec32 {
   float4 a, b;
 };
 
+// The owner's record of a contact at its pair index, the neighbour's at its
+// incoming slot.
+__device__ __forceinline__ void put_records(const PairTerms& o, long long cc, const int* __restrict__ in_pos,
+                                            Rec32* __restrict__ rec_own, Rec32* __restrict__ rec_in) {
+  const float rol = o.kn * o.ov;
+  Rec32 ro, ri;
+  ro.a = make_float4(o.fc[0], o.fc[1], o.fc[2], rol);
+  ro.b = make_float4(o.dcl2 * o.tf[0], o.dcl2 * o.tf[1], o.dcl2 * o.tf[2], 0.f);
+  ri.a = make_float4(-o.fc[0], -o.fc[1], -o.fc[2], rol);
+  ri.b = make_float4(o.dci2 * o.tf[0], o.dci2 * o.tf[1], o.dci2 * o.tf[2], 0.f);
+  rec_own[cc] = ro;
+  rec_in[in_pos[cc]] = ri;
+}
+
 // Kernel 1 (per pair): one CC iteration of CALC_FORCE_DEM, evaluated once.
 // A pair that the build's gap and the displacement bound since prove apart
 // (history zero) is skipped after reading its flag and gap.  Four
@@ -152,7 +232,7 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
               const uint8_t* __restrict__ phase, double* __restrict__ pft, uint8_t* __restrict__ pflag,
               uint8_t* __restrict__ in_flag, uint8_t* __restrict__ touched, const float* __restrict__ pgap,
               const double* __restrict__ skin, Rec32* __restrict__ rec_own, Rec32* __restrict__ rec_in,
-              DevErr* __restrict__ err) {
+              SlipFix* __restrict__ fix, DevErr* __restrict__ err) {
   const long long np = min((long long)*d_np, cap);
   const long long stride = (long long)gridDim.x * blockDim.x;
   // the bound in FP32, rounded up: a pair is skipped only when its gap
@@ -235,16 +315,19 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
             PairTerms o;
             // one solids phase: no phase to look up
             const int phl = p.nph > 1 ? phase[ll] : 0, phi = p.nph > 1 ? phase[i] : 0;
-            split_contact<COLL>(p, a, va, wa, phl, b, vb, wb, phi, dist, d2, r_lm * r_lm - d2, pin, ot, o);
-            po[0] = ot[0]; po[1] = ot[1]; po[2] = ot[2];
-            const float rol = o.kn * o.ov;
-            Rec32 ro, ri;
-            ro.a = make_float4(o.fc[0], o.fc[1], o.fc[2], rol);
-            ro.b = make_float4(o.dcl2 * o.tf[0], o.dcl2 * o.tf[1], o.dcl2 * o.tf[2], 0.f);
-            ri.a = make_float4(-o.fc[0], -o.fc[1], -o.fc[2], rol);
-            ri.b = make_float4(o.dci2 * o.tf[0], o.dci2 * o.tf[1], o.dci2 * o.tf[2], 0.f);
-            rec_own[cc] = ro;
-            rec_in[in_pos[cc]] = ri;
+            split_contact<COLL, false>(p, a, va, wa, phl, b, vb, wb, phi, dist, d2, r_lm * r_lm - d2, pin, ot, o);
+            // near the onset of slip k_slip_fix evaluates the contact again,
+            // from the history as it was (left in place here)
+            bool deferred = false;
+            if (o.near) {
+              const unsigned t = atomicAdd(&fix->count, 1u);
+              if (t < (unsigned)SLIP_FIX_CAP) {
+                fix->pair[t] = 2 * cc + ((f0 & PF_HIST) ? 1 : 0);
+                deferred = true;
+              }
+            }
+            if (!deferred) { po[0] = ot[0]; po[1] = ot[1]; po[2] = ot[2]; }
+            put_records(o, cc, in_pos, rec_own, rec_in);
             touched[ll] = 1;
             touched[i] = 1;
             f = PF_CONTACT | ((ot[0] != 0.0 || ot[1] != 0.0 || ot[2] != 0.0) ? PF_HIST : 0);
@@ -267,6 +350,51 @@ k_pairs_split(DevParams p0, BatchView bv, const int* __restrict__ d_np, long lon
     if (ncont) atomicAdd(&err->n_contacts, ncont);
     if (eflags) atomicOr(&err->flags, eflags);
   }
+}
+
+// The contacts k_pairs_split left near the onset of slip, evaluated again
+// with the onset decided in FP64 (slip_fp64): history, flag and both
+// records rewritten.  Their history is still the one the pair kernel read.
+// One block; it clears the count for the next pair pass when done.
+template <int COLL, bool B>
+__global__ void __launch_bounds__(128)
+k_slip_fix(DevParams p0, BatchView bv, SlipFix* __restrict__ fix, const int* __restrict__ owner,
+           const int* __restrict__ nbrs, const int* __restrict__ in_pos, const double4* __restrict__ pos4,
+           const double4* __restrict__ vel4, const double4* __restrict__ omg4, const uint8_t* __restrict__ phase,
+           double* __restrict__ pft, uint8_t* __restrict__ pflag, Rec32* __restrict__ rec_own,
+           Rec32* __restrict__ rec_in) {
+  const unsigned n = min(fix->count, (unsigned)SLIP_FIX_CAP);
+  for (unsigned t = threadIdx.x; t < n; t += blockDim.x) {
+    const long long code = fix->pair[t];
+    const long long cc = code >> 1;
+    const int ll = owner[cc], i = nbrs[cc];
+    const DevParams& p = sysp<B>(p0, bv, ll);
+    const double4 a = pos4[ll], b = pos4[i];
+    const double xl[3] = {a.x, a.y, a.z}, xi[3] = {b.x, b.y, b.z};
+    double dist[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double pj = xi[c];
+      const double s = periodic_shift(p, c, pj - xl[c]);
+      if (s != 0.0) pj = pj + s;
+      dist[c] = pj - xl[c];
+    }
+    const double r_lm = a.w + b.w;
+    const double d2 = dist[0] * dist[0] + dist[1] * dist[1] + dist[2] * dist[2];
+    const double4 va = vel4[ll], vb = vel4[i], wa = omg4[ll], wb = omg4[i];
+    double* po = pft + 3 * cc;
+    double pin[3] = {0.0, 0.0, 0.0};
+    if (code & 1) { pin[0] = po[0]; pin[1] = po[1]; pin[2] = po[2]; }
+    const int phl = p.nph > 1 ? phase[ll] : 0, phi = p.nph > 1 ? phase[i] : 0;
+    double ot[3];
+    PairTerms o;
+    split_contact<COLL, true>(p, a, va, wa, phl, b, vb, wb, phi, dist, d2, r_lm * r_lm - d2, pin, ot, o);
+    po[0] = ot[0]; po[1] = ot[1]; po[2] = ot[2];
+    put_records(o, cc, in_pos, rec_own, rec_in);
+    pflag[cc] = PF_CONTACT | ((ot[0] != 0.0 || ot[1] != 0.0 || ot[2] != 0.0) ? PF_HIST : 0);
+  }
+  __syncthreads();  // every thread has read the count
+  if (threadIdx.x == 0) fix->count = 0;
 }
 
 // Contact bits (PF_CONTACT, bit 0 of each flag byte) of flags[base,
@@ -390,7 +518,11 @@ static void launch_pairs_split_t(dem_handle* h) {
   k_pairs_split<COLL, B><<<(unsigned)(h->n_sm * h->tune.pair_bpsm), T, 0, h->stream>>>(
       h->dp, h->bview(), h->d_np, h->pair_cap, h->pair_owner, h->nbrs[h->rb], h->in_pos, h->pos4[c], h->vel4[c],
       h->omg4[c], h->state, h->phase, h->pft[h->pcur], h->pflag(), h->in_flag, h->touched, h->pgap, h->skin,
-      rec_own_of(h), rec_in_of(h), h->derr);
+      rec_own_of(h), rec_in_of(h), h->slipfix, h->derr);
+  DEM_LAUNCH(h);
+  k_slip_fix<COLL, B><<<1, 128, 0, h->stream>>>(h->dp, h->bview(), h->slipfix, h->pair_owner, h->nbrs[h->rb],
+                                                h->in_pos, h->pos4[c], h->vel4[c], h->omg4[c], h->phase,
+                                                h->pft[h->pcur], h->pflag(), rec_own_of(h), rec_in_of(h));
   DEM_LAUNCH(h);
 }
 
