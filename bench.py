@@ -699,10 +699,9 @@ def run_ours(args):
                              "force_rel_error_first_last": other["force_error"],
                              "force_error_note": ("max over particles and components of |F_split - F_fp64| / "
                                                   "max |F_fp64| on one state, before and after the timed "
-                                                  "steps; the friction law turns the tangential force at "
-                                                  "the onset of slip (calc_force_dem.f:330-342), so a "
-                                                  "contact within FP32 rounding of that threshold takes "
-                                                  "the other branch and can set the max alone"),
+                                                  "steps; contacts within 1e-4 of the onset of slip, where "
+                                                  "the friction law turns the tangential force "
+                                                  "(calc_force_dem.f:330-342), take the FP64 test's branch"),
                              "contacts_last_step": other["contacts"], "rebuilds_timed": other["rebuilds_timed"],
                              "rebuilds_timed_from_candidate_list": other["rebuilds_timed_filtered"],
                              "roofline": other["roofline"], "gpu_launches": other["launches"],
